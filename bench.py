@@ -1,0 +1,465 @@
+"""Benchmark of the B200 mesh-adaptation pass (libosh_b200.so).
+
+Workload: the 48^3 unit-cube box (663,552 tets, 6 per hex), interior
+vertices perturbed by up to 0.1 h0, isotropic size h(x) = 0.01 + 0.04 |x - c|
+with c drawn from the seeded stream, adapted by mesh_adapt(1/3, 0.3, 4, 50)
+to convergence. A step is one full mesh_adapt of that input.
+
+Metric: adapted tets/s = (elements entering every pass that changed the mesh,
+summed) / (time of those adapt calls). `value` times K steps back to back on
+meshes already resident in HBM (one prepared copy per step), with CUDA events
+on the stream the library launches on, bracketed by a barrier and a device
+synchronise. `e2e` times the same work through the C ABI from pinned host
+buffers: osh_new / osh_build_ents / fields / labels uploaded, osh_adapt, and
+the adapted tets and coordinates read back, every step.
+
+--impl reference times the reference's own OpenMP build (compiled from its
+sources by oracle/Makefile) on the host cores, on the same workload.
+
+Multi-GPU: one mesh per rank (replicas only; a single mesh does not shard);
+value = all ranks' tets / max-over-ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import signal
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "adapted tets/s per refine+coarsen+swap pass"
+UNIT = "tets/s"
+N_BOX = 48
+H0, H1 = 0.01, 0.04
+SIZE_FLOOR, GOOD_QUAL, NLAYERS, MAX_OPS = 1.0 / 3.0, 0.3, 4, 50
+L2_BYTES = 126 * 2 ** 20
+
+
+def workload_config():
+    return {"workload": "box48_radial_size_mesh_adapt", "box_n": N_BOX,
+            "tets_in": 6 * N_BOX ** 3, "size_field": "0.01+0.04|x-c|, c~U[0.3,0.7]^3 seed 0",
+            "adapt": "mesh_adapt(1/3, 0.3, 4, 50)", "parallelism": "replicas",
+            "l2": "inputs larger than L2: each step adapts its own resident copy and "
+                  "grows it to ~2.3M tets (>500 MB of connectivity and adjacency)"}
+
+
+def measured_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, device):
+        self.p = None
+        try:
+            self.p = subprocess.Popen(
+                ["nvidia-smi", "-i", str(device),
+                 "--query-gpu=clocks.sm,clocks.max.sm,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.send_signal(signal.SIGTERM)
+        try:
+            out, _ = self.p.communicate(timeout=5)
+        except Exception:
+            self.p.kill()
+            out, _ = self.p.communicate()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx = float(parts[1])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[3:7]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing (replicas)
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------------------
+# our arm
+
+def build_input(G):
+    """The config's classified full-topology box with its size field, on the
+    GPU (input preparation, not timed)."""
+    coords, conn, center = G.box(N_BOX, 0, 0.1)
+    m = G.Mesh.reduced(3, coords, conn)
+    m.derive_model_full()
+    d = coords.reshape(-1, 3) - center
+    h = H0 + H1 * np.sqrt(d[:, 0] * d[:, 0] + d[:, 1] * d[:, 1] + d[:, 2] * d[:, 2])
+    m.add_field(0, "adapt_size", h)
+    return m
+
+
+def host_input(m):
+    """Host copies of everything the C API needs to rebuild the input."""
+    snap = m.snapshot()
+    arrays = {"conn": {d: np.ascontiguousarray(snap.conn[d]) for d in snap.conn},
+              "counts": snap.counts, "tags": {}}
+    for d in range(4):
+        arrays["tags"][d] = [(t.name, t.type, t.ncomps, t.transfer,
+                              np.ascontiguousarray(t.data)) for t in snap.tags[d]]
+    return arrays
+
+
+def pin(a):
+    """A page-locked copy of a numpy array (cudaHostAlloc through torch)."""
+    import torch
+    t = torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
+    return t
+
+
+def e2e_step(G, L, inp, stream_ptr):
+    """One adapt through the public C ABI from pinned host buffers."""
+    h2d = 0
+    m = L.osh_new(3)
+    G.check()
+    L.osh_b200_set_stream(m, C.c_void_p(stream_ptr))
+    G.check()
+    nv = inp["counts"][0]
+    L.osh_build_ents(m, 0, nv)
+    for d in (1, 2, 3):
+        arr = inp["pinned_conn"][d]
+        p = L.osh_build_ents(m, d, inp["counts"][d])
+        L.osh_b200_copy_to_device(p, C.c_void_p(arr.data_ptr()), arr.numel() * 4)
+        h2d += arr.numel() * 4
+    for d in range(4):
+        for (name, ty, nc, tr, _), arr in zip(inp["tags"][d], inp["pinned_tags"][d]):
+            if ty == G.T_F64:
+                p = L.osh_new_field(m, d, name.encode(), nc, tr)
+            else:
+                p = L.osh_new_label(m, d, name.encode(), nc)
+            nbytes = arr.numel() * arr.element_size()
+            L.osh_b200_copy_to_device(p, C.c_void_p(arr.data_ptr()), nbytes)
+            h2d += nbytes
+    G.check()
+    L.osh_adapt(m, SIZE_FLOOR, GOOD_QUAL, NLAYERS, MAX_OPS)
+    G.check()
+    passes, elems = C.c_uint(), C.c_double()
+    L.osh_b200_adapt_stats(C.byref(passes), C.byref(elems))
+    nt = L.osh_count(m, 3)
+    nvo = L.osh_count(m, 0)
+    out_conn = np.empty(nt * 4, np.uint32)
+    out_x = np.empty(nvo * 3, np.float64)
+    L.osh_b200_copy_to_host(out_conn.ctypes.data_as(C.c_void_p), L.osh_down(m, 3, 0),
+                            out_conn.nbytes)
+    L.osh_b200_copy_to_host(out_x.ctypes.data_as(C.c_void_p), L.osh_coords(m), out_x.nbytes)
+    G.check()
+    d2h = out_conn.nbytes + out_x.nbytes
+    L.osh_free(m)
+    return elems.value, h2d, d2h
+
+
+def run_ours(args, world, rank, local):
+    import torch
+    import omega_h_v1_b200 as G
+    torch.cuda.set_device(local)
+    L = G.lib()
+    # the library works on the legacy default stream here, so events recorded
+    # on it bracket every launch and copy of the timed region
+    stream = torch.cuda.default_stream()
+    stream_ptr = 0
+    base = build_input(G)
+    tets_in = base.count(3)
+    nsteps = args.warmup + args.steps
+    # one resident copy per step, prepared before timing
+    copies = []
+    for _ in range(nsteps):
+        h = L.osh_b200_clone(base.h)
+        G.check()
+        L.osh_b200_set_stream(h, C.c_void_p(stream_ptr))
+        copies.append(h)
+    torch.cuda.synchronize()
+    elems = []
+
+    def adapt(h):
+        L.osh_adapt(h, SIZE_FLOOR, GOOD_QUAL, NLAYERS, MAX_OPS)
+        G.check()
+        passes, e = C.c_uint(), C.c_double()
+        L.osh_b200_adapt_stats(C.byref(passes), C.byref(e))
+        return e.value, passes.value
+
+    for i in range(args.warmup):
+        adapt(copies[i])
+        L.osh_free(copies[i])
+    torch.cuda.synchronize()
+    # the probe of the dominant kernel runs live inside the timed region
+    probe_id = args.probe
+    L.osh_b200_probe_reset()
+    L.osh_b200_probe_enable(1 << probe_id)
+    launches0 = L.osh_b200_launch_count()
+    clocks = Clocks(local)
+    barrier(world)
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    npass = []
+    for i in range(args.warmup, nsteps):
+        e, p = adapt(copies[i])
+        elems.append(e)
+        npass.append(p)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    clk = clocks.stop()
+    launches = L.osh_b200_launch_count() - launches0
+    L.osh_b200_probe_enable(0)
+    ms_local = ev0.elapsed_time(ev1)
+    plaunch, pms, pbytes = C.c_uint(), C.c_double(), C.c_double()
+    L.osh_b200_probe_read(probe_id, C.byref(plaunch), C.byref(pms), C.byref(pbytes))
+    for i in range(args.warmup, nsteps):
+        L.osh_free(copies[i])
+    ms = max_over_ranks(ms_local, world)
+    units = sum_over_ranks(float(sum(elems)), world)
+    value = units / (ms / 1e3)
+
+    e2e = None
+    if not args.no_e2e:
+        e2e = e2e_leg(G, L, base, args, world, stream, stream_ptr)
+    peak, peak_kind = measured_peak()
+    roof = None
+    if plaunch.value:
+        avg_ms = pms.value / plaunch.value
+        avg_bytes = pbytes.value / plaunch.value
+        achieved = avg_bytes / (avg_ms / 1e3) / 1e9
+        roof = {"bound": "hbm", "kernel": L.osh_b200_probe_name(probe_id).decode(),
+                "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "peak_source": peak_kind,
+                "launches": plaunch.value, "avg_launch_us": round(avg_ms * 1e3, 2),
+                "algorithmic_bytes_per_launch": round(avg_bytes),
+                "traffic": args.traffic}
+    base.close()
+    return {
+        "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded 48^3 box, radial size field)",
+        "config": workload_config(),
+        "roofline": roof,
+        "e2e": e2e,
+        "gpu_launches": int(launches),
+        "clocks": clk,
+        "tets_in": tets_in,
+        "passes_per_step": npass[0] if npass else None,
+    }
+
+
+def e2e_leg(G, L, base, args, world, stream, stream_ptr):
+    """End to end through the C ABI from pinned host memory."""
+    import torch
+    inp = host_input(base)
+    inp["pinned_conn"] = {d: pin(inp["conn"][d]) for d in (1, 2, 3)}
+    inp["pinned_tags"] = {d: [pin(t[4]) for t in inp["tags"][d]] for d in range(4)}
+    for _ in range(max(1, min(args.warmup, 1))):
+        e2e_step(G, L, inp, stream_ptr)
+    torch.cuda.synchronize()
+    barrier(world)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    e_units, h2d, d2h = 0.0, 0, 0
+    for _ in range(args.steps):
+        u, a, b = e2e_step(G, L, inp, stream_ptr)
+        e_units += u
+        h2d, d2h = a, b
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    e_ms = max_over_ranks(e0.elapsed_time(e1), world)
+    e_units = sum_over_ranks(e_units, world)
+    return {"value": round(e_units / (e_ms / 1e3), 1), "unit": UNIT,
+            "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+            "ms_per_step": round(e_ms / args.steps, 3)}
+
+
+# ---------------------------------------------------------------------------
+# CPU arms (reference build of the same path)
+
+class _Quiet:
+    """Silence the reference's printf output on fd 1 while it runs."""
+
+    def __enter__(self):
+        sys.stdout.flush()
+        self.saved = os.dup(1)
+        self.null = os.open(os.devnull, os.O_WRONLY)
+        os.dup2(self.null, 1)
+
+    def __exit__(self, *a):
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+        os.close(self.null)
+
+
+def cpu_reference_run(nsteps_total, ntimed):
+    """Times the reference's OpenMP build of mesh_adapt on the workload:
+    returns (tets/s, cores, sample description, ms per step)."""
+    from oracle import oracle as O
+    if not O.have_reference():
+        return None
+    coords, conn, center = O.box(N_BOX, 0, 0.1)
+    h = O.radial_size(coords, center, H0, H1)
+    lib = O._lib(O.REF_OMP_SO, "refd_").lib
+    lib.refd_adapt_counted.restype = C.c_uint
+    lib.refd_adapt_counted.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_uint,
+                                       C.c_uint, C.POINTER(C.c_uint), C.POINTER(C.c_double)]
+
+    def fresh():
+        m = O.Reference(3, coords, conn)
+        m.derive_model_full()
+        m.add_field(0, "adapt_size", h)
+        return m
+
+    # pass count and elements entering them (untimed)
+    m = fresh()
+    passes, elems = C.c_uint(), C.c_double()
+    with _Quiet():
+        lib.refd_adapt_counted(m.h, SIZE_FLOOR, GOOD_QUAL, NLAYERS, MAX_OPS,
+                               C.byref(passes), C.byref(elems))
+    m.close()
+    times = []
+    for i in range(nsteps_total):
+        m = fresh()
+        with _Quiet():
+            t0 = time.perf_counter()
+            m.adapt(SIZE_FLOOR, GOOD_QUAL, NLAYERS, MAX_OPS)
+            t1 = time.perf_counter()
+        m.close()
+        if i >= nsteps_total - ntimed:
+            times.append(t1 - t0)
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    t = float(sum(times))
+    return (elems.value * len(times) / t, cores,
+            "%d full mesh_adapt runs of the 48^3 workload (%d passes, %.0f tets in)"
+            % (len(times), passes.value, elems.value), 1e3 * t / len(times))
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return None
+    r = cpu_reference_run(args.warmup + args.steps, args.steps)
+    if r is None:
+        return {"impl": "reference", "unavailable": "reference library not built "
+                "(oracle/_ref missing; run __graft_entry__.build() where the reference is)"}
+    value, cores, sample, ms = r
+    return {"impl": "reference", "metric": METRIC, "value": round(value, 1), "unit": UNIT,
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(ms, 3), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded 48^3 box, radial size field)",
+            "config": workload_config(),
+            "cpu_baseline": {"value": round(value, 1), "unit": UNIT, "cores": cores,
+                             "kind": "reference", "sample": sample},
+            "e2e": {"value": round(value, 1), "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--probe", type=int, default=int(os.environ.get("OSH_BENCH_PROBE", "0")),
+                    help="probe id of the kernel whose roofline is reported")
+    ap.add_argument("--traffic", type=float, default=None,
+                    help="DRAM bytes per launch of that kernel from an ncu capture")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling)")
+    args = ap.parse_args()
+    world, rank, local = dist_setup()
+    if args.impl == "reference":
+        out = run_reference(args, world, rank)
+        if rank == 0:
+            print(json.dumps(out), flush=True)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
+    out = run_ours(args, world, rank, local)
+    if rank == 0:
+        if not args.no_cpu:
+            r = cpu_reference_run(1, 1)
+            if r is not None:
+                v, cores, sample, _ = r
+                out["cpu_baseline"] = {"value": round(v, 1), "unit": UNIT, "cores": cores,
+                                       "kind": "reference", "sample": sample}
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

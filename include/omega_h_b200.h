@@ -1,0 +1,151 @@
+/*
+ * omega_h_b200.h -- entry points of libosh_b200.so beyond the public
+ * omega_h.h. They expose the reference's internal C++ entry points for the
+ * adaptation pass (C linkage here) plus the helpers a caller needs with a
+ * device-resident mesh. All mesh arrays are device memory; arguments named
+ * host_* are host memory.
+ */
+#ifndef OMEGA_H_B200_H
+#define OMEGA_H_B200_H
+
+#include <stddef.h>
+
+#include "omega_h.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- error reporting (the reference asserts / aborts instead) ---------- */
+enum osh_b200_error {
+  OSH_B200_OK = 0,
+  OSH_B200_E_CUDA = 1,
+  OSH_B200_E_NOCONVERGE = 2, /* independent set not settled in 100 rounds */
+  OSH_B200_E_MAXOPS = 3,     /* mesh_adapt exceeded max_passes */
+  OSH_B200_E_ARG = 4,
+  OSH_B200_E_NOMEM = 5,
+  OSH_B200_E_UNSUPPORTED = 6,
+  OSH_B200_E_TIMEOUT = 7,
+  OSH_B200_E_INVERTED = 8
+};
+int osh_b200_last_error(void) OSH_PUBLIC;
+char const* osh_b200_last_error_message(void) OSH_PUBLIC;
+void osh_b200_clear_error(void) OSH_PUBLIC;
+
+/* ---- the adaptation passes (reference C++ entry points) ---------------- */
+/* refine_by_size (refine.hpp:8, refine.cpp:17-27) */
+unsigned osh_b200_refine_by_size(osh_t m, double qual_floor) OSH_PUBLIC;
+/* uniformly_refine (refine.hpp:9, refine.cpp:29-35) */
+void osh_b200_uniformly_refine(osh_t m) OSH_PUBLIC;
+/* coarsen_by_size (coarsen.hpp:8-11, coarsen.cpp:23-36) */
+unsigned osh_b200_coarsen_by_size(osh_t m, double qual_floor,
+    double size_ratio_floor) OSH_PUBLIC;
+/* coarsen_slivers (coarsen.hpp:13-16, coarsen.cpp:51-70) */
+unsigned osh_b200_coarsen_slivers(osh_t m, double qual_floor,
+    unsigned nlayers) OSH_PUBLIC;
+/* swap_slivers (swap.hpp:8-11, swap.cpp:138-154) */
+unsigned osh_b200_swap_slivers(osh_t m, double good_qual,
+    unsigned nlayers) OSH_PUBLIC;
+/* mesh_adapt (adapt.hpp:8-12, adapt.cpp:82-94); same as osh_adapt */
+unsigned osh_b200_mesh_adapt(osh_t m, double size_ratio_floor,
+    double good_qual, unsigned nsliver_layers, unsigned max_passes) OSH_PUBLIC;
+/* mesh_min_quality (quality.cpp:67-73), minimum over every element */
+double osh_b200_min_quality(osh_t m) OSH_PUBLIC;
+
+/* statistics of the last pass run on this thread: op (1 refine, 2 coarsen,
+   3 swap, 4 coarsen slivers), elements in / out, selected entities and
+   independent-set rounds */
+void osh_b200_last_pass(unsigned* op, unsigned* elems_in, unsigned* elems_out,
+    unsigned* nselected, unsigned* rounds) OSH_PUBLIC;
+
+/* ---- per-stage selections of one pass, without changing the mesh ------ */
+/* Layouts follow refine_by_size / coarsen_common / swap_common: every output
+   is a host array sized by the entity counts of the current mesh. */
+unsigned osh_b200_refine_sets(osh_t m, double qual_floor,
+    unsigned* host_cand, unsigned* host_good, double* host_quals,
+    unsigned* host_indset) OSH_PUBLIC;
+unsigned osh_b200_coarsen_sets(osh_t m, double qual_floor, double size_floor,
+    unsigned* host_codes_size, unsigned* host_codes_class,
+    unsigned* host_codes_qual, double* host_quals2, unsigned* host_cand,
+    double* host_col_qual, unsigned* host_indset,
+    unsigned* host_gen_vert) OSH_PUBLIC;
+unsigned osh_b200_swap_sets(osh_t m, double good_qual, unsigned nlayers,
+    unsigned* host_slivers, unsigned* host_cand, unsigned* host_interior,
+    unsigned* host_good, double* host_quals, unsigned* host_ring_sizes,
+    unsigned* host_indset) OSH_PUBLIC;
+
+/* ---- mesh construction -------------------------------------------------- */
+/* A reduced-representation mesh (elements only) from host arrays, with a
+   "coordinates" vertex field: new_mesh(dim, MESH_REDUCED, 0) +
+   mesh_set_ents + mesh_add_tag (mesh.cpp:56-66). */
+osh_t osh_b200_new_reduced(unsigned elem_dim, unsigned nverts,
+    double const* host_coords, unsigned nelems,
+    unsigned const* host_conn) OSH_PUBLIC;
+/* mesh_derive_model (derive_model.cpp:444-448) then mesh_set_rep(FULL) */
+void osh_b200_derive_model(osh_t m, double crease_angle) OSH_PUBLIC;
+/* mesh_make_parallel (mesh.cpp:320-327): single-rank global numbering */
+void osh_b200_make_parallel(osh_t m) OSH_PUBLIC;
+/* deep copy of a mesh on the same GPU (connectivity, fields, labels, global
+   numbers); derived adjacency is rebuilt on demand. No reference
+   counterpart: the reference copies meshes only through files. */
+osh_t osh_b200_clone(osh_t m) OSH_PUBLIC;
+
+/* n^3 hexahedra of the unit cube, each split into 6 tets like the
+   reference's single-cube box (tables.cpp:29-36); interior vertices moved by
+   up to pert/n per axis from a splitmix64 stream seeded with `seed`;
+   host_center receives the next three draws scaled to [0.3, 0.7]. */
+void osh_b200_box(unsigned n, unsigned long seed, double pert,
+    double* host_coords, unsigned* host_conn, double* host_center) OSH_PUBLIC;
+
+/* generic tags from host data: type 0 u8, 1 u32, 2 u64, 3 f64 (tag.hpp) */
+void osh_b200_add_tag(osh_t m, unsigned dim, char const* name, unsigned type,
+    unsigned ncomps, unsigned transfer, void const* host_data) OSH_PUBLIC;
+unsigned osh_b200_ntags(osh_t m, unsigned dim) OSH_PUBLIC;
+char const* osh_b200_tag_name(osh_t m, unsigned dim, unsigned i) OSH_PUBLIC;
+void osh_b200_tag_info(osh_t m, unsigned dim, unsigned i, unsigned* type,
+    unsigned* ncomps, unsigned* transfer) OSH_PUBLIC;
+void const* osh_b200_tag_data(osh_t m, unsigned dim, unsigned i) OSH_PUBLIC;
+void osh_b200_set_globals(osh_t m, unsigned dim,
+    unsigned long const* host_globals) OSH_PUBLIC;
+/* element dual (mesh_ask_dual, mesh.cpp:252-261), device array */
+unsigned const* osh_b200_dual(osh_t m) OSH_PUBLIC;
+/* element qualities and edge metric lengths into host arrays */
+void osh_b200_qualities(osh_t m, double* host_out) OSH_PUBLIC;
+void osh_b200_edge_lengths(osh_t m, double* host_out) OSH_PUBLIC;
+
+/* statistics of the last osh_adapt on this thread: passes that changed the
+   mesh and the elements entering them, summed */
+void osh_b200_adapt_stats(unsigned* passes, double* elems_in) OSH_PUBLIC;
+/* kernels launched by this library so far in the process */
+unsigned long long osh_b200_launch_count(void) OSH_PUBLIC;
+/* run all further work of mesh m on the CUDA stream `stream` (a
+   cudaStream_t; 0 is the legacy default stream); the caller keeps it alive */
+void osh_b200_set_stream(osh_t m, void* stream) OSH_PUBLIC;
+
+/* ---- per-kernel event probes (bench instrumentation) -------------------- */
+/* Bit i of mask enables probe i: each launch of that kernel is bracketed by
+   CUDA events on its stream and credited with its algorithmic bytes. */
+void osh_b200_probe_enable(unsigned mask) OSH_PUBLIC;
+void osh_b200_probe_reset(void) OSH_PUBLIC;
+unsigned osh_b200_probe_count(void) OSH_PUBLIC;
+char const* osh_b200_probe_name(unsigned id) OSH_PUBLIC;
+void osh_b200_probe_read(unsigned id, unsigned* launches, double* total_ms,
+    double* total_bytes) OSH_PUBLIC;
+
+/* ---- memory helpers ----------------------------------------------------- */
+void osh_b200_copy_to_host(void* host_dst, void const* dev_src, size_t bytes) OSH_PUBLIC;
+void osh_b200_copy_to_device(void* dev_dst, void const* host_src, size_t bytes) OSH_PUBLIC;
+void osh_b200_synchronize(osh_t m) OSH_PUBLIC;
+
+/* polygon triangulation table used by edge swapping (edge_swap.cpp:21-228):
+   per ring size 3..7, the triangles (3 ring-vertex ids each) of every
+   triangulation and its interior edges. Returns 0 for other sizes. */
+unsigned osh_b200_swap_table(unsigned ring_size, unsigned* ntri,
+    unsigned* nmesh, unsigned* nint, unsigned* host_tris,
+    unsigned* host_iedges) OSH_PUBLIC;
+
+#ifdef __cplusplus
+} /* extern "C" */
+#endif
+
+#endif

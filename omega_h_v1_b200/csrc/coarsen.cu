@@ -1,0 +1,732 @@
+// Edge collapse on sm_100a: coarsen_by_size / coarsen_slivers
+// (coarsen.cpp:13-70, coarsen_common.cpp:29-239, check_collapse_class.cpp,
+// coarsen_qualities.cpp:12-79, collapses_to_verts.cpp, collapses_to_ents.cpp,
+// coarsen_topology.cpp, coarsen_conserve.cpp, coarsen_fit.cpp, qr.cpp).
+#include "passes.hpp"
+
+namespace osh {
+
+__device__ inline u32 collapses(u32 code, u32 dir) { return (code >> dir) & 1u; }
+
+// coarsen_size_code (coarsen.cpp:13-21) fused with measure_edge
+__global__ void k_coarsen_size_codes(u32 ne, u32 const* __restrict__ voe,
+    double const* __restrict__ x, double const* __restrict__ h, double size_floor,
+    u32* __restrict__ codes, u32* any)
+{
+  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+  u32 c = 0;
+  if (i < ne) {
+    u32 a = voe[i * 2], b = voe[i * 2 + 1];
+    double xa[3], xb[3];
+    load3(x, a, xa);
+    load3(x, b, xb);
+    double len = sqrt(sqdist3(xb, xa));
+    double want = (h[a] + h[b]) / 2;
+    c = ((len / want) < size_floor) ? (u32)COLLAPSE_BOTH : (u32)DONT_COLLAPSE;
+    codes[i] = c;
+  }
+  if (__any_sync(0xffffffffu, c) && (threadIdx.x & 31) == 0) atomicOr(any, 1u);
+}
+
+// coarsen_sliver_code (coarsen.cpp:38-49)
+__global__ void k_coarsen_sliver_codes(u32 ne, u32 const* __restrict__ voe,
+    u32 const* __restrict__ marked, u32* __restrict__ codes, u32* any)
+{
+  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+  u32 c = 0;
+  if (i < ne) {
+    if (marked[voe[i * 2]]) c |= 1u;
+    if (marked[voe[i * 2 + 1]]) c |= 2u;
+    codes[i] = c;
+  }
+  if (__any_sync(0xffffffffu, c) && (threadIdx.x & 31) == 0) atomicOr(any, 1u);
+}
+
+// check_basic_edge_class (check_collapse_class.cpp:12-37)
+__global__ void k_check_basic_class(u32 ne, u32 const* __restrict__ voe,
+    u32 const* __restrict__ cdv, u32 const* __restrict__ cde, u32* __restrict__ codes)
+{
+  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= ne) return;
+  u32 code = codes[i];
+  if (code == DONT_COLLAPSE) return;
+  u32 c0 = cdv[voe[i * 2]], c1 = cdv[voe[i * 2 + 1]], ce = cde[i];
+  if (c0 == c1) {
+    if (c0 != ce) codes[i] = DONT_COLLAPSE;
+    return;
+  }
+  if (collapses(code, 0) && c0 != ce) code &= ~1u;
+  if (collapses(code, 1) && c1 != ce) code &= ~2u;
+  codes[i] = code;
+}
+
+// check_for_exposed_side (check_collapse_class.cpp:55-103)
+__global__ void k_check_exposed_sides(u32 ed, u32 ne, u32 const* __restrict__ u_offs,
+    u32 const* __restrict__ u_adj, u32 const* __restrict__ u_dirs,
+    u32 const* __restrict__ vot, u32 const* __restrict__ voe, u32 const* __restrict__ sot,
+    u32 const* __restrict__ cdt, u32 const* __restrict__ cds, u32* __restrict__ codes)
+{
+  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= ne) return;
+  u32 code = codes[i];
+  if (code == DONT_COLLAPSE) return;
+  u32 vpt = deg(ed, 0), spt = deg(ed, ed - 1);
+  for (u32 j = u_offs[i]; j < u_offs[i + 1]; ++j) {
+    u32 t = u_adj[j], dir = u_dirs[j];
+    u32 tcd = cdt[t];
+    for (u32 k = 0; k < 2; ++k) {
+      if (!collapses(code, k)) continue;
+      u32 va = voe[i * 2 + (1 - k)];
+      for (u32 l = 0; l < 2; ++l) {
+        u32 eev = canon(ed, 1, 0, dir, l);
+        if (vot[(size_t)t * vpt + eev] == va) {
+          u32 side = sot[(size_t)t * spt + opp(ed, 0, eev)];
+          if (cds[side] != tcd) code &= ~(1u << k);
+          break;
+        }
+      }
+    }
+  }
+  codes[i] = code;
+}
+
+// coarsen_quality (coarsen_qualities.cpp:12-79): worst element of the cavity
+// after collapsing each allowed direction
+__global__ void k_coarsen_quality(u32 dim, u32 ne, u32 const* __restrict__ voe1,
+    u32 const* __restrict__ voe, u32 const* __restrict__ ev_offs,
+    u32 const* __restrict__ ev, u32 const* __restrict__ ev_dirs,
+    double const* __restrict__ x, double const* __restrict__ eq, double floor_q,
+    u32* __restrict__ codes, double* __restrict__ out, u32* any)
+{
+  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+  u32 keep = 0;
+  if (i < ne) {
+    u32 code = codes[i];
+    if (code != DONT_COLLAPSE) {
+      u32 vpe = deg(dim, 0);
+      double const perfect = dim == 3 ? perfect_tet_quality() : perfect_tri_quality();
+      for (u32 j = 0; j < 2; ++j) {
+        if (!collapses(code, j)) continue;
+        double minq = 1, old_minq = 1;
+        u32 col = voe1[i * 2 + j], gen = voe1[i * 2 + 1 - j];
+        double ex[4][3];
+        load3(x, gen, ex[vpe - 1]);
+        for (u32 k = ev_offs[col]; k < ev_offs[col + 1]; ++k) {
+          u32 e = ev[k];
+          u32 const* ve = voe + (size_t)e * vpe;
+          if (eq && eq[e] < old_minq) old_minq = eq[e];
+          bool adjacent = false;
+          for (u32 l = 0; l < vpe; ++l)
+            if (ve[l] == gen) adjacent = true;
+          if (adjacent) continue;
+          u32 base = opp(dim, 0, ev_dirs[k]);
+          for (u32 l = 0; l + 1 < vpe; ++l) load3(x, ve[canon(dim, dim - 1, 0, base, l)], ex[l]);
+          double q = dim == 3 ? tet_quality(ex, perfect) : tri_quality(ex, 1, perfect);
+          if (q < minq) minq = q;
+        }
+        if (minq < floor_q || (eq && minq <= old_minq))
+          code &= ~(1u << j);
+        else
+          out[i * 2 + j] = minq;
+      }
+      codes[i] = code;
+      keep = code != DONT_COLLAPSE;
+    }
+  }
+  if (__any_sync(0xffffffffu, keep) && (threadIdx.x & 31) == 0) atomicOr(any, 1u);
+}
+
+// collapse_to_vert (collapses_to_verts.cpp:13-42)
+__global__ void k_collapses_to_verts(u32 nv, u32 const* __restrict__ ue_offs,
+    u32 const* __restrict__ ue, u32 const* __restrict__ ue_dirs,
+    u32 const* __restrict__ codes, double const* __restrict__ q2, u32* __restrict__ cand,
+    double* __restrict__ colq)
+{
+  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nv) return;
+  double maxq = 0;
+  u32 c = 0;
+  for (u32 j = ue_offs[i]; j < ue_offs[i + 1]; ++j) {
+    u32 e = ue[j], d = ue_dirs[j];
+    if (!collapses(codes[e], d)) continue;
+    double q = q2[e * 2 + d];
+    if (!c) {
+      c = 1;
+      maxq = q;
+    } else if (q > maxq) {
+      maxq = q;
+    }
+  }
+  cand[i] = c;
+  colq[i] = c ? maxq : 0.0;
+}
+
+// vertex_dest (collapses_to_verts.cpp:72-105): first edge in upward order
+// whose collapse quality equals the vertex's best
+__global__ void k_vertex_dest(u32 nv, u32 const* __restrict__ ue_offs,
+    u32 const* __restrict__ ue, u32 const* __restrict__ ue_dirs,
+    u32 const* __restrict__ voe1, u32 const* __restrict__ ind,
+    double const* __restrict__ colq, u32 const* __restrict__ codes,
+    double const* __restrict__ q2, u32* __restrict__ gen_vert)
+{
+  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nv) return;
+  u32 g = INV;
+  if (ind[i]) {
+    double maxq = colq[i];
+    if (maxq == 1e10) maxq = -1e10;
+    for (u32 j = ue_offs[i]; j < ue_offs[i + 1]; ++j) {
+      u32 e = ue[j], d = ue_dirs[j];
+      if (!collapses(codes[e], d)) continue;
+      double q = q2[e * 2 + d];
+      if (q == 1e10) q = -1e10;
+      if (q == maxq) {
+        g = voe1[e * 2 + (1 - d)];
+        break;
+      }
+    }
+  }
+  gen_vert[i] = g;
+}
+
+// collapse_to_ent (collapses_to_ents.cpp:11-64)
+__global__ void k_collapse_to_ent(u32 ed, u32 n, u32 const* __restrict__ voe,
+    u32 const* __restrict__ soe, u32 const* __restrict__ gen_offs_v,
+    u32 const* __restrict__ gen_vert_v, u32 const* __restrict__ fused_ents,
+    u32* __restrict__ is_same, u32* __restrict__ fused_sides, u32* __restrict__ will_gen,
+    u32* __restrict__ gen_vert, u32* __restrict__ gen_dir)
+{
+  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  u32 vpe = deg(ed, 0), spe = deg(ed, ed - 1);
+  u32 const* v = voe + (size_t)i * vpe;
+  u32 col = INV, dir = INV;
+  for (u32 j = 0; j < vpe; ++j)
+    if (gen_offs_v[v[j]] != gen_offs_v[v[j] + 1]) {
+      col = v[j];
+      dir = j;
+    }
+  u32 wg = 0;
+  if (dir == INV) {
+    is_same[i] = 1;
+    will_gen[i] = 0;
+    return;
+  }
+  is_same[i] = 0;
+  u32 gv = gen_vert_v[col], gd = INV;
+  for (u32 j = 0; j < vpe; ++j)
+    if (v[j] == gv) gd = j;
+  if (gd != INV) {
+    fused_sides[soe[(size_t)i * spe + opp(ed, 0, gd)]] = 1;
+  } else if (!(fused_ents && fused_ents[i])) {
+    wg = 1;
+    gen_vert[i] = gv;
+    gen_dir[i] = dir;
+  }
+  will_gen[i] = wg;
+}
+
+// coarsen_elem (coarsen_topology.cpp:9-34) writing straight into the new
+// connectivity after the same entities, with remap_conn applied
+// (coarsen_common.cpp:29-33)
+__global__ void k_coarsen_topology(u32 ed, u32 n, u32 const* __restrict__ voe,
+    u32 const* __restrict__ gen_offs, u32 const* __restrict__ gen_vert,
+    u32 const* __restrict__ gen_dir, u32 const* __restrict__ same_v,
+    u32* __restrict__ out)
+{
+  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n || gen_offs[i] == gen_offs[i + 1]) return;
+  u32 vpe = deg(ed, 0);
+  u32* o = out + (size_t)gen_offs[i] * vpe;
+  u32 b = opp(ed, 0, gen_dir[i]);
+  for (u32 j = 0; j + 1 < vpe; ++j)
+    o[j] = same_v[voe[(size_t)i * vpe + canon(ed, ed - 1, 0, b, j)]];
+  o[vpe - 1] = same_v[gen_vert[i]];
+}
+
+// expansion of the surviving entities' vertices, renumbered
+__global__ void k_same_conn(u32 n, u32 vpe, u32 const* __restrict__ voe,
+    u32 const* __restrict__ same_e, u32 const* __restrict__ same_v, u32* __restrict__ out)
+{
+  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n || same_e[i] == same_e[i + 1]) return;
+  u32 o = same_e[i];
+  for (u32 j = 0; j < vpe; ++j) out[(size_t)o * vpe + j] = same_v[voe[(size_t)i * vpe + j]];
+}
+
+// coarsen_conserve_cavity (coarsen_conserve.cpp:15-55)
+__global__ void k_coarsen_conserve(u32 nv, u32 nc, u32 nsame,
+    u32 const* __restrict__ gen_offs_v, u32 const* __restrict__ gen_offs_e,
+    u32 const* __restrict__ ev_offs, u32 const* __restrict__ ev,
+    double const* __restrict__ in, double const* __restrict__ sizes,
+    double* __restrict__ gen)
+{
+  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nv || gen_offs_v[i] == gen_offs_v[i + 1]) return;
+  u32 f = ev_offs[i], e = ev_offs[i + 1];
+  double sum[MAX_NCOMPS];
+  for (u32 c = 0; c < nc; ++c) sum[c] = 0;
+  for (u32 j = f; j < e; ++j)
+    for (u32 c = 0; c < nc; ++c) sum[c] = sum[c] + in[(size_t)ev[j] * nc + c];
+  double cav = 0;
+  for (u32 j = f; j < e; ++j) {
+    u32 el = ev[j];
+    if (gen_offs_e[el] == gen_offs_e[el + 1]) continue;
+    cav += sizes[gen_offs_e[el] + nsame];
+  }
+  for (u32 j = f; j < e; ++j) {
+    u32 el = ev[j];
+    if (gen_offs_e[el] == gen_offs_e[el + 1]) continue;
+    u32 ge = gen_offs_e[el];
+    double sc = sizes[ge + nsame] / cav;
+    for (u32 c = 0; c < nc; ++c) gen[(size_t)ge * nc + c] = sum[c] * sc;
+  }
+}
+
+// ---- least-squares linear fit (qr.cpp:42-205, coarsen_fit.cpp:17-86) ----
+__device__ inline double sgn(double x) { return (x < 0) ? -1 : 1; }
+
+__device__ u32 qr_decomp2(double (*a)[4], double (*q)[MAX_PTS], double (*r)[4], u32 npts)
+{
+  for (u32 i = 0; i < npts; ++i)
+    for (u32 j = 0; j < 4; ++j) r[i][j] = a[i][j];
+  for (u32 i = 0; i < npts; ++i)
+    for (u32 j = 0; j < npts; ++j) q[i][j] = (double)(i == j);
+  double v[MAX_PTS];
+  for (u32 i = 0; i < MAX_PTS; ++i) v[i] = 0;
+  u32 rank = 0;
+  for (u32 k = 0; k < 4; ++k) {
+    // get_reflector2
+    double cnorm = 0;
+    for (u32 i = k; i < npts; ++i) cnorm += r[i][k] * r[i][k];
+    cnorm = sqrt(cnorm);
+    if (cnorm < 1e-6) continue;
+    for (u32 i = 0; i < k; ++i) v[i] = 0;
+    for (u32 i = k; i < npts; ++i) v[i] = r[i][k];
+    v[k] += sgn(r[k][k]) * cnorm;
+    double rnorm = 0;
+    for (u32 i = k; i < npts; ++i) rnorm += v[i] * v[i];
+    rnorm = sqrt(rnorm);
+    for (u32 i = k; i < npts; ++i) v[i] /= rnorm;
+    // reflect_columns2 / reflect_rows2
+    for (u32 j = 0; j < 4; ++j) {
+      double dot = 0;
+      for (u32 i = k; i < npts; ++i) dot += r[i][j] * v[i];
+      for (u32 i = k; i < npts; ++i) r[i][j] -= 2 * dot * v[i];
+    }
+    for (u32 i = 0; i < npts; ++i) {
+      double dot = 0;
+      for (u32 j = k; j < npts; ++j) dot += q[i][j] * v[j];
+      for (u32 j = k; j < npts; ++j) q[i][j] -= 2 * dot * v[j];
+    }
+    ++rank;
+  }
+  return rank;
+}
+
+__device__ void qr_solve2(double (*q)[MAX_PTS], double (*r)[4], double const* b, u32 npts,
+    double* xo)
+{
+  double y[4];
+  for (u32 i = 0; i < 4; ++i) {
+    y[i] = 0;
+    for (u32 j = 0; j < npts; ++j) y[i] += q[j][i] * b[j];
+  }
+  for (u32 ii = 0; ii < 4; ++ii) {
+    u32 i = 4 - ii - 1;
+    xo[i] = y[i];
+    for (u32 j = i + 1; j < 4; ++j) xo[i] -= r[i][j] * xo[j];
+    xo[i] /= r[i][i];
+  }
+}
+
+__global__ void k_coarsen_fit(u32 nv, u32 nc, u32 nsame, u32 const* __restrict__ gen_offs_v,
+    u32 const* __restrict__ gen_offs_e, u32 const* __restrict__ ev_offs,
+    u32 const* __restrict__ ev, double const* __restrict__ oldx,
+    double const* __restrict__ newx, double const* __restrict__ in,
+    double* __restrict__ gen)
+{
+  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nv || gen_offs_v[i] == gen_offs_v[i + 1]) return;
+  u32 f = ev_offs[i], e = ev_offs[i + 1];
+  u32 npts = e - f;
+  if (npts > MAX_PTS) npts = MAX_PTS;
+  bool fit = npts >= 4;
+  double q[MAX_PTS][MAX_PTS];
+  double r[MAX_PTS][4];
+  if (fit) {
+    double a[MAX_PTS][4];
+    for (u32 j = 0; j < npts; ++j) {
+      u32 oe = ev[f + j];
+      a[j][0] = 1.0;
+      a[j][1] = oldx[oe * 3 + 0];
+      a[j][2] = oldx[oe * 3 + 1];
+      a[j][3] = oldx[oe * 3 + 2];
+    }
+    if (qr_decomp2(a, q, r, npts) < 4) fit = false;
+  }
+  for (u32 j = 0; j < nc; ++j) {
+    double b[MAX_PTS], c[4], avg = 0;
+    if (fit) {
+      for (u32 k = 0; k < npts; ++k) b[k] = in[(size_t)ev[f + k] * nc + j];
+      qr_solve2(q, r, b, npts, c);
+    } else {
+      avg = 0;
+      for (u32 k = f; k < e; ++k) avg += in[(size_t)ev[k] * nc + j];
+      avg /= (e - f);
+    }
+    for (u32 k = f; k < e; ++k) {
+      u32 oe = ev[k];
+      if (gen_offs_e[oe] == gen_offs_e[oe + 1]) continue;
+      u32 ge = gen_offs_e[oe];
+      if (fit) {
+        double const* nx = newx + (size_t)(ge + nsame) * 3;
+        double dd = 0;
+        dd += c[1] * nx[0];
+        dd += c[2] * nx[1];
+        dd += c[3] * nx[2];
+        gen[(size_t)ge * nc + j] = c[0] + dd;
+      } else {
+        gen[(size_t)ge * nc + j] = avg;
+      }
+    }
+  }
+}
+
+static void coarsen_transfer(Mesh& m, Mesh& out, u32 const* gen_offs_v,
+    u32 const* gen_offs_e, u32 const* same_e, u32 nsame, u32 ngen)
+{
+  cudaStream_t s = m.s;
+  u32 dim = m.dim, nv = m.count(0), ne = m.count(dim);
+  UpAdj const& ev = m.ask_up(0, dim);
+  bool any_f64 = false, any_fit = false;
+  for (auto const& t : m.tags[dim]) {
+    if (t.type == T_F64) any_f64 = true;
+    if (t.type == T_F64 && t.transfer == X_POINTWISE) any_fit = true;
+  }
+  if (any_f64) {
+    double* sizes = out.element_sizes();
+    for (auto const& t : m.tags[dim]) {
+      if (t.type != T_F64 || t.transfer != X_CONSERVE) continue;
+      u32 nc = t.ncomps;
+      if (nc > MAX_NCOMPS) throw Failure(E_ARG, "conserved field wider than 32");
+      double* data = dalloc<double>((size_t)(nsame + ngen) * nc, s);
+      expand_scaled(t.data, same_e, 1, ne, nc, 8, data, s);
+      if (nv) {
+        k_coarsen_conserve<<<grid_for(nv), BLOCK, 0, s>>>(nv, nc, nsame, gen_offs_v,
+            gen_offs_e, ev.offs, ev.adj, static_cast<double const*>(t.data), sizes,
+            data + (size_t)nsame * nc);
+        CK_LAUNCH();
+      }
+      out.add_tag(dim, T_F64, t.name.c_str(), nc, t.transfer, data);
+    }
+    dev_free(sizes, s);
+  }
+  if (!any_fit) return;
+  if (!m.find_tag(dim, "coordinates")) interp_coords_to_elems(m);
+  interp_coords_to_elems(out);
+  double const* oldx = static_cast<double const*>(m.find_tag(dim, "coordinates")->data);
+  double const* newx = static_cast<double const*>(out.find_tag(dim, "coordinates")->data);
+  for (auto const& t : m.tags[dim]) {
+    if (t.type != T_F64 || t.transfer != X_POINTWISE) continue;
+    u32 nc = t.ncomps;
+    double* data = dalloc<double>((size_t)(nsame + ngen) * nc, s);
+    expand_scaled(t.data, same_e, 1, ne, nc, 8, data, s);
+    if (nv) {
+      k_coarsen_fit<<<ceil_div(nv, 128), 128, 0, s>>>(nv, nc, nsame, gen_offs_v, gen_offs_e,
+          ev.offs, ev.adj, oldx, newx, static_cast<double const*>(t.data),
+          data + (size_t)nsame * nc);
+      CK_LAUNCH();
+    }
+    out.add_tag(dim, T_F64, t.name.c_str(), nc, t.transfer, data);
+  }
+}
+
+// check_coarsen_class + check_coarsen_quality + valid_collapses_to_verts +
+// the vertex independent set (coarsen_common.cpp:109-189). codes is updated
+// in place; returns false when no collapse survives.
+struct CoarsenSel {
+  double* q2 = nullptr;
+  u32* cand = nullptr;
+  double* colq = nullptr;
+  u32* ind = nullptr;
+  u32* gen_vert = nullptr;
+  void free(cudaStream_t s)
+  {
+    dev_free(q2, s);
+    dev_free(cand, s);
+    dev_free(colq, s);
+    dev_free(ind, s);
+    dev_free(gen_vert, s);
+  }
+};
+
+static bool coarsen_select(Mesh& m, u32* codes, double qual_floor, bool require_better,
+    CoarsenSel& sel, u32* codes_class_out, u32* codes_qual_out)
+{
+  cudaStream_t s = m.s;
+  u32 dim = m.dim, ne = m.count(1), nv = m.count(0);
+  Tag* cdv = m.find_tag(0, "class_dim");
+  Tag* cde = m.find_tag(1, "class_dim");
+  if (!cdv || !cde) throw Failure(E_ARG, "coarsening needs class_dim on every dimension");
+  u32 const* voe1 = m.ask_down(1, 0);
+  if (ne) {
+    k_check_basic_class<<<grid_for(ne), BLOCK, 0, s>>>(ne, voe1,
+        static_cast<u32 const*>(cdv->data), static_cast<u32 const*>(cde->data), codes);
+    CK_LAUNCH();
+  }
+  for (u32 ed = 2; ed <= dim; ++ed) {
+    UpAdj const& u = m.ask_up(1, ed);
+    Tag* cdt = m.find_tag(ed, "class_dim");
+    Tag* cds = m.find_tag(ed - 1, "class_dim");
+    if (!cdt || !cds) throw Failure(E_ARG, "coarsening needs class_dim on every dimension");
+    if (ne) {
+      k_check_exposed_sides<<<grid_for(ne), BLOCK, 0, s>>>(ed, ne, u.offs, u.adj, u.dirs,
+          m.ask_down(ed, 0), voe1, m.ask_down(ed, ed - 1),
+          static_cast<u32 const*>(cdt->data), static_cast<u32 const*>(cds->data), codes);
+      CK_LAUNCH();
+    }
+  }
+  if (codes_class_out)
+    CK(cudaMemcpyAsync(codes_class_out, codes, sizeof(u32) * ne, cudaMemcpyDeviceToDevice, s));
+  if (codes_qual_out)
+    CK(cudaMemcpyAsync(codes_qual_out, codes, sizeof(u32) * ne, cudaMemcpyDeviceToDevice, s));
+  if (!max_u32(codes, ne, s)) return false;
+  sel.q2 = dalloc<double>((size_t)ne * 2, s);
+  CK(cudaMemsetAsync(sel.q2, 0, sizeof(double) * ne * 2, s));
+  u32* any = m.mb->dev + 4;
+  CK(cudaMemsetAsync(any, 0, sizeof(u32), s));
+  if (dim >= 2) {
+    double const* eq = require_better ? m.qualities() : nullptr;
+    UpAdj const& ev = m.ask_up(0, dim);
+    if (ne) {
+      double nel = m.counts[dim];
+      PROBE(P_COARSEN_QUALITY, s, 4.0 * (nv + 1) + 8.0 * deg(dim, 0) * nel + 8.0 * ne +
+          4.0 * deg(dim, 0) * nel + 24.0 * nv + 8.0 * ne + 16.0 * ne);
+      k_coarsen_quality<<<grid_for(ne), BLOCK, 0, s>>>(dim, ne, voe1, m.ask_down(dim, 0),
+          ev.offs, ev.adj, ev.dirs, m.coords(), eq, qual_floor, codes, sel.q2, any);
+      CK_LAUNCH();
+    }
+  }
+  if (codes_qual_out)
+    CK(cudaMemcpyAsync(codes_qual_out, codes, sizeof(u32) * ne, cudaMemcpyDeviceToDevice, s));
+  if (!read_u32(any, s)) return false;
+  UpAdj const& ue = m.ask_up(0, 1);
+  sel.cand = dalloc<u32>(nv, s);
+  sel.colq = dalloc<double>(nv, s);
+  if (nv) {
+    k_collapses_to_verts<<<grid_for(nv), BLOCK, 0, s>>>(nv, ue.offs, ue.adj, ue.dirs, codes,
+        sel.q2, sel.cand, sel.colq);
+    CK_LAUNCH();
+  }
+  sel.ind = find_indset(m, 0, sel.cand, sel.colq);
+  sel.gen_vert = dalloc<u32>(nv, s);
+  if (nv) {
+    k_vertex_dest<<<grid_for(nv), BLOCK, 0, s>>>(nv, ue.offs, ue.adj, ue.dirs, voe1, sel.ind,
+        sel.colq, codes, sel.q2, sel.gen_vert);
+    CK_LAUNCH();
+  }
+  return true;
+}
+
+// coarsen_interior + coarsen_all_ents (coarsen_common.cpp:35-219)
+static void coarsen_build(Mesh& m, CoarsenSel const& sel)
+{
+  cudaStream_t s = m.s;
+  u32 dim = m.dim, nv = m.count(0);
+  u32* gen_offs_v = exscan_new(sel.ind, nv, s);
+  u32* same_v = negate_offsets(gen_offs_v, nv, s);
+  u32 nv_out = read_u32(same_v + nv, s);
+  last_pass_stats().nselected = nv - nv_out;
+  Mesh* out = m.spawn();
+  out->set_ents(0, nv_out, nullptr);
+  // tags_subset (subset.cpp:15-43): every vertex tag survives
+  for (auto const& t : m.tags[0]) {
+    u32 esz = tag_esz(t.type);
+    void* d = dev_alloc((size_t)nv_out * t.ncomps * esz, s);
+    expand_scaled(t.data, same_v, 1, nv, t.ncomps, esz, d, s);
+    out->add_tag(0, t.type, t.name.c_str(), t.ncomps, t.transfer, d);
+  }
+  if (m.parallel) inherit_globals(*out, 0, nv_out);
+  u32* fused[4] = {nullptr, nullptr, nullptr, nullptr};
+  for (u32 dd = 0; dd < dim; ++dd) {
+    u32 ed = dim - dd;
+    u32 n = m.count(ed), vpe = deg(ed, 0);
+    u32 const* voe = m.ask_down(ed, 0);
+    u32 const* soe = m.ask_down(ed, ed - 1);
+    u32 nsides = m.count(ed - 1);
+    fused[ed - 1] = dalloc<u32>(nsides, s);
+    CK(cudaMemsetAsync(fused[ed - 1], 0, sizeof(u32) * nsides, s));
+    u32* is_same = dalloc<u32>(n, s);
+    u32* will_gen = dalloc<u32>(n, s);
+    u32* gvert = dalloc<u32>(n, s);
+    u32* gdir = dalloc<u32>(n, s);
+    if (n) {
+      PROBE(P_COLLAPSE_TO_ENT, s, 4.0 * (vpe + deg(ed, ed - 1)) * n + 8.0 * (nv + 1) +
+          4.0 * n * 4 + 4.0 * nsides);
+      k_collapse_to_ent<<<grid_for(n), BLOCK, 0, s>>>(ed, n, voe, soe, gen_offs_v,
+          sel.gen_vert, fused[ed], is_same, fused[ed - 1], will_gen, gvert, gdir);
+      CK_LAUNCH();
+    }
+    u32* gen_offs = exscan_new(will_gen, n, s);
+    u32* same_e = exscan_new(is_same, n, s);
+    dev_free(will_gen, s);
+    dev_free(is_same, s);
+    CK(cudaMemcpyAsync(m.mb->dev + 16, gen_offs + n, sizeof(u32), cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemcpyAsync(m.mb->dev + 17, same_e + n, sizeof(u32), cudaMemcpyDeviceToDevice, s));
+    m.mb->fetch(s, 18);
+    u32 ngen = m.mb->host[16], nsame = m.mb->host[17];
+    u32 nout = nsame + ngen;
+    u32* conn = dalloc<u32>((size_t)nout * vpe, s);
+    if (n) {
+      k_same_conn<<<grid_for(n), BLOCK, 0, s>>>(n, vpe, voe, same_e, same_v, conn);
+      CK_LAUNCH();
+      k_coarsen_topology<<<grid_for(n), BLOCK, 0, s>>>(ed, n, voe, gen_offs, gvert, gdir,
+          same_v, conn + (size_t)nsame * vpe);
+      CK_LAUNCH();
+    }
+    dev_free(gvert, s);
+    dev_free(gdir, s);
+    out->set_ents(ed, nout, conn);
+    // setup_coarsen (inherit.cpp:140-157)
+    Doms d;
+    d.ndoms[0] = n;
+    d.offs[0] = same_e;
+    d.ngen[0] = nsame;
+    d.ndoms[ed] = n;
+    d.offs[ed] = gen_offs;
+    d.ngen[ed] = ngen;
+    d.finish();
+    inherit_class(m, *out, ed, d);
+    if (m.parallel) inherit_globals(*out, ed, nout);
+    if (ed == dim) coarsen_transfer(m, *out, gen_offs_v, gen_offs, same_e, nsame, ngen);
+    dev_free(gen_offs, s);
+    dev_free(same_e, s);
+  }
+  for (u32 d = 0; d < 4; ++d) dev_free(fused[d], s);
+  dev_free(gen_offs_v, s);
+  dev_free(same_v, s);
+  m.overwrite(out);
+}
+
+static u32 coarsen_common(Mesh& m, u32* codes, double qual_floor, bool require_better)
+{
+  CoarsenSel sel;
+  bool ok = false;
+  try {
+    ok = coarsen_select(m, codes, qual_floor, require_better, sel, nullptr, nullptr);
+    if (ok) coarsen_build(m, sel);
+  } catch (...) {
+    sel.free(m.s);
+    throw;
+  }
+  sel.free(m.s);
+  if (ok) last_pass_stats().elems_out = m.count(m.dim);
+  return ok ? 1 : 0;
+}
+
+u32 coarsen_by_size(Mesh& m, double qual_floor, double size_floor)
+{
+  cudaStream_t s = m.s;
+  PassStats& st = last_pass_stats();
+  st = PassStats();
+  st.op = 2;
+  st.elems_in = m.count(m.dim);
+  u32 ne = m.count(1);
+  Tag* h = m.find_tag(0, "adapt_size");
+  if (!h) throw Failure(E_ARG, "mesh has no adapt_size vertex field");
+  u32* codes = dalloc<u32>(ne, s);
+  u32* any = m.mb->dev + 5;
+  CK(cudaMemsetAsync(any, 0, sizeof(u32), s));
+  if (ne) {
+    k_coarsen_size_codes<<<grid_for(ne), BLOCK, 0, s>>>(ne, m.ask_down(1, 0), m.coords(),
+        static_cast<double const*>(h->data), size_floor, codes, any);
+    CK_LAUNCH();
+  }
+  u32 r = 0;
+  try {
+    if (read_u32(any, s)) r = coarsen_common(m, codes, qual_floor, false);
+  } catch (...) {
+    dev_free(codes, s);
+    throw;
+  }
+  dev_free(codes, s);
+  return r;
+}
+
+u32 coarsen_slivers(Mesh& m, double qual_floor, u32 nlayers)
+{
+  cudaStream_t s = m.s;
+  PassStats& st = last_pass_stats();
+  st = PassStats();
+  st.op = 4;
+  st.elems_in = m.count(m.dim);
+  u32 ne = m.count(1);
+  u32* sl = mark_slivers(m, qual_floor, nlayers);
+  u32* mv = mark_down(m, m.dim, 0, sl);
+  dev_free(sl, s);
+  u32* codes = dalloc<u32>(ne, s);
+  u32* any = m.mb->dev + 5;
+  CK(cudaMemsetAsync(any, 0, sizeof(u32), s));
+  if (ne) {
+    k_coarsen_sliver_codes<<<grid_for(ne), BLOCK, 0, s>>>(ne, m.ask_down(1, 0), mv, codes, any);
+    CK_LAUNCH();
+  }
+  dev_free(mv, s);
+  u32 r = 0;
+  try {
+    if (read_u32(any, s)) r = coarsen_common(m, codes, 0.0, true);
+  } catch (...) {
+    dev_free(codes, s);
+    throw;
+  }
+  dev_free(codes, s);
+  return r;
+}
+
+u32 coarsen_sets(Mesh& m, double qual_floor, double size_floor, u32* codes_size,
+    u32* codes_class, u32* codes_qual, double* quals2, u32* cand, double* col_qual,
+    u32* indset, u32* gen_vert)
+{
+  cudaStream_t s = m.s;
+  u32 ne = m.count(1), nv = m.count(0);
+  Tag* h = m.find_tag(0, "adapt_size");
+  if (!h) throw Failure(E_ARG, "mesh has no adapt_size vertex field");
+  u32* any = m.mb->dev + 5;
+  CK(cudaMemsetAsync(any, 0, sizeof(u32), s));
+  CK(cudaMemsetAsync(quals2, 0, sizeof(double) * ne * 2, s));
+  CK(cudaMemsetAsync(cand, 0, sizeof(u32) * nv, s));
+  CK(cudaMemsetAsync(col_qual, 0, sizeof(double) * nv, s));
+  CK(cudaMemsetAsync(indset, 0, sizeof(u32) * nv, s));
+  CK(cudaMemsetAsync(gen_vert, 0xff, sizeof(u32) * nv, s));
+  if (ne) {
+    k_coarsen_size_codes<<<grid_for(ne), BLOCK, 0, s>>>(ne, m.ask_down(1, 0), m.coords(),
+        static_cast<double const*>(h->data), size_floor, codes_size, any);
+    CK_LAUNCH();
+  }
+  u32* codes = dalloc<u32>(ne, s);
+  CK(cudaMemcpyAsync(codes, codes_size, sizeof(u32) * ne, cudaMemcpyDeviceToDevice, s));
+  CK(cudaMemcpyAsync(codes_class, codes_size, sizeof(u32) * ne, cudaMemcpyDeviceToDevice, s));
+  CK(cudaMemcpyAsync(codes_qual, codes_size, sizeof(u32) * ne, cudaMemcpyDeviceToDevice, s));
+  CoarsenSel sel;
+  bool ok = false;
+  if (read_u32(any, s)) {
+    ok = coarsen_select(m, codes, qual_floor, false, sel, codes_class, codes_qual);
+    if (sel.q2) {
+      // only the directions that still collapse carry a quality
+      CK(cudaMemcpyAsync(quals2, sel.q2, sizeof(double) * ne * 2, cudaMemcpyDeviceToDevice, s));
+    }
+    if (ok) {
+      CK(cudaMemcpyAsync(cand, sel.cand, sizeof(u32) * nv, cudaMemcpyDeviceToDevice, s));
+      CK(cudaMemcpyAsync(col_qual, sel.colq, sizeof(double) * nv, cudaMemcpyDeviceToDevice, s));
+      CK(cudaMemcpyAsync(indset, sel.ind, sizeof(u32) * nv, cudaMemcpyDeviceToDevice, s));
+      CK(cudaMemcpyAsync(gen_vert, sel.gen_vert, sizeof(u32) * nv, cudaMemcpyDeviceToDevice, s));
+    }
+  }
+  CK(cudaStreamSynchronize(s));
+  sel.free(s);
+  dev_free(codes, s);
+  return ok ? 1 : 0;
+}
+
+}  // namespace osh

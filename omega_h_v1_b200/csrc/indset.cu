@@ -1,0 +1,347 @@
+// Luby-style maximal independent set with goodness priority (indset.cpp) and
+// the small shared kernels of the passes: marking, class inheritance,
+// expansion, global renumbering.
+//
+// The star graph is never materialised for the independent set: an edge's
+// neighbours are the other edges of the tets around it (up(1,3) then
+// down(3,1)), a vertex's neighbours the far ends of its edges (up(0,1)).
+// That is exactly the neighbour set of the reference's star(1,3) /
+// star(0,1) (star.cpp:135-293); the selection rule depends only on that set.
+#include "passes.hpp"
+
+namespace osh {
+
+PassStats& last_pass_stats()
+{
+  static thread_local PassStats s;
+  return s;
+}
+
+__global__ void k_indset_init(u32 n, u32 const* __restrict__ filter, u32* __restrict__ st)
+{
+  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) st[i] = filter[i] ? (u32)UNKNOWN : (u32)NOT_IN_SET;
+}
+
+// neighbourhood walks: mode 0 = vertices via edges, mode 1 = edges via
+// elements (3D tets or 2D triangles)
+struct Nbrs {
+  u32 mode;
+  u32 const* offs;   // up(ent, via)
+  u32 const* adj;
+  u32 const* dirs;
+  u32 const* down;   // down(via, ent) or verts_of_edges
+  u32 per;           // entities per via-entity
+};
+
+template <class F>
+__device__ inline bool for_nbrs(Nbrs const& g, u32 i, F&& f)
+{
+  u32 b = g.offs[i], e = g.offs[i + 1];
+  if (g.mode == 0) {
+    for (u32 j = b; j < e; ++j)
+      if (!f(g.down[g.adj[j] * 2 + (1 - g.dirs[j])])) return false;
+  } else {
+    for (u32 j = b; j < e; ++j) {
+      u32 const* ds = g.down + (size_t)g.adj[j] * g.per;
+      for (u32 k = 0; k < g.per; ++k) {
+        u32 o = ds[k];
+        if (o != i && !f(o)) return false;
+      }
+    }
+  }
+  return true;
+}
+
+// one round of indset_at_vert (indset.cpp:55-84) over all entities
+__global__ void k_indset_round(u32 n, Nbrs g, u32 const* __restrict__ old_st,
+    u32* __restrict__ st, double const* __restrict__ good,
+    u64 const* __restrict__ glob, u32* unknown_left)
+{
+  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  u32 s0 = old_st[i];
+  if (s0 != UNKNOWN) {
+    st[i] = s0;
+    return;
+  }
+  bool any_in = !for_nbrs(g, i, [&](u32 o) { return old_st[o] != IN_SET; });
+  if (any_in) {
+    st[i] = NOT_IN_SET;
+    return;
+  }
+  double myg = good[i];
+  u64 myid = glob ? glob[i] : (u64)i;
+  bool win = for_nbrs(g, i, [&](u32 o) {
+    if (old_st[o] == NOT_IN_SET) return true;
+    double og = good[o];
+    u64 oid = glob ? glob[o] : (u64)o;
+    if (myg == og && oid < myid) return false;
+    if (myg < og) return false;
+    return true;
+  });
+  if (win) {
+    st[i] = IN_SET;
+  } else {
+    st[i] = UNKNOWN;
+    *unknown_left = 1;
+  }
+}
+
+// number of upward uses walked per round (edges of vertices / elements of
+// edges), for the probe's byte count
+static u32 read_cached_uses(Mesh& m, u32 ent_dim)
+{
+  return ent_dim == 0 ? 2u * m.counts[1] : deg(m.dim, 1) * m.counts[m.dim];
+}
+
+u32* find_indset(Mesh& m, u32 ent_dim, u32 const* filter, double const* good)
+{
+  u32 n = m.count(ent_dim);
+  Nbrs g{};
+  if (ent_dim == 0) {
+    UpAdj const& u = m.ask_up(0, 1);
+    g.mode = 0;
+    g.offs = u.offs;
+    g.adj = u.adj;
+    g.dirs = u.dirs;
+    g.down = m.ask_down(1, 0);
+    g.per = 2;
+  } else if (ent_dim == 1 && m.dim >= 2) {
+    UpAdj const& u = m.ask_up(1, m.dim);
+    g.mode = 1;
+    g.offs = u.offs;
+    g.adj = u.adj;
+    g.dirs = u.dirs;
+    g.down = m.ask_down(m.dim, 1);
+    g.per = deg(m.dim, 1);
+  } else {
+    throw Failure(E_ARG, "independent sets are built on vertices or edges");
+  }
+  u64 const* glob = (m.parallel && m.globals[ent_dim]) ? m.globals[ent_dim] : nullptr;
+  double via_bytes = ent_dim == 0 ? 8.0 * m.counts[1] : 4.0 * g.per * m.counts[m.dim];
+  u32* a = dalloc<u32>(n, m.s);
+  u32* b = dalloc<u32>(n, m.s);
+  u32* flag = m.mb->dev + 0;
+  if (n) {
+    k_indset_init<<<grid_for(n), BLOCK, 0, m.s>>>(n, filter, a);
+    CK_LAUNCH();
+  }
+  u32 rounds = 0;
+  bool done = (n == 0);
+  for (u32 it = 0; it < MAX_INDSET_ROUNDS && !done; ++it) {
+    CK(cudaMemsetAsync(flag, 0, sizeof(u32), m.s));
+    {
+      // offsets, upward lists, the via-entities' down lists, states,
+      // goodness and (parallel) globals read once; states written once
+      double nuse = (double)read_cached_uses(m, ent_dim);
+      PROBE(P_INDSET_ROUND, m.s, 4.0 * (n + 1.0) + 4.0 * nuse + via_bytes +
+          4.0 * n + 8.0 * n + (glob ? 8.0 * n : 0.0) + 4.0 * n);
+      k_indset_round<<<grid_for(n), BLOCK, 0, m.s>>>(n, g, a, b, good, glob, flag);
+      CK_LAUNCH();
+    }
+    std::swap(a, b);
+    ++rounds;
+    if (!read_u32(flag, m.s)) done = true;
+  }
+  dev_free(b, m.s);
+  last_pass_stats().indset_rounds = rounds;
+  if (!done) {
+    dev_free(a, m.s);
+    throw Failure(E_NOCONVERGE, "independent set did not settle in 100 rounds");
+  }
+  return a;
+}
+
+// ---------------------------------------------------------------------------
+// expansion and inheritance
+
+template <class T>
+__global__ void k_expand_scaled(T const* __restrict__ in, u32 const* __restrict__ offs,
+    u32 k, u32 n, u32 width, T* __restrict__ out)
+{
+  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  u32 f = offs[i] * k, e = offs[i + 1] * k;
+  for (u32 j = f; j < e; ++j)
+    for (u32 c = 0; c < width; ++c) out[(size_t)j * width + c] = in[(size_t)i * width + c];
+}
+
+void expand_scaled(void const* in, u32 const* offs, u32 k, u32 n, u32 width,
+    u32 esz, void* out, cudaStream_t s)
+{
+  if (!n || !width || !k) return;
+  PROBE(P_EXPAND, s, 4.0 * (n + 1) + 2.0 * (double)n * width * esz * k);
+  if (esz == 1)
+    k_expand_scaled<unsigned char><<<grid_for(n), BLOCK, 0, s>>>(
+        (unsigned char const*)in, offs, k, n, width, (unsigned char*)out);
+  else if (esz == 4)
+    k_expand_scaled<u32><<<grid_for(n), BLOCK, 0, s>>>(
+        (u32 const*)in, offs, k, n, width, (u32*)out);
+  else
+    k_expand_scaled<unsigned long long><<<grid_for(n), BLOCK, 0, s>>>(
+        (unsigned long long const*)in, offs, k, n, width, (unsigned long long*)out);
+  CK_LAUNCH();
+}
+
+static void inherit_u32_tag(Mesh& m, Mesh& out, u32 prod, Doms const& d, char const* name)
+{
+  Tag* t = m.find_tag(prod, name);
+  if (!t) throw Failure(E_ARG, std::string("missing tag ") + name);
+  u32 nc = t->ncomps;
+  u32* data = dalloc<u32>((size_t)d.ngo[4] * nc, m.s);
+  for (u32 k = 0; k < 4; ++k) {
+    if (!d.ndoms[k] || !d.offs[k] || !d.ngen[k]) continue;
+    Tag* tk = (k == 0) ? t : m.find_tag(k, name);
+    if (!tk) continue;
+    expand_scaled(tk->data, d.offs[k], d.scale[k], d.ndoms[k], nc, 4,
+        data + (size_t)d.ngo[k] * nc, m.s);
+  }
+  out.add_tag(prod, T_U32, name, nc, X_NOT, data);
+}
+
+void inherit_class(Mesh& m, Mesh& out, u32 prod, Doms const& d)
+{
+  if (!m.find_tag(0, "class_dim")) return;
+  inherit_u32_tag(m, out, prod, d, "class_dim");
+  if (m.find_tag(0, "class_id")) inherit_u32_tag(m, out, prod, d, "class_id");
+}
+
+void inherit_globals(Mesh& out, u32 d, u32 n)
+{
+  u64* g = dalloc<u64>(n, out.s);
+  iota_u64(g, n, out.s);
+  out.set_globals(d, g);
+}
+
+__global__ void k_interp_coords(u32 ne, u32 vpe, u32 const* __restrict__ voe,
+    double const* __restrict__ x, double* __restrict__ out)
+{
+  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= ne) return;
+  // average_element_field (element_field.hpp:9-25)
+  double o0 = 0, o1 = 0, o2 = 0;
+  for (u32 j = 0; j < vpe; ++j) {
+    u32 v = voe[(size_t)i * vpe + j];
+    o0 += x[v * 3 + 0];
+    o1 += x[v * 3 + 1];
+    o2 += x[v * 3 + 2];
+  }
+  out[i * 3 + 0] = o0 / vpe;
+  out[i * 3 + 1] = o1 / vpe;
+  out[i * 3 + 2] = o2 / vpe;
+}
+
+void interp_coords_to_elems(Mesh& m)
+{
+  u32 ne = m.count(m.dim), vpe = deg(m.dim, 0);
+  double* out = dalloc<double>((size_t)ne * 3, m.s);
+  if (ne) {
+    k_interp_coords<<<grid_for(ne), BLOCK, 0, m.s>>>(ne, vpe, m.ask_down(m.dim, 0),
+        m.coords(), out);
+    CK_LAUNCH();
+  }
+  m.add_tag(m.dim, T_F64, "coordinates", 3, X_NOT, out);
+}
+
+// ---------------------------------------------------------------------------
+// marking (mark.cpp)
+
+__global__ void k_mark_down(u32 n, u32 const* __restrict__ offs, u32 const* __restrict__ adj,
+    u32 const* __restrict__ marked, u32* __restrict__ out)
+{
+  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  u32 r = 0;
+  for (u32 j = offs[i]; j < offs[i + 1]; ++j)
+    if (marked[adj[j]]) {
+      r = 1;
+      break;
+    }
+  out[i] = r;
+}
+
+u32* mark_down(Mesh& m, u32 high, u32 low, u32 const* marked)
+{
+  u32 n = m.count(low);
+  UpAdj const& u = m.ask_up(low, high);
+  u32* out = dalloc<u32>(n, m.s);
+  if (n) {
+    k_mark_down<<<grid_for(n), BLOCK, 0, m.s>>>(n, u.offs, u.adj, marked, out);
+    CK_LAUNCH();
+  }
+  return out;
+}
+
+__global__ void k_mark_up(u32 n, u32 lph, u32 const* __restrict__ loh,
+    u32 const* __restrict__ marked, u32* __restrict__ out)
+{
+  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  u32 r = 0;
+  for (u32 j = 0; j < lph; ++j)
+    if (marked[loh[(size_t)i * lph + j]]) {
+      r = 1;
+      break;
+    }
+  out[i] = r;
+}
+
+u32* mark_up(Mesh& m, u32 low, u32 high, u32 const* marked)
+{
+  u32 n = m.count(high);
+  u32* out = dalloc<u32>(n, m.s);
+  if (n) {
+    k_mark_up<<<grid_for(n), BLOCK, 0, m.s>>>(n, deg(high, low), m.ask_down(high, low),
+        marked, out);
+    CK_LAUNCH();
+  }
+  return out;
+}
+
+__global__ void k_mark_slivers(u32 n, double const* __restrict__ q, double gq,
+    u32* __restrict__ out)
+{
+  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = (q[i] < gq) ? 1u : 0u;
+}
+
+__global__ void k_dual_layer(u32 n, u32 degr, u32 const* __restrict__ dual,
+    u32 const* __restrict__ in, u32* __restrict__ out)
+{
+  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  u32 r = in[i];
+  for (u32 j = 0; j < degr; ++j) {
+    u32 e = dual[(size_t)i * degr + j];
+    if (e != INV && in[e]) r = 1;
+  }
+  out[i] = r;
+}
+
+// mesh_mark_slivers + mesh_mark_dual_layers (mark.cpp:101-147,218-243)
+u32* mark_slivers(Mesh& m, double gq, u32 nlayers)
+{
+  u32 n = m.count(m.dim);
+  double const* q = m.qualities();
+  u32* a = dalloc<u32>(n, m.s);
+  if (n) {
+    k_mark_slivers<<<grid_for(n), BLOCK, 0, m.s>>>(n, q, gq, a);
+    CK_LAUNCH();
+  }
+  if (!nlayers) return a;
+  u32 const* du = m.ask_dual();
+  u32* b = dalloc<u32>(n, m.s);
+  u32 degr = deg(m.dim, m.dim - 1);
+  for (u32 l = 0; l < nlayers; ++l) {
+    if (n) {
+      k_dual_layer<<<grid_for(n), BLOCK, 0, m.s>>>(n, degr, du, a, b);
+      CK_LAUNCH();
+    }
+    std::swap(a, b);
+  }
+  dev_free(b, m.s);
+  return a;
+}
+
+}  // namespace osh

@@ -1,0 +1,896 @@
+// Mesh store, lazy adjacency derivation and per-element geometry on sm_100a.
+//
+// Adjacency kernels (all one pass over their inputs, no host round trips
+// except where an output size must be known to allocate):
+//   up_from_down   counting by atomics, one scan, atomic fill, then a
+//                  warp-per-row rank sort that restores the deterministic
+//                  row order of the reference's CPU invert_map
+//                  (invert_map.cpp:92-136) and splits use -> (high, dir)
+//   reflect_down   one thread per (high entity, local low slot); searches the
+//                  first vertex's upward list (reflect_down.cpp:13-38,
+//                  find_by_verts.hpp:14-55)
+//   dual / stars   star.cpp, dual.cpp, bridge_graph.cpp, derive_sides.cpp
+#include <cfloat>
+#include <cmath>
+#include <cstring>
+
+#include "mesh.hpp"
+
+namespace osh {
+
+// ---------------------------------------------------------------------------
+// Mesh lifetime and tags
+
+static void release_mailbox(Mailbox* m)
+{
+  m->release();
+  delete m;
+}
+
+Mesh::Mesh(u32 d, bool f, bool p, cudaStream_t stream,
+    std::shared_ptr<Mailbox> mailbox)
+    : dim(d), full(f), parallel(p), s(stream), mb(mailbox)
+{
+  if (!s) {
+    CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    own_stream = true;
+  }
+  if (!mb) {
+    mb = std::shared_ptr<Mailbox>(new Mailbox(), release_mailbox);
+    mb->init(s);
+  }
+}
+
+Mesh::~Mesh()
+{
+  try {
+    clear_contents();
+  } catch (...) {
+  }
+  if (own_stream) {
+    mb.reset();
+    cudaStreamSynchronize(s);
+    cudaStreamDestroy(s);
+  }
+}
+
+Mesh* Mesh::spawn() const
+{
+  return new Mesh(dim, full, parallel, s, mb);
+}
+
+Mesh* Mesh::clone()
+{
+  Mesh* c = new Mesh(dim, full, parallel, nullptr);
+  CK(cudaStreamSynchronize(s));
+  try {
+    for (u32 d = 0; d <= dim; ++d) {
+      if (!has_dim(d)) continue;
+      u32 n = counts[d];
+      u32* v = nullptr;
+      if (d) {
+        size_t bytes = sizeof(u32) * (size_t)n * deg(d, 0);
+        v = static_cast<u32*>(dev_alloc(bytes, c->s));
+        CK(cudaMemcpyAsync(v, down[d][0], bytes, cudaMemcpyDeviceToDevice, c->s));
+      }
+      c->set_ents(d, n, v);
+      for (auto const& t : tags[d]) {
+        size_t bytes = (size_t)n * t.ncomps * tag_esz(t.type);
+        void* p = dev_alloc(bytes, c->s);
+        CK(cudaMemcpyAsync(p, t.data, bytes, cudaMemcpyDeviceToDevice, c->s));
+        c->add_tag(d, t.type, t.name.c_str(), t.ncomps, t.transfer, p);
+      }
+      if (globals[d]) {
+        u64* g = dalloc<u64>(n, c->s);
+        CK(cudaMemcpyAsync(g, globals[d], sizeof(u64) * n, cudaMemcpyDeviceToDevice, c->s));
+        c->globals[d] = g;
+      }
+    }
+    c->ghost_layers = ghost_layers;
+    CK(cudaStreamSynchronize(c->s));
+  } catch (...) {
+    delete c;
+    throw;
+  }
+  return c;
+}
+
+void Mesh::use_stream(cudaStream_t stream)
+{
+  CK(cudaStreamSynchronize(s));
+  if (own_stream) CK(cudaStreamDestroy(s));
+  own_stream = false;
+  s = stream;
+}
+
+void Mesh::clear_contents()
+{
+  for (u32 h = 0; h < 4; ++h)
+    for (u32 l = 0; l < 4; ++l) {
+      dev_free(down[h][l], s);
+      down[h][l] = nullptr;
+      if (have_up[l][h]) {
+        dev_free(up[l][h].offs, s);
+        dev_free(up[l][h].adj, s);
+        dev_free(up[l][h].dirs, s);
+        up[l][h] = UpAdj();
+        have_up[l][h] = false;
+      }
+      if (have_star[l][h]) {
+        dev_free(star[l][h].offs, s);
+        dev_free(star[l][h].adj, s);
+        star[l][h] = Graph();
+        have_star[l][h] = false;
+      }
+    }
+  dev_free(dual, s);
+  dual = nullptr;
+  for (u32 d = 0; d < 4; ++d) {
+    for (auto& t : tags[d]) dev_free(t.data, s);
+    tags[d].clear();
+    dev_free(globals[d], s);
+    globals[d] = nullptr;
+    dev_free(own_ranks[d], s);
+    own_ranks[d] = nullptr;
+    dev_free(own_ids[d], s);
+    own_ids[d] = nullptr;
+    counts[d] = 0;
+  }
+  dev_free(qual_cache, s);
+  qual_cache = nullptr;
+}
+
+void Mesh::overwrite(Mesh* with)
+{
+  clear_contents();
+  dim = with->dim;
+  full = with->full;
+  parallel = with->parallel;
+  for (u32 h = 0; h < 4; ++h)
+    for (u32 l = 0; l < 4; ++l) {
+      down[h][l] = with->down[h][l];
+      up[h][l] = with->up[h][l];
+      have_up[h][l] = with->have_up[h][l];
+      star[h][l] = with->star[h][l];
+      have_star[h][l] = with->have_star[h][l];
+      with->down[h][l] = nullptr;
+      with->have_up[h][l] = false;
+      with->have_star[h][l] = false;
+    }
+  dual = with->dual;
+  with->dual = nullptr;
+  for (u32 d = 0; d < 4; ++d) {
+    counts[d] = with->counts[d];
+    tags[d].swap(with->tags[d]);
+    globals[d] = with->globals[d];
+    with->globals[d] = nullptr;
+    own_ranks[d] = with->own_ranks[d];
+    with->own_ranks[d] = nullptr;
+    own_ids[d] = with->own_ids[d];
+    with->own_ids[d] = nullptr;
+  }
+  qual_cache = with->qual_cache;
+  with->qual_cache = nullptr;
+  delete with;
+}
+
+void Mesh::set_ents(u32 d, u32 n, u32* verts)
+{
+  counts[d] = n;
+  down[d][0] = verts;
+}
+
+u32 Mesh::count(u32 d)
+{
+  if (d > dim) return 0;
+  if (d) ask_down(d, 0);
+  return counts[d];
+}
+
+Tag* Mesh::find_tag(u32 d, char const* name)
+{
+  for (auto& t : tags[d])
+    if (t.name == name) return &t;
+  return nullptr;
+}
+
+Tag& Mesh::add_tag(u32 d, u32 type, char const* name, u32 ncomps, u32 transfer,
+    void* data)
+{
+  if (find_tag(d, name)) throw Failure(E_ARG, std::string("duplicate tag ") + name);
+  Tag t;
+  t.name = name;
+  t.type = type;
+  t.ncomps = ncomps;
+  t.transfer = transfer;
+  t.data = data;
+  tags[d].push_back(t);
+  return tags[d].back();
+}
+
+void Mesh::remove_tag(u32 d, char const* name)
+{
+  for (size_t i = 0; i < tags[d].size(); ++i)
+    if (tags[d][i].name == name) {
+      dev_free(tags[d][i].data, s);
+      tags[d].erase(tags[d].begin() + i);
+      return;
+    }
+  throw Failure(E_ARG, std::string("no tag ") + name);
+}
+
+double const* Mesh::coords()
+{
+  Tag* t = find_tag(0, "coordinates");
+  if (!t) throw Failure(E_ARG, "mesh has no coordinates");
+  return static_cast<double const*>(t->data);
+}
+
+void Mesh::set_globals(u32 d, u64* g)
+{
+  dev_free(globals[d], s);
+  globals[d] = g;
+}
+
+void Mesh::make_parallel()
+{
+  parallel = true;
+  for (u32 d = 0; d <= dim; ++d)
+    if (has_dim(d)) {
+      u32 n = count(d);
+      u64* g = dalloc<u64>(n, s);
+      iota_u64(g, n, s);
+      set_globals(d, g);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// upward adjacency (up_from_down.cpp:24-47, invert_map.cpp:70-136)
+
+__global__ void k_count_lows(u32 const* __restrict__ loh, u32 nuses, u32* cnt)
+{
+  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < nuses) atomicAdd(&cnt[loh[i]], 1u);
+}
+
+__global__ void k_fill_uses(u32 const* __restrict__ loh, u32 nuses,
+    u32 const* __restrict__ offs, u32* cur, u32* __restrict__ tmp)
+{
+  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nuses) return;
+  u32 l = loh[i];
+  u32 slot = atomicAdd(&cur[l], 1u);
+  tmp[offs[l] + slot] = i;
+}
+
+// One warp per row: every lane ranks its element against the whole row and
+// writes it to its sorted position (rows hold distinct use indices).
+__global__ void k_rank_rows(u32 const* __restrict__ offs, u32 const* __restrict__ tmp,
+    u32 nrows, u32 lph, u32* __restrict__ adj, u32* __restrict__ dirs)
+{
+  u32 row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  u32 lane = threadIdx.x & 31;
+  if (row >= nrows) return;
+  u32 f = offs[row], len = offs[row + 1] - f;
+  for (u32 base = 0; base < len; base += 32) {
+    u32 idx = base + lane;
+    u32 my = idx < len ? tmp[f + idx] : INV;
+    u32 rank = 0;
+    for (u32 cb = 0; cb < len; cb += 32) {
+      u32 other = (cb + lane < len) ? tmp[f + cb + lane] : INV;
+      u32 lim = len - cb < 32 ? len - cb : 32;
+      for (u32 j = 0; j < lim; ++j) {
+        u32 v = __shfl_sync(0xffffffffu, other, j);
+        rank += (v < my) ? 1u : 0u;
+      }
+    }
+    if (idx < len) {
+      adj[f + rank] = my / lph;
+      dirs[f + rank] = my % lph;
+    }
+  }
+}
+
+void up_from_down(u32 high, u32 low, u32 nhighs, u32 nlows, u32 const* loh,
+    UpAdj& out, cudaStream_t s)
+{
+  u32 lph = deg(high, low);
+  u32 nuses = nhighs * lph;
+  u32* cnt = dalloc<u32>((size_t)nlows + 1, s);
+  CK(cudaMemsetAsync(cnt, 0, sizeof(u32) * ((size_t)nlows + 1), s));
+  if (nuses) {
+    PROBE(P_UP_COUNT, s, 4.0 * nuses + 4.0 * nlows);
+    k_count_lows<<<grid_for(nuses), BLOCK, 0, s>>>(loh, nuses, cnt);
+    CK_LAUNCH();
+  }
+  out.offs = exscan_new(cnt, nlows, s);
+  CK(cudaMemsetAsync(cnt, 0, sizeof(u32) * ((size_t)nlows + 1), s));
+  u32* tmp = dalloc<u32>(nuses, s);
+  out.adj = dalloc<u32>(nuses, s);
+  out.dirs = dalloc<u32>(nuses, s);
+  if (nuses) {
+    {
+      PROBE(P_UP_FILL, s, 8.0 * nuses + 4.0 * (nlows + 1.0) + 4.0 * nlows);
+      k_fill_uses<<<grid_for(nuses), BLOCK, 0, s>>>(loh, nuses, out.offs, cnt, tmp);
+      CK_LAUNCH();
+    }
+    u64 threads = (u64)nlows * 32;
+    {
+      PROBE(P_UP_RANK, s, 12.0 * nuses + 4.0 * (nlows + 1.0));
+      k_rank_rows<<<grid_for(threads), BLOCK, 0, s>>>(out.offs, tmp, nlows, lph,
+          out.adj, out.dirs);
+      CK_LAUNCH();
+    }
+  }
+  dev_free(tmp, s);
+  dev_free(cnt, s);
+}
+
+// ---------------------------------------------------------------------------
+// downward adjacency by search (reflect_down.cpp:13-81)
+
+__global__ void k_reflect_down(u32 high, u32 low, u32 nh, u32 const* __restrict__ voh,
+    u32 const* __restrict__ vol, u32 const* __restrict__ lv_offs,
+    u32 const* __restrict__ lv_adj, u32 const* __restrict__ lv_dirs,
+    u32* __restrict__ out)
+{
+  u32 lph = deg(high, low), vph = deg(high, 0);
+  u32 idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= nh * lph) return;
+  u32 i = idx / lph, j = idx % lph;
+  u32 const* vh = voh + (size_t)i * vph;
+  u32 w0 = vh[canon(high, low, 0, j, 0)];
+  u32 w1 = vh[canon(high, low, 0, j, 1)];
+  u32 f = lv_offs[w0], e = lv_offs[w0 + 1];
+  u32 found = INV;
+  if (low == 1) {
+    for (u32 r = f; r < e; ++r) {
+      u32 ed = lv_adj[r], d = lv_dirs[r];
+      if (vol[ed * 2 + (1 - d)] == w1) {
+        found = ed;
+        break;
+      }
+    }
+  } else {
+    u32 w2 = vh[canon(high, low, 0, j, 2)];
+    for (u32 r = f; r < e; ++r) {
+      u32 t = lv_adj[r], d = lv_dirs[r];
+      u32 a = vol[t * 3 + (d + 1) % 3], b = vol[t * 3 + (d + 2) % 3];
+      if ((a == w1 && b == w2) || (a == w2 && b == w1)) {
+        found = t;
+        break;
+      }
+    }
+  }
+  out[idx] = found;
+}
+
+// ---------------------------------------------------------------------------
+// star graphs (star.cpp)
+
+__global__ void k_vertex_edge_star(u32 nadj, u32 const* __restrict__ adj,
+    u32 const* __restrict__ dirs, u32 const* __restrict__ voe, u32* __restrict__ star)
+{
+  u32 j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j < nadj) star[j] = voe[adj[j] * 2 + (1 - dirs[j])];
+}
+
+__global__ void k_scale_offsets(u32 const* __restrict__ in, u32 n1, u32 k,
+    u32* __restrict__ out)
+{
+  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n1) out[i] = in[i] * k;
+}
+
+__global__ void k_edge_tri_star(u32 nadj, u32 const* __restrict__ adj,
+    u32 const* __restrict__ dirs, u32 const* __restrict__ eot, u32* __restrict__ star)
+{
+  u32 j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= nadj) return;
+  u32 t = adj[j], d = dirs[j];
+  star[j * 2 + 0] = eot[t * 3 + (d + 1) % 3];
+  star[j * 2 + 1] = eot[t * 3 + (d + 2) % 3];
+}
+
+__global__ void k_sum_degrees(u32 n, u32 const* __restrict__ a, u32 const* __restrict__ b,
+    u32* __restrict__ deg_out)
+{
+  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) deg_out[i] = (a[i + 1] - a[i]) + (b[i + 1] - b[i]);
+}
+
+__global__ void k_edge_tet_star(u32 n, u32 const* __restrict__ so,
+    u32 const* __restrict__ ts_offs, u32 const* __restrict__ ts,
+    u32 const* __restrict__ roe_offs, u32 const* __restrict__ roe,
+    u32 const* __restrict__ roe_dirs, u32 const* __restrict__ eor, u32* __restrict__ star)
+{
+  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  u32 o = so[i];
+  for (u32 j = ts_offs[i]; j < ts_offs[i + 1]; ++j) star[o++] = ts[j];
+  for (u32 j = roe_offs[i]; j < roe_offs[i + 1]; ++j)
+    star[o++] = eor[roe[j] * 6 + tet_opp_edge(roe_dirs[j])];
+}
+
+constexpr u32 STAR_BUF = 256;
+
+// get_ent_star_general (star.cpp:14-34); pass 0 counts, pass 1 fills
+__global__ void k_star_general(u32 n, u32 const* __restrict__ hl_offs,
+    u32 const* __restrict__ hl, u32 const* __restrict__ loh, u32 lph,
+    u32 const* __restrict__ star_offs, u32* __restrict__ deg_out,
+    u32* __restrict__ star, u32* err)
+{
+  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  u32 buf[STAR_BUF];
+  u32 size = 0;
+  for (u32 j = hl_offs[i]; j < hl_offs[i + 1]; ++j) {
+    u32 h = hl[j];
+    for (u32 k = 0; k < lph; ++k) {
+      u32 sl = loh[h * lph + k];
+      if (sl == i) continue;
+      bool have = false;
+      for (u32 a = 0; a < size; ++a)
+        if (buf[a] == sl) {
+          have = true;
+          break;
+        }
+      if (have) continue;
+      if (size == STAR_BUF) {
+        atomicOr(err, 1u);
+        continue;
+      }
+      buf[size++] = sl;
+    }
+  }
+  if (star)
+    for (u32 a = 0; a < size; ++a) star[star_offs[i] + a] = buf[a];
+  else
+    deg_out[i] = size;
+}
+
+// ---------------------------------------------------------------------------
+// element dual (dual.cpp)
+
+__global__ void k_dual_from_sides(u32 ne, u32 spe, u32 const* __restrict__ soe,
+    u32 const* __restrict__ es_offs, u32 const* __restrict__ es, u32* __restrict__ out)
+{
+  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= ne) return;
+  for (u32 j = 0; j < spe; ++j) {
+    u32 s = soe[i * spe + j];
+    u32 o = INV;
+    for (u32 k = es_offs[s]; k < es_offs[s + 1]; ++k)
+      if (es[k] != i) {
+        o = es[k];
+        break;
+      }
+    out[i * spe + j] = o;
+  }
+}
+
+__global__ void k_dual_from_verts(u32 dim, u32 ne, u32 const* __restrict__ voe,
+    u32 const* __restrict__ ev_offs, u32 const* __restrict__ ev,
+    u32* __restrict__ out, u32* err)
+{
+  u32 spe = deg(dim, dim - 1), vpe = deg(dim, 0), vps = deg(dim - 1, 0);
+  u32 idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= ne * spe) return;
+  u32 i = idx / spe, j = idx % spe;
+  u32 buf[STAR_BUF];
+  u32 n = 0;
+  for (u32 k = 0; k < vps; ++k) {
+    u32 v = voe[(size_t)i * vpe + canon(dim, dim - 1, 0, j, k)];
+    u32 f = ev_offs[v], e = ev_offs[v + 1];
+    if (k) {
+      u32 nn = 0;
+      for (u32 a = 0; a < n; ++a) {
+        bool has = false;
+        for (u32 b = f; b < e; ++b)
+          if (ev[b] == buf[a]) {
+            has = true;
+            break;
+          }
+        if (has) buf[nn++] = buf[a];
+      }
+      n = nn;
+    } else {
+      for (u32 a = f; a < e; ++a)
+        if (ev[a] != i) {
+          if (n == STAR_BUF) {
+            atomicOr(err, 1u);
+            break;
+          }
+          buf[n++] = ev[a];
+        }
+    }
+  }
+  out[idx] = n ? buf[0] : INV;
+}
+
+// bridge graphs (bridge_graph.cpp): degree then fill
+__global__ void k_bridge_degree(u32 n, u32 const* __restrict__ offs, u32 stride,
+    u32 const* __restrict__ adj, u32* __restrict__ degree)
+{
+  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  u32 f = offs ? offs[i] : i * stride, e = offs ? offs[i + 1] : (i + 1) * stride;
+  u32 d = 0;
+  for (u32 j = f; j < e; ++j)
+    if (i < adj[j]) ++d;
+  degree[i] = d;
+}
+
+__global__ void k_bridge_edges(u32 n, u32 const* __restrict__ offs,
+    u32 const* __restrict__ adj, u32 const* __restrict__ bo, u32* __restrict__ voe)
+{
+  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  u32 e = bo[i];
+  for (u32 j = offs[i]; j < offs[i + 1]; ++j)
+    if (i < adj[j]) {
+      voe[e * 2 + 0] = i;
+      voe[e * 2 + 1] = adj[j];
+      ++e;
+    }
+}
+
+// bridge_dual_graph + derive_side: sides in (element, local side) order
+__global__ void k_derive_sides(u32 dim, u32 ne, u32 const* __restrict__ dual,
+    u32 const* __restrict__ bo, u32 const* __restrict__ voe, u32* __restrict__ vos)
+{
+  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= ne) return;
+  u32 spe = deg(dim, dim - 1), vpe = deg(dim, 0), vps = deg(dim - 1, 0);
+  u32 s = bo[i];
+  for (u32 j = 0; j < spe; ++j)
+    if (i < dual[i * spe + j]) {
+      for (u32 k = 0; k < vps; ++k)
+        vos[(size_t)s * vps + k] = voe[(size_t)i * vpe + canon(dim, dim - 1, 0, j, k)];
+      ++s;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Mesh::ask_* (mesh.cpp:136-261)
+
+u32 const* Mesh::ask_down(u32 high, u32 low)
+{
+  if (down[high][low]) return down[high][low];
+  if (low == high) {
+    u32 n = counts[high];
+    u32* a = dalloc<u32>(n, s);
+    iota_u32(a, n, 1, s);
+    down[high][low] = a;
+  } else if (low > 0) {
+    u32 nh = count(high);
+    u32 const* voh = ask_down(high, 0);
+    UpAdj const& lv = ask_up(0, low);
+    u32 const* vol = ask_down(low, 0);
+    u32 n = nh * deg(high, low);
+    u32* out = dalloc<u32>(n, s);
+    if (n) {
+      // voh once, the first vertices' upward CSR once, vol once, out once
+      double nl = counts[low], nuse = (double)nl * deg(low, 0);
+      PROBE(P_REFLECT_DOWN, s, 4.0 * deg(high, 0) * nh + 4.0 * (counts[0] + 1.0) +
+          8.0 * nuse + 4.0 * deg(low, 0) * nl + 4.0 * n);
+      k_reflect_down<<<grid_for(n), BLOCK, 0, s>>>(high, low, nh, voh, vol, lv.offs,
+          lv.adj, lv.dirs, out);
+      CK_LAUNCH();
+    }
+    down[high][low] = out;
+  } else if (high == 1 && dim == 3) {
+    // edges in 3D bridge the vertex star (mesh.cpp:160-168)
+    Graph const& vv = ask_star(0, dim);
+    u32 nv = counts[0];
+    u32* degree = dalloc<u32>(nv, s);
+    if (nv) {
+      k_bridge_degree<<<grid_for(nv), BLOCK, 0, s>>>(nv, vv.offs, 0, vv.adj, degree);
+      CK_LAUNCH();
+    }
+    u32* bo = exscan_new(degree, nv, s);
+    dev_free(degree, s);
+    u32 ne = read_u32(bo + nv, s);
+    u32* voe = dalloc<u32>((size_t)ne * 2, s);
+    if (nv) {
+      k_bridge_edges<<<grid_for(nv), BLOCK, 0, s>>>(nv, vv.offs, vv.adj, bo, voe);
+      CK_LAUNCH();
+    }
+    dev_free(bo, s);
+    set_ents(1, ne, voe);
+  } else {
+    // sides from the element dual (mesh.cpp:169-179)
+    u32 const* du = ask_dual();
+    u32 nel = counts[dim];
+    u32 spe = deg(dim, dim - 1);
+    u32* degree = dalloc<u32>(nel, s);
+    if (nel) {
+      k_bridge_degree<<<grid_for(nel), BLOCK, 0, s>>>(nel, nullptr, spe, du, degree);
+      CK_LAUNCH();
+    }
+    u32* bo = exscan_new(degree, nel, s);
+    dev_free(degree, s);
+    u32 ns = read_u32(bo + nel, s);
+    u32 vps = deg(dim - 1, 0);
+    u32* vos = dalloc<u32>((size_t)ns * vps, s);
+    if (nel) {
+      k_derive_sides<<<grid_for(nel), BLOCK, 0, s>>>(dim, nel, du, bo, down[dim][0], vos);
+      CK_LAUNCH();
+    }
+    dev_free(bo, s);
+    set_ents(dim - 1, ns, vos);
+  }
+  return down[high][low];
+}
+
+UpAdj const& Mesh::ask_up(u32 low, u32 high)
+{
+  if (have_up[low][high]) return up[low][high];
+  if (low == high) {
+    u32 n = counts[high];
+    UpAdj u;
+    u.offs = dalloc<u32>((size_t)n + 1, s);
+    iota_u32(u.offs, n + 1, 1, s);
+    u.adj = dalloc<u32>(n, s);
+    iota_u32(u.adj, n, 1, s);
+    u.dirs = dalloc<u32>(n, s);
+    fill_u32(u.dirs, n, 0, s);
+    up[low][high] = u;
+  } else {
+    u32 const* loh = ask_down(high, low);
+    up_from_down(high, low, counts[high], counts[low], loh, up[low][high], s);
+  }
+  have_up[low][high] = true;
+  return up[low][high];
+}
+
+Graph const& Mesh::ask_star(u32 low, u32 high)
+{
+  if (have_star[low][high]) return star[low][high];
+  Graph g;
+  if (low == high) {
+    u32 n = counts[low];
+    g.offs = dalloc<u32>((size_t)n + 1, s);
+    fill_u32(g.offs, n + 1, 0, s);
+    g.adj = dalloc<u32>(1, s);
+  } else if (low == 0 && high == dim && dim != 1 && has_dim(1)) {
+    Graph const& vv = ask_star(0, 1);
+    u32 n = counts[0];
+    g.offs = dalloc<u32>((size_t)n + 1, s);
+    CK(cudaMemcpyAsync(g.offs, vv.offs, sizeof(u32) * (n + 1), cudaMemcpyDeviceToDevice, s));
+    g.nadj = vv.nadj;
+    g.adj = dalloc<u32>(g.nadj, s);
+    CK(cudaMemcpyAsync(g.adj, vv.adj, sizeof(u32) * g.nadj, cudaMemcpyDeviceToDevice, s));
+  } else if (low == 0 && high == 1) {
+    // get_vertex_edge_star (star.cpp:135-160)
+    u32 n = count(0);
+    u32 const* voe = ask_down(1, 0);
+    UpAdj const& ev = ask_up(0, 1);
+    g.nadj = counts[1] * 2;
+    g.offs = dalloc<u32>((size_t)n + 1, s);
+    CK(cudaMemcpyAsync(g.offs, ev.offs, sizeof(u32) * (n + 1), cudaMemcpyDeviceToDevice, s));
+    g.adj = dalloc<u32>(g.nadj, s);
+    if (g.nadj) {
+      k_vertex_edge_star<<<grid_for(g.nadj), BLOCK, 0, s>>>(g.nadj, ev.adj, ev.dirs, voe, g.adj);
+      CK_LAUNCH();
+    }
+  } else if (low == 1 && high == 2) {
+    // get_edge_triangle_star (star.cpp:189-218)
+    u32 n = count(1);
+    u32 const* eot = ask_down(2, 1);
+    UpAdj const& te = ask_up(1, 2);
+    u32 nuse = counts[2] * 3;
+    g.nadj = nuse * 2;
+    g.offs = dalloc<u32>((size_t)n + 1, s);
+    k_scale_offsets<<<grid_for(n + 1), BLOCK, 0, s>>>(te.offs, n + 1, 2, g.offs);
+    CK_LAUNCH();
+    g.adj = dalloc<u32>(g.nadj, s);
+    if (nuse) {
+      k_edge_tri_star<<<grid_for(nuse), BLOCK, 0, s>>>(nuse, te.adj, te.dirs, eot, g.adj);
+      CK_LAUNCH();
+    }
+  } else if (low == 1 && high == 3 && has_dim(2)) {
+    // get_edge_tet_star (star.cpp:255-293)
+    Graph const& ts = ask_star(1, 2);
+    u32 n = count(1);
+    u32 const* eor = ask_down(3, 1);
+    UpAdj const& re = ask_up(1, 3);
+    u32* degree = dalloc<u32>(n, s);
+    if (n) {
+      k_sum_degrees<<<grid_for(n), BLOCK, 0, s>>>(n, ts.offs, re.offs, degree);
+      CK_LAUNCH();
+    }
+    g.offs = exscan_new(degree, n, s);
+    dev_free(degree, s);
+    g.nadj = ts.nadj + counts[3] * 6;
+    g.adj = dalloc<u32>(g.nadj, s);
+    if (n) {
+      k_edge_tet_star<<<grid_for(n), BLOCK, 0, s>>>(n, g.offs, ts.offs, ts.adj, re.offs,
+          re.adj, re.dirs, eor, g.adj);
+      CK_LAUNCH();
+    }
+  } else {
+    // get_star_general (star.cpp:14-111)
+    u32 n = count(low);
+    UpAdj const& hl = ask_up(low, high);
+    u32 const* loh = ask_down(high, low);
+    u32 lph = deg(high, low);
+    u32* degree = dalloc<u32>(n, s);
+    u32* err = mb->dev + 60;
+    CK(cudaMemsetAsync(err, 0, sizeof(u32), s));
+    if (n) {
+      k_star_general<<<grid_for(n), BLOCK, 0, s>>>(n, hl.offs, hl.adj, loh, lph,
+          nullptr, degree, nullptr, err);
+      CK_LAUNCH();
+    }
+    g.offs = exscan_new(degree, n, s);
+    dev_free(degree, s);
+    g.nadj = read_u32(g.offs + n, s);
+    g.adj = dalloc<u32>(g.nadj, s);
+    if (n) {
+      k_star_general<<<grid_for(n), BLOCK, 0, s>>>(n, hl.offs, hl.adj, loh, lph, g.offs,
+          nullptr, g.adj, err);
+      CK_LAUNCH();
+    }
+    if (read_u32(err, s)) throw Failure(E_ARG, "star wider than 256 entries");
+  }
+  star[low][high] = g;
+  have_star[low][high] = true;
+  return star[low][high];
+}
+
+u32 const* Mesh::ask_dual()
+{
+  if (dual) return dual;
+  u32 nel = count(dim), spe = deg(dim, dim - 1);
+  u32* out = dalloc<u32>((size_t)nel * spe, s);
+  if (has_dim(dim - 1)) {
+    u32 const* soe = ask_down(dim, dim - 1);
+    UpAdj const& es = ask_up(dim - 1, dim);
+    if (nel) {
+      k_dual_from_sides<<<grid_for(nel), BLOCK, 0, s>>>(nel, spe, soe, es.offs, es.adj, out);
+      CK_LAUNCH();
+    }
+  } else {
+    u32 const* voe = ask_down(dim, 0);
+    UpAdj const& ev = ask_up(0, dim);
+    u32* err = mb->dev + 61;
+    CK(cudaMemsetAsync(err, 0, sizeof(u32), s));
+    if (nel) {
+      k_dual_from_verts<<<grid_for((u64)nel * spe), BLOCK, 0, s>>>(dim, nel, voe, ev.offs,
+          ev.adj, out, err);
+      CK_LAUNCH();
+    }
+    if (read_u32(err, s)) throw Failure(E_ARG, "vertex with more than 256 elements");
+  }
+  dual = out;
+  return dual;
+}
+
+// ---------------------------------------------------------------------------
+// geometry: qualities, sizes, edge lengths (quality.cpp, size.cpp)
+
+__device__ inline unsigned long long order_key(double x)
+{
+  unsigned long long b = (unsigned long long)__double_as_longlong(x);
+  return (b >> 63) ? ~b : (b | (1ull << 63));
+}
+
+__host__ inline double from_order_key(unsigned long long k)
+{
+  unsigned long long b = (k >> 63) ? (k & ~(1ull << 63)) : ~k;
+  double x;
+  std::memcpy(&x, &b, sizeof(x));
+  return x;
+}
+
+__global__ void k_elem_quality(u32 dim, u32 ne, u32 const* __restrict__ voe,
+    double const* __restrict__ x, double* __restrict__ q,
+    unsigned long long* minkey)
+{
+  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+  double qi = DBL_MAX;
+  if (i < ne) {
+    u32 vpe = deg(dim, 0);
+    double ex[4][3];
+    for (u32 j = 0; j < vpe; ++j) load3(x, voe[(size_t)i * vpe + j], ex[j]);
+    qi = dim >= 2 ? elem_quality(dim, ex, 1) : 1.0;
+    q[i] = qi;
+  }
+  // min over elements below DBL_MAX, as doubles_min's `a[i] < min` keeps
+  unsigned long long key = (qi < DBL_MAX) ? order_key(qi) : ~0ull;
+  for (int o = 16; o; o >>= 1) {
+    unsigned long long other = __shfl_xor_sync(0xffffffffu, key, o);
+    key = other < key ? other : key;
+  }
+  if ((threadIdx.x & 31) == 0 && key != ~0ull) atomicMin(minkey, key);
+}
+
+// The cache holds ne qualities followed by one 8-byte slot with the
+// order-preserving key of their minimum.
+double const* Mesh::qualities()
+{
+  if (qual_cache) return qual_cache;
+  u32 ne = count(dim);
+  qual_cache = dalloc<double>((size_t)ne + 1, s);
+  unsigned long long* mk = reinterpret_cast<unsigned long long*>(qual_cache + ne);
+  CK(cudaMemsetAsync(mk, 0xff, sizeof(unsigned long long), s));
+  if (ne) {
+    PROBE(P_ELEM_QUALITY, s, 4.0 * deg(dim, 0) * ne + 24.0 * counts[0] + 8.0 * ne);
+    k_elem_quality<<<grid_for(ne), BLOCK, 0, s>>>(dim, ne, ask_down(dim, 0), coords(),
+        qual_cache, mk);
+    CK_LAUNCH();
+  }
+  return qual_cache;
+}
+
+// mesh_min_quality (quality.cpp:67-73) over every element
+double Mesh::min_quality()
+{
+  double const* q = qualities();
+  u32 ne = count(dim);
+  unsigned long long k;
+  CK(cudaMemcpyAsync(&k, q + ne, sizeof(k), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  if (k == ~0ull) return DBL_MAX;
+  return from_order_key(k);
+}
+
+__global__ void k_elem_size(u32 dim, u32 ne, u32 const* __restrict__ voe,
+    double const* __restrict__ x, double* __restrict__ out)
+{
+  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= ne) return;
+  u32 vpe = deg(dim, 0);
+  double ex[4][3];
+  for (u32 j = 0; j < vpe; ++j) load3(x, voe[(size_t)i * vpe + j], ex[j]);
+  double v;
+  if (dim == 3)
+    v = tet_volume(ex);
+  else if (dim == 2)
+    v = tri_area(ex[0], ex[1], ex[2]);
+  else
+    v = sqrt(sqdist3(ex[1], ex[0]));
+  out[i] = v;
+}
+
+double* Mesh::element_sizes()
+{
+  u32 ne = count(dim);
+  double* out = dalloc<double>(ne, s);
+  if (ne) {
+    k_elem_size<<<grid_for(ne), BLOCK, 0, s>>>(dim, ne, ask_down(dim, 0), coords(), out);
+    CK_LAUNCH();
+  }
+  return out;
+}
+
+__global__ void k_measure_edges(u32 ne, u32 const* __restrict__ voe,
+    double const* __restrict__ x, double const* __restrict__ h, double* __restrict__ out)
+{
+  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= ne) return;
+  u32 a = voe[i * 2], b = voe[i * 2 + 1];
+  double xa[3], xb[3];
+  load3(x, a, xa);
+  load3(x, b, xb);
+  double len = sqrt(sqdist3(xb, xa));
+  double want = (h[a] + h[b]) / 2;
+  out[i] = len / want;
+}
+
+double* Mesh::measure_edges()
+{
+  u32 ne = count(1);
+  Tag* t = find_tag(0, "adapt_size");
+  if (!t) throw Failure(E_ARG, "mesh has no adapt_size vertex field");
+  double* out = dalloc<double>(ne, s);
+  if (ne) {
+    k_measure_edges<<<grid_for(ne), BLOCK, 0, s>>>(ne, ask_down(1, 0), coords(),
+        static_cast<double const*>(t->data), out);
+    CK_LAUNCH();
+  }
+  return out;
+}
+
+}  // namespace osh

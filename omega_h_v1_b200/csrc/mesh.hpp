@@ -1,0 +1,119 @@
+// Device-resident mesh store with the reference's lazy adjacency cache
+// (mesh.cpp:27-334): per-dimension entity-to-vertex connectivity, tags,
+// upward / downward / star / dual adjacency derived on first request and
+// dropped when a pass replaces the mesh.
+//
+// Layout in HBM (all u32 local ids, f64 fields, u64 global numbers):
+//   down[d][0]        verts_of_ents, deg(d,0) per entity, entity-major
+//   down[h][l]        lows_of_highs (0 < l < h), deg(h,l) per high entity
+//   up[l][h]          CSR: offs[n_l+1], adj[n_uses], dirs[n_uses]; each row
+//                     sorted by use index (high * deg + dir), which is the
+//                     order the reference's CPU invert_map produces
+//   tags[d]           ordered list of named arrays, n_d * ncomps values each
+//   globals[d]        u64 global numbers (parallel meshes only)
+#pragma once
+
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "runtime.hpp"
+
+namespace osh {
+
+struct Tag {
+  std::string name;
+  u32 type = T_F64;
+  u32 ncomps = 1;
+  u32 transfer = X_NOT;
+  void* data = nullptr;  // device
+};
+
+inline u32 tag_esz(u32 type)
+{
+  return type == T_U8 ? 1u : type == T_U32 ? 4u : 8u;
+}
+
+struct UpAdj {
+  u32* offs = nullptr;
+  u32* adj = nullptr;
+  u32* dirs = nullptr;
+};
+
+struct Graph {
+  u32* offs = nullptr;
+  u32* adj = nullptr;
+  u32 nadj = 0;
+};
+
+struct Mesh {
+  u32 dim = 3;
+  bool full = false;
+  bool parallel = false;
+  u32 counts[4] = {0, 0, 0, 0};
+  u32* down[4][4] = {};
+  UpAdj up[4][4] = {};
+  bool have_up[4][4] = {};
+  Graph star[4][4] = {};
+  bool have_star[4][4] = {};
+  u32* dual = nullptr;
+  std::vector<Tag> tags[4];
+  u64* globals[4] = {};
+  u32* own_ranks[4] = {};   // cached zeros (single rank), API only
+  u32* own_ids[4] = {};     // cached iota, API only
+  u32 ghost_layers = 0;
+  double* qual_cache = nullptr;  // element qualities of this mesh state
+  cudaStream_t s = nullptr;
+  bool own_stream = false;
+  std::shared_ptr<Mailbox> mb;  // shared by a mesh and the meshes it spawns
+
+  // stream == nullptr creates (and later destroys) a stream of its own
+  Mesh(u32 dim, bool full, bool parallel, cudaStream_t stream,
+      std::shared_ptr<Mailbox> mailbox = nullptr);
+  ~Mesh();
+  Mesh(Mesh const&) = delete;
+  Mesh& operator=(Mesh const&) = delete;
+
+  // a new empty mesh on the same stream (m_out of a pass)
+  Mesh* spawn() const;
+  // a deep copy (connectivity, tags, globals; no derived adjacency) on a
+  // stream of its own
+  Mesh* clone();
+  // run all further work of this mesh on `stream` (not owned)
+  void use_stream(cudaStream_t stream);
+  // replace every array of this mesh with those of `with` (which is deleted);
+  // overwrite_mesh (mesh.cpp:329-334)
+  void overwrite(Mesh* with);
+  void clear_contents();
+
+  void set_ents(u32 d, u32 n, u32* verts);
+  bool has_dim(u32 d) const { return d == 0 || down[d][0] != nullptr; }
+  u32 count(u32 d);
+
+  u32 const* ask_down(u32 high, u32 low);
+  UpAdj const& ask_up(u32 low, u32 high);
+  Graph const& ask_star(u32 low, u32 high);
+  u32 const* ask_dual();
+
+  Tag* find_tag(u32 d, char const* name);
+  Tag& add_tag(u32 d, u32 type, char const* name, u32 ncomps, u32 transfer,
+      void* data);
+  void remove_tag(u32 d, char const* name);
+  double const* coords();
+
+  // element qualities (cached until the mesh changes) and their minimum
+  double const* qualities();
+  double min_quality();
+  double* element_sizes();      // caller frees
+  double* measure_edges();      // caller frees: |x1-x0| / mean size
+
+  void set_globals(u32 d, u64* g);
+  void derive_model(double crease_angle);  // host classification
+  void make_parallel();
+};
+
+// derivation helpers (mesh.cu)
+void up_from_down(u32 high, u32 low, u32 nhighs, u32 nlows, u32 const* lows_of_highs,
+    UpAdj& out, cudaStream_t s);
+
+}  // namespace osh

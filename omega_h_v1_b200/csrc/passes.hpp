@@ -1,0 +1,100 @@
+// The adaptation passes (refine / coarsen / swap / adapt driver) and the
+// pieces they share: independent sets, class inheritance, expansion.
+#pragma once
+
+#include "mesh.hpp"
+
+namespace osh {
+
+// Luby independent set over the star graph of `ent_dim` entities
+// (mesh_find_indset, indset.cpp:119-139). filter and goodness are device
+// arrays; returns a device state array (1 = in set) or throws E_NOCONVERGE.
+u32* find_indset(Mesh& m, u32 ent_dim, u32 const* filter, double const* goodness);
+
+// copy rows of `width` elements: out[j] = in[i] for j in
+// [offs[i]*k, offs[i+1]*k), for T of 1, 4 or 8 bytes
+void expand_scaled(void const* in, u32 const* offs, u32 k, u32 n, u32 width,
+    u32 esz, void* out, cudaStream_t s);
+
+// Per-dimension domains that produce entities of one dimension during a
+// pass: ndoms[d] entities of dimension d, each producing
+// (offs[d][i+1]-offs[d][i]) * scale[d] products. Slot 0 is the "same"
+// entities carried over from the old mesh. (inherit.cpp:8-138)
+struct Doms {
+  u32 ndoms[4] = {0, 0, 0, 0};
+  u32 const* offs[4] = {nullptr, nullptr, nullptr, nullptr};
+  u32 scale[4] = {1, 1, 1, 1};
+  u32 ngen[4] = {0, 0, 0, 0};  // host copy of each domain's product count
+  u32 ngo[5] = {0, 0, 0, 0, 0};
+  void finish()
+  {
+    ngo[0] = 0;
+    for (u32 i = 0; i < 4; ++i) ngo[i + 1] = ngo[i] + ngen[i];
+  }
+};
+
+// class_dim / class_id of the products of `prod_dim` (inherit_class,
+// inherit.cpp:217-232)
+void inherit_class(Mesh& m, Mesh& out, u32 prod_dim, Doms const& d);
+
+// u64 global numbering of a single-rank parallel mesh after a pass
+// (inherit_globals, parallel_modify.cpp:79-111): survivors keep their order,
+// new entities follow.
+void inherit_globals(Mesh& out, u32 d, u32 n);
+
+// element coordinates (interp_to_elems of "coordinates", element_field.cpp)
+void interp_coords_to_elems(Mesh& m);
+
+u32 refine_by_size(Mesh& m, double qual_floor);
+void uniformly_refine(Mesh& m);
+u32 coarsen_by_size(Mesh& m, double qual_floor, double size_floor);
+u32 coarsen_slivers(Mesh& m, double qual_floor, u32 nlayers);
+u32 swap_slivers(Mesh& m, double good_qual, u32 nlayers);
+u32 mesh_adapt(Mesh& m, double size_floor, double good_qual, u32 nlayers, u32 max_ops);
+
+// per-stage sets of each pass, without modifying the mesh (device outputs)
+u32 refine_sets(Mesh& m, double qual_floor, u32* cand, u32* good, double* quals,
+    u32* indset);
+u32 coarsen_sets(Mesh& m, double qual_floor, double size_floor, u32* codes_size,
+    u32* codes_class, u32* codes_qual, double* quals2, u32* cand, double* col_qual,
+    u32* indset, u32* gen_vert);
+u32 swap_sets(Mesh& m, double good_qual, u32 nlayers, u32* slivers, u32* cand,
+    u32* interior, u32* good, double* quals, u32* ring_sizes, u32* indset);
+
+// mark helpers (mark.cpp)
+u32* mark_down(Mesh& m, u32 high, u32 low, u32 const* marked_highs);
+u32* mark_up(Mesh& m, u32 low, u32 high, u32 const* marked_lows);
+u32* mark_slivers(Mesh& m, double good_qual, u32 nlayers);
+
+// small device counter helpers
+struct Counter {
+  u32* d;
+  cudaStream_t s;
+  explicit Counter(cudaStream_t st) : s(st)
+  {
+    d = dalloc<u32>(1, s);
+    CK(cudaMemsetAsync(d, 0, sizeof(u32), s));
+  }
+  ~Counter() { cudaFreeAsync(d, s); }
+  void zero() { CK(cudaMemsetAsync(d, 0, sizeof(u32), s)); }
+  u32 get() { return read_u32(d, s); }
+};
+
+// per-pass statistics, read by the C API for reporting
+struct PassStats {
+  u32 op = 0;            // 1 refine, 2 coarsen, 3 swap, 4 coarsen_slivers
+  u32 elems_in = 0;
+  u32 elems_out = 0;
+  u32 nselected = 0;     // split edges / collapsed verts / swapped edges
+  u32 indset_rounds = 0;
+};
+PassStats& last_pass_stats();
+
+// statistics of the last mesh_adapt call on this thread
+struct AdaptStats {
+  u32 passes = 0;          // passes that changed the mesh
+  double elems_in = 0;     // elements entering those passes, summed
+};
+AdaptStats& last_adapt_stats();
+
+}  // namespace osh

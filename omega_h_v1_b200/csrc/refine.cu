@@ -1,0 +1,412 @@
+// Edge refinement on sm_100a: refine_by_size / uniformly_refine
+// (refine.cpp:11-35, refine_common.cpp:29-190, refine_qualities.cpp:16-82,
+// splits_to_domains.cpp:13-56, refine_topology.cpp:26-120,
+// refine_nodal.cpp:10-46, refine_conserve.cpp, refine_fit.cpp).
+//
+// Numbering of the new mesh follows the reference exactly: entities that do
+// not split keep their order; products follow, grouped by the dimension of
+// the domain that produced them and ordered by that domain's index (exclusive
+// scans of the split marks), with new vertices appended in split-edge order.
+#include "passes.hpp"
+
+namespace osh {
+
+// refine_candidate (refine.cpp:11-15) fused with measure_edge (size.cpp:57)
+__global__ void k_refine_candidates(u32 ne, u32 const* __restrict__ voe,
+    double const* __restrict__ x, double const* __restrict__ h, u32* __restrict__ cand,
+    u32* any)
+{
+  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+  u32 c = 0;
+  if (i < ne) {
+    u32 a = voe[i * 2], b = voe[i * 2 + 1];
+    double xa[3], xb[3];
+    load3(x, a, xa);
+    load3(x, b, xb);
+    double len = sqrt(sqdist3(xb, xa));
+    double want = (h[a] + h[b]) / 2;
+    c = (len / want) > 1.0;
+    cand[i] = c;
+  }
+  if (__any_sync(0xffffffffu, c) && (threadIdx.x & 31) == 0) atomicOr(any, 1u);
+}
+
+// refine_quality (refine_qualities.cpp:16-82) for edges, require_better = 0:
+// the worst child of every element around the edge, split at its midpoint
+__global__ void k_refine_quality(u32 dim, u32 ne, u32 const* __restrict__ voe1,
+    u32 const* __restrict__ voe, u32 const* __restrict__ eo_offs,
+    u32 const* __restrict__ eo, u32 const* __restrict__ eo_dirs,
+    double const* __restrict__ x, double qual_floor, u32* __restrict__ cand,
+    double* __restrict__ out, u32* any, u32* inverted)
+{
+  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+  u32 keep = 0;
+  if (i < ne && cand[i]) {
+    u32 vpe = deg(dim, 0);
+    double const perfect = dim == 3 ? perfect_tet_quality() : perfect_tri_quality();
+    u32 a = voe1[i * 2], b = voe1[i * 2 + 1];
+    double split[3];
+    // average_element_field: (0 + x_a + x_b) / 2 per component
+    for (u32 c = 0; c < 3; ++c) {
+      double acc = 0;
+      acc += x[a * 3 + c];
+      acc += x[b * 3 + c];
+      split[c] = acc / 2u;
+    }
+    double minq = 1;
+    for (u32 j = eo_offs[i]; j < eo_offs[i + 1]; ++j) {
+      u32 dir = eo_dirs[j], e = eo[j];
+      u32 const* ve = voe + (size_t)e * vpe;
+      for (u32 k = 0; k < 2; ++k) {
+        u32 o = canon(dim, 1, 0, dir, k);
+        u32 base = opp(dim, 0, o);
+        double ex[4][3];
+        for (u32 l = 0; l + 1 < vpe; ++l) load3(x, ve[canon(dim, dim - 1, 0, base, l)], ex[l]);
+        ex[vpe - 1][0] = split[0];
+        ex[vpe - 1][1] = split[1];
+        ex[vpe - 1][2] = split[2];
+        double q = dim == 3 ? tet_quality(ex, perfect) : tri_quality(ex, 0, perfect);
+        if (!(q > 0)) atomicOr(inverted, 1u);
+        if (q < minq) minq = q;
+      }
+    }
+    if (minq < qual_floor) {
+      cand[i] = 0;
+    } else {
+      out[i] = minq;
+      keep = 1;
+    }
+  }
+  if (__any_sync(0xffffffffu, keep) && (threadIdx.x & 31) == 0) atomicOr(any, 1u);
+}
+
+// refine_node (refine_nodal.cpp:10-25)
+__global__ void k_refine_nodal(u32 ne, u32 nv, u32 const* __restrict__ voe,
+    u32 const* __restrict__ gen_offs, u32 nc, double const* __restrict__ f,
+    double* __restrict__ out)
+{
+  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= ne || gen_offs[i] == gen_offs[i + 1]) return;
+  u32 a = voe[i * 2], b = voe[i * 2 + 1];
+  double* o = out + (size_t)(nv + gen_offs[i]) * nc;
+  for (u32 c = 0; c < nc; ++c) {
+    double acc = 0;
+    acc += f[(size_t)a * nc + c];
+    acc += f[(size_t)b * nc + c];
+    o[c] = acc / 2u;
+  }
+}
+
+// split_to_domain (splits_to_domains.cpp:13-31): first split edge of each
+// domain, in the domain's local edge order
+__global__ void k_split_to_domain(u32 nd, u32 spd, u32 const* __restrict__ sod,
+    u32 const* __restrict__ gen_offs, u32 nv, u32* __restrict__ will,
+    u32* __restrict__ dir, u32* __restrict__ vert)
+{
+  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nd) return;
+  u32 w = 0, d = INV, v = INV;
+  for (u32 j = 0; j < spd; ++j) {
+    u32 s = sod ? sod[(size_t)i * spd + j] : i;
+    if (gen_offs[s] == gen_offs[s + 1]) continue;
+    w = 1;
+    d = j;
+    v = nv + gen_offs[s];
+    break;
+  }
+  will[i] = w;
+  dir[i] = d;
+  vert[i] = v;
+}
+
+// refine_domain_entity (refine_topology.cpp:26-64)
+__global__ void k_refine_topology(u32 dd, u32 prod, u32 nd, u32 const* __restrict__ vod,
+    u32 const* __restrict__ offs, u32 const* __restrict__ dir,
+    u32 const* __restrict__ vert, u32* __restrict__ out)
+{
+  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nd || offs[i] == offs[i + 1]) return;
+  u32 base_dim = prod - 1, opp_dim = dd - 1 - base_dim;
+  u32 ops = deg(1, opp_dim), vpp = deg(prod, 0), vpb = vpp - 1, vpd = deg(dd, 0);
+  u32* p = out + (size_t)offs[i] * ops * vpp;
+  u32 di = dir[i];
+  for (u32 j = 0; j < ops; ++j) {
+    u32 o = canon(dd, 1, opp_dim, di, j);
+    u32 b = opp(dd, opp_dim, o);
+    for (u32 k = 0; k < vpb; ++k) p[k] = vod[(size_t)i * vpd + canon(dd, base_dim, 0, b, k)];
+    p[vpb] = vert[i];
+    p += vpp;
+  }
+}
+
+// refine_conserve_elem / refine_fit_elem (refine_conserve.cpp:10-21,
+// refine_fit.cpp:10-20): each product gets the value (divided by the number
+// of products when conserving)
+__global__ void k_refine_elem_field(u32 n, u32 const* __restrict__ offs, u32 k,
+    u32 nc, int conserve, double const* __restrict__ in, double* __restrict__ out)
+{
+  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  u32 f = offs[i] * k, e = offs[i + 1] * k;
+  double denom = e - f;
+  for (u32 j = f; j < e; ++j)
+    for (u32 c = 0; c < nc; ++c)
+      out[(size_t)j * nc + c] = conserve ? in[(size_t)i * nc + c] / denom : in[(size_t)i * nc + c];
+}
+
+static u32 prods_per_dom(u32 dom, u32 src, u32 prod)
+{
+  // get_prods_per_dom (refine_topology.cpp:110-120)
+  if (prod == 0) return dom == src ? 1 : 0;
+  u32 base = prod - 1, o = dom - 1 - base;
+  if (src < o) return 0;
+  return deg(src, o);
+}
+
+struct Splits {
+  u32* offs = nullptr;
+  u32* dir = nullptr;
+  u32* vert = nullptr;
+  u32 nsplit = 0;
+};
+
+static void refine_build(Mesh& m, u32 const* gen_offs, u32 nsplit)
+{
+  cudaStream_t s = m.s;
+  u32 dim = m.dim, src = 1;
+  u32 nv = m.count(0), ns = m.count(src);
+  Mesh* out = m.spawn();
+  // refine_verts (refine_common.cpp:29-54)
+  u32 nv_out = nv + nsplit;
+  out->set_ents(0, nv_out, nullptr);
+  u32 const* voe1 = m.ask_down(1, 0);
+  for (auto const& t : m.tags[0]) {
+    if (t.type != T_F64) continue;
+    double* d = dalloc<double>((size_t)nv_out * t.ncomps, s);
+    CK(cudaMemcpyAsync(d, t.data, sizeof(double) * nv * t.ncomps, cudaMemcpyDeviceToDevice, s));
+    if (ns) {
+      k_refine_nodal<<<grid_for(ns), BLOCK, 0, s>>>(ns, nv, voe1, gen_offs, t.ncomps,
+          static_cast<double const*>(t.data), d);
+      CK_LAUNCH();
+    }
+    out->add_tag(0, T_F64, t.name.c_str(), t.ncomps, X_NOT, d);
+  }
+  if (m.parallel) inherit_globals(*out, 0, nv_out);
+  // splits_to_domains for every domain dimension
+  Splits sp[4];
+  u32* zero_v = dalloc<u32>((size_t)nv + 1, s);
+  fill_u32(zero_v, nv + 1, 0, s);
+  sp[0].offs = zero_v;
+  for (u32 dd = 1; dd <= dim; ++dd) {
+    if (!m.has_dim(dd)) continue;
+    u32 nd = m.count(dd);
+    u32 const* sod = dd == 1 ? nullptr : m.ask_down(dd, 1);
+    u32* will = dalloc<u32>(nd, s);
+    sp[dd].dir = dalloc<u32>(nd, s);
+    sp[dd].vert = dalloc<u32>(nd, s);
+    if (nd) {
+      k_split_to_domain<<<grid_for(nd), BLOCK, 0, s>>>(nd, deg(dd, 1), sod, gen_offs, nv,
+          will, sp[dd].dir, sp[dd].vert);
+      CK_LAUNCH();
+    }
+    sp[dd].offs = exscan_new(will, nd, s);
+    dev_free(will, s);
+    CK(cudaMemcpyAsync(m.mb->dev + 8 + dd, sp[dd].offs + nd, sizeof(u32),
+        cudaMemcpyDeviceToDevice, s));
+  }
+  m.mb->fetch(s, 16);
+  for (u32 dd = 1; dd <= dim; ++dd)
+    if (m.has_dim(dd)) sp[dd].nsplit = m.mb->host[8 + dd];
+  // products of every dimension (refine_common.cpp:90-123, inherit.cpp:104-138)
+  for (u32 prod = 0; prod <= dim; ++prod) {
+    if (!m.full && 0 < prod && prod < dim) continue;
+    u32 np = m.count(prod);
+    Doms d;
+    u32* same = negate_offsets(sp[prod].offs, np, s);
+    d.ndoms[0] = np;
+    d.offs[0] = same;
+    d.scale[0] = 1;
+    u32 first, last;
+    if (m.full) {
+      first = src > prod ? src : prod;
+      last = dim;
+    } else {
+      first = last = (prod == 0) ? src : dim;
+    }
+    for (u32 dd = first; dd <= last; ++dd) {
+      d.ndoms[dd] = m.count(dd);
+      d.offs[dd] = sp[dd].offs;
+      d.scale[dd] = prods_per_dom(dd, src, prod);
+      d.ngen[dd] = sp[dd].nsplit * d.scale[dd];
+    }
+    d.ngen[0] = np - sp[prod].nsplit;
+    d.finish();
+    if (prod) {
+      u32 vpp = deg(prod, 0), nout = d.ngo[4];
+      u32* conn = dalloc<u32>((size_t)nout * vpp, s);
+      expand_scaled(m.ask_down(prod, 0), same, 1, np, vpp, 4, conn, s);
+      for (u32 dd = first; dd <= last; ++dd) {
+        if (!d.ndoms[dd] || !d.scale[dd] || !sp[dd].nsplit) continue;
+        u32 nd = d.ndoms[dd];
+        PROBE(P_REFINE_TOPOLOGY, s, 4.0 * deg(dd, 0) * nd + 12.0 * nd + 4.0 * (nd + 1) +
+            4.0 * vpp * (double)d.ngen[dd]);
+        k_refine_topology<<<grid_for(nd), BLOCK, 0, s>>>(dd, prod, nd, m.ask_down(dd, 0),
+            sp[dd].offs, sp[dd].dir, sp[dd].vert, conn + (size_t)d.ngo[dd] * vpp);
+        CK_LAUNCH();
+      }
+      out->set_ents(prod, nout, conn);
+      if (m.parallel) inherit_globals(*out, prod, nout);
+    }
+    inherit_class(m, *out, prod, d);
+    if (prod == dim) {
+      for (int pass = 0; pass < 2; ++pass) {
+        u32 want = pass == 0 ? X_CONSERVE : X_POINTWISE;
+        for (auto const& t : m.tags[dim]) {
+          if (t.type != T_F64 || t.transfer != want) continue;
+          u32 nc = t.ncomps;
+          double* data = dalloc<double>((size_t)d.ngo[4] * nc, s);
+          expand_scaled(t.data, same, 1, np, nc, 8, data, s);
+          if (d.ngen[dim]) {
+            k_refine_elem_field<<<grid_for(np), BLOCK, 0, s>>>(np, sp[dim].offs,
+                d.scale[dim], nc, pass == 0, static_cast<double const*>(t.data),
+                data + (size_t)d.ngo[dim] * nc);
+            CK_LAUNCH();
+          }
+          out->add_tag(dim, T_F64, t.name.c_str(), nc, t.transfer, data);
+        }
+      }
+    }
+    dev_free(same, s);
+  }
+  for (u32 dd = 0; dd <= dim; ++dd) {
+    dev_free(sp[dd].offs, s);
+    dev_free(sp[dd].dir, s);
+    dev_free(sp[dd].vert, s);
+  }
+  m.overwrite(out);
+}
+
+// choose_refinement_indset (refine_common.cpp:131-160) on a candidate array
+// the caller owns; returns the independent set or nullptr when nothing
+// qualifies. quals_out (optional) receives the goodness.
+static u32* choose_refinement(Mesh& m, u32* cand, double qual_floor, double** quals_out)
+{
+  cudaStream_t s = m.s;
+  u32 ne = m.count(1), dim = m.dim;
+  double* q = dalloc<double>(ne, s);
+  CK(cudaMemsetAsync(q, 0, sizeof(double) * ne, s));
+  u32* any = m.mb->dev + 1;
+  u32* inverted = m.mb->dev + 2;
+  CK(cudaMemsetAsync(any, 0, 2 * sizeof(u32), s));
+  if (dim >= 2) {
+    UpAdj const& eo = m.ask_up(1, dim);
+    if (ne) {
+      // refine_quality bytes (edges' up CSR, elements, coordinates, flags)
+      double nel = m.counts[dim];
+      PROBE(P_REFINE_QUALITY, s, 4.0 * (ne + 1) + 8.0 * deg(dim, 1) * nel + 8.0 * ne +
+          4.0 * deg(dim, 0) * nel + 24.0 * m.counts[0] + 8.0 * ne + 8.0 * ne);
+      k_refine_quality<<<grid_for(ne), BLOCK, 0, s>>>(dim, ne, m.ask_down(1, 0),
+          m.ask_down(dim, 0), eo.offs, eo.adj, eo.dirs, m.coords(), qual_floor, cand, q,
+          any, inverted);
+      CK_LAUNCH();
+    }
+    m.mb->fetch(s, 4);
+  } else {
+    m.mb->host[1] = max_u32(cand, ne, s) ? 1 : 0;
+  }
+  if (!m.mb->host[1]) {
+    if (quals_out)
+      *quals_out = q;
+    else
+      dev_free(q, s);
+    return nullptr;
+  }
+  u32* ind = find_indset(m, 1, cand, q);
+  if (quals_out)
+    *quals_out = q;
+  else
+    dev_free(q, s);
+  return ind;
+}
+
+static u32 refine_common(Mesh& m, u32* cand, double qual_floor)
+{
+  cudaStream_t s = m.s;
+  PassStats& st = last_pass_stats();
+  st = PassStats();
+  st.op = 1;
+  st.elems_in = m.count(m.dim);
+  u32 ne = m.count(1);
+  u32* ind = choose_refinement(m, cand, qual_floor, nullptr);
+  if (!ind) return 0;
+  u32* gen_offs = exscan_new(ind, ne, s);
+  dev_free(ind, s);
+  u32 nsplit = read_u32(gen_offs + ne, s);
+  refine_build(m, gen_offs, nsplit);
+  dev_free(gen_offs, s);
+  st.nselected = nsplit;
+  st.elems_out = m.count(m.dim);
+  return 1;
+}
+
+u32 refine_by_size(Mesh& m, double qual_floor)
+{
+  cudaStream_t s = m.s;
+  u32 ne = m.count(1);
+  Tag* h = m.find_tag(0, "adapt_size");
+  if (!h) throw Failure(E_ARG, "mesh has no adapt_size vertex field");
+  u32* cand = dalloc<u32>(ne, s);
+  u32* any = m.mb->dev + 3;
+  CK(cudaMemsetAsync(any, 0, sizeof(u32), s));
+  if (ne) {
+    PROBE(P_REFINE_CANDIDATES, s, 8.0 * ne + 32.0 * m.counts[0] + 4.0 * ne);
+    k_refine_candidates<<<grid_for(ne), BLOCK, 0, s>>>(ne, m.ask_down(1, 0), m.coords(),
+        static_cast<double const*>(h->data), cand, any);
+    CK_LAUNCH();
+  }
+  u32 r = 0;
+  if (read_u32(any, s)) r = refine_common(m, cand, qual_floor);
+  dev_free(cand, s);
+  return r;
+}
+
+void uniformly_refine(Mesh& m)
+{
+  u32 ne = m.count(1);
+  u32* cand = dalloc<u32>(ne, m.s);
+  fill_u32(cand, ne, 1, m.s);
+  if (ne) refine_common(m, cand, 0.0);
+  dev_free(cand, m.s);
+}
+
+u32 refine_sets(Mesh& m, double qual_floor, u32* cand_out, u32* good_out,
+    double* quals_out, u32* indset_out)
+{
+  cudaStream_t s = m.s;
+  u32 ne = m.count(1);
+  Tag* h = m.find_tag(0, "adapt_size");
+  if (!h) throw Failure(E_ARG, "mesh has no adapt_size vertex field");
+  u32* any = m.mb->dev + 3;
+  CK(cudaMemsetAsync(any, 0, sizeof(u32), s));
+  CK(cudaMemsetAsync(indset_out, 0, sizeof(u32) * ne, s));
+  if (ne) {
+    k_refine_candidates<<<grid_for(ne), BLOCK, 0, s>>>(ne, m.ask_down(1, 0), m.coords(),
+        static_cast<double const*>(h->data), cand_out, any);
+    CK_LAUNCH();
+  }
+  CK(cudaMemcpyAsync(good_out, cand_out, sizeof(u32) * ne, cudaMemcpyDeviceToDevice, s));
+  double* q = nullptr;
+  u32* ind = choose_refinement(m, good_out, qual_floor, &q);
+  CK(cudaMemcpyAsync(quals_out, q, sizeof(double) * ne, cudaMemcpyDeviceToDevice, s));
+  dev_free(q, s);
+  if (!ind) {
+    CK(cudaStreamSynchronize(s));
+    return 0;
+  }
+  CK(cudaMemcpyAsync(indset_out, ind, sizeof(u32) * ne, cudaMemcpyDeviceToDevice, s));
+  dev_free(ind, s);
+  CK(cudaStreamSynchronize(s));
+  return 1;
+}
+
+}  // namespace osh

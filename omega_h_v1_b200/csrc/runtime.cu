@@ -1,0 +1,493 @@
+// Device runtime for the adaptation pass: error state, stream-ordered
+// allocation, the decoupled look-back exclusive scan and small array kernels.
+#include <cstdio>
+#include <cstring>
+#include <atomic>
+#include <mutex>
+#include <vector>
+
+#include "runtime.hpp"
+
+namespace osh {
+
+// ---------------------------------------------------------------------------
+// errors
+
+namespace {
+thread_local int t_err = 0;
+thread_local std::string t_msg;
+}  // namespace
+
+void set_error(int code, char const* msg)
+{
+  t_err = code;
+  t_msg = msg ? msg : "";
+}
+int last_error() { return t_err; }
+char const* last_error_message() { return t_msg.c_str(); }
+void clear_error()
+{
+  t_err = 0;
+  t_msg.clear();
+}
+
+void check_cuda(cudaError_t e, char const* what, char const* file, int line)
+{
+  if (e == cudaSuccess) return;
+  char buf[512];
+  snprintf(buf, sizeof(buf), "%s failed: %s (%s:%d)", what, cudaGetErrorString(e),
+      file, line);
+  throw Failure(e == cudaErrorMemoryAllocation ? E_NOMEM : E_CUDA, buf);
+}
+
+// ---------------------------------------------------------------------------
+// launch counter (every kernel launch goes through CK_LAUNCH)
+
+namespace {
+std::atomic<unsigned long long> g_launches{0};
+}
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+unsigned long long launch_count() { return g_launches.load(); }
+
+// ---------------------------------------------------------------------------
+// probes
+
+namespace {
+struct ProbeState {
+  u32 mask = 0;
+  struct Rec {
+    cudaEvent_t a, b;
+    double bytes;
+  };
+  std::vector<Rec> recs[P_NPROBES];
+  u32 launches[P_NPROBES] = {};
+  double ms[P_NPROBES] = {};
+  double bytes[P_NPROBES] = {};
+  std::mutex mu;
+};
+ProbeState& probes()
+{
+  static ProbeState p;
+  return p;
+}
+char const* const g_probe_names[P_NPROBES] = {"reflect_down", "up_count", "up_fill",
+    "up_rank", "exscan", "elem_quality", "refine_candidates", "refine_quality",
+    "indset_round", "coarsen_quality", "swap_quality", "refine_topology",
+    "collapse_to_ent", "expand"};
+}  // namespace
+
+char const* probe_name(u32 id) { return id < P_NPROBES ? g_probe_names[id] : nullptr; }
+
+void probe_enable(u32 mask) { probes().mask = mask; }
+
+static void probe_resolve(ProbeState& p)
+{
+  for (u32 i = 0; i < P_NPROBES; ++i) {
+    for (auto& r : p.recs[i]) {
+      float t = 0;
+      CK(cudaEventSynchronize(r.b));
+      CK(cudaEventElapsedTime(&t, r.a, r.b));
+      p.launches[i] += 1;
+      p.ms[i] += t;
+      p.bytes[i] += r.bytes;
+      cudaEventDestroy(r.a);
+      cudaEventDestroy(r.b);
+    }
+    p.recs[i].clear();
+  }
+}
+
+void probe_reset()
+{
+  ProbeState& p = probes();
+  std::lock_guard<std::mutex> g(p.mu);
+  probe_resolve(p);
+  for (u32 i = 0; i < P_NPROBES; ++i) {
+    p.launches[i] = 0;
+    p.ms[i] = 0;
+    p.bytes[i] = 0;
+  }
+}
+
+void probe_read(u32 id, u32* launches, double* ms, double* bytes)
+{
+  ProbeState& p = probes();
+  std::lock_guard<std::mutex> g(p.mu);
+  probe_resolve(p);
+  *launches = p.launches[id];
+  *ms = p.ms[id];
+  *bytes = p.bytes[id];
+}
+
+ProbeScope::ProbeScope(u32 i, cudaStream_t st, double by) : id(i), bytes(by), s(st)
+{
+  if (!((probes().mask >> id) & 1u)) return;
+  CK(cudaEventCreate(&a));
+  CK(cudaEventCreate(&b));
+  CK(cudaEventRecord(a, s));
+}
+
+ProbeScope::~ProbeScope()
+{
+  if (!a) return;
+  cudaEventRecord(b, s);
+  ProbeState& p = probes();
+  std::lock_guard<std::mutex> g(p.mu);
+  p.recs[id].push_back({a, b, bytes});
+}
+
+// ---------------------------------------------------------------------------
+// allocation: the device's default memory pool, never trimmed between passes
+
+namespace {
+std::once_flag g_pool_once[64];
+}
+
+static void setup_pool()
+{
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  std::call_once(g_pool_once[dev & 63], [dev]() {
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+      unsigned long long thr = ~0ull;
+      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    }
+  });
+}
+
+void* dev_alloc(size_t bytes, cudaStream_t s)
+{
+  setup_pool();
+  void* p = nullptr;
+  if (bytes < 16) bytes = 16;
+  cudaError_t e = cudaMallocAsync(&p, bytes, s);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    char buf[128];
+    snprintf(buf, sizeof(buf), "device allocation of %zu bytes failed", bytes);
+    throw Failure(E_NOMEM, buf);
+  }
+  return p;
+}
+
+void dev_free(void* p, cudaStream_t s)
+{
+  if (p) CK(cudaFreeAsync(p, s));
+}
+
+u32 read_u32(u32 const* d, cudaStream_t s)
+{
+  u32 v = 0;
+  CK(cudaMemcpyAsync(&v, d, sizeof(u32), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  return v;
+}
+
+double read_f64(double const* d, cudaStream_t s)
+{
+  double v = 0;
+  CK(cudaMemcpyAsync(&v, d, sizeof(double), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  return v;
+}
+
+void Mailbox::init(cudaStream_t s)
+{
+  if (host) return;
+  CK(cudaMallocHost(&host, 64 * sizeof(u32)));
+  dev = dalloc<u32>(64, s);
+  clear(s);
+}
+
+void Mailbox::release()
+{
+  if (host) cudaFreeHost(host);
+  if (dev) cudaFree(dev);
+  host = nullptr;
+  dev = nullptr;
+}
+
+void Mailbox::clear(cudaStream_t s)
+{
+  CK(cudaMemsetAsync(dev, 0, 64 * sizeof(u32), s));
+}
+
+void Mailbox::fetch(cudaStream_t s, u32 nslots)
+{
+  CK(cudaMemcpyAsync(host, dev, nslots * sizeof(u32), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+}
+
+// ---------------------------------------------------------------------------
+// exclusive scan, single pass with decoupled look-back.
+//
+// Tiles are claimed through an atomic ticket, so every tile a block waits on
+// was claimed (and is running or done) before it. Each tile publishes its
+// aggregate, then walks back over predecessors until it meets an inclusive
+// prefix. The walk is bounded: after SCAN_SPIN_LIMIT empty polls it records
+// E_TIMEOUT in the error word and stops instead of spinning forever.
+
+constexpr int SCAN_THREADS = 256;
+constexpr int SCAN_ITEMS = 8;
+constexpr int SCAN_TILE = SCAN_THREADS * SCAN_ITEMS;
+constexpr int SCAN_WARPS = SCAN_THREADS / 32;
+constexpr unsigned long long FLAG_AGG = 1ull << 62;
+constexpr unsigned long long FLAG_PRE = 2ull << 62;
+constexpr u32 SCAN_SPIN_LIMIT = 1u << 24;
+
+// set by any bounded device wait that gave up; read by check_device_timeouts
+__device__ u32 d_wait_timeouts;
+
+__global__ void __launch_bounds__(SCAN_THREADS)
+k_exscan(u32 const* __restrict__ in, u32* __restrict__ out, u32 n, u32 ntiles,
+    unsigned long long* status, u32* ticket_and_err)
+{
+  __shared__ u32 s_tile;
+  __shared__ u32 s_warp[SCAN_WARPS];
+  __shared__ u32 s_prefix;
+  __shared__ u32 s_buf[SCAN_TILE + SCAN_TILE / 32];
+  if (threadIdx.x == 0) s_tile = atomicAdd(ticket_and_err, 1u);
+  __syncthreads();
+  u32 const tile = s_tile;
+  if (tile >= ntiles) return;
+  size_t const base = (size_t)tile * SCAN_TILE;
+  // coalesced load into shared memory (padded to avoid bank conflicts)
+#pragma unroll
+  for (int k = 0; k < SCAN_ITEMS; ++k) {
+    u32 li = k * SCAN_THREADS + threadIdx.x;
+    size_t gi = base + li;
+    s_buf[li + (li >> 5)] = gi < n ? in[gi] : 0u;
+  }
+  __syncthreads();
+  u32 v[SCAN_ITEMS];
+  u32 sum = 0;
+#pragma unroll
+  for (int k = 0; k < SCAN_ITEMS; ++k) {
+    u32 li = threadIdx.x * SCAN_ITEMS + k;
+    v[k] = s_buf[li + (li >> 5)];
+    sum += v[k];
+  }
+  u32 const lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  u32 x = sum;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    u32 y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= (u32)o) x += y;
+  }
+  if (lane == 31) s_warp[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    u32 w = lane < SCAN_WARPS ? s_warp[lane] : 0u;
+#pragma unroll
+    for (int o = 1; o < SCAN_WARPS; o <<= 1) {
+      u32 y = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= (u32)o) w += y;
+    }
+    if (lane < SCAN_WARPS) s_warp[lane] = w;
+  }
+  __syncthreads();
+  u32 const thread_excl = (warp ? s_warp[warp - 1] : 0u) + x - sum;
+  u32 const total = s_warp[SCAN_WARPS - 1];
+  if (threadIdx.x == 0) {
+    u32 prefix = 0;
+    if (tile == 0) {
+      atomicExch(&status[0], FLAG_PRE | (unsigned long long)total);
+    } else {
+      atomicExch(&status[tile], FLAG_AGG | (unsigned long long)total);
+      int p = (int)tile - 1;
+      u32 spins = 0;
+      while (p >= 0) {
+        unsigned long long st = *((volatile unsigned long long*)&status[p]);
+        unsigned long long flag = st & (3ull << 62);
+        if (flag == 0) {
+          if (++spins > SCAN_SPIN_LIMIT) {
+            atomicOr(&d_wait_timeouts, 1u);
+            break;
+          }
+          continue;
+        }
+        prefix += (u32)st;
+        if (flag == FLAG_PRE) break;
+        --p;
+      }
+      atomicExch(&status[tile], FLAG_PRE | (unsigned long long)(prefix + total));
+    }
+    s_prefix = prefix;
+  }
+  __syncthreads();
+  u32 run = s_prefix + thread_excl;
+#pragma unroll
+  for (int k = 0; k < SCAN_ITEMS; ++k) {
+    u32 li = threadIdx.x * SCAN_ITEMS + k;
+    s_buf[li + (li >> 5)] = run;
+    run += v[k];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < SCAN_ITEMS; ++k) {
+    u32 li = k * SCAN_THREADS + threadIdx.x;
+    size_t gi = base + li;
+    if (gi < n) out[gi] = s_buf[li + (li >> 5)];
+  }
+  if (tile == ntiles - 1 && threadIdx.x == 0) out[n] = s_prefix + total;
+}
+
+__global__ void k_set_zero_total(u32* out) { out[0] = 0; }
+
+void exscan_u32(u32 const* in, u32* out, u32 n, cudaStream_t s)
+{
+  if (n == 0) {
+    k_set_zero_total<<<1, 1, 0, s>>>(out);
+    CK_LAUNCH();
+    return;
+  }
+  u32 ntiles = ceil_div(n, SCAN_TILE);
+  // [ticket, error, pad, pad][status per tile]
+  size_t words = 4 + 2 * (size_t)ntiles;
+  u32* scratch = dalloc<u32>(words, s);
+  CK(cudaMemsetAsync(scratch, 0, words * sizeof(u32), s));
+  {
+    PROBE(P_EXSCAN, s, 4.0 * n + 4.0 * (n + 1));
+    k_exscan<<<ntiles, SCAN_THREADS, 0, s>>>(in, out, n, ntiles,
+        reinterpret_cast<unsigned long long*>(scratch + 4), scratch);
+    CK_LAUNCH();
+  }
+  dev_free(scratch, s);
+}
+
+void check_device_timeouts(cudaStream_t s)
+{
+  u32 v = 0;
+  CK(cudaMemcpyFromSymbolAsync(&v, d_wait_timeouts, sizeof(u32), 0,
+      cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  if (v) {
+    u32 zero = 0;
+    CK(cudaMemcpyToSymbolAsync(d_wait_timeouts, &zero, sizeof(u32), 0,
+        cudaMemcpyHostToDevice, s));
+    CK(cudaStreamSynchronize(s));
+    throw Failure(E_TIMEOUT, "a bounded device wait gave up (scan look-back)");
+  }
+}
+
+u32* exscan_new(u32 const* in, u32 n, cudaStream_t s)
+{
+  u32* out = dalloc<u32>((size_t)n + 1, s);
+  exscan_u32(in, out, n, s);
+  return out;
+}
+
+__global__ void k_negate_diff(u32 const* __restrict__ offs, u32* __restrict__ o, u32 n)
+{
+  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) o[i] = (offs[i + 1] == offs[i]) ? 1u : 0u;
+}
+
+u32* negate_offsets(u32 const* offs, u32 n, cudaStream_t s)
+{
+  u32* t = dalloc<u32>(n, s);
+  if (n) {
+    k_negate_diff<<<grid_for(n), BLOCK, 0, s>>>(offs, t, n);
+    CK_LAUNCH();
+  }
+  u32* o = exscan_new(t, n, s);
+  dev_free(t, s);
+  return o;
+}
+
+__global__ void k_fill(u32* a, u32 n, u32 v)
+{
+  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) a[i] = v;
+}
+
+void fill_u32(u32* a, u32 n, u32 v, cudaStream_t s)
+{
+  if (!n) return;
+  k_fill<<<grid_for(n), BLOCK, 0, s>>>(a, n, v);
+  CK_LAUNCH();
+}
+
+__global__ void k_iota(u32* a, u32 n, u32 stride)
+{
+  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) a[i] = i * stride;
+}
+
+void iota_u32(u32* a, u32 n, u32 stride, cudaStream_t s)
+{
+  if (!n) return;
+  k_iota<<<grid_for(n), BLOCK, 0, s>>>(a, n, stride);
+  CK_LAUNCH();
+}
+
+__global__ void k_iota64(u64* a, u32 n)
+{
+  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) a[i] = i;
+}
+
+void iota_u64(u64* a, u32 n, cudaStream_t s)
+{
+  if (!n) return;
+  k_iota64<<<grid_for(n), BLOCK, 0, s>>>(a, n);
+  CK_LAUNCH();
+}
+
+template <class T>
+__global__ void k_expand(T const* __restrict__ in, u32 const* __restrict__ offs,
+    u32 n, u32 width, T* __restrict__ out)
+{
+  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  u32 f = offs[i], e = offs[i + 1];
+  for (u32 j = f; j < e; ++j)
+    for (u32 k = 0; k < width; ++k) out[(size_t)j * width + k] = in[(size_t)i * width + k];
+}
+
+void expand_rows(void const* in, u32 const* offs, u32 n, u32 width, u32 esz,
+    void* out, cudaStream_t s)
+{
+  if (!n || !width) return;
+  PROBE(P_EXPAND, s, 4.0 * (n + 1) + 2.0 * (double)n * width * esz);
+  switch (esz) {
+    case 1:
+      k_expand<unsigned char><<<grid_for(n), BLOCK, 0, s>>>(
+          (unsigned char const*)in, offs, n, width, (unsigned char*)out);
+      break;
+    case 4:
+      k_expand<u32><<<grid_for(n), BLOCK, 0, s>>>((u32 const*)in, offs, n, width, (u32*)out);
+      break;
+    default:
+      k_expand<unsigned long long><<<grid_for(n), BLOCK, 0, s>>>(
+          (unsigned long long const*)in, offs, n, width, (unsigned long long*)out);
+      break;
+  }
+  CK_LAUNCH();
+}
+
+__global__ void k_max_u32(u32 const* __restrict__ a, u32 n, u32* out)
+{
+  u32 m = 0;
+  for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    m = max(m, a[i]);
+  for (int o = 16; o; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0 && m) atomicMax(out, m);
+}
+
+u32 max_u32(u32 const* a, u32 n, cudaStream_t s)
+{
+  if (!n) return 0;
+  u32* d = dalloc<u32>(1, s);
+  CK(cudaMemsetAsync(d, 0, sizeof(u32), s));
+  u32 g = grid_for(n);
+  if (g > 4096) g = 4096;
+  k_max_u32<<<g, BLOCK, 0, s>>>(a, n, d);
+  CK_LAUNCH();
+  u32 v = read_u32(d, s);
+  dev_free(d, s);
+  return v;
+}
+
+}  // namespace osh

@@ -1,0 +1,87 @@
+// Host-callable device primitives used by every pass: scans, reductions,
+// fills, compaction by offsets. All work is issued on the caller's stream.
+#pragma once
+
+#include "common.cuh"
+
+namespace osh {
+
+// thread-local error state behind osh_b200_last_error()
+void set_error(int code, char const* msg);
+int last_error();
+char const* last_error_message();
+void clear_error();
+
+// Exclusive scan with the total appended: out has n+1 entries and
+// out[n] = sum(in). Single-pass decoupled look-back (uints_exscan, ints.cpp).
+void exscan_u32(u32 const* in, u32* out, u32 n, cudaStream_t s);
+u32* exscan_new(u32 const* in, u32 n, cudaStream_t s);
+
+// throws E_TIMEOUT if a bounded device-side wait gave up since the last check
+void check_device_timeouts(cudaStream_t s);
+
+// out[i] = !(offs[i+1] - offs[i]) scanned (uints_negate_offsets, ints.cpp:227)
+u32* negate_offsets(u32 const* offs, u32 n, cudaStream_t s);
+
+void fill_u32(u32* a, u32 n, u32 v, cudaStream_t s);
+void iota_u32(u32* a, u32 n, u32 stride, cudaStream_t s);
+void iota_u64(u64* a, u32 n, cudaStream_t s);
+
+// expand_array (arrays.cpp:170-192): rows of `width` elements of size esz
+// copied to every slot [offs[i], offs[i+1]); output rows start at out.
+void expand_rows(void const* in, u32 const* offs, u32 n, u32 width, u32 esz,
+    void* out, cudaStream_t s);
+
+// max over a u32 array (uints_max)
+u32 max_u32(u32 const* a, u32 n, cudaStream_t s);
+
+// Per-kernel event probes. When a probe is enabled, every launch it wraps is
+// bracketed by CUDA events on the launching stream and credited with the
+// launch's algorithmic bytes (each input read once, each output written
+// once); the pairs are resolved after the timed region by probe_read.
+enum ProbeId {
+  P_REFLECT_DOWN = 0,
+  P_UP_COUNT,
+  P_UP_FILL,
+  P_UP_RANK,
+  P_EXSCAN,
+  P_ELEM_QUALITY,
+  P_REFINE_CANDIDATES,
+  P_REFINE_QUALITY,
+  P_INDSET_ROUND,
+  P_COARSEN_QUALITY,
+  P_SWAP_QUALITY,
+  P_REFINE_TOPOLOGY,
+  P_COLLAPSE_TO_ENT,
+  P_EXPAND,
+  P_NPROBES
+};
+char const* probe_name(u32 id);
+void probe_enable(u32 mask);
+void probe_reset();
+void probe_read(u32 id, u32* launches, double* ms, double* bytes);
+
+struct ProbeScope {
+  cudaEvent_t a = nullptr, b = nullptr;
+  u32 id;
+  double bytes;
+  cudaStream_t s;
+  ProbeScope(u32 id, cudaStream_t s, double bytes);
+  ~ProbeScope();
+};
+#define PROBE(id, stream, bytes) ::osh::ProbeScope osh_probe_scope_((id), (stream), (double)(bytes))
+
+// number of kernels this library launched in the process
+unsigned long long launch_count();
+
+// small pinned host mailbox for reading several device scalars at once
+struct Mailbox {
+  u32* host = nullptr;   // pinned
+  u32* dev = nullptr;    // device, 64 slots
+  void init(cudaStream_t s);
+  void release();
+  void clear(cudaStream_t s);                 // zero the device slots
+  void fetch(cudaStream_t s, u32 nslots = 64);  // copy back and synchronise
+};
+
+}  // namespace osh

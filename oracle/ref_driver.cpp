@@ -211,6 +211,53 @@ unsigned refd_adapt(void* p, double sf, double gq, unsigned nl, unsigned mo)
   return mesh_adapt(M(p), sf, gq, nl, mo);
 }
 
+/* The pass sequence of mesh_adapt (adapt.cpp:47-94) calling the reference's
+   own passes, counting the passes that change the mesh and the elements
+   entering them (the throughput metric's numerator). Returns 1 on success,
+   0 when max_ops is exceeded (the reference would abort). */
+unsigned refd_adapt_counted(void* p, double sf, double gq, unsigned nl,
+    unsigned max_ops, unsigned* passes, double* elems_in)
+{
+  struct mesh* m = M(p);
+  unsigned ops = 0;
+  double in = 0;
+  unsigned dim = mesh_dim(m);
+  double qf = mesh_min_quality(m);
+  if (gq < qf) qf = gq;
+  unsigned before = mesh_count(m, dim);
+#define COUNTED(call)                 \
+  (before = mesh_count(m, dim), (call))
+#define INCR()                        \
+  do {                                \
+    in += before;                     \
+    if (ops > max_ops) {              \
+      *passes = ops;                  \
+      *elems_in = in;                 \
+      return 0;                       \
+    }                                 \
+    ++ops;                            \
+  } while (0)
+  while (COUNTED(refine_by_size(m, qf))) INCR();
+  while (COUNTED(coarsen_by_size(m, qf, sf))) INCR();
+  for (;;) {
+    if (mesh_min_quality(m) >= gq) break;
+    if (dim == 3 && COUNTED(swap_slivers(m, gq, nl))) {
+      INCR();
+      continue;
+    }
+    if (COUNTED(coarsen_slivers(m, gq, nl))) {
+      INCR();
+      continue;
+    }
+    break;
+  }
+#undef INCR
+#undef COUNTED
+  *passes = ops;
+  *elems_in = in;
+  return 1;
+}
+
 /* Refine selection on the current mesh, without modifying it: the steps of
    refine_by_size (refine.cpp:17-27) and choose_refinement_indset
    (refine_common.cpp:131-160). Outputs are per edge. Returns 1 when an
