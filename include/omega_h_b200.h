@@ -132,6 +132,34 @@ char const* osh_b200_probe_name(unsigned id) OSH_PUBLIC;
 void osh_b200_probe_read(unsigned id, unsigned* launches, double* total_ms,
     double* total_bytes) OSH_PUBLIC;
 
+/* ---- upward adjacency without device allocation -------------------------- */
+/* No counterpart in the reference. For callers that cannot allocate device
+   memory when they need it: work issued while a stream is captured into a
+   CUDA graph, host callbacks and real-time loops that must not wait on the
+   allocator, and host codes that give the GPU a fixed memory budget.
+   Computes the same upward adjacency as osh_up_offs / osh_up / osh_up_dirs
+   (rows sorted by use index) from a device array lows_of_highs of
+   nhighs * deg(high_dim, low_dim) entries into caller-allocated device arrays
+   offsets[nlows + 1], highs_of_lows[nuses] and directions[nuses], enqueued
+   on `stream` (a cudaStream_t, 0 = legacy default stream) without
+   synchronising. It calls no allocator: its scratch is one fixed device
+   array inside the library (about 8.4 MB, held by every GPU that loads the
+   library until the process exits), so the sizes are capped at
+   OSH_B200_NOALLOC_MAX_USES uses and OSH_B200_NOALLOC_MAX_LOWS rows; larger
+   requests return OSH_B200_E_ARG without launching anything. The first call
+   on each device looks up the array's device address, so make it before any
+   stream capture on that device. Every call shares the one array and each
+   clears what it needs, so calls that may run at the same time on the GPU
+   (different streams, no ordering between them) race and must not be
+   issued. Returns 0, or the error code also recorded for
+   osh_b200_last_error(). */
+#define OSH_B200_NOALLOC_MAX_USES (1u << 20)
+#define OSH_B200_NOALLOC_MAX_LOWS (1u << 20)
+int osh_b200_up_from_down_noalloc(unsigned high_dim, unsigned low_dim,
+    unsigned nhighs, unsigned nlows, unsigned const* lows_of_highs,
+    unsigned* offsets, unsigned* highs_of_lows, unsigned* directions,
+    void* stream) OSH_PUBLIC;
+
 /* ---- memory helpers ----------------------------------------------------- */
 void osh_b200_copy_to_host(void* host_dst, void const* dev_src, size_t bytes) OSH_PUBLIC;
 void osh_b200_copy_to_device(void* dev_dst, void const* host_src, size_t bytes) OSH_PUBLIC;

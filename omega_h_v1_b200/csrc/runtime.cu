@@ -371,6 +371,27 @@ void check_device_timeouts(cudaStream_t s)
   }
 }
 
+size_t exscan_scratch_words(u32 n)
+{
+  return 4 + 2 * (size_t)ceil_div(n ? n : 1, SCAN_TILE);
+}
+
+void exscan_u32_scratch(u32 const* in, u32* out, u32 n, u32* scratch, cudaStream_t s)
+{
+  if (reinterpret_cast<uintptr_t>(scratch) % 16 != 0)
+    throw Failure(E_ARG, "scan scratch must start on a 16-byte boundary");
+  if (n == 0) {
+    k_set_zero_total<<<1, 1, 0, s>>>(out);
+    CK_LAUNCH();
+    return;
+  }
+  u32 ntiles = ceil_div(n, SCAN_TILE);
+  CK(cudaMemsetAsync(scratch, 0, exscan_scratch_words(n) * sizeof(u32), s));
+  k_exscan<<<ntiles, SCAN_THREADS, 0, s>>>(in, out, n, ntiles,
+      reinterpret_cast<unsigned long long*>(scratch + 4), scratch);
+  CK_LAUNCH();
+}
+
 u32* exscan_new(u32 const* in, u32 n, cudaStream_t s)
 {
   u32* out = dalloc<u32>((size_t)n + 1, s);

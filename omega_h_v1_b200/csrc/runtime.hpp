@@ -17,6 +17,11 @@ void clear_error();
 void exscan_u32(u32 const* in, u32* out, u32 n, cudaStream_t s);
 u32* exscan_new(u32 const* in, u32 n, cudaStream_t s);
 
+// The same scan with caller-provided scratch of at least
+// exscan_scratch_words(n) 32-bit words (zeroed here); allocates nothing.
+size_t exscan_scratch_words(u32 n);
+void exscan_u32_scratch(u32 const* in, u32* out, u32 n, u32* scratch, cudaStream_t s);
+
 // throws E_TIMEOUT if a bounded device-side wait gave up since the last check
 void check_device_timeouts(cudaStream_t s);
 
