@@ -127,24 +127,35 @@ def barrier(world):
         dist.barrier()
 
 
-def max_over_ranks(x, world):
+def _reduce(x, world, op):
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=op)
     return float(t.item())
+
+
+def max_over_ranks(x, world):
+    """Step times are the slowest rank's (replicas finish independently)."""
+    import torch.distributed as dist
+    return _reduce(x, world, dist.ReduceOp.MAX) if world > 1 else x
 
 
 def sum_over_ranks(x, world):
-    if world == 1:
-        return x
-    import torch
+    """Work units add up over the replicas."""
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.SUM)
-    return float(t.item())
+    return _reduce(x, world, dist.ReduceOp.SUM) if world > 1 else x
+
+
+def replica_throughput(units_local, ms_local, world):
+    """Whole-job throughput of independent replicas: all ranks' units over
+    the slowest rank's time."""
+    ms = max_over_ranks(ms_local, world)
+    units = sum_over_ranks(units_local, world)
+    return units / (ms / 1e3), ms, units
 
 
 # ---------------------------------------------------------------------------
@@ -281,9 +292,7 @@ def run_ours(args, world, rank, local):
     L.osh_b200_probe_read(probe_id, C.byref(plaunch), C.byref(pms), C.byref(pbytes))
     for i in range(args.warmup, nsteps):
         L.osh_free(copies[i])
-    ms = max_over_ranks(ms_local, world)
-    units = sum_over_ranks(float(sum(elems)), world)
-    value = units / (ms / 1e3)
+    value, ms, units = replica_throughput(float(sum(elems)), ms_local, world)
 
     e2e = None
     if not args.no_e2e:

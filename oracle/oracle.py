@@ -352,6 +352,58 @@ def swap_table(ring_size):
             ied[: nm * ni * 2].reshape(nm, ni, 2))
 
 
+# -- fixtures ----------------------------------------------------------------------
+
+def snapshot_digest(s: MeshSnapshot) -> str:
+    """SHA-256 over a mesh's counts, connectivity, tags (name, type, ncomps,
+    transfer, raw bytes in order) and global numbers."""
+    import hashlib
+    h = hashlib.sha256()
+    h.update(np.asarray(s.counts, np.uint64).tobytes())
+    for d in range(1, s.dim + 1):
+        h.update(np.ascontiguousarray(s.conn[d], np.uint32).tobytes())
+    for d in range(s.dim + 1):
+        for t in s.tags[d]:
+            h.update(t.name.encode())
+            h.update(np.asarray([t.type, t.ncomps, t.transfer], np.uint32).tobytes())
+            h.update(np.ascontiguousarray(t.data).tobytes())
+    for d in sorted(s.globals):
+        h.update(np.ascontiguousarray(s.globals[d], np.uint64).tobytes())
+    return h.hexdigest()
+
+
+def snapshot_to_npz(s: MeshSnapshot, path: str, **extra):
+    arrays = {"counts": np.asarray(s.counts, np.uint32)}
+    names = []
+    for d in range(1, s.dim + 1):
+        arrays["conn%d" % d] = s.conn[d]
+    for d in range(s.dim + 1):
+        for i, t in enumerate(s.tags[d]):
+            key = "tag%d_%d" % (d, i)
+            arrays[key] = t.data
+            names.append("%d|%d|%s|%d|%d|%d" % (d, i, t.name, t.type, t.ncomps, t.transfer))
+    for d, g in s.globals.items():
+        arrays["glob%d" % d] = g
+    arrays["tagmeta"] = np.asarray(names)
+    for k, v in extra.items():
+        arrays["x_" + k] = v
+    np.savez_compressed(path, **arrays)
+
+
+def snapshot_from_npz(path: str):
+    z = np.load(path, allow_pickle=False)
+    counts = [int(c) for c in z["counts"]]
+    dim = len(counts) - 1
+    conn = {d: z["conn%d" % d] for d in range(1, dim + 1)}
+    tags = {d: [] for d in range(dim + 1)}
+    for meta in z["tagmeta"]:
+        d, i, name, ty, nc, tr = str(meta).split("|")
+        tags[int(d)].append(Tag(name, int(ty), int(nc), int(tr), z["tag%s_%s" % (d, i)]))
+    glob = {int(k[4:]): z[k] for k in z.files if k.startswith("glob")}
+    extra = {k[2:]: z[k] for k in z.files if k.startswith("x_")}
+    return MeshSnapshot(dim, counts, conn, tags, glob), extra
+
+
 # -- comparison ------------------------------------------------------------------
 
 def mesh_diff(a: MeshSnapshot, b: MeshSnapshot, rel_tol=1e-12, floor=0.0,
