@@ -125,6 +125,10 @@ void Mesh::clear_contents()
     }
   dev_free(dual, s);
   dual = nullptr;
+  for (u32 d = 0; d < 3; ++d) {
+    dev_free(up_other[d], s);
+    up_other[d] = nullptr;
+  }
   for (u32 d = 0; d < 4; ++d) {
     for (auto& t : tags[d]) dev_free(t.data, s);
     tags[d].clear();
@@ -159,6 +163,10 @@ void Mesh::overwrite(Mesh* with)
     }
   dual = with->dual;
   with->dual = nullptr;
+  for (u32 d = 0; d < 3; ++d) {
+    up_other[d] = with->up_other[d];
+    with->up_other[d] = nullptr;
+  }
   for (u32 d = 0; d < 4; ++d) {
     counts[d] = with->counts[d];
     tags[d].swap(with->tags[d]);
@@ -291,6 +299,92 @@ __global__ void k_rank_rows(u32 const* __restrict__ offs, u32 const* __restrict_
   }
 }
 
+// Each row (the uses of one low entity, filled in arbitrary order) is
+// sorted by a group of G lanes holding K elements each: a bitonic network
+// over N = G*K slots in registers, partners across lanes exchanged by
+// shuffles, the missing slots padded with the largest key. Rows longer than
+// N (rare: N is at least 2.5x the mean degree) are ranked by the group from
+// global memory after the network, outside any shuffle.
+template <int G, int K>
+__global__ void __launch_bounds__(256)
+k_sort_rows(u32 const* __restrict__ offs, u32 const* __restrict__ tmp, u32 nrows, u32 lph,
+    u32* __restrict__ adj, u32* __restrict__ dirs)
+{
+  constexpr int N = G * K;
+  u32 row = (blockIdx.x * blockDim.x + threadIdx.x) / G;
+  u32 l = threadIdx.x % G;
+  u32 f = 0, len = 0;
+  if (row < nrows) {
+    f = offs[row];
+    len = offs[row + 1] - f;
+  }
+  u32 v[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    u32 idx = k * G + l;
+    v[k] = (idx < len && len <= (u32)N) ? tmp[f + idx] : 0xffffffffu;
+  }
+#pragma unroll
+  for (int size = 2; size <= N; size <<= 1) {
+#pragma unroll
+    for (int j = size >> 1; j > 0; j >>= 1) {
+      u32 nv[K];
+#pragma unroll
+      for (int k = 0; k < K; ++k) {
+        u32 i = k * G + l;
+        u32 other = (j < G) ? __shfl_xor_sync(0xffffffffu, v[k], j) : v[k ^ (j / G)];
+        bool up = (i & size) == 0;
+        bool lower = (i & j) == 0;
+        u32 mn = v[k] < other ? v[k] : other;
+        u32 mx = v[k] < other ? other : v[k];
+        nv[k] = (lower == up) ? mn : mx;
+      }
+#pragma unroll
+      for (int k = 0; k < K; ++k) v[k] = nv[k];
+    }
+  }
+  if (len <= (u32)N) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      u32 idx = k * G + l;
+      if (idx < len) {
+        adj[f + idx] = v[k] / lph;
+        dirs[f + idx] = v[k] % lph;
+      }
+    }
+  } else {
+    for (u32 a = l; a < len; a += G) {
+      u32 x = tmp[f + a], rank = 0;
+      for (u32 b = 0; b < len; ++b) rank += (tmp[f + b] < x) ? 1u : 0u;
+      adj[f + rank] = x / lph;
+      dirs[f + rank] = x % lph;
+    }
+  }
+}
+
+template <int G, int K>
+static void launch_sort_rows(u32 const* offs, u32 const* tmp, u32 nrows, u32 lph, u32* adj,
+    u32* dirs, cudaStream_t s)
+{
+  u64 threads = (u64)nrows * G;
+  k_sort_rows<G, K><<<grid_for(threads), 256, 0, s>>>(offs, tmp, nrows, lph, adj, dirs);
+  CK_LAUNCH();
+}
+
+static void rank_rows(u32 const* offs, u32 const* tmp, u32 nrows, u32 nuses, u32 lph,
+    u32* adj, u32* dirs, cudaStream_t s)
+{
+  double avg = nrows ? (double)nuses / nrows : 1.0;
+  double want = 2.5 * avg;
+  if (want <= 2) launch_sort_rows<2, 1>(offs, tmp, nrows, lph, adj, dirs, s);
+  else if (want <= 4) launch_sort_rows<4, 1>(offs, tmp, nrows, lph, adj, dirs, s);
+  else if (want <= 8) launch_sort_rows<8, 1>(offs, tmp, nrows, lph, adj, dirs, s);
+  else if (want <= 16) launch_sort_rows<16, 1>(offs, tmp, nrows, lph, adj, dirs, s);
+  else if (want <= 32) launch_sort_rows<32, 1>(offs, tmp, nrows, lph, adj, dirs, s);
+  else if (want <= 64) launch_sort_rows<32, 2>(offs, tmp, nrows, lph, adj, dirs, s);
+  else launch_sort_rows<32, 4>(offs, tmp, nrows, lph, adj, dirs, s);
+}
+
 void up_from_down(u32 high, u32 low, u32 nhighs, u32 nlows, u32 const* loh,
     UpAdj& out, cudaStream_t s)
 {
@@ -314,12 +408,9 @@ void up_from_down(u32 high, u32 low, u32 nhighs, u32 nlows, u32 const* loh,
       k_fill_uses<<<grid_for(nuses), BLOCK, 0, s>>>(loh, nuses, out.offs, cnt, tmp);
       CK_LAUNCH();
     }
-    u64 threads = (u64)nlows * 32;
-    {
+    if (nlows) {
       PROBE(P_UP_RANK, s, 12.0 * nuses + 4.0 * (nlows + 1.0));
-      k_rank_rows<<<grid_for(threads), BLOCK, 0, s>>>(out.offs, tmp, nlows, lph,
-          out.adj, out.dirs);
-      CK_LAUNCH();
+      rank_rows(out.offs, tmp, nlows, nuses, lph, out.adj, out.dirs, s);
     }
   }
   dev_free(tmp, s);
@@ -395,6 +486,72 @@ __global__ void k_reflect_down(u32 high, u32 low, u32 nh, u32 const* __restrict_
       u32 a = vol[t * 3 + (d + 1) % 3], b = vol[t * 3 + (d + 2) % 3];
       if ((a == w1 && b == w2) || (a == w2 && b == w1)) {
         found = t;
+        break;
+      }
+    }
+  }
+  out[idx] = found;
+}
+
+// Rows for the search: per use of up(0,1) the edge's other vertex, per use of
+// up(0,2) the triangle's other two vertices (cyclic after the vertex).
+__global__ void k_other_verts(u32 low, u32 nuse, u32 const* __restrict__ adj,
+    u32 const* __restrict__ dirs, u32 const* __restrict__ vol, u32* __restrict__ other)
+{
+  u32 j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= nuse) return;
+  u32 e = adj[j], d = dirs[j];
+  if (low == 1) {
+    other[j] = vol[e * 2 + (1 - d)];
+  } else {
+    uint2 o;
+    o.x = vol[e * 3 + (d + 1) % 3];
+    o.y = vol[e * 3 + (d + 2) % 3];
+    reinterpret_cast<uint2*>(other)[j] = o;
+  }
+}
+
+// reflect_down_entity / find_by_verts (reflect_down.cpp:13-38,
+// find_by_verts.hpp:14-55): the low entity with the wanted vertices is
+// unique, so the search may start from whichever of its vertices has the
+// shortest upward row; each candidate costs one contiguous load.
+__global__ void k_reflect_rows(u32 high, u32 low, u32 nh, u32 const* __restrict__ voh,
+    u32 const* __restrict__ lv_offs, u32 const* __restrict__ lv_adj,
+    u32 const* __restrict__ other, u32* __restrict__ out)
+{
+  u32 lph = deg(high, low), vph = deg(high, 0);
+  u32 idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= nh * lph) return;
+  u32 i = idx / lph, j = idx % lph;
+  u32 const* vh = voh + (size_t)i * vph;
+  u32 w[3];
+  w[0] = vh[canon(high, low, 0, j, 0)];
+  w[1] = vh[canon(high, low, 0, j, 1)];
+  w[2] = low == 2 ? vh[canon(high, low, 0, j, 2)] : INV;
+  u32 best = 0, f = lv_offs[w[0]], e = lv_offs[w[0] + 1];
+  for (u32 k = 1; k <= low; ++k) {
+    u32 fk = lv_offs[w[k]], ek = lv_offs[w[k] + 1];
+    if (ek - fk < e - f) {
+      best = k;
+      f = fk;
+      e = ek;
+    }
+  }
+  u32 found = INV;
+  if (low == 1) {
+    u32 want = w[1 - best];
+    for (u32 r = f; r < e; ++r)
+      if (other[r] == want) {
+        found = lv_adj[r];
+        break;
+      }
+  } else {
+    u32 a = w[best == 0 ? 1 : 0], b = w[best == 2 ? 1 : 2];
+    uint2 const* o2 = reinterpret_cast<uint2 const*>(other);
+    for (u32 r = f; r < e; ++r) {
+      uint2 o = o2[r];
+      if ((o.x == a && o.y == b) || (o.x == b && o.y == a)) {
+        found = lv_adj[r];
         break;
       }
     }
@@ -606,13 +763,23 @@ u32 const* Mesh::ask_down(u32 high, u32 low)
     u32 const* vol = ask_down(low, 0);
     u32 n = nh * deg(high, low);
     u32* out = dalloc<u32>(n, s);
+    if (!up_other[low]) {
+      u32 nuse = counts[low] * deg(low, 0);
+      up_other[low] = dalloc<u32>((size_t)nuse * low, s);
+      if (nuse) {
+        k_other_verts<<<grid_for(nuse), BLOCK, 0, s>>>(low, nuse, lv.adj, lv.dirs, vol,
+            up_other[low]);
+        CK_LAUNCH();
+      }
+    }
     if (n) {
-      // voh once, the first vertices' upward CSR once, vol once, out once
+      // voh once, the vertices' upward CSR (offsets, ids, other vertices)
+      // once, out once
       double nl = counts[low], nuse = (double)nl * deg(low, 0);
       PROBE(P_REFLECT_DOWN, s, 4.0 * deg(high, 0) * nh + 4.0 * (counts[0] + 1.0) +
-          8.0 * nuse + 4.0 * deg(low, 0) * nl + 4.0 * n);
-      k_reflect_down<<<grid_for(n), BLOCK, 0, s>>>(high, low, nh, voh, vol, lv.offs,
-          lv.adj, lv.dirs, out);
+          4.0 * nuse + 4.0 * low * nuse + 4.0 * n);
+      k_reflect_rows<<<grid_for(n), BLOCK, 0, s>>>(high, low, nh, voh, lv.offs, lv.adj,
+          up_other[low], out);
       CK_LAUNCH();
     }
     down[high][low] = out;

@@ -57,6 +57,9 @@ struct Mesh {
   Graph star[4][4] = {};
   bool have_star[4][4] = {};
   u32* dual = nullptr;
+  // per use of up(0,1): the edge's other vertex; per use of up(0,2): the
+  // triangle's other two vertices in its cyclic order (reflect_down's rows)
+  u32* up_other[3] = {nullptr, nullptr, nullptr};
   std::vector<Tag> tags[4];
   u64* globals[4] = {};
   u32* own_ranks[4] = {};   // cached zeros (single rank), API only

@@ -239,6 +239,9 @@ constexpr u32 SCAN_SPIN_LIMIT = 1u << 24;
 // set by any bounded device wait that gave up; read by check_device_timeouts
 __device__ u32 d_wait_timeouts;
 
+// mode 0 scans in[i]; mode 1 scans (in[i + 1] == in[i]), i.e. the
+// survivors of an offsets array (uints_negate_offsets, ints.cpp:227-235)
+template <int MODE>
 __global__ void __launch_bounds__(SCAN_THREADS)
 k_exscan(u32 const* __restrict__ in, u32* __restrict__ out, u32 n, u32 ntiles,
     unsigned long long* status, u32* ticket_and_err)
@@ -257,7 +260,9 @@ k_exscan(u32 const* __restrict__ in, u32* __restrict__ out, u32 n, u32 ntiles,
   for (int k = 0; k < SCAN_ITEMS; ++k) {
     u32 li = k * SCAN_THREADS + threadIdx.x;
     size_t gi = base + li;
-    s_buf[li + (li >> 5)] = gi < n ? in[gi] : 0u;
+    u32 v = 0;
+    if (gi < n) v = MODE == 0 ? in[gi] : (in[gi + 1] == in[gi] ? 1u : 0u);
+    s_buf[li + (li >> 5)] = v;
   }
   __syncthreads();
   u32 v[SCAN_ITEMS];
@@ -289,31 +294,43 @@ k_exscan(u32 const* __restrict__ in, u32* __restrict__ out, u32 n, u32 ntiles,
   __syncthreads();
   u32 const thread_excl = (warp ? s_warp[warp - 1] : 0u) + x - sum;
   u32 const total = s_warp[SCAN_WARPS - 1];
-  if (threadIdx.x == 0) {
+  if (warp == 0) {
+    // warp-cooperative look-back: lane l inspects tile (p - l)
     u32 prefix = 0;
     if (tile == 0) {
-      atomicExch(&status[0], FLAG_PRE | (unsigned long long)total);
+      if (lane == 0) atomicExch(&status[0], FLAG_PRE | (unsigned long long)total);
     } else {
-      atomicExch(&status[tile], FLAG_AGG | (unsigned long long)total);
+      if (lane == 0) atomicExch(&status[tile], FLAG_AGG | (unsigned long long)total);
       int p = (int)tile - 1;
       u32 spins = 0;
-      while (p >= 0) {
-        unsigned long long st = *((volatile unsigned long long*)&status[p]);
-        unsigned long long flag = st & (3ull << 62);
-        if (flag == 0) {
+      bool gave_up = false;
+      for (;;) {
+        int idx = p - (int)lane;
+        unsigned long long st = FLAG_PRE;  // before tile 0: an empty prefix
+        if (idx >= 0) st = *((volatile unsigned long long*)&status[idx]);
+        while (__any_sync(0xffffffffu, (st >> 62) == 0)) {
           if (++spins > SCAN_SPIN_LIMIT) {
-            atomicOr(&d_wait_timeouts, 1u);
+            gave_up = true;
             break;
           }
-          continue;
+          if (idx >= 0 && (st >> 62) == 0) st = *((volatile unsigned long long*)&status[idx]);
         }
-        prefix += (u32)st;
-        if (flag == FLAG_PRE) break;
-        --p;
+        if (gave_up) {
+          if (lane == 0) atomicOr(&d_wait_timeouts, 1u);
+          break;
+        }
+        u32 pre = __ballot_sync(0xffffffffu, (st & (3ull << 62)) == FLAG_PRE);
+        u32 stop = pre ? (u32)(__ffs(pre) - 1) : 31u;
+        u32 val = (lane <= stop) ? (u32)st : 0u;
+#pragma unroll
+        for (int o = 16; o; o >>= 1) val += __shfl_xor_sync(0xffffffffu, val, o);
+        prefix += val;
+        if (pre) break;
+        p -= 32;
       }
-      atomicExch(&status[tile], FLAG_PRE | (unsigned long long)(prefix + total));
+      if (lane == 0) atomicExch(&status[tile], FLAG_PRE | (unsigned long long)(prefix + total));
     }
-    s_prefix = prefix;
+    if (lane == 0) s_prefix = prefix;
   }
   __syncthreads();
   u32 run = s_prefix + thread_excl;
@@ -349,7 +366,7 @@ void exscan_u32(u32 const* in, u32* out, u32 n, cudaStream_t s)
   CK(cudaMemsetAsync(scratch, 0, words * sizeof(u32), s));
   {
     PROBE(P_EXSCAN, s, 4.0 * n + 4.0 * (n + 1));
-    k_exscan<<<ntiles, SCAN_THREADS, 0, s>>>(in, out, n, ntiles,
+    k_exscan<0><<<ntiles, SCAN_THREADS, 0, s>>>(in, out, n, ntiles,
         reinterpret_cast<unsigned long long*>(scratch + 4), scratch);
     CK_LAUNCH();
   }
@@ -387,7 +404,7 @@ void exscan_u32_scratch(u32 const* in, u32* out, u32 n, u32* scratch, cudaStream
   }
   u32 ntiles = ceil_div(n, SCAN_TILE);
   CK(cudaMemsetAsync(scratch, 0, exscan_scratch_words(n) * sizeof(u32), s));
-  k_exscan<<<ntiles, SCAN_THREADS, 0, s>>>(in, out, n, ntiles,
+  k_exscan<0><<<ntiles, SCAN_THREADS, 0, s>>>(in, out, n, ntiles,
       reinterpret_cast<unsigned long long*>(scratch + 4), scratch);
   CK_LAUNCH();
 }
@@ -399,21 +416,25 @@ u32* exscan_new(u32 const* in, u32 n, cudaStream_t s)
   return out;
 }
 
-__global__ void k_negate_diff(u32 const* __restrict__ offs, u32* __restrict__ o, u32 n)
-{
-  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) o[i] = (offs[i + 1] == offs[i]) ? 1u : 0u;
-}
-
 u32* negate_offsets(u32 const* offs, u32 n, cudaStream_t s)
 {
-  u32* t = dalloc<u32>(n, s);
-  if (n) {
-    k_negate_diff<<<grid_for(n), BLOCK, 0, s>>>(offs, t, n);
+  u32* o = dalloc<u32>((size_t)n + 1, s);
+  if (n == 0) {
+    k_set_zero_total<<<1, 1, 0, s>>>(o);
+    CK_LAUNCH();
+    return o;
+  }
+  u32 ntiles = ceil_div(n, SCAN_TILE);
+  size_t words = 4 + 2 * (size_t)ntiles;
+  u32* scratch = dalloc<u32>(words, s);
+  CK(cudaMemsetAsync(scratch, 0, words * sizeof(u32), s));
+  {
+    PROBE(P_EXSCAN, s, 4.0 * (n + 1) + 4.0 * (n + 1));
+    k_exscan<1><<<ntiles, SCAN_THREADS, 0, s>>>(offs, o, n, ntiles,
+        reinterpret_cast<unsigned long long*>(scratch + 4), scratch);
     CK_LAUNCH();
   }
-  u32* o = exscan_new(t, n, s);
-  dev_free(t, s);
+  dev_free(scratch, s);
   return o;
 }
 
