@@ -476,7 +476,7 @@ static bool coarsen_select(Mesh& m, u32* codes, double qual_floor, bool require_
     CK_LAUNCH();
   }
   for (u32 ed = 2; ed <= dim; ++ed) {
-    UpAdj const& u = m.ask_up(1, ed);
+    UpAdj const& u = m.ask_up(1, ed, false);
     Tag* cdt = m.find_tag(ed, "class_dim");
     Tag* cds = m.find_tag(ed - 1, "class_dim");
     if (!cdt || !cds) throw Failure(E_ARG, "coarsening needs class_dim on every dimension");
@@ -498,7 +498,7 @@ static bool coarsen_select(Mesh& m, u32* codes, double qual_floor, bool require_
   CK(cudaMemsetAsync(any, 0, sizeof(u32), s));
   if (dim >= 2) {
     double const* eq = require_better ? m.qualities() : nullptr;
-    UpAdj const& ev = m.ask_up(0, dim);
+    UpAdj const& ev = m.ask_up(0, dim, false);
     if (ne) {
       double nel = m.counts[dim];
       PROBE(P_COARSEN_QUALITY, s, 4.0 * (nv + 1) + 8.0 * deg(dim, 0) * nel + 8.0 * ne +

@@ -100,7 +100,7 @@ u32* find_indset(Mesh& m, u32 ent_dim, u32 const* filter, double const* good)
   u32 n = m.count(ent_dim);
   Nbrs g{};
   if (ent_dim == 0) {
-    UpAdj const& u = m.ask_up(0, 1);
+    UpAdj const& u = m.ask_up(0, 1, false);
     g.mode = 0;
     g.offs = u.offs;
     g.adj = u.adj;
@@ -108,7 +108,7 @@ u32* find_indset(Mesh& m, u32 ent_dim, u32 const* filter, double const* good)
     g.down = m.ask_down(1, 0);
     g.per = 2;
   } else if (ent_dim == 1 && m.dim >= 2) {
-    UpAdj const& u = m.ask_up(1, m.dim);
+    UpAdj const& u = m.ask_up(1, m.dim, false);
     g.mode = 1;
     g.offs = u.offs;
     g.adj = u.adj;
@@ -264,7 +264,7 @@ __global__ void k_mark_down(u32 n, u32 const* __restrict__ offs, u32 const* __re
 u32* mark_down(Mesh& m, u32 high, u32 low, u32 const* marked)
 {
   u32 n = m.count(low);
-  UpAdj const& u = m.ask_up(low, high);
+  UpAdj const& u = m.ask_up(low, high, false);
   u32* out = dalloc<u32>(n, m.s);
   if (n) {
     k_mark_down<<<grid_for(n), BLOCK, 0, m.s>>>(n, u.offs, u.adj, marked, out);

@@ -115,6 +115,7 @@ void Mesh::clear_contents()
         dev_free(up[l][h].dirs, s);
         up[l][h] = UpAdj();
         have_up[l][h] = false;
+        up_sorted[l][h] = false;
       }
       if (have_star[l][h]) {
         dev_free(star[l][h].offs, s);
@@ -155,6 +156,7 @@ void Mesh::overwrite(Mesh* with)
       down[h][l] = with->down[h][l];
       up[h][l] = with->up[h][l];
       have_up[h][l] = with->have_up[h][l];
+      up_sorted[h][l] = with->up_sorted[h][l];
       star[h][l] = with->star[h][l];
       have_star[h][l] = with->have_star[h][l];
       with->down[h][l] = nullptr;
@@ -383,6 +385,65 @@ static void rank_rows(u32 const* offs, u32 const* tmp, u32 nrows, u32 nuses, u32
   else if (want <= 32) launch_sort_rows<32, 1>(offs, tmp, nrows, lph, adj, dirs, s);
   else if (want <= 64) launch_sort_rows<32, 2>(offs, tmp, nrows, lph, adj, dirs, s);
   else launch_sort_rows<32, 4>(offs, tmp, nrows, lph, adj, dirs, s);
+}
+
+__global__ void k_fill_uses_split(u32 const* __restrict__ loh, u32 nuses, u32 lph,
+    u32 const* __restrict__ offs, u32* cur, u32* __restrict__ adj, u32* __restrict__ dirs)
+{
+  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nuses) return;
+  u32 l = loh[i];
+  u32 slot = offs[l] + atomicAdd(&cur[l], 1u);
+  adj[slot] = i / lph;
+  dirs[slot] = i % lph;
+}
+
+__global__ void k_join_uses(u32 n, u32 lph, u32 const* __restrict__ adj,
+    u32 const* __restrict__ dirs, u32* __restrict__ uses)
+{
+  u32 j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j < n) uses[j] = adj[j] * lph + dirs[j];
+}
+
+void up_from_down_unsorted(u32 high, u32 low, u32 nhighs, u32 nlows, u32 const* loh,
+    UpAdj& out, cudaStream_t s)
+{
+  u32 lph = deg(high, low);
+  u32 nuses = nhighs * lph;
+  u32* cnt = dalloc<u32>((size_t)nlows + 1, s);
+  CK(cudaMemsetAsync(cnt, 0, sizeof(u32) * ((size_t)nlows + 1), s));
+  if (nuses) {
+    PROBE(P_UP_COUNT, s, 4.0 * nuses + 4.0 * nlows);
+    k_count_lows<<<grid_for(nuses), BLOCK, 0, s>>>(loh, nuses, cnt);
+    CK_LAUNCH();
+  }
+  out.offs = exscan_new(cnt, nlows, s);
+  CK(cudaMemsetAsync(cnt, 0, sizeof(u32) * ((size_t)nlows + 1), s));
+  out.adj = dalloc<u32>(nuses, s);
+  out.dirs = dalloc<u32>(nuses, s);
+  if (nuses) {
+    PROBE(P_UP_FILL, s, 4.0 * nuses + 4.0 * (nlows + 1.0) + 4.0 * nlows + 8.0 * nuses);
+    k_fill_uses_split<<<grid_for(nuses), BLOCK, 0, s>>>(loh, nuses, lph, out.offs, cnt,
+        out.adj, out.dirs);
+    CK_LAUNCH();
+  }
+  dev_free(cnt, s);
+}
+
+void sort_up_rows(u32 high, u32 low, u32 nhighs, u32 nlows, UpAdj const& u,
+    cudaStream_t s)
+{
+  u32 lph = deg(high, low);
+  u32 nuses = nhighs * lph;
+  if (!nuses || !nlows) return;
+  u32* uses = dalloc<u32>(nuses, s);
+  k_join_uses<<<grid_for(nuses), BLOCK, 0, s>>>(nuses, lph, u.adj, u.dirs, uses);
+  CK_LAUNCH();
+  {
+    PROBE(P_UP_RANK, s, 12.0 * nuses + 4.0 * (nlows + 1.0));
+    rank_rows(u.offs, uses, nlows, nuses, lph, u.adj, u.dirs, s);
+  }
+  dev_free(uses, s);
 }
 
 void up_from_down(u32 high, u32 low, u32 nhighs, u32 nlows, u32 const* loh,
@@ -759,7 +820,7 @@ u32 const* Mesh::ask_down(u32 high, u32 low)
   } else if (low > 0) {
     u32 nh = count(high);
     u32 const* voh = ask_down(high, 0);
-    UpAdj const& lv = ask_up(0, low);
+    UpAdj const& lv = ask_up(0, low, false);
     u32 const* vol = ask_down(low, 0);
     u32 n = nh * deg(high, low);
     u32* out = dalloc<u32>(n, s);
@@ -827,9 +888,20 @@ u32 const* Mesh::ask_down(u32 high, u32 low)
   return down[high][low];
 }
 
-UpAdj const& Mesh::ask_up(u32 low, u32 high)
+UpAdj const& Mesh::ask_up(u32 low, u32 high, bool sorted)
 {
-  if (have_up[low][high]) return up[low][high];
+  if (have_up[low][high]) {
+    if (sorted && !up_sorted[low][high]) {
+      sort_up_rows(high, low, counts[high], counts[low], up[low][high], s);
+      up_sorted[low][high] = true;
+      // reflect_down's cached rows follow the old row order
+      if (low == 0 && high < 3) {
+        dev_free(up_other[high], s);
+        up_other[high] = nullptr;
+      }
+    }
+    return up[low][high];
+  }
   if (low == high) {
     u32 n = counts[high];
     UpAdj u;
@@ -840,9 +912,16 @@ UpAdj const& Mesh::ask_up(u32 low, u32 high)
     u.dirs = dalloc<u32>(n, s);
     fill_u32(u.dirs, n, 0, s);
     up[low][high] = u;
+    up_sorted[low][high] = true;
   } else {
     u32 const* loh = ask_down(high, low);
-    up_from_down(high, low, counts[high], counts[low], loh, up[low][high], s);
+    if (sorted) {
+      up_from_down(high, low, counts[high], counts[low], loh, up[low][high], s);
+      up_sorted[low][high] = true;
+    } else {
+      up_from_down_unsorted(high, low, counts[high], counts[low], loh, up[low][high], s);
+      up_sorted[low][high] = false;
+    }
   }
   have_up[low][high] = true;
   return up[low][high];
@@ -950,7 +1029,7 @@ u32 const* Mesh::ask_dual()
   u32* out = dalloc<u32>((size_t)nel * spe, s);
   if (has_dim(dim - 1)) {
     u32 const* soe = ask_down(dim, dim - 1);
-    UpAdj const& es = ask_up(dim - 1, dim);
+    UpAdj const& es = ask_up(dim - 1, dim, false);
     if (nel) {
       k_dual_from_sides<<<grid_for(nel), BLOCK, 0, s>>>(nel, spe, soe, es.offs, es.adj, out);
       CK_LAUNCH();

@@ -54,6 +54,7 @@ struct Mesh {
   u32* down[4][4] = {};
   UpAdj up[4][4] = {};
   bool have_up[4][4] = {};
+  bool up_sorted[4][4] = {};  // rows in use-index order (the reference's)
   Graph star[4][4] = {};
   bool have_star[4][4] = {};
   u32* dual = nullptr;
@@ -94,7 +95,11 @@ struct Mesh {
   u32 count(u32 d);
 
   u32 const* ask_down(u32 high, u32 low);
-  UpAdj const& ask_up(u32 low, u32 high);
+  // Upward adjacency. Rows are always the same sets; `sorted` asks for the
+  // reference's row order (ascending use index), which only some consumers
+  // depend on (edge rings, transfers, vertex_dest, the C API). Rows built
+  // for order-free consumers are sorted in place on the first ordered ask.
+  UpAdj const& ask_up(u32 low, u32 high, bool sorted = true);
   Graph const& ask_star(u32 low, u32 high);
   u32 const* ask_dual();
 
@@ -118,6 +123,12 @@ struct Mesh {
 // derivation helpers (mesh.cu)
 void up_from_down(u32 high, u32 low, u32 nhighs, u32 nlows, u32 const* lows_of_highs,
     UpAdj& out, cudaStream_t s);
+// the same rows in arbitrary order within each row
+void up_from_down_unsorted(u32 high, u32 low, u32 nhighs, u32 nlows,
+    u32 const* lows_of_highs, UpAdj& out, cudaStream_t s);
+// put the rows of an upward adjacency into ascending use order, in place
+void sort_up_rows(u32 high, u32 low, u32 nhighs, u32 nlows, UpAdj const& u,
+    cudaStream_t s);
 
 // up_from_down into caller-provided outputs, with caller-provided scratch of
 // up_from_down_scratch_words(nuses, nlows) 32-bit words; allocates nothing

@@ -299,7 +299,7 @@ static u32* choose_refinement(Mesh& m, u32* cand, double qual_floor, double** qu
   u32* inverted = m.mb->dev + 2;
   CK(cudaMemsetAsync(any, 0, 2 * sizeof(u32), s));
   if (dim >= 2) {
-    UpAdj const& eo = m.ask_up(1, dim);
+    UpAdj const& eo = m.ask_up(1, dim, false);
     if (ne) {
       // refine_quality bytes (edges' up CSR, elements, coordinates, flags)
       double nel = m.counts[dim];
