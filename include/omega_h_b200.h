@@ -116,8 +116,10 @@ void osh_b200_edge_lengths(osh_t m, double* host_out) OSH_PUBLIC;
 /* statistics of the last osh_adapt on this thread: passes that changed the
    mesh and the elements entering them, summed */
 void osh_b200_adapt_stats(unsigned* passes, double* elems_in) OSH_PUBLIC;
-/* kernels launched by this library so far in the process */
+/* kernels launched by this library so far in the process, and the times it
+   waited for the device (stream synchronisations) */
 unsigned long long osh_b200_launch_count(void) OSH_PUBLIC;
+unsigned long long osh_b200_sync_count(void) OSH_PUBLIC;
 /* run all further work of mesh m on the CUDA stream `stream` (a
    cudaStream_t; 0 is the legacy default stream); the caller keeps it alive */
 void osh_b200_set_stream(osh_t m, void* stream) OSH_PUBLIC;

@@ -131,6 +131,7 @@ def lib():
     f("osh_b200_set_stream", None, vp, vp)
     f("osh_b200_adapt_stats", None, C.POINTER(C.c_uint), C.POINTER(C.c_double))
     f("osh_b200_launch_count", C.c_ulonglong)
+    f("osh_b200_sync_count", C.c_ulonglong)
     f("osh_b200_probe_enable", None, C.c_uint)
     f("osh_b200_probe_reset", None)
     f("osh_b200_probe_count", C.c_uint)

@@ -57,7 +57,7 @@ void need(bool ok, char const* what)
 
 void sync(Mesh* m)
 {
-  CK(cudaStreamSynchronize(m->s));
+  osh::stream_sync(m->s);
   osh::check_device_timeouts(m->s);
 }
 
@@ -797,6 +797,7 @@ void osh_b200_adapt_stats(unsigned* passes, double* elems_in)
 }
 
 unsigned long long osh_b200_launch_count(void) { return osh::launch_count(); }
+unsigned long long osh_b200_sync_count(void) { return osh::sync_count(); }
 
 void osh_b200_set_stream(osh_t h, void* stream)
 {

@@ -723,7 +723,7 @@ u32 coarsen_sets(Mesh& m, double qual_floor, double size_floor, u32* codes_size,
       CK(cudaMemcpyAsync(gen_vert, sel.gen_vert, sizeof(u32) * nv, cudaMemcpyDeviceToDevice, s));
     }
   }
-  CK(cudaStreamSynchronize(s));
+  stream_sync(s);
   sel.free(s);
   dev_free(codes, s);
   return ok ? 1 : 0;

@@ -31,9 +31,9 @@ static HostUp host_up(Mesh& m, u32 low, u32 high)
   HostUp h;
   u32 n = m.count(low);
   h.offs = to_host(u.offs, (size_t)n + 1, m.s);
-  CK(cudaStreamSynchronize(m.s));
+  stream_sync(m.s);
   h.adj = to_host(u.adj, h.offs[n], m.s);
-  CK(cudaStreamSynchronize(m.s));
+  stream_sync(m.s);
   return h;
 }
 
@@ -42,7 +42,7 @@ static u32* upload(std::vector<u32> const& h, cudaStream_t s)
   u32* d = dalloc<u32>(h.size(), s);
   if (!h.empty())
     CK(cudaMemcpyAsync(d, h.data(), h.size() * sizeof(u32), cudaMemcpyHostToDevice, s));
-  CK(cudaStreamSynchronize(s));
+  stream_sync(s);
   return d;
 }
 
@@ -64,7 +64,7 @@ void Mesh::derive_model(double crease)
   std::vector<double> x = to_host(coords(), (size_t)count(0) * 3, s);
   u32 vps = deg(D - 1, 0);
   std::vector<u32> vos = to_host(ask_down(D - 1, 0), (size_t)ns * vps, s);
-  CK(cudaStreamSynchronize(s));
+  stream_sync(s);
   // boundary side normals (derive_model.cpp:17-76)
   std::vector<double> nrm((size_t)ns * 3, 0.0);
   for (u32 i = 0; i < ns; ++i) {
@@ -123,7 +123,7 @@ void Mesh::derive_model(double crease)
   for (u32 d = 0; d <= D; ++d) {
     cd[d] = to_host(static_cast<u32 const*>(find_tag(d, "class_dim")->data), count(d), s);
   }
-  CK(cudaStreamSynchronize(s));
+  stream_sync(s);
   {
     u32 nv = count(0), k = 0;
     cid[0].assign(nv, INV);
@@ -135,7 +135,7 @@ void Mesh::derive_model(double crease)
     // classified on d, numbered by their smallest member
     u32 n = count(d), spd = deg(d, d - 1);
     std::vector<u32> sod = to_host(ask_down(d, d - 1), (size_t)n * spd, s);
-    CK(cudaStreamSynchronize(s));
+    stream_sync(s);
     HostUp dos = host_up(*this, d - 1, d);
     std::vector<u32>& id = cid[d];
     id.assign(n, INV);

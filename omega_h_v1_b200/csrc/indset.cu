@@ -127,11 +127,17 @@ u32* find_indset(Mesh& m, u32 ent_dim, u32 const* filter, double const* good)
     k_indset_init<<<grid_for(n), BLOCK, 0, m.s>>>(n, filter, a);
     CK_LAUNCH();
   }
+  // Rounds are issued in batches and the "anything left" flag is read once
+  // per batch: a round applied to a settled state leaves it unchanged, so
+  // the extra rounds of a batch cannot alter the result, and the total stays
+  // capped at 100 rounds as in the reference.
   u32 rounds = 0;
   bool done = (n == 0);
-  for (u32 it = 0; it < MAX_INDSET_ROUNDS && !done; ++it) {
-    CK(cudaMemsetAsync(flag, 0, sizeof(u32), m.s));
-    {
+  while (!done && rounds < MAX_INDSET_ROUNDS) {
+    u32 batch = rounds == 0 ? 3u : 1u;
+    if (rounds + batch > MAX_INDSET_ROUNDS) batch = MAX_INDSET_ROUNDS - rounds;
+    for (u32 r = 0; r < batch; ++r) {
+      if (r + 1 == batch) CK(cudaMemsetAsync(flag, 0, sizeof(u32), m.s));
       // offsets, upward lists, the via-entities' down lists, states,
       // goodness and (parallel) globals read once; states written once
       double nuse = (double)read_cached_uses(m, ent_dim);
@@ -139,9 +145,9 @@ u32* find_indset(Mesh& m, u32 ent_dim, u32 const* filter, double const* good)
           4.0 * n + 8.0 * n + (glob ? 8.0 * n : 0.0) + 4.0 * n);
       k_indset_round<<<grid_for(n), BLOCK, 0, m.s>>>(n, g, a, b, good, glob, flag);
       CK_LAUNCH();
+      std::swap(a, b);
+      ++rounds;
     }
-    std::swap(a, b);
-    ++rounds;
     if (!read_u32(flag, m.s)) done = true;
   }
   dev_free(b, m.s);

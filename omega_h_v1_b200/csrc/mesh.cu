@@ -62,7 +62,7 @@ Mesh* Mesh::spawn() const
 Mesh* Mesh::clone()
 {
   Mesh* c = new Mesh(dim, full, parallel, nullptr);
-  CK(cudaStreamSynchronize(s));
+  stream_sync(s);
   try {
     for (u32 d = 0; d <= dim; ++d) {
       if (!has_dim(d)) continue;
@@ -87,7 +87,7 @@ Mesh* Mesh::clone()
       }
     }
     c->ghost_layers = ghost_layers;
-    CK(cudaStreamSynchronize(c->s));
+    stream_sync(c->s);
   } catch (...) {
     delete c;
     throw;
@@ -97,7 +97,7 @@ Mesh* Mesh::clone()
 
 void Mesh::use_stream(cudaStream_t stream)
 {
-  CK(cudaStreamSynchronize(s));
+  stream_sync(s);
   if (own_stream) CK(cudaStreamDestroy(s));
   own_stream = false;
   s = stream;
@@ -1114,7 +1114,7 @@ double Mesh::min_quality()
   u32 ne = count(dim);
   unsigned long long k;
   CK(cudaMemcpyAsync(&k, q + ne, sizeof(k), cudaMemcpyDeviceToHost, s));
-  CK(cudaStreamSynchronize(s));
+  stream_sync(s);
   if (k == ~0ull) return DBL_MAX;
   return from_order_key(k);
 }

@@ -364,8 +364,9 @@ u32 refine_by_size(Mesh& m, double qual_floor)
         static_cast<double const*>(h->data), cand, any);
     CK_LAUNCH();
   }
-  u32 r = 0;
-  if (read_u32(any, s)) r = refine_common(m, cand, qual_floor);
+  // no separate check for "any candidate": with none, the quality kernel
+  // keeps none and refine_common returns 0 after its single read-back
+  u32 r = refine_common(m, cand, qual_floor);
   dev_free(cand, s);
   return r;
 }
@@ -400,12 +401,12 @@ u32 refine_sets(Mesh& m, double qual_floor, u32* cand_out, u32* good_out,
   CK(cudaMemcpyAsync(quals_out, q, sizeof(double) * ne, cudaMemcpyDeviceToDevice, s));
   dev_free(q, s);
   if (!ind) {
-    CK(cudaStreamSynchronize(s));
+    stream_sync(s);
     return 0;
   }
   CK(cudaMemcpyAsync(indset_out, ind, sizeof(u32) * ne, cudaMemcpyDeviceToDevice, s));
   dev_free(ind, s);
-  CK(cudaStreamSynchronize(s));
+  stream_sync(s);
   return 1;
 }
 

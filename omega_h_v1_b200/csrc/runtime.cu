@@ -49,6 +49,16 @@ std::atomic<unsigned long long> g_launches{0};
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 unsigned long long launch_count() { return g_launches.load(); }
 
+namespace {
+std::atomic<unsigned long long> g_syncs{0};
+}
+unsigned long long sync_count() { return g_syncs.load(); }
+void stream_sync(cudaStream_t s)
+{
+  g_syncs.fetch_add(1, std::memory_order_relaxed);
+  CK(cudaStreamSynchronize(s));
+}
+
 // ---------------------------------------------------------------------------
 // probes
 
@@ -180,7 +190,7 @@ u32 read_u32(u32 const* d, cudaStream_t s)
 {
   u32 v = 0;
   CK(cudaMemcpyAsync(&v, d, sizeof(u32), cudaMemcpyDeviceToHost, s));
-  CK(cudaStreamSynchronize(s));
+  stream_sync(s);
   return v;
 }
 
@@ -188,7 +198,7 @@ double read_f64(double const* d, cudaStream_t s)
 {
   double v = 0;
   CK(cudaMemcpyAsync(&v, d, sizeof(double), cudaMemcpyDeviceToHost, s));
-  CK(cudaStreamSynchronize(s));
+  stream_sync(s);
   return v;
 }
 
@@ -216,7 +226,7 @@ void Mailbox::clear(cudaStream_t s)
 void Mailbox::fetch(cudaStream_t s, u32 nslots)
 {
   CK(cudaMemcpyAsync(host, dev, nslots * sizeof(u32), cudaMemcpyDeviceToHost, s));
-  CK(cudaStreamSynchronize(s));
+  stream_sync(s);
 }
 
 // ---------------------------------------------------------------------------
@@ -378,12 +388,12 @@ void check_device_timeouts(cudaStream_t s)
   u32 v = 0;
   CK(cudaMemcpyFromSymbolAsync(&v, d_wait_timeouts, sizeof(u32), 0,
       cudaMemcpyDeviceToHost, s));
-  CK(cudaStreamSynchronize(s));
+  stream_sync(s);
   if (v) {
     u32 zero = 0;
     CK(cudaMemcpyToSymbolAsync(d_wait_timeouts, &zero, sizeof(u32), 0,
         cudaMemcpyHostToDevice, s));
-    CK(cudaStreamSynchronize(s));
+    stream_sync(s);
     throw Failure(E_TIMEOUT, "a bounded device wait gave up (scan look-back)");
   }
 }

@@ -76,8 +76,11 @@ struct ProbeScope {
 };
 #define PROBE(id, stream, bytes) ::osh::ProbeScope osh_probe_scope_((id), (stream), (double)(bytes))
 
-// number of kernels this library launched in the process
+// number of kernels this library launched in the process, and the number of
+// times it waited for the device
 unsigned long long launch_count();
+unsigned long long sync_count();
+void stream_sync(cudaStream_t s);
 
 // small pinned host mailbox for reading several device scalars at once
 struct Mailbox {

@@ -559,7 +559,7 @@ u32 swap_sets(Mesh& m, double gq, u32 nlayers, u32* slivers, u32* cand, u32* int
     CK(cudaMemcpyAsync(ring_sizes, sel.rs, sizeof(u32) * ne, cudaMemcpyDeviceToDevice, s));
   }
   if (ok) CK(cudaMemcpyAsync(indset, sel.ind, sizeof(u32) * ne, cudaMemcpyDeviceToDevice, s));
-  CK(cudaStreamSynchronize(s));
+  stream_sync(s);
   sel.free(s);
   return ok ? 1 : 0;
 }
