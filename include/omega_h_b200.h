@@ -58,6 +58,27 @@ double osh_b200_min_quality(osh_t m) OSH_PUBLIC;
 void osh_b200_last_pass(unsigned* op, unsigned* elems_in, unsigned* elems_out,
     unsigned* nselected, unsigned* rounds) OSH_PUBLIC;
 
+/* ---- many meshes adapted together --------------------------------------- */
+/* No single counterpart in the reference: mesh_adapt (adapt.cpp:82-94) of
+   every mesh in `meshes`, with the meshes concatenated into disjoint unions
+   of at most max_union_elems input elements (0 = one union) so that each
+   stage of a pass is one launch for all of them. Each mesh ends exactly as
+   osh_adapt would leave it; meshes that changed are replaced in place.
+   changed[i] (optional) receives what osh_adapt would return for mesh i and
+   status[i] (optional) 0 or OSH_B200_E_MAXOPS. All meshes must have the same
+   dimension, representation and tags. Returns 0 or an error code. */
+int osh_b200_adapt_batch(osh_t* meshes, unsigned nmeshes, double size_ratio_floor,
+    double good_qual, unsigned nsliver_layers, unsigned max_passes,
+    unsigned long long max_union_elems, unsigned* changed, int* status) OSH_PUBLIC;
+/* statistics of the last osh_b200_adapt_batch on this thread: unions,
+   scheduling steps, passes over whole unions, passes that changed a mesh
+   (summed over meshes) and the elements entering those passes */
+void osh_b200_batch_stats(unsigned* unions, unsigned* steps, unsigned* union_passes,
+    unsigned* mesh_passes, double* elems_in) OSH_PUBLIC;
+/* per-mesh statistics of the last osh_b200_adapt_batch on this thread, for
+   mesh i of that call: passes that changed it and the elements entering them */
+void osh_b200_batch_mesh_stats(unsigned i, unsigned* passes, double* elems_in) OSH_PUBLIC;
+
 /* ---- per-stage selections of one pass, without changing the mesh ------ */
 /* Layouts follow refine_by_size / coarsen_common / swap_common: every output
    is a host array sized by the entity counts of the current mesh. */

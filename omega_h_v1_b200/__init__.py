@@ -130,6 +130,10 @@ def lib():
     f("osh_b200_clone", vp, vp)
     f("osh_b200_set_stream", None, vp, vp)
     f("osh_b200_adapt_stats", None, C.POINTER(C.c_uint), C.POINTER(C.c_double))
+    f("osh_b200_adapt_batch", C.c_int, C.POINTER(vp), C.c_uint, C.c_double, C.c_double,
+      C.c_uint, C.c_uint, C.c_ulonglong, C.POINTER(C.c_uint), C.POINTER(C.c_int))
+    f("osh_b200_batch_stats", None, *([C.POINTER(C.c_uint)] * 4), C.POINTER(C.c_double))
+    f("osh_b200_batch_mesh_stats", None, C.c_uint, C.POINTER(C.c_uint), C.POINTER(C.c_double))
     f("osh_b200_launch_count", C.c_ulonglong)
     f("osh_b200_sync_count", C.c_ulonglong)
     f("osh_b200_probe_enable", None, C.c_uint)
@@ -214,6 +218,12 @@ class Mesh:
                                        conn.size // DEG[dim][0], conn)
         check()
         return cls(h)
+
+    def clone(self):
+        """A deep copy on the same GPU (connectivity, tags, global numbers)."""
+        h = self.L.osh_b200_clone(self.h)
+        self._chk()
+        return Mesh(h)
 
     def close(self):
         if self.h:
@@ -402,6 +412,33 @@ class Mesh:
     def synchronize(self):
         self.L.osh_b200_synchronize(self.h)
         self._chk()
+
+
+def adapt_batch(meshes, size_floor, good_qual, nlayers, max_ops, max_union_elems=0):
+    """mesh_adapt of every mesh, adapted together in disjoint unions of at most
+    ``max_union_elems`` input elements (0 = one union). Returns (changed, status)
+    per mesh and the batch statistics."""
+    L = lib()
+    n = len(meshes)
+    hs = (C.c_void_p * max(n, 1))(*[m.h for m in meshes])
+    changed = (C.c_uint * max(n, 1))()
+    status = (C.c_int * max(n, 1))()
+    rc = L.osh_b200_adapt_batch(hs, n, size_floor, good_qual, nlayers, max_ops,
+                                max_union_elems, changed, status)
+    if rc:
+        check()
+        raise OshError(rc, "osh_b200_adapt_batch failed")
+    u, st, up, mp = (C.c_uint() for _ in range(4))
+    e = C.c_double()
+    L.osh_b200_batch_stats(C.byref(u), C.byref(st), C.byref(up), C.byref(mp), C.byref(e))
+    per = []
+    for i in range(n):
+        p, ei = C.c_uint(), C.c_double()
+        L.osh_b200_batch_mesh_stats(i, C.byref(p), C.byref(ei))
+        per.append((p.value, ei.value))
+    stats = dict(unions=u.value, steps=st.value, union_passes=up.value,
+                 mesh_passes=mp.value, elems_in=e.value, per_mesh=per)
+    return list(changed[:n]), list(status[:n]), stats
 
 
 def new_box_mesh(n, seed=0, pert=0.1, size=None, radial=None, parallel=False):

@@ -1,0 +1,873 @@
+// Batched adaptation of many meshes as one disjoint union (see batch.hpp).
+//
+// Concatenation: per dimension, the meshes' connectivity is laid end to end
+// with each mesh's vertex ids shifted by the vertices before it, tags are
+// laid end to end, and every vertex records its segment (mesh index). One
+// launch per array does the copy for all meshes.
+//
+// Splitting: per dimension, a stable counting sort by segment (one warp per
+// tile of entities builds a segment-major histogram of tiles, an exclusive
+// scan turns it into positions, and the same warps scatter), then one launch
+// per array writes every mesh's part straight into that mesh's own arrays,
+// with vertex ids renumbered to the mesh's local numbering.
+#include <algorithm>
+#include <cfloat>
+
+#include "batch.hpp"
+
+namespace osh {
+
+BatchStats& last_batch_stats()
+{
+  static thread_local BatchStats s;
+  return s;
+}
+
+namespace {
+
+constexpr u32 FULL_MASK = 0xffffffffu;
+constexpr u32 SPLIT_TILE = 2048;   // entities per warp in the counting sort
+constexpr u32 CAP_GRID = 148 * 16; // grid-stride kernels: 16 blocks per SM
+
+u32 capped_grid(u64 n) { return n ? (u32)std::min<u64>(ceil_div(n, BLOCK), CAP_GRID) : 1; }
+
+// index of the segment holding unit `unit`: offs[lo] <= unit < offs[lo + 1]
+__device__ inline u32 find_seg(u32 nm, u32 const* __restrict__ offs, u32 unit)
+{
+  u32 lo = 0, hi = nm;
+  while (hi - lo > 1) {
+    u32 mid = (lo + hi) >> 1;
+    if (offs[mid] <= unit)
+      lo = mid;
+    else
+      hi = mid;
+  }
+  return lo;
+}
+
+// out[j] = src[m][j - offs[m]*width] (+ add[m]) for the segment m of unit j/width
+template <class T>
+__global__ void k_concat(u32 nm, T const* const* __restrict__ src, u32 const* __restrict__ offs,
+    u32 width, T const* __restrict__ add, T* __restrict__ out)
+{
+  u64 total = (u64)offs[nm] * width;
+  for (u64 j = blockIdx.x * (u64)blockDim.x + threadIdx.x; j < total;
+       j += (u64)gridDim.x * blockDim.x) {
+    u32 m = find_seg(nm, offs, (u32)(j / width));
+    T v = src[m][j - (u64)offs[m] * width];
+    if (add) v += add[m];
+    out[j] = v;
+  }
+}
+
+__global__ void k_seg_fill(u32 nm, u32 const* __restrict__ offs, u32* __restrict__ out)
+{
+  u32 total = offs[nm];
+  for (u32 j = blockIdx.x * blockDim.x + threadIdx.x; j < total; j += gridDim.x * blockDim.x)
+    out[j] = find_seg(nm, offs, j);
+}
+
+// segment of every entity: that of its first vertex
+__global__ void k_ent_seg(u32 n, u32 const* __restrict__ voe, u32 vpe,
+    u32 const* __restrict__ seg, u32* __restrict__ out)
+{
+  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = seg[voe[(size_t)i * vpe]];
+}
+
+// per tile of SPLIT_TILE entities (one warp), the count of each segment,
+// stored segment-major: hist[seg * ntiles + tile]
+__global__ void k_tile_hist(u32 n, u32 const* __restrict__ es, u32 ntiles, u32* __restrict__ hist)
+{
+  u32 tile = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (tile >= ntiles) return;
+  u32 base = tile * SPLIT_TILE;
+  for (u32 c = 0; c < SPLIT_TILE; c += 32) {
+    u32 i = base + c + lane;
+    bool on = i < n;
+    u32 mask = __ballot_sync(FULL_MASK, on);
+    if (!mask) break;
+    if (on) {
+      u32 sg = es[i];
+      u32 peers = __match_any_sync(mask, sg);
+      if (lane == (u32)(__ffs(peers) - 1)) hist[(size_t)sg * ntiles + tile] += __popc(peers);
+    }
+    __syncwarp();
+  }
+}
+
+// stable positions: run[seg * ntiles + tile] starts at the scanned histogram
+// and advances as the warp walks its tile in order
+__global__ void k_tile_scatter(u32 n, u32 const* __restrict__ es, u32 ntiles, u32* __restrict__ run,
+    u32* __restrict__ perm)
+{
+  u32 tile = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (tile >= ntiles) return;
+  u32 base = tile * SPLIT_TILE;
+  u32 lt = (1u << lane) - 1u;
+  for (u32 c = 0; c < SPLIT_TILE; c += 32) {
+    u32 i = base + c + lane;
+    bool on = i < n;
+    u32 mask = __ballot_sync(FULL_MASK, on);
+    if (!mask) break;
+    if (on) {
+      u32 sg = es[i];
+      u32 peers = __match_any_sync(mask, sg);
+      u32 leader = (u32)(__ffs(peers) - 1);
+      size_t slot = (size_t)sg * ntiles + tile;
+      u32 b = 0;
+      if (lane == leader) b = run[slot];
+      b = __shfl_sync(peers, b, leader);
+      perm[i] = b + __popc(peers & lt);
+      if (lane == leader) run[slot] = b + __popc(peers);
+    }
+    __syncwarp();
+  }
+}
+
+// first position of every segment (and the total at [nseg])
+__global__ void k_seg_bases(u32 nseg, u32 ntiles, u32 const* __restrict__ scan,
+    u32* __restrict__ out)
+{
+  u32 s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s <= nseg) out[s] = scan[(size_t)s * ntiles];
+}
+
+__global__ void k_local_ids(u32 n, u32 const* __restrict__ es, u32 const* __restrict__ perm,
+    u32 const* __restrict__ bases, u32* __restrict__ out)
+{
+  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = perm[i] - bases[es[i]];
+}
+
+// dst[seg][local * width + k] = in[i * width + k], vertex ids mapped through
+// vloc when given
+template <class T>
+__global__ void k_scatter_meshes(u32 n, u32 width, T const* __restrict__ in,
+    u32 const* __restrict__ es, u32 const* __restrict__ local, u32 const* __restrict__ vloc,
+    T* const* __restrict__ dst)
+{
+  u64 total = (u64)n * width;
+  for (u64 j = blockIdx.x * (u64)blockDim.x + threadIdx.x; j < total;
+       j += (u64)gridDim.x * blockDim.x) {
+    u32 i = (u32)(j / width), k = (u32)(j - (u64)i * width);
+    T v = in[j];
+    if (vloc) v = (T)vloc[(u32)v];
+    dst[es[i]][(u64)local[i] * width + k] = v;
+  }
+}
+
+// global numbers of a single-rank mesh after a pass: the local index
+__global__ void k_scatter_iota64(u32 n, u32 const* __restrict__ es,
+    u32 const* __restrict__ local, u64* const* __restrict__ dst)
+{
+  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) dst[es[i]][local[i]] = local[i];
+}
+
+// per-segment minimum of element qualities (order-preserving keys)
+__global__ void k_seg_min_quality(u32 n, double const* __restrict__ q,
+    u32 const* __restrict__ voe, u32 vpe, u32 const* __restrict__ seg,
+    unsigned long long* __restrict__ out)
+{
+  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+  bool on = i < n;
+  u32 mask = __ballot_sync(FULL_MASK, on);
+  if (!on) return;
+  u32 sg = seg[voe[(size_t)i * vpe]];
+  unsigned long long key = order_key(q[i]);
+  u32 peers = __match_any_sync(mask, sg);
+  if (peers == FULL_MASK) {
+    for (int o = 16; o; o >>= 1) {
+      unsigned long long other = __shfl_xor_sync(FULL_MASK, key, o);
+      key = other < key ? other : key;
+    }
+    if ((threadIdx.x & 31) == 0) atomicMin(&out[sg], key);
+  } else {
+    atomicMin(&out[sg], key);
+  }
+}
+
+// per-segment count of elements
+__global__ void k_seg_count(u32 n, u32 const* __restrict__ voe, u32 vpe,
+    u32 const* __restrict__ seg, u32* __restrict__ out)
+{
+  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+  bool on = i < n;
+  u32 mask = __ballot_sync(FULL_MASK, on);
+  if (!on) return;
+  u32 sg = seg[voe[(size_t)i * vpe]];
+  u32 peers = __match_any_sync(mask, sg);
+  if ((threadIdx.x & 31) == (u32)(__ffs(peers) - 1)) atomicAdd(&out[sg], (u32)__popc(peers));
+}
+
+// small device arrays of pointers / offsets built on the host, uploaded at once
+struct Meta {
+  std::vector<u64> words;
+  size_t add(void const* const* p, u32 n)
+  {
+    size_t at = words.size();
+    for (u32 i = 0; i < n; ++i) words.push_back((u64)(uintptr_t)p[i]);
+    return at;
+  }
+  size_t add_u32(u32 const* p, u32 n)
+  {
+    size_t at = words.size();
+    words.resize(at + (n + 1) / 2, 0);
+    std::memcpy(words.data() + at, p, sizeof(u32) * n);
+    return at;
+  }
+  size_t add_u64(u64 const* p, u32 n)
+  {
+    size_t at = words.size();
+    words.insert(words.end(), p, p + n);
+    return at;
+  }
+  u64* dev = nullptr;
+  void upload(cudaStream_t s)
+  {
+    dev = dalloc<u64>(words.size() ? words.size() : 1, s);
+    if (!words.empty())
+      CK(cudaMemcpyAsync(dev, words.data(), sizeof(u64) * words.size(), cudaMemcpyHostToDevice, s));
+  }
+  template <class T>
+  T* at(size_t w) const
+  {
+    return reinterpret_cast<T*>(dev + w);
+  }
+};
+
+template <class T>
+void launch_concat(u32 nm, Meta const& meta, size_t src_at, size_t offs_at, u32 width,
+    T const* add, u64 total, void* out, cudaStream_t s)
+{
+  if (!total) return;
+  k_concat<T><<<capped_grid(total), BLOCK, 0, s>>>(nm, meta.at<T const* const>(src_at),
+      meta.at<u32 const>(offs_at), width, add, static_cast<T*>(out));
+  CK_LAUNCH();
+}
+
+template <class T>
+void launch_scatter(u32 n, u32 width, void const* in, u32 const* es, u32 const* local,
+    u32 const* vloc, Meta const& meta, size_t dst_at, cudaStream_t s)
+{
+  u64 total = (u64)n * width;
+  if (!total) return;
+  k_scatter_meshes<T><<<capped_grid(total), BLOCK, 0, s>>>(n, width, static_cast<T const*>(in),
+      es, local, vloc, meta.at<T* const>(dst_at));
+  CK_LAUNCH();
+}
+
+bool same_tags(Mesh& a, Mesh& b, u32 d)
+{
+  if (a.tags[d].size() != b.tags[d].size()) return false;
+  for (size_t i = 0; i < a.tags[d].size(); ++i) {
+    Tag const& x = a.tags[d][i];
+    Tag const& y = b.tags[d][i];
+    if (x.name != y.name || x.type != y.type || x.ncomps != y.ncomps ||
+        x.transfer != y.transfer)
+      return false;
+  }
+  return true;
+}
+
+}  // namespace
+
+Mesh* concat_meshes(std::vector<Mesh*> const& ms)
+{
+  if (ms.empty()) throw Failure(E_ARG, "a batch needs at least one mesh");
+  Mesh& a = *ms[0];
+  u32 nm = (u32)ms.size(), dim = a.dim;
+  for (Mesh* m : ms) {
+    if (m->dim != dim || m->full != a.full || m->parallel != a.parallel)
+      throw Failure(E_ARG, "batched meshes differ in dimension, representation or parallelism");
+    if (!m->full) throw Failure(E_ARG, "batched meshes need the full representation");
+    for (Tag const& t : m->tags[0])
+      if (t.type != T_F64 && t.name != "class_dim" && t.name != "class_id")
+        throw Failure(E_ARG, "batched meshes may carry only f64 fields and class labels on "
+                             "vertices (refinement drops other vertex tags)");
+    for (u32 d = 0; d <= dim; ++d) {
+      if (m->has_dim(d) != a.has_dim(d) || !same_tags(*m, a, d))
+        throw Failure(E_ARG, "batched meshes differ in their entities or tags");
+      if (a.parallel && (m->globals[d] == nullptr) != (a.globals[d] == nullptr))
+        throw Failure(E_ARG, "batched meshes differ in their global numbers");
+    }
+    stream_sync(m->s);
+  }
+  Mesh* u = new Mesh(dim, a.full, a.parallel, nullptr);
+  cudaStream_t s = u->s;
+  try {
+    Meta meta;
+    std::vector<u32> offs[4];
+    size_t offs_at[4] = {0, 0, 0, 0}, goff_at[4] = {0, 0, 0, 0};
+    for (u32 d = 0; d <= dim; ++d) {
+      if (!a.has_dim(d)) continue;
+      offs[d].assign(nm + 1, 0);
+      u64 total = 0;
+      for (u32 k = 0; k < nm; ++k) {
+        total += ms[k]->counts[d];
+        if (total * deg(d, 0) >= (1ull << 32))
+          throw Failure(E_ARG, "a union of these meshes exceeds 32-bit entity ids");
+        offs[d][k + 1] = (u32)total;
+      }
+      offs_at[d] = meta.add_u32(offs[d].data(), nm + 1);
+      std::vector<u64> g(offs[d].begin(), offs[d].end() - 1);
+      goff_at[d] = meta.add_u64(g.data(), nm);
+    }
+    // source pointers: connectivity, then each tag, then globals
+    std::vector<void const*> p(nm);
+    size_t conn_at[4] = {0, 0, 0, 0}, glob_at[4] = {0, 0, 0, 0};
+    std::vector<size_t> tag_at[4];
+    for (u32 d = 0; d <= dim; ++d) {
+      if (!a.has_dim(d)) continue;
+      if (d) {
+        for (u32 k = 0; k < nm; ++k) p[k] = ms[k]->down[d][0];
+        conn_at[d] = meta.add(p.data(), nm);
+      }
+      for (size_t t = 0; t < a.tags[d].size(); ++t) {
+        for (u32 k = 0; k < nm; ++k) p[k] = ms[k]->tags[d][t].data;
+        tag_at[d].push_back(meta.add(p.data(), nm));
+      }
+      if (a.parallel && a.globals[d]) {
+        for (u32 k = 0; k < nm; ++k) p[k] = ms[k]->globals[d];
+        glob_at[d] = meta.add(p.data(), nm);
+      }
+    }
+    meta.upload(s);
+    for (u32 d = 0; d <= dim; ++d) {
+      if (!a.has_dim(d)) continue;
+      u32 n = offs[d][nm];
+      u32* conn = nullptr;
+      if (d) {
+        u32 vpe = deg(d, 0);
+        conn = dalloc<u32>((size_t)n * vpe, s);
+        launch_concat<u32>(nm, meta, conn_at[d], offs_at[d], vpe,
+            meta.at<u32 const>(offs_at[0]), (u64)n * vpe, conn, s);
+      }
+      u->set_ents(d, n, conn);
+      for (size_t t = 0; t < a.tags[d].size(); ++t) {
+        Tag const& tg = a.tags[d][t];
+        u32 esz = tag_esz(tg.type);
+        void* data = dev_alloc((size_t)n * tg.ncomps * esz, s);
+        u64 total = (u64)n * tg.ncomps;
+        if (esz == 1)
+          launch_concat<unsigned char>(nm, meta, tag_at[d][t], offs_at[d], tg.ncomps, nullptr,
+              total, data, s);
+        else if (esz == 4)
+          launch_concat<u32>(nm, meta, tag_at[d][t], offs_at[d], tg.ncomps, nullptr, total,
+              data, s);
+        else
+          launch_concat<u64>(nm, meta, tag_at[d][t], offs_at[d], tg.ncomps, nullptr, total,
+              data, s);
+        u->add_tag(d, tg.type, tg.name.c_str(), tg.ncomps, tg.transfer, data);
+      }
+      if (a.parallel && a.globals[d]) {
+        u64* g = dalloc<u64>(n, s);
+        launch_concat<u64>(nm, meta, glob_at[d], offs_at[d], 1, meta.at<u64 const>(goff_at[d]),
+            n, g, s);
+        u->set_globals(d, g);
+      }
+    }
+    u->nseg = nm;
+    u32 nv = offs[0][nm];
+    u->seg = dalloc<u32>(nv, s);
+    if (nv) {
+      k_seg_fill<<<capped_grid(nv), BLOCK, 0, s>>>(nm, meta.at<u32 const>(offs_at[0]), u->seg);
+      CK_LAUNCH();
+    }
+    dev_free(meta.dev, s);
+  } catch (...) {
+    delete u;
+    throw;
+  }
+  return u;
+}
+
+std::vector<Mesh*> split_union(Mesh& u, cudaStream_t stream)
+{
+  cudaStream_t s = u.s;
+  u32 nm = u.nseg, dim = u.dim;
+  if (!u.seg) throw Failure(E_ARG, "mesh is not a union of meshes");
+  std::vector<Mesh*> out(nm, nullptr);
+  u32* es[4] = {};
+  u32* local[4] = {};
+  std::vector<u32> counts[4];
+  try {
+    for (u32 k = 0; k < nm; ++k) out[k] = new Mesh(dim, u.full, u.parallel, stream, u.mb);
+    // stable counting sort of every dimension's entities by segment
+    for (u32 d = 0; d <= dim; ++d) {
+      if (!u.has_dim(d)) continue;
+      u32 n = u.count(d);
+      if (d) {
+        es[d] = dalloc<u32>(n ? n : 1, s);
+        if (n) {
+          k_ent_seg<<<grid_for(n), BLOCK, 0, s>>>(n, u.ask_down(d, 0), deg(d, 0), u.seg, es[d]);
+          CK_LAUNCH();
+        }
+      } else {
+        es[0] = u.seg;
+      }
+      u32 ntiles = n ? ceil_div(n, SPLIT_TILE) : 1;
+      u64 nh = (u64)nm * ntiles;
+      if (nh >= (1ull << 32) - 1) throw Failure(E_ARG, "too many meshes in one union to split");
+      u32* hist = dalloc<u32>(nh, s);
+      CK(cudaMemsetAsync(hist, 0, sizeof(u32) * nh, s));
+      u32 warps_per_block = BLOCK / 32;
+      if (n) {
+        k_tile_hist<<<ceil_div(ntiles, warps_per_block), BLOCK, 0, s>>>(n, es[d], ntiles, hist);
+        CK_LAUNCH();
+      }
+      u32* scan = exscan_new(hist, (u32)nh, s);
+      dev_free(hist, s);
+      u32* bases = dalloc<u32>(nm + 1, s);
+      k_seg_bases<<<grid_for(nm + 1), BLOCK, 0, s>>>(nm, ntiles, scan, bases);
+      CK_LAUNCH();
+      u32* perm = dalloc<u32>(n ? n : 1, s);
+      if (n) {
+        k_tile_scatter<<<ceil_div(ntiles, warps_per_block), BLOCK, 0, s>>>(n, es[d], ntiles,
+            scan, perm);
+        CK_LAUNCH();
+      }
+      dev_free(scan, s);
+      local[d] = dalloc<u32>(n ? n : 1, s);
+      if (n) {
+        k_local_ids<<<grid_for(n), BLOCK, 0, s>>>(n, es[d], perm, bases, local[d]);
+        CK_LAUNCH();
+      }
+      dev_free(perm, s);
+      counts[d].resize(nm + 1);
+      CK(cudaMemcpyAsync(counts[d].data(), bases, sizeof(u32) * (nm + 1), cudaMemcpyDeviceToHost, s));
+      dev_free(bases, s);
+    }
+    stream_sync(s);
+    for (u32 d = 0; d <= dim; ++d) {
+      if (!u.has_dim(d)) continue;
+      std::vector<u32>& c = counts[d];
+      for (u32 k = nm; k > 0; --k) c[k] -= c[k - 1];  // bases -> per-segment counts at [1..nm]
+    }
+    // allocate every mesh's arrays, then one scatter launch per array
+    Meta meta;
+    size_t conn_at[4] = {0, 0, 0, 0}, glob_at[4] = {0, 0, 0, 0};
+    std::vector<size_t> tag_at[4];
+    std::vector<void const*> p(nm);
+    for (u32 d = 0; d <= dim; ++d) {
+      if (!u.has_dim(d)) continue;
+      if (d) {
+        u32 vpe = deg(d, 0);
+        for (u32 k = 0; k < nm; ++k) {
+          u32 nk = counts[d][k + 1];
+          u32* conn = dalloc<u32>((size_t)nk * vpe, s);
+          out[k]->set_ents(d, nk, conn);
+          p[k] = conn;
+        }
+        conn_at[d] = meta.add(p.data(), nm);
+      } else {
+        for (u32 k = 0; k < nm; ++k) out[k]->set_ents(0, counts[0][k + 1], nullptr);
+      }
+      for (Tag const& t : u.tags[d]) {
+        for (u32 k = 0; k < nm; ++k) {
+          u32 nk = counts[d][k + 1];
+          void* data = dev_alloc((size_t)nk * t.ncomps * tag_esz(t.type), s);
+          out[k]->add_tag(d, t.type, t.name.c_str(), t.ncomps, t.transfer, data);
+          p[k] = data;
+        }
+        tag_at[d].push_back(meta.add(p.data(), nm));
+      }
+      if (u.parallel && u.globals[d]) {
+        for (u32 k = 0; k < nm; ++k) {
+          u64* g = dalloc<u64>(counts[d][k + 1], s);
+          out[k]->set_globals(d, g);
+          p[k] = g;
+        }
+        glob_at[d] = meta.add(p.data(), nm);
+      }
+    }
+    meta.upload(s);
+    for (u32 d = 0; d <= dim; ++d) {
+      if (!u.has_dim(d)) continue;
+      u32 n = u.count(d);
+      if (d) launch_scatter<u32>(n, deg(d, 0), u.down[d][0], es[d], local[d], local[0], meta,
+          conn_at[d], s);
+      for (size_t t = 0; t < u.tags[d].size(); ++t) {
+        Tag const& tg = u.tags[d][t];
+        u32 esz = tag_esz(tg.type);
+        if (esz == 1)
+          launch_scatter<unsigned char>(n, tg.ncomps, tg.data, es[d], local[d], nullptr, meta,
+              tag_at[d][t], s);
+        else if (esz == 4)
+          launch_scatter<u32>(n, tg.ncomps, tg.data, es[d], local[d], nullptr, meta,
+              tag_at[d][t], s);
+        else
+          launch_scatter<u64>(n, tg.ncomps, tg.data, es[d], local[d], nullptr, meta,
+              tag_at[d][t], s);
+      }
+      if (u.parallel && u.globals[d] && n) {
+        k_scatter_iota64<<<grid_for(n), BLOCK, 0, s>>>(n, es[d], local[d],
+            meta.at<u64* const>(glob_at[d]));
+        CK_LAUNCH();
+      }
+    }
+    stream_sync(s);
+    dev_free(meta.dev, s);
+  } catch (...) {
+    for (Mesh* m : out) delete m;
+    for (u32 d = 1; d < 4; ++d) dev_free(es[d], s);
+    for (u32 d = 0; d < 4; ++d) dev_free(local[d], s);
+    throw;
+  }
+  for (u32 d = 1; d < 4; ++d) dev_free(es[d], s);
+  for (u32 d = 0; d < 4; ++d) dev_free(local[d], s);
+  stream_sync(s);
+  return out;
+}
+
+// ---------------------------------------------------------------------------
+// the per-mesh pass loop over a union
+
+namespace {
+
+enum : u32 { ST_REFINE, ST_COARSEN, ST_SHAPE, ST_DONE, ST_FAILED };
+enum : u32 { OP_REFINE, OP_COARSEN, OP_SWAP, OP_CSLIVERS };
+
+struct UnionCtl {
+  Mesh& u;
+  u32 nm;
+  u32* active = nullptr;          // device
+  double* floor = nullptr;        // device
+  u32* selected = nullptr;        // device
+  u32* elems = nullptr;           // device
+  unsigned long long* minkey = nullptr;  // device
+  u32* h_u32 = nullptr;           // pinned: selected[nm], elems[nm]
+  unsigned long long* h_key = nullptr;   // pinned: minkey[nm]
+  SegCtl ctl;
+
+  explicit UnionCtl(Mesh& m) : u(m), nm(m.nseg)
+  {
+    cudaStream_t s = u.s;
+    active = dalloc<u32>(nm, s);
+    floor = dalloc<double>(nm, s);
+    selected = dalloc<u32>(nm, s);
+    elems = dalloc<u32>(nm, s);
+    minkey = dalloc<unsigned long long>(nm, s);
+    CK(cudaMallocHost(&h_u32, sizeof(u32) * 2 * nm));
+    CK(cudaMallocHost(&h_key, sizeof(unsigned long long) * nm));
+  }
+  ~UnionCtl()
+  {
+    cudaStream_t s = u.s;
+    u.ctl = nullptr;
+    cudaStreamSynchronize(s);
+    dev_free(active, s);
+    dev_free(floor, s);
+    dev_free(selected, s);
+    dev_free(elems, s);
+    dev_free(minkey, s);
+    cudaFreeHost(h_u32);
+    cudaFreeHost(h_key);
+  }
+
+  // per-segment minimum element quality (mesh_min_quality of each mesh)
+  std::vector<double> min_quality()
+  {
+    cudaStream_t s = u.s;
+    u32 ne = u.count(u.dim);
+    double const* q = u.qualities();
+    CK(cudaMemsetAsync(minkey, 0xff, sizeof(unsigned long long) * nm, s));
+    if (ne) {
+      k_seg_min_quality<<<grid_for(ne), BLOCK, 0, s>>>(ne, q, u.ask_down(u.dim, 0),
+          deg(u.dim, 0), u.seg, minkey);
+      CK_LAUNCH();
+    }
+    CK(cudaMemcpyAsync(h_key, minkey, sizeof(unsigned long long) * nm, cudaMemcpyDeviceToHost, s));
+    stream_sync(s);
+    std::vector<double> r(nm);
+    for (u32 k = 0; k < nm; ++k) r[k] = h_key[k] == ~0ull ? DBL_MAX : from_order_key(h_key[k]);
+    return r;
+  }
+
+  // one pass over the union acting on `group`; returns per-segment selected
+  // counts in h_u32[0..nm) and elements entering the pass in h_u32[nm..2nm)
+  void run(u32 op, std::vector<u32> const& group, std::vector<double> const& floors,
+      double size_floor, double good_qual, u32 nlayers)
+  {
+    cudaStream_t s = u.s;
+    std::vector<u32> act(nm, 0);
+    for (u32 k : group) act[k] = 1;
+    CK(cudaMemcpyAsync(active, act.data(), sizeof(u32) * nm, cudaMemcpyHostToDevice, s));
+    bool with_floor = op == OP_REFINE || op == OP_COARSEN;
+    if (with_floor)
+      CK(cudaMemcpyAsync(floor, floors.data(), sizeof(double) * nm, cudaMemcpyHostToDevice, s));
+    CK(cudaMemsetAsync(selected, 0, sizeof(u32) * nm, s));
+    CK(cudaMemsetAsync(elems, 0, sizeof(u32) * nm, s));
+    u32 ne = u.count(u.dim);
+    if (ne) {
+      k_seg_count<<<grid_for(ne), BLOCK, 0, s>>>(ne, u.ask_down(u.dim, 0), deg(u.dim, 0), u.seg,
+          elems);
+      CK_LAUNCH();
+    }
+    ctl.active = active;
+    ctl.floor = with_floor ? floor : nullptr;
+    ctl.selected = selected;
+    u.ctl = &ctl;
+    switch (op) {
+      case OP_REFINE: refine_by_size(u, 0.0); break;
+      case OP_COARSEN: coarsen_by_size(u, 0.0, size_floor); break;
+      case OP_SWAP: swap_slivers(u, good_qual, nlayers); break;
+      default: coarsen_slivers(u, good_qual, nlayers); break;
+    }
+    u.ctl = nullptr;
+    CK(cudaMemcpyAsync(h_u32, selected, sizeof(u32) * nm, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(h_u32 + nm, elems, sizeof(u32) * nm, cudaMemcpyDeviceToHost, s));
+    stream_sync(s);
+    last_batch_stats().union_passes += 1;
+  }
+};
+
+}  // namespace
+
+void adapt_union(Mesh& u, double size_floor, double good_qual, u32 nlayers, u32 max_ops,
+    std::vector<BatchMeshResult>& res)
+{
+  u32 nm = u.nseg;
+  res.assign(nm, BatchMeshResult());
+  if (!nm) return;
+  BatchStats& bs = last_batch_stats();
+  bs.unions += 1;
+  UnionCtl c(u);
+  std::vector<u32> state(nm, ST_REFINE), ops(nm, 0);
+  // satisfy_size's floor (adapt.cpp:47-52), one per mesh
+  std::vector<double> qf = c.min_quality();
+  for (u32 k = 0; k < nm; ++k)
+    if (good_qual < qf[k]) qf[k] = good_qual;
+  // incr_op_count (adapt.cpp:36-45) for mesh k after a pass that changed it
+  u32 cur_op = 0;
+  auto counted = [&](u32 k) {
+    res[k].ops.push_back(cur_op);
+    res[k].passes += 1;
+    res[k].elems_in += c.h_u32[nm + k];
+    bs.mesh_passes += 1;
+    bs.elems_in += c.h_u32[nm + k];
+    if (ops[k] > max_ops) {
+      res[k].status = E_MAXOPS;
+      state[k] = ST_FAILED;
+      return false;
+    }
+    ++ops[k];
+    return true;
+  };
+  auto members = [&](u32 st) {
+    std::vector<u32> g;
+    for (u32 k = 0; k < nm; ++k)
+      if (state[k] == st) g.push_back(k);
+    return g;
+  };
+  for (;;) {
+    bool live = false;
+    for (u32 k = 0; k < nm; ++k) live = live || state[k] < ST_DONE;
+    if (!live) break;
+    bs.steps += 1;
+    // satisfy_size: refine while it changes the mesh, then coarsen
+    std::vector<u32> g = members(ST_REFINE);
+    if (!g.empty()) {
+      cur_op = OP_REFINE;
+      c.run(OP_REFINE, g, qf, size_floor, good_qual, nlayers);
+      for (u32 k : g)
+        if (c.h_u32[k])
+          counted(k);
+        else
+          state[k] = ST_COARSEN;
+    }
+    g = members(ST_COARSEN);
+    if (!g.empty()) {
+      cur_op = OP_COARSEN;
+      c.run(OP_COARSEN, g, qf, size_floor, good_qual, nlayers);
+      for (u32 k : g)
+        if (c.h_u32[k])
+          counted(k);
+        else
+          state[k] = ST_SHAPE;
+    }
+    // satisfy_shape (adapt.cpp:58-80): swap, else collapse slivers
+    g = members(ST_SHAPE);
+    if (g.empty()) continue;
+    std::vector<double> mq = c.min_quality();
+    std::vector<u32> g2;
+    for (u32 k : g)
+      if (mq[k] >= good_qual)
+        state[k] = ST_DONE;
+      else
+        g2.push_back(k);
+    std::vector<u32> g3;
+    if (u.dim == 3 && !g2.empty()) {
+      cur_op = OP_SWAP;
+      c.run(OP_SWAP, g2, qf, size_floor, good_qual, nlayers);
+      for (u32 k : g2)
+        if (c.h_u32[k])
+          counted(k);
+        else
+          g3.push_back(k);
+    } else {
+      g3 = g2;
+    }
+    if (!g3.empty()) {
+      cur_op = OP_CSLIVERS;
+      c.run(OP_CSLIVERS, g3, qf, size_floor, good_qual, nlayers);
+      for (u32 k : g3)
+        if (c.h_u32[k])
+          counted(k);
+        else
+          state[k] = ST_DONE;  // shape quality could not be satisfied
+    }
+  }
+  for (u32 k = 0; k < nm; ++k) res[k].changed = ops[k] > 0 || res[k].passes > 0;
+}
+
+// ---------------------------------------------------------------------------
+// tag lists: which tags a pass leaves on each dimension, and in what order.
+// A union's tag list follows the passes the union ran; each mesh's must
+// follow the passes that changed it, so the split replays those.
+
+namespace {
+
+struct Layout {
+  std::vector<Tag> tags[4];  // name, type, ncomps, transfer (data unused)
+};
+
+Layout layout_of(Mesh& m)
+{
+  Layout l;
+  for (u32 d = 0; d <= m.dim; ++d)
+    for (Tag const& t : m.tags[d]) {
+      Tag x = t;
+      x.data = nullptr;
+      l.tags[d].push_back(x);
+    }
+  return l;
+}
+
+Tag const* find_in(std::vector<Tag> const& v, char const* name)
+{
+  for (Tag const& t : v)
+    if (t.name == name) return &t;
+  return nullptr;
+}
+
+// the tag lists refine_build, coarsen_build and swap_build produce
+Layout layout_after(u32 op, Layout const& in, u32 dim)
+{
+  Layout out;
+  std::vector<Tag> cls;
+  if (find_in(in.tags[0], "class_dim")) {
+    for (char const* nm : {"class_dim", "class_id"})
+      for (u32 d = 0; d <= dim; ++d)
+        if (Tag const* t = find_in(in.tags[d], nm)) {
+          if (d == 0) {
+            Tag x = *t;
+            cls.push_back(x);
+          }
+        }
+  }
+  auto class_of = [&](u32 d) {
+    std::vector<Tag> v;
+    for (Tag const& c : cls)
+      if (Tag const* t = find_in(in.tags[d], c.name.c_str())) v.push_back(*t);
+    return v;
+  };
+  // vertices: refinement keeps the f64 fields, then the class labels;
+  // collapses and swaps keep every vertex tag in place
+  if (op == OP_REFINE) {
+    for (Tag const& t : in.tags[0])
+      if (t.type == T_F64) out.tags[0].push_back(t);
+    for (Tag const& t : class_of(0)) out.tags[0].push_back(t);
+  } else {
+    out.tags[0] = in.tags[0];
+  }
+  for (u32 d = 1; d <= dim; ++d) {
+    out.tags[d] = class_of(d);
+    if (d != dim) continue;
+    for (Tag const& t : in.tags[d])
+      if (t.type == T_F64 && t.transfer == X_CONSERVE) out.tags[d].push_back(t);
+    bool any_fit = false;
+    for (Tag const& t : in.tags[d])
+      if (t.type == T_F64 && t.transfer == X_POINTWISE) any_fit = true;
+    if (any_fit && (op == OP_COARSEN || op == OP_CSLIVERS)) {
+      Tag x;
+      x.name = "coordinates";
+      x.type = T_F64;
+      x.ncomps = 3;
+      x.transfer = X_NOT;
+      out.tags[d].push_back(x);
+    }
+    for (Tag const& t : in.tags[d])
+      if (t.type == T_F64 && t.transfer == X_POINTWISE) out.tags[d].push_back(t);
+  }
+  return out;
+}
+
+// give mesh m exactly the tags of `want`, in its order: element coordinates
+// (which a collapse leaves behind) are recomputed when wanted, dropped when not
+void apply_layout(Mesh& m, Layout const& want)
+{
+  u32 dim = m.dim;
+  if (m.find_tag(dim, "coordinates")) m.remove_tag(dim, "coordinates");
+  if (find_in(want.tags[dim], "coordinates")) interp_coords_to_elems(m);
+  for (u32 d = 0; d <= dim; ++d) {
+    std::vector<Tag> next;
+    for (Tag const& w : want.tags[d]) {
+      Tag* t = m.find_tag(d, w.name.c_str());
+      if (!t) throw Failure(E_ARG, "batched mesh lost tag " + w.name);
+      next.push_back(*t);
+      t->data = nullptr;
+    }
+    for (Tag& t : m.tags[d]) dev_free(t.data, m.s);
+    m.tags[d].swap(next);
+  }
+}
+
+}  // namespace
+
+void adapt_batch(std::vector<Mesh*> const& ms, double size_floor, double good_qual,
+    u32 nlayers, u32 max_ops, unsigned long long max_union_elems,
+    std::vector<BatchMeshResult>& res)
+{
+  last_batch_stats() = BatchStats();
+  res.assign(ms.size(), BatchMeshResult());
+  size_t i = 0;
+  while (i < ms.size()) {
+    // the next union: consecutive meshes up to max_union_elems input elements
+    size_t j = i;
+    unsigned long long sum = 0;
+    while (j < ms.size()) {
+      unsigned long long ne = ms[j]->count(ms[j]->dim);
+      if (j > i && max_union_elems && sum + ne > max_union_elems) break;
+      sum += ne;
+      ++j;
+    }
+    std::vector<Mesh*> group(ms.begin() + i, ms.begin() + j);
+    Mesh* u = concat_meshes(group);
+    try {
+      Layout start = layout_of(*u);
+      std::vector<BatchMeshResult> r;
+      adapt_union(*u, size_floor, good_qual, nlayers, max_ops, r);
+      std::vector<Mesh*> outs = split_union(*u, u->s);
+      for (size_t k = 0; k < group.size(); ++k) {
+        res[i + k] = r[k];
+        if (r[k].passes) {
+          Layout want = start;
+          for (u32 op : r[k].ops) want = layout_after(op, want, u->dim);
+          apply_layout(*outs[k], want);
+          group[k]->overwrite(outs[k]);
+        } else {
+          delete outs[k];
+        }
+      }
+    } catch (...) {
+      delete u;
+      throw;
+    }
+    delete u;
+    i = j;
+  }
+}
+
+}  // namespace osh

@@ -8,6 +8,7 @@
 
 #include "../../include/omega_h.h"
 #include "../../include/omega_h_b200.h"
+#include "batch.hpp"
 #include "passes.hpp"
 
 using osh::Failure;
@@ -499,6 +500,47 @@ unsigned osh_b200_swap_slivers(osh_t h, double gq, unsigned nl)
 unsigned osh_b200_mesh_adapt(osh_t h, double sf, double gq, unsigned nl, unsigned mo)
 {
   return osh_adapt(h, sf, gq, nl, mo);
+}
+
+static thread_local std::vector<osh::BatchMeshResult> t_batch_res;
+
+int osh_b200_adapt_batch(osh_t* meshes, unsigned n, double sf, double gq, unsigned nl,
+    unsigned mo, unsigned long long max_union_elems, unsigned* changed, int* status)
+{
+  API_TRY
+  need(meshes != nullptr || n == 0, "meshes is NULL");
+  std::vector<Mesh*> ms(n);
+  for (unsigned i = 0; i < n; ++i) {
+    need(meshes[i] != nullptr, "a mesh handle is NULL");
+    ms[i] = M(meshes[i]);
+  }
+  t_batch_res.clear();
+  if (n) osh::adapt_batch(ms, sf, gq, nl, mo, max_union_elems, t_batch_res);
+  for (unsigned i = 0; i < n; ++i) {
+    if (changed) changed[i] = t_batch_res[i].changed;
+    if (status) status[i] = t_batch_res[i].status;
+    sync(ms[i]);
+  }
+  return 0;
+  API_CATCH(osh::last_error())
+}
+
+void osh_b200_batch_stats(unsigned* unions, unsigned* steps, unsigned* union_passes,
+    unsigned* mesh_passes, double* elems_in)
+{
+  osh::BatchStats const& b = osh::last_batch_stats();
+  if (unions) *unions = b.unions;
+  if (steps) *steps = b.steps;
+  if (union_passes) *union_passes = b.union_passes;
+  if (mesh_passes) *mesh_passes = b.mesh_passes;
+  if (elems_in) *elems_in = b.elems_in;
+}
+
+void osh_b200_batch_mesh_stats(unsigned i, unsigned* passes, double* elems_in)
+{
+  bool ok = i < t_batch_res.size();
+  if (passes) *passes = ok ? t_batch_res[i].passes : 0;
+  if (elems_in) *elems_in = ok ? t_batch_res[i].elems_in : 0;
 }
 
 double osh_b200_min_quality(osh_t h)

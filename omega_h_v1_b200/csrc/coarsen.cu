@@ -11,7 +11,7 @@ __device__ inline u32 collapses(u32 code, u32 dir) { return (code >> dir) & 1u; 
 // coarsen_size_code (coarsen.cpp:13-21) fused with measure_edge
 __global__ void k_coarsen_size_codes(u32 ne, u32 const* __restrict__ voe,
     double const* __restrict__ x, double const* __restrict__ h, double size_floor,
-    u32* __restrict__ codes, u32* any)
+    SegView sv, u32* __restrict__ codes, u32* any)
 {
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   u32 c = 0;
@@ -22,7 +22,8 @@ __global__ void k_coarsen_size_codes(u32 ne, u32 const* __restrict__ voe,
     load3(x, b, xb);
     double len = sqrt(sqdist3(xb, xa));
     double want = (h[a] + h[b]) / 2;
-    c = ((len / want) < size_floor) ? (u32)COLLAPSE_BOTH : (u32)DONT_COLLAPSE;
+    c = ((len / want) < size_floor && seg_acts(sv, a)) ? (u32)COLLAPSE_BOTH
+                                                        : (u32)DONT_COLLAPSE;
     codes[i] = c;
   }
   if (__any_sync(0xffffffffu, c) && (threadIdx.x & 31) == 0) atomicOr(any, 1u);
@@ -96,7 +97,7 @@ __global__ void k_coarsen_quality(u32 dim, u32 ne, u32 const* __restrict__ voe1,
     u32 const* __restrict__ voe, u32 const* __restrict__ ev_offs,
     u32 const* __restrict__ ev, u32 const* __restrict__ ev_dirs,
     double const* __restrict__ x, double const* __restrict__ eq, double floor_q,
-    u32* __restrict__ codes, double* __restrict__ out, u32* any)
+    SegView sv, u32* __restrict__ codes, double* __restrict__ out, u32* any)
 {
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   u32 keep = 0;
@@ -105,6 +106,7 @@ __global__ void k_coarsen_quality(u32 dim, u32 ne, u32 const* __restrict__ voe1,
     if (code != DONT_COLLAPSE) {
       u32 vpe = deg(dim, 0);
       double const perfect = dim == 3 ? perfect_tet_quality() : perfect_tri_quality();
+      double const fq = seg_floor(sv, voe1[i * 2], floor_q);
       for (u32 j = 0; j < 2; ++j) {
         if (!collapses(code, j)) continue;
         double minq = 1, old_minq = 1;
@@ -124,7 +126,7 @@ __global__ void k_coarsen_quality(u32 dim, u32 ne, u32 const* __restrict__ voe1,
           double q = dim == 3 ? tet_quality(ex, perfect) : tri_quality(ex, 1, perfect);
           if (q < minq) minq = q;
         }
-        if (minq < floor_q || (eq && minq <= old_minq))
+        if (minq < fq || (eq && minq <= old_minq))
           code &= ~(1u << j);
         else
           out[i * 2 + j] = minq;
@@ -504,7 +506,8 @@ static bool coarsen_select(Mesh& m, u32* codes, double qual_floor, bool require_
       PROBE(P_COARSEN_QUALITY, s, 4.0 * (nv + 1) + 8.0 * deg(dim, 0) * nel + 8.0 * ne +
           4.0 * deg(dim, 0) * nel + 24.0 * nv + 8.0 * ne + 16.0 * ne);
       k_coarsen_quality<<<grid_for(ne), BLOCK, 0, s>>>(dim, ne, voe1, m.ask_down(dim, 0),
-          ev.offs, ev.adj, ev.dirs, m.coords(), eq, qual_floor, codes, sel.q2, any);
+          ev.offs, ev.adj, ev.dirs, m.coords(), eq, qual_floor, m.segview(), codes, sel.q2,
+          any);
       CK_LAUNCH();
     }
   }
@@ -546,6 +549,10 @@ static void coarsen_build(Mesh& m, CoarsenSel const& sel)
     void* d = dev_alloc((size_t)nv_out * t.ncomps * esz, s);
     expand_scaled(t.data, same_v, 1, nv, t.ncomps, esz, d, s);
     out->add_tag(0, t.type, t.name.c_str(), t.ncomps, t.transfer, d);
+  }
+  if (m.seg) {
+    out->seg = dalloc<u32>(nv_out, s);
+    expand_scaled(m.seg, same_v, 1, nv, 1, 4, out->seg, s);
   }
   if (m.parallel) inherit_globals(*out, 0, nv_out);
   u32* fused[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -615,7 +622,10 @@ static u32 coarsen_common(Mesh& m, u32* codes, double qual_floor, bool require_b
   bool ok = false;
   try {
     ok = coarsen_select(m, codes, qual_floor, require_better, sel, nullptr, nullptr);
-    if (ok) coarsen_build(m, sel);
+    if (ok) {
+      seg_tally(m, 0, sel.ind);
+      coarsen_build(m, sel);
+    }
   } catch (...) {
     sel.free(m.s);
     throw;
@@ -640,7 +650,7 @@ u32 coarsen_by_size(Mesh& m, double qual_floor, double size_floor)
   CK(cudaMemsetAsync(any, 0, sizeof(u32), s));
   if (ne) {
     k_coarsen_size_codes<<<grid_for(ne), BLOCK, 0, s>>>(ne, m.ask_down(1, 0), m.coords(),
-        static_cast<double const*>(h->data), size_floor, codes, any);
+        static_cast<double const*>(h->data), size_floor, m.segview(), codes, any);
     CK_LAUNCH();
   }
   u32 r = 0;
@@ -701,7 +711,7 @@ u32 coarsen_sets(Mesh& m, double qual_floor, double size_floor, u32* codes_size,
   CK(cudaMemsetAsync(gen_vert, 0xff, sizeof(u32) * nv, s));
   if (ne) {
     k_coarsen_size_codes<<<grid_for(ne), BLOCK, 0, s>>>(ne, m.ask_down(1, 0), m.coords(),
-        static_cast<double const*>(h->data), size_floor, codes_size, any);
+        static_cast<double const*>(h->data), size_floor, m.segview(), codes_size, any);
     CK_LAUNCH();
   }
   u32* codes = dalloc<u32>(ne, s);

@@ -12,6 +12,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <cstring>
 #include <stdexcept>
 #include <string>
 
@@ -59,6 +60,21 @@ void count_launch();
   } while (0)
 
 inline u32 ceil_div(u64 a, u64 b) { return (u32)((a + b - 1) / b); }
+
+// order-preserving 64-bit key of a double (min of keys = min of values)
+__device__ inline unsigned long long order_key(double x)
+{
+  unsigned long long b = (unsigned long long)__double_as_longlong(x);
+  return (b >> 63) ? ~b : (b | (1ull << 63));
+}
+
+__host__ inline double from_order_key(unsigned long long k)
+{
+  unsigned long long b = (k >> 63) ? (k & ~(1ull << 63)) : ~k;
+  double x;
+  std::memcpy(&x, &b, sizeof(x));
+  return x;
+}
 
 constexpr int BLOCK = 256;
 inline u32 grid_for(u64 n) { return n ? ceil_div(n, BLOCK) : 1; }

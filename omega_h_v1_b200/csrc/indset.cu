@@ -306,10 +306,34 @@ u32* mark_up(Mesh& m, u32 low, u32 high, u32 const* marked)
 }
 
 __global__ void k_mark_slivers(u32 n, double const* __restrict__ q, double gq,
-    u32* __restrict__ out)
+    u32 const* __restrict__ voe, u32 vpe, SegView sv, u32* __restrict__ out)
 {
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) out[i] = (q[i] < gq) ? 1u : 0u;
+  if (i < n) out[i] = (q[i] < gq && (!sv.active || seg_acts(sv, voe[(size_t)i * vpe]))) ? 1u : 0u;
+}
+
+// warp-aggregated per-segment count of flagged entities
+__global__ void k_seg_tally(u32 n, u32 const* __restrict__ flags, u32 const* __restrict__ voe,
+    u32 vpe, u32 const* __restrict__ seg, u32* __restrict__ out)
+{
+  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+  bool on = i < n && flags[i] != 0;
+  u32 mask = __ballot_sync(0xffffffffu, on);
+  if (!on) return;
+  u32 sg = seg[voe ? voe[(size_t)i * vpe] : i];
+  u32 peers = __match_any_sync(mask, sg);
+  if ((threadIdx.x & 31) == (u32)(__ffs(peers) - 1)) atomicAdd(&out[sg], (u32)__popc(peers));
+}
+
+void seg_tally(Mesh& m, u32 ent_dim, u32 const* flags)
+{
+  if (!m.seg || !m.ctl || !m.ctl->selected) return;
+  u32 n = m.count(ent_dim);
+  if (!n) return;
+  u32 const* voe = ent_dim ? m.ask_down(ent_dim, 0) : nullptr;
+  k_seg_tally<<<grid_for(n), BLOCK, 0, m.s>>>(n, flags, voe, deg(ent_dim, 0), m.seg,
+      m.ctl->selected);
+  CK_LAUNCH();
 }
 
 __global__ void k_dual_layer(u32 n, u32 degr, u32 const* __restrict__ dual,
@@ -332,7 +356,9 @@ u32* mark_slivers(Mesh& m, double gq, u32 nlayers)
   double const* q = m.qualities();
   u32* a = dalloc<u32>(n, m.s);
   if (n) {
-    k_mark_slivers<<<grid_for(n), BLOCK, 0, m.s>>>(n, q, gq, a);
+    SegView sv = m.segview();
+    k_mark_slivers<<<grid_for(n), BLOCK, 0, m.s>>>(n, q, gq,
+        sv.active ? m.ask_down(m.dim, 0) : nullptr, deg(m.dim, 0), sv, a);
     CK_LAUNCH();
   }
   if (!nlayers) return a;

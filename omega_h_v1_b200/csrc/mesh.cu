@@ -56,7 +56,10 @@ Mesh::~Mesh()
 
 Mesh* Mesh::spawn() const
 {
-  return new Mesh(dim, full, parallel, s, mb);
+  Mesh* m = new Mesh(dim, full, parallel, s, mb);
+  m->nseg = nseg;
+  m->ctl = ctl;
+  return m;
 }
 
 Mesh* Mesh::clone()
@@ -87,6 +90,12 @@ Mesh* Mesh::clone()
       }
     }
     c->ghost_layers = ghost_layers;
+    if (seg) {
+      c->nseg = nseg;
+      c->seg = dalloc<u32>(counts[0], c->s);
+      CK(cudaMemcpyAsync(c->seg, seg, sizeof(u32) * counts[0], cudaMemcpyDeviceToDevice,
+          c->s));
+    }
     stream_sync(c->s);
   } catch (...) {
     delete c;
@@ -143,6 +152,8 @@ void Mesh::clear_contents()
   }
   dev_free(qual_cache, s);
   qual_cache = nullptr;
+  dev_free(seg, s);
+  seg = nullptr;
 }
 
 void Mesh::overwrite(Mesh* with)
@@ -181,6 +192,9 @@ void Mesh::overwrite(Mesh* with)
   }
   qual_cache = with->qual_cache;
   with->qual_cache = nullptr;
+  nseg = with->nseg;
+  seg = with->seg;
+  with->seg = nullptr;
   delete with;
 }
 
@@ -1053,19 +1067,6 @@ u32 const* Mesh::ask_dual()
 // ---------------------------------------------------------------------------
 // geometry: qualities, sizes, edge lengths (quality.cpp, size.cpp)
 
-__device__ inline unsigned long long order_key(double x)
-{
-  unsigned long long b = (unsigned long long)__double_as_longlong(x);
-  return (b >> 63) ? ~b : (b | (1ull << 63));
-}
-
-__host__ inline double from_order_key(unsigned long long k)
-{
-  unsigned long long b = (k >> 63) ? (k & ~(1ull << 63)) : ~k;
-  double x;
-  std::memcpy(&x, &b, sizeof(x));
-  return x;
-}
 
 __global__ void k_elem_quality(u32 dim, u32 ne, u32 const* __restrict__ voe,
     double const* __restrict__ x, double* __restrict__ q,

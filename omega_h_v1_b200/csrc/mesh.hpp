@@ -46,6 +46,23 @@ struct Graph {
   u32 nadj = 0;
 };
 
+// Several meshes adapted together as one disjoint union. Every vertex knows
+// the mesh ("segment") it came from; a pass reads the per-segment controls
+// below so that it acts only on some segments, with a quality floor of each
+// segment's own, and reports how many entities it selected per segment.
+struct SegCtl {
+  u32 const* active = nullptr;    // device, per segment: the pass may act
+  double const* floor = nullptr;  // device, per segment: quality floor
+  u32* selected = nullptr;        // device, per segment: entities selected
+};
+
+// what a kernel sees of SegCtl (all null for a single mesh)
+struct SegView {
+  u32 const* seg = nullptr;
+  u32 const* active = nullptr;
+  double const* floor = nullptr;
+};
+
 struct Mesh {
   u32 dim = 3;
   bool full = false;
@@ -67,6 +84,11 @@ struct Mesh {
   u32* own_ids[4] = {};     // cached iota, API only
   u32 ghost_layers = 0;
   double* qual_cache = nullptr;  // element qualities of this mesh state
+  // disjoint union of nseg meshes: segment of every vertex (owned), and the
+  // controls of the running pass (not owned; null = every segment acts)
+  u32 nseg = 0;
+  u32* seg = nullptr;
+  SegCtl const* ctl = nullptr;
   cudaStream_t s = nullptr;
   bool own_stream = false;
   std::shared_ptr<Mailbox> mb;  // shared by a mesh and the meshes it spawns
@@ -114,6 +136,17 @@ struct Mesh {
   double min_quality();
   double* element_sizes();      // caller frees
   double* measure_edges();      // caller frees: |x1-x0| / mean size
+
+  SegView segview() const
+  {
+    SegView v;
+    if (seg && ctl) {
+      v.seg = seg;
+      v.active = ctl->active;
+      v.floor = ctl->floor;
+    }
+    return v;
+  }
 
   void set_globals(u32 d, u64* g);
   void derive_model(double crease_angle);  // host classification

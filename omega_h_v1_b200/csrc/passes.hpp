@@ -6,6 +6,21 @@
 
 namespace osh {
 
+// segment controls of a disjoint union of meshes (SegCtl): whether the pass
+// acts on the segment of vertex `vert`, and that segment's quality floor
+__device__ inline bool seg_acts(SegView const& v, u32 vert)
+{
+  return !v.active || v.active[v.seg[vert]] != 0;
+}
+__device__ inline double seg_floor(SegView const& v, u32 vert, double f)
+{
+  return v.floor ? v.floor[v.seg[vert]] : f;
+}
+
+// add, per segment, the number of flagged entities of dimension ent_dim to
+// m.ctl->selected (no-op for a single mesh)
+void seg_tally(Mesh& m, u32 ent_dim, u32 const* flags);
+
 // Luby independent set over the star graph of `ent_dim` entities
 // (mesh_find_indset, indset.cpp:119-139). filter and goodness are device
 // arrays; returns a device state array (1 = in set) or throws E_NOCONVERGE.

@@ -13,8 +13,8 @@ namespace osh {
 
 // refine_candidate (refine.cpp:11-15) fused with measure_edge (size.cpp:57)
 __global__ void k_refine_candidates(u32 ne, u32 const* __restrict__ voe,
-    double const* __restrict__ x, double const* __restrict__ h, u32* __restrict__ cand,
-    u32* any)
+    double const* __restrict__ x, double const* __restrict__ h, SegView sv,
+    u32* __restrict__ cand, u32* any)
 {
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   u32 c = 0;
@@ -25,7 +25,7 @@ __global__ void k_refine_candidates(u32 ne, u32 const* __restrict__ voe,
     load3(x, b, xb);
     double len = sqrt(sqdist3(xb, xa));
     double want = (h[a] + h[b]) / 2;
-    c = (len / want) > 1.0;
+    c = (len / want) > 1.0 && seg_acts(sv, a);
     cand[i] = c;
   }
   if (__any_sync(0xffffffffu, c) && (threadIdx.x & 31) == 0) atomicOr(any, 1u);
@@ -36,7 +36,7 @@ __global__ void k_refine_candidates(u32 ne, u32 const* __restrict__ voe,
 __global__ void k_refine_quality(u32 dim, u32 ne, u32 const* __restrict__ voe1,
     u32 const* __restrict__ voe, u32 const* __restrict__ eo_offs,
     u32 const* __restrict__ eo, u32 const* __restrict__ eo_dirs,
-    double const* __restrict__ x, double qual_floor, u32* __restrict__ cand,
+    double const* __restrict__ x, double qual_floor, SegView sv, u32* __restrict__ cand,
     double* __restrict__ out, u32* any, u32* inverted)
 {
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -70,7 +70,7 @@ __global__ void k_refine_quality(u32 dim, u32 ne, u32 const* __restrict__ voe1,
         if (q < minq) minq = q;
       }
     }
-    if (minq < qual_floor) {
+    if (minq < seg_floor(sv, a, qual_floor)) {
       cand[i] = 0;
     } else {
       out[i] = minq;
@@ -95,6 +95,15 @@ __global__ void k_refine_nodal(u32 ne, u32 nv, u32 const* __restrict__ voe,
     acc += f[(size_t)b * nc + c];
     o[c] = acc / 2u;
   }
+}
+
+// segment of each new vertex: the segment of its edge's first vertex
+__global__ void k_refine_seg(u32 ne, u32 nv, u32 const* __restrict__ voe,
+    u32 const* __restrict__ gen_offs, u32 const* __restrict__ seg, u32* __restrict__ out)
+{
+  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= ne || gen_offs[i] == gen_offs[i + 1]) return;
+  out[nv + gen_offs[i]] = seg[voe[i * 2]];
 }
 
 // split_to_domain (splits_to_domains.cpp:13-31): first split edge of each
@@ -192,6 +201,14 @@ static void refine_build(Mesh& m, u32 const* gen_offs, u32 nsplit)
     out->add_tag(0, T_F64, t.name.c_str(), t.ncomps, X_NOT, d);
   }
   if (m.parallel) inherit_globals(*out, 0, nv_out);
+  if (m.seg) {
+    out->seg = dalloc<u32>(nv_out, s);
+    CK(cudaMemcpyAsync(out->seg, m.seg, sizeof(u32) * nv, cudaMemcpyDeviceToDevice, s));
+    if (ns) {
+      k_refine_seg<<<grid_for(ns), BLOCK, 0, s>>>(ns, nv, voe1, gen_offs, m.seg, out->seg);
+      CK_LAUNCH();
+    }
+  }
   // splits_to_domains for every domain dimension
   Splits sp[4];
   u32* zero_v = dalloc<u32>((size_t)nv + 1, s);
@@ -306,8 +323,8 @@ static u32* choose_refinement(Mesh& m, u32* cand, double qual_floor, double** qu
       PROBE(P_REFINE_QUALITY, s, 4.0 * (ne + 1) + 8.0 * deg(dim, 1) * nel + 8.0 * ne +
           4.0 * deg(dim, 0) * nel + 24.0 * m.counts[0] + 8.0 * ne + 8.0 * ne);
       k_refine_quality<<<grid_for(ne), BLOCK, 0, s>>>(dim, ne, m.ask_down(1, 0),
-          m.ask_down(dim, 0), eo.offs, eo.adj, eo.dirs, m.coords(), qual_floor, cand, q,
-          any, inverted);
+          m.ask_down(dim, 0), eo.offs, eo.adj, eo.dirs, m.coords(), qual_floor, m.segview(),
+          cand, q, any, inverted);
       CK_LAUNCH();
     }
     m.mb->fetch(s, 4);
@@ -339,6 +356,7 @@ static u32 refine_common(Mesh& m, u32* cand, double qual_floor)
   u32 ne = m.count(1);
   u32* ind = choose_refinement(m, cand, qual_floor, nullptr);
   if (!ind) return 0;
+  seg_tally(m, 1, ind);
   u32* gen_offs = exscan_new(ind, ne, s);
   dev_free(ind, s);
   u32 nsplit = read_u32(gen_offs + ne, s);
@@ -361,7 +379,7 @@ u32 refine_by_size(Mesh& m, double qual_floor)
   if (ne) {
     PROBE(P_REFINE_CANDIDATES, s, 8.0 * ne + 32.0 * m.counts[0] + 4.0 * ne);
     k_refine_candidates<<<grid_for(ne), BLOCK, 0, s>>>(ne, m.ask_down(1, 0), m.coords(),
-        static_cast<double const*>(h->data), cand, any);
+        static_cast<double const*>(h->data), m.segview(), cand, any);
     CK_LAUNCH();
   }
   // no separate check for "any candidate": with none, the quality kernel
@@ -392,7 +410,7 @@ u32 refine_sets(Mesh& m, double qual_floor, u32* cand_out, u32* good_out,
   CK(cudaMemsetAsync(indset_out, 0, sizeof(u32) * ne, s));
   if (ne) {
     k_refine_candidates<<<grid_for(ne), BLOCK, 0, s>>>(ne, m.ask_down(1, 0), m.coords(),
-        static_cast<double const*>(h->data), cand_out, any);
+        static_cast<double const*>(h->data), m.segview(), cand_out, any);
     CK_LAUNCH();
   }
   CK(cudaMemcpyAsync(good_out, cand_out, sizeof(u32) * ne, cudaMemcpyDeviceToDevice, s));

@@ -435,6 +435,10 @@ static void swap_build(Mesh& m, SwapSel const& sel)
     CK(cudaMemcpyAsync(d, t.data, bytes, cudaMemcpyDeviceToDevice, s));
     out->add_tag(0, t.type, t.name.c_str(), t.ncomps, t.transfer, d);
   }
+  if (m.seg) {
+    out->seg = dalloc<u32>(nv, s);
+    CK(cudaMemcpyAsync(out->seg, m.seg, sizeof(u32) * nv, cudaMemcpyDeviceToDevice, s));
+  }
   if (m.parallel && m.globals[0]) {
     u64* g = dalloc<u64>(nv, s);
     CK(cudaMemcpyAsync(g, m.globals[0], sizeof(u64) * nv, cudaMemcpyDeviceToDevice, s));
@@ -529,6 +533,7 @@ u32 swap_slivers(Mesh& m, double gq, u32 nlayers)
   try {
     ok = swap_select(m, gq, nlayers, sel, nullptr, nullptr, nullptr);
     if (ok) {
+      seg_tally(m, 1, sel.ind);
       st.nselected = 0;
       swap_build(m, sel);
       st.elems_out = m.count(3);
