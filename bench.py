@@ -354,6 +354,189 @@ def e2e_leg(G, L, base, args, world, stream, stream_ptr):
 
 
 # ---------------------------------------------------------------------------
+# batched workload: 512 box meshes of uneven sizes
+
+BATCH_CHUNK_EST_TETS = 60e6     # estimated output tets per adapt_batch call
+BATCH_UNION_ELEMS = 400000      # input elements per union inside a call
+
+
+def batched_chunks(jobs):
+    """Jobs in ascending input size, cut into calls of about
+    BATCH_CHUNK_EST_TETS estimated output tets (bounds the memory held)."""
+    order = sorted(range(len(jobs)), key=lambda i: (jobs[i].tets, i))
+    chunks, cur, est = [], [], 0.0
+    for i in order:
+        e = jobs[i].estimated_output_tets()
+        if cur and est + e > BATCH_CHUNK_EST_TETS:
+            chunks.append(cur)
+            cur, est = [], 0.0
+        cur.append(i)
+        est += e
+    if cur:
+        chunks.append(cur)
+    return chunks
+
+
+def run_batched(args, world, rank, local):
+    """512 meshes adapted one by one (plain FP64 path) and together
+    (adapt_batch), same inputs, same call order; every mesh's result must
+    have the same device digest in both legs."""
+    import torch
+    import omega_h_v1_b200 as G
+    from omega_h_v1_b200 import workloads as W
+    torch.cuda.set_device(local)
+    L = G.lib()
+    stream = torch.cuda.default_stream()
+    jobs = W.batched_boxes(args.batch_count, seed=1)
+    t0 = time.perf_counter()
+    bases = [W.build_job_mesh(G, j) for j in jobs]
+    prep_s = time.perf_counter() - t0
+    chunks = batched_chunks(jobs)
+
+    def clones():
+        out = []
+        for b in bases:
+            h = L.osh_b200_clone(b.h)
+            G.check()
+            L.osh_b200_set_stream(h, C.c_void_p(0))
+            out.append(h)
+        return out
+
+    def plain_leg(hs, idx):
+        digests, elems = {}, 0.0
+        for i in idx:
+            L.osh_adapt(hs[i], SIZE_FLOOR, GOOD_QUAL, NLAYERS, MAX_OPS)
+            G.check()
+            p, e = C.c_uint(), C.c_double()
+            L.osh_b200_adapt_stats(C.byref(p), C.byref(e))
+            elems += e.value
+            digests[i] = L.osh_b200_digest(hs[i])
+            L.osh_free(hs[i])
+        return digests, elems
+
+    def batch_leg(hs, chunk_list):
+        digests, elems, unions, upasses = {}, 0.0, 0, 0
+        for idx in chunk_list:
+            arr = (C.c_void_p * len(idx))(*[hs[i] for i in idx])
+            rc = L.osh_b200_adapt_batch(arr, len(idx), SIZE_FLOOR, GOOD_QUAL, NLAYERS,
+                                        MAX_OPS, BATCH_UNION_ELEMS, None, None)
+            if rc:
+                G.check()
+            u, st, up, mp = (C.c_uint() for _ in range(4))
+            e = C.c_double()
+            L.osh_b200_batch_stats(C.byref(u), C.byref(st), C.byref(up), C.byref(mp),
+                                   C.byref(e))
+            elems += e.value
+            unions += u.value
+            upasses += up.value
+            for i in idx:
+                digests[i] = L.osh_b200_digest(hs[i])
+                L.osh_free(hs[i])
+        return digests, elems, unions, upasses
+
+    # warm-up on the smallest meshes through both paths (untimed)
+    warm = chunks[0][:16]
+    hs = clones()
+    plain_leg(hs, warm)
+    for i in range(len(hs)):
+        if i not in warm:
+            L.osh_free(hs[i])
+    hs = clones()
+    batch_leg(hs, [warm])
+    for i in range(len(hs)):
+        if i not in warm:
+            L.osh_free(hs[i])
+    order = [i for c in chunks for i in c]
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        r = fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return r, e0.elapsed_time(e1)
+
+    hs = clones()
+    torch.cuda.synchronize()
+    launches0 = L.osh_b200_launch_count()
+    (pd, pe), plain_ms = timed(lambda: plain_leg(hs, order))
+    plain_launches = L.osh_b200_launch_count() - launches0
+    hs = clones()
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    launches0 = L.osh_b200_launch_count()
+    (bd, be, unions, upasses), batch_ms = timed(lambda: batch_leg(hs, chunks))
+    batch_launches = L.osh_b200_launch_count() - launches0
+    clk = clocks.stop()
+    same = all(pd[i] == bd[i] for i in range(len(jobs)))
+    for b in bases:
+        b.close()
+    value = be / (batch_ms / 1e3)
+    plain_value = pe / (plain_ms / 1e3)
+    out = {
+        "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world,
+        "steps": 1, "warmup": 1, "ms_per_step": round(batch_ms, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded box meshes, uniform size fields)",
+        "config": {"workload": "batched_512_boxes", "meshes": len(jobs),
+                   "n": "log-uniform in [4,40], seed 1", "size": "U[0.3/n, 1.5/n]",
+                   "tets_in": int(sum(j.tets for j in jobs)),
+                   "adapt": "mesh_adapt(1/3, 0.3, 4, 50) of every mesh",
+                   "calls": len(chunks), "union_input_elems": BATCH_UNION_ELEMS,
+                   "l2": "inputs larger than L2 (26M tets in, hundreds of M out)"},
+        "plain": {"value": round(plain_value, 1), "ms": round(plain_ms, 3),
+                  "gpu_launches": int(plain_launches)},
+        "speedup_vs_plain": round(plain_ms / batch_ms, 3),
+        "identical_to_plain": bool(same and abs(pe - be) < 0.5),
+        "elems_in": be, "unions": unions, "union_passes": upasses,
+        "gpu_launches": int(batch_launches), "clocks": clk,
+        "prep_s": round(prep_s, 1),
+    }
+    if not args.no_cpu and rank == 0:
+        out["cpu_baseline"] = batched_cpu_sample(jobs)
+    return out
+
+
+def batched_cpu_sample(jobs, budget_est_tets=12e6):
+    """The reference's OpenMP mesh_adapt on the first jobs of the seeded list
+    (up to budget_est_tets estimated output tets)."""
+    from oracle import oracle as O
+    import omega_h_v1_b200 as G
+    from omega_h_v1_b200 import workloads as W
+    if not O.have_reference():
+        return None
+    lib = O._lib(O.REF_OMP_SO, "refd_").lib
+    lib.refd_adapt_counted.restype = C.c_uint
+    lib.refd_adapt_counted.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_uint,
+                                       C.c_uint, C.POINTER(C.c_uint), C.POINTER(C.c_double)]
+    elems, secs, used, est = 0.0, 0.0, 0, 0.0
+    for j in jobs:
+        if est > budget_est_tets:
+            break
+        est += j.estimated_output_tets()
+        coords, conn, h = W.job_host_input(G, j)
+        m = O.Reference(3, coords, conn)
+        m.derive_model_full()
+        m.add_field(0, "adapt_size", h)
+        p, e = C.c_uint(), C.c_double()
+        with _Quiet():
+            t0 = time.perf_counter()
+            lib.refd_adapt_counted(m.h, SIZE_FLOOR, GOOD_QUAL, NLAYERS, MAX_OPS,
+                                   C.byref(p), C.byref(e))
+            secs += time.perf_counter() - t0
+        m.close()
+        elems += e.value
+        used += 1
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    return {"value": round(elems / secs, 1), "unit": UNIT, "cores": cores,
+            "kind": "reference",
+            "sample": "mesh_adapt of the first %d of the 512 seeded meshes (%.0f tets in "
+                      "over their passes)" % (used, elems)}
+
+
+# ---------------------------------------------------------------------------
 # CPU arms (reference build of the same path)
 
 class _Quiet:
@@ -446,6 +629,10 @@ def main():
                     help="DRAM bytes per launch of that kernel from an ncu capture")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling)")
+    ap.add_argument("--workload", default="box48", choices=["box48", "batched"],
+                    help="box48: the 48^3 radial-size adapt; batched: 512 uneven boxes, "
+                         "plain one-by-one path against adapt_batch")
+    ap.add_argument("--batch-count", type=int, default=512)
     args = ap.parse_args()
     world, rank, local = dist_setup()
     if args.impl == "reference":
@@ -456,7 +643,10 @@ def main():
             import torch.distributed as dist
             dist.destroy_process_group()
         return
-    out = run_ours(args, world, rank, local)
+    if args.workload == "batched":
+        out = run_batched(args, world, rank, local)
+    else:
+        out = run_ours(args, world, rank, local)
     if rank == 0:
         if not args.no_cpu:
             r = cpu_reference_run(1, 1)

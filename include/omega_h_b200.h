@@ -79,6 +79,11 @@ void osh_b200_batch_stats(unsigned* unions, unsigned* steps, unsigned* union_pas
    mesh i of that call: passes that changed it and the elements entering them */
 void osh_b200_batch_mesh_stats(unsigned i, unsigned* passes, double* elems_in) OSH_PUBLIC;
 
+/* order-sensitive 64-bit digest of a mesh (connectivity of every dimension,
+   tag names, kinds and data, global numbers), computed on the device; equal
+   meshes give equal digests. No counterpart in the reference. */
+unsigned long long osh_b200_digest(osh_t m) OSH_PUBLIC;
+
 /* ---- per-stage selections of one pass, without changing the mesh ------ */
 /* Layouts follow refine_by_size / coarsen_common / swap_common: every output
    is a host array sized by the entity counts of the current mesh. */

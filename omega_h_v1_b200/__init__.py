@@ -134,6 +134,7 @@ def lib():
       C.c_uint, C.c_uint, C.c_ulonglong, C.POINTER(C.c_uint), C.POINTER(C.c_int))
     f("osh_b200_batch_stats", None, *([C.POINTER(C.c_uint)] * 4), C.POINTER(C.c_double))
     f("osh_b200_batch_mesh_stats", None, C.c_uint, C.POINTER(C.c_uint), C.POINTER(C.c_double))
+    f("osh_b200_digest", C.c_ulonglong, vp)
     f("osh_b200_launch_count", C.c_ulonglong)
     f("osh_b200_sync_count", C.c_ulonglong)
     f("osh_b200_probe_enable", None, C.c_uint)
@@ -224,6 +225,10 @@ class Mesh:
         h = self.L.osh_b200_clone(self.h)
         self._chk()
         return Mesh(h)
+
+    def digest(self):
+        """Order-sensitive 64-bit hash of every array of the mesh (device)."""
+        return self._chk(self.L.osh_b200_digest(self.h))
 
     def close(self):
         if self.h:

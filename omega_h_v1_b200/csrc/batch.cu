@@ -275,6 +275,11 @@ bool same_tags(Mesh& a, Mesh& b, u32 d)
 
 Mesh* concat_meshes(std::vector<Mesh*> const& ms)
 {
+  return concat_meshes(ms, nullptr);
+}
+
+Mesh* concat_meshes(std::vector<Mesh*> const& ms, cudaStream_t stream)
+{
   if (ms.empty()) throw Failure(E_ARG, "a batch needs at least one mesh");
   Mesh& a = *ms[0];
   u32 nm = (u32)ms.size(), dim = a.dim;
@@ -294,7 +299,7 @@ Mesh* concat_meshes(std::vector<Mesh*> const& ms)
     }
     stream_sync(m->s);
   }
-  Mesh* u = new Mesh(dim, a.full, a.parallel, nullptr);
+  Mesh* u = new Mesh(dim, a.full, a.parallel, stream);
   cudaStream_t s = u->s;
   try {
     Meta meta;
@@ -723,6 +728,89 @@ void adapt_union(Mesh& u, double size_floor, double good_qual, u32 nlayers, u32 
 }
 
 // ---------------------------------------------------------------------------
+// content digest: an order-sensitive 64-bit hash of every array of a mesh
+
+namespace {
+
+__device__ inline u64 mix64(u64 z)
+{
+  z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+  z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+  return z ^ (z >> 31);
+}
+
+// sum over words of mix(word, position, salt); wraps modulo 2^64
+__global__ void k_digest(u64 nwords, u32 const* __restrict__ w, u64 salt, u64* out)
+{
+  u64 acc = 0;
+  for (u64 j = blockIdx.x * (u64)blockDim.x + threadIdx.x; j < nwords;
+       j += (u64)gridDim.x * blockDim.x)
+    acc += mix64(((u64)w[j] << 32) ^ mix64(j + salt));
+  for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(FULL_MASK, acc, o);
+  if ((threadIdx.x & 31) == 0) atomicAdd((unsigned long long*)out, (unsigned long long)acc);
+}
+
+u64 host_mix(u64 z)
+{
+  z += 0x9e3779b97f4a7c15ull;
+  z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+  z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+  return z ^ (z >> 31);
+}
+
+u64 str_hash(std::string const& x)
+{
+  u64 h = 1469598103934665603ull;
+  for (unsigned char c : x) h = (h ^ c) * 1099511628211ull;
+  return h;
+}
+
+}  // namespace
+
+u64 mesh_digest(Mesh& m)
+{
+  cudaStream_t s = m.s;
+  u64* acc = dalloc<u64>(1, s);
+  CK(cudaMemsetAsync(acc, 0, sizeof(u64), s));
+  u64 h = host_mix(m.dim);
+  u64 salt = 0;
+  auto add = [&](void const* p, u64 bytes) {
+    salt = host_mix(salt + 1);
+    u64 nw = bytes / 4;
+    if (nw) {
+      k_digest<<<capped_grid(nw), BLOCK, 0, s>>>(nw, static_cast<u32 const*>(p), salt, acc);
+      CK_LAUNCH();
+    }
+    // a trailing partial word (u8 tags) enters through the host
+    if (bytes % 4) {
+      unsigned char tail[4] = {0, 0, 0, 0};
+      CK(cudaMemcpyAsync(tail, static_cast<unsigned char const*>(p) + nw * 4, bytes % 4,
+          cudaMemcpyDeviceToHost, s));
+      stream_sync(s);
+      u32 t;
+      std::memcpy(&t, tail, 4);
+      h = host_mix(h ^ t ^ salt);
+    }
+  };
+  for (u32 d = 0; d <= m.dim; ++d) {
+    if (!m.has_dim(d)) continue;
+    u32 n = m.count(d);
+    h = host_mix(h ^ (((u64)d << 32) | n));
+    if (d) add(m.ask_down(d, 0), (u64)n * deg(d, 0) * 4);
+    for (Tag const& t : m.tags[d]) {
+      h = host_mix(h ^ str_hash(t.name) ^ ((u64)t.type << 40) ^ ((u64)t.ncomps << 20) ^ t.transfer);
+      add(t.data, (u64)n * t.ncomps * tag_esz(t.type));
+    }
+    if (m.globals[d]) add(m.globals[d], (u64)n * 8);
+  }
+  u64 dev = 0;
+  CK(cudaMemcpyAsync(&dev, acc, sizeof(u64), cudaMemcpyDeviceToHost, s));
+  stream_sync(s);
+  dev_free(acc, s);
+  return host_mix(h ^ dev);
+}
+
+// ---------------------------------------------------------------------------
 // tag lists: which tags a pass leaves on each dimension, and in what order.
 // A union's tag list follows the passes the union ran; each mesh's must
 // follow the passes that changed it, so the split replays those.
@@ -844,7 +932,7 @@ void adapt_batch(std::vector<Mesh*> const& ms, double size_floor, double good_qu
       ++j;
     }
     std::vector<Mesh*> group(ms.begin() + i, ms.begin() + j);
-    Mesh* u = concat_meshes(group);
+    Mesh* u = concat_meshes(group, group[0]->s);
     try {
       Layout start = layout_of(*u);
       std::vector<BatchMeshResult> r;

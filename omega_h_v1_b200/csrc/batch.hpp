@@ -17,6 +17,11 @@ namespace osh {
 // one disjoint union of the meshes, on a stream of its own; every mesh must
 // have the same dimension, representation and tag list
 Mesh* concat_meshes(std::vector<Mesh*> const& ms);
+Mesh* concat_meshes(std::vector<Mesh*> const& ms, cudaStream_t stream);
+
+// order-sensitive 64-bit hash of a mesh's connectivity, tags (names, kinds
+// and data) and global numbers, computed on the device
+u64 mesh_digest(Mesh& m);
 
 // the meshes of a union, in segment order (new Mesh objects on `stream`,
 // or on streams of their own when stream is null)

@@ -525,6 +525,13 @@ int osh_b200_adapt_batch(osh_t* meshes, unsigned n, double sf, double gq, unsign
   API_CATCH(osh::last_error())
 }
 
+unsigned long long osh_b200_digest(osh_t h)
+{
+  API_TRY
+  return osh::mesh_digest(*M(h));
+  API_CATCH(0)
+}
+
 void osh_b200_batch_stats(unsigned* unions, unsigned* steps, unsigned* union_passes,
     unsigned* mesh_passes, double* elems_in)
 {

@@ -1,0 +1,121 @@
+"""Seeded synthetic workloads of the adaptation path (no dataset exists for
+them; every draw comes from a splitmix64 stream of the stated seed).
+
+* batched boxes: `count` box meshes with grid edge n log-uniform in
+  [nmin, nmax] and a uniform target size h drawn in [0.3/n, 1.5/n], each box
+  perturbed by up to 0.1 h0 with its index as the perturbation seed;
+* serving stream: Poisson arrivals of adaptation jobs (rate `rate` per
+  second) whose tet count is log-uniform in [2e3, 2e6] (n = round((tets/6)^(1/3))),
+  half with a uniform size h in [1.0/n, 1.6/n], half with a radial size
+  0.8/n (1 + 4 |x - c|) around a centre drawn in [0.3, 0.7]^3.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass
+
+import numpy as np
+
+MASK = (1 << 64) - 1
+
+
+class SplitMix64:
+    """splitmix64 (Steele, Lea, Flood 2014), uniform doubles from the top 53 bits."""
+
+    def __init__(self, seed: int):
+        self.state = seed & MASK
+
+    def next(self) -> int:
+        self.state = (self.state + 0x9E3779B97F4A7C15) & MASK
+        z = self.state
+        z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & MASK
+        z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & MASK
+        return z ^ (z >> 31)
+
+    def uniform(self) -> float:
+        return (self.next() >> 11) * 2.0 ** -53
+
+
+@dataclass
+class BoxJob:
+    index: int
+    n: int             # grid edge: 6 n^3 tets
+    size: float        # uniform target size h (0 = radial field below)
+    seed: int          # perturbation seed
+    radial: tuple | None = None   # (h0, h1, cx, cy, cz) for h0 + h1 |x - c|
+    arrival: float = 0.0          # seconds from the start of a serving run
+
+    @property
+    def tets(self) -> int:
+        return 6 * self.n ** 3
+
+    def estimated_output_tets(self) -> float:
+        """Rough size after adaptation (fit of mesh_adapt on uniform boxes:
+        about 6.9 / (h n)^3 times the input); used only to plan memory."""
+        if self.radial is None:
+            c = self.size * self.n
+            return self.tets * max(6.9 / c ** 3, 0.5)
+        h0, h1 = self.radial[:2]
+        # mean size over the unit cube is about h0 + 0.5 h1
+        c = (h0 + 0.5 * h1) * self.n
+        return self.tets * max(6.9 / c ** 3, 0.5)
+
+
+def batched_boxes(count=512, seed=1, nmin=4, nmax=40):
+    rng = SplitMix64(seed)
+    out = []
+    lo, hi = math.log(nmin), math.log(nmax)
+    for i in range(count):
+        n = int(round(math.exp(lo + rng.uniform() * (hi - lo))))
+        h = (0.3 + 1.2 * rng.uniform()) / n
+        out.append(BoxJob(i, n, h, i))
+    return out
+
+
+def serving_stream(count=200, seed=2, rate=200.0, tmin=2e3, tmax=2e6):
+    rng = SplitMix64(seed)
+    out = []
+    t = 0.0
+    lo, hi = math.log(tmin), math.log(tmax)
+    for i in range(count):
+        t += -math.log(1.0 - rng.uniform()) / rate
+        tets = math.exp(lo + rng.uniform() * (hi - lo))
+        n = max(2, int(round((tets / 6.0) ** (1.0 / 3.0))))
+        if rng.uniform() < 0.5:
+            h = (1.0 + 0.6 * rng.uniform()) / n
+            out.append(BoxJob(i, n, h, i, None, t))
+        else:
+            c = tuple(0.3 + 0.4 * rng.uniform() for _ in range(3))
+            h0 = 0.8 / n
+            out.append(BoxJob(i, n, 0.0, i, (h0, 4.0 * h0) + c, t))
+    return out
+
+
+def build_job_mesh(G, job: BoxJob, pert=0.1):
+    """The job's classified full-topology box on the current GPU with its
+    adapt_size field (input preparation)."""
+    coords, conn, _ = G.box(job.n, job.seed, pert)
+    m = G.Mesh.reduced(3, coords, conn)
+    m.derive_model_full()
+    nv = coords.size // 3
+    if job.radial is None:
+        h = np.full(nv, job.size)
+    else:
+        h0, h1, cx, cy, cz = job.radial
+        d = coords.reshape(-1, 3) - np.array([cx, cy, cz])
+        h = h0 + h1 * np.sqrt(d[:, 0] * d[:, 0] + d[:, 1] * d[:, 1] + d[:, 2] * d[:, 2])
+    m.add_field(0, "adapt_size", h)
+    return m
+
+
+def job_host_input(G, job: BoxJob, pert=0.1):
+    """Host arrays of the job's input for the CPU checkers: coords, conn, h."""
+    coords, conn, _ = G.box(job.n, job.seed, pert)
+    nv = coords.size // 3
+    if job.radial is None:
+        h = np.full(nv, job.size)
+    else:
+        h0, h1, cx, cy, cz = job.radial
+        d = coords.reshape(-1, 3) - np.array([cx, cy, cz])
+        h = h0 + h1 * np.sqrt(d[:, 0] * d[:, 0] + d[:, 1] * d[:, 1] + d[:, 2] * d[:, 2])
+    return coords, conn, h

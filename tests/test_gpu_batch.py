@@ -63,6 +63,7 @@ def _check_batch(cases, max_union_elems, **extra):
             assert stats["per_mesh"][i][0] == passes, "mesh %d passes" % i
         errs = O.mesh_diff(batch[i].snapshot(), m.snapshot(), rel_tol=REL)
         assert not errs, "mesh %d (%s): %s" % (i, cases[i], errs[:5])
+        assert batch[i].digest() == m.digest(), "mesh %d digest" % i
     return stats
 
 
@@ -121,3 +122,13 @@ def test_batch_rejects_vertex_labels_refinement_would_drop():
         G.adapt_batch([a], *ARGS)
     assert e.value.code == 4
     G.lib().osh_b200_clear_error()
+
+
+def test_digest_tracks_content():
+    a = build_gpu(4, size=0.2, fields=True)
+    b = a.clone()
+    assert a.digest() == b.digest()
+    b.refine_by_size(0.0)
+    assert a.digest() != b.digest()
+    c = build_gpu(4, size=0.2, fields=True, seed=1)
+    assert a.digest() != c.digest()
