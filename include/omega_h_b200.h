@@ -84,6 +84,40 @@ void osh_b200_batch_mesh_stats(unsigned i, unsigned* passes, double* elems_in) O
    meshes give equal digests. No counterpart in the reference. */
 unsigned long long osh_b200_digest(osh_t m) OSH_PUBLIC;
 
+/* ---- serving: continuous batching of adaptation jobs ------------------- */
+/* No counterpart in the reference. A server adapts jobs (a simplex mesh with
+   a vertex size field, given in host memory) with mesh_adapt's parameters.
+   Jobs wait until the device-memory budget (bytes, estimated from each job's
+   size field) admits them; admitted jobs are classified (crease pi/4), join
+   the running batch at the next step and leave it when their pass loop ends,
+   so jobs that arrive while others run share every launch with them. Each
+   result equals what osh_adapt gives the same job alone. Not thread-safe:
+   call one server from one thread. */
+typedef struct osh_b200_server* osh_b200_server_t;
+osh_b200_server_t osh_b200_server_new(double size_ratio_floor, double good_qual,
+    unsigned nsliver_layers, unsigned max_passes,
+    unsigned long long mem_budget_bytes) OSH_PUBLIC;
+void osh_b200_server_free(osh_b200_server_t sv) OSH_PUBLIC;
+/* queue a job (arrays are copied); returns its id, or -1 */
+int osh_b200_server_submit(osh_b200_server_t sv, unsigned dim, unsigned nverts,
+    double const* coords, unsigned nelems, unsigned const* conn,
+    double const* size) OSH_PUBLIC;
+/* admit, run one step over every resident job, retire finished jobs;
+   returns the number of jobs queued or running, or -1 on error */
+int osh_b200_server_step(osh_b200_server_t sv) OSH_PUBLIC;
+/* ids of finished jobs not yet reported (at most max_ids); returns the count */
+unsigned osh_b200_server_poll(osh_b200_server_t sv, unsigned* ids,
+    unsigned max_ids) OSH_PUBLIC;
+/* the adapted mesh of a finished job; the caller frees it with osh_free */
+osh_t osh_b200_server_take(osh_b200_server_t sv, unsigned id) OSH_PUBLIC;
+/* times in seconds since osh_b200_server_new; returns 1 if finished, 0 if
+   not yet, -1 for an unknown id */
+int osh_b200_server_job_info(osh_b200_server_t sv, unsigned id, double* t_submit,
+    double* t_admit, double* t_done, unsigned* passes, double* elems_in,
+    int* status) OSH_PUBLIC;
+void osh_b200_server_stats(osh_b200_server_t sv, unsigned* steps, unsigned* active,
+    unsigned* queued, unsigned long long* reserved_bytes, double* now) OSH_PUBLIC;
+
 /* ---- per-stage selections of one pass, without changing the mesh ------ */
 /* Layouts follow refine_by_size / coarsen_common / swap_common: every output
    is a host array sized by the entity counts of the current mesh. */

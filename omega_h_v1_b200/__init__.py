@@ -135,6 +135,16 @@ def lib():
     f("osh_b200_batch_stats", None, *([C.POINTER(C.c_uint)] * 4), C.POINTER(C.c_double))
     f("osh_b200_batch_mesh_stats", None, C.c_uint, C.POINTER(C.c_uint), C.POINTER(C.c_double))
     f("osh_b200_digest", C.c_ulonglong, vp)
+    f("osh_b200_server_new", vp, C.c_double, C.c_double, C.c_uint, C.c_uint, C.c_ulonglong)
+    f("osh_b200_server_free", None, vp)
+    f("osh_b200_server_submit", C.c_int, vp, C.c_uint, C.c_uint, _f64p, C.c_uint, _u32p, _f64p)
+    f("osh_b200_server_step", C.c_int, vp)
+    f("osh_b200_server_poll", C.c_uint, vp, C.POINTER(C.c_uint), C.c_uint)
+    f("osh_b200_server_take", vp, vp, C.c_uint)
+    f("osh_b200_server_job_info", C.c_int, vp, C.c_uint, *([C.POINTER(C.c_double)] * 3),
+      C.POINTER(C.c_uint), C.POINTER(C.c_double), C.POINTER(C.c_int))
+    f("osh_b200_server_stats", None, vp, *([C.POINTER(C.c_uint)] * 3),
+      C.POINTER(C.c_ulonglong), C.POINTER(C.c_double))
     f("osh_b200_launch_count", C.c_ulonglong)
     f("osh_b200_sync_count", C.c_ulonglong)
     f("osh_b200_probe_enable", None, C.c_uint)
@@ -444,6 +454,75 @@ def adapt_batch(meshes, size_floor, good_qual, nlayers, max_ops, max_union_elems
     stats = dict(unions=u.value, steps=st.value, union_passes=up.value,
                  mesh_passes=mp.value, elems_in=e.value, per_mesh=per)
     return list(changed[:n]), list(status[:n]), stats
+
+
+class Server:
+    """Continuous-batching adaptation server (osh_b200_server_*): jobs are
+    host arrays (coords, element connectivity, vertex size field)."""
+
+    def __init__(self, size_floor, good_qual, nlayers, max_ops, budget_bytes):
+        self.L = lib()
+        self.h = self.L.osh_b200_server_new(size_floor, good_qual, nlayers, max_ops,
+                                            int(budget_bytes))
+        if not self.h:
+            check()
+
+    def submit(self, coords, conn, size, dim=3):
+        coords = np.ascontiguousarray(coords, dtype=np.float64).ravel()
+        conn = np.ascontiguousarray(conn, dtype=np.uint32).ravel()
+        size = np.ascontiguousarray(size, dtype=np.float64).ravel()
+        r = self.L.osh_b200_server_submit(self.h, dim, coords.size // 3, coords,
+                                          conn.size // (dim + 1), conn, size)
+        if r < 0:
+            check()
+        return r
+
+    def step(self):
+        r = self.L.osh_b200_server_step(self.h)
+        if r < 0:
+            check()
+        return r
+
+    def poll(self, max_ids=4096):
+        ids = (C.c_uint * max_ids)()
+        n = self.L.osh_b200_server_poll(self.h, ids, max_ids)
+        check()
+        return list(ids[:n])
+
+    def take(self, job):
+        h = self.L.osh_b200_server_take(self.h, job)
+        check()
+        return Mesh(h)
+
+    def job_info(self, job):
+        ts, ta, td, e = (C.c_double() for _ in range(4))
+        p, st = C.c_uint(), C.c_int()
+        r = self.L.osh_b200_server_job_info(self.h, job, C.byref(ts), C.byref(ta),
+                                            C.byref(td), C.byref(p), C.byref(e), C.byref(st))
+        if r < 0:
+            check()
+        return dict(finished=bool(r), t_submit=ts.value, t_admit=ta.value, t_done=td.value,
+                    passes=p.value, elems_in=e.value, status=st.value)
+
+    def stats(self):
+        steps, active, queued = C.c_uint(), C.c_uint(), C.c_uint()
+        res, now = C.c_ulonglong(), C.c_double()
+        self.L.osh_b200_server_stats(self.h, C.byref(steps), C.byref(active), C.byref(queued),
+                                     C.byref(res), C.byref(now))
+        check()
+        return dict(steps=steps.value, active=active.value, queued=queued.value,
+                    reserved=res.value, now=now.value)
+
+    def close(self):
+        if self.h:
+            self.L.osh_b200_server_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def new_box_mesh(n, seed=0, pert=0.1, size=None, radial=None, parallel=False):

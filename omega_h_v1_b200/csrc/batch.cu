@@ -60,11 +60,17 @@ __global__ void k_concat(u32 nm, T const* const* __restrict__ src, u32 const* __
   }
 }
 
-__global__ void k_seg_fill(u32 nm, u32 const* __restrict__ offs, u32* __restrict__ out)
+// segment of every vertex of the union: the input's index, or, for an input
+// that is itself a union, its own segment shifted by the segments before it
+__global__ void k_seg_concat(u32 nm, u32 const* __restrict__ offs,
+    u32 const* const* __restrict__ src, u32 const* __restrict__ base, u32* __restrict__ out)
 {
   u32 total = offs[nm];
-  for (u32 j = blockIdx.x * blockDim.x + threadIdx.x; j < total; j += gridDim.x * blockDim.x)
-    out[j] = find_seg(nm, offs, j);
+  for (u32 j = blockIdx.x * blockDim.x + threadIdx.x; j < total; j += gridDim.x * blockDim.x) {
+    u32 k = find_seg(nm, offs, j);
+    u32 const* sk = src[k];
+    out[j] = base[k] + (sk ? sk[j - offs[k]] : 0u);
+  }
 }
 
 // segment of every entity: that of its first vertex
@@ -258,15 +264,15 @@ void launch_scatter(u32 n, u32 width, void const* in, u32 const* es, u32 const* 
   CK_LAUNCH();
 }
 
+// the same tags (names, types, widths) on dimension d, in any order; the
+// transfer kind may differ (refinement resets it on vertex fields), each
+// mesh's own is restored when it leaves the union
 bool same_tags(Mesh& a, Mesh& b, u32 d)
 {
   if (a.tags[d].size() != b.tags[d].size()) return false;
-  for (size_t i = 0; i < a.tags[d].size(); ++i) {
-    Tag const& x = a.tags[d][i];
-    Tag const& y = b.tags[d][i];
-    if (x.name != y.name || x.type != y.type || x.ncomps != y.ncomps ||
-        x.transfer != y.transfer)
-      return false;
+  for (Tag const& x : a.tags[d]) {
+    Tag const* y = b.find_tag(d, x.name.c_str());
+    if (!y || x.type != y->type || x.ncomps != y->ncomps) return false;
   }
   return true;
 }
@@ -330,7 +336,7 @@ Mesh* concat_meshes(std::vector<Mesh*> const& ms, cudaStream_t stream)
         conn_at[d] = meta.add(p.data(), nm);
       }
       for (size_t t = 0; t < a.tags[d].size(); ++t) {
-        for (u32 k = 0; k < nm; ++k) p[k] = ms[k]->tags[d][t].data;
+        for (u32 k = 0; k < nm; ++k) p[k] = ms[k]->find_tag(d, a.tags[d][t].name.c_str())->data;
         tag_at[d].push_back(meta.add(p.data(), nm));
       }
       if (a.parallel && a.globals[d]) {
@@ -338,6 +344,14 @@ Mesh* concat_meshes(std::vector<Mesh*> const& ms, cudaStream_t stream)
         glob_at[d] = meta.add(p.data(), nm);
       }
     }
+    // segments: one per plain input, all of an input union's
+    std::vector<u32> segbase(nm + 1, 0);
+    for (u32 k = 0; k < nm; ++k) {
+      p[k] = ms[k]->seg;
+      segbase[k + 1] = segbase[k] + (ms[k]->seg ? ms[k]->nseg : 1u);
+    }
+    size_t segsrc_at = meta.add(p.data(), nm);
+    size_t segbase_at = meta.add_u32(segbase.data(), nm + 1);
     meta.upload(s);
     for (u32 d = 0; d <= dim; ++d) {
       if (!a.has_dim(d)) continue;
@@ -373,11 +387,12 @@ Mesh* concat_meshes(std::vector<Mesh*> const& ms, cudaStream_t stream)
         u->set_globals(d, g);
       }
     }
-    u->nseg = nm;
+    u->nseg = segbase[nm];
     u32 nv = offs[0][nm];
     u->seg = dalloc<u32>(nv, s);
     if (nv) {
-      k_seg_fill<<<capped_grid(nv), BLOCK, 0, s>>>(nm, meta.at<u32 const>(offs_at[0]), u->seg);
+      k_seg_concat<<<capped_grid(nv), BLOCK, 0, s>>>(nm, meta.at<u32 const>(offs_at[0]),
+          meta.at<u32 const* const>(segsrc_at), meta.at<u32 const>(segbase_at), u->seg);
       CK_LAUNCH();
     }
     dev_free(meta.dev, s);
@@ -531,181 +546,178 @@ std::vector<Mesh*> split_union(Mesh& u, cudaStream_t stream)
 
 namespace {
 
-enum : u32 { ST_REFINE, ST_COARSEN, ST_SHAPE, ST_DONE, ST_FAILED };
-enum : u32 { OP_REFINE, OP_COARSEN, OP_SWAP, OP_CSLIVERS };
+__global__ void k_seg_min_quality(u32 n, double const* __restrict__ q,
+    u32 const* __restrict__ voe, u32 vpe, u32 const* __restrict__ seg,
+    unsigned long long* __restrict__ out);
+__global__ void k_seg_count(u32 n, u32 const* __restrict__ voe, u32 vpe,
+    u32 const* __restrict__ seg, u32* __restrict__ out);
 
-struct UnionCtl {
-  Mesh& u;
-  u32 nm;
-  u32* active = nullptr;          // device
-  double* floor = nullptr;        // device
-  u32* selected = nullptr;        // device
-  u32* elems = nullptr;           // device
-  unsigned long long* minkey = nullptr;  // device
-  u32* h_u32 = nullptr;           // pinned: selected[nm], elems[nm]
-  unsigned long long* h_key = nullptr;   // pinned: minkey[nm]
-  SegCtl ctl;
+}  // namespace
 
-  explicit UnionCtl(Mesh& m) : u(m), nm(m.nseg)
-  {
-    cudaStream_t s = u.s;
-    active = dalloc<u32>(nm, s);
-    floor = dalloc<double>(nm, s);
-    selected = dalloc<u32>(nm, s);
-    elems = dalloc<u32>(nm, s);
-    minkey = dalloc<unsigned long long>(nm, s);
-    CK(cudaMallocHost(&h_u32, sizeof(u32) * 2 * nm));
-    CK(cudaMallocHost(&h_key, sizeof(unsigned long long) * nm));
+UnionCtl::UnionCtl(Mesh& m) : u(m), nm(m.nseg)
+{
+  cudaStream_t s = u.s;
+  active = dalloc<u32>(nm, s);
+  floor = dalloc<double>(nm, s);
+  selected = dalloc<u32>(nm, s);
+  elems = dalloc<u32>(nm, s);
+  minkey = dalloc<unsigned long long>(nm, s);
+  CK(cudaMallocHost(&h_u32, sizeof(u32) * 2 * nm));
+  CK(cudaMallocHost(&h_key, sizeof(unsigned long long) * nm));
+}
+
+UnionCtl::~UnionCtl()
+{
+  cudaStream_t s = u.s;
+  u.ctl = nullptr;
+  cudaStreamSynchronize(s);
+  dev_free(active, s);
+  dev_free(floor, s);
+  dev_free(selected, s);
+  dev_free(elems, s);
+  dev_free(minkey, s);
+  cudaFreeHost(h_u32);
+  cudaFreeHost(h_key);
+}
+
+std::vector<double> UnionCtl::min_quality()
+{
+  cudaStream_t s = u.s;
+  u32 ne = u.count(u.dim);
+  double const* q = u.qualities();
+  CK(cudaMemsetAsync(minkey, 0xff, sizeof(unsigned long long) * nm, s));
+  if (ne) {
+    k_seg_min_quality<<<grid_for(ne), BLOCK, 0, s>>>(ne, q, u.ask_down(u.dim, 0),
+        deg(u.dim, 0), u.seg, minkey);
+    CK_LAUNCH();
   }
-  ~UnionCtl()
-  {
-    cudaStream_t s = u.s;
-    u.ctl = nullptr;
-    cudaStreamSynchronize(s);
-    dev_free(active, s);
-    dev_free(floor, s);
-    dev_free(selected, s);
-    dev_free(elems, s);
-    dev_free(minkey, s);
-    cudaFreeHost(h_u32);
-    cudaFreeHost(h_key);
-  }
+  CK(cudaMemcpyAsync(h_key, minkey, sizeof(unsigned long long) * nm, cudaMemcpyDeviceToHost, s));
+  stream_sync(s);
+  std::vector<double> r(nm);
+  for (u32 k = 0; k < nm; ++k) r[k] = h_key[k] == ~0ull ? DBL_MAX : from_order_key(h_key[k]);
+  return r;
+}
 
-  // per-segment minimum element quality (mesh_min_quality of each mesh)
-  std::vector<double> min_quality()
-  {
-    cudaStream_t s = u.s;
-    u32 ne = u.count(u.dim);
-    double const* q = u.qualities();
-    CK(cudaMemsetAsync(minkey, 0xff, sizeof(unsigned long long) * nm, s));
-    if (ne) {
-      k_seg_min_quality<<<grid_for(ne), BLOCK, 0, s>>>(ne, q, u.ask_down(u.dim, 0),
-          deg(u.dim, 0), u.seg, minkey);
-      CK_LAUNCH();
-    }
-    CK(cudaMemcpyAsync(h_key, minkey, sizeof(unsigned long long) * nm, cudaMemcpyDeviceToHost, s));
-    stream_sync(s);
-    std::vector<double> r(nm);
-    for (u32 k = 0; k < nm; ++k) r[k] = h_key[k] == ~0ull ? DBL_MAX : from_order_key(h_key[k]);
-    return r;
+void UnionCtl::run(u32 op, std::vector<u32> const& group, std::vector<double> const& floors,
+    double size_floor, double good_qual, u32 nlayers)
+{
+  cudaStream_t s = u.s;
+  std::vector<u32> act(nm, 0);
+  for (u32 k : group) act[k] = 1;
+  CK(cudaMemcpyAsync(active, act.data(), sizeof(u32) * nm, cudaMemcpyHostToDevice, s));
+  bool with_floor = op == OP_REFINE || op == OP_COARSEN;
+  if (with_floor)
+    CK(cudaMemcpyAsync(floor, floors.data(), sizeof(double) * nm, cudaMemcpyHostToDevice, s));
+  CK(cudaMemsetAsync(selected, 0, sizeof(u32) * nm, s));
+  CK(cudaMemsetAsync(elems, 0, sizeof(u32) * nm, s));
+  u32 ne = u.count(u.dim);
+  if (ne) {
+    k_seg_count<<<grid_for(ne), BLOCK, 0, s>>>(ne, u.ask_down(u.dim, 0), deg(u.dim, 0), u.seg,
+        elems);
+    CK_LAUNCH();
   }
-
-  // one pass over the union acting on `group`; returns per-segment selected
-  // counts in h_u32[0..nm) and elements entering the pass in h_u32[nm..2nm)
-  void run(u32 op, std::vector<u32> const& group, std::vector<double> const& floors,
-      double size_floor, double good_qual, u32 nlayers)
-  {
-    cudaStream_t s = u.s;
-    std::vector<u32> act(nm, 0);
-    for (u32 k : group) act[k] = 1;
-    CK(cudaMemcpyAsync(active, act.data(), sizeof(u32) * nm, cudaMemcpyHostToDevice, s));
-    bool with_floor = op == OP_REFINE || op == OP_COARSEN;
-    if (with_floor)
-      CK(cudaMemcpyAsync(floor, floors.data(), sizeof(double) * nm, cudaMemcpyHostToDevice, s));
-    CK(cudaMemsetAsync(selected, 0, sizeof(u32) * nm, s));
-    CK(cudaMemsetAsync(elems, 0, sizeof(u32) * nm, s));
-    u32 ne = u.count(u.dim);
-    if (ne) {
-      k_seg_count<<<grid_for(ne), BLOCK, 0, s>>>(ne, u.ask_down(u.dim, 0), deg(u.dim, 0), u.seg,
-          elems);
-      CK_LAUNCH();
-    }
-    ctl.active = active;
-    ctl.floor = with_floor ? floor : nullptr;
-    ctl.selected = selected;
-    u.ctl = &ctl;
+  ctl.active = active;
+  ctl.floor = with_floor ? floor : nullptr;
+  ctl.selected = selected;
+  u.ctl = &ctl;
+  try {
     switch (op) {
       case OP_REFINE: refine_by_size(u, 0.0); break;
       case OP_COARSEN: coarsen_by_size(u, 0.0, size_floor); break;
       case OP_SWAP: swap_slivers(u, good_qual, nlayers); break;
       default: coarsen_slivers(u, good_qual, nlayers); break;
     }
+  } catch (...) {
     u.ctl = nullptr;
-    CK(cudaMemcpyAsync(h_u32, selected, sizeof(u32) * nm, cudaMemcpyDeviceToHost, s));
-    CK(cudaMemcpyAsync(h_u32 + nm, elems, sizeof(u32) * nm, cudaMemcpyDeviceToHost, s));
-    stream_sync(s);
-    last_batch_stats().union_passes += 1;
+    throw;
   }
-};
+  u.ctl = nullptr;
+  CK(cudaMemcpyAsync(h_u32, selected, sizeof(u32) * nm, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(h_u32 + nm, elems, sizeof(u32) * nm, cudaMemcpyDeviceToHost, s));
+  stream_sync(s);
+  last_batch_stats().union_passes += 1;
+}
 
-}  // namespace
-
-void adapt_union(Mesh& u, double size_floor, double good_qual, u32 nlayers, u32 max_ops,
-    std::vector<BatchMeshResult>& res)
+bool union_step(UnionCtl& c, std::vector<SegState>& st, AdaptParams const& ap)
 {
-  u32 nm = u.nseg;
-  res.assign(nm, BatchMeshResult());
-  if (!nm) return;
+  Mesh& u = c.u;
+  u32 nm = c.nm;
   BatchStats& bs = last_batch_stats();
-  bs.unions += 1;
-  UnionCtl c(u);
-  std::vector<u32> state(nm, ST_REFINE), ops(nm, 0);
-  // satisfy_size's floor (adapt.cpp:47-52), one per mesh
-  std::vector<double> qf = c.min_quality();
-  for (u32 k = 0; k < nm; ++k)
-    if (good_qual < qf[k]) qf[k] = good_qual;
-  // incr_op_count (adapt.cpp:36-45) for mesh k after a pass that changed it
+  bool live = false;
+  for (u32 k = 0; k < nm; ++k) live = live || st[k].state < ST_DONE;
+  if (!live) return false;
+  bs.steps += 1;
+  // satisfy_size's floor (adapt.cpp:47-52), once per mesh on its first step
+  bool fresh = false;
+  for (u32 k = 0; k < nm; ++k) fresh = fresh || st[k].state == ST_INIT;
+  if (fresh) {
+    std::vector<double> mq = c.min_quality();
+    for (u32 k = 0; k < nm; ++k)
+      if (st[k].state == ST_INIT) {
+        st[k].qf = mq[k];
+        if (ap.good_qual < st[k].qf) st[k].qf = ap.good_qual;
+        st[k].state = ST_REFINE;
+      }
+  }
+  std::vector<double> qf(nm);
+  for (u32 k = 0; k < nm; ++k) qf[k] = st[k].qf;
   u32 cur_op = 0;
+  // incr_op_count (adapt.cpp:36-45) for mesh k after a pass that changed it
   auto counted = [&](u32 k) {
-    res[k].ops.push_back(cur_op);
-    res[k].passes += 1;
-    res[k].elems_in += c.h_u32[nm + k];
+    BatchMeshResult& r = st[k].res;
+    r.ops.push_back(cur_op);
+    r.passes += 1;
+    r.elems_in += c.h_u32[nm + k];
     bs.mesh_passes += 1;
     bs.elems_in += c.h_u32[nm + k];
-    if (ops[k] > max_ops) {
-      res[k].status = E_MAXOPS;
-      state[k] = ST_FAILED;
-      return false;
+    if (st[k].ops > ap.max_ops) {
+      r.status = E_MAXOPS;
+      st[k].state = ST_FAILED;
+      return;
     }
-    ++ops[k];
-    return true;
+    ++st[k].ops;
   };
-  auto members = [&](u32 st) {
+  auto members = [&](u32 state) {
     std::vector<u32> g;
     for (u32 k = 0; k < nm; ++k)
-      if (state[k] == st) g.push_back(k);
+      if (st[k].state == state) g.push_back(k);
     return g;
   };
-  for (;;) {
-    bool live = false;
-    for (u32 k = 0; k < nm; ++k) live = live || state[k] < ST_DONE;
-    if (!live) break;
-    bs.steps += 1;
-    // satisfy_size: refine while it changes the mesh, then coarsen
-    std::vector<u32> g = members(ST_REFINE);
-    if (!g.empty()) {
-      cur_op = OP_REFINE;
-      c.run(OP_REFINE, g, qf, size_floor, good_qual, nlayers);
-      for (u32 k : g)
-        if (c.h_u32[k])
-          counted(k);
-        else
-          state[k] = ST_COARSEN;
-    }
-    g = members(ST_COARSEN);
-    if (!g.empty()) {
-      cur_op = OP_COARSEN;
-      c.run(OP_COARSEN, g, qf, size_floor, good_qual, nlayers);
-      for (u32 k : g)
-        if (c.h_u32[k])
-          counted(k);
-        else
-          state[k] = ST_SHAPE;
-    }
-    // satisfy_shape (adapt.cpp:58-80): swap, else collapse slivers
-    g = members(ST_SHAPE);
-    if (g.empty()) continue;
+  // satisfy_size: refine while it changes the mesh, then coarsen
+  std::vector<u32> g = members(ST_REFINE);
+  if (!g.empty()) {
+    cur_op = OP_REFINE;
+    c.run(OP_REFINE, g, qf, ap.size_floor, ap.good_qual, ap.nlayers);
+    for (u32 k : g)
+      if (c.h_u32[k])
+        counted(k);
+      else
+        st[k].state = ST_COARSEN;
+  }
+  g = members(ST_COARSEN);
+  if (!g.empty()) {
+    cur_op = OP_COARSEN;
+    c.run(OP_COARSEN, g, qf, ap.size_floor, ap.good_qual, ap.nlayers);
+    for (u32 k : g)
+      if (c.h_u32[k])
+        counted(k);
+      else
+        st[k].state = ST_SHAPE;
+  }
+  // satisfy_shape (adapt.cpp:58-80): swap, else collapse slivers
+  g = members(ST_SHAPE);
+  if (!g.empty()) {
     std::vector<double> mq = c.min_quality();
     std::vector<u32> g2;
     for (u32 k : g)
-      if (mq[k] >= good_qual)
-        state[k] = ST_DONE;
+      if (mq[k] >= ap.good_qual)
+        st[k].state = ST_DONE;
       else
         g2.push_back(k);
     std::vector<u32> g3;
     if (u.dim == 3 && !g2.empty()) {
       cur_op = OP_SWAP;
-      c.run(OP_SWAP, g2, qf, size_floor, good_qual, nlayers);
+      c.run(OP_SWAP, g2, qf, ap.size_floor, ap.good_qual, ap.nlayers);
       for (u32 k : g2)
         if (c.h_u32[k])
           counted(k);
@@ -716,15 +728,33 @@ void adapt_union(Mesh& u, double size_floor, double good_qual, u32 nlayers, u32 
     }
     if (!g3.empty()) {
       cur_op = OP_CSLIVERS;
-      c.run(OP_CSLIVERS, g3, qf, size_floor, good_qual, nlayers);
+      c.run(OP_CSLIVERS, g3, qf, ap.size_floor, ap.good_qual, ap.nlayers);
       for (u32 k : g3)
         if (c.h_u32[k])
           counted(k);
         else
-          state[k] = ST_DONE;  // shape quality could not be satisfied
+          st[k].state = ST_DONE;  // shape quality could not be satisfied
     }
   }
-  for (u32 k = 0; k < nm; ++k) res[k].changed = ops[k] > 0 || res[k].passes > 0;
+  for (u32 k = 0; k < nm; ++k) st[k].res.changed = st[k].res.passes > 0;
+  live = false;
+  for (u32 k = 0; k < nm; ++k) live = live || st[k].state < ST_DONE;
+  return live;
+}
+
+void adapt_union(Mesh& u, double size_floor, double good_qual, u32 nlayers, u32 max_ops,
+    std::vector<BatchMeshResult>& res)
+{
+  u32 nm = u.nseg;
+  res.assign(nm, BatchMeshResult());
+  if (!nm) return;
+  last_batch_stats().unions += 1;
+  UnionCtl c(u);
+  std::vector<SegState> st(nm);
+  AdaptParams ap{size_floor, good_qual, nlayers, max_ops};
+  while (union_step(c, st, ap)) {
+  }
+  for (u32 k = 0; k < nm; ++k) res[k] = st[k].res;
 }
 
 // ---------------------------------------------------------------------------
@@ -817,9 +847,14 @@ u64 mesh_digest(Mesh& m)
 
 namespace {
 
-struct Layout {
-  std::vector<Tag> tags[4];  // name, type, ncomps, transfer (data unused)
-};
+Tag const* find_in(std::vector<Tag> const& v, char const* name)
+{
+  for (Tag const& t : v)
+    if (t.name == name) return &t;
+  return nullptr;
+}
+
+}  // namespace
 
 Layout layout_of(Mesh& m)
 {
@@ -831,13 +866,6 @@ Layout layout_of(Mesh& m)
       l.tags[d].push_back(x);
     }
   return l;
-}
-
-Tag const* find_in(std::vector<Tag> const& v, char const* name)
-{
-  for (Tag const& t : v)
-    if (t.name == name) return &t;
-  return nullptr;
 }
 
 // the tag lists refine_build, coarsen_build and swap_build produce
@@ -865,7 +893,11 @@ Layout layout_after(u32 op, Layout const& in, u32 dim)
   // collapses and swaps keep every vertex tag in place
   if (op == OP_REFINE) {
     for (Tag const& t : in.tags[0])
-      if (t.type == T_F64) out.tags[0].push_back(t);
+      if (t.type == T_F64) {
+        Tag x = t;
+        x.transfer = X_NOT;  // refine_build re-adds vertex fields untransferred
+        out.tags[0].push_back(x);
+      }
     for (Tag const& t : class_of(0)) out.tags[0].push_back(t);
   } else {
     out.tags[0] = in.tags[0];
@@ -905,14 +937,13 @@ void apply_layout(Mesh& m, Layout const& want)
       Tag* t = m.find_tag(d, w.name.c_str());
       if (!t) throw Failure(E_ARG, "batched mesh lost tag " + w.name);
       next.push_back(*t);
+      next.back().transfer = w.transfer;
       t->data = nullptr;
     }
     for (Tag& t : m.tags[d]) dev_free(t.data, m.s);
     m.tags[d].swap(next);
   }
 }
-
-}  // namespace
 
 void adapt_batch(std::vector<Mesh*> const& ms, double size_floor, double good_qual,
     u32 nlayers, u32 max_ops, unsigned long long max_union_elems,

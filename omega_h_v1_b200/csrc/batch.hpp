@@ -44,6 +44,65 @@ struct BatchStats {
 };
 BatchStats& last_batch_stats();
 
+// mesh_adapt's pass loop (adapt.cpp:47-94) for every segment of a union,
+// one scheduling step at a time: each step runs at most one refine pass, one
+// coarsen pass and one shape step (swap, else collapse slivers) over the whole
+// union, each acting on the segments that are at that point of their loop.
+enum : u32 { ST_INIT, ST_REFINE, ST_COARSEN, ST_SHAPE, ST_DONE, ST_FAILED };
+enum : u32 { OP_REFINE, OP_COARSEN, OP_SWAP, OP_CSLIVERS };
+
+struct AdaptParams {
+  double size_floor;
+  double good_qual;
+  u32 nlayers;
+  u32 max_ops;
+};
+
+struct SegState {
+  u32 state = ST_INIT;
+  u32 ops = 0;
+  double qf = 0;          // satisfy_size's quality floor
+  BatchMeshResult res;
+};
+
+// per-segment control arrays of a union and the host copies of their results
+struct UnionCtl {
+  Mesh& u;
+  u32 nm;
+  u32* active = nullptr;                 // device
+  double* floor = nullptr;               // device
+  u32* selected = nullptr;               // device
+  u32* elems = nullptr;                  // device
+  unsigned long long* minkey = nullptr;  // device
+  u32* h_u32 = nullptr;                  // pinned: selected[nm], elems[nm]
+  unsigned long long* h_key = nullptr;   // pinned: minkey[nm]
+  SegCtl ctl;
+
+  explicit UnionCtl(Mesh& m);
+  ~UnionCtl();
+  UnionCtl(UnionCtl const&) = delete;
+  UnionCtl& operator=(UnionCtl const&) = delete;
+  // mesh_min_quality of every segment
+  std::vector<double> min_quality();
+  // one pass over the union acting on `group`: per-segment selected counts
+  // land in h_u32[0..nm), elements entering the pass in h_u32[nm..2nm)
+  void run(u32 op, std::vector<u32> const& group, std::vector<double> const& floors,
+      double size_floor, double good_qual, u32 nlayers);
+};
+
+// one step for every live segment; returns whether any is still live
+bool union_step(UnionCtl& c, std::vector<SegState>& st, AdaptParams const& ap);
+
+// the tag list a mesh has after the passes `ops` (refine_build, coarsen_build
+// and swap_build keep, drop and order tags by fixed rules), applied to a mesh
+// split out of a union
+struct Layout {
+  std::vector<Tag> tags[4];  // name, type, ncomps, transfer (data unused)
+};
+Layout layout_of(Mesh& m);
+Layout layout_after(u32 op, Layout const& in, u32 dim);
+void apply_layout(Mesh& m, Layout const& want);
+
 // mesh_adapt of every segment of the union (in place)
 void adapt_union(Mesh& u, double size_floor, double good_qual, u32 nlayers, u32 max_ops,
     std::vector<BatchMeshResult>& res);

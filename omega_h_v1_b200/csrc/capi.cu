@@ -9,6 +9,7 @@
 #include "../../include/omega_h.h"
 #include "../../include/omega_h_b200.h"
 #include "batch.hpp"
+#include "serve.hpp"
 #include "passes.hpp"
 
 using osh::Failure;
@@ -523,6 +524,91 @@ int osh_b200_adapt_batch(osh_t* meshes, unsigned n, double sf, double gq, unsign
   }
   return 0;
   API_CATCH(osh::last_error())
+}
+
+#define SV(h) reinterpret_cast<osh::Server*>(h)
+
+osh_b200_server_t osh_b200_server_new(double sf, double gq, unsigned nl, unsigned mo,
+    unsigned long long budget)
+{
+  API_TRY
+  osh::AdaptParams ap{sf, gq, nl, mo};
+  return reinterpret_cast<osh_b200_server_t>(osh::server_new(ap, budget));
+  API_CATCH(nullptr)
+}
+
+void osh_b200_server_free(osh_b200_server_t sv)
+{
+  API_TRY
+  osh::server_free(SV(sv));
+  API_CATCH_VOID
+}
+
+int osh_b200_server_submit(osh_b200_server_t sv, unsigned dim, unsigned nverts,
+    double const* coords, unsigned nelems, unsigned const* conn, double const* size)
+{
+  API_TRY
+  need(sv != nullptr, "server is NULL");
+  return (int)osh::server_submit(SV(sv), dim, nverts, coords, nelems, conn, size);
+  API_CATCH(-1)
+}
+
+int osh_b200_server_step(osh_b200_server_t sv)
+{
+  API_TRY
+  need(sv != nullptr, "server is NULL");
+  u32 r = osh::server_step(SV(sv));
+  osh::check_device_timeouts(nullptr);
+  return (int)r;
+  API_CATCH(-1)
+}
+
+unsigned osh_b200_server_poll(osh_b200_server_t sv, unsigned* ids, unsigned max_ids)
+{
+  API_TRY
+  need(sv != nullptr, "server is NULL");
+  std::vector<u32> r = osh::server_poll(SV(sv), ids ? max_ids : 0);
+  for (size_t i = 0; i < r.size(); ++i) ids[i] = r[i];
+  return (unsigned)r.size();
+  API_CATCH(0)
+}
+
+osh_t osh_b200_server_take(osh_b200_server_t sv, unsigned id)
+{
+  API_TRY
+  need(sv != nullptr, "server is NULL");
+  return reinterpret_cast<osh_t>(osh::server_take(SV(sv), id));
+  API_CATCH(nullptr)
+}
+
+int osh_b200_server_job_info(osh_b200_server_t sv, unsigned id, double* t_submit,
+    double* t_admit, double* t_done, unsigned* passes, double* elems_in, int* status)
+{
+  API_TRY
+  need(sv != nullptr, "server is NULL");
+  osh::ServeJobInfo r = osh::server_job_info(SV(sv), id);
+  if (t_submit) *t_submit = r.t_submit;
+  if (t_admit) *t_admit = r.t_admit;
+  if (t_done) *t_done = r.t_done;
+  if (passes) *passes = r.passes;
+  if (elems_in) *elems_in = r.elems_in;
+  if (status) *status = r.status;
+  return r.finished ? 1 : 0;
+  API_CATCH(-1)
+}
+
+void osh_b200_server_stats(osh_b200_server_t sv, unsigned* steps, unsigned* active,
+    unsigned* queued, unsigned long long* reserved, double* now)
+{
+  API_TRY
+  need(sv != nullptr, "server is NULL");
+  osh::ServeStats r = osh::server_stats(SV(sv));
+  if (steps) *steps = r.steps;
+  if (active) *active = r.active;
+  if (queued) *queued = r.queued;
+  if (reserved) *reserved = r.reserved;
+  if (now) *now = r.now;
+  API_CATCH_VOID
 }
 
 unsigned long long osh_b200_digest(osh_t h)

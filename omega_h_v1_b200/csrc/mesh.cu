@@ -104,6 +104,16 @@ Mesh* Mesh::clone()
   return c;
 }
 
+void Mesh::own_new_stream()
+{
+  stream_sync(s);
+  if (own_stream) return;
+  CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  own_stream = true;
+  mb = std::shared_ptr<Mailbox>(new Mailbox(), release_mailbox);
+  mb->init(s);
+}
+
 void Mesh::use_stream(cudaStream_t stream)
 {
   stream_sync(s);

@@ -107,6 +107,8 @@ struct Mesh {
   Mesh* clone();
   // run all further work of this mesh on `stream` (not owned)
   void use_stream(cudaStream_t stream);
+  // a stream and a mailbox of its own (for a mesh handed out of a batch)
+  void own_new_stream();
   // replace every array of this mesh with those of `with` (which is deleted);
   // overwrite_mesh (mesh.cpp:329-334)
   void overwrite(Mesh* with);

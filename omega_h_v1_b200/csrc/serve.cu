@@ -1,0 +1,303 @@
+// Serving: a request loop over the batched union (batch.hpp) with continuous
+// batching. Jobs (a tet mesh and its vertex size field, in host memory) wait
+// in a queue until the device-memory budget admits them; an admitted job is
+// classified (mesh_derive_model, crease pi/4), joins the running union at the
+// next step boundary and takes its own place in mesh_adapt's pass loop; a job
+// whose loop ends is split out of the union at that step's end and handed
+// back, while the others keep running. Every step is one launch sequence for
+// all resident jobs, so jobs that arrive while others run share their passes.
+#include <chrono>
+#include <cmath>
+#include <deque>
+#include <map>
+#include <memory>
+
+#include "batch.hpp"
+#include "serve.hpp"
+
+namespace osh {
+
+namespace {
+
+double now_s()
+{
+  using namespace std::chrono;
+  return duration<double>(steady_clock::now().time_since_epoch()).count();
+}
+
+// elements an adapted mesh will hold, from the size field: sum over elements
+// of volume / (volume of the regular element whose edge is the mean size)
+double estimate_elements(u32 dim, u32 nv, double const* x, u32 ne, u32 const* conn,
+    double const* h)
+{
+  double sum = 0;
+  u32 vpe = dim + 1;
+  for (u32 i = 0; i < ne; ++i) {
+    u32 const* c = conn + (size_t)i * vpe;
+    double hm = 0;
+    for (u32 j = 0; j < vpe; ++j) hm += h[c[j]];
+    hm /= vpe;
+    double a[3], b[3], d[3];
+    for (u32 k = 0; k < 3; ++k) {
+      a[k] = x[c[1] * 3 + k] - x[c[0] * 3 + k];
+      b[k] = x[c[2] * 3 + k] - x[c[0] * 3 + k];
+      d[k] = dim == 3 ? x[c[3] * 3 + k] - x[c[0] * 3 + k] : 0.0;
+    }
+    double cr[3] = {a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2],
+        a[0] * b[1] - a[1] * b[0]};
+    double meas, ideal;
+    if (dim == 3) {
+      meas = std::fabs(cr[0] * d[0] + cr[1] * d[1] + cr[2] * d[2]) / 6.0;
+      ideal = hm * hm * hm / (6.0 * std::sqrt(2.0));
+    } else {
+      meas = std::sqrt(cr[0] * cr[0] + cr[1] * cr[1] + cr[2] * cr[2]) / 2.0;
+      ideal = hm * hm * std::sqrt(3.0) / 4.0;
+    }
+    if (ideal > 0) sum += meas / ideal;
+  }
+  (void)nv;
+  return sum;
+}
+
+}  // namespace
+
+struct ServeJob {
+  u32 id = 0;
+  u32 dim = 3, nverts = 0, nelems = 0;
+  std::vector<double> coords, size;
+  std::vector<u32> conn;
+  unsigned long long est_bytes = 0;
+  Mesh* mesh = nullptr;  // the input before it joins, the result after
+  SegState st;
+  Layout start;
+  double t_submit = 0, t_admit = 0, t_done = 0;
+  bool finished = false, taken = false, polled = false;
+  ~ServeJob() { delete mesh; }
+};
+
+struct Server {
+  AdaptParams ap;
+  unsigned long long budget = 0, reserved = 0;
+  double t0 = 0;
+  cudaStream_t s = nullptr;
+  std::map<u32, std::unique_ptr<ServeJob>> jobs;
+  std::deque<ServeJob*> queue;
+  std::vector<ServeJob*> active;  // segment order of `u`
+  std::vector<SegState> st;       // their loop states while they run
+  Mesh* u = nullptr;
+  std::unique_ptr<UnionCtl> ctl;
+  u32 next_id = 0;
+  u32 steps = 0, rebuilds = 0;
+
+  ~Server()
+  {
+    ctl.reset();
+    delete u;
+    jobs.clear();
+    if (s) {
+      cudaStreamSynchronize(s);
+      cudaStreamDestroy(s);
+    }
+  }
+
+  void admit(std::vector<ServeJob*>& joining)
+  {
+    while (!queue.empty()) {
+      ServeJob* j = queue.front();
+      bool busy = !active.empty() || !joining.empty();
+      if (busy && reserved + j->est_bytes > budget) break;
+      queue.pop_front();
+      reserved += j->est_bytes;
+      Mesh* m = new Mesh(j->dim, false, false, s);
+      try {
+        m->set_ents(0, j->nverts, nullptr);
+        u32 vpe = deg(j->dim, 0);
+        u32* c = dalloc<u32>((size_t)j->nelems * vpe, s);
+        CK(cudaMemcpyAsync(c, j->conn.data(), sizeof(u32) * j->conn.size(),
+            cudaMemcpyHostToDevice, s));
+        m->set_ents(j->dim, j->nelems, c);
+        double* x = dalloc<double>((size_t)j->nverts * 3, s);
+        CK(cudaMemcpyAsync(x, j->coords.data(), sizeof(double) * j->coords.size(),
+            cudaMemcpyHostToDevice, s));
+        m->add_tag(0, T_F64, "coordinates", 3, X_NOT, x);
+        m->derive_model(3.14159265359 / 4.0);  // PI / 4 with algebra.hpp:8's PI
+        double* h = dalloc<double>(j->nverts, s);
+        CK(cudaMemcpyAsync(h, j->size.data(), sizeof(double) * j->size.size(),
+            cudaMemcpyHostToDevice, s));
+        m->add_tag(0, T_F64, "adapt_size", 1, X_POINTWISE, h);
+        stream_sync(s);
+      } catch (...) {
+        delete m;
+        throw;
+      }
+      j->mesh = m;
+      j->start = layout_of(*m);
+      j->t_admit = now_s() - t0;
+      // the host copy is no longer needed
+      std::vector<double>().swap(j->coords);
+      std::vector<double>().swap(j->size);
+      std::vector<u32>().swap(j->conn);
+      joining.push_back(j);
+    }
+  }
+
+  u32 step()
+  {
+    std::vector<ServeJob*> joining;
+    admit(joining);
+    if (!joining.empty()) {
+      std::vector<Mesh*> parts;
+      if (u) parts.push_back(u);
+      for (ServeJob* j : joining) parts.push_back(j->mesh);
+      Mesh* old = u;
+      u = nullptr;
+      ctl.reset();
+      Mesh* nu = concat_meshes(parts, s);
+      delete old;
+      for (ServeJob* j : joining) {
+        delete j->mesh;
+        j->mesh = nullptr;
+        active.push_back(j);
+        st.push_back(SegState());
+      }
+      u = nu;
+      ctl.reset(new UnionCtl(*u));
+      rebuilds += 1;
+    }
+    if (!u) return (u32)queue.size();
+    steps += 1;
+    union_step(*ctl, st, ap);
+    bool any_done = false;
+    for (SegState const& x : st) any_done = any_done || x.state >= ST_DONE;
+    if (any_done) {
+      ctl.reset();
+      std::vector<Mesh*> outs = split_union(*u, s);
+      std::vector<Mesh*> keep;
+      std::vector<ServeJob*> still;
+      std::vector<SegState> still_st;
+      double t = now_s() - t0;
+      for (size_t k = 0; k < outs.size(); ++k) {
+        ServeJob* j = active[k];
+        if (st[k].state >= ST_DONE) {
+          j->st = st[k];
+          Layout want = j->start;
+          for (u32 op : st[k].res.ops) want = layout_after(op, want, u->dim);
+          apply_layout(*outs[k], want);
+          outs[k]->own_new_stream();
+          j->mesh = outs[k];
+          j->finished = true;
+          j->t_done = t;
+          reserved -= j->est_bytes;
+        } else {
+          keep.push_back(outs[k]);
+          still.push_back(j);
+          still_st.push_back(st[k]);
+        }
+      }
+      Mesh* nu = keep.empty() ? nullptr : concat_meshes(keep, s);
+      for (Mesh* m : keep) delete m;
+      delete u;
+      u = nu;
+      active.swap(still);
+      st.swap(still_st);
+      if (u) ctl.reset(new UnionCtl(*u));
+      rebuilds += 1;
+    }
+    return (u32)(active.size() + queue.size());
+  }
+};
+
+Server* server_new(AdaptParams const& ap, unsigned long long budget)
+{
+  Server* sv = new Server();
+  sv->ap = ap;
+  sv->budget = budget;
+  sv->t0 = now_s();
+  CK(cudaStreamCreateWithFlags(&sv->s, cudaStreamNonBlocking));
+  return sv;
+}
+
+void server_free(Server* sv) { delete sv; }
+
+u32 server_submit(Server* sv, u32 dim, u32 nverts, double const* coords, u32 nelems,
+    u32 const* conn, double const* size)
+{
+  if (dim < 2 || dim > 3) throw Failure(E_ARG, "jobs are 2D or 3D simplex meshes");
+  if (!nverts || !nelems || !coords || !conn || !size) throw Failure(E_ARG, "empty job");
+  std::unique_ptr<ServeJob> j(new ServeJob());
+  j->id = sv->next_id++;
+  j->dim = dim;
+  j->nverts = nverts;
+  j->nelems = nelems;
+  u32 vpe = dim + 1;
+  j->coords.assign(coords, coords + (size_t)nverts * 3);
+  j->conn.assign(conn, conn + (size_t)nelems * vpe);
+  j->size.assign(size, size + nverts);
+  for (u32 c : j->conn)
+    if (c >= nverts) throw Failure(E_ARG, "job connectivity names a missing vertex");
+  double est = estimate_elements(dim, nverts, coords, nelems, conn, size);
+  if (est < nelems) est = nelems;
+  // device bytes per element while a mesh adapts (connectivity of every
+  // dimension, the adjacency a pass derives, and the next mesh being built)
+  j->est_bytes = (unsigned long long)(est * 900.0);
+  j->t_submit = now_s() - sv->t0;
+  sv->queue.push_back(j.get());
+  u32 id = j->id;
+  sv->jobs[id] = std::move(j);
+  return id;
+}
+
+u32 server_step(Server* sv) { return sv->step(); }
+
+std::vector<u32> server_poll(Server* sv, u32 max_ids)
+{
+  std::vector<u32> out;
+  for (auto& kv : sv->jobs)
+    if (kv.second->finished && !kv.second->polled && out.size() < max_ids) {
+      kv.second->polled = true;
+      out.push_back(kv.first);
+    }
+  return out;
+}
+
+Mesh* server_take(Server* sv, u32 id)
+{
+  auto it = sv->jobs.find(id);
+  if (it == sv->jobs.end() || !it->second->finished || it->second->taken)
+    throw Failure(E_ARG, "no finished job with that id to take");
+  Mesh* m = it->second->mesh;
+  it->second->mesh = nullptr;
+  it->second->taken = true;
+  return m;
+}
+
+ServeJobInfo server_job_info(Server* sv, u32 id)
+{
+  auto it = sv->jobs.find(id);
+  if (it == sv->jobs.end()) throw Failure(E_ARG, "no job with that id");
+  ServeJob const& j = *it->second;
+  ServeJobInfo r;
+  r.t_submit = j.t_submit;
+  r.t_admit = j.t_admit;
+  r.t_done = j.t_done;
+  r.finished = j.finished;
+  r.passes = j.st.res.passes;
+  r.elems_in = j.st.res.elems_in;
+  r.status = j.st.res.status;
+  r.changed = j.st.res.changed;
+  return r;
+}
+
+ServeStats server_stats(Server* sv)
+{
+  ServeStats r;
+  r.steps = sv->steps;
+  r.rebuilds = sv->rebuilds;
+  r.active = (u32)sv->active.size();
+  r.queued = (u32)sv->queue.size();
+  r.reserved = sv->reserved;
+  r.now = now_s() - sv->t0;
+  return r;
+}
+
+}  // namespace osh
