@@ -387,7 +387,7 @@ def run_batched(args, world, rank, local):
     torch.cuda.set_device(local)
     L = G.lib()
     stream = torch.cuda.default_stream()
-    jobs = W.batched_boxes(args.batch_count, seed=1)
+    jobs = W.batched_boxes(args.batch_count, seed=1, nmax=args.batch_nmax)
     t0 = time.perf_counter()
     bases = [W.build_job_mesh(G, j) for j in jobs]
     prep_s = time.perf_counter() - t0
@@ -480,8 +480,10 @@ def run_batched(args, world, rank, local):
         "steps": 1, "warmup": 1, "ms_per_step": round(batch_ms, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded box meshes, uniform size fields)",
-        "config": {"workload": "batched_512_boxes", "meshes": len(jobs),
-                   "n": "log-uniform in [4,40], seed 1", "size": "U[0.3/n, 1.5/n]",
+        "config": {"workload": "batched_%d_boxes_n4_%d" % (len(jobs), args.batch_nmax),
+                   "meshes": len(jobs),
+                   "n": "log-uniform in [4,%d], seed 1" % args.batch_nmax,
+                   "size": "U[0.3/n, 1.5/n]",
                    "tets_in": int(sum(j.tets for j in jobs)),
                    "adapt": "mesh_adapt(1/3, 0.3, 4, 50) of every mesh",
                    "calls": len(chunks), "union_input_elems": BATCH_UNION_ELEMS,
@@ -497,6 +499,87 @@ def run_batched(args, world, rank, local):
     if not args.no_cpu and rank == 0:
         out["cpu_baseline"] = batched_cpu_sample(jobs)
     return out
+
+
+def run_serving(args, world, rank, local):
+    """Poisson arrivals (seed 2, args.rate per second) of box jobs with
+    log-uniform tet counts, served with continuous batching; latency is each
+    job's completion time minus its scheduled arrival."""
+    import torch
+    import omega_h_v1_b200 as G
+    from omega_h_v1_b200 import workloads as W
+    torch.cuda.set_device(local)
+    L = G.lib()
+    jobs = W.serving_stream(args.serve_count, seed=2, rate=args.rate)
+    inputs = [W.job_host_input(G, j) for j in jobs]
+    free, total = torch.cuda.mem_get_info()
+    budget = int(0.6 * free)
+    # warm-up: two small jobs through a throwaway server
+    warm = G.Server(SIZE_FLOOR, GOOD_QUAL, NLAYERS, MAX_OPS, budget)
+    small = sorted(range(len(jobs)), key=lambda i: jobs[i].tets)[:2]
+    for i in small:
+        warm.submit(*inputs[i])
+    while warm.step() > 0:
+        pass
+    for i in warm.poll():
+        warm.take(i).close()
+    warm.close()
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    launches0 = L.osh_b200_launch_count()
+    sv = G.Server(SIZE_FLOOR, GOOD_QUAL, NLAYERS, MAX_OPS, budget)
+    t0 = time.perf_counter() - sv.stats()["now"]   # server clock origin
+    ids = {}
+    nxt = 0
+    remaining = 0
+    active_samples = []
+    while nxt < len(jobs) or remaining > 0:
+        now = time.perf_counter() - t0
+        while nxt < len(jobs) and jobs[nxt].arrival <= now:
+            ids[sv.submit(*inputs[nxt])] = nxt
+            nxt += 1
+        if sv.stats()["queued"] + sv.stats()["active"] > 0:
+            remaining = sv.step()
+            active_samples.append(sv.stats()["active"])
+            for j in sv.poll():
+                sv.take(j).close()
+        else:
+            remaining = 0
+            if nxt < len(jobs):
+                time.sleep(max(0.0, jobs[nxt].arrival - (time.perf_counter() - t0)))
+    torch.cuda.synchronize()
+    makespan = time.perf_counter() - t0
+    clk = clocks.stop()
+    launches = L.osh_b200_launch_count() - launches0
+    lat, elems, tets_in = [], 0.0, 0
+    for jid, i in ids.items():
+        info = sv.job_info(jid)
+        lat.append(info["t_done"] - jobs[i].arrival)
+        elems += info["elems_in"]
+        tets_in += jobs[i].tets
+    st = sv.stats()
+    sv.close()
+    lat = np.sort(np.array(lat))
+    p50 = float(np.percentile(lat, 50))
+    p99 = float(np.percentile(lat, 99))
+    span = makespan - jobs[0].arrival
+    return {
+        "metric": METRIC, "value": round(elems / span, 1), "unit": UNIT, "n_gpus": world,
+        "steps": 1, "warmup": 1, "ms_per_step": round(span * 1e3, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded Poisson stream of box jobs)",
+        "config": {"workload": "serving_poisson", "jobs": len(jobs), "rate_per_s": args.rate,
+                   "tets": "log-uniform in [2e3, 2e6] per job, seed 2",
+                   "size": "half uniform U[1.0/n, 1.6/n], half radial 0.8/n (1 + 4|x-c|)",
+                   "tets_in": int(tets_in), "budget_bytes": budget,
+                   "adapt": "mesh_adapt(1/3, 0.3, 4, 50) per job",
+                   "l2": "inputs larger than L2 (hundreds of MB resident)"},
+        "latency_ms": {"p50": round(p50 * 1e3, 2), "p99": round(p99 * 1e3, 2),
+                       "max": round(float(lat[-1]) * 1e3, 2)},
+        "mean_active_jobs": round(float(np.mean(active_samples)), 2) if active_samples else 0,
+        "server_steps": st["steps"], "elems_in": elems,
+        "gpu_launches": int(launches), "clocks": clk,
+    }
 
 
 def batched_cpu_sample(jobs, budget_est_tets=12e6):
@@ -620,7 +703,7 @@ def run_reference(args, world, rank):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--probe", type=int, default=int(os.environ.get("OSH_BENCH_PROBE", "0")),
@@ -629,10 +712,15 @@ def main():
                     help="DRAM bytes per launch of that kernel from an ncu capture")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling)")
-    ap.add_argument("--workload", default="box48", choices=["box48", "batched"],
+    ap.add_argument("--workload", default="box48", choices=["box48", "batched", "serving"],
                     help="box48: the 48^3 radial-size adapt; batched: 512 uneven boxes, "
-                         "plain one-by-one path against adapt_batch")
+                         "plain one-by-one path against adapt_batch; serving: Poisson "
+                         "stream of jobs through the continuous-batching server")
     ap.add_argument("--batch-count", type=int, default=512)
+    ap.add_argument("--batch-nmax", type=int, default=40,
+                    help="largest grid edge of the batched boxes (40 = the full workload)")
+    ap.add_argument("--serve-count", type=int, default=200)
+    ap.add_argument("--rate", type=float, default=200.0)
     args = ap.parse_args()
     world, rank, local = dist_setup()
     if args.impl == "reference":
@@ -645,6 +733,8 @@ def main():
         return
     if args.workload == "batched":
         out = run_batched(args, world, rank, local)
+    elif args.workload == "serving":
+        out = run_serving(args, world, rank, local)
     else:
         out = run_ours(args, world, rank, local)
     if rank == 0:

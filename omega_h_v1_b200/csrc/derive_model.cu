@@ -1,11 +1,19 @@
-// Geometric classification of a mesh (mesh_derive_model, derive_model.cpp:
-// 218-448): class_dim from boundary sides, crease angles and corners, then
-// class_id from connected components of equal-order entities (bfs.cpp) and
-// projection onto lower dimensions.
+// Geometric classification of a mesh on the device (mesh_derive_model,
+// derive_model.cpp:218-448): class_dim from boundary sides, crease angles and
+// corners, then class_id from connected components of equally classified
+// entities (the reference's breadth-first search, bfs.cpp) and projection
+// onto lower dimensions.
 //
-// This is one-time input preparation, done on the host from adjacency the
-// device derived: the crease test calls acos, and running it on the host
-// keeps every crease decision identical to the reference's.
+// Crease test: the reference compares acos(n0 . n1) with the crease angle.
+// acos is decreasing, so every hinge whose dot product lies more than 1e-9
+// away from cos(crease) is decided on the device by comparing the dot
+// product; the few inside that band are sent to the host, which applies the
+// reference's own test with std::acos, so every decision is the reference's.
+//
+// Components: union-find in which a root only ever hooks under a smaller
+// root, so the final root of a component is its smallest member, and the
+// components are numbered in the order of their smallest members, which is
+// the order in which the reference's search meets them.
 #include <cmath>
 #include <vector>
 
@@ -13,168 +21,364 @@
 
 namespace osh {
 
-template <class T>
-static std::vector<T> to_host(T const* d, size_t n, cudaStream_t s)
+namespace {
+
+constexpr u32 UF_CAP = 1u << 24;  // bound on any union-find walk or retry loop
+
+// boundary sides (fewer than two elements) and their class_dim
+__global__ void k_side_class(u32 ns, u32 D, u32 const* __restrict__ offs,
+    u32* __restrict__ bside, u32* __restrict__ scd)
 {
-  std::vector<T> h(n);
-  if (n) CK(cudaMemcpyAsync(h.data(), d, n * sizeof(T), cudaMemcpyDeviceToHost, s));
-  return h;
+  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= ns) return;
+  u32 b = (offs[i + 1] - offs[i]) < 2 ? 1u : 0u;
+  bside[i] = b;
+  scd[i] = D - b;
 }
 
-struct HostUp {
-  std::vector<u32> offs, adj;
-};
-
-static HostUp host_up(Mesh& m, u32 low, u32 high)
+// unit normals of boundary sides (derive_model.cpp:17-76): the edge vector
+// in 2D, the triangle's (v1 - v0) x (v2 - v0) in 3D
+__global__ void k_side_normals(u32 ns, u32 D, u32 const* __restrict__ vos,
+    double const* __restrict__ x, u32 const* __restrict__ bside, double* __restrict__ nrm)
 {
-  UpAdj const& u = m.ask_up(low, high);
-  HostUp h;
-  u32 n = m.count(low);
-  h.offs = to_host(u.offs, (size_t)n + 1, m.s);
-  stream_sync(m.s);
-  h.adj = to_host(u.adj, h.offs[n], m.s);
-  stream_sync(m.s);
-  return h;
+  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= ns) return;
+  double nn[3] = {0.0, 0.0, 0.0};
+  if (bside[i]) {
+    if (D == 2) {
+      double a[3], b[3];
+      load3(x, vos[i * 2 + 1], a);
+      load3(x, vos[i * 2], b);
+      sub3(a, b, nn);
+    } else {
+      double p0[3], p1[3], p2[3], b0[3], b1[3];
+      load3(x, vos[i * 3], p0);
+      load3(x, vos[i * 3 + 1], p1);
+      load3(x, vos[i * 3 + 2], p2);
+      sub3(p1, p0, b0);
+      sub3(p2, p0, b1);
+      cross3(b0, b1, nn);
+    }
+    double sc = 1.0 / sqrt(dot3(nn, nn));
+    for (u32 k = 0; k < 3; ++k) nn[k] = nn[k] * sc;
+  }
+  nrm[i * 3 + 0] = nn[0];
+  nrm[i * 3 + 1] = nn[1];
+  nrm[i * 3 + 2] = nn[2];
 }
 
-static u32* upload(std::vector<u32> const& h, cudaStream_t s)
+// hinges (derive_model.cpp:78-138): on the boundary if any adjacent side is;
+// the crease angle is between the first two boundary sides in row order (a
+// missing second side reads side 0, as the reference's zeroed pair does)
+__global__ void k_hinge_class(u32 nh, u32 const* __restrict__ offs, u32 const* __restrict__ adj,
+    u32 const* __restrict__ bside, double const* __restrict__ nrm, double cos_lo,
+    double cos_hi, u32* __restrict__ bh, u32* __restrict__ crease, double* __restrict__ dots,
+    u32* __restrict__ namb, u32* __restrict__ amb)
 {
-  u32* d = dalloc<u32>(h.size(), s);
-  if (!h.empty())
-    CK(cudaMemcpyAsync(d, h.data(), h.size() * sizeof(u32), cudaMemcpyHostToDevice, s));
-  stream_sync(s);
-  return d;
+  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nh) return;
+  u32 a[2] = {0, 0}, na = 0;
+  for (u32 j = offs[i]; j < offs[i + 1]; ++j)
+    if (bside[adj[j]] && na < 2) a[na++] = adj[j];
+  u32 b = na > 0 ? 1u : 0u, c = 0;
+  if (b) {
+    double d = dot3(nrm + (size_t)a[0] * 3, nrm + (size_t)a[1] * 3);
+    dots[i] = d;
+    if (d < cos_lo) {
+      c = 1;
+    } else if (!(d > cos_hi)) {
+      // within the band, or NaN: the host decides with acos
+      u32 k = atomicAdd(namb, 1u);
+      amb[k] = i;
+    }
+  }
+  bh[i] = b;
+  crease[i] = c;
 }
 
-void Mesh::derive_model(double crease)
+__global__ void k_set_flags(u32 n, u32 const* __restrict__ idx, u32 const* __restrict__ val,
+    u32* __restrict__ out)
+{
+  u32 k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n) out[idx[k]] = val[k];
+}
+
+__global__ void k_hinge_cd(u32 nh, u32 D, u32 const* __restrict__ bh,
+    u32 const* __restrict__ crease, u32* __restrict__ hcd)
+{
+  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < nh) hcd[i] = D - bh[i] - crease[i];
+}
+
+// 3D vertices (derive_model.cpp:140-216): the lowest class_dim of their
+// edges, one lower again at a corner of more than two crease edges
+__global__ void k_vertex_class(u32 nv, u32 const* __restrict__ offs, u32 const* __restrict__ adj,
+    u32 const* __restrict__ crease, u32 const* __restrict__ hcd, u32* __restrict__ vcd)
+{
+  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nv) return;
+  u32 nin = 0, d = 3;
+  for (u32 j = offs[i]; j < offs[i + 1]; ++j) {
+    u32 e = adj[j];
+    if (crease[e]) ++nin;
+    if (hcd[e] < d) d = hcd[e];
+  }
+  vcd[i] = d - (nin > 2 ? 1u : 0u);
+}
+
+__global__ void k_is_value(u32 n, u32 const* __restrict__ a, u32 v, u32* __restrict__ out)
+{
+  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = a[i] == v ? 1u : 0u;
+}
+
+__global__ void k_vertex_ids(u32 n, u32 const* __restrict__ cd, u32 const* __restrict__ scan,
+    u32* __restrict__ cid)
+{
+  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) cid[i] = cd[i] == 0 ? scan[i] : INV;
+}
+
+__device__ u32 uf_find(u32* parent, u32 x, u32* fail)
+{
+  for (u32 it = 0; it < UF_CAP; ++it) {
+    u32 p = __ldcg(parent + x);
+    if (p == x) return x;
+    u32 gp = __ldcg(parent + p);
+    if (gp != p) atomicMin(parent + x, gp);  // path halving; parents only shrink
+    x = gp;
+  }
+  atomicOr(fail, 1u);
+  return x;
+}
+
+__global__ void k_cc_init(u32 n, u32 const* __restrict__ cd, u32 d, u32* __restrict__ parent)
+{
+  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) parent[i] = cd[i] == d ? i : INV;
+}
+
+// entity u and every other entity classified on d that shares with it a
+// side classified on d are in one component
+__global__ void k_cc_hook(u32 n, u32 spd, u32 const* __restrict__ sod,
+    u32 const* __restrict__ cds, u32 const* __restrict__ offs, u32 const* __restrict__ adj,
+    u32 const* __restrict__ cdd, u32 d, u32* parent, u32* fail)
+{
+  u32 t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n * spd) return;
+  u32 u = t / spd;
+  if (cdd[u] != d) return;
+  u32 sd = sod[t];
+  if (cds[sd] != d) return;
+  for (u32 j = offs[sd]; j < offs[sd + 1]; ++j) {
+    u32 o = adj[j];
+    if (o == u || cdd[o] != d) continue;
+    u32 ra = uf_find(parent, u, fail), rb = uf_find(parent, o, fail);
+    u32 it = 0;
+    while (ra != rb) {
+      if (++it > UF_CAP) {
+        atomicOr(fail, 1u);
+        break;
+      }
+      if (ra < rb) {
+        u32 x = ra;
+        ra = rb;
+        rb = x;
+      }
+      u32 old = atomicCAS(parent + ra, ra, rb);
+      if (old == ra) break;
+      ra = uf_find(parent, old, fail);
+      rb = uf_find(parent, rb, fail);
+    }
+  }
+}
+
+__global__ void k_cc_flatten(u32 n, u32* parent, u32* __restrict__ is_root, u32* fail)
+{
+  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  u32 p = parent[i];
+  if (p == INV) {
+    is_root[i] = 0;
+    return;
+  }
+  u32 r = uf_find(parent, i, fail);
+  parent[i] = r;
+  is_root[i] = r == i ? 1u : 0u;
+}
+
+__global__ void k_cc_ids(u32 n, u32 const* __restrict__ parent, u32 const* __restrict__ scan,
+    u32* __restrict__ cid)
+{
+  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  u32 p = parent[i];
+  cid[i] = p == INV ? INV : scan[p];
+}
+
+// project_class_id_onto (derive_model.cpp:392-412): the last upward entity
+// (row order) with the same class_dim gives its class_id
+__global__ void k_project_ids(u32 n, u32 const* __restrict__ offs, u32 const* __restrict__ adj,
+    u32 const* __restrict__ cd_hi, u32 const* __restrict__ cid_hi,
+    u32 const* __restrict__ cd_lo, u32* __restrict__ cid_lo)
+{
+  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  u32 c = cd_lo[i], id = cid_lo[i];
+  for (u32 j = offs[i]; j < offs[i + 1]; ++j)
+    if (cd_hi[adj[j]] == c) id = cid_hi[adj[j]];
+  cid_lo[i] = id;
+}
+
+}  // namespace
+
+void Mesh::derive_model(double crease_angle)
 {
   u32 const D = dim;
   if (D < 2) throw Failure(E_ARG, "classification needs a 2D or 3D mesh");
   u32 nel = count(D);
-  std::vector<u32> ecd(nel, D);
-  add_tag(D, T_U32, "class_dim", 1, X_NOT, upload(ecd, s));
+  u32* cd[4] = {nullptr, nullptr, nullptr, nullptr};
+  // elements
+  cd[D] = dalloc<u32>(nel, s);
+  fill_u32(cd[D], nel, D, s);
+  add_tag(D, T_U32, "class_dim", 1, X_NOT, cd[D]);
+  // sides
   u32 ns = count(D - 1);
-  HostUp es = host_up(*this, D - 1, D);
-  std::vector<u32> bside(ns), scd(ns);
-  for (u32 i = 0; i < ns; ++i) {
-    bside[i] = (es.offs[i + 1] - es.offs[i]) < 2;
-    scd[i] = D - bside[i];
+  UpAdj const& es = ask_up(D - 1, D, false);
+  u32* bside = dalloc<u32>(ns, s);
+  cd[D - 1] = dalloc<u32>(ns, s);
+  if (ns) {
+    k_side_class<<<grid_for(ns), BLOCK, 0, s>>>(ns, D, es.offs, bside, cd[D - 1]);
+    CK_LAUNCH();
   }
-  add_tag(D - 1, T_U32, "class_dim", 1, X_NOT, upload(scd, s));
-  std::vector<double> x = to_host(coords(), (size_t)count(0) * 3, s);
-  u32 vps = deg(D - 1, 0);
-  std::vector<u32> vos = to_host(ask_down(D - 1, 0), (size_t)ns * vps, s);
-  stream_sync(s);
-  // boundary side normals (derive_model.cpp:17-76)
-  std::vector<double> nrm((size_t)ns * 3, 0.0);
-  for (u32 i = 0; i < ns; ++i) {
-    if (!bside[i]) continue;
-    double* nn = &nrm[(size_t)i * 3];
-    if (D - 1 == 1) {
-      sub3(&x[vos[i * 2 + 1] * 3], &x[vos[i * 2] * 3], nn);
-    } else {
-      double b0[3], b1[3];
-      sub3(&x[vos[i * 3 + 1] * 3], &x[vos[i * 3] * 3], b0);
-      sub3(&x[vos[i * 3 + 2] * 3], &x[vos[i * 3] * 3], b1);
-      cross3(b0, b1, nn);
-    }
-    double sc = 1.0 / std::sqrt(dot3(nn, nn));
-    for (u32 k = 0; k < 3; ++k) nn[k] = nn[k] * sc;
+  add_tag(D - 1, T_U32, "class_dim", 1, X_NOT, cd[D - 1]);
+  double* nrm = dalloc<double>((size_t)ns * 3, s);
+  if (ns) {
+    k_side_normals<<<grid_for(ns), BLOCK, 0, s>>>(ns, D, ask_down(D - 1, 0), coords(), bside,
+        nrm);
+    CK_LAUNCH();
   }
-  // hinges: boundary marks, angles, creases (derive_model.cpp:78-138)
+  // hinges
   u32 nh = count(D - 2);
-  HostUp sh = host_up(*this, D - 2, D - 1);
-  std::vector<u32> bh(nh, 0), crease_h(nh, 0), hcd(nh);
-  for (u32 i = 0; i < nh; ++i) {
-    for (u32 j = sh.offs[i]; j < sh.offs[i + 1]; ++j)
-      if (bside[sh.adj[j]]) {
-        bh[i] = 1;
-        break;
-      }
-    double ang = 0;
-    if (bh[i]) {
-      u32 adj[2] = {0, 0}, na = 0;
-      for (u32 j = sh.offs[i]; j < sh.offs[i + 1]; ++j)
-        if (bside[sh.adj[j]] && na < 2) adj[na++] = sh.adj[j];
-      ang = std::acos(dot3(&nrm[adj[0] * 3], &nrm[adj[1] * 3]));
-    }
-    crease_h[i] = ang > crease;
-    hcd[i] = D - bh[i] - crease_h[i];
+  UpAdj const& sh = ask_up(D - 2, D - 1, true);
+  u32* bh = dalloc<u32>(nh, s);
+  u32* crease = dalloc<u32>(nh, s);
+  double* dots = dalloc<double>(nh, s);
+  u32* amb = dalloc<u32>(nh ? nh : 1, s);
+  u32* namb = mb->dev + 24;
+  CK(cudaMemsetAsync(namb, 0, sizeof(u32), s));
+  double cc = std::cos(crease_angle);
+  if (nh) {
+    k_hinge_class<<<grid_for(nh), BLOCK, 0, s>>>(nh, sh.offs, sh.adj, bside, nrm, cc - 1e-9,
+        cc + 1e-9, bh, crease, dots, namb, amb);
+    CK_LAUNCH();
   }
-  add_tag(D - 2, T_U32, "class_dim", 1, X_NOT, upload(hcd, s));
-  if (D == 3) {
-    // corners and vertex class_dim (derive_model.cpp:140-216)
-    u32 nv = count(0);
-    HostUp ev = host_up(*this, 0, 1);
-    std::vector<u32> vcd(nv);
-    for (u32 i = 0; i < nv; ++i) {
-      u32 nin = 0, d = 3;
-      for (u32 j = ev.offs[i]; j < ev.offs[i + 1]; ++j) {
-        u32 e = ev.adj[j];
-        if (crease_h[e]) ++nin;
-        if (hcd[e] < d) d = hcd[e];
-      }
-      vcd[i] = d - (nin > 2 ? 1u : 0u);
-    }
-    add_tag(0, T_U32, "class_dim", 1, X_NOT, upload(vcd, s));
-  }
-  // class ids (derive_model.cpp:414-442)
-  std::vector<std::vector<u32>> cd(D + 1), cid(D + 1);
-  for (u32 d = 0; d <= D; ++d) {
-    cd[d] = to_host(static_cast<u32 const*>(find_tag(d, "class_dim")->data), count(d), s);
-  }
-  stream_sync(s);
-  {
-    u32 nv = count(0), k = 0;
-    cid[0].assign(nv, INV);
-    for (u32 i = 0; i < nv; ++i)
-      if (cd[0][i] == 0) cid[0][i] = k++;
-  }
-  for (u32 d = 1; d <= D; ++d) {
-    // components of entities classified on d, joined through sides also
-    // classified on d, numbered by their smallest member
-    u32 n = count(d), spd = deg(d, d - 1);
-    std::vector<u32> sod = to_host(ask_down(d, d - 1), (size_t)n * spd, s);
+  mb->fetch(s, 25);
+  u32 na = mb->host[24];
+  if (na) {
+    // the reference's own test for the hinges inside the band
+    std::vector<u32> idx(na), val(na);
+    std::vector<double> dv(na);
+    CK(cudaMemcpyAsync(idx.data(), amb, sizeof(u32) * na, cudaMemcpyDeviceToHost, s));
     stream_sync(s);
-    HostUp dos = host_up(*this, d - 1, d);
-    std::vector<u32>& id = cid[d];
-    id.assign(n, INV);
-    std::vector<u32> queue(n);
-    u32 comp = 0;
-    for (u32 i = 0; i < n; ++i) {
-      if (cd[d][i] != d || id[i] != INV) continue;
-      u32 b = 0, e = 0;
-      queue[e++] = i;
-      id[i] = comp;
-      while (b != e) {
-        u32 u = queue[b++];
-        for (u32 j = 0; j < spd; ++j) {
-          u32 sd = sod[(size_t)u * spd + j];
-          if (cd[d - 1][sd] != d) continue;
-          for (u32 l = dos.offs[sd]; l < dos.offs[sd + 1]; ++l) {
-            u32 o = dos.adj[l];
-            if (o == u || cd[d][o] != d) continue;
-            if (id[o] == INV) {
-              id[o] = comp;
-              queue[e++] = o;
-            }
-            break;
-          }
-        }
-      }
-      ++comp;
+    double* dsel = dalloc<double>(na, s);
+    for (u32 k = 0; k < na; ++k)
+      CK(cudaMemcpyAsync(dsel + k, dots + idx[k], sizeof(double), cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemcpyAsync(dv.data(), dsel, sizeof(double) * na, cudaMemcpyDeviceToHost, s));
+    stream_sync(s);
+    dev_free(dsel, s);
+    for (u32 k = 0; k < na; ++k) val[k] = std::acos(dv[k]) > crease_angle ? 1u : 0u;
+    u32* di = dalloc<u32>(2 * (size_t)na, s);
+    CK(cudaMemcpyAsync(di, idx.data(), sizeof(u32) * na, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(di + na, val.data(), sizeof(u32) * na, cudaMemcpyHostToDevice, s));
+    k_set_flags<<<grid_for(na), BLOCK, 0, s>>>(na, di, di + na, crease);
+    CK_LAUNCH();
+    stream_sync(s);
+    dev_free(di, s);
+  }
+  dev_free(dots, s);
+  dev_free(amb, s);
+  dev_free(nrm, s);
+  cd[D - 2] = dalloc<u32>(nh, s);
+  if (nh) {
+    k_hinge_cd<<<grid_for(nh), BLOCK, 0, s>>>(nh, D, bh, crease, cd[D - 2]);
+    CK_LAUNCH();
+  }
+  add_tag(D - 2, T_U32, "class_dim", 1, X_NOT, cd[D - 2]);
+  if (D == 3) {
+    u32 nv = count(0);
+    UpAdj const& ev = ask_up(0, 1, false);
+    cd[0] = dalloc<u32>(nv, s);
+    if (nv) {
+      k_vertex_class<<<grid_for(nv), BLOCK, 0, s>>>(nv, ev.offs, ev.adj, crease, cd[D - 2],
+          cd[0]);
+      CK_LAUNCH();
     }
+    add_tag(0, T_U32, "class_dim", 1, X_NOT, cd[0]);
+  }
+  dev_free(bside, s);
+  dev_free(bh, s);
+  dev_free(crease, s);
+  // class ids (derive_model.cpp:414-442)
+  u32* cid[4] = {nullptr, nullptr, nullptr, nullptr};
+  {
+    u32 nv = count(0);
+    u32* f = dalloc<u32>(nv ? nv : 1, s);
+    if (nv) {
+      k_is_value<<<grid_for(nv), BLOCK, 0, s>>>(nv, cd[0], 0, f);
+      CK_LAUNCH();
+    }
+    u32* sc = exscan_new(f, nv, s);
+    cid[0] = dalloc<u32>(nv, s);
+    if (nv) {
+      k_vertex_ids<<<grid_for(nv), BLOCK, 0, s>>>(nv, cd[0], sc, cid[0]);
+      CK_LAUNCH();
+    }
+    dev_free(sc, s);
+    dev_free(f, s);
+  }
+  u32* fail = mb->dev + 25;
+  CK(cudaMemsetAsync(fail, 0, sizeof(u32), s));
+  for (u32 d = 1; d <= D; ++d) {
+    u32 n = count(d), spd = deg(d, d - 1);
+    u32 const* sod = ask_down(d, d - 1);
+    UpAdj const& dos = ask_up(d - 1, d, false);
+    cid[d] = dalloc<u32>(n, s);
+    u32* roots = dalloc<u32>(n ? n : 1, s);
+    if (n) {
+      k_cc_init<<<grid_for(n), BLOCK, 0, s>>>(n, cd[d], d, cid[d]);
+      CK_LAUNCH();
+      k_cc_hook<<<grid_for((u64)n * spd), BLOCK, 0, s>>>(n, spd, sod, cd[d - 1], dos.offs,
+          dos.adj, cd[d], d, cid[d], fail);
+      CK_LAUNCH();
+      k_cc_flatten<<<grid_for(n), BLOCK, 0, s>>>(n, cid[d], roots, fail);
+      CK_LAUNCH();
+    }
+    u32* sc = exscan_new(roots, n, s);
+    if (n) {
+      k_cc_ids<<<grid_for(n), BLOCK, 0, s>>>(n, cid[d], sc, cid[d]);
+      CK_LAUNCH();
+    }
+    dev_free(sc, s);
+    dev_free(roots, s);
+  }
+  mb->fetch(s, 26);
+  if (mb->host[25]) {
+    for (u32 d = 0; d <= D; ++d) dev_free(cid[d], s);
+    throw Failure(E_TIMEOUT, "classification: a union-find walk exceeded its bound");
   }
   for (u32 dd = 1; dd <= D; ++dd) {
-    // project_class_id_onto (derive_model.cpp:392-412)
     u32 d = D - dd, nl = count(d);
-    HostUp u = host_up(*this, d, d + 1);
-    for (u32 i = 0; i < nl; ++i)
-      for (u32 j = u.offs[i]; j < u.offs[i + 1]; ++j)
-        if (cd[d + 1][u.adj[j]] == cd[d][i]) cid[d][i] = cid[d + 1][u.adj[j]];
+    UpAdj const& u = ask_up(d, d + 1, true);
+    if (nl) {
+      k_project_ids<<<grid_for(nl), BLOCK, 0, s>>>(nl, u.offs, u.adj, cd[d + 1], cid[d + 1],
+          cd[d], cid[d]);
+      CK_LAUNCH();
+    }
   }
-  for (u32 d = 0; d <= D; ++d) add_tag(d, T_U32, "class_id", 1, X_NOT, upload(cid[d], s));
-  // the reference adds tags in this order: dim, dim-1, ..., then class_id 0..dim
+  for (u32 d = 0; d <= D; ++d) add_tag(d, T_U32, "class_id", 1, X_NOT, cid[d]);
+  // the reference adds tags in this order: class_dim of dim, dim-1, ...,
+  // then class_id of 0..dim
   full = true;
 }
 

@@ -146,8 +146,10 @@ void Mesh::clear_contents()
   dev_free(dual, s);
   dual = nullptr;
   for (u32 d = 0; d < 3; ++d) {
-    dev_free(up_other[d], s);
-    up_other[d] = nullptr;
+    dev_free(low_row_offs[d], s);
+    dev_free(low_rows[d], s);
+    low_row_offs[d] = nullptr;
+    low_rows[d] = nullptr;
   }
   for (u32 d = 0; d < 4; ++d) {
     for (auto& t : tags[d]) dev_free(t.data, s);
@@ -187,8 +189,10 @@ void Mesh::overwrite(Mesh* with)
   dual = with->dual;
   with->dual = nullptr;
   for (u32 d = 0; d < 3; ++d) {
-    up_other[d] = with->up_other[d];
-    with->up_other[d] = nullptr;
+    low_row_offs[d] = with->low_row_offs[d];
+    low_rows[d] = with->low_rows[d];
+    with->low_row_offs[d] = nullptr;
+    with->low_rows[d] = nullptr;
   }
   for (u32 d = 0; d < 4; ++d) {
     counts[d] = with->counts[d];
@@ -542,106 +546,105 @@ void up_from_down_scratch(u32 high, u32 low, u32 nhighs, u32 nlows, u32 const* l
 // ---------------------------------------------------------------------------
 // downward adjacency by search (reflect_down.cpp:13-81)
 
-__global__ void k_reflect_down(u32 high, u32 low, u32 nh, u32 const* __restrict__ voh,
-    u32 const* __restrict__ vol, u32 const* __restrict__ lv_offs,
-    u32 const* __restrict__ lv_adj, u32 const* __restrict__ lv_dirs,
-    u32* __restrict__ out)
-{
-  u32 lph = deg(high, low), vph = deg(high, 0);
-  u32 idx = blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= nh * lph) return;
-  u32 i = idx / lph, j = idx % lph;
-  u32 const* vh = voh + (size_t)i * vph;
-  u32 w0 = vh[canon(high, low, 0, j, 0)];
-  u32 w1 = vh[canon(high, low, 0, j, 1)];
-  u32 f = lv_offs[w0], e = lv_offs[w0 + 1];
-  u32 found = INV;
-  if (low == 1) {
-    for (u32 r = f; r < e; ++r) {
-      u32 ed = lv_adj[r], d = lv_dirs[r];
-      if (vol[ed * 2 + (1 - d)] == w1) {
-        found = ed;
-        break;
-      }
-    }
-  } else {
-    u32 w2 = vh[canon(high, low, 0, j, 2)];
-    for (u32 r = f; r < e; ++r) {
-      u32 t = lv_adj[r], d = lv_dirs[r];
-      u32 a = vol[t * 3 + (d + 1) % 3], b = vol[t * 3 + (d + 2) % 3];
-      if ((a == w1 && b == w2) || (a == w2 && b == w1)) {
-        found = t;
-        break;
-      }
-    }
-  }
-  out[idx] = found;
-}
-
-// Rows for the search: per use of up(0,1) the edge's other vertex, per use of
-// up(0,2) the triangle's other two vertices (cyclic after the vertex).
-__global__ void k_other_verts(u32 low, u32 nuse, u32 const* __restrict__ adj,
-    u32 const* __restrict__ dirs, u32 const* __restrict__ vol, u32* __restrict__ other)
-{
-  u32 j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= nuse) return;
-  u32 e = adj[j], d = dirs[j];
-  if (low == 1) {
-    other[j] = vol[e * 2 + (1 - d)];
-  } else {
-    uint2 o;
-    o.x = vol[e * 3 + (d + 1) % 3];
-    o.y = vol[e * 3 + (d + 2) % 3];
-    reinterpret_cast<uint2*>(other)[j] = o;
-  }
-}
-
 // reflect_down_entity / find_by_verts (reflect_down.cpp:13-38,
-// find_by_verts.hpp:14-55): the low entity with the wanted vertices is
-// unique, so the search may start from whichever of its vertices has the
-// shortest upward row; each candidate costs one contiguous load.
-__global__ void k_reflect_rows(u32 high, u32 low, u32 nh, u32 const* __restrict__ voh,
-    u32 const* __restrict__ lv_offs, u32 const* __restrict__ lv_adj,
-    u32 const* __restrict__ other, u32* __restrict__ out)
+// find_by_verts.hpp:14-76): the low entity with the wanted vertices is
+// unique, so it is found in the row of its smallest vertex, where every low
+// entity is listed once with its other vertices (half the records of the
+// vertices' upward adjacency, and one contiguous row to scan).
+
+__device__ inline void sort_small(u32* w, u32 n)
 {
-  u32 lph = deg(high, low), vph = deg(high, 0);
-  u32 idx = blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= nh * lph) return;
-  u32 i = idx / lph, j = idx % lph;
-  u32 const* vh = voh + (size_t)i * vph;
-  u32 w[3];
-  w[0] = vh[canon(high, low, 0, j, 0)];
-  w[1] = vh[canon(high, low, 0, j, 1)];
-  w[2] = low == 2 ? vh[canon(high, low, 0, j, 2)] : INV;
-  u32 best = 0, f = lv_offs[w[0]], e = lv_offs[w[0] + 1];
-  for (u32 k = 1; k <= low; ++k) {
-    u32 fk = lv_offs[w[k]], ek = lv_offs[w[k] + 1];
-    if (ek - fk < e - f) {
-      best = k;
-      f = fk;
-      e = ek;
+  for (u32 i = 1; i < n; ++i)
+    for (u32 j = i; j > 0 && w[j - 1] > w[j]; --j) {
+      u32 t = w[j];
+      w[j] = w[j - 1];
+      w[j - 1] = t;
+    }
+}
+
+__global__ void k_count_min_vert(u32 low, u32 nl, u32 const* __restrict__ vol, u32* cnt)
+{
+  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nl) return;
+  u32 vpl = low + 1, m = vol[(size_t)i * vpl];
+  for (u32 k = 1; k < vpl; ++k) m = min(m, vol[(size_t)i * vpl + k]);
+  atomicAdd(&cnt[m], 1u);
+}
+
+__global__ void k_fill_min_vert(u32 low, u32 nl, u32 const* __restrict__ vol,
+    u32 const* __restrict__ offs, u32* cur, u32* __restrict__ rows)
+{
+  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nl) return;
+  u32 vpl = low + 1, w[3];
+  for (u32 k = 0; k < vpl; ++k) w[k] = vol[(size_t)i * vpl + k];
+  sort_small(w, vpl);
+  u32 slot = offs[w[0]] + atomicAdd(&cur[w[0]], 1u);
+  if (low == 1)
+    reinterpret_cast<uint2*>(rows)[slot] = make_uint2(w[1], i);
+  else
+    reinterpret_cast<uint4*>(rows)[slot] = make_uint4(w[1], w[2], i, 0u);
+}
+
+// One thread per high entity: its low entities are looked up grouped by
+// their smallest vertex, so each row is scanned once for every wanted entity
+// it holds (a tet's four triangles live in two rows, its six edges in three).
+template <u32 HIGH, u32 LOW>
+__global__ void k_reflect_grouped(u32 nh, u32 const* __restrict__ voh,
+    u32 const* __restrict__ offs, u32 const* __restrict__ rows, u32* __restrict__ out)
+{
+  constexpr u32 LPH = HIGH == 3 ? (LOW == 1 ? 6 : 4) : 3;
+  constexpr u32 VPH = HIGH + 1, VPL = LOW + 1;
+  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nh) return;
+  u32 v[VPH];
+#pragma unroll
+  for (u32 k = 0; k < VPH; ++k) v[k] = voh[(size_t)i * VPH + k];
+  u32 t[LPH][VPL], found[LPH];
+#pragma unroll
+  for (u32 j = 0; j < LPH; ++j) {
+#pragma unroll
+    for (u32 k = 0; k < VPL; ++k) t[j][k] = v[canon(HIGH, LOW, 0, j, k)];
+    sort_small(t[j], VPL);
+    found[j] = INV;
+  }
+#pragma unroll
+  for (u32 j = 0; j < LPH; ++j) {
+    if (found[j] != INV) continue;
+    u32 m = t[j][0];
+    u32 f = offs[m], e = offs[m + 1];
+    bool pending = true;
+    for (u32 k = f; k < e && pending; k += 4) {
+      if (LOW == 1) {
+        uint2 x[4];
+        uint2 const* r = reinterpret_cast<uint2 const*>(rows);
+#pragma unroll
+        for (u32 q = 0; q < 4; ++q) x[q] = k + q < e ? __ldg(r + k + q) : make_uint2(INV, INV);
+#pragma unroll
+        for (u32 q = 0; q < 4; ++q)
+#pragma unroll
+          for (u32 l = j; l < LPH; ++l)
+            if (found[l] == INV && t[l][0] == m && x[q].x == t[l][1]) found[l] = x[q].y;
+      } else {
+        uint4 x[4];
+        uint4 const* r = reinterpret_cast<uint4 const*>(rows);
+#pragma unroll
+        for (u32 q = 0; q < 4; ++q)
+          x[q] = k + q < e ? __ldg(r + k + q) : make_uint4(INV, INV, INV, INV);
+#pragma unroll
+        for (u32 q = 0; q < 4; ++q)
+#pragma unroll
+          for (u32 l = j; l < LPH; ++l)
+            if (found[l] == INV && t[l][0] == m && x[q].x == t[l][1] && x[q].y == t[l][2])
+              found[l] = x[q].z;
+      }
+      pending = false;
+#pragma unroll
+      for (u32 l = j; l < LPH; ++l) pending = pending || (found[l] == INV && t[l][0] == m);
     }
   }
-  u32 found = INV;
-  if (low == 1) {
-    u32 want = w[1 - best];
-    for (u32 r = f; r < e; ++r)
-      if (other[r] == want) {
-        found = lv_adj[r];
-        break;
-      }
-  } else {
-    u32 a = w[best == 0 ? 1 : 0], b = w[best == 2 ? 1 : 2];
-    uint2 const* o2 = reinterpret_cast<uint2 const*>(other);
-    for (u32 r = f; r < e; ++r) {
-      uint2 o = o2[r];
-      if ((o.x == a && o.y == b) || (o.x == b && o.y == a)) {
-        found = lv_adj[r];
-        break;
-      }
-    }
-  }
-  out[idx] = found;
+#pragma unroll
+  for (u32 j = 0; j < LPH; ++j) out[(size_t)i * LPH + j] = found[j];
 }
 
 // ---------------------------------------------------------------------------
@@ -844,27 +847,42 @@ u32 const* Mesh::ask_down(u32 high, u32 low)
   } else if (low > 0) {
     u32 nh = count(high);
     u32 const* voh = ask_down(high, 0);
-    UpAdj const& lv = ask_up(0, low, false);
     u32 const* vol = ask_down(low, 0);
+    u32 nl = counts[low];
     u32 n = nh * deg(high, low);
     u32* out = dalloc<u32>(n, s);
-    if (!up_other[low]) {
-      u32 nuse = counts[low] * deg(low, 0);
-      up_other[low] = dalloc<u32>((size_t)nuse * low, s);
-      if (nuse) {
-        k_other_verts<<<grid_for(nuse), BLOCK, 0, s>>>(low, nuse, lv.adj, lv.dirs, vol,
-            up_other[low]);
+    if (!low_rows[low]) {
+      u32 nv = counts[0];
+      u32* cnt = dalloc<u32>((size_t)nv + 1, s);
+      CK(cudaMemsetAsync(cnt, 0, sizeof(u32) * ((size_t)nv + 1), s));
+      if (nl) {
+        k_count_min_vert<<<grid_for(nl), BLOCK, 0, s>>>(low, nl, vol, cnt);
         CK_LAUNCH();
       }
+      low_row_offs[low] = exscan_new(cnt, nv, s);
+      CK(cudaMemsetAsync(cnt, 0, sizeof(u32) * ((size_t)nv + 1), s));
+      low_rows[low] = dalloc<u32>((size_t)nl * (low == 1 ? 2 : 4), s);
+      if (nl) {
+        k_fill_min_vert<<<grid_for(nl), BLOCK, 0, s>>>(low, nl, vol, low_row_offs[low], cnt,
+            low_rows[low]);
+        CK_LAUNCH();
+      }
+      dev_free(cnt, s);
     }
     if (n) {
-      // voh once, the vertices' upward CSR (offsets, ids, other vertices)
-      // once, out once
-      double nl = counts[low], nuse = (double)nl * deg(low, 0);
+      // voh once, the row offsets and every row record once, out once
+      double nld = nl, rec = low == 1 ? 8.0 : 16.0;
       PROBE(P_REFLECT_DOWN, s, 4.0 * deg(high, 0) * nh + 4.0 * (counts[0] + 1.0) +
-          4.0 * nuse + 4.0 * low * nuse + 4.0 * n);
-      k_reflect_rows<<<grid_for(n), BLOCK, 0, s>>>(high, low, nh, voh, lv.offs, lv.adj,
-          up_other[low], out);
+          rec * nld + 4.0 * n);
+      if (high == 3 && low == 2)
+        k_reflect_grouped<3, 2><<<grid_for(nh), BLOCK, 0, s>>>(nh, voh, low_row_offs[low],
+            low_rows[low], out);
+      else if (high == 3)
+        k_reflect_grouped<3, 1><<<grid_for(nh), BLOCK, 0, s>>>(nh, voh, low_row_offs[low],
+            low_rows[low], out);
+      else
+        k_reflect_grouped<2, 1><<<grid_for(nh), BLOCK, 0, s>>>(nh, voh, low_row_offs[low],
+            low_rows[low], out);
       CK_LAUNCH();
     }
     down[high][low] = out;
@@ -918,11 +936,6 @@ UpAdj const& Mesh::ask_up(u32 low, u32 high, bool sorted)
     if (sorted && !up_sorted[low][high]) {
       sort_up_rows(high, low, counts[high], counts[low], up[low][high], s);
       up_sorted[low][high] = true;
-      // reflect_down's cached rows follow the old row order
-      if (low == 0 && high < 3) {
-        dev_free(up_other[high], s);
-        up_other[high] = nullptr;
-      }
     }
     return up[low][high];
   }

@@ -75,9 +75,11 @@ struct Mesh {
   Graph star[4][4] = {};
   bool have_star[4][4] = {};
   u32* dual = nullptr;
-  // per use of up(0,1): the edge's other vertex; per use of up(0,2): the
-  // triangle's other two vertices in its cyclic order (reflect_down's rows)
-  u32* up_other[3] = {nullptr, nullptr, nullptr};
+  // reflect_down's search rows: every edge (1) / triangle (2) listed once, in
+  // the row of its smallest vertex, as (other vertices..., id) records:
+  // uint2 {v1, id} for edges, uint4 {v1, v2, id, 0} for triangles
+  u32* low_row_offs[3] = {nullptr, nullptr, nullptr};
+  u32* low_rows[3] = {nullptr, nullptr, nullptr};
   std::vector<Tag> tags[4];
   u64* globals[4] = {};
   u32* own_ranks[4] = {};   // cached zeros (single rank), API only
