@@ -357,7 +357,13 @@ def e2e_leg(G, L, base, args, world, stream, stream_ptr):
 # batched workload: 512 box meshes of uneven sizes
 
 BATCH_CHUNK_EST_TETS = 60e6     # estimated output tets per adapt_batch call
-BATCH_UNION_ELEMS = 400000      # input elements per union inside a call
+BATCH_UNION_ELEMS = 1000000     # current elements per union inside a call
+
+
+def batch_times(L):
+    c, p, s = C.c_double(), C.c_double(), C.c_double()
+    L.osh_b200_batch_times(C.byref(c), C.byref(p), C.byref(s))
+    return {"concat": round(c.value, 3), "passes": round(p.value, 3), "split": round(s.value, 3)}
 
 
 def batched_chunks(jobs):
@@ -414,7 +420,10 @@ def run_batched(args, world, rank, local):
             L.osh_free(hs[i])
         return digests, elems
 
+    batch_secs = {}
+
     def batch_leg(hs, chunk_list):
+        batch_secs.clear()
         digests, elems, unions, upasses = {}, 0.0, 0, 0
         for idx in chunk_list:
             arr = (C.c_void_p * len(idx))(*[hs[i] for i in idx])
@@ -429,6 +438,8 @@ def run_batched(args, world, rank, local):
             elems += e.value
             unions += u.value
             upasses += up.value
+            for k, v in batch_times(L).items():
+                batch_secs[k] = round(batch_secs.get(k, 0.0) + v, 3)
             for i in idx:
                 digests[i] = L.osh_b200_digest(hs[i])
                 L.osh_free(hs[i])
@@ -493,6 +504,7 @@ def run_batched(args, world, rank, local):
         "speedup_vs_plain": round(plain_ms / batch_ms, 3),
         "identical_to_plain": bool(same and abs(pe - be) < 0.5),
         "elems_in": be, "unions": unions, "union_passes": upasses,
+        "union_secs": batch_secs,
         "gpu_launches": int(batch_launches), "clocks": clk,
         "prep_s": round(prep_s, 1),
     }
@@ -532,11 +544,14 @@ def run_serving(args, world, rank, local):
     ids = {}
     nxt = 0
     remaining = 0
+    submit_secs = 0.0
     active_samples = []
     while nxt < len(jobs) or remaining > 0:
         now = time.perf_counter() - t0
         while nxt < len(jobs) and jobs[nxt].arrival <= now:
+            ts = time.perf_counter()
             ids[sv.submit(*inputs[nxt])] = nxt
+            submit_secs += time.perf_counter() - ts
             nxt += 1
         if sv.stats()["queued"] + sv.stats()["active"] > 0:
             remaining = sv.step()
@@ -578,6 +593,10 @@ def run_serving(args, world, rank, local):
                        "max": round(float(lat[-1]) * 1e3, 2)},
         "mean_active_jobs": round(float(np.mean(active_samples)), 2) if active_samples else 0,
         "server_steps": st["steps"], "elems_in": elems,
+        "server_secs": {k: round(st[k], 3) for k in
+                        ("secs_admit", "secs_join", "secs_passes", "secs_retire")},
+        "submit_secs": round(submit_secs, 3),
+        "union_secs": batch_times(L),
         "gpu_launches": int(launches), "clocks": clk,
     }
 

@@ -75,6 +75,9 @@ int osh_b200_adapt_batch(osh_t* meshes, unsigned nmeshes, double size_ratio_floo
    (summed over meshes) and the elements entering those passes */
 void osh_b200_batch_stats(unsigned* unions, unsigned* steps, unsigned* union_passes,
     unsigned* mesh_passes, double* elems_in) OSH_PUBLIC;
+/* host seconds of the last osh_b200_adapt_batch on this thread (and of the
+   serving steps since) spent forming unions, in passes, splitting meshes out */
+void osh_b200_batch_times(double* concat, double* passes, double* split) OSH_PUBLIC;
 /* per-mesh statistics of the last osh_b200_adapt_batch on this thread, for
    mesh i of that call: passes that changed it and the elements entering them */
 void osh_b200_batch_mesh_stats(unsigned i, unsigned* passes, double* elems_in) OSH_PUBLIC;
@@ -102,6 +105,10 @@ void osh_b200_server_free(osh_b200_server_t sv) OSH_PUBLIC;
 int osh_b200_server_submit(osh_b200_server_t sv, unsigned dim, unsigned nverts,
     double const* coords, unsigned nelems, unsigned const* conn,
     double const* size) OSH_PUBLIC;
+/* largest batch one pass forms, in current elements (default 4e6; 0 = no
+   limit): larger batches need fewer launches, smaller ones gather from L2 */
+void osh_b200_server_set_union_elems(osh_b200_server_t sv,
+    unsigned long long max_elems) OSH_PUBLIC;
 /* admit, run one step over every resident job, retire finished jobs;
    returns the number of jobs queued or running, or -1 on error */
 int osh_b200_server_step(osh_b200_server_t sv) OSH_PUBLIC;
@@ -117,6 +124,10 @@ int osh_b200_server_job_info(osh_b200_server_t sv, unsigned id, double* t_submit
     int* status) OSH_PUBLIC;
 void osh_b200_server_stats(osh_b200_server_t sv, unsigned* steps, unsigned* active,
     unsigned* queued, unsigned long long* reserved_bytes, double* now) OSH_PUBLIC;
+/* host seconds spent so far admitting jobs (upload and classification),
+   joining them to the running batch, in passes, and retiring finished jobs */
+void osh_b200_server_times(osh_b200_server_t sv, double* admit, double* join,
+    double* passes, double* retire) OSH_PUBLIC;
 
 /* ---- per-stage selections of one pass, without changing the mesh ------ */
 /* Layouts follow refine_by_size / coarsen_common / swap_common: every output

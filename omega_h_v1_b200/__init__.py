@@ -134,17 +134,20 @@ def lib():
       C.c_uint, C.c_uint, C.c_ulonglong, C.POINTER(C.c_uint), C.POINTER(C.c_int))
     f("osh_b200_batch_stats", None, *([C.POINTER(C.c_uint)] * 4), C.POINTER(C.c_double))
     f("osh_b200_batch_mesh_stats", None, C.c_uint, C.POINTER(C.c_uint), C.POINTER(C.c_double))
+    f("osh_b200_batch_times", None, *([C.POINTER(C.c_double)] * 3))
     f("osh_b200_digest", C.c_ulonglong, vp)
     f("osh_b200_server_new", vp, C.c_double, C.c_double, C.c_uint, C.c_uint, C.c_ulonglong)
     f("osh_b200_server_free", None, vp)
     f("osh_b200_server_submit", C.c_int, vp, C.c_uint, C.c_uint, _f64p, C.c_uint, _u32p, _f64p)
     f("osh_b200_server_step", C.c_int, vp)
+    f("osh_b200_server_set_union_elems", None, vp, C.c_ulonglong)
     f("osh_b200_server_poll", C.c_uint, vp, C.POINTER(C.c_uint), C.c_uint)
     f("osh_b200_server_take", vp, vp, C.c_uint)
     f("osh_b200_server_job_info", C.c_int, vp, C.c_uint, *([C.POINTER(C.c_double)] * 3),
       C.POINTER(C.c_uint), C.POINTER(C.c_double), C.POINTER(C.c_int))
     f("osh_b200_server_stats", None, vp, *([C.POINTER(C.c_uint)] * 3),
       C.POINTER(C.c_ulonglong), C.POINTER(C.c_double))
+    f("osh_b200_server_times", None, vp, *([C.POINTER(C.c_double)] * 4))
     f("osh_b200_launch_count", C.c_ulonglong)
     f("osh_b200_sync_count", C.c_ulonglong)
     f("osh_b200_probe_enable", None, C.c_uint)
@@ -477,6 +480,10 @@ class Server:
             check()
         return r
 
+    def set_union_elems(self, n):
+        self.L.osh_b200_server_set_union_elems(self.h, int(n))
+        check()
+
     def step(self):
         r = self.L.osh_b200_server_step(self.h)
         if r < 0:
@@ -510,8 +517,11 @@ class Server:
         self.L.osh_b200_server_stats(self.h, C.byref(steps), C.byref(active), C.byref(queued),
                                      C.byref(res), C.byref(now))
         check()
+        a, j, p, r = (C.c_double() for _ in range(4))
+        self.L.osh_b200_server_times(self.h, C.byref(a), C.byref(j), C.byref(p), C.byref(r))
         return dict(steps=steps.value, active=active.value, queued=queued.value,
-                    reserved=res.value, now=now.value)
+                    reserved=res.value, now=now.value, secs_admit=a.value, secs_join=j.value,
+                    secs_passes=p.value, secs_retire=r.value)
 
     def close(self):
         if self.h:

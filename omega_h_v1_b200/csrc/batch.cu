@@ -12,6 +12,7 @@
 // with vertex ids renumbered to the mesh's local numbering.
 #include <algorithm>
 #include <cfloat>
+#include <chrono>
 
 #include "batch.hpp"
 
@@ -157,9 +158,11 @@ __global__ void k_scatter_meshes(u32 n, u32 width, T const* __restrict__ in,
   for (u64 j = blockIdx.x * (u64)blockDim.x + threadIdx.x; j < total;
        j += (u64)gridDim.x * blockDim.x) {
     u32 i = (u32)(j / width), k = (u32)(j - (u64)i * width);
+    T* d = dst[es[i]];
+    if (!d) continue;  // a segment the caller does not want back
     T v = in[j];
     if (vloc) v = (T)vloc[(u32)v];
-    dst[es[i]][(u64)local[i] * width + k] = v;
+    d[(u64)local[i] * width + k] = v;
   }
 }
 
@@ -168,7 +171,9 @@ __global__ void k_scatter_iota64(u32 n, u32 const* __restrict__ es,
     u32 const* __restrict__ local, u64* const* __restrict__ dst)
 {
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) dst[es[i]][local[i]] = local[i];
+  if (i >= n) return;
+  u64* d = dst[es[i]];
+  if (d) d[local[i]] = local[i];
 }
 
 // per-segment minimum of element qualities (order-preserving keys)
@@ -264,17 +269,30 @@ void launch_scatter(u32 n, u32 width, void const* in, u32 const* es, u32 const* 
   CK_LAUNCH();
 }
 
+// Element coordinates are a by-product of collapses (coarsen_transfer adds
+// them to the new mesh); every pass recomputes or drops them, so a union
+// leaves them out and a mesh leaving it gets them back if its own passes
+// would have left them.
+bool skipped_tag(Mesh const& m, u32 d, Tag const& t)
+{
+  return d == m.dim && t.name == "coordinates";
+}
+
 // the same tags (names, types, widths) on dimension d, in any order; the
 // transfer kind may differ (refinement resets it on vertex fields), each
 // mesh's own is restored when it leaves the union
 bool same_tags(Mesh& a, Mesh& b, u32 d)
 {
-  if (a.tags[d].size() != b.tags[d].size()) return false;
+  size_t na = 0, nb = 0;
   for (Tag const& x : a.tags[d]) {
+    if (skipped_tag(a, d, x)) continue;
+    ++na;
     Tag const* y = b.find_tag(d, x.name.c_str());
     if (!y || x.type != y->type || x.ncomps != y->ncomps) return false;
   }
-  return true;
+  for (Tag const& y : b.tags[d])
+    if (!skipped_tag(b, d, y)) ++nb;
+  return na == nb;
 }
 
 }  // namespace
@@ -282,6 +300,28 @@ bool same_tags(Mesh& a, Mesh& b, u32 d)
 Mesh* concat_meshes(std::vector<Mesh*> const& ms)
 {
   return concat_meshes(ms, nullptr);
+}
+
+void check_batchable(std::vector<Mesh*> const& ms)
+{
+  if (ms.empty()) throw Failure(E_ARG, "a batch needs at least one mesh");
+  Mesh& a = *ms[0];
+  u32 dim = a.dim;
+  for (Mesh* m : ms) {
+    if (m->dim != dim || m->full != a.full || m->parallel != a.parallel)
+      throw Failure(E_ARG, "batched meshes differ in dimension, representation or parallelism");
+    if (!m->full) throw Failure(E_ARG, "batched meshes need the full representation");
+    for (Tag const& t : m->tags[0])
+      if (t.type != T_F64 && t.name != "class_dim" && t.name != "class_id")
+        throw Failure(E_ARG, "batched meshes may carry only f64 fields and class labels on "
+                             "vertices (refinement drops other vertex tags)");
+    for (u32 d = 0; d <= dim; ++d) {
+      if (m->has_dim(d) != a.has_dim(d) || !same_tags(*m, a, d))
+        throw Failure(E_ARG, "batched meshes differ in their entities or tags");
+      if (a.parallel && (m->globals[d] == nullptr) != (a.globals[d] == nullptr))
+        throw Failure(E_ARG, "batched meshes differ in their global numbers");
+    }
+  }
 }
 
 Mesh* concat_meshes(std::vector<Mesh*> const& ms, cudaStream_t stream)
@@ -336,6 +376,10 @@ Mesh* concat_meshes(std::vector<Mesh*> const& ms, cudaStream_t stream)
         conn_at[d] = meta.add(p.data(), nm);
       }
       for (size_t t = 0; t < a.tags[d].size(); ++t) {
+        if (skipped_tag(a, d, a.tags[d][t])) {
+          tag_at[d].push_back(0);
+          continue;
+        }
         for (u32 k = 0; k < nm; ++k) p[k] = ms[k]->find_tag(d, a.tags[d][t].name.c_str())->data;
         tag_at[d].push_back(meta.add(p.data(), nm));
       }
@@ -366,6 +410,7 @@ Mesh* concat_meshes(std::vector<Mesh*> const& ms, cudaStream_t stream)
       u->set_ents(d, n, conn);
       for (size_t t = 0; t < a.tags[d].size(); ++t) {
         Tag const& tg = a.tags[d][t];
+        if (skipped_tag(a, d, tg)) continue;
         u32 esz = tag_esz(tg.type);
         void* data = dev_alloc((size_t)n * tg.ncomps * esz, s);
         u64 total = (u64)n * tg.ncomps;
@@ -405,6 +450,11 @@ Mesh* concat_meshes(std::vector<Mesh*> const& ms, cudaStream_t stream)
 
 std::vector<Mesh*> split_union(Mesh& u, cudaStream_t stream)
 {
+  return split_union(u, stream, nullptr);
+}
+
+std::vector<Mesh*> split_union(Mesh& u, cudaStream_t stream, std::vector<char> const* want)
+{
   cudaStream_t s = u.s;
   u32 nm = u.nseg, dim = u.dim;
   if (!u.seg) throw Failure(E_ARG, "mesh is not a union of meshes");
@@ -413,7 +463,8 @@ std::vector<Mesh*> split_union(Mesh& u, cudaStream_t stream)
   u32* local[4] = {};
   std::vector<u32> counts[4];
   try {
-    for (u32 k = 0; k < nm; ++k) out[k] = new Mesh(dim, u.full, u.parallel, stream, u.mb);
+    for (u32 k = 0; k < nm; ++k)
+      if (!want || (*want)[k]) out[k] = new Mesh(dim, u.full, u.parallel, stream, u.mb);
     // stable counting sort of every dimension's entities by segment
     for (u32 d = 0; d <= dim; ++d) {
       if (!u.has_dim(d)) continue;
@@ -475,6 +526,8 @@ std::vector<Mesh*> split_union(Mesh& u, cudaStream_t stream)
       if (d) {
         u32 vpe = deg(d, 0);
         for (u32 k = 0; k < nm; ++k) {
+          p[k] = nullptr;
+          if (!out[k]) continue;
           u32 nk = counts[d][k + 1];
           u32* conn = dalloc<u32>((size_t)nk * vpe, s);
           out[k]->set_ents(d, nk, conn);
@@ -482,10 +535,13 @@ std::vector<Mesh*> split_union(Mesh& u, cudaStream_t stream)
         }
         conn_at[d] = meta.add(p.data(), nm);
       } else {
-        for (u32 k = 0; k < nm; ++k) out[k]->set_ents(0, counts[0][k + 1], nullptr);
+        for (u32 k = 0; k < nm; ++k)
+          if (out[k]) out[k]->set_ents(0, counts[0][k + 1], nullptr);
       }
       for (Tag const& t : u.tags[d]) {
         for (u32 k = 0; k < nm; ++k) {
+          p[k] = nullptr;
+          if (!out[k]) continue;
           u32 nk = counts[d][k + 1];
           void* data = dev_alloc((size_t)nk * t.ncomps * tag_esz(t.type), s);
           out[k]->add_tag(d, t.type, t.name.c_str(), t.ncomps, t.transfer, data);
@@ -495,6 +551,8 @@ std::vector<Mesh*> split_union(Mesh& u, cudaStream_t stream)
       }
       if (u.parallel && u.globals[d]) {
         for (u32 k = 0; k < nm; ++k) {
+          p[k] = nullptr;
+          if (!out[k]) continue;
           u64* g = dalloc<u64>(counts[d][k + 1], s);
           out[k]->set_globals(d, g);
           p[k] = g;
@@ -638,38 +696,62 @@ void UnionCtl::run(u32 op, std::vector<u32> const& group, std::vector<double> co
   last_batch_stats().union_passes += 1;
 }
 
-bool union_step(UnionCtl& c, std::vector<SegState>& st, AdaptParams const& ap)
+namespace {
+
+double wall_s()
 {
-  Mesh& u = c.u;
-  u32 nm = c.nm;
+  using namespace std::chrono;
+  return duration<double>(steady_clock::now().time_since_epoch()).count();
+}
+
+// consecutive runs of `idx` whose current elements sum to at most `max`
+// (0 = no limit); each run holds at least one mesh
+std::vector<std::vector<u32>> chunks_of(std::vector<Mesh*>& ms, std::vector<u32> const& idx,
+    unsigned long long max)
+{
+  std::vector<std::vector<u32>> out;
+  std::vector<u32> cur;
+  unsigned long long sum = 0;
+  for (u32 k : idx) {
+    unsigned long long ne = ms[k]->count(ms[k]->dim);
+    if (!cur.empty() && max && sum + ne > max) {
+      out.push_back(cur);
+      cur.clear();
+      sum = 0;
+    }
+    cur.push_back(k);
+    sum += ne;
+  }
+  if (!cur.empty()) out.push_back(cur);
+  return out;
+}
+
+}  // namespace
+
+bool GroupRunner::step(std::vector<Mesh*>& ms, std::vector<SegState>& st,
+    std::vector<char>& owned)
+{
   BatchStats& bs = last_batch_stats();
+  u32 n = (u32)ms.size();
   bool live = false;
-  for (u32 k = 0; k < nm; ++k) live = live || st[k].state < ST_DONE;
+  for (u32 k = 0; k < n; ++k) live = live || st[k].state < ST_DONE;
   if (!live) return false;
   bs.steps += 1;
-  // satisfy_size's floor (adapt.cpp:47-52), once per mesh on its first step
-  bool fresh = false;
-  for (u32 k = 0; k < nm; ++k) fresh = fresh || st[k].state == ST_INIT;
-  if (fresh) {
-    std::vector<double> mq = c.min_quality();
-    for (u32 k = 0; k < nm; ++k)
-      if (st[k].state == ST_INIT) {
-        st[k].qf = mq[k];
-        if (ap.good_qual < st[k].qf) st[k].qf = ap.good_qual;
-        st[k].state = ST_REFINE;
-      }
-  }
-  std::vector<double> qf(nm);
-  for (u32 k = 0; k < nm; ++k) qf[k] = st[k].qf;
-  u32 cur_op = 0;
+  auto group = [&](u32 state) {
+    std::vector<u32> g;
+    for (u32 k = 0; k < n; ++k)
+      if (st[k].state == state) g.push_back(k);
+    return g;
+  };
   // incr_op_count (adapt.cpp:36-45) for mesh k after a pass that changed it
-  auto counted = [&](u32 k) {
+  auto counted = [&](u32 k, u32 op, u32 elems) {
     BatchMeshResult& r = st[k].res;
-    r.ops.push_back(cur_op);
+    r.ops.push_back(op);
     r.passes += 1;
-    r.elems_in += c.h_u32[nm + k];
+    r.changed = 1;
+    r.elems_in += elems;
     bs.mesh_passes += 1;
-    bs.elems_in += c.h_u32[nm + k];
+    bs.elems_in += elems;
     if (st[k].ops > ap.max_ops) {
       r.status = E_MAXOPS;
       st[k].state = ST_FAILED;
@@ -677,84 +759,167 @@ bool union_step(UnionCtl& c, std::vector<SegState>& st, AdaptParams const& ap)
     }
     ++st[k].ops;
   };
-  auto members = [&](u32 state) {
-    std::vector<u32> g;
-    for (u32 k = 0; k < nm; ++k)
-      if (st[k].state == state) g.push_back(k);
-    return g;
+  auto replace = [&](u32 k, Mesh* m) {
+    if (owned[k]) delete ms[k];
+    ms[k] = m;
+    owned[k] = 1;
   };
-  // satisfy_size: refine while it changes the mesh, then coarsen
-  std::vector<u32> g = members(ST_REFINE);
-  if (!g.empty()) {
-    cur_op = OP_REFINE;
-    c.run(OP_REFINE, g, qf, ap.size_floor, ap.good_qual, ap.nlayers);
-    for (u32 k : g)
-      if (c.h_u32[k])
-        counted(k);
-      else
-        st[k].state = ST_COARSEN;
+  // a union of the meshes c; a lone mesh is its own union of one segment,
+  // changed in place by the pass with nothing to copy in or out
+  auto gather = [&](std::vector<u32> const& c) {
+    if (c.size() == 1) {
+      Mesh* m = ms[c[0]];
+      if (!m->seg) {
+        u32 nv = m->count(0);
+        m->seg = dalloc<u32>(nv ? nv : 1, m->s);
+        CK(cudaMemsetAsync(m->seg, 0, sizeof(u32) * (nv ? nv : 1), m->s));
+        m->nseg = 1;
+      }
+      return m;
+    }
+    std::vector<Mesh*> parts;
+    for (u32 k : c) parts.push_back(ms[k]);
+    bs.unions += 1;
+    double t = wall_s();
+    Mesh* u = concat_meshes(parts, s);
+    stream_sync(s);
+    bs.secs_concat += wall_s() - t;
+    return u;
+  };
+  auto release = [&](Mesh* u, std::vector<u32> const& c) {
+    if (c.size() != 1) delete u;
+  };
+  auto split = [&](Mesh& u, std::vector<char> const& want) {
+    double t = wall_s();
+    std::vector<Mesh*> o = split_union(u, s, &want);
+    bs.secs_split += wall_s() - t;
+    return o;
+  };
+  // satisfy_size's floor (adapt.cpp:47-52), once per mesh
+  for (auto const& c : chunks_of(ms, group(ST_INIT), max_union_elems)) {
+    Mesh* u = gather(c);
+    std::vector<double> mq;
+    try {
+      UnionCtl ctl(*u);
+      mq = ctl.min_quality();
+    } catch (...) {
+      release(u, c);
+      throw;
+    }
+    release(u, c);
+    for (u32 j = 0; j < c.size(); ++j) {
+      SegState& x = st[c[j]];
+      x.qf = mq[j];
+      if (ap.good_qual < x.qf) x.qf = ap.good_qual;
+      x.state = ST_REFINE;
+    }
   }
-  g = members(ST_COARSEN);
-  if (!g.empty()) {
-    cur_op = OP_COARSEN;
-    c.run(OP_COARSEN, g, qf, ap.size_floor, ap.good_qual, ap.nlayers);
-    for (u32 k : g)
-      if (c.h_u32[k])
-        counted(k);
-      else
-        st[k].state = ST_SHAPE;
+  // satisfy_size: refine while it changes a mesh, then coarsen
+  for (u32 op : {OP_REFINE, OP_COARSEN}) {
+    u32 here = op == OP_REFINE ? ST_REFINE : ST_COARSEN;
+    u32 next = op == OP_REFINE ? ST_COARSEN : ST_SHAPE;
+    for (auto const& c : chunks_of(ms, group(here), max_union_elems)) {
+      Mesh* u = gather(c);
+      u32 m = (u32)c.size();
+      std::vector<u32> sel(m), elems(m), all(m);
+      std::vector<double> qf(m);
+      for (u32 j = 0; j < m; ++j) {
+        all[j] = j;
+        qf[j] = st[c[j]].qf;
+      }
+      std::vector<Mesh*> outs;
+      try {
+        {
+          double t = wall_s();
+          UnionCtl ctl(*u);
+          ctl.run(op, all, qf, ap.size_floor, ap.good_qual, ap.nlayers);
+          bs.secs_passes += wall_s() - t;
+          for (u32 j = 0; j < m; ++j) {
+            sel[j] = ctl.h_u32[j];
+            elems[j] = ctl.h_u32[m + j];
+          }
+        }
+        if (m > 1) {
+          std::vector<char> want(m);
+          for (u32 j = 0; j < m; ++j) want[j] = sel[j] ? 1 : 0;
+          outs = split(*u, want);
+        }
+      } catch (...) {
+        release(u, c);
+        throw;
+      }
+      release(u, c);
+      for (u32 j = 0; j < m; ++j) {
+        u32 k = c[j];
+        if (sel[j]) {
+          counted(k, op, elems[j]);
+          if (m > 1) replace(k, outs[j]);
+        } else {
+          st[k].state = next;
+        }
+      }
+    }
   }
   // satisfy_shape (adapt.cpp:58-80): swap, else collapse slivers
-  g = members(ST_SHAPE);
-  if (!g.empty()) {
-    std::vector<double> mq = c.min_quality();
-    std::vector<u32> g2;
-    for (u32 k : g)
-      if (mq[k] >= ap.good_qual)
-        st[k].state = ST_DONE;
-      else
-        g2.push_back(k);
-    std::vector<u32> g3;
-    if (u.dim == 3 && !g2.empty()) {
-      cur_op = OP_SWAP;
-      c.run(OP_SWAP, g2, qf, ap.size_floor, ap.good_qual, ap.nlayers);
-      for (u32 k : g2)
-        if (c.h_u32[k])
-          counted(k);
+  for (auto const& c : chunks_of(ms, group(ST_SHAPE), max_union_elems)) {
+    Mesh* u = gather(c);
+    u32 m = (u32)c.size();
+    std::vector<char> changed(m, 0);
+    std::vector<Mesh*> outs;
+    try {
+      double t = wall_s();
+      UnionCtl ctl(*u);
+      std::vector<double> mq = ctl.min_quality(), qf(m, 0.0);
+      std::vector<u32> g2, g3;
+      for (u32 j = 0; j < m; ++j)
+        if (mq[j] >= ap.good_qual)
+          st[c[j]].state = ST_DONE;
         else
-          g3.push_back(k);
-    } else {
-      g3 = g2;
+          g2.push_back(j);
+      if (u->dim == 3 && !g2.empty()) {
+        ctl.run(OP_SWAP, g2, qf, ap.size_floor, ap.good_qual, ap.nlayers);
+        for (u32 j : g2)
+          if (ctl.h_u32[j]) {
+            counted(c[j], OP_SWAP, ctl.h_u32[m + j]);
+            changed[j] = 1;
+          } else {
+            g3.push_back(j);
+          }
+      } else {
+        g3 = g2;
+      }
+      if (!g3.empty()) {
+        ctl.run(OP_CSLIVERS, g3, qf, ap.size_floor, ap.good_qual, ap.nlayers);
+        for (u32 j : g3)
+          if (ctl.h_u32[j]) {
+            counted(c[j], OP_CSLIVERS, ctl.h_u32[m + j]);
+            changed[j] = 1;
+          } else {
+            st[c[j]].state = ST_DONE;  // shape quality could not be satisfied
+          }
+      }
+      bs.secs_passes += wall_s() - t;
+    } catch (...) {
+      release(u, c);
+      throw;
     }
-    if (!g3.empty()) {
-      cur_op = OP_CSLIVERS;
-      c.run(OP_CSLIVERS, g3, qf, ap.size_floor, ap.good_qual, ap.nlayers);
-      for (u32 k : g3)
-        if (c.h_u32[k])
-          counted(k);
-        else
-          st[k].state = ST_DONE;  // shape quality could not be satisfied
+    bool any = false;
+    for (char x : changed) any = any || x;
+    if (any && m > 1) {
+      try {
+        outs = split(*u, changed);
+      } catch (...) {
+        release(u, c);
+        throw;
+      }
+      for (u32 j = 0; j < m; ++j)
+        if (changed[j]) replace(c[j], outs[j]);
     }
+    release(u, c);
   }
-  for (u32 k = 0; k < nm; ++k) st[k].res.changed = st[k].res.passes > 0;
   live = false;
-  for (u32 k = 0; k < nm; ++k) live = live || st[k].state < ST_DONE;
+  for (u32 k = 0; k < n; ++k) live = live || st[k].state < ST_DONE;
   return live;
-}
-
-void adapt_union(Mesh& u, double size_floor, double good_qual, u32 nlayers, u32 max_ops,
-    std::vector<BatchMeshResult>& res)
-{
-  u32 nm = u.nseg;
-  res.assign(nm, BatchMeshResult());
-  if (!nm) return;
-  last_batch_stats().unions += 1;
-  UnionCtl c(u);
-  std::vector<SegState> st(nm);
-  AdaptParams ap{size_floor, good_qual, nlayers, max_ops};
-  while (union_step(c, st, ap)) {
-  }
-  for (u32 k = 0; k < nm; ++k) res[k] = st[k].res;
 }
 
 // ---------------------------------------------------------------------------
@@ -945,48 +1110,59 @@ void apply_layout(Mesh& m, Layout const& want)
   }
 }
 
+void drop_segments(Mesh& m)
+{
+  dev_free(m.seg, m.s);
+  m.seg = nullptr;
+  m.nseg = 0;
+}
+
 void adapt_batch(std::vector<Mesh*> const& ms, double size_floor, double good_qual,
     u32 nlayers, u32 max_ops, unsigned long long max_union_elems,
     std::vector<BatchMeshResult>& res)
 {
   last_batch_stats() = BatchStats();
-  res.assign(ms.size(), BatchMeshResult());
-  size_t i = 0;
-  while (i < ms.size()) {
-    // the next union: consecutive meshes up to max_union_elems input elements
-    size_t j = i;
-    unsigned long long sum = 0;
-    while (j < ms.size()) {
-      unsigned long long ne = ms[j]->count(ms[j]->dim);
-      if (j > i && max_union_elems && sum + ne > max_union_elems) break;
-      sum += ne;
-      ++j;
+  u32 n = (u32)ms.size();
+  res.assign(n, BatchMeshResult());
+  if (!n) return;
+  check_batchable(ms);
+  for (Mesh* m : ms) stream_sync(m->s);
+  GroupRunner run;
+  run.ap = AdaptParams{size_floor, good_qual, nlayers, max_ops};
+  run.max_union_elems = max_union_elems;
+  CK(cudaStreamCreateWithFlags(&run.s, cudaStreamNonBlocking));
+  std::vector<Mesh*> cur(ms.begin(), ms.end());
+  std::vector<char> owned(n, 0);
+  std::vector<SegState> st(n);
+  std::vector<Layout> start(n);
+  for (u32 k = 0; k < n; ++k) start[k] = layout_of(*ms[k]);
+  auto cleanup = [&]() {
+    for (u32 k = 0; k < n; ++k)
+      if (owned[k]) delete cur[k];
+    cudaStreamSynchronize(run.s);
+    cudaStreamDestroy(run.s);
+  };
+  try {
+    while (run.step(cur, st, owned)) {
     }
-    std::vector<Mesh*> group(ms.begin() + i, ms.begin() + j);
-    Mesh* u = concat_meshes(group, group[0]->s);
-    try {
-      Layout start = layout_of(*u);
-      std::vector<BatchMeshResult> r;
-      adapt_union(*u, size_floor, good_qual, nlayers, max_ops, r);
-      std::vector<Mesh*> outs = split_union(*u, u->s);
-      for (size_t k = 0; k < group.size(); ++k) {
-        res[i + k] = r[k];
-        if (r[k].passes) {
-          Layout want = start;
-          for (u32 op : r[k].ops) want = layout_after(op, want, u->dim);
-          apply_layout(*outs[k], want);
-          group[k]->overwrite(outs[k]);
-        } else {
-          delete outs[k];
-        }
-      }
-    } catch (...) {
-      delete u;
-      throw;
+    stream_sync(run.s);
+    for (u32 k = 0; k < n; ++k) {
+      res[k] = st[k].res;
+      drop_segments(*cur[k]);
+      if (!st[k].res.passes) continue;  // no pass changed this mesh
+      Layout want = start[k];
+      for (u32 op : st[k].res.ops) want = layout_after(op, want, ms[k]->dim);
+      apply_layout(*cur[k], want);
+      if (!owned[k]) continue;  // changed in place
+      stream_sync(cur[k]->s);
+      ms[k]->overwrite(cur[k]);
+      owned[k] = 0;
     }
-    delete u;
-    i = j;
+  } catch (...) {
+    cleanup();
+    throw;
   }
+  cleanup();
 }
 
 }  // namespace osh

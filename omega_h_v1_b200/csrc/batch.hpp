@@ -16,6 +16,11 @@ namespace osh {
 
 // one disjoint union of the meshes, on a stream of its own; every mesh must
 // have the same dimension, representation and tag list
+// forget the segment numbers of a mesh that leaves batched adaptation
+void drop_segments(Mesh& m);
+
+// throws E_ARG unless the meshes can share a union
+void check_batchable(std::vector<Mesh*> const& ms);
 Mesh* concat_meshes(std::vector<Mesh*> const& ms);
 Mesh* concat_meshes(std::vector<Mesh*> const& ms, cudaStream_t stream);
 
@@ -26,6 +31,8 @@ u64 mesh_digest(Mesh& m);
 // the meshes of a union, in segment order (new Mesh objects on `stream`,
 // or on streams of their own when stream is null)
 std::vector<Mesh*> split_union(Mesh& u, cudaStream_t stream);
+// only the segments k with (*want)[k] (the others come back as null)
+std::vector<Mesh*> split_union(Mesh& u, cudaStream_t stream, std::vector<char> const* want);
 
 struct BatchMeshResult {
   std::vector<u32> ops;  // the passes that changed this mesh, in order
@@ -41,6 +48,8 @@ struct BatchStats {
   u32 union_passes = 0;  // passes run over whole unions
   u32 mesh_passes = 0;   // passes that changed a mesh, summed over meshes
   double elems_in = 0;   // elements entering those passes, summed
+  // host seconds in forming unions, in passes, and in splitting meshes out
+  double secs_concat = 0, secs_passes = 0, secs_split = 0;
 };
 BatchStats& last_batch_stats();
 
@@ -90,8 +99,20 @@ struct UnionCtl {
       double size_floor, double good_qual, u32 nlayers);
 };
 
-// one step for every live segment; returns whether any is still live
-bool union_step(UnionCtl& c, std::vector<SegState>& st, AdaptParams const& ap);
+// Runs mesh_adapt's loop for many meshes held apart between passes: every
+// step gathers the meshes that are at the same point of their loop into
+// unions of at most max_union_elems current elements (0 = no limit), runs
+// that pass over each union (one launch per stage), and splits out the
+// meshes it changed. A union thus only holds meshes its pass acts on.
+struct GroupRunner {
+  AdaptParams ap{1.0 / 3.0, 0.3, 4, 50};
+  unsigned long long max_union_elems = 0;
+  cudaStream_t s = nullptr;  // unions and the meshes split out of them
+  // one step for every live mesh; ms[k] is replaced (and owned[k] set) when
+  // a pass changes it, the previous ms[k] deleted if it was owned. Returns
+  // whether any mesh is still live.
+  bool step(std::vector<Mesh*>& ms, std::vector<SegState>& st, std::vector<char>& owned);
+};
 
 // the tag list a mesh has after the passes `ops` (refine_build, coarsen_build
 // and swap_build keep, drop and order tags by fixed rules), applied to a mesh
@@ -103,13 +124,9 @@ Layout layout_of(Mesh& m);
 Layout layout_after(u32 op, Layout const& in, u32 dim);
 void apply_layout(Mesh& m, Layout const& want);
 
-// mesh_adapt of every segment of the union (in place)
-void adapt_union(Mesh& u, double size_floor, double good_qual, u32 nlayers, u32 max_ops,
-    std::vector<BatchMeshResult>& res);
-
-// mesh_adapt of every mesh in `ms`, adapted in unions of at most
-// `max_union_elems` input elements (0 = one union); each mesh that changed
-// is overwritten with its result
+// mesh_adapt of every mesh in `ms` through a GroupRunner with unions of at
+// most max_union_elems current elements (0 = no limit); each mesh that
+// changed is overwritten with its result
 void adapt_batch(std::vector<Mesh*> const& ms, double size_floor, double good_qual,
     u32 nlayers, u32 max_ops, unsigned long long max_union_elems,
     std::vector<BatchMeshResult>& res);

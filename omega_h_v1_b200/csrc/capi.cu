@@ -553,6 +553,14 @@ int osh_b200_server_submit(osh_b200_server_t sv, unsigned dim, unsigned nverts,
   API_CATCH(-1)
 }
 
+void osh_b200_server_set_union_elems(osh_b200_server_t sv, unsigned long long n)
+{
+  API_TRY
+  need(sv != nullptr, "server is NULL");
+  osh::server_set_union_elems(SV(sv), n);
+  API_CATCH_VOID
+}
+
 int osh_b200_server_step(osh_b200_server_t sv)
 {
   API_TRY
@@ -611,6 +619,19 @@ void osh_b200_server_stats(osh_b200_server_t sv, unsigned* steps, unsigned* acti
   API_CATCH_VOID
 }
 
+void osh_b200_server_times(osh_b200_server_t sv, double* admit, double* join,
+    double* passes, double* retire)
+{
+  API_TRY
+  need(sv != nullptr, "server is NULL");
+  osh::ServeStats r = osh::server_stats(SV(sv));
+  if (admit) *admit = r.secs_admit;
+  if (join) *join = r.secs_join;
+  if (passes) *passes = r.secs_passes;
+  if (retire) *retire = r.secs_retire;
+  API_CATCH_VOID
+}
+
 unsigned long long osh_b200_digest(osh_t h)
 {
   API_TRY
@@ -627,6 +648,14 @@ void osh_b200_batch_stats(unsigned* unions, unsigned* steps, unsigned* union_pas
   if (union_passes) *union_passes = b.union_passes;
   if (mesh_passes) *mesh_passes = b.mesh_passes;
   if (elems_in) *elems_in = b.elems_in;
+}
+
+void osh_b200_batch_times(double* concat, double* passes, double* split)
+{
+  osh::BatchStats const& b = osh::last_batch_stats();
+  if (concat) *concat = b.secs_concat;
+  if (passes) *passes = b.secs_passes;
+  if (split) *split = b.secs_split;
 }
 
 void osh_b200_batch_mesh_stats(unsigned i, unsigned* passes, double* elems_in)

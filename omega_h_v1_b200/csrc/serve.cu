@@ -32,7 +32,10 @@ double estimate_elements(u32 dim, u32 nv, double const* x, u32 ne, u32 const* co
 {
   double sum = 0;
   u32 vpe = dim + 1;
-  for (u32 i = 0; i < ne; ++i) {
+  // a strided sample of at most 4096 elements, scaled to all of them
+  u32 stride = ne > 4096 ? ne / 4096 : 1, taken = 0;
+  for (u32 i = 0; i < ne; i += stride) {
+    ++taken;
     u32 const* c = conn + (size_t)i * vpe;
     double hm = 0;
     for (u32 j = 0; j < vpe; ++j) hm += h[c[j]];
@@ -56,7 +59,7 @@ double estimate_elements(u32 dim, u32 nv, double const* x, u32 ne, u32 const* co
     if (ideal > 0) sum += meas / ideal;
   }
   (void)nv;
-  return sum;
+  return taken ? sum * ((double)ne / taken) : 0.0;
 }
 
 }  // namespace
@@ -76,36 +79,37 @@ struct ServeJob {
 };
 
 struct Server {
-  AdaptParams ap;
   unsigned long long budget = 0, reserved = 0;
   double t0 = 0;
-  cudaStream_t s = nullptr;
+  GroupRunner run;
   std::map<u32, std::unique_ptr<ServeJob>> jobs;
   std::deque<ServeJob*> queue;
-  std::vector<ServeJob*> active;  // segment order of `u`
-  std::vector<SegState> st;       // their loop states while they run
-  Mesh* u = nullptr;
-  std::unique_ptr<UnionCtl> ctl;
+  // resident jobs, each mesh held apart and regrouped per pass
+  std::vector<ServeJob*> active;
+  std::vector<Mesh*> ms;
+  std::vector<SegState> st;
+  std::vector<char> owned;
   u32 next_id = 0;
-  u32 steps = 0, rebuilds = 0;
+  u32 steps = 0, unions = 0;
+  double secs_admit = 0, secs_passes = 0, secs_retire = 0;
 
   ~Server()
   {
-    ctl.reset();
-    delete u;
+    for (size_t k = 0; k < ms.size(); ++k)
+      if (owned[k]) delete ms[k];
     jobs.clear();
-    if (s) {
-      cudaStreamSynchronize(s);
-      cudaStreamDestroy(s);
+    if (run.s) {
+      cudaStreamSynchronize(run.s);
+      cudaStreamDestroy(run.s);
     }
   }
 
-  void admit(std::vector<ServeJob*>& joining)
+  void admit()
   {
+    cudaStream_t s = run.s;
     while (!queue.empty()) {
       ServeJob* j = queue.front();
-      bool busy = !active.empty() || !joining.empty();
-      if (busy && reserved + j->est_bytes > budget) break;
+      if (!active.empty() && reserved + j->est_bytes > budget) break;
       queue.pop_front();
       reserved += j->est_bytes;
       Mesh* m = new Mesh(j->dim, false, false, s);
@@ -130,79 +134,63 @@ struct Server {
         delete m;
         throw;
       }
-      j->mesh = m;
       j->start = layout_of(*m);
       j->t_admit = now_s() - t0;
       // the host copy is no longer needed
       std::vector<double>().swap(j->coords);
       std::vector<double>().swap(j->size);
       std::vector<u32>().swap(j->conn);
-      joining.push_back(j);
+      active.push_back(j);
+      ms.push_back(m);
+      st.push_back(SegState());
+      owned.push_back(1);
     }
   }
 
   u32 step()
   {
-    std::vector<ServeJob*> joining;
-    admit(joining);
-    if (!joining.empty()) {
-      std::vector<Mesh*> parts;
-      if (u) parts.push_back(u);
-      for (ServeJob* j : joining) parts.push_back(j->mesh);
-      Mesh* old = u;
-      u = nullptr;
-      ctl.reset();
-      Mesh* nu = concat_meshes(parts, s);
-      delete old;
-      for (ServeJob* j : joining) {
-        delete j->mesh;
-        j->mesh = nullptr;
-        active.push_back(j);
-        st.push_back(SegState());
-      }
-      u = nu;
-      ctl.reset(new UnionCtl(*u));
-      rebuilds += 1;
-    }
-    if (!u) return (u32)queue.size();
+    double t_a = now_s();
+    admit();
+    double t_b = now_s();
+    secs_admit += t_b - t_a;
+    if (active.empty()) return (u32)queue.size();
     steps += 1;
-    union_step(*ctl, st, ap);
-    bool any_done = false;
-    for (SegState const& x : st) any_done = any_done || x.state >= ST_DONE;
-    if (any_done) {
-      ctl.reset();
-      std::vector<Mesh*> outs = split_union(*u, s);
-      std::vector<Mesh*> keep;
-      std::vector<ServeJob*> still;
-      std::vector<SegState> still_st;
-      double t = now_s() - t0;
-      for (size_t k = 0; k < outs.size(); ++k) {
-        ServeJob* j = active[k];
-        if (st[k].state >= ST_DONE) {
-          j->st = st[k];
-          Layout want = j->start;
-          for (u32 op : st[k].res.ops) want = layout_after(op, want, u->dim);
-          apply_layout(*outs[k], want);
-          outs[k]->own_new_stream();
-          j->mesh = outs[k];
-          j->finished = true;
-          j->t_done = t;
-          reserved -= j->est_bytes;
-        } else {
-          keep.push_back(outs[k]);
-          still.push_back(j);
-          still_st.push_back(st[k]);
-        }
+    u32 u0 = last_batch_stats().unions;
+    run.step(ms, st, owned);
+    unions += last_batch_stats().unions - u0;
+    double t_c = now_s();
+    secs_passes += t_c - t_b;
+    // retire the jobs whose loop ended
+    size_t w = 0;
+    double t = t_c - t0;
+    for (size_t k = 0; k < active.size(); ++k) {
+      ServeJob* j = active[k];
+      if (st[k].state >= ST_DONE) {
+        j->st = st[k];
+        Mesh* m = ms[k];
+        if (!owned[k]) throw Failure(E_ARG, "server lost a job's mesh");
+        drop_segments(*m);
+        Layout want = j->start;
+        for (u32 op : st[k].res.ops) want = layout_after(op, want, m->dim);
+        apply_layout(*m, want);
+        m->own_new_stream();
+        j->mesh = m;
+        j->finished = true;
+        j->t_done = t;
+        reserved -= j->est_bytes;
+        continue;
       }
-      Mesh* nu = keep.empty() ? nullptr : concat_meshes(keep, s);
-      for (Mesh* m : keep) delete m;
-      delete u;
-      u = nu;
-      active.swap(still);
-      st.swap(still_st);
-      if (u) ctl.reset(new UnionCtl(*u));
-      rebuilds += 1;
+      active[w] = active[k];
+      ms[w] = ms[k];
+      st[w] = st[k];
+      owned[w] = owned[k];
+      ++w;
     }
+    active.resize(w);
+    ms.resize(w);
+    st.resize(w);
+    owned.resize(w);
+    secs_retire += now_s() - t_c;
     return (u32)(active.size() + queue.size());
   }
 };
@@ -210,10 +198,14 @@ struct Server {
 Server* server_new(AdaptParams const& ap, unsigned long long budget)
 {
   Server* sv = new Server();
-  sv->ap = ap;
+  last_batch_stats() = BatchStats();
+  sv->run.ap = ap;
+  // unions of a few million elements: enough work per launch, and a working
+  // set that keeps most gathers in L2
+  sv->run.max_union_elems = 4000000ull;
   sv->budget = budget;
   sv->t0 = now_s();
-  CK(cudaStreamCreateWithFlags(&sv->s, cudaStreamNonBlocking));
+  CK(cudaStreamCreateWithFlags(&sv->run.s, cudaStreamNonBlocking));
   return sv;
 }
 
@@ -248,6 +240,8 @@ u32 server_submit(Server* sv, u32 dim, u32 nverts, double const* coords, u32 nel
 }
 
 u32 server_step(Server* sv) { return sv->step(); }
+
+void server_set_union_elems(Server* sv, unsigned long long n) { sv->run.max_union_elems = n; }
 
 std::vector<u32> server_poll(Server* sv, u32 max_ids)
 {
@@ -292,11 +286,15 @@ ServeStats server_stats(Server* sv)
 {
   ServeStats r;
   r.steps = sv->steps;
-  r.rebuilds = sv->rebuilds;
+  r.rebuilds = sv->unions;
   r.active = (u32)sv->active.size();
   r.queued = (u32)sv->queue.size();
   r.reserved = sv->reserved;
   r.now = now_s() - sv->t0;
+  r.secs_admit = sv->secs_admit;
+  r.secs_join = 0;
+  r.secs_passes = sv->secs_passes;
+  r.secs_retire = sv->secs_retire;
   return r;
 }
 

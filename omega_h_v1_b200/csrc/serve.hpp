@@ -19,9 +19,12 @@ struct ServeJobInfo {
 };
 
 struct ServeStats {
-  u32 steps = 0, rebuilds = 0, active = 0, queued = 0;
+  u32 steps = 0, rebuilds = 0, active = 0, queued = 0;  // rebuilds: unions formed
   unsigned long long reserved = 0;  // estimated device bytes of resident jobs
   double now = 0;
+  // host wall time spent admitting (upload + classification), joining jobs to
+  // the running union, in passes, and retiring finished jobs
+  double secs_admit = 0, secs_join = 0, secs_passes = 0, secs_retire = 0;
 };
 
 Server* server_new(AdaptParams const& ap, unsigned long long budget_bytes);
@@ -32,6 +35,8 @@ u32 server_submit(Server* sv, u32 dim, u32 nverts, double const* coords, u32 nel
 // admit what the budget allows, run one step over every resident job, hand
 // back the jobs whose loop ended; returns the jobs still queued or running
 u32 server_step(Server* sv);
+// largest union a pass forms, in current elements (0 = no limit)
+void server_set_union_elems(Server* sv, unsigned long long n);
 // finished jobs not yet reported, at most max_ids of them
 std::vector<u32> server_poll(Server* sv, u32 max_ids);
 Mesh* server_take(Server* sv, u32 id);
