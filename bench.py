@@ -399,12 +399,13 @@ def run_batched(args, world, rank, local):
     prep_s = time.perf_counter() - t0
     chunks = batched_chunks(jobs)
 
-    def clones():
+    def clones(fp32=False):
         out = []
         for b in bases:
             h = L.osh_b200_clone(b.h)
             G.check()
             L.osh_b200_set_stream(h, C.c_void_p(0))
+            L.osh_b200_set_fp32_filter(h, 1 if fp32 else 0)
             out.append(h)
         return out
 
@@ -476,12 +477,19 @@ def run_batched(args, world, rank, local):
     plain_launches = L.osh_b200_launch_count() - launches0
     hs = clones()
     torch.cuda.synchronize()
+    (bd64, be64, _, _), batch64_ms = timed(lambda: batch_leg(hs, chunks))
+    secs64 = dict(batch_secs)
+    # the batched path with the single-precision filter (double recheck)
+    hs = clones(fp32=True)
+    torch.cuda.synchronize()
+    L.osh_b200_fp32_stats_reset()
     clocks = Clocks(local)
     launches0 = L.osh_b200_launch_count()
     (bd, be, unions, upasses), batch_ms = timed(lambda: batch_leg(hs, chunks))
     batch_launches = L.osh_b200_launch_count() - launches0
     clk = clocks.stop()
-    same = all(pd[i] == bd[i] for i in range(len(jobs)))
+    fs = G.fp32_stats()
+    same = all(pd[i] == bd[i] == bd64[i] for i in range(len(jobs)))
     for b in bases:
         b.close()
     value = be / (batch_ms / 1e3)
@@ -499,10 +507,17 @@ def run_batched(args, world, rank, local):
                    "adapt": "mesh_adapt(1/3, 0.3, 4, 50) of every mesh",
                    "calls": len(chunks), "union_input_elems": BATCH_UNION_ELEMS,
                    "l2": "inputs larger than L2 (26M tets in, hundreds of M out)"},
+        "path": "batched, single-precision filter with double recheck",
         "plain": {"value": round(plain_value, 1), "ms": round(plain_ms, 3),
-                  "gpu_launches": int(plain_launches)},
+                  "gpu_launches": int(plain_launches),
+                  "path": "one mesh_adapt per mesh, double"},
+        "batched_fp64": {"value": round(be64 / (batch64_ms / 1e3), 1),
+                         "ms": round(batch64_ms, 3), "union_secs": secs64},
         "speedup_vs_plain": round(plain_ms / batch_ms, 3),
-        "identical_to_plain": bool(same and abs(pe - be) < 0.5),
+        "identical_to_plain": bool(same and abs(pe - be) < 0.5 and abs(pe - be64) < 0.5),
+        "fp32": {"decided_single": fs["decided"], "rechecked_double": fs["rechecked"],
+                 "max_quality_error": fs["max_error"],
+                 "bound_exceeded": fs["bound_exceeded"]},
         "elems_in": be, "unions": unions, "union_passes": upasses,
         "union_secs": batch_secs,
         "gpu_launches": int(batch_launches), "clocks": clk,

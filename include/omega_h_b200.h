@@ -82,6 +82,22 @@ void osh_b200_batch_times(double* concat, double* passes, double* split) OSH_PUB
    mesh i of that call: passes that changed it and the elements entering them */
 void osh_b200_batch_mesh_stats(unsigned i, unsigned* passes, double* elems_in) OSH_PUBLIC;
 
+/* ---- single-precision filter with double recheck ------------------------ */
+/* No counterpart in the reference. With the filter on (per mesh, inherited by
+   the meshes its passes produce), the edge-length tests of refine_by_size and
+   coarsen_by_size and the quality tests of refine_quality, coarsen_quality
+   and swap_quality first use a single-precision estimate that carries an
+   error bound; a candidate is decided on the estimate only when the bound
+   puts it clearly on one side of its threshold, and every value that is kept
+   is computed in double. Decisions, and so meshes, equal those without the
+   filter. Counters (device-wide): candidates decided on the estimate,
+   candidates recomputed in double, the largest |estimate - double| seen and
+   how often that exceeded the bound (always 0 when the bound holds). */
+void osh_b200_set_fp32_filter(osh_t m, int on) OSH_PUBLIC;
+void osh_b200_fp32_stats(unsigned long long* decided, unsigned long long* rechecked,
+    double* max_error, unsigned* bound_exceeded) OSH_PUBLIC;
+void osh_b200_fp32_stats_reset(void) OSH_PUBLIC;
+
 /* order-sensitive 64-bit digest of a mesh (connectivity of every dimension,
    tag names, kinds and data, global numbers), computed on the device; equal
    meshes give equal digests. No counterpart in the reference. */

@@ -136,6 +136,10 @@ def lib():
     f("osh_b200_batch_mesh_stats", None, C.c_uint, C.POINTER(C.c_uint), C.POINTER(C.c_double))
     f("osh_b200_batch_times", None, *([C.POINTER(C.c_double)] * 3))
     f("osh_b200_digest", C.c_ulonglong, vp)
+    f("osh_b200_set_fp32_filter", None, vp, C.c_int)
+    f("osh_b200_fp32_stats", None, C.POINTER(C.c_ulonglong), C.POINTER(C.c_ulonglong),
+      C.POINTER(C.c_double), C.POINTER(C.c_uint))
+    f("osh_b200_fp32_stats_reset", None)
     f("osh_b200_server_new", vp, C.c_double, C.c_double, C.c_uint, C.c_uint, C.c_ulonglong)
     f("osh_b200_server_free", None, vp)
     f("osh_b200_server_submit", C.c_int, vp, C.c_uint, C.c_uint, _f64p, C.c_uint, _u32p, _f64p)
@@ -238,6 +242,12 @@ class Mesh:
         h = self.L.osh_b200_clone(self.h)
         self._chk()
         return Mesh(h)
+
+    def set_fp32_filter(self, on=True):
+        """Decide far-from-threshold candidates on single-precision estimates
+        (double recheck near thresholds; results unchanged)."""
+        self.L.osh_b200_set_fp32_filter(self.h, 1 if on else 0)
+        self._chk()
 
     def digest(self):
         """Order-sensitive 64-bit hash of every array of the mesh (device)."""
@@ -430,6 +440,20 @@ class Mesh:
     def synchronize(self):
         self.L.osh_b200_synchronize(self.h)
         self._chk()
+
+
+def fp32_stats(reset=False):
+    """(decided on the estimate, rechecked in double, max |estimate - double|,
+    times the bound was exceeded) since the last reset."""
+    L = lib()
+    d, r = C.c_ulonglong(), C.c_ulonglong()
+    e, b = C.c_double(), C.c_uint()
+    L.osh_b200_fp32_stats(C.byref(d), C.byref(r), C.byref(e), C.byref(b))
+    check()
+    if reset:
+        L.osh_b200_fp32_stats_reset()
+        check()
+    return dict(decided=d.value, rechecked=r.value, max_error=e.value, bound_exceeded=b.value)
 
 
 def adapt_batch(meshes, size_floor, good_qual, nlayers, max_ops, max_union_elems=0):

@@ -346,6 +346,7 @@ Mesh* concat_meshes(std::vector<Mesh*> const& ms, cudaStream_t stream)
     stream_sync(m->s);
   }
   Mesh* u = new Mesh(dim, a.full, a.parallel, stream);
+  u->fp32_filter = a.fp32_filter;
   cudaStream_t s = u->s;
   try {
     Meta meta;
@@ -464,7 +465,10 @@ std::vector<Mesh*> split_union(Mesh& u, cudaStream_t stream, std::vector<char> c
   std::vector<u32> counts[4];
   try {
     for (u32 k = 0; k < nm; ++k)
-      if (!want || (*want)[k]) out[k] = new Mesh(dim, u.full, u.parallel, stream, u.mb);
+      if (!want || (*want)[k]) {
+        out[k] = new Mesh(dim, u.full, u.parallel, stream, u.mb);
+        out[k]->fp32_filter = u.fp32_filter;
+      }
     // stable counting sort of every dimension's entities by segment
     for (u32 d = 0; d <= dim; ++d) {
       if (!u.has_dim(d)) continue;

@@ -632,6 +632,29 @@ void osh_b200_server_times(osh_b200_server_t sv, double* admit, double* join,
   API_CATCH_VOID
 }
 
+void osh_b200_set_fp32_filter(osh_t h, int on)
+{
+  API_TRY
+  need(h != nullptr, "mesh is NULL");
+  M(h)->fp32_filter = on != 0;
+  API_CATCH_VOID
+}
+
+void osh_b200_fp32_stats(unsigned long long* decided, unsigned long long* rechecked,
+    double* max_error, unsigned* bound_exceeded)
+{
+  API_TRY
+  osh::fp32_stats_read(decided, rechecked, max_error, bound_exceeded);
+  API_CATCH_VOID
+}
+
+void osh_b200_fp32_stats_reset(void)
+{
+  API_TRY
+  osh::fp32_stats_reset();
+  API_CATCH_VOID
+}
+
 unsigned long long osh_b200_digest(osh_t h)
 {
   API_TRY

@@ -11,7 +11,7 @@ __device__ inline u32 collapses(u32 code, u32 dir) { return (code >> dir) & 1u; 
 // coarsen_size_code (coarsen.cpp:13-21) fused with measure_edge
 __global__ void k_coarsen_size_codes(u32 ne, u32 const* __restrict__ voe,
     double const* __restrict__ x, double const* __restrict__ h, double size_floor,
-    SegView sv, u32* __restrict__ codes, u32* any)
+    SegView sv, Fp32Stats* fs, u32* __restrict__ codes, u32* any)
 {
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   u32 c = 0;
@@ -20,10 +20,18 @@ __global__ void k_coarsen_size_codes(u32 ne, u32 const* __restrict__ voe,
     double xa[3], xb[3];
     load3(x, a, xa);
     load3(x, b, xb);
-    double len = sqrt(sqdist3(xb, xa));
-    double want = (h[a] + h[b]) / 2;
-    c = ((len / want) < size_floor && seg_acts(sv, a)) ? (u32)COLLAPSE_BOTH
-                                                        : (u32)DONT_COLLAPSE;
+    int r32 = fs ? edge_ratio_side_f32(xa, xb, h[a], h[b], size_floor) : 0;
+    bool shorter;
+    if (r32) {
+      atomicAdd(&fs->decided, 1ull);
+      shorter = r32 < 0;
+    } else {
+      if (fs) atomicAdd(&fs->rechecked, 1ull);
+      double len = sqrt(sqdist3(xb, xa));
+      double want = (h[a] + h[b]) / 2;
+      shorter = (len / want) < size_floor;
+    }
+    c = (shorter && seg_acts(sv, a)) ? (u32)COLLAPSE_BOTH : (u32)DONT_COLLAPSE;
     codes[i] = c;
   }
   if (__any_sync(0xffffffffu, c) && (threadIdx.x & 31) == 0) atomicOr(any, 1u);
@@ -97,7 +105,7 @@ __global__ void k_coarsen_quality(u32 dim, u32 ne, u32 const* __restrict__ voe1,
     u32 const* __restrict__ voe, u32 const* __restrict__ ev_offs,
     u32 const* __restrict__ ev, u32 const* __restrict__ ev_dirs,
     double const* __restrict__ x, double const* __restrict__ eq, double floor_q,
-    SegView sv, u32* __restrict__ codes, double* __restrict__ out, u32* any)
+    SegView sv, Fp32Stats* fs, u32* __restrict__ codes, double* __restrict__ out, u32* any)
 {
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   u32 keep = 0;
@@ -113,6 +121,31 @@ __global__ void k_coarsen_quality(u32 dim, u32 ne, u32 const* __restrict__ voe1,
         u32 col = voe1[i * 2 + j], gen = voe1[i * 2 + 1 - j];
         double ex[4][3];
         load3(x, gen, ex[vpe - 1]);
+        if (fs && dim == 3) {
+          // reject on the estimate when the cavity's worst element is surely
+          // below the floor, or surely no better than before
+          float upper = 1.0f;
+          for (u32 k = ev_offs[col]; k < ev_offs[col + 1]; ++k) {
+            u32 e = ev[k];
+            u32 const* ve = voe + (size_t)e * vpe;
+            if (eq && eq[e] < old_minq) old_minq = eq[e];
+            bool adjacent = false;
+            for (u32 l = 0; l < vpe; ++l)
+              if (ve[l] == gen) adjacent = true;
+            if (adjacent) continue;
+            u32 base = opp(dim, 0, ev_dirs[k]);
+            for (u32 l = 0; l + 1 < vpe; ++l) load3(x, ve[canon(dim, dim - 1, 0, base, l)], ex[l]);
+            Q32 q = tet_quality_f32(ex, (float)perfect);
+            upper = fminf(upper, q.q + q.err);
+          }
+          if ((double)upper < fq || (eq && (double)upper <= old_minq)) {
+            atomicAdd(&fs->decided, 1ull);
+            code &= ~(1u << j);
+            continue;
+          }
+          atomicAdd(&fs->rechecked, 1ull);
+          old_minq = 1;
+        }
         for (u32 k = ev_offs[col]; k < ev_offs[col + 1]; ++k) {
           u32 e = ev[k];
           u32 const* ve = voe + (size_t)e * vpe;
@@ -124,6 +157,7 @@ __global__ void k_coarsen_quality(u32 dim, u32 ne, u32 const* __restrict__ voe1,
           u32 base = opp(dim, 0, ev_dirs[k]);
           for (u32 l = 0; l + 1 < vpe; ++l) load3(x, ve[canon(dim, dim - 1, 0, base, l)], ex[l]);
           double q = dim == 3 ? tet_quality(ex, perfect) : tri_quality(ex, 1, perfect);
+          if (fs && dim == 3) fp32_note_error(fs, tet_quality_f32(ex, (float)perfect), q);
           if (q < minq) minq = q;
         }
         if (minq < fq || (eq && minq <= old_minq))
@@ -506,8 +540,8 @@ static bool coarsen_select(Mesh& m, u32* codes, double qual_floor, bool require_
       PROBE(P_COARSEN_QUALITY, s, 4.0 * (nv + 1) + 8.0 * deg(dim, 0) * nel + 8.0 * ne +
           4.0 * deg(dim, 0) * nel + 24.0 * nv + 8.0 * ne + 16.0 * ne);
       k_coarsen_quality<<<grid_for(ne), BLOCK, 0, s>>>(dim, ne, voe1, m.ask_down(dim, 0),
-          ev.offs, ev.adj, ev.dirs, m.coords(), eq, qual_floor, m.segview(), codes, sel.q2,
-          any);
+          ev.offs, ev.adj, ev.dirs, m.coords(), eq, qual_floor, m.segview(),
+          m.fp32_filter ? fp32_stats_dev() : nullptr, codes, sel.q2, any);
       CK_LAUNCH();
     }
   }
@@ -650,7 +684,8 @@ u32 coarsen_by_size(Mesh& m, double qual_floor, double size_floor)
   CK(cudaMemsetAsync(any, 0, sizeof(u32), s));
   if (ne) {
     k_coarsen_size_codes<<<grid_for(ne), BLOCK, 0, s>>>(ne, m.ask_down(1, 0), m.coords(),
-        static_cast<double const*>(h->data), size_floor, m.segview(), codes, any);
+        static_cast<double const*>(h->data), size_floor, m.segview(),
+        m.fp32_filter ? fp32_stats_dev() : nullptr, codes, any);
     CK_LAUNCH();
   }
   u32 r = 0;
@@ -711,7 +746,8 @@ u32 coarsen_sets(Mesh& m, double qual_floor, double size_floor, u32* codes_size,
   CK(cudaMemsetAsync(gen_vert, 0xff, sizeof(u32) * nv, s));
   if (ne) {
     k_coarsen_size_codes<<<grid_for(ne), BLOCK, 0, s>>>(ne, m.ask_down(1, 0), m.coords(),
-        static_cast<double const*>(h->data), size_floor, m.segview(), codes_size, any);
+        static_cast<double const*>(h->data), size_floor, m.segview(),
+        m.fp32_filter ? fp32_stats_dev() : nullptr, codes_size, any);
     CK_LAUNCH();
   }
   u32* codes = dalloc<u32>(ne, s);

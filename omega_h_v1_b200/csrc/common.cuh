@@ -233,6 +233,90 @@ __host__ __device__ inline double perfect_tet_quality()
   return (sqrt(2.0) / 12.0) / (s * s * s);
 }
 
+// Single-precision filter for quality decisions. The estimate is formed
+// from coordinates relative to the first vertex (each difference taken in
+// double, then rounded), with a running bound on its error: the triple
+// product and the face areas are each off by at most a few float epsilons
+// of the products of the edge lengths that form them, which the bound
+// scales by the same normalisation as the quality. A candidate is rejected
+// on the estimate only when estimate + bound is already below the
+// threshold; every other decision, and every value that is kept, comes from
+// the double computation, so all decisions equal the double path's.
+struct Q32 {
+  float q;    // estimate of tet_quality
+  float err;  // bound on |estimate - tet_quality|; inf when unbounded
+};
+
+__device__ inline float3 f3sub(float3 a, float3 b) { return make_float3(a.x - b.x, a.y - b.y, a.z - b.z); }
+__device__ inline float3 f3cross(float3 a, float3 b)
+{
+  return make_float3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+__device__ inline float f3dot(float3 a, float3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ inline float f3norm(float3 a) { return sqrtf(f3dot(a, a)); }
+
+__device__ inline Q32 tet_quality_f32(double const (*x)[3], float perfect)
+{
+  float3 d0 = make_float3((float)(x[1][0] - x[0][0]), (float)(x[1][1] - x[0][1]),
+      (float)(x[1][2] - x[0][2]));
+  float3 d1 = make_float3((float)(x[2][0] - x[0][0]), (float)(x[2][1] - x[0][1]),
+      (float)(x[2][2] - x[0][2]));
+  float3 d2 = make_float3((float)(x[3][0] - x[0][0]), (float)(x[3][1] - x[0][1]),
+      (float)(x[3][2] - x[0][2]));
+  float3 e12 = f3sub(d1, d0), e13 = f3sub(d2, d0), e23 = f3sub(d2, d1);
+  float3 c0 = f3cross(d0, d1), c1 = f3cross(d0, e13), c2 = f3cross(e12, e23), c3 = f3cross(d1, d2);
+  float sum_asq = 0.25f * (f3dot(c0, c0) + f3dot(c1, c1) + f3dot(c2, c2) + f3dot(c3, c3));
+  float arms = sqrtf(sum_asq * 0.25f);
+  float v = f3dot(c0, d2) * (1.0f / 6.0f);
+  float r = sqrtf(arms);
+  float den = r * r * r * perfect;
+  Q32 out;
+  out.q = v / den;
+  // the triple product is off by at most 64 eps |d0||d1||d2|; each face
+  // area by 12 eps of the square of the longest edge, so the denominator by
+  // 24 eps lmax^2 / A_rms relative; the divisions and roots add 32 eps
+  float n0 = f3dot(d0, d0), n1 = f3dot(d1, d1), n2 = f3dot(d2, d2);
+  float lmax2 = fmaxf(fmaxf(fmaxf(n0, n1), fmaxf(n2, f3dot(e12, e12))),
+      fmaxf(f3dot(e13, e13), f3dot(e23, e23)));
+  float eps = 5.9604645e-08f;
+  out.err = 64.0f * eps * (sqrtf(n0) * sqrtf(n1) * sqrtf(n2) / 6.0f) / den +
+      fabsf(out.q) * eps * (32.0f + 24.0f * lmax2 / arms) + 1e-30f;
+  if (!(den > 0.0f) || !isfinite(out.q) || !isfinite(out.err)) out.err = __int_as_float(0x7f800000);
+  return out;
+}
+
+// which side of `thr` the metric edge length |xb - xa| / ((ha + hb) / 2)
+// lies on, from a single-precision estimate: +1 above, -1 below, 0 when the
+// estimate is within 64 float epsilons (relative) of the threshold
+__device__ inline int edge_ratio_side_f32(double const* xa, double const* xb, double ha,
+    double hb, double thr)
+{
+  float3 d = make_float3((float)(xb[0] - xa[0]), (float)(xb[1] - xa[1]), (float)(xb[2] - xa[2]));
+  float r = sqrtf(f3dot(d, d)) / (float)((ha + hb) / 2);
+  float t = (float)thr, band = 64.0f * 5.9604645e-08f * t;
+  if (!isfinite(r)) return 0;
+  if (r > t + band) return 1;
+  if (r < t - band) return -1;
+  return 0;
+}
+
+// device counters of the filter: candidates rejected on the estimate,
+// candidates recomputed in double, the largest |estimate - double| seen and
+// the number of times that exceeded the bound
+struct Fp32Stats {
+  unsigned long long decided;
+  unsigned long long rechecked;
+  unsigned int max_err_bits;
+  unsigned int bound_exceeded;
+};
+
+__device__ inline void fp32_note_error(Fp32Stats* st, Q32 e, double q64)
+{
+  float diff = fabsf((float)(q64 - (double)e.q));
+  atomicMax(&st->max_err_bits, __float_as_uint(diff));
+  if ((double)diff > (double)e.err) atomicAdd(&st->bound_exceeded, 1u);
+}
+
 // tet_quality (quality.hpp:68-89): Shewchuk's V / A_rms^(3/2), normalised
 __host__ __device__ inline double tet_quality(double const (*x)[3], double perfect)
 {

@@ -59,6 +59,7 @@ Mesh* Mesh::spawn() const
   Mesh* m = new Mesh(dim, full, parallel, s, mb);
   m->nseg = nseg;
   m->ctl = ctl;
+  m->fp32_filter = fp32_filter;
   return m;
 }
 
@@ -90,6 +91,7 @@ Mesh* Mesh::clone()
       }
     }
     c->ghost_layers = ghost_layers;
+    c->fp32_filter = fp32_filter;
     if (seg) {
       c->nseg = nseg;
       c->seg = dalloc<u32>(counts[0], c->s);

@@ -91,6 +91,9 @@ struct Mesh {
   u32 nseg = 0;
   u32* seg = nullptr;
   SegCtl const* ctl = nullptr;
+  // reject quality candidates on a single-precision estimate with an error
+  // bound before computing them in double (decisions are unchanged)
+  bool fp32_filter = false;
   cudaStream_t s = nullptr;
   bool own_stream = false;
   std::shared_ptr<Mailbox> mb;  // shared by a mesh and the meshes it spawns

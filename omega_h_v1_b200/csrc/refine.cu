@@ -14,7 +14,7 @@ namespace osh {
 // refine_candidate (refine.cpp:11-15) fused with measure_edge (size.cpp:57)
 __global__ void k_refine_candidates(u32 ne, u32 const* __restrict__ voe,
     double const* __restrict__ x, double const* __restrict__ h, SegView sv,
-    u32* __restrict__ cand, u32* any)
+    Fp32Stats* fs, u32* __restrict__ cand, u32* any)
 {
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   u32 c = 0;
@@ -23,9 +23,17 @@ __global__ void k_refine_candidates(u32 ne, u32 const* __restrict__ voe,
     double xa[3], xb[3];
     load3(x, a, xa);
     load3(x, b, xb);
-    double len = sqrt(sqdist3(xb, xa));
-    double want = (h[a] + h[b]) / 2;
-    c = (len / want) > 1.0 && seg_acts(sv, a);
+    int r32 = fs ? edge_ratio_side_f32(xa, xb, h[a], h[b], 1.0) : 0;
+    if (r32) {
+      atomicAdd(&fs->decided, 1ull);
+      c = r32 > 0;
+    } else {
+      if (fs) atomicAdd(&fs->rechecked, 1ull);
+      double len = sqrt(sqdist3(xb, xa));
+      double want = (h[a] + h[b]) / 2;
+      c = (len / want) > 1.0;
+    }
+    c = c && seg_acts(sv, a);
     cand[i] = c;
   }
   if (__any_sync(0xffffffffu, c) && (threadIdx.x & 31) == 0) atomicOr(any, 1u);
@@ -36,8 +44,8 @@ __global__ void k_refine_candidates(u32 ne, u32 const* __restrict__ voe,
 __global__ void k_refine_quality(u32 dim, u32 ne, u32 const* __restrict__ voe1,
     u32 const* __restrict__ voe, u32 const* __restrict__ eo_offs,
     u32 const* __restrict__ eo, u32 const* __restrict__ eo_dirs,
-    double const* __restrict__ x, double qual_floor, SegView sv, u32* __restrict__ cand,
-    double* __restrict__ out, u32* any, u32* inverted)
+    double const* __restrict__ x, double qual_floor, SegView sv, Fp32Stats* fs,
+    u32* __restrict__ cand, double* __restrict__ out, u32* any, u32* inverted)
 {
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   u32 keep = 0;
@@ -53,7 +61,39 @@ __global__ void k_refine_quality(u32 dim, u32 ne, u32 const* __restrict__ voe1,
       acc += x[b * 3 + c];
       split[c] = acc / 2u;
     }
+    double const fl = seg_floor(sv, a, qual_floor);
+    bool filtered = false;
+    if (fs && dim == 3) {
+      // reject on the estimate only when every child is surely upright and
+      // the worst child is surely below the floor
+      float upper = 1.0f;
+      bool upright = true;
+      for (u32 j = eo_offs[i]; j < eo_offs[i + 1]; ++j) {
+        u32 dir = eo_dirs[j], e = eo[j];
+        u32 const* ve = voe + (size_t)e * vpe;
+        for (u32 k = 0; k < 2; ++k) {
+          u32 o = canon(dim, 1, 0, dir, k);
+          u32 base = opp(dim, 0, o);
+          double ex[4][3];
+          for (u32 l = 0; l + 1 < vpe; ++l) load3(x, ve[canon(dim, dim - 1, 0, base, l)], ex[l]);
+          ex[3][0] = split[0];
+          ex[3][1] = split[1];
+          ex[3][2] = split[2];
+          Q32 q = tet_quality_f32(ex, (float)perfect);
+          upright = upright && (q.q - q.err > 0.0f);
+          upper = fminf(upper, q.q + q.err);
+        }
+      }
+      if (upright && (double)upper < fl) {
+        filtered = true;
+        atomicAdd(&fs->decided, 1ull);
+        cand[i] = 0;
+      } else {
+        atomicAdd(&fs->rechecked, 1ull);
+      }
+    }
     double minq = 1;
+    if (!filtered) {
     for (u32 j = eo_offs[i]; j < eo_offs[i + 1]; ++j) {
       u32 dir = eo_dirs[j], e = eo[j];
       u32 const* ve = voe + (size_t)e * vpe;
@@ -66,15 +106,17 @@ __global__ void k_refine_quality(u32 dim, u32 ne, u32 const* __restrict__ voe1,
         ex[vpe - 1][1] = split[1];
         ex[vpe - 1][2] = split[2];
         double q = dim == 3 ? tet_quality(ex, perfect) : tri_quality(ex, 0, perfect);
+        if (fs && dim == 3) fp32_note_error(fs, tet_quality_f32(ex, (float)perfect), q);
         if (!(q > 0)) atomicOr(inverted, 1u);
         if (q < minq) minq = q;
       }
     }
-    if (minq < seg_floor(sv, a, qual_floor)) {
+    if (minq < fl) {
       cand[i] = 0;
     } else {
       out[i] = minq;
       keep = 1;
+    }
     }
   }
   if (__any_sync(0xffffffffu, keep) && (threadIdx.x & 31) == 0) atomicOr(any, 1u);
@@ -324,7 +366,7 @@ static u32* choose_refinement(Mesh& m, u32* cand, double qual_floor, double** qu
           4.0 * deg(dim, 0) * nel + 24.0 * m.counts[0] + 8.0 * ne + 8.0 * ne);
       k_refine_quality<<<grid_for(ne), BLOCK, 0, s>>>(dim, ne, m.ask_down(1, 0),
           m.ask_down(dim, 0), eo.offs, eo.adj, eo.dirs, m.coords(), qual_floor, m.segview(),
-          cand, q, any, inverted);
+          m.fp32_filter ? fp32_stats_dev() : nullptr, cand, q, any, inverted);
       CK_LAUNCH();
     }
     m.mb->fetch(s, 4);
@@ -379,7 +421,8 @@ u32 refine_by_size(Mesh& m, double qual_floor)
   if (ne) {
     PROBE(P_REFINE_CANDIDATES, s, 8.0 * ne + 32.0 * m.counts[0] + 4.0 * ne);
     k_refine_candidates<<<grid_for(ne), BLOCK, 0, s>>>(ne, m.ask_down(1, 0), m.coords(),
-        static_cast<double const*>(h->data), m.segview(), cand, any);
+        static_cast<double const*>(h->data), m.segview(),
+        m.fp32_filter ? fp32_stats_dev() : nullptr, cand, any);
     CK_LAUNCH();
   }
   // no separate check for "any candidate": with none, the quality kernel
@@ -410,7 +453,8 @@ u32 refine_sets(Mesh& m, double qual_floor, u32* cand_out, u32* good_out,
   CK(cudaMemsetAsync(indset_out, 0, sizeof(u32) * ne, s));
   if (ne) {
     k_refine_candidates<<<grid_for(ne), BLOCK, 0, s>>>(ne, m.ask_down(1, 0), m.coords(),
-        static_cast<double const*>(h->data), m.segview(), cand_out, any);
+        static_cast<double const*>(h->data), m.segview(),
+        m.fp32_filter ? fp32_stats_dev() : nullptr, cand_out, any);
     CK_LAUNCH();
   }
   CK(cudaMemcpyAsync(good_out, cand_out, sizeof(u32) * ne, cudaMemcpyDeviceToDevice, s));

@@ -88,6 +88,45 @@ char const* const g_probe_names[P_NPROBES] = {"reflect_down", "up_count", "up_fi
 
 char const* probe_name(u32 id) { return id < P_NPROBES ? g_probe_names[id] : nullptr; }
 
+namespace {
+std::once_flag g_fp32_once[64];
+Fp32Stats* g_fp32[64] = {};
+}
+
+Fp32Stats* fp32_stats_dev()
+{
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) throw Failure(E_ARG, "device index out of range");
+  std::call_once(g_fp32_once[dev], [dev]() {
+    void* p = nullptr;
+    CK(cudaMalloc(&p, sizeof(Fp32Stats)));
+    CK(cudaMemset(p, 0, sizeof(Fp32Stats)));
+    g_fp32[dev] = static_cast<Fp32Stats*>(p);
+  });
+  return g_fp32[dev];
+}
+
+void fp32_stats_read(unsigned long long* decided, unsigned long long* rechecked,
+    double* max_err, unsigned* bound_exceeded)
+{
+  Fp32Stats h;
+  CK(cudaDeviceSynchronize());
+  CK(cudaMemcpy(&h, fp32_stats_dev(), sizeof(h), cudaMemcpyDeviceToHost));
+  float e;
+  std::memcpy(&e, &h.max_err_bits, sizeof(e));
+  if (decided) *decided = h.decided;
+  if (rechecked) *rechecked = h.rechecked;
+  if (max_err) *max_err = e;
+  if (bound_exceeded) *bound_exceeded = h.bound_exceeded;
+}
+
+void fp32_stats_reset()
+{
+  CK(cudaDeviceSynchronize());
+  CK(cudaMemset(fp32_stats_dev(), 0, sizeof(Fp32Stats)));
+}
+
 void probe_enable(u32 mask) { probes().mask = mask; }
 
 static void probe_resolve(ProbeState& p)

@@ -62,6 +62,13 @@ enum ProbeId {
   P_NPROBES
 };
 char const* probe_name(u32 id);
+// the single-precision filter's device counters (one buffer per device)
+struct Fp32Stats;
+Fp32Stats* fp32_stats_dev();
+void fp32_stats_read(unsigned long long* decided, unsigned long long* rechecked,
+    double* max_err, unsigned* bound_exceeded);
+void fp32_stats_reset();
+
 void probe_enable(u32 mask);
 void probe_reset();
 void probe_read(u32 id, u32* launches, double* ms, double* bytes);

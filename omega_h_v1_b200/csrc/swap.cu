@@ -195,6 +195,51 @@ __device__ void choose_edge_swap(u32 rs, double const (*ex)[3], double const (*r
   *q_out = best;
 }
 
+// Upper bound, from single-precision estimates, on the best triangulation's
+// worst tet as choose_edge_swap would find it, valid whenever that value is
+// positive (a triangulation it stops early on has a negative value).
+__device__ float best_swap_upper_f32(u32 rs, double const (*ex)[3], double const (*rx)[3],
+    float perfect)
+{
+  float cache[35];
+  unsigned long long cached = 0;
+  float best = -1.0f;
+  u32 nm = c_swap.nmesh[rs], nt = c_swap.ntri[rs];
+  for (u32 i = 0; i < nm; ++i) {
+    float mesh_upper = 1.0f;
+    for (u32 j = 0; j < nt; ++j) {
+      u32 slot = c_swap.uniq[rs][i][j];
+      if (!((cached >> slot) & 1ull)) {
+        double tx[4][3];
+        for (u32 k = 0; k < 3; ++k) {
+          u32 r = c_swap.tri[rs][i][j][k];
+          tx[k][0] = rx[r][0];
+          tx[k][1] = rx[r][1];
+          tx[k][2] = rx[r][2];
+        }
+        float tri_upper = 1.0f;
+        for (u32 k = 0; k < 2; ++k) {
+          tx[3][0] = ex[1 - k][0];
+          tx[3][1] = ex[1 - k][1];
+          tx[3][2] = ex[1 - k][2];
+          Q32 q = tet_quality_f32(tx, perfect);
+          tri_upper = fminf(tri_upper, q.q + q.err);
+          for (u32 c = 0; c < 3; ++c) {
+            double tmp = tx[0][c];
+            tx[0][c] = tx[1][c];
+            tx[1][c] = tmp;
+          }
+        }
+        cached |= 1ull << slot;
+        cache[slot] = tri_upper;
+      }
+      mesh_upper = fminf(mesh_upper, cache[slot]);
+    }
+    best = fmaxf(best, mesh_upper);
+  }
+  return best;
+}
+
 // unmark_boundary (mark.cpp:198-204)
 __global__ void k_unmark_boundary(u32 n, u32 dim, u32 const* __restrict__ cd,
     u32* __restrict__ marked, u32* any)
@@ -212,9 +257,9 @@ __global__ void k_unmark_boundary(u32 n, u32 dim, u32 const* __restrict__ cd,
 __global__ void k_swap_quality(u32 ne, u32 const* __restrict__ te_offs,
     u32 const* __restrict__ te, u32 const* __restrict__ te_dirs,
     u32 const* __restrict__ voe1, u32 const* __restrict__ vot,
-    double const* __restrict__ x, double const* __restrict__ eq, u32* __restrict__ cand,
-    double* __restrict__ quals, u32* __restrict__ ring_sizes, u32* __restrict__ codes,
-    u32* any)
+    double const* __restrict__ x, double const* __restrict__ eq, Fp32Stats* fs,
+    u32* __restrict__ cand, double* __restrict__ quals, u32* __restrict__ ring_sizes,
+    u32* __restrict__ codes, u32* any)
 {
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   u32 keep = 0;
@@ -232,9 +277,21 @@ __global__ void k_swap_quality(u32 ne, u32 const* __restrict__ te_offs,
       load3(x, ev[1], ex[1]);
       for (u32 j = 0; j < rs; ++j) load3(x, rv[j], rx[j]);
       u32 code;
-      double q;
-      choose_edge_swap(rs, ex, rx, perfect_tet_quality(), &code, &q);
-      if (q > old_minq) {
+      double q = -1;
+      // a swap is kept only if it beats old_minq; when old_minq is positive
+      // an upper bound at or below it settles the rejection
+      bool filtered = false;
+      if (fs && old_minq > 0) {
+        float ub = best_swap_upper_f32(rs, ex, rx, (float)perfect_tet_quality());
+        if ((double)ub <= old_minq) {
+          filtered = true;
+          atomicAdd(&fs->decided, 1ull);
+        } else {
+          atomicAdd(&fs->rechecked, 1ull);
+        }
+      }
+      if (!filtered) choose_edge_swap(rs, ex, rx, perfect_tet_quality(), &code, &q);
+      if (!filtered && q > old_minq) {
         quals[i] = q;
         ring_sizes[i] = rs;
         codes[i] = code;
@@ -415,7 +472,8 @@ static bool swap_select(Mesh& m, double gq, u32 nlayers, SwapSel& sel, u32* sliv
   PROBE(P_SWAP_QUALITY, s, 4.0 * (ne + 1) + 8.0 * 6.0 * m.counts[3] + 8.0 * ne +
       16.0 * m.counts[3] + 24.0 * m.counts[0] + 8.0 * m.counts[3] + 4.0 * ne + 16.0 * ne);
   k_swap_quality<<<ceil_div(ne, 128), 128, 0, s>>>(ne, te.offs, te.adj, te.dirs, m.ask_down(1, 0),
-      m.ask_down(3, 0), m.coords(), eq, sel.cand, sel.quals, sel.rs, sel.codes, any);
+      m.ask_down(3, 0), m.coords(), eq, m.fp32_filter ? fp32_stats_dev() : nullptr, sel.cand,
+      sel.quals, sel.rs, sel.codes, any);
   CK_LAUNCH();
   if (!read_u32(any, s)) return false;
   sel.ind = find_indset(m, 1, sel.cand, sel.quals);
