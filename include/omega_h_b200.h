@@ -82,6 +82,26 @@ void osh_b200_batch_times(double* concat, double* passes, double* split) OSH_PUB
    mesh i of that call: passes that changed it and the elements entering them */
 void osh_b200_batch_mesh_stats(unsigned i, unsigned* passes, double* elems_in) OSH_PUBLIC;
 
+/* ---- size-field producers ------------------------------------------------ */
+/* mesh_element_gradients (element_gradients.cpp:72-91): element field
+   "grad_<name>" with 3 components per component of the vertex field name */
+void osh_b200_element_gradients(osh_t m, char const* name) OSH_PUBLIC;
+/* mesh_recover_by_volume (recover_by_volume.cpp:55-68): vertex field name,
+   the volume-weighted average of the element field name around each vertex */
+void osh_b200_recover_by_volume(osh_t m, char const* name) OSH_PUBLIC;
+/* mesh_size_from_hessian (size_from_hessian.cpp:44-72): vertex field
+   "adapt_size" = max(max_h - sum_j weights[j] |H_j|, min_h) from the vertex
+   field hess_name (9 components per solution component; weights host array,
+   or NULL for all 1) */
+void osh_b200_size_from_hessian(osh_t m, char const* hess_name, double const* weights,
+    double min_h, double max_h) OSH_PUBLIC;
+/* mesh_warp_to_limit (warp_to_limit.cpp:31-81): coordinates += f * warp with
+   f = 1, 1/2, 1/4 ... until the minimum element quality is at least
+   qual_floor; "warp" keeps the part not yet applied. Returns 1 if the whole
+   warp was applied. Where the reference would halve forever (a floor the
+   unwarped mesh already fails), this build stops with OSH_B200_E_NOCONVERGE. */
+unsigned osh_b200_warp_to_limit(osh_t m, double qual_floor) OSH_PUBLIC;
+
 /* ---- single-precision filter with double recheck ------------------------ */
 /* No counterpart in the reference. With the filter on (per mesh, inherited by
    the meshes its passes produce), the edge-length tests of refine_by_size and

@@ -137,6 +137,11 @@ def lib():
     f("osh_b200_batch_times", None, *([C.POINTER(C.c_double)] * 3))
     f("osh_b200_digest", C.c_ulonglong, vp)
     f("osh_b200_set_fp32_filter", None, vp, C.c_int)
+    f("osh_b200_element_gradients", None, vp, C.c_char_p)
+    f("osh_b200_recover_by_volume", None, vp, C.c_char_p)
+    f("osh_b200_size_from_hessian", None, vp, C.c_char_p, C.c_void_p, C.c_double, C.c_double)
+    f("osh_b200_warp_to_limit", C.c_uint, vp, C.c_double)
+    f("osh_free_field", None, vp, C.c_uint, C.c_char_p)
     f("osh_b200_fp32_stats", None, C.POINTER(C.c_ulonglong), C.POINTER(C.c_ulonglong),
       C.POINTER(C.c_double), C.POINTER(C.c_uint))
     f("osh_b200_fp32_stats_reset", None)
@@ -242,6 +247,35 @@ class Mesh:
         h = self.L.osh_b200_clone(self.h)
         self._chk()
         return Mesh(h)
+
+    def has_tag(self, dim, name):
+        n = self.L.osh_b200_ntags(self.h, dim)
+        return any(self.L.osh_b200_tag_name(self.h, dim, i).decode() == name for i in range(n))
+
+    # size-field producers ----------------------------------------------------
+    def element_gradients(self, name):
+        self.L.osh_b200_element_gradients(self.h, name.encode())
+        self._chk()
+
+    def recover_by_volume(self, name):
+        self.L.osh_b200_recover_by_volume(self.h, name.encode())
+        self._chk()
+
+    def size_from_hessian(self, hess_name, weights, min_h, max_h):
+        w = None
+        if weights is not None:
+            w = np.ascontiguousarray(weights, dtype=np.float64)
+        self.L.osh_b200_size_from_hessian(self.h, hess_name.encode(),
+                                          None if w is None else w.ctypes.data_as(C.c_void_p),
+                                          min_h, max_h)
+        self._chk()
+
+    def warp_to_limit(self, qual_floor):
+        return self._chk(self.L.osh_b200_warp_to_limit(self.h, qual_floor))
+
+    def free_tag(self, dim, name):
+        self.L.osh_free_field(self.h, dim, name.encode())
+        self._chk()
 
     def set_fp32_filter(self, on=True):
         """Decide far-from-threshold candidates on single-precision estimates

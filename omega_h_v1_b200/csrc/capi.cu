@@ -9,6 +9,7 @@
 #include "../../include/omega_h.h"
 #include "../../include/omega_h_b200.h"
 #include "batch.hpp"
+#include "fields.hpp"
 #include "serve.hpp"
 #include "passes.hpp"
 
@@ -630,6 +631,44 @@ void osh_b200_server_times(osh_b200_server_t sv, double* admit, double* join,
   if (passes) *passes = r.secs_passes;
   if (retire) *retire = r.secs_retire;
   API_CATCH_VOID
+}
+
+void osh_b200_element_gradients(osh_t h, char const* name)
+{
+  API_TRY
+  need(h && name, "mesh or name is NULL");
+  osh::element_gradients(*M(h), name);
+  sync(M(h));
+  API_CATCH_VOID
+}
+
+void osh_b200_recover_by_volume(osh_t h, char const* name)
+{
+  API_TRY
+  need(h && name, "mesh or name is NULL");
+  osh::recover_by_volume(*M(h), name);
+  sync(M(h));
+  API_CATCH_VOID
+}
+
+void osh_b200_size_from_hessian(osh_t h, char const* hess_name, double const* weights,
+    double min_h, double max_h)
+{
+  API_TRY
+  need(h && hess_name, "mesh or name is NULL");
+  osh::size_from_hessian(*M(h), hess_name, weights, min_h, max_h);
+  sync(M(h));
+  API_CATCH_VOID
+}
+
+unsigned osh_b200_warp_to_limit(osh_t h, double qual_floor)
+{
+  API_TRY
+  need(h != nullptr, "mesh is NULL");
+  u32 r = osh::warp_to_limit(*M(h), qual_floor);
+  sync(M(h));
+  return r;
+  API_CATCH(0)
 }
 
 void osh_b200_set_fp32_filter(osh_t h, int on)

@@ -119,3 +119,52 @@ def job_host_input(G, job: BoxJob, pert=0.1):
         d = coords.reshape(-1, 3) - np.array([cx, cy, cz])
         h = h0 + h1 * np.sqrt(d[:, 0] * d[:, 0] + d[:, 1] * d[:, 1] + d[:, 2] * d[:, 2])
     return coords, conn, h
+
+
+# ---------------------------------------------------------------------------
+# the anisotropic-front workload: a tanh front, its recovered Hessian as the
+# size field, and a rotation warp applied in steps
+
+FRONT_SHARPNESS = 50.0
+HESSIAN_WEIGHT = 2.5e-5     # max_h - w |H| reaches min_h across the front
+MIN_H, MAX_H = 0.002, 0.05
+
+
+def front_field(coords, offset=0.5):
+    """u = tanh(50 (x - offset - 0.1 sin(2 pi y))) at every vertex."""
+    x = np.asarray(coords, dtype=np.float64).reshape(-1, 3)
+    return np.tanh(FRONT_SHARPNESS * (x[:, 0] - offset - 0.1 * np.sin(2.0 * np.pi * x[:, 1])))
+
+
+def rotation_warp(coords, angle):
+    """Displacement that turns every point within 0.5 of the axis x = y = 0.5
+    by angle * 2 (0.5 - r) about that axis (r: distance to it), and leaves the
+    rest in place."""
+    x = np.asarray(coords, dtype=np.float64).reshape(-1, 3)
+    dx, dy = x[:, 0] - 0.5, x[:, 1] - 0.5
+    r = np.sqrt(dx * dx + dy * dy)
+    a = np.arctan2(dy, dx)
+    rot = np.where(r < 0.5, angle * 2.0 * (0.5 - r), 0.0)
+    out = np.zeros_like(x)
+    out[:, 0] = np.cos(a + rot) * r - dx
+    out[:, 1] = np.sin(a + rot) * r - dy
+    return out.ravel()
+
+
+def hessian_size_field(m, dye="dye", weight=HESSIAN_WEIGHT, min_h=MIN_H, max_h=MAX_H):
+    """adapt_size from the recovered Hessian of the vertex field `dye`, the
+    chain the reference's warp test uses (test_warp.cpp:70-83): element
+    gradients, recovery to vertices, again, then size_from_hessian. Works on
+    the library's meshes and on the CPU checkers alike."""
+    d = m.dim() if callable(getattr(m, "dim", None)) else m.dim
+    if m.has_tag(0, "adapt_size"):
+        m.free_tag(0, "adapt_size")
+    m.element_gradients(dye)
+    m.recover_by_volume("grad_" + dye)
+    m.free_tag(d, "grad_" + dye)
+    m.element_gradients("grad_" + dye)
+    m.free_tag(0, "grad_" + dye)
+    m.recover_by_volume("grad_grad_" + dye)
+    m.free_tag(d, "grad_grad_" + dye)
+    m.size_from_hessian("grad_grad_" + dye, [weight], min_h, max_h)
+    m.free_tag(0, "grad_grad_" + dye)

@@ -117,6 +117,11 @@ class _Lib:
                               _u32p, _u32p, _u32p, _f64p, _u32p, _f64p, _u32p, _u32p)
         self.swap_sets = f("swap_sets", C.c_uint, vp, C.c_double, C.c_uint,
                            _u32p, _u32p, _u32p, _u32p, _f64p, _u32p, _u32p)
+        self.element_gradients = f("element_gradients", None, vp, C.c_char_p)
+        self.recover_by_volume = f("recover_by_volume", None, vp, C.c_char_p)
+        self.size_from_hessian = f("size_from_hessian", None, vp, C.c_char_p, C.c_void_p,
+                                   C.c_double, C.c_double)
+        self.warp_to_limit = f("warp_to_limit", C.c_uint, vp, C.c_double)
 
 
 _LIBS: dict = {}
@@ -270,6 +275,26 @@ class CpuMesh:
 
     def adapt(self, size_floor, good_qual, nlayers, max_ops):
         return self.L.adapt(self.h, size_floor, good_qual, nlayers, max_ops)
+
+    def has_tag(self, dim, name):
+        n = self.L.ntags(self.h, dim)
+        return any(self.L.tag_name(self.h, dim, i).decode() == name for i in range(n))
+
+    # size-field producers ----------------------------------------------------
+    def element_gradients(self, name):
+        self.L.element_gradients(self.h, name.encode())
+
+    def recover_by_volume(self, name):
+        self.L.recover_by_volume(self.h, name.encode())
+
+    def size_from_hessian(self, hess_name, weights, min_h, max_h):
+        w = None if weights is None else np.ascontiguousarray(weights, dtype=np.float64)
+        self.L.size_from_hessian(self.h, hess_name.encode(),
+                                 None if w is None else w.ctypes.data_as(C.c_void_p),
+                                 min_h, max_h)
+
+    def warp_to_limit(self, qual_floor):
+        return self.L.warp_to_limit(self.h, qual_floor)
 
     def refine_sets(self, qual_floor):
         ne = self.count(1)

@@ -2786,3 +2786,187 @@ EXPORT u32 or_swap_table(u32 rs, u32* ntri, u32* nmesh, u32* nint, u32* tris,
   }
   return 1;
 }
+
+/* ---- size-field producers ------------------------------------------------ */
+
+/* dot_product (algebra.hpp) over n components */
+static double dot_n(double const* a, double const* b, u32 n)
+{
+  double d = 0;
+  for (u32 i = 0; i < n; ++i) d += a[i] * b[i];
+  return d;
+}
+
+/* element_jacobian / invert_jacobian (jacobian.cpp:7-66) with
+   invert_3x3 / invert_2x2 (algebra.hpp) */
+static void or_invert_jacobian(u32 dim, double in[3][3], double out[3][3])
+{
+  if (dim == 3) {
+    double tmp[3][3], c[3];
+    cross3(in[0], in[1], c);
+    double d = dot3(in[2], c);
+    cross3(in[1], in[2], tmp[0]);
+    cross3(in[2], in[0], tmp[1]);
+    cross3(in[0], in[1], tmp[2]);
+    double s = 1.0 / d;
+    for (u32 i = 0; i < 3; ++i)
+      for (u32 j = 0; j < 3; ++j) tmp[i][j] = tmp[i][j] * s;
+    for (u32 i = 0; i < 3; ++i)
+      for (u32 j = 0; j < 3; ++j) out[i][j] = tmp[j][i];
+  } else if (dim == 2) {
+    double nrm[2][2];
+    for (u32 i = 0; i < 2; ++i)
+      for (u32 j = 0; j < 2; ++j) {
+        nrm[i][j] = 0;
+        for (u32 k = 0; k < 3; ++k) nrm[i][j] += in[i][k] * in[j][k];
+      }
+    double d = nrm[0][0] * nrm[1][1] - nrm[0][1] * nrm[1][0];
+    double inv[2][2];
+    inv[0][0] = nrm[1][1] / d;
+    inv[0][1] = -nrm[0][1] / d;
+    inv[1][0] = -nrm[1][0] / d;
+    inv[1][1] = nrm[0][0] / d;
+    for (u32 i = 0; i < 3; ++i)
+      for (u32 j = 0; j < 3; ++j) out[i][j] = 0;
+    for (u32 i = 0; i < 3; ++i)
+      for (u32 j = 0; j < 2; ++j)
+        for (u32 k = 0; k < 2; ++k) out[i][j] += in[k][i] * inv[k][j];
+  } else {
+    double msq = dot3(in[0], in[0]);
+    for (u32 i = 0; i < 3; ++i) out[i][0] = in[0][i] / msq;
+    for (u32 i = 0; i < 3; ++i)
+      for (u32 j = 1; j < 3; ++j) out[i][j] = 0;
+  }
+}
+
+/* mesh_element_gradients (element_gradients.cpp:15-91) */
+EXPORT void or_element_gradients(omesh* m, char const* name)
+{
+  u32 dim = m->dim, ne = count(m, dim), vpe = DEG[dim][0];
+  otag* t = tags_find(&m->tags[0], name);
+  if (!t) return;
+  u32 nc = t->ncomps;
+  double const* f = (double const*)t->data;
+  u32 const* voe = ask_down(m, dim, 0);
+  double const* x = coords_of(m);
+  double* out = NEW(double, (size_t)ne * nc * 3);
+  for (u32 i = 0; i < ne; ++i) {
+    u32 const* ve = voe + (size_t)i * vpe;
+    double ex[4][3];
+    gather_x(x, ve, vpe, ex);
+    double jac[3][3];
+    for (u32 a = 0; a < 3; ++a)
+      for (u32 b = 0; b < 3; ++b) jac[a][b] = 0;
+    for (u32 a = 0; a < dim; ++a)
+      for (u32 b = 0; b < 3; ++b) jac[b][a] = ex[a + 1][b] - ex[0][b];
+    double jaci[3][3];
+    or_invert_jacobian(dim, jac, jaci);
+    double* g = out + (size_t)i * nc * 3;
+    for (u32 k = 0; k < nc * 3; ++k) g[k] = 0;
+    for (u32 j = 0; j < dim; ++j)
+      for (u32 k = 0; k < nc; ++k)
+        for (u32 l = 0; l < 3; ++l)
+          g[k * 3 + l] += jaci[j][l] * (f[(size_t)ve[j + 1] * nc + k] - f[(size_t)ve[0] * nc + k]);
+  }
+  char gname[256];
+  snprintf(gname, sizeof gname, "grad_%s", name);
+  tags_add(&m->tags[dim], T_F64, gname, nc * 3, X_NOT, out);
+}
+
+/* mesh_recover_by_volume (recover_by_volume.cpp:10-68) */
+EXPORT void or_recover_by_volume(omesh* m, char const* name)
+{
+  u32 dim = m->dim, nv = count(m, 0);
+  otag* t = tags_find(&m->tags[dim], name);
+  if (!t) return;
+  u32 nc = t->ncomps;
+  double const* f = (double const*)t->data;
+  oup* u = ask_up(m, 0, dim);
+  double* sizes = element_sizes(m);
+  double* out = NEW(double, (size_t)nv * nc);
+  for (u32 i = 0; i < nv; ++i) {
+    double* o = out + (size_t)i * nc;
+    for (u32 k = 0; k < nc; ++k) o[k] = 0;
+    double size_sum = 0;
+    for (u32 j = u->offs[i]; j < u->offs[i + 1]; ++j) {
+      u32 e = u->adj[j];
+      double es = sizes[e];
+      size_sum += es;
+      for (u32 k = 0; k < nc; ++k) o[k] += es * f[(size_t)e * nc + k];
+    }
+    for (u32 k = 0; k < nc; ++k) o[k] /= size_sum;
+  }
+  free(sizes);
+  tags_add(&m->tags[0], T_F64, name, nc, X_NOT, out);
+}
+
+/* mesh_size_from_hessian (size_from_hessian.cpp:12-72) */
+EXPORT void or_size_from_hessian(omesh* m, char const* hess_name, double const* weights,
+    double min_h, double max_h)
+{
+  u32 nv = count(m, 0);
+  otag* t = tags_find(&m->tags[0], hess_name);
+  if (!t) return;
+  u32 nhc = t->ncomps, nsol = nhc / 9;
+  double const* hess = (double const*)t->data;
+  double* out = NEW(double, nv);
+  for (u32 i = 0; i < nv; ++i) {
+    double const* hs = hess + (size_t)i * nhc;
+    double total = 0;
+    for (u32 j = 0; j < nsol; ++j) {
+      double norm = sqrt(dot_n(hs, hs, 9));
+      double hw = weights ? weights[j] : 1.0;
+      total += hw * norm;
+      hs += 9;
+    }
+    double o = max_h - total;
+    if (o < min_h) o = min_h;
+    out[i] = o;
+  }
+  tags_add(&m->tags[0], T_F64, "adapt_size", 1, X_NOT, out);
+}
+
+/* mesh_warp_to_limit (warp_to_limit.cpp:14-81); gives up (returns 2) after
+   the halvings that leave the warp without effect, where the reference
+   would loop forever */
+EXPORT u32 or_warp_to_limit(omesh* m, double qual_floor)
+{
+  u32 n = count(m, 0) * 3;
+  otag* xt = tags_find(&m->tags[0], "coordinates");
+  otag* wt = tags_find(&m->tags[0], "warp");
+  if (!xt || !wt) return 2;
+  double const* x = (double const*)xt->data;
+  double const* w = (double const*)wt->data;
+  double* xo = NEW(double, n);
+  double factor = 1;
+  u32 hit = 0;
+  for (u32 i = 0; i < n; ++i) xo[i] = factor * w[i] + x[i];
+  u32 it = 0;
+  for (;;) {
+    /* exceeds_limit: min element quality of the warped coordinates */
+    u32 dim = m->dim, ne = count(m, dim), vpe = DEG[dim][0];
+    u32 const* voe = ask_down(m, dim, 0);
+    double mq = DBL_MAX;
+    for (u32 e = 0; e < ne; ++e) {
+      double ex[4][3];
+      gather_x(xo, voe + (size_t)e * vpe, vpe, ex);
+      double q = element_quality(dim, ex);
+      if (q < mq) mq = q;
+    }
+    if (!(mq < qual_floor)) break;
+    if (++it > 1100) {
+      free(xo);
+      return 2;
+    }
+    hit = 1;
+    factor /= 2;
+    for (u32 i = 0; i < n; ++i) xo[i] = factor * w[i] + x[i];
+  }
+  double* wo = NEW(double, n);
+  for (u32 i = 0; i < n; ++i) wo[i] = -factor * w[i] + w[i];
+  tags_remove(&m->tags[0], "coordinates");
+  tags_remove(&m->tags[0], "warp");
+  tags_add(&m->tags[0], T_F64, "coordinates", 3, X_NOT, xo);
+  tags_add(&m->tags[0], T_F64, "warp", 3, X_NOT, wo);
+  return hit ? 0 : 1;
+}

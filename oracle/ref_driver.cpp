@@ -22,19 +22,23 @@
 #include "collapse_codes.hpp"
 #include "collapses_to_verts.hpp"
 #include "derive_model.hpp"
+#include "element_gradients.hpp"
 #include "doubles.hpp"
 #include "indset.hpp"
 #include "mark.hpp"
 #include "mesh.hpp"
 #include "parallel_mesh.hpp"
 #include "quality.hpp"
+#include "recover_by_volume.hpp"
 #include "refine.hpp"
 #include "refine_qualities.hpp"
 #include "size.hpp"
+#include "size_from_hessian.hpp"
 #include "swap.hpp"
 #include "swap_qualities.hpp"
 #include "tables.hpp"
 #include "tag.hpp"
+#include "warp_to_limit.hpp"
 
 using namespace omega_h;
 
@@ -407,6 +411,22 @@ unsigned refd_swap_sets(void* p, double good_qual, unsigned nlayers,
   loop_free(q);
   loop_free(rs);
   return any;
+}
+
+
+// size-field producers (element_gradients.cpp, recover_by_volume.cpp,
+// size_from_hessian.cpp, warp_to_limit.cpp); callers only warp meshes whose
+// unwarped quality meets the floor, so the halving loop ends
+void refd_element_gradients(void* p, char const* name) { mesh_element_gradients(M(p), name); }
+void refd_recover_by_volume(void* p, char const* name) { mesh_recover_by_volume(M(p), name); }
+void refd_size_from_hessian(void* p, char const* hess_name, double const* weights,
+    double min_h, double max_h)
+{
+  mesh_size_from_hessian(M(p), hess_name, weights, min_h, max_h);
+}
+unsigned refd_warp_to_limit(void* p, double qual_floor)
+{
+  return mesh_warp_to_limit(M(p), qual_floor);
 }
 
 }

@@ -77,3 +77,37 @@ def radial_size_np(coords, center, h0, h1):
     """h0 + h1 |x - c|, evaluated in the oracle's operation order."""
     d = coords.reshape(-1, 3) - center
     return h0 + h1 * np.sqrt(d[:, 0] * d[:, 0] + d[:, 1] * d[:, 1] + d[:, 2] * d[:, 2])
+
+
+def vertex_field(m, name):
+    for t in m.tags(0):
+        if t.name == name:
+            return t.data
+    return None
+
+
+def front_warp_run(m, steps=2, angle=0.25, weight=4e-4, min_h=0.04, max_h=0.2,
+                   warp_floor=0.2, adapt=True):
+    """The reference's warp-test flow (test_warp.cpp:70-98) at test sizes on
+    any of the three implementations: a tanh front carried as the vertex
+    field "dye", its recovered-Hessian size field, mesh_adapt, then warp
+    steps (rotation field, warp_to_limit, new size field, adapt until the
+    warp is used up). Returns the warp_to_limit results."""
+    from omega_h_v1_b200 import workloads as W
+    m.add_field(0, "dye", W.front_field(vertex_field(m, "coordinates")))
+    W.hessian_size_field(m, weight=weight, min_h=min_h, max_h=max_h)
+    if adapt:
+        m.adapt(1 / 3., 0.3, 4, 50)
+    oks = []
+    for _ in range(steps):
+        m.add_field(0, "warp", W.rotation_warp(vertex_field(m, "coordinates"), angle), 3)
+        for _ in range(3):
+            ok = m.warp_to_limit(warp_floor)
+            oks.append(ok)
+            W.hessian_size_field(m, weight=weight, min_h=min_h, max_h=max_h)
+            if adapt:
+                m.adapt(1 / 3., 0.3, 4, 50)
+            if ok:
+                break
+        m.free_tag(0, "warp")
+    return oks
