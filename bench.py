@@ -616,6 +616,125 @@ def run_serving(args, world, rank, local):
     }
 
 
+WARP_N, WARP_STEPS, WARP_ANGLE = 96, 8, 0.5
+WARP_ARGS = (1.0 / 3.0, 0.4, 0, 500)   # test_warp.cpp's floors; a pass cap the front needs
+WARP_QUAL_FLOOR = 0.1
+
+
+def run_warp(args, world, rank, local):
+    """The anisotropic-front workload: a 96^3 box, u = tanh(50 (x - 0.5 -
+    0.1 sin 2 pi y)) carried as a vertex field, adapt_size from its recovered
+    Hessian (min_h 0.002, max_h 0.05), mesh_adapt, then 8 warp steps rotating
+    the region within 0.5 of the axis x = y = 0.5 by 0.5 rad in total, each
+    warp_to_limit (floor 0.1), new size field and mesh_adapt until the warp
+    is used up. value = elements entering adapt passes / time in adapt calls."""
+    import torch
+    import omega_h_v1_b200 as G
+    from omega_h_v1_b200 import workloads as W
+    torch.cuda.set_device(local)
+    L = G.lib()
+    stream = torch.cuda.default_stream()
+    coords, conn, _ = G.box(WARP_N, 0, 0.1)
+    m = G.Mesh.reduced(3, coords, conn)
+    m.derive_model_full()
+    L.osh_b200_set_stream(m.h, C.c_void_p(0))
+    m.add_field(0, "dye", W.front_field(coords))
+    tets_in = m.count(3)
+    ev = []
+
+    def adapt():
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        m.adapt(*WARP_ARGS)
+        e1.record(stream)
+        p, e = C.c_uint(), C.c_double()
+        L.osh_b200_adapt_stats(C.byref(p), C.byref(e))
+        ev.append((e0, e1, e.value, p.value))
+
+    def field_xyz(name):
+        p = L.osh_get_field(m.h, 0, name.encode())
+        G.check()
+        out = np.empty(m.count(0) * 3, np.float64)
+        L.osh_b200_copy_to_host(out.ctypes.data_as(C.c_void_p), p, out.nbytes)
+        return out
+
+    clocks = Clocks(local)
+    launches0 = L.osh_b200_launch_count()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    W.hessian_size_field(m)
+    adapt()
+    tries = []
+    for _ in range(WARP_STEPS):
+        m.add_field(0, "warp", W.rotation_warp(field_xyz("coordinates"),
+                                               WARP_ANGLE / WARP_STEPS), 3)
+        for k in range(4):
+            ok = m.warp_to_limit(WARP_QUAL_FLOOR)
+            W.hessian_size_field(m)
+            adapt()
+            if ok:
+                break
+        tries.append(k + 1)
+        m.free_tag(0, "warp")
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    clk = clocks.stop()
+    launches = L.osh_b200_launch_count() - launches0
+    adapt_ms = sum(a.elapsed_time(b) for a, b, _, _ in ev)
+    elems = sum(e for _, _, e, _ in ev)
+    passes = sum(p for _, _, _, p in ev)
+    out = {
+        "metric": METRIC, "value": round(elems / (adapt_ms / 1e3), 1), "unit": UNIT,
+        "n_gpus": world, "steps": 1, "warmup": 0, "ms_per_step": round(adapt_ms, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded 96^3 box, tanh front, rotation warp)",
+        "config": {"workload": "front_warp_box96", "box_n": WARP_N, "tets_in": tets_in,
+                   "field": "tanh(50(x-0.5-0.1 sin 2 pi y)), Hessian weight %g" %
+                            W.HESSIAN_WEIGHT,
+                   "min_h": W.MIN_H, "max_h": W.MAX_H, "warp_steps": WARP_STEPS,
+                   "rotation_rad": WARP_ANGLE, "warp_floor": WARP_QUAL_FLOOR,
+                   "adapt": "mesh_adapt(1/3, 0.4, 0, 500) after each warp",
+                   "l2": "inputs larger than L2 (5.3M to 30M tets resident)"},
+        "adapt_calls": len(ev), "passes": passes, "elems_in": elems,
+        "tets_out": m.count(3), "warp_tries": tries, "procedure_s": round(wall, 3),
+        "gpu_launches": int(launches), "clocks": clk,
+    }
+    m.close()
+    return out
+
+
+def warp_cpu_sample():
+    """The reference's OpenMP build on the front workload's first stage:
+    the Hessian size field and the first mesh_adapt of the 96^3 box."""
+    from oracle import oracle as O
+    import omega_h_v1_b200 as G
+    from omega_h_v1_b200 import workloads as W
+    if not O.have_reference():
+        return None
+    lib = O._lib(O.REF_OMP_SO, "refd_").lib
+    lib.refd_adapt_counted.restype = C.c_uint
+    lib.refd_adapt_counted.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_uint,
+                                       C.c_uint, C.POINTER(C.c_uint), C.POINTER(C.c_double)]
+    coords, conn, _ = G.box(WARP_N, 0, 0.1)
+    m = O.Reference(3, coords, conn)
+    m.derive_model_full()
+    m.add_field(0, "adapt_size", np.full(coords.size // 3, W.MAX_H))
+    m.add_field(0, "dye", W.front_field(coords))
+    p, e = C.c_uint(), C.c_double()
+    with _Quiet():
+        t0 = time.perf_counter()
+        W.hessian_size_field(m)
+        lib.refd_adapt_counted(m.h, *WARP_ARGS, C.byref(p), C.byref(e))
+        secs = time.perf_counter() - t0
+    m.close()
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    return {"value": round(e.value / secs, 1), "unit": UNIT, "cores": cores,
+            "kind": "reference",
+            "sample": "size field and first mesh_adapt of the 96^3 front workload "
+                      "(%d passes, %.0f tets in)" % (p.value, e.value)}
+
+
 def batched_cpu_sample(jobs, budget_est_tets=12e6):
     """The reference's OpenMP mesh_adapt on the first jobs of the seeded list
     (up to budget_est_tets estimated output tets)."""
@@ -649,7 +768,7 @@ def batched_cpu_sample(jobs, budget_est_tets=12e6):
     cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
     return {"value": round(elems / secs, 1), "unit": UNIT, "cores": cores,
             "kind": "reference",
-            "sample": "mesh_adapt of the first %d of the 512 seeded meshes (%.0f tets in "
+            "sample": "mesh_adapt of the first %d jobs of the seeded list (%.0f tets in "
                       "over their passes)" % (used, elems)}
 
 
@@ -746,10 +865,12 @@ def main():
                     help="DRAM bytes per launch of that kernel from an ncu capture")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling)")
-    ap.add_argument("--workload", default="box48", choices=["box48", "batched", "serving"],
+    ap.add_argument("--workload", default="box48",
+                    choices=["box48", "batched", "serving", "warp"],
                     help="box48: the 48^3 radial-size adapt; batched: 512 uneven boxes, "
                          "plain one-by-one path against adapt_batch; serving: Poisson "
-                         "stream of jobs through the continuous-batching server")
+                         "stream of jobs through the continuous-batching server; warp: "
+                         "96^3 tanh-front Hessian size field with 8 warp steps")
     ap.add_argument("--batch-count", type=int, default=512)
     ap.add_argument("--batch-nmax", type=int, default=40,
                     help="largest grid edge of the batched boxes (40 = the full workload)")
@@ -769,10 +890,18 @@ def main():
         out = run_batched(args, world, rank, local)
     elif args.workload == "serving":
         out = run_serving(args, world, rank, local)
+    elif args.workload == "warp":
+        out = run_warp(args, world, rank, local)
     else:
         out = run_ours(args, world, rank, local)
     if rank == 0:
-        if not args.no_cpu:
+        if not args.no_cpu and args.workload == "serving":
+            from omega_h_v1_b200 import workloads as W
+            out["cpu_baseline"] = batched_cpu_sample(
+                W.serving_stream(args.serve_count, seed=2, rate=args.rate), 20e6)
+        elif not args.no_cpu and args.workload == "warp":
+            out["cpu_baseline"] = warp_cpu_sample()
+        elif not args.no_cpu and args.workload == "box48":
             r = cpu_reference_run(1, 1)
             if r is not None:
                 v, cores, sample, _ = r
