@@ -2,6 +2,8 @@
 // (coarsen.cpp:13-70, coarsen_common.cpp:29-239, check_collapse_class.cpp,
 // coarsen_qualities.cpp:12-79, collapses_to_verts.cpp, collapses_to_ents.cpp,
 // coarsen_topology.cpp, coarsen_conserve.cpp, coarsen_fit.cpp, qr.cpp).
+#include <algorithm>
+
 #include "passes.hpp"
 
 namespace osh {
@@ -100,76 +102,140 @@ __global__ void k_check_exposed_sides(u32 ed, u32 ne, u32 const* __restrict__ u_
 }
 
 // coarsen_quality (coarsen_qualities.cpp:12-79): worst element of the cavity
-// after collapsing each allowed direction
-__global__ void k_coarsen_quality(u32 dim, u32 ne, u32 const* __restrict__ voe1,
-    u32 const* __restrict__ voe, u32 const* __restrict__ ev_offs,
-    u32 const* __restrict__ ev, u32 const* __restrict__ ev_dirs,
-    double const* __restrict__ x, double const* __restrict__ eq, double floor_q,
-    SegView sv, Fp32Stats* fs, u32* __restrict__ codes, double* __restrict__ out, u32* any)
+// after collapsing each allowed direction. One warp per candidate edge (from
+// a compact list): the lanes share the collapsing vertex's elements, so a
+// few candidates with long rows no longer idle the other lanes of a warp.
+// Each minimum is reduced as (value, position) pairs, so the value kept is
+// the one the sequential loop keeps: the first in row order among equals
+// (which decides the sign of a zero), with NaN never taken.
+struct FirstMin {
+  double v;
+  u32 k;  // 0 = the loop's initial value, else 1 + position in the row
+};
+
+__device__ inline void first_min_add(FirstMin& m, double q, u32 k)
 {
-  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
-  u32 keep = 0;
-  if (i < ne) {
+  if (q < m.v) {
+    m.v = q;
+    m.k = k;
+  }
+}
+
+__device__ inline double warp_first_min(FirstMin m)
+{
+  for (int o = 16; o; o >>= 1) {
+    double ov = __shfl_xor_sync(0xffffffffu, m.v, o);
+    u32 ok = __shfl_xor_sync(0xffffffffu, m.k, o);
+    if (ov < m.v || (ov == m.v && ok < m.k)) {
+      m.v = ov;
+      m.k = ok;
+    }
+  }
+  return m.v;
+}
+
+__device__ inline float warp_minf(float v)
+{
+  for (int o = 16; o; o >>= 1) v = fminf(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+__global__ void k_coarsen_quality(u32 dim, u32 const* __restrict__ list,
+    u32 const* __restrict__ nlist, u32 const* __restrict__ voe1, u32 const* __restrict__ voe,
+    u32 const* __restrict__ ev_offs, u32 const* __restrict__ ev,
+    u32 const* __restrict__ ev_dirs, double const* __restrict__ x,
+    double const* __restrict__ eq, double floor_q, SegView sv, Fp32Stats* fs,
+    u32* __restrict__ codes, double* __restrict__ out, u32* any)
+{
+  u32 lane = threadIdx.x & 31;
+  u32 n = *nlist;
+  u32 vpe = deg(dim, 0);
+  double const perfect = dim == 3 ? perfect_tet_quality() : perfect_tri_quality();
+  bool const use32 = fs && dim == 3;
+  for (u32 w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < n;
+       w += (gridDim.x * blockDim.x) >> 5) {
+    u32 i = list[w];
     u32 code = codes[i];
-    if (code != DONT_COLLAPSE) {
-      u32 vpe = deg(dim, 0);
-      double const perfect = dim == 3 ? perfect_tet_quality() : perfect_tri_quality();
-      double const fq = seg_floor(sv, voe1[i * 2], floor_q);
-      for (u32 j = 0; j < 2; ++j) {
-        if (!collapses(code, j)) continue;
-        double minq = 1, old_minq = 1;
-        u32 col = voe1[i * 2 + j], gen = voe1[i * 2 + 1 - j];
-        double ex[4][3];
-        load3(x, gen, ex[vpe - 1]);
-        if (fs && dim == 3) {
-          // reject on the estimate when the cavity's worst element is surely
-          // below the floor, or surely no better than before
-          float upper = 1.0f;
-          for (u32 k = ev_offs[col]; k < ev_offs[col + 1]; ++k) {
-            u32 e = ev[k];
-            u32 const* ve = voe + (size_t)e * vpe;
-            if (eq && eq[e] < old_minq) old_minq = eq[e];
-            bool adjacent = false;
-            for (u32 l = 0; l < vpe; ++l)
-              if (ve[l] == gen) adjacent = true;
-            if (adjacent) continue;
-            u32 base = opp(dim, 0, ev_dirs[k]);
-            for (u32 l = 0; l + 1 < vpe; ++l) load3(x, ve[canon(dim, dim - 1, 0, base, l)], ex[l]);
-            Q32 q = tet_quality_f32(ex, (float)perfect);
-            upper = fminf(upper, q.q + q.err);
-          }
-          if ((double)upper < fq || (eq && (double)upper <= old_minq)) {
-            atomicAdd(&fs->decided, 1ull);
-            code &= ~(1u << j);
-            continue;
-          }
-          atomicAdd(&fs->rechecked, 1ull);
-          old_minq = 1;
-        }
-        for (u32 k = ev_offs[col]; k < ev_offs[col + 1]; ++k) {
-          u32 e = ev[k];
-          u32 const* ve = voe + (size_t)e * vpe;
-          if (eq && eq[e] < old_minq) old_minq = eq[e];
+    double const fq = seg_floor(sv, voe1[i * 2], floor_q);
+    for (u32 j = 0; j < 2; ++j) {
+      if (!collapses(code, j)) continue;
+      u32 col = voe1[i * 2 + j], gen = voe1[i * 2 + 1 - j];
+      u32 f = ev_offs[col], e = ev_offs[col + 1];
+      double ex[4][3];
+      load3(x, gen, ex[vpe - 1]);
+      FirstMin om{1.0, 0};
+      if (eq)
+        for (u32 k = f + lane; k < e; k += 32) first_min_add(om, eq[ev[k]], k - f + 1);
+      double old_minq = warp_first_min(om);
+      float upper = 1.0f;
+      if (use32) {
+        // reject on the estimate when the cavity's worst element is surely
+        // below the floor, or surely no better than before
+        for (u32 k = f + lane; k < e; k += 32) {
+          u32 const* ve = voe + (size_t)ev[k] * vpe;
           bool adjacent = false;
-          for (u32 l = 0; l < vpe; ++l)
-            if (ve[l] == gen) adjacent = true;
+          for (u32 l = 0; l < vpe; ++l) adjacent = adjacent || ve[l] == gen;
           if (adjacent) continue;
           u32 base = opp(dim, 0, ev_dirs[k]);
           for (u32 l = 0; l + 1 < vpe; ++l) load3(x, ve[canon(dim, dim - 1, 0, base, l)], ex[l]);
-          double q = dim == 3 ? tet_quality(ex, perfect) : tri_quality(ex, 1, perfect);
-          if (fs && dim == 3) fp32_note_error(fs, tet_quality_f32(ex, (float)perfect), q);
-          if (q < minq) minq = q;
+          Q32 q = tet_quality_f32(ex, (float)perfect);
+          upper = fminf(upper, q.q + q.err);
         }
-        if (minq < fq || (eq && minq <= old_minq))
+        upper = warp_minf(upper);
+        if ((double)upper < fq || (eq && (double)upper <= old_minq)) {
+          if (lane == 0) atomicAdd(&fs->decided, 1ull);
           code &= ~(1u << j);
-        else
-          out[i * 2 + j] = minq;
+          continue;
+        }
+        if (lane == 0) atomicAdd(&fs->rechecked, 1ull);
       }
+      FirstMin mm{1.0, 0};
+      for (u32 k = f + lane; k < e; k += 32) {
+        u32 const* ve = voe + (size_t)ev[k] * vpe;
+        bool adjacent = false;
+        for (u32 l = 0; l < vpe; ++l) adjacent = adjacent || ve[l] == gen;
+        if (adjacent) continue;
+        u32 base = opp(dim, 0, ev_dirs[k]);
+        for (u32 l = 0; l + 1 < vpe; ++l) load3(x, ve[canon(dim, dim - 1, 0, base, l)], ex[l]);
+        if (use32) {
+          // only an element whose estimate - bound reaches `upper` can hold
+          // the minimum; the others are not computed in double
+          Q32 q32 = tet_quality_f32(ex, (float)perfect);
+          if ((double)q32.q - (double)q32.err > (double)upper) continue;
+          double q = tet_quality(ex, perfect);
+          fp32_note_error(fs, q32, q);
+          first_min_add(mm, q, k - f + 1);
+        } else {
+          first_min_add(mm, dim == 3 ? tet_quality(ex, perfect) : tri_quality(ex, 1, perfect),
+              k - f + 1);
+        }
+      }
+      double minq = warp_first_min(mm);
+      if (minq < fq || (eq && minq <= old_minq))
+        code &= ~(1u << j);
+      else if (lane == 0)
+        out[i * 2 + j] = minq;
+    }
+    if (lane == 0) {
       codes[i] = code;
-      keep = code != DONT_COLLAPSE;
+      if (code != DONT_COLLAPSE) atomicOr(any, 1u);
     }
   }
-  if (__any_sync(0xffffffffu, keep) && (threadIdx.x & 31) == 0) atomicOr(any, 1u);
+}
+
+// ids of the entities with a nonzero flag, in no particular order
+__global__ void k_list_nonzero(u32 n, u32 const* __restrict__ flags, u32* __restrict__ list,
+    u32* count)
+{
+  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+  bool on = i < n && flags[i] != 0;
+  u32 mask = __ballot_sync(0xffffffffu, on);
+  if (!mask) return;
+  u32 lane = threadIdx.x & 31, leader = __ffs(mask) - 1;
+  u32 base = 0;
+  if (lane == leader) base = atomicAdd(count, (u32)__popc(mask));
+  base = __shfl_sync(0xffffffffu, base, leader);
+  if (on) list[base + __popc(mask & ((1u << lane) - 1u))] = i;
 }
 
 // collapse_to_vert (collapses_to_verts.cpp:13-42)
@@ -527,7 +593,20 @@ static bool coarsen_select(Mesh& m, u32* codes, double qual_floor, bool require_
     CK(cudaMemcpyAsync(codes_class_out, codes, sizeof(u32) * ne, cudaMemcpyDeviceToDevice, s));
   if (codes_qual_out)
     CK(cudaMemcpyAsync(codes_qual_out, codes, sizeof(u32) * ne, cudaMemcpyDeviceToDevice, s));
-  if (!max_u32(codes, ne, s)) return false;
+  // the candidate edges, listed (this read-back also tells whether any is left)
+  u32* clist = dalloc<u32>(ne ? ne : 1, s);
+  u32* ncand = m.mb->dev + 7;
+  CK(cudaMemsetAsync(ncand, 0, sizeof(u32), s));
+  if (ne) {
+    k_list_nonzero<<<grid_for(ne), BLOCK, 0, s>>>(ne, codes, clist, ncand);
+    CK_LAUNCH();
+  }
+  m.mb->fetch(s, 8);
+  u32 nc = m.mb->host[7];
+  if (!nc) {
+    dev_free(clist, s);
+    return false;
+  }
   sel.q2 = dalloc<double>((size_t)ne * 2, s);
   CK(cudaMemsetAsync(sel.q2, 0, sizeof(double) * ne * 2, s));
   u32* any = m.mb->dev + 4;
@@ -535,16 +614,16 @@ static bool coarsen_select(Mesh& m, u32* codes, double qual_floor, bool require_
   if (dim >= 2) {
     double const* eq = require_better ? m.qualities() : nullptr;
     UpAdj const& ev = m.ask_up(0, dim, false);
-    if (ne) {
-      double nel = m.counts[dim];
-      PROBE(P_COARSEN_QUALITY, s, 4.0 * (nv + 1) + 8.0 * deg(dim, 0) * nel + 8.0 * ne +
-          4.0 * deg(dim, 0) * nel + 24.0 * nv + 8.0 * ne + 16.0 * ne);
-      k_coarsen_quality<<<grid_for(ne), BLOCK, 0, s>>>(dim, ne, voe1, m.ask_down(dim, 0),
-          ev.offs, ev.adj, ev.dirs, m.coords(), eq, qual_floor, m.segview(),
-          m.fp32_filter ? fp32_stats_dev() : nullptr, codes, sel.q2, any);
-      CK_LAUNCH();
-    }
+    double nel = m.counts[dim];
+    PROBE(P_COARSEN_QUALITY, s, 4.0 * (nv + 1) + 8.0 * deg(dim, 0) * nel + 8.0 * ne +
+        4.0 * deg(dim, 0) * nel + 24.0 * nv + 8.0 * ne + 16.0 * ne);
+    u32 blocks = (u32)std::min<u64>(ceil_div((u64)nc * 32, BLOCK), 148u * 64u);
+    k_coarsen_quality<<<blocks, BLOCK, 0, s>>>(dim, clist, ncand, voe1, m.ask_down(dim, 0),
+        ev.offs, ev.adj, ev.dirs, m.coords(), eq, qual_floor, m.segview(),
+        m.fp32_filter ? fp32_stats_dev() : nullptr, codes, sel.q2, any);
+    CK_LAUNCH();
   }
+  dev_free(clist, s);
   if (codes_qual_out)
     CK(cudaMemcpyAsync(codes_qual_out, codes, sizeof(u32) * ne, cudaMemcpyDeviceToDevice, s));
   if (!read_u32(any, s)) return false;

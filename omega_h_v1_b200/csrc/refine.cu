@@ -88,6 +88,36 @@ __global__ void k_refine_quality(u32 dim, u32 ne, u32 const* __restrict__ voe1,
         filtered = true;
         atomicAdd(&fs->decided, 1ull);
         cand[i] = 0;
+      } else if (upright) {
+        // the worst child has estimate - bound <= upper: only such children
+        // are computed in double, in order, and their minimum is exact
+        atomicAdd(&fs->rechecked, 1ull);
+        filtered = true;
+        double minq = 1;
+        for (u32 j = eo_offs[i]; j < eo_offs[i + 1]; ++j) {
+          u32 dir = eo_dirs[j], e = eo[j];
+          u32 const* ve = voe + (size_t)e * vpe;
+          for (u32 k = 0; k < 2; ++k) {
+            u32 o = canon(dim, 1, 0, dir, k);
+            u32 base = opp(dim, 0, o);
+            double ex[4][3];
+            for (u32 l = 0; l + 1 < vpe; ++l) load3(x, ve[canon(dim, dim - 1, 0, base, l)], ex[l]);
+            ex[3][0] = split[0];
+            ex[3][1] = split[1];
+            ex[3][2] = split[2];
+            Q32 q32 = tet_quality_f32(ex, (float)perfect);
+            if ((double)q32.q - (double)q32.err > (double)upper) continue;
+            double q = tet_quality(ex, perfect);
+            fp32_note_error(fs, q32, q);
+            if (q < minq) minq = q;
+          }
+        }
+        if (minq < fl) {
+          cand[i] = 0;
+        } else {
+          out[i] = minq;
+          keep = 1;
+        }
       } else {
         atomicAdd(&fs->rechecked, 1ull);
       }
@@ -106,7 +136,6 @@ __global__ void k_refine_quality(u32 dim, u32 ne, u32 const* __restrict__ voe1,
         ex[vpe - 1][1] = split[1];
         ex[vpe - 1][2] = split[2];
         double q = dim == 3 ? tet_quality(ex, perfect) : tri_quality(ex, 0, perfect);
-        if (fs && dim == 3) fp32_note_error(fs, tet_quality_f32(ex, (float)perfect), q);
         if (!(q > 0)) atomicOr(inverted, 1u);
         if (q < minq) minq = q;
       }

@@ -58,3 +58,18 @@ def test_filter_in_a_batch():
     G.adapt_batch(filt, *ARGS)
     for x, y in zip(plain, filt):
         assert x.digest() == y.digest()
+
+
+def test_filter_in_the_front_warp_flow():
+    """Graded Hessian sizes and warped (poorly shaped) elements: the cases
+    where most qualities are computed only in single precision."""
+    import omega_h_v1_b200 as G
+    from conftest import front_warp_run
+    a = build_gpu(10, size=0.1)
+    b = a.clone()
+    b.set_fp32_filter(True)
+    G.fp32_stats(reset=True)
+    assert front_warp_run(a, angle=0.4) == front_warp_run(b, angle=0.4)
+    assert a.digest() == b.digest()
+    st = G.fp32_stats(reset=True)
+    assert st["bound_exceeded"] == 0 and st["decided"] > 0
