@@ -278,7 +278,10 @@ def run_ours(args, world, rank, local):
     ev0.record(stream)
     npass = []
     for i in range(args.warmup, nsteps):
+        # a step adapts its resident copy and releases the result (as the
+        # warm-up steps did), so the device pool holds one step's memory
         e, p = adapt(copies[i])
+        L.osh_free(copies[i])
         elems.append(e)
         npass.append(p)
     ev1.record(stream)
@@ -290,8 +293,6 @@ def run_ours(args, world, rank, local):
     ms_local = ev0.elapsed_time(ev1)
     plaunch, pms, pbytes = C.c_uint(), C.c_double(), C.c_double()
     L.osh_b200_probe_read(probe_id, C.byref(plaunch), C.byref(pms), C.byref(pbytes))
-    for i in range(args.warmup, nsteps):
-        L.osh_free(copies[i])
     value, ms, units = replica_throughput(float(sum(elems)), ms_local, world)
 
     e2e = None
@@ -360,6 +361,18 @@ BATCH_CHUNK_EST_TETS = 60e6     # estimated output tets per adapt_batch call
 BATCH_UNION_ELEMS = 1000000     # current elements per union inside a call
 
 
+def reserve_pool(G, fraction=0.5):
+    """Grow the library's device memory pool up front (input preparation, not
+    timed), as a long-running service would, so that growing meshes do not
+    pay for pool growth inside their passes; returns the bytes reserved."""
+    import torch
+    free, _ = torch.cuda.mem_get_info()
+    nbytes = int(fraction * free)
+    G.pool_reserve(nbytes)
+    G.pool_stats(reset_high=True)
+    return nbytes
+
+
 def batch_times(L):
     c, p, s = C.c_double(), C.c_double(), C.c_double()
     L.osh_b200_batch_times(C.byref(c), C.byref(p), C.byref(s))
@@ -394,6 +407,7 @@ def run_batched(args, world, rank, local):
     L = G.lib()
     stream = torch.cuda.default_stream()
     jobs = W.batched_boxes(args.batch_count, seed=1, nmax=args.batch_nmax)
+    reserve_pool(G)
     t0 = time.perf_counter()
     bases = [W.build_job_mesh(G, j) for j in jobs]
     prep_s = time.perf_counter() - t0
@@ -522,6 +536,7 @@ def run_batched(args, world, rank, local):
         "union_secs": batch_secs,
         "gpu_launches": int(batch_launches), "clocks": clk,
         "prep_s": round(prep_s, 1),
+        "device_peak_bytes": G.pool_stats()["peak"],
     }
     if not args.no_cpu and rank == 0:
         out["cpu_baseline"] = batched_cpu_sample(jobs)
@@ -541,6 +556,7 @@ def run_serving(args, world, rank, local):
     inputs = [W.job_host_input(G, j) for j in jobs]
     free, total = torch.cuda.mem_get_info()
     budget = int(0.6 * free)
+    reserve_pool(G)
     # warm-up: two small jobs through a throwaway server
     warm = G.Server(SIZE_FLOOR, GOOD_QUAL, NLAYERS, MAX_OPS, budget)
     small = sorted(range(len(jobs)), key=lambda i: jobs[i].tets)[:2]
@@ -608,6 +624,7 @@ def run_serving(args, world, rank, local):
                        "max": round(float(lat[-1]) * 1e3, 2)},
         "mean_active_jobs": round(float(np.mean(active_samples)), 2) if active_samples else 0,
         "server_steps": st["steps"], "elems_in": elems,
+        "device_peak_bytes": G.pool_stats()["peak"],
         "server_secs": {k: round(st[k], 3) for k in
                         ("secs_admit", "secs_join", "secs_passes", "secs_retire")},
         "submit_secs": round(submit_secs, 3),
@@ -634,6 +651,7 @@ def run_warp(args, world, rank, local):
     torch.cuda.set_device(local)
     L = G.lib()
     stream = torch.cuda.default_stream()
+    reserve_pool(G)
     coords, conn, _ = G.box(WARP_N, 0, 0.1)
     m = G.Mesh.reduced(3, coords, conn)
     m.derive_model_full()
@@ -698,6 +716,7 @@ def run_warp(args, world, rank, local):
                    "l2": "inputs larger than L2 (5.3M to 30M tets resident)"},
         "adapt_calls": len(ev), "passes": passes, "elems_in": elems,
         "tets_out": m.count(3), "warp_tries": tries, "procedure_s": round(wall, 3),
+        "device_peak_bytes": G.pool_stats()["peak"],
         "gpu_launches": int(launches), "clocks": clk,
     }
     m.close()

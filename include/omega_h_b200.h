@@ -118,6 +118,18 @@ void osh_b200_fp32_stats(unsigned long long* decided, unsigned long long* rechec
     double* max_error, unsigned* bound_exceeded) OSH_PUBLIC;
 void osh_b200_fp32_stats_reset(void) OSH_PUBLIC;
 
+/* ---- device memory -------------------------------------------------------- */
+/* All device memory of this library comes from the current device's default
+   memory pool, which keeps what it has grown to. osh_b200_pool_reserve grows
+   it to at least `bytes` up front, so that a workload whose meshes grow does
+   not pay for growing the pool inside its passes. osh_b200_pool_stats reads
+   the bytes the pool holds, the bytes in use and the peak in use (reset to
+   the current use when reset_high is nonzero). No counterpart in the
+   reference. */
+void osh_b200_pool_reserve(unsigned long long bytes) OSH_PUBLIC;
+void osh_b200_pool_stats(unsigned long long* reserved, unsigned long long* used,
+    unsigned long long* used_high, int reset_high) OSH_PUBLIC;
+
 /* order-sensitive 64-bit digest of a mesh (connectivity of every dimension,
    tag names, kinds and data, global numbers), computed on the device; equal
    meshes give equal digests. No counterpart in the reference. */

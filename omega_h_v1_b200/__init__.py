@@ -136,6 +136,8 @@ def lib():
     f("osh_b200_batch_mesh_stats", None, C.c_uint, C.POINTER(C.c_uint), C.POINTER(C.c_double))
     f("osh_b200_batch_times", None, *([C.POINTER(C.c_double)] * 3))
     f("osh_b200_digest", C.c_ulonglong, vp)
+    f("osh_b200_pool_reserve", None, C.c_ulonglong)
+    f("osh_b200_pool_stats", None, *([C.POINTER(C.c_ulonglong)] * 3), C.c_int)
     f("osh_b200_set_fp32_filter", None, vp, C.c_int)
     f("osh_b200_element_gradients", None, vp, C.c_char_p)
     f("osh_b200_recover_by_volume", None, vp, C.c_char_p)
@@ -488,6 +490,20 @@ def fp32_stats(reset=False):
         L.osh_b200_fp32_stats_reset()
         check()
     return dict(decided=d.value, rechecked=r.value, max_error=e.value, bound_exceeded=b.value)
+
+
+def pool_reserve(nbytes):
+    """Grow the device memory pool to at least nbytes now."""
+    lib().osh_b200_pool_reserve(int(nbytes))
+    check()
+
+
+def pool_stats(reset_high=False):
+    """Bytes the device pool holds, bytes in use, and the peak in use."""
+    r, u, h = C.c_ulonglong(), C.c_ulonglong(), C.c_ulonglong()
+    lib().osh_b200_pool_stats(C.byref(r), C.byref(u), C.byref(h), 1 if reset_high else 0)
+    check()
+    return dict(reserved=r.value, used=u.value, peak=h.value)
 
 
 def adapt_batch(meshes, size_floor, good_qual, nlayers, max_ops, max_union_elems=0):

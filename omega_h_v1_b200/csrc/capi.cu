@@ -694,6 +694,21 @@ void osh_b200_fp32_stats_reset(void)
   API_CATCH_VOID
 }
 
+void osh_b200_pool_reserve(unsigned long long bytes)
+{
+  API_TRY
+  osh::pool_reserve(bytes);
+  API_CATCH_VOID
+}
+
+void osh_b200_pool_stats(unsigned long long* reserved, unsigned long long* used,
+    unsigned long long* used_high, int reset_high)
+{
+  API_TRY
+  osh::pool_stats(reserved, used, used_high, reset_high);
+  API_CATCH_VOID
+}
+
 unsigned long long osh_b200_digest(osh_t h)
 {
   API_TRY

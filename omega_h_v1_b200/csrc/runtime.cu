@@ -220,6 +220,41 @@ void* dev_alloc(size_t bytes, cudaStream_t s)
   return p;
 }
 
+void pool_reserve(unsigned long long bytes)
+{
+  setup_pool();
+  if (!bytes) return;
+  void* p = nullptr;
+  cudaError_t e = cudaMallocAsync(&p, bytes, 0);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    throw Failure(E_NOMEM, "could not reserve the requested device memory");
+  }
+  CK(cudaFreeAsync(p, 0));
+  CK(cudaStreamSynchronize(0));
+}
+
+void pool_stats(unsigned long long* reserved, unsigned long long* used,
+    unsigned long long* used_high, int reset_high)
+{
+  setup_pool();
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  cudaMemPool_t pool;
+  CK(cudaDeviceGetDefaultMemPool(&pool, dev));
+  unsigned long long r = 0, u = 0, h = 0;
+  CK(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &r));
+  CK(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &u));
+  CK(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemHigh, &h));
+  if (reserved) *reserved = r;
+  if (used) *used = u;
+  if (used_high) *used_high = h;
+  if (reset_high) {
+    unsigned long long zero = 0;
+    CK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrUsedMemHigh, &zero));
+  }
+}
+
 void dev_free(void* p, cudaStream_t s)
 {
   if (p) CK(cudaFreeAsync(p, s));

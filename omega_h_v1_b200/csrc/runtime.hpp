@@ -29,6 +29,12 @@ void check_device_timeouts(cudaStream_t s);
 u32* negate_offsets(u32 const* offs, u32 n, cudaStream_t s);
 
 void fill_u32(u32* a, u32 n, u32 v, cudaStream_t s);
+
+// grow the device's memory pool to at least `bytes` now (the pool keeps what
+// it holds), so that later passes do not pay for growing it
+void pool_reserve(unsigned long long bytes);
+void pool_stats(unsigned long long* reserved, unsigned long long* used,
+    unsigned long long* used_high, int reset_high);
 void iota_u32(u32* a, u32 n, u32 stride, cudaStream_t s);
 void iota_u64(u64* a, u32 n, cudaStream_t s);
 
