@@ -41,6 +41,10 @@ N_BOX = 48
 H0, H1 = 0.01, 0.04
 SIZE_FLOOR, GOOD_QUAL, NLAYERS, MAX_OPS = 1.0 / 3.0, 0.3, 4, 50
 L2_BYTES = 126 * 2 ** 20
+# DRAM bytes (read + write) per launch of the reflect_down kernels over one
+# adapt of this workload, from the ncu capture summarised in
+# profiles/k_reflect_down_box48_adapt.md (mean over the adapt's 37 launches)
+REFLECT_TRAFFIC_PER_LAUNCH = 75.3e6
 
 
 def workload_config():
@@ -309,7 +313,8 @@ def run_ours(args, world, rank, local):
                 "frac": round(achieved / peak, 4), "peak_source": peak_kind,
                 "launches": plaunch.value, "avg_launch_us": round(avg_ms * 1e3, 2),
                 "algorithmic_bytes_per_launch": round(avg_bytes),
-                "traffic": args.traffic}
+                "traffic": args.traffic if args.traffic is not None else
+                (REFLECT_TRAFFIC_PER_LAUNCH if probe_id == 0 else None)}
     base.close()
     return {
         "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world,
