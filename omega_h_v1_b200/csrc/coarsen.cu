@@ -669,6 +669,8 @@ static void coarsen_build(Mesh& m, CoarsenSel const& sel)
   }
   if (m.parallel) inherit_globals(*out, 0, nv_out);
   u32* fused[4] = {nullptr, nullptr, nullptr, nullptr};
+  u32* same_of[4] = {nullptr, nullptr, nullptr, nullptr};
+  u32 nsame_of[4] = {0, 0, 0, 0};
   for (u32 dd = 0; dd < dim; ++dd) {
     u32 ed = dim - dd;
     u32 n = m.count(ed), vpe = deg(ed, 0);
@@ -721,9 +723,18 @@ static void coarsen_build(Mesh& m, CoarsenSel const& sel)
     if (m.parallel) inherit_globals(*out, ed, nout);
     if (ed == dim) coarsen_transfer(m, *out, gen_offs_v, gen_offs, same_e, nsame, ngen);
     dev_free(gen_offs, s);
-    dev_free(same_e, s);
+    same_of[ed] = same_e;
+    nsame_of[ed] = nsame;
   }
-  for (u32 d = 0; d < 4; ++d) dev_free(fused[d], s);
+  // downward adjacency of the survivors carries over; the products are searched
+  for (u32 h = 2; h <= dim; ++h)
+    for (u32 l = 1; l < h; ++l)
+      if (same_of[h] && same_of[l])
+        carry_down(m, *out, h, l, same_of[h], nsame_of[h], same_of[l]);
+  for (u32 d = 0; d < 4; ++d) {
+    dev_free(fused[d], s);
+    dev_free(same_of[d], s);
+  }
   dev_free(gen_offs_v, s);
   dev_free(same_v, s);
   m.overwrite(out);

@@ -28,10 +28,10 @@ static void release_mailbox(Mailbox* m)
 }
 
 Mesh::Mesh(u32 d, bool f, bool p, cudaStream_t stream,
-    std::shared_ptr<Mailbox> mailbox)
+    std::shared_ptr<Mailbox> mailbox, bool exact_stream)
     : dim(d), full(f), parallel(p), s(stream), mb(mailbox)
 {
-  if (!s) {
+  if (!s && !exact_stream) {
     CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
     own_stream = true;
   }
@@ -56,7 +56,8 @@ Mesh::~Mesh()
 
 Mesh* Mesh::spawn() const
 {
-  Mesh* m = new Mesh(dim, full, parallel, s, mb);
+  // the same stream as this mesh, the legacy default stream included
+  Mesh* m = new Mesh(dim, full, parallel, s, mb, true);
   m->nseg = nseg;
   m->ctl = ctl;
   m->fp32_filter = fp32_filter;
@@ -592,12 +593,12 @@ __global__ void k_fill_min_vert(u32 low, u32 nl, u32 const* __restrict__ vol,
 // their smallest vertex, so each row is scanned once for every wanted entity
 // it holds (a tet's four triangles live in two rows, its six edges in three).
 template <u32 HIGH, u32 LOW>
-__global__ void k_reflect_grouped(u32 nh, u32 const* __restrict__ voh,
+__global__ void k_reflect_grouped(u32 first, u32 nh, u32 const* __restrict__ voh,
     u32 const* __restrict__ offs, u32 const* __restrict__ rows, u32* __restrict__ out)
 {
   constexpr u32 LPH = HIGH == 3 ? (LOW == 1 ? 6 : 4) : 3;
   constexpr u32 VPH = HIGH + 1, VPL = LOW + 1;
-  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+  u32 i = first + blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nh) return;
   u32 v[VPH];
 #pragma unroll
@@ -838,6 +839,84 @@ __global__ void k_derive_sides(u32 dim, u32 ne, u32 const* __restrict__ dual,
 // ---------------------------------------------------------------------------
 // Mesh::ask_* (mesh.cpp:136-261)
 
+void Mesh::build_low_rows(u32 low)
+{
+  if (low_rows[low]) return;
+  u32 const* vol = ask_down(low, 0);
+  u32 nl = counts[low], nv = counts[0];
+  u32* cnt = dalloc<u32>((size_t)nv + 1, s);
+  CK(cudaMemsetAsync(cnt, 0, sizeof(u32) * ((size_t)nv + 1), s));
+  if (nl) {
+    k_count_min_vert<<<grid_for(nl), BLOCK, 0, s>>>(low, nl, vol, cnt);
+    CK_LAUNCH();
+  }
+  low_row_offs[low] = exscan_new(cnt, nv, s);
+  CK(cudaMemsetAsync(cnt, 0, sizeof(u32) * ((size_t)nv + 1), s));
+  low_rows[low] = dalloc<u32>((size_t)nl * (low == 1 ? 2 : 4), s);
+  if (nl) {
+    k_fill_min_vert<<<grid_for(nl), BLOCK, 0, s>>>(low, nl, vol, low_row_offs[low], cnt,
+        low_rows[low]);
+    CK_LAUNCH();
+  }
+  dev_free(cnt, s);
+}
+
+void Mesh::reflect_range(u32 high, u32 low, u32 first, u32* out)
+{
+  u32 nh = count(high);
+  if (first >= nh) return;
+  u32 const* voh = ask_down(high, 0);
+  build_low_rows(low);
+  u32 nl = counts[low], n = (nh - first) * deg(high, low);
+  // voh once, the row offsets and every row record once, out once
+  double nld = nl, rec = low == 1 ? 8.0 : 16.0;
+  PROBE(P_REFLECT_DOWN, s, 4.0 * deg(high, 0) * (nh - first) + 4.0 * (counts[0] + 1.0) +
+      rec * nld + 4.0 * n);
+  u32 g = grid_for(nh - first);
+  if (high == 3 && low == 2)
+    k_reflect_grouped<3, 2><<<g, BLOCK, 0, s>>>(first, nh, voh, low_row_offs[low],
+        low_rows[low], out);
+  else if (high == 3)
+    k_reflect_grouped<3, 1><<<g, BLOCK, 0, s>>>(first, nh, voh, low_row_offs[low],
+        low_rows[low], out);
+  else
+    k_reflect_grouped<2, 1><<<g, BLOCK, 0, s>>>(first, nh, voh, low_row_offs[low],
+        low_rows[low], out);
+  CK_LAUNCH();
+}
+
+// new ids of a surviving high entity's lows: its old lows through the lows'
+// survivor offsets (a surviving entity's lows all survive)
+__global__ void k_carry_down(u32 nh_old, u32 lph, u32 const* __restrict__ same_h,
+    u32 const* __restrict__ same_l, u32 const* __restrict__ old_down, u32* __restrict__ out)
+{
+  u32 t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nh_old * lph) return;
+  u32 i = t / lph, k = t - i * lph;
+  u32 ni = same_h[i];
+  if (same_h[i + 1] == ni) return;
+  out[(size_t)ni * lph + k] = same_l[old_down[t]];
+}
+
+void carry_down(Mesh& m, Mesh& out, u32 high, u32 low, u32 const* same_h, u32 nsame,
+    u32 const* same_l)
+{
+  if (!m.down[high][low] || out.down[high][low] || !out.has_dim(high) || !out.has_dim(low))
+    return;
+  cudaStream_t s = out.s;
+  u32 nh_old = m.counts[high], nh = out.count(high), lph = deg(high, low);
+  out.count(low);
+  u32* dn = dalloc<u32>((size_t)nh * lph, s);
+  if (nh_old) {
+    k_carry_down<<<grid_for((u64)nh_old * lph), BLOCK, 0, s>>>(nh_old, lph, same_h, same_l,
+        m.down[high][low], dn);
+    CK_LAUNCH();
+  }
+  // the survivors come first; the entities the pass made are searched
+  out.reflect_range(high, low, nsame, dn);
+  out.down[high][low] = dn;
+}
+
 u32 const* Mesh::ask_down(u32 high, u32 low)
 {
   if (down[high][low]) return down[high][low];
@@ -848,45 +927,8 @@ u32 const* Mesh::ask_down(u32 high, u32 low)
     down[high][low] = a;
   } else if (low > 0) {
     u32 nh = count(high);
-    u32 const* voh = ask_down(high, 0);
-    u32 const* vol = ask_down(low, 0);
-    u32 nl = counts[low];
-    u32 n = nh * deg(high, low);
-    u32* out = dalloc<u32>(n, s);
-    if (!low_rows[low]) {
-      u32 nv = counts[0];
-      u32* cnt = dalloc<u32>((size_t)nv + 1, s);
-      CK(cudaMemsetAsync(cnt, 0, sizeof(u32) * ((size_t)nv + 1), s));
-      if (nl) {
-        k_count_min_vert<<<grid_for(nl), BLOCK, 0, s>>>(low, nl, vol, cnt);
-        CK_LAUNCH();
-      }
-      low_row_offs[low] = exscan_new(cnt, nv, s);
-      CK(cudaMemsetAsync(cnt, 0, sizeof(u32) * ((size_t)nv + 1), s));
-      low_rows[low] = dalloc<u32>((size_t)nl * (low == 1 ? 2 : 4), s);
-      if (nl) {
-        k_fill_min_vert<<<grid_for(nl), BLOCK, 0, s>>>(low, nl, vol, low_row_offs[low], cnt,
-            low_rows[low]);
-        CK_LAUNCH();
-      }
-      dev_free(cnt, s);
-    }
-    if (n) {
-      // voh once, the row offsets and every row record once, out once
-      double nld = nl, rec = low == 1 ? 8.0 : 16.0;
-      PROBE(P_REFLECT_DOWN, s, 4.0 * deg(high, 0) * nh + 4.0 * (counts[0] + 1.0) +
-          rec * nld + 4.0 * n);
-      if (high == 3 && low == 2)
-        k_reflect_grouped<3, 2><<<grid_for(nh), BLOCK, 0, s>>>(nh, voh, low_row_offs[low],
-            low_rows[low], out);
-      else if (high == 3)
-        k_reflect_grouped<3, 1><<<grid_for(nh), BLOCK, 0, s>>>(nh, voh, low_row_offs[low],
-            low_rows[low], out);
-      else
-        k_reflect_grouped<2, 1><<<grid_for(nh), BLOCK, 0, s>>>(nh, voh, low_row_offs[low],
-            low_rows[low], out);
-      CK_LAUNCH();
-    }
+    u32* out = dalloc<u32>((size_t)nh * deg(high, low), s);
+    reflect_range(high, low, 0, out);
     down[high][low] = out;
   } else if (high == 1 && dim == 3) {
     // edges in 3D bridge the vertex star (mesh.cpp:160-168)

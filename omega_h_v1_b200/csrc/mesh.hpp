@@ -98,9 +98,10 @@ struct Mesh {
   bool own_stream = false;
   std::shared_ptr<Mailbox> mb;  // shared by a mesh and the meshes it spawns
 
-  // stream == nullptr creates (and later destroys) a stream of its own
+  // stream == nullptr creates (and later destroys) a stream of its own,
+  // unless exact_stream is set: then nullptr is the legacy default stream
   Mesh(u32 dim, bool full, bool parallel, cudaStream_t stream,
-      std::shared_ptr<Mailbox> mailbox = nullptr);
+      std::shared_ptr<Mailbox> mailbox = nullptr, bool exact_stream = false);
   ~Mesh();
   Mesh(Mesh const&) = delete;
   Mesh& operator=(Mesh const&) = delete;
@@ -124,6 +125,10 @@ struct Mesh {
   u32 count(u32 d);
 
   u32 const* ask_down(u32 high, u32 low);
+  // reflect_down's rows for lows of dimension `low` (built once per state)
+  void build_low_rows(u32 low);
+  // down(high, low) of the high entities [first, n_high) by search, into out
+  void reflect_range(u32 high, u32 low, u32 first, u32* out);
   // Upward adjacency. Rows are always the same sets; `sorted` asks for the
   // reference's row order (ascending use index), which only some consumers
   // depend on (edge rings, transfers, vertex_dest, the C API). Rows built
@@ -159,6 +164,13 @@ struct Mesh {
   void derive_model(double crease_angle);  // host classification
   void make_parallel();
 };
+
+// down(high, low) of `out`, the mesh a pass built from `m`, when m has it:
+// surviving high entities (same_h: survivor offsets of m's highs; the nsame
+// survivors are numbered first in out) take their old lows through same_l
+// (the lows' survivor offsets); the entities the pass made are searched
+void carry_down(Mesh& m, Mesh& out, u32 high, u32 low, u32 const* same_h, u32 nsame,
+    u32 const* same_l);
 
 // derivation helpers (mesh.cu)
 void up_from_down(u32 high, u32 low, u32 nhighs, u32 nlows, u32 const* lows_of_highs,

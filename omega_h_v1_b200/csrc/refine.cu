@@ -306,6 +306,8 @@ static void refine_build(Mesh& m, u32 const* gen_offs, u32 nsplit)
   for (u32 dd = 1; dd <= dim; ++dd)
     if (m.has_dim(dd)) sp[dd].nsplit = m.mb->host[8 + dd];
   // products of every dimension (refine_common.cpp:90-123, inherit.cpp:104-138)
+  u32* same_of[4] = {nullptr, nullptr, nullptr, nullptr};
+  u32 nsame_of[4] = {0, 0, 0, 0};
   for (u32 prod = 0; prod <= dim; ++prod) {
     if (!m.full && 0 < prod && prod < dim) continue;
     u32 np = m.count(prod);
@@ -364,9 +366,16 @@ static void refine_build(Mesh& m, u32 const* gen_offs, u32 nsplit)
         }
       }
     }
-    dev_free(same, s);
+    same_of[prod] = same;
+    nsame_of[prod] = np - sp[prod].nsplit;
   }
+  // downward adjacency of the survivors carries over; the products are searched
+  for (u32 h = 2; h <= dim; ++h)
+    for (u32 l = 1; l < h; ++l)
+      if (same_of[h] && same_of[l])
+        carry_down(m, *out, h, l, same_of[h], nsame_of[h], same_of[l]);
   for (u32 dd = 0; dd <= dim; ++dd) {
+    dev_free(same_of[dd], s);
     dev_free(sp[dd].offs, s);
     dev_free(sp[dd].dir, s);
     dev_free(sp[dd].vert, s);

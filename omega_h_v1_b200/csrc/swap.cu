@@ -506,6 +506,8 @@ static void swap_build(Mesh& m, SwapSel const& sel)
   u32 const* voe1 = m.ask_down(1, 0);
   u32 const* vot = m.ask_down(3, 0);
   u32* cnt = dalloc<u32>(ne, s);
+  u32* same_of[4] = {nullptr, nullptr, nullptr, nullptr};
+  u32 nsame_of[4] = {0, 0, 0, 0};
   for (u32 ed = m.full ? 1u : dim; ed <= dim; ++ed) {
     u32 n = m.count(ed), vpe = deg(ed, 0);
     k_swap_counts<<<grid_for(ne), BLOCK, 0, s>>>(ne, ed, sel.ind, sel.rs, cnt);
@@ -573,9 +575,16 @@ static void swap_build(Mesh& m, SwapSel const& sel)
       }
     }
     dev_free(gen_offs, s);
-    dev_free(same_offs, s);
+    same_of[ed] = same_offs;
+    nsame_of[ed] = nsame;
   }
   dev_free(cnt, s);
+  // downward adjacency of the survivors carries over; the products are searched
+  for (u32 h = 2; h <= dim; ++h)
+    for (u32 l = 1; l < h; ++l)
+      if (same_of[h] && same_of[l])
+        carry_down(m, *out, h, l, same_of[h], nsame_of[h], same_of[l]);
+  for (u32 d = 0; d < 4; ++d) dev_free(same_of[d], s);
   m.overwrite(out);
 }
 
