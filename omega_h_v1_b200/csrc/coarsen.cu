@@ -656,17 +656,32 @@ static void coarsen_build(Mesh& m, CoarsenSel const& sel)
   last_pass_stats().nselected = nv - nv_out;
   Mesh* out = m.spawn();
   out->set_ents(0, nv_out, nullptr);
-  // tags_subset (subset.cpp:15-43): every vertex tag survives
+  // tags_subset (subset.cpp:15-43): every vertex tag survives (one launch)
+  std::vector<ExpandJob> vjobs;
   for (auto const& t : m.tags[0]) {
     u32 esz = tag_esz(t.type);
     void* d = dev_alloc((size_t)nv_out * t.ncomps * esz, s);
-    expand_scaled(t.data, same_v, 1, nv, t.ncomps, esz, d, s);
+    ExpandJob jb;
+    jb.in = t.data;
+    jb.offs = same_v;
+    jb.out = d;
+    jb.n = nv;
+    jb.width = t.ncomps;
+    jb.esz = esz;
+    vjobs.push_back(jb);
     out->add_tag(0, t.type, t.name.c_str(), t.ncomps, t.transfer, d);
   }
   if (m.seg) {
     out->seg = dalloc<u32>(nv_out, s);
-    expand_scaled(m.seg, same_v, 1, nv, 1, 4, out->seg, s);
+    ExpandJob jb;
+    jb.in = m.seg;
+    jb.offs = same_v;
+    jb.out = out->seg;
+    jb.n = nv;
+    jb.width = 1;
+    vjobs.push_back(jb);
   }
+  expand_many(vjobs, s);
   if (m.parallel) inherit_globals(*out, 0, nv_out);
   u32* fused[4] = {nullptr, nullptr, nullptr, nullptr};
   u32* same_of[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -726,17 +741,22 @@ static void coarsen_build(Mesh& m, CoarsenSel const& sel)
     same_of[ed] = same_e;
     nsame_of[ed] = nsame;
   }
+  same_of[0] = same_v;
+  nsame_of[0] = nv_out;
   // downward adjacency of the survivors carries over; the products are searched
   for (u32 h = 2; h <= dim; ++h)
     for (u32 l = 1; l < h; ++l)
       if (same_of[h] && same_of[l])
         carry_down(m, *out, h, l, same_of[h], nsame_of[h], same_of[l]);
+  for (u32 h = 1; h <= dim; ++h)
+    for (u32 l = 0; l < h; ++l)
+      if (same_of[h] && same_of[l])
+        carry_up(m, *out, l, h, same_of[l], same_of[h], nsame_of[h]);
   for (u32 d = 0; d < 4; ++d) {
     dev_free(fused[d], s);
     dev_free(same_of[d], s);
   }
   dev_free(gen_offs_v, s);
-  dev_free(same_v, s);
   m.overwrite(out);
 }
 

@@ -7,6 +7,9 @@
 // down(3,1)), a vertex's neighbours the far ends of its edges (up(0,1)).
 // That is exactly the neighbour set of the reference's star(1,3) /
 // star(0,1) (star.cpp:135-293); the selection rule depends only on that set.
+#include <algorithm>
+#include <vector>
+
 #include "passes.hpp"
 
 namespace osh {
@@ -190,27 +193,90 @@ void expand_scaled(void const* in, u32 const* offs, u32 k, u32 n, u32 width,
   CK_LAUNCH();
 }
 
-static void inherit_u32_tag(Mesh& m, Mesh& out, u32 prod, Doms const& d, char const* name)
+// Several row expansions in one launch: blockIdx.y picks the job, the x
+// blocks stride over its rows (the same copy as k_expand_scaled)
+struct ExpandJobs {
+  ExpandJob j[8];
+};
+
+__global__ void k_expand_many(ExpandJobs jobs)
 {
-  Tag* t = m.find_tag(prod, name);
-  if (!t) throw Failure(E_ARG, std::string("missing tag ") + name);
-  u32 nc = t->ncomps;
-  u32* data = dalloc<u32>((size_t)d.ngo[4] * nc, m.s);
-  for (u32 k = 0; k < 4; ++k) {
-    if (!d.ndoms[k] || !d.offs[k] || !d.ngen[k]) continue;
-    Tag* tk = (k == 0) ? t : m.find_tag(k, name);
-    if (!tk) continue;
-    expand_scaled(tk->data, d.offs[k], d.scale[k], d.ndoms[k], nc, 4,
-        data + (size_t)d.ngo[k] * nc, m.s);
+  ExpandJob const jb = jobs.j[blockIdx.y];
+  for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < jb.n; i += gridDim.x * blockDim.x) {
+    u32 f = jb.offs[i] * jb.k, e = jb.offs[i + 1] * jb.k;
+    for (u32 j = f; j < e; ++j) {
+      if (jb.esz == 4) {
+        u32 const* in = static_cast<u32 const*>(jb.in) + (size_t)i * jb.width;
+        u32* out = static_cast<u32*>(jb.out) + (size_t)j * jb.width;
+        for (u32 c = 0; c < jb.width; ++c) out[c] = in[c];
+      } else if (jb.esz == 8) {
+        unsigned long long const* in =
+            static_cast<unsigned long long const*>(jb.in) + (size_t)i * jb.width;
+        unsigned long long* out = static_cast<unsigned long long*>(jb.out) + (size_t)j * jb.width;
+        for (u32 c = 0; c < jb.width; ++c) out[c] = in[c];
+      } else {
+        unsigned char const* in = static_cast<unsigned char const*>(jb.in) + (size_t)i * jb.width;
+        unsigned char* out = static_cast<unsigned char*>(jb.out) + (size_t)j * jb.width;
+        for (u32 c = 0; c < jb.width; ++c) out[c] = in[c];
+      }
+    }
   }
-  out.add_tag(prod, T_U32, name, nc, X_NOT, data);
 }
 
+void expand_many(std::vector<ExpandJob> const& jobs, cudaStream_t s)
+{
+  std::vector<ExpandJob> live;
+  for (ExpandJob const& jb : jobs)
+    if (jb.n && jb.width && jb.k) live.push_back(jb);
+  for (size_t at = 0; at < live.size(); at += 8) {
+    ExpandJobs pack;
+    u32 cnt = (u32)std::min<size_t>(8, live.size() - at), nmax = 0;
+    double bytes = 0;
+    for (u32 q = 0; q < cnt; ++q) {
+      pack.j[q] = live[at + q];
+      nmax = std::max(nmax, pack.j[q].n);
+      bytes += 4.0 * (pack.j[q].n + 1) +
+          2.0 * (double)pack.j[q].n * pack.j[q].width * pack.j[q].esz * pack.j[q].k;
+    }
+    PROBE(P_EXPAND, s, bytes);
+    dim3 grid(std::min<u32>(grid_for(nmax), 148u * 16u), cnt);
+    k_expand_many<<<grid, BLOCK, 0, s>>>(pack);
+    CK_LAUNCH();
+  }
+}
+
+// class_dim / class_id of the products: every domain of both labels in one
+// launch
 void inherit_class(Mesh& m, Mesh& out, u32 prod, Doms const& d)
 {
   if (!m.find_tag(0, "class_dim")) return;
-  inherit_u32_tag(m, out, prod, d, "class_dim");
-  if (m.find_tag(0, "class_id")) inherit_u32_tag(m, out, prod, d, "class_id");
+  char const* names[2] = {"class_dim", "class_id"};
+  u32 nnames = m.find_tag(0, "class_id") ? 2 : 1;
+  std::vector<ExpandJob> jobs;
+  u32* data[2] = {nullptr, nullptr};
+  u32 nc[2] = {1, 1};
+  for (u32 q = 0; q < nnames; ++q) {
+    Tag* t = m.find_tag(prod, names[q]);
+    if (!t) throw Failure(E_ARG, std::string("missing tag ") + names[q]);
+    nc[q] = t->ncomps;
+    data[q] = dalloc<u32>((size_t)d.ngo[4] * nc[q], m.s);
+    for (u32 k = 0; k < 4; ++k) {
+      if (!d.ndoms[k] || !d.offs[k] || !d.ngen[k]) continue;
+      Tag* tk = (k == 0) ? t : m.find_tag(k, names[q]);
+      if (!tk) continue;
+      ExpandJob jb;
+      jb.in = tk->data;
+      jb.offs = d.offs[k];
+      jb.out = data[q] + (size_t)d.ngo[k] * nc[q];
+      jb.k = d.scale[k];
+      jb.n = d.ndoms[k];
+      jb.width = nc[q];
+      jb.esz = 4;
+      jobs.push_back(jb);
+    }
+  }
+  expand_many(jobs, m.s);
+  for (u32 q = 0; q < nnames; ++q) out.add_tag(prod, T_U32, names[q], nc[q], X_NOT, data[q]);
 }
 
 void inherit_globals(Mesh& out, u32 d, u32 n)

@@ -135,6 +135,7 @@ void Mesh::clear_contents()
         dev_free(up[l][h].offs, s);
         dev_free(up[l][h].adj, s);
         dev_free(up[l][h].dirs, s);
+        dev_free(up[l][h].pre, s);
         up[l][h] = UpAdj();
         have_up[l][h] = false;
         up_sorted[l][h] = false;
@@ -340,15 +341,16 @@ __global__ void k_rank_rows(u32 const* __restrict__ offs, u32 const* __restrict_
 // global memory after the network, outside any shuffle.
 template <int G, int K>
 __global__ void __launch_bounds__(256)
-k_sort_rows(u32 const* __restrict__ offs, u32 const* __restrict__ tmp, u32 nrows, u32 lph,
-    u32* __restrict__ adj, u32* __restrict__ dirs)
+k_sort_rows(u32 const* __restrict__ offs, u32 const* __restrict__ pre,
+    u32 const* __restrict__ tmp, u32 nrows, u32 lph, u32* __restrict__ adj,
+    u32* __restrict__ dirs)
 {
   constexpr int N = G * K;
   u32 row = (blockIdx.x * blockDim.x + threadIdx.x) / G;
   u32 l = threadIdx.x % G;
   u32 f = 0, len = 0;
   if (row < nrows) {
-    f = offs[row];
+    f = offs[row] + (pre ? pre[row] : 0u);
     len = offs[row + 1] - f;
   }
   u32 v[K];
@@ -396,26 +398,28 @@ k_sort_rows(u32 const* __restrict__ offs, u32 const* __restrict__ tmp, u32 nrows
 }
 
 template <int G, int K>
-static void launch_sort_rows(u32 const* offs, u32 const* tmp, u32 nrows, u32 lph, u32* adj,
-    u32* dirs, cudaStream_t s)
+static void launch_sort_rows(u32 const* offs, u32 const* pre, u32 const* tmp, u32 nrows,
+    u32 lph, u32* adj, u32* dirs, cudaStream_t s)
 {
   u64 threads = (u64)nrows * G;
-  k_sort_rows<G, K><<<grid_for(threads), 256, 0, s>>>(offs, tmp, nrows, lph, adj, dirs);
+  k_sort_rows<G, K><<<grid_for(threads), 256, 0, s>>>(offs, pre, tmp, nrows, lph, adj, dirs);
   CK_LAUNCH();
 }
 
-static void rank_rows(u32 const* offs, u32 const* tmp, u32 nrows, u32 nuses, u32 lph,
-    u32* adj, u32* dirs, cudaStream_t s)
+// sort every row (or, given pre, every row's part after its first pre[l]
+// uses); nsort = the uses to be sorted in all
+static void rank_rows(u32 const* offs, u32 const* pre, u32 const* tmp, u32 nrows, u32 nsort,
+    u32 lph, u32* adj, u32* dirs, cudaStream_t s)
 {
-  double avg = nrows ? (double)nuses / nrows : 1.0;
+  double avg = nrows ? (double)nsort / nrows : 1.0;
   double want = 2.5 * avg;
-  if (want <= 2) launch_sort_rows<2, 1>(offs, tmp, nrows, lph, adj, dirs, s);
-  else if (want <= 4) launch_sort_rows<4, 1>(offs, tmp, nrows, lph, adj, dirs, s);
-  else if (want <= 8) launch_sort_rows<8, 1>(offs, tmp, nrows, lph, adj, dirs, s);
-  else if (want <= 16) launch_sort_rows<16, 1>(offs, tmp, nrows, lph, adj, dirs, s);
-  else if (want <= 32) launch_sort_rows<32, 1>(offs, tmp, nrows, lph, adj, dirs, s);
-  else if (want <= 64) launch_sort_rows<32, 2>(offs, tmp, nrows, lph, adj, dirs, s);
-  else launch_sort_rows<32, 4>(offs, tmp, nrows, lph, adj, dirs, s);
+  if (want <= 2) launch_sort_rows<2, 1>(offs, pre, tmp, nrows, lph, adj, dirs, s);
+  else if (want <= 4) launch_sort_rows<4, 1>(offs, pre, tmp, nrows, lph, adj, dirs, s);
+  else if (want <= 8) launch_sort_rows<8, 1>(offs, pre, tmp, nrows, lph, adj, dirs, s);
+  else if (want <= 16) launch_sort_rows<16, 1>(offs, pre, tmp, nrows, lph, adj, dirs, s);
+  else if (want <= 32) launch_sort_rows<32, 1>(offs, pre, tmp, nrows, lph, adj, dirs, s);
+  else if (want <= 64) launch_sort_rows<32, 2>(offs, pre, tmp, nrows, lph, adj, dirs, s);
+  else launch_sort_rows<32, 4>(offs, pre, tmp, nrows, lph, adj, dirs, s);
 }
 
 __global__ void k_fill_uses_split(u32 const* __restrict__ loh, u32 nuses, u32 lph,
@@ -471,8 +475,9 @@ void sort_up_rows(u32 high, u32 low, u32 nhighs, u32 nlows, UpAdj const& u,
   k_join_uses<<<grid_for(nuses), BLOCK, 0, s>>>(nuses, lph, u.adj, u.dirs, uses);
   CK_LAUNCH();
   {
-    PROBE(P_UP_RANK, s, 12.0 * nuses + 4.0 * (nlows + 1.0));
-    rank_rows(u.offs, uses, nlows, nuses, lph, u.adj, u.dirs, s);
+    u32 nsort = u.pre ? nuses - u.npre : nuses;
+    PROBE(P_UP_RANK, s, 12.0 * nsort + 4.0 * (nlows + 1.0));
+    rank_rows(u.offs, u.pre, uses, nlows, nsort, lph, u.adj, u.dirs, s);
   }
   dev_free(uses, s);
 }
@@ -502,7 +507,7 @@ void up_from_down(u32 high, u32 low, u32 nhighs, u32 nlows, u32 const* loh,
     }
     if (nlows) {
       PROBE(P_UP_RANK, s, 12.0 * nuses + 4.0 * (nlows + 1.0));
-      rank_rows(out.offs, tmp, nlows, nuses, lph, out.adj, out.dirs, s);
+      rank_rows(out.offs, nullptr, tmp, nlows, nuses, lph, out.adj, out.dirs, s);
     }
   }
   dev_free(tmp, s);
@@ -917,6 +922,120 @@ void carry_down(Mesh& m, Mesh& out, u32 high, u32 low, u32 const* same_h, u32 ns
   out.down[high][low] = dn;
 }
 
+// up(low, high) carried through a pass. A surviving low keeps the uses of
+// its old row whose high entity survived, in the old order, mapped to new
+// ids, followed by the uses of the entities the pass made; a low the pass
+// made has only such uses (a surviving high entity's lows all survive).
+__global__ void k_up_surv_count(u32 nl_old, u32 const* __restrict__ same_l,
+    u32 const* __restrict__ same_h, u32 const* __restrict__ offs, u32 const* __restrict__ adj,
+    u32* __restrict__ cnt, u32* __restrict__ surv)
+{
+  u32 j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= nl_old) return;
+  u32 nj = same_l[j];
+  if (same_l[j + 1] == nj) return;
+  u32 c = 0;
+  for (u32 r = offs[j]; r < offs[j + 1]; ++r) {
+    u32 a = adj[r];
+    c += same_h[a + 1] != same_h[a] ? 1u : 0u;
+  }
+  cnt[nj] = c;
+  surv[nj] = c;
+}
+
+__global__ void k_up_gen_count(u32 first, u32 nuses, u32 const* __restrict__ loh,
+    u32* __restrict__ cnt)
+{
+  u32 u = first + blockIdx.x * blockDim.x + threadIdx.x;
+  if (u < nuses) atomicAdd(&cnt[loh[u]], 1u);
+}
+
+__global__ void k_up_surv_fill(u32 nl_old, u32 const* __restrict__ same_l,
+    u32 const* __restrict__ same_h, u32 const* __restrict__ offs_old,
+    u32 const* __restrict__ adj_old, u32 const* __restrict__ dirs_old,
+    u32 const* __restrict__ offs, u32* __restrict__ adj, u32* __restrict__ dirs)
+{
+  u32 j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= nl_old) return;
+  u32 nj = same_l[j];
+  if (same_l[j + 1] == nj) return;
+  u32 w = offs[nj];
+  for (u32 r = offs_old[j]; r < offs_old[j + 1]; ++r) {
+    u32 a = adj_old[r], na = same_h[a];
+    if (same_h[a + 1] == na) continue;
+    adj[w] = na;
+    dirs[w] = dirs_old[r];
+    ++w;
+  }
+}
+
+__global__ void k_up_gen_fill(u32 first, u32 nuses, u32 lph, u32 const* __restrict__ loh,
+    u32 const* __restrict__ offs, u32* cur, u32* __restrict__ adj, u32* __restrict__ dirs)
+{
+  u32 u = first + blockIdx.x * blockDim.x + threadIdx.x;
+  if (u >= nuses) return;
+  u32 l = loh[u];
+  u32 slot = offs[l] + atomicAdd(&cur[l], 1u);
+  adj[slot] = u / lph;
+  dirs[slot] = u % lph;
+}
+
+void carry_up(Mesh& m, Mesh& out, u32 low, u32 high, u32 const* same_l, u32 const* same_h,
+    u32 nsame_h)
+{
+  if (!m.have_up[low][high] || out.have_up[low][high]) return;
+  if (!out.has_dim(high) || !out.has_dim(low)) return;
+  if (low > 0 && !out.down[high][low]) return;  // its search is not worth it here
+  cudaStream_t s = out.s;
+  u32 nl_old = m.counts[low], nl = out.count(low), nh = out.count(high);
+  u32 lph = deg(high, low), nuses = nh * lph, first = nsame_h * lph;
+  u32 const* loh = out.ask_down(high, low);
+  UpAdj const& old = m.up[low][high];
+  u32* cnt = dalloc<u32>((size_t)nl + 1, s);
+  u32* surv = dalloc<u32>((size_t)nl + 1, s);
+  CK(cudaMemsetAsync(cnt, 0, sizeof(u32) * ((size_t)nl + 1), s));
+  CK(cudaMemsetAsync(surv, 0, sizeof(u32) * ((size_t)nl + 1), s));
+  if (nl_old) {
+    k_up_surv_count<<<grid_for(nl_old), BLOCK, 0, s>>>(nl_old, same_l, same_h, old.offs,
+        old.adj, cnt, surv);
+    CK_LAUNCH();
+  }
+  if (nuses > first) {
+    PROBE(P_UP_COUNT, s, 4.0 * (nuses - first) + 4.0 * nl);
+    k_up_gen_count<<<grid_for(nuses - first), BLOCK, 0, s>>>(first, nuses, loh, cnt);
+    CK_LAUNCH();
+  }
+  UpAdj u;
+  u.offs = exscan_new(cnt, nl, s);
+  // cnt becomes the fill cursor (starting after each row's survivors); surv
+  // stays as the count of each row's leading uses, in order when the old
+  // rows were
+  CK(cudaMemcpyAsync(cnt, surv, sizeof(u32) * ((size_t)nl + 1), cudaMemcpyDeviceToDevice, s));
+  u.adj = dalloc<u32>(nuses, s);
+  u.dirs = dalloc<u32>(nuses, s);
+  if (nl_old) {
+    k_up_surv_fill<<<grid_for(nl_old), BLOCK, 0, s>>>(nl_old, same_l, same_h, old.offs, old.adj,
+        old.dirs, u.offs, u.adj, u.dirs);
+    CK_LAUNCH();
+  }
+  if (nuses > first) {
+    PROBE(P_UP_FILL, s, 4.0 * (nuses - first) + 8.0 * nl + 8.0 * (nuses - first));
+    k_up_gen_fill<<<grid_for(nuses - first), BLOCK, 0, s>>>(first, nuses, lph, loh, u.offs,
+        cnt, u.adj, u.dirs);
+    CK_LAUNCH();
+  }
+  dev_free(cnt, s);
+  if (m.up_sorted[low][high]) {
+    u.pre = surv;
+    u.npre = first;
+  } else {
+    dev_free(surv, s);
+  }
+  out.up[low][high] = u;
+  out.have_up[low][high] = true;
+  out.up_sorted[low][high] = false;
+}
+
 u32 const* Mesh::ask_down(u32 high, u32 low)
 {
   if (down[high][low]) return down[high][low];
@@ -980,6 +1099,9 @@ UpAdj const& Mesh::ask_up(u32 low, u32 high, bool sorted)
     if (sorted && !up_sorted[low][high]) {
       sort_up_rows(high, low, counts[high], counts[low], up[low][high], s);
       up_sorted[low][high] = true;
+      dev_free(up[low][high].pre, s);
+      up[low][high].pre = nullptr;
+      up[low][high].npre = 0;
     }
     return up[low][high];
   }

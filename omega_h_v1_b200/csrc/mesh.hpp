@@ -38,6 +38,10 @@ struct UpAdj {
   u32* offs = nullptr;
   u32* adj = nullptr;
   u32* dirs = nullptr;
+  // rows carried through a pass: the first pre[l] uses of row l are already
+  // in order and precede the rest (null when nothing is known)
+  u32* pre = nullptr;
+  u32 npre = 0;  // sum of pre
 };
 
 struct Graph {
@@ -171,6 +175,12 @@ struct Mesh {
 // (the lows' survivor offsets); the entities the pass made are searched
 void carry_down(Mesh& m, Mesh& out, u32 high, u32 low, u32 const* same_h, u32 nsame,
     u32 const* same_l);
+
+// up(low, high) of `out` when m has it: surviving lows keep their old rows'
+// uses by surviving highs (mapped, in order), then the uses of the entities
+// the pass made are added; rows come out unsorted
+void carry_up(Mesh& m, Mesh& out, u32 low, u32 high, u32 const* same_l, u32 const* same_h,
+    u32 nsame_h);
 
 // derivation helpers (mesh.cu)
 void up_from_down(u32 high, u32 low, u32 nhighs, u32 nlows, u32 const* lows_of_highs,

@@ -2,6 +2,8 @@
 // pieces they share: independent sets, class inheritance, expansion.
 #pragma once
 
+#include <vector>
+
 #include "mesh.hpp"
 
 namespace osh {
@@ -30,6 +32,16 @@ u32* find_indset(Mesh& m, u32 ent_dim, u32 const* filter, double const* goodness
 // [offs[i]*k, offs[i+1]*k), for T of 1, 4 or 8 bytes
 void expand_scaled(void const* in, u32 const* offs, u32 k, u32 n, u32 width,
     u32 esz, void* out, cudaStream_t s);
+
+// one row expansion (as expand_scaled); expand_many runs up to eight per
+// launch
+struct ExpandJob {
+  void const* in = nullptr;
+  u32 const* offs = nullptr;
+  void* out = nullptr;
+  u32 k = 1, n = 0, width = 0, esz = 4;
+};
+void expand_many(std::vector<ExpandJob> const& jobs, cudaStream_t s);
 
 // Per-dimension domains that produce entities of one dimension during a
 // pass: ndoms[d] entities of dimension d, each producing

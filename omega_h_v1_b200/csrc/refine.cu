@@ -374,6 +374,10 @@ static void refine_build(Mesh& m, u32 const* gen_offs, u32 nsplit)
     for (u32 l = 1; l < h; ++l)
       if (same_of[h] && same_of[l])
         carry_down(m, *out, h, l, same_of[h], nsame_of[h], same_of[l]);
+  for (u32 h = 1; h <= dim; ++h)
+    for (u32 l = 0; l < h; ++l)
+      if (same_of[h] && same_of[l])
+        carry_up(m, *out, l, h, same_of[l], same_of[h], nsame_of[h]);
   for (u32 dd = 0; dd <= dim; ++dd) {
     dev_free(same_of[dd], s);
     dev_free(sp[dd].offs, s);

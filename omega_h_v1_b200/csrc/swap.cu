@@ -579,11 +579,18 @@ static void swap_build(Mesh& m, SwapSel const& sel)
     nsame_of[ed] = nsame;
   }
   dev_free(cnt, s);
+  same_of[0] = dalloc<u32>((size_t)nv + 1, s);  // vertices all survive, in order
+  iota_u32(same_of[0], nv + 1, 1, s);
+  nsame_of[0] = nv;
   // downward adjacency of the survivors carries over; the products are searched
   for (u32 h = 2; h <= dim; ++h)
     for (u32 l = 1; l < h; ++l)
       if (same_of[h] && same_of[l])
         carry_down(m, *out, h, l, same_of[h], nsame_of[h], same_of[l]);
+  for (u32 h = 1; h <= dim; ++h)
+    for (u32 l = 0; l < h; ++l)
+      if (same_of[h] && same_of[l])
+        carry_up(m, *out, l, h, same_of[l], same_of[h], nsame_of[h]);
   for (u32 d = 0; d < 4; ++d) dev_free(same_of[d], s);
   m.overwrite(out);
 }
