@@ -142,8 +142,8 @@ unsigned long long osh_b200_digest(osh_t m) OSH_PUBLIC;
    size field) admits them; admitted jobs are classified (crease pi/4), join
    the running batch at the next step and leave it when their pass loop ends,
    so jobs that arrive while others run share every launch with them. Each
-   result equals what osh_adapt gives the same job alone. Not thread-safe:
-   call one server from one thread. */
+   result equals what osh_adapt gives the same job alone. Without an engine
+   thread (below), call one server from one thread. */
 typedef struct osh_b200_server* osh_b200_server_t;
 osh_b200_server_t osh_b200_server_new(double size_ratio_floor, double good_qual,
     unsigned nsliver_layers, unsigned max_passes,
@@ -160,6 +160,18 @@ void osh_b200_server_set_union_elems(osh_b200_server_t sv,
 /* admit, run one step over every resident job, retire finished jobs;
    returns the number of jobs queued or running, or -1 on error */
 int osh_b200_server_step(osh_b200_server_t sv) OSH_PUBLIC;
+/* run the steps on an engine thread of the server's own, so that jobs
+   submitted from the caller's thread join while others run; after start,
+   osh_b200_server_step must not be called. osh_b200_server_wait blocks until
+   every submitted job has finished or timeout_s seconds pass (negative: no
+   limit) and returns the number of jobs not finished, or -1 on an error (the
+   engine stops at its first error; its code and message are then reported
+   here). osh_b200_server_stop ends the engine after its current step (also
+   done by osh_b200_server_free). Submit, poll, take and the info calls may be
+   used from one other thread while the engine runs. */
+void osh_b200_server_start(osh_b200_server_t sv) OSH_PUBLIC;
+int osh_b200_server_wait(osh_b200_server_t sv, double timeout_s) OSH_PUBLIC;
+void osh_b200_server_stop(osh_b200_server_t sv) OSH_PUBLIC;
 /* ids of finished jobs not yet reported (at most max_ids); returns the count */
 unsigned osh_b200_server_poll(osh_b200_server_t sv, unsigned* ids,
     unsigned max_ids) OSH_PUBLIC;

@@ -151,6 +151,9 @@ def lib():
     f("osh_b200_server_free", None, vp)
     f("osh_b200_server_submit", C.c_int, vp, C.c_uint, C.c_uint, _f64p, C.c_uint, _u32p, _f64p)
     f("osh_b200_server_step", C.c_int, vp)
+    f("osh_b200_server_start", None, vp)
+    f("osh_b200_server_stop", None, vp)
+    f("osh_b200_server_wait", C.c_int, vp, C.c_double)
     f("osh_b200_server_set_union_elems", None, vp, C.c_ulonglong)
     f("osh_b200_server_poll", C.c_uint, vp, C.POINTER(C.c_uint), C.c_uint)
     f("osh_b200_server_take", vp, vp, C.c_uint)
@@ -553,6 +556,23 @@ class Server:
         if r < 0:
             check()
         return r
+
+    def start(self):
+        """Run steps on the server's own engine thread."""
+        self.L.osh_b200_server_start(self.h)
+        check()
+
+    def wait(self, timeout=-1.0):
+        """Block until every submitted job finished (or timeout seconds);
+        returns the jobs not finished."""
+        r = self.L.osh_b200_server_wait(self.h, timeout)
+        if r < 0:
+            check()
+        return r
+
+    def stop(self):
+        self.L.osh_b200_server_stop(self.h)
+        check()
 
     def set_union_elems(self, n):
         self.L.osh_b200_server_set_union_elems(self.h, int(n))

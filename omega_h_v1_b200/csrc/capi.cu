@@ -572,6 +572,30 @@ int osh_b200_server_step(osh_b200_server_t sv)
   API_CATCH(-1)
 }
 
+void osh_b200_server_start(osh_b200_server_t sv)
+{
+  API_TRY
+  need(sv != nullptr, "server is NULL");
+  osh::server_start(SV(sv));
+  API_CATCH_VOID
+}
+
+void osh_b200_server_stop(osh_b200_server_t sv)
+{
+  API_TRY
+  need(sv != nullptr, "server is NULL");
+  osh::server_stop(SV(sv));
+  API_CATCH_VOID
+}
+
+int osh_b200_server_wait(osh_b200_server_t sv, double timeout_s)
+{
+  API_TRY
+  need(sv != nullptr, "server is NULL");
+  return osh::server_wait(SV(sv), timeout_s);
+  API_CATCH(-1)
+}
+
 unsigned osh_b200_server_poll(osh_b200_server_t sv, unsigned* ids, unsigned max_ids)
 {
   API_TRY

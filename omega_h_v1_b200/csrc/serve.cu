@@ -6,11 +6,15 @@
 // whose loop ends is split out of the union at that step's end and handed
 // back, while the others keep running. Every step is one launch sequence for
 // all resident jobs, so jobs that arrive while others run share their passes.
+#include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <condition_variable>
 #include <deque>
 #include <map>
 #include <memory>
+#include <mutex>
+#include <thread>
 
 #include "batch.hpp"
 #include "serve.hpp"
@@ -92,9 +96,19 @@ struct Server {
   u32 next_id = 0;
   u32 steps = 0, unions = 0;
   double secs_admit = 0, secs_passes = 0, secs_retire = 0;
+  // the engine thread (server_start): it runs steps while there is work;
+  // `mu` guards the queue, the job table and the finished flags
+  std::mutex mu;
+  std::condition_variable cv;
+  std::thread engine;
+  bool running = false, stopping = false;
+  int device = 0;
+  int err_code = 0;
+  std::string err_msg;
 
   ~Server()
   {
+    stop();
     for (size_t k = 0; k < ms.size(); ++k)
       if (owned[k]) delete ms[k];
     jobs.clear();
@@ -104,13 +118,57 @@ struct Server {
     }
   }
 
+  void stop()
+  {
+    {
+      std::lock_guard<std::mutex> g(mu);
+      if (!running) return;
+      stopping = true;
+    }
+    cv.notify_all();
+    engine.join();
+    running = false;
+    stopping = false;
+  }
+
+  void engine_loop()
+  {
+    cudaSetDevice(device);
+    for (;;) {
+      {
+        std::unique_lock<std::mutex> g(mu);
+        cv.wait(g, [&] { return stopping || !queue.empty() || !active.empty(); });
+        if (stopping) return;
+      }
+      try {
+        step();
+      } catch (Failure const& f) {
+        std::lock_guard<std::mutex> g(mu);
+        err_code = f.code;
+        err_msg = f.what();
+        return;
+      } catch (std::exception const& e) {
+        std::lock_guard<std::mutex> g(mu);
+        err_code = E_CUDA;
+        err_msg = e.what();
+        return;
+      }
+      cv.notify_all();  // waiters see finished jobs
+    }
+  }
+
   void admit()
   {
     cudaStream_t s = run.s;
-    while (!queue.empty()) {
-      ServeJob* j = queue.front();
-      if (!active.empty() && reserved + j->est_bytes > budget) break;
-      queue.pop_front();
+    for (;;) {
+      ServeJob* j = nullptr;
+      {
+        std::lock_guard<std::mutex> g(mu);
+        if (queue.empty()) break;
+        j = queue.front();
+        if (!active.empty() && reserved + j->est_bytes > budget) break;
+        queue.pop_front();
+      }
       reserved += j->est_bytes;
       Mesh* m = new Mesh(j->dim, false, false, s);
       try {
@@ -153,7 +211,11 @@ struct Server {
     admit();
     double t_b = now_s();
     secs_admit += t_b - t_a;
-    if (active.empty()) return (u32)queue.size();
+    if (active.empty()) {
+      std::lock_guard<std::mutex> g(mu);
+      publish();
+      return (u32)queue.size();
+    }
     steps += 1;
     u32 u0 = last_batch_stats().unions;
     run.step(ms, st, owned);
@@ -166,7 +228,6 @@ struct Server {
     for (size_t k = 0; k < active.size(); ++k) {
       ServeJob* j = active[k];
       if (st[k].state >= ST_DONE) {
-        j->st = st[k];
         Mesh* m = ms[k];
         if (!owned[k]) throw Failure(E_ARG, "server lost a job's mesh");
         drop_segments(*m);
@@ -174,9 +235,13 @@ struct Server {
         for (u32 op : st[k].res.ops) want = layout_after(op, want, m->dim);
         apply_layout(*m, want);
         m->own_new_stream();
-        j->mesh = m;
-        j->finished = true;
-        j->t_done = t;
+        {
+          std::lock_guard<std::mutex> g(mu);
+          j->st = st[k];
+          j->mesh = m;
+          j->finished = true;
+          j->t_done = t;
+        }
         reserved -= j->est_bytes;
         continue;
       }
@@ -191,7 +256,22 @@ struct Server {
     st.resize(w);
     owned.resize(w);
     secs_retire += now_s() - t_c;
+    std::lock_guard<std::mutex> g(mu);
+    publish();
     return (u32)(active.size() + queue.size());
+  }
+
+  // the counters server_stats reports, copied under `mu`
+  ServeStats snap;
+  void publish()
+  {
+    snap.steps = steps;
+    snap.rebuilds = unions;
+    snap.active = (u32)active.size();
+    snap.reserved = reserved;
+    snap.secs_admit = secs_admit;
+    snap.secs_passes = secs_passes;
+    snap.secs_retire = secs_retire;
   }
 };
 
@@ -217,7 +297,6 @@ u32 server_submit(Server* sv, u32 dim, u32 nverts, double const* coords, u32 nel
   if (dim < 2 || dim > 3) throw Failure(E_ARG, "jobs are 2D or 3D simplex meshes");
   if (!nverts || !nelems || !coords || !conn || !size) throw Failure(E_ARG, "empty job");
   std::unique_ptr<ServeJob> j(new ServeJob());
-  j->id = sv->next_id++;
   j->dim = dim;
   j->nverts = nverts;
   j->nelems = nelems;
@@ -232,19 +311,61 @@ u32 server_submit(Server* sv, u32 dim, u32 nverts, double const* coords, u32 nel
   // device bytes per element while a mesh adapts (connectivity of every
   // dimension, the adjacency a pass derives, and the next mesh being built)
   j->est_bytes = (unsigned long long)(est * 900.0);
-  j->t_submit = now_s() - sv->t0;
-  sv->queue.push_back(j.get());
-  u32 id = j->id;
-  sv->jobs[id] = std::move(j);
+  u32 id;
+  {
+    std::lock_guard<std::mutex> g(sv->mu);
+    j->id = sv->next_id++;
+    j->t_submit = now_s() - sv->t0;
+    sv->queue.push_back(j.get());
+    id = j->id;
+    sv->jobs[id] = std::move(j);
+  }
+  sv->cv.notify_all();
   return id;
 }
 
-u32 server_step(Server* sv) { return sv->step(); }
+u32 server_step(Server* sv)
+{
+  if (sv->running) throw Failure(E_ARG, "the server's engine thread runs its steps");
+  return sv->step();
+}
+
+void server_start(Server* sv)
+{
+  std::lock_guard<std::mutex> g(sv->mu);
+  if (sv->running) return;
+  CK(cudaGetDevice(&sv->device));
+  sv->running = true;
+  sv->engine = std::thread([sv] { sv->engine_loop(); });
+}
+
+void server_stop(Server* sv) { sv->stop(); }
+
+int server_wait(Server* sv, double timeout_s)
+{
+  std::unique_lock<std::mutex> g(sv->mu);
+  auto pending = [&] {
+    u32 n = (u32)sv->queue.size();
+    for (auto const& kv : sv->jobs)
+      if (!kv.second->finished && std::find(sv->queue.begin(), sv->queue.end(),
+                                              kv.second.get()) == sv->queue.end())
+        ++n;
+    return n;
+  };
+  auto done = [&] { return sv->err_code != 0 || pending() == 0; };
+  if (timeout_s < 0)
+    sv->cv.wait(g, done);
+  else
+    sv->cv.wait_for(g, std::chrono::duration<double>(timeout_s), done);
+  if (sv->err_code) throw Failure(sv->err_code, sv->err_msg);
+  return (int)pending();
+}
 
 void server_set_union_elems(Server* sv, unsigned long long n) { sv->run.max_union_elems = n; }
 
 std::vector<u32> server_poll(Server* sv, u32 max_ids)
 {
+  std::lock_guard<std::mutex> g(sv->mu);
   std::vector<u32> out;
   for (auto& kv : sv->jobs)
     if (kv.second->finished && !kv.second->polled && out.size() < max_ids) {
@@ -256,6 +377,7 @@ std::vector<u32> server_poll(Server* sv, u32 max_ids)
 
 Mesh* server_take(Server* sv, u32 id)
 {
+  std::lock_guard<std::mutex> g(sv->mu);
   auto it = sv->jobs.find(id);
   if (it == sv->jobs.end() || !it->second->finished || it->second->taken)
     throw Failure(E_ARG, "no finished job with that id to take");
@@ -267,6 +389,7 @@ Mesh* server_take(Server* sv, u32 id)
 
 ServeJobInfo server_job_info(Server* sv, u32 id)
 {
+  std::lock_guard<std::mutex> g(sv->mu);
   auto it = sv->jobs.find(id);
   if (it == sv->jobs.end()) throw Failure(E_ARG, "no job with that id");
   ServeJob const& j = *it->second;
@@ -284,17 +407,10 @@ ServeJobInfo server_job_info(Server* sv, u32 id)
 
 ServeStats server_stats(Server* sv)
 {
-  ServeStats r;
-  r.steps = sv->steps;
-  r.rebuilds = sv->unions;
-  r.active = (u32)sv->active.size();
+  std::lock_guard<std::mutex> g(sv->mu);
+  ServeStats r = sv->snap;
   r.queued = (u32)sv->queue.size();
-  r.reserved = sv->reserved;
   r.now = now_s() - sv->t0;
-  r.secs_admit = sv->secs_admit;
-  r.secs_join = 0;
-  r.secs_passes = sv->secs_passes;
-  r.secs_retire = sv->secs_retire;
   return r;
 }
 

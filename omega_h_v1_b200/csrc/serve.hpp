@@ -35,6 +35,12 @@ u32 server_submit(Server* sv, u32 dim, u32 nverts, double const* coords, u32 nel
 // admit what the budget allows, run one step over every resident job, hand
 // back the jobs whose loop ended; returns the jobs still queued or running
 u32 server_step(Server* sv);
+// run steps on an engine thread of the server's own (submissions then
+// overlap the GPU work); server_wait blocks until every submitted job has
+// finished or timeout_s passes (< 0: no limit) and returns the jobs left
+void server_start(Server* sv);
+void server_stop(Server* sv);
+int server_wait(Server* sv, double timeout_s);
 // largest union a pass forms, in current elements (0 = no limit)
 void server_set_union_elems(Server* sv, unsigned long long n);
 // finished jobs not yet reported, at most max_ids of them

@@ -85,3 +85,23 @@ def test_memory_budget_admits_one_job_at_a_time():
     # admitted in submission order, one after another
     assert info[1]["t_admit"] >= info[0]["t_done"]
     sv.close()
+
+
+def test_engine_thread_results_equal_alone():
+    """The server's own engine thread runs the steps while jobs are still
+    being submitted from this thread; every result equals osh_adapt alone."""
+    import time
+    import omega_h_v1_b200 as G
+    inputs = _jobs()
+    sv = G.Server(*ARGS, 1 << 40)
+    sv.start()
+    ids = []
+    for k, (_, coords, conn, h) in enumerate(inputs):
+        ids.append(sv.submit(coords, conn, h))
+        time.sleep(0.002 * k)
+    assert sv.wait(120.0) == 0
+    for i, (_, c, k, h) in enumerate(inputs):
+        m, _ = _alone(c, k, h)
+        assert sv.take(ids[i]).digest() == m.digest(), "job %d" % i
+    sv.stop()
+    sv.close()
