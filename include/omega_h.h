@@ -31,8 +31,12 @@ void osh_fini(void) OSH_PUBLIC;
 /* omega_h.h:15 */
 void osh_free(osh_t m) OSH_PUBLIC;
 
-/* omega_h.h:17-18 -- VTU I/O is not part of this build: osh_read_vtk
-   returns NULL and osh_write_vtk does nothing; both set E_UNSUPPORTED. */
+/* omega_h.h:17-18 (omega_h.cpp:127-154, vtk_io.cpp:787-830) -- the
+   reference's VTU format byte for byte. "x.vtu" is a serial mesh; "x.pvtu"
+   names the parallel index file of the single piece "x.vtu" (one rank).
+   osh_write_vtk writes binary (base64) arrays without compression, as the
+   reference's default build does; osh_b200_write_vtk_opts (omega_h_b200.h)
+   selects ASCII or zlib. A missing or malformed file sets OSH_B200_E_IO. */
 osh_t osh_read_vtk(char const* filename) OSH_PUBLIC;
 void osh_write_vtk(osh_t m, char const* filename) OSH_PUBLIC;
 

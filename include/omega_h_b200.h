@@ -26,7 +26,8 @@ enum osh_b200_error {
   OSH_B200_E_NOMEM = 5,
   OSH_B200_E_UNSUPPORTED = 6,
   OSH_B200_E_TIMEOUT = 7,
-  OSH_B200_E_INVERTED = 8
+  OSH_B200_E_INVERTED = 8,
+  OSH_B200_E_IO = 9          /* a mesh file could not be opened, read or parsed */
 };
 int osh_b200_last_error(void) OSH_PUBLIC;
 char const* osh_b200_last_error_message(void) OSH_PUBLIC;
@@ -129,6 +130,12 @@ void osh_b200_fp32_stats_reset(void) OSH_PUBLIC;
 void osh_b200_pool_reserve(unsigned long long bytes) OSH_PUBLIC;
 void osh_b200_pool_stats(unsigned long long* reserved, unsigned long long* used,
     unsigned long long* used_high, int reset_high) OSH_PUBLIC;
+
+/* ---- mesh files ------------------------------------------------------------ */
+/* write_mesh_vtk_opts (vtk_io.cpp:807-826): ascii != 0 writes ASCII arrays
+   (VTK_ASCII); otherwise binary arrays, zlib-compressed when compress != 0
+   (the reference's USE_ZLIB build). osh_read_vtk reads all three. */
+void osh_b200_write_vtk_opts(osh_t m, char const* filename, int ascii, int compress) OSH_PUBLIC;
 
 /* order-sensitive 64-bit digest of a mesh (connectivity of every dimension,
    tag names, kinds and data, global numbers), computed on the device; equal

@@ -26,7 +26,8 @@ X_NOT, X_POINTWISE, X_CONSERVE, X_INHERIT = 0, 1, 2, 3
 DEG = [[1, 0, 0, 0], [2, 1, 0, 0], [3, 3, 1, 0], [4, 6, 4, 1]]
 _NP = {T_U8: np.uint8, T_U32: np.uint32, T_U64: np.uint64, T_F64: np.float64}
 ERRORS = {0: "ok", 1: "cuda", 2: "no convergence", 3: "max passes", 4: "argument",
-          5: "out of memory", 6: "unsupported", 7: "timeout", 8: "inverted element"}
+          5: "out of memory", 6: "unsupported", 7: "timeout", 8: "inverted element",
+          9: "file"}
 
 _u32p = np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")
 _u64p = np.ctypeslib.ndpointer(np.uint64, flags="C_CONTIGUOUS")
@@ -136,6 +137,11 @@ def lib():
     f("osh_b200_batch_mesh_stats", None, C.c_uint, C.POINTER(C.c_uint), C.POINTER(C.c_double))
     f("osh_b200_batch_times", None, *([C.POINTER(C.c_double)] * 3))
     f("osh_b200_digest", C.c_ulonglong, vp)
+    f("osh_ghost", None, vp, C.c_uint)
+    f("osh_num_ghost_layers", C.c_uint, vp)
+    f("osh_read_vtk", vp, C.c_char_p)
+    f("osh_write_vtk", None, vp, C.c_char_p)
+    f("osh_b200_write_vtk_opts", None, vp, C.c_char_p, C.c_int, C.c_int)
     f("osh_b200_pool_reserve", None, C.c_ulonglong)
     f("osh_b200_pool_stats", None, *([C.POINTER(C.c_ulonglong)] * 3), C.c_int)
     f("osh_b200_set_fp32_filter", None, vp, C.c_int)
@@ -286,6 +292,32 @@ class Mesh:
         """Decide far-from-threshold candidates on single-precision estimates
         (double recheck near thresholds; results unchanged)."""
         self.L.osh_b200_set_fp32_filter(self.h, 1 if on else 0)
+        self._chk()
+
+    def ghost(self, nlayers):
+        """osh_ghost: on one rank, records the layers (and owner caches)."""
+        self.L.osh_ghost(self.h, nlayers)
+        self._chk()
+
+    def ghost_layers(self):
+        return self.L.osh_num_ghost_layers(self.h)
+
+    @classmethod
+    def read_vtk(cls, path):
+        """osh_read_vtk: a ".vtu" file, or the one piece of a ".pvtu" file
+        (as a parallel mesh)."""
+        h = lib().osh_read_vtk(os.fsencode(path))
+        check()
+        return cls(h)
+
+    def write_vtk(self, path, ascii=False, compress=False):
+        """osh_write_vtk (binary) or, with ascii / compress,
+        osh_b200_write_vtk_opts; a ".pvtu" path also writes "<stem>.vtu"."""
+        if ascii or compress:
+            self.L.osh_b200_write_vtk_opts(self.h, os.fsencode(path), int(bool(ascii)),
+                                           int(bool(compress)))
+        else:
+            self.L.osh_write_vtk(self.h, os.fsencode(path))
         self._chk()
 
     def digest(self):

@@ -12,6 +12,7 @@
 #include "fields.hpp"
 #include "serve.hpp"
 #include "passes.hpp"
+#include "vtk_io.hpp"
 
 using osh::Failure;
 using osh::Mesh;
@@ -135,15 +136,20 @@ void osh_free(osh_t h)
   API_CATCH_VOID
 }
 
-osh_t osh_read_vtk(char const*)
+osh_t osh_read_vtk(char const* filename)
 {
-  osh::set_error(osh::E_UNSUPPORTED, "VTU input is not part of this build");
-  return nullptr;
+  API_TRY
+  need(filename != nullptr, "filename is NULL");
+  return reinterpret_cast<osh_t>(osh::read_vtk(filename));
+  API_CATCH(nullptr)
 }
 
-void osh_write_vtk(osh_t, char const*)
+void osh_write_vtk(osh_t h, char const* filename)
 {
-  osh::set_error(osh::E_UNSUPPORTED, "VTU output is not part of this build");
+  API_TRY
+  need(h != nullptr && filename != nullptr, "mesh or filename is NULL");
+  osh::write_vtk(*M(h), filename, false, false);
+  API_CATCH_VOID
 }
 
 osh_t osh_new(unsigned elem_dim)
@@ -265,9 +271,14 @@ unsigned const* osh_own_rank(osh_t h, unsigned dim)
   Mesh* m = M(h);
   need(dim <= m->dim, "bad dimension");
   if (!m->own_ranks[dim]) {
-    u32 n = m->count(dim);
-    m->own_ranks[dim] = osh::dalloc<u32>(n, m->s);
-    osh::fill_u32(m->own_ranks[dim], n, 0, m->s);
+    if (m->parallel) {
+      // mesh_ask_own_ranks (parallel_mesh.cpp:77-84) derives ranks and ids
+      m->note_exchange(dim);
+    } else {
+      u32 n = m->count(dim);
+      m->own_ranks[dim] = osh::dalloc<u32>(n, m->s);
+      osh::fill_u32(m->own_ranks[dim], n, 0, m->s);
+    }
   }
   sync(m);
   return m->own_ranks[dim];
@@ -417,8 +428,21 @@ void osh_mark_classified(osh_t h, unsigned ent_dim, unsigned class_dim, unsigned
   API_CATCH_VOID
 }
 
-void osh_ghost(osh_t h, unsigned nlayers) { M(h)->ghost_layers = nlayers; }
-unsigned osh_num_ghost_layers(osh_t h) { return M(h)->ghost_layers; }
+// mesh_ensure_ghosting (omega_h.cpp:944-947): on one rank the entities stay
+// as they are; the layer count and the owner caches change as the
+// reference's do
+void osh_ghost(osh_t h, unsigned nlayers)
+{
+  API_TRY
+  Mesh* m = M(h);
+  need(m->parallel || nlayers == 0, "ghosting needs a parallel mesh");
+  m->ensure_ghosting(nlayers);
+  sync(m);
+  API_CATCH_VOID
+}
+
+// mesh_ghost_layers (parallel_mesh.cpp:175-180): 0 for a serial mesh
+unsigned osh_num_ghost_layers(osh_t h) { return M(h)->parallel ? M(h)->ghost_layers : 0; }
 
 unsigned osh_adapt(osh_t h, double size_ratio_floor, double good_element_quality,
     unsigned nsliver_layers, unsigned max_passes)
@@ -730,6 +754,14 @@ void osh_b200_pool_stats(unsigned long long* reserved, unsigned long long* used,
 {
   API_TRY
   osh::pool_stats(reserved, used, used_high, reset_high);
+  API_CATCH_VOID
+}
+
+void osh_b200_write_vtk_opts(osh_t h, char const* filename, int ascii, int compress)
+{
+  API_TRY
+  need(h != nullptr && filename != nullptr, "mesh or filename is NULL");
+  osh::write_vtk(*M(h), filename, ascii != 0, compress != 0);
   API_CATCH_VOID
 }
 

@@ -607,6 +607,10 @@ static bool coarsen_select(Mesh& m, u32* codes, double qual_floor, bool require_
     dev_free(clist, s);
     return false;
   }
+  // check_coarsen_quality (coarsen_common.cpp:139-180) ghosts a parallel
+  // mesh and exchanges the collapse codes whatever it then finds
+  m.ensure_ghosting(1);
+  m.note_exchange(1);
   sel.q2 = dalloc<double>((size_t)ne * 2, s);
   CK(cudaMemsetAsync(sel.q2, 0, sizeof(double) * ne * 2, s));
   u32* any = m.mb->dev + 4;
@@ -817,8 +821,13 @@ u32 coarsen_slivers(Mesh& m, double qual_floor, u32 nlayers)
   st.op = 4;
   st.elems_in = m.count(m.dim);
   u32 ne = m.count(1);
+  // coarsen_slivers (coarsen.cpp:51-70) ghosts a parallel mesh; marking the
+  // sliver layers exchanges element marks, marking their vertices vertex marks
+  m.ensure_ghosting(1);
   u32* sl = mark_slivers(m, qual_floor, nlayers);
+  if (nlayers) m.note_exchange(m.dim);
   u32* mv = mark_down(m, m.dim, 0, sl);
+  m.note_exchange(0);
   dev_free(sl, s);
   u32* codes = dalloc<u32>(ne, s);
   u32* any = m.mb->dev + 5;

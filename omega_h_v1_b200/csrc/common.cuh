@@ -43,6 +43,7 @@ enum Error {
   E_UNSUPPORTED = 6,  // entry point not available in this build
   E_TIMEOUT = 7,      // a bounded device wait gave up
   E_INVERTED = 8,     // refinement met an inverted element (reference asserts)
+  E_IO = 9,           // a mesh file could not be opened, read or parsed
 };
 
 struct Failure : std::runtime_error {

@@ -90,6 +90,14 @@ Mesh* Mesh::clone()
         CK(cudaMemcpyAsync(g, globals[d], sizeof(u64) * n, cudaMemcpyDeviceToDevice, c->s));
         c->globals[d] = g;
       }
+      u32* const* own[2] = {&own_ranks[d], &own_ids[d]};
+      u32** cown[2] = {&c->own_ranks[d], &c->own_ids[d]};
+      for (u32 k = 0; k < 2; ++k)
+        if (*own[k]) {
+          *cown[k] = dalloc<u32>(n ? n : 1, c->s);
+          CK(cudaMemcpyAsync(*cown[k], *own[k], sizeof(u32) * n, cudaMemcpyDeviceToDevice,
+              c->s));
+        }
     }
     c->ghost_layers = ghost_layers;
     c->fp32_filter = fp32_filter;
@@ -208,6 +216,7 @@ void Mesh::overwrite(Mesh* with)
     own_ids[d] = with->own_ids[d];
     with->own_ids[d] = nullptr;
   }
+  ghost_layers = with->ghost_layers;
   qual_cache = with->qual_cache;
   with->qual_cache = nullptr;
   nseg = with->nseg;
@@ -272,6 +281,45 @@ void Mesh::set_globals(u32 d, u64* g)
 {
   dev_free(globals[d], s);
   globals[d] = g;
+  dev_free(own_ranks[d], s);
+  own_ranks[d] = nullptr;
+  dev_free(own_ids[d], s);
+  own_ids[d] = nullptr;
+}
+
+void Mesh::ensure_ghosting(u32 nlayers)
+{
+  if (!parallel || seg || nlayers == ghost_layers) return;
+  // unghost_mesh / ghost_mesh rebuild the mesh: owners are forgotten, and
+  // ghosting tags the owner ranks of every dimension it holds
+  for (u32 d = 0; d < 4; ++d) {
+    dev_free(own_ranks[d], s);
+    own_ranks[d] = nullptr;
+    dev_free(own_ids[d], s);
+    own_ids[d] = nullptr;
+  }
+  ghost_layers = nlayers;
+  if (!nlayers) return;
+  for (u32 d = 0; d <= dim; ++d)
+    if (has_dim(d)) {
+      u32 n = count(d);
+      own_ranks[d] = dalloc<u32>(n ? n : 1, s);
+      fill_u32(own_ranks[d], n, 0, s);
+    }
+}
+
+void Mesh::note_exchange(u32 d)
+{
+  if (!parallel || seg || d > dim) return;
+  u32 n = count(d);
+  if (!own_ranks[d]) {
+    own_ranks[d] = dalloc<u32>(n ? n : 1, s);
+    fill_u32(own_ranks[d], n, 0, s);
+  }
+  if (!own_ids[d]) {
+    own_ids[d] = dalloc<u32>(n ? n : 1, s);
+    iota_u32(own_ids[d], n, 1, s);
+  }
 }
 
 void Mesh::make_parallel()

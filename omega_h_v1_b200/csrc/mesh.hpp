@@ -164,7 +164,24 @@ struct Mesh {
     return v;
   }
 
+  // replaces the global numbers of dimension d and forgets its owners
+  // (mesh_set_globals, parallel_mesh.cpp:191-196)
   void set_globals(u32 d, u64* g);
+
+  // Ghosting bookkeeping of a single-rank parallel mesh. The reference ghosts
+  // a parallel mesh at the start of every pass (mesh_ensure_ghosting,
+  // ghost_mesh.cpp:283-291), which on one rank leaves the entities as they
+  // are but records one ghost layer and the owner ranks of every dimension;
+  // each exchange on a dimension (mesh_ask_exchanger, parallel_mesh.cpp:
+  // 96-105) adds owner ranks and ids there. A pass that then finds nothing
+  // to do leaves the mesh in that state, which shows in
+  // osh_num_ghost_layers, osh_own_rank / osh_own_id and the own_rank /
+  // own_id arrays of its files. On one rank the owner rank is 0 and the
+  // owner id the entity's own index, so own_ranks / own_ids hold exactly
+  // those values whenever the reference would hold them. No-ops unless the
+  // mesh is parallel and not a union of segments.
+  void ensure_ghosting(u32 nlayers);
+  void note_exchange(u32 d);
   void derive_model(double crease_angle);  // host classification
   void make_parallel();
 };

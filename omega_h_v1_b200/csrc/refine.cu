@@ -390,7 +390,10 @@ static void refine_build(Mesh& m, u32 const* gen_offs, u32 nsplit)
 // choose_refinement_indset (refine_common.cpp:131-160) on a candidate array
 // the caller owns; returns the independent set or nullptr when nothing
 // qualifies. quals_out (optional) receives the goodness.
-static u32* choose_refinement(Mesh& m, u32* cand, double qual_floor, double** quals_out)
+// uniform: every edge is a candidate; otherwise the candidate kernel of
+// refine_by_size / refine_sets left "any candidate" in mailbox slot 3
+static u32* choose_refinement(Mesh& m, u32* cand, double qual_floor, double** quals_out,
+    bool uniform)
 {
   cudaStream_t s = m.s;
   u32 ne = m.count(1), dim = m.dim;
@@ -415,6 +418,13 @@ static u32* choose_refinement(Mesh& m, u32* cand, double qual_floor, double** qu
   } else {
     m.mb->host[1] = max_u32(cand, ne, s) ? 1 : 0;
   }
+  // choose_refinement_indset (refine_common.cpp:131-160) ghosts a parallel
+  // mesh, and exchanges the edge qualities once any edge is a candidate
+  if (m.parallel && !m.seg) {
+    m.ensure_ghosting(1);
+    bool any_cand = uniform ? ne > 0 : dim >= 2 ? m.mb->host[3] != 0 : m.mb->host[1] != 0;
+    if (any_cand) m.note_exchange(1);
+  }
   if (!m.mb->host[1]) {
     if (quals_out)
       *quals_out = q;
@@ -430,7 +440,7 @@ static u32* choose_refinement(Mesh& m, u32* cand, double qual_floor, double** qu
   return ind;
 }
 
-static u32 refine_common(Mesh& m, u32* cand, double qual_floor)
+static u32 refine_common(Mesh& m, u32* cand, double qual_floor, bool uniform)
 {
   cudaStream_t s = m.s;
   PassStats& st = last_pass_stats();
@@ -438,7 +448,7 @@ static u32 refine_common(Mesh& m, u32* cand, double qual_floor)
   st.op = 1;
   st.elems_in = m.count(m.dim);
   u32 ne = m.count(1);
-  u32* ind = choose_refinement(m, cand, qual_floor, nullptr);
+  u32* ind = choose_refinement(m, cand, qual_floor, nullptr, uniform);
   if (!ind) return 0;
   seg_tally(m, 1, ind);
   u32* gen_offs = exscan_new(ind, ne, s);
@@ -469,7 +479,7 @@ u32 refine_by_size(Mesh& m, double qual_floor)
   }
   // no separate check for "any candidate": with none, the quality kernel
   // keeps none and refine_common returns 0 after its single read-back
-  u32 r = refine_common(m, cand, qual_floor);
+  u32 r = refine_common(m, cand, qual_floor, false);
   dev_free(cand, s);
   return r;
 }
@@ -479,7 +489,7 @@ void uniformly_refine(Mesh& m)
   u32 ne = m.count(1);
   u32* cand = dalloc<u32>(ne, m.s);
   fill_u32(cand, ne, 1, m.s);
-  if (ne) refine_common(m, cand, 0.0);
+  if (ne) refine_common(m, cand, 0.0, true);
   dev_free(cand, m.s);
 }
 
@@ -501,7 +511,7 @@ u32 refine_sets(Mesh& m, double qual_floor, u32* cand_out, u32* good_out,
   }
   CK(cudaMemcpyAsync(good_out, cand_out, sizeof(u32) * ne, cudaMemcpyDeviceToDevice, s));
   double* q = nullptr;
-  u32* ind = choose_refinement(m, good_out, qual_floor, &q);
+  u32* ind = choose_refinement(m, good_out, qual_floor, &q, false);
   CK(cudaMemcpyAsync(quals_out, q, sizeof(double) * ne, cudaMemcpyDeviceToDevice, s));
   dev_free(q, s);
   if (!ind) {

@@ -439,10 +439,15 @@ static bool swap_select(Mesh& m, double gq, u32 nlayers, SwapSel& sel, u32* sliv
   cudaStream_t s = m.s;
   ensure_swap_tables();
   u32 ne = m.count(1), nel = m.count(3);
+  // swap_slivers (swap.cpp:180-196) ghosts a parallel mesh; marking the
+  // sliver layers exchanges element marks, marking their edges edge marks
+  m.ensure_ghosting(1);
   u32* sl = mark_slivers(m, gq, nlayers);
+  if (nlayers) m.note_exchange(3);
   if (slivers_out)
     CK(cudaMemcpyAsync(slivers_out, sl, sizeof(u32) * nel, cudaMemcpyDeviceToDevice, s));
   sel.cand = mark_down(m, 3, 1, sl);
+  m.note_exchange(1);
   dev_free(sl, s);
   if (cand_out)
     CK(cudaMemcpyAsync(cand_out, sel.cand, sizeof(u32) * ne, cudaMemcpyDeviceToDevice, s));

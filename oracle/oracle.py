@@ -23,6 +23,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_OMP_SO = os.path.join(HERE, "_ref", "libosh_ref_omp.so")
 REF_SERIAL_SO = os.path.join(HERE, "_ref", "libosh_ref_serial.so")
+REF_ZLIB_SO = os.path.join(HERE, "_ref", "libosh_ref_zlib.so")
 
 T_U8, T_U32, T_U64, T_F64 = 0, 1, 2, 3
 X_NOT, X_POINTWISE, X_CONSERVE, X_INHERIT = 0, 1, 2, 3
@@ -122,6 +123,13 @@ class _Lib:
         self.size_from_hessian = f("size_from_hessian", None, vp, C.c_char_p, C.c_void_p,
                                    C.c_double, C.c_double)
         self.warp_to_limit = f("warp_to_limit", C.c_uint, vp, C.c_double)
+        if prefix == "refd_":
+            # VTU files (vtk_io.cpp), only in the reference driver
+            self.read_vtk = f("read_vtk", vp, C.c_char_p)
+            self.write_vtk = f("write_vtk", None, vp, C.c_char_p, C.c_uint)
+            self.is_full = f("is_full", C.c_uint, vp)
+            self.is_parallel = f("is_parallel", C.c_uint, vp)
+            self.ghost_layers = f("ghost_layers", C.c_uint, vp)
 
 
 _LIBS: dict = {}
@@ -145,10 +153,30 @@ class CpuMesh:
         nelems = conn.size // DEG[dim][0]
         self.h = lib.new_reduced(dim, nverts, coords.ravel(), nelems, conn.ravel())
 
+    @classmethod
+    def adopt(cls, lib: _Lib, handle):
+        m = cls.__new__(cls)
+        m.L, m.h = lib, handle
+        return m
+
     def close(self):
         if self.h:
             self.L.free(self.h)
             self.h = None
+
+    def write_vtk(self, path, ascii=False):
+        """write_mesh_vtk_opts of the reference (binary is zlib-compressed in
+        the zlib build)."""
+        self.L.write_vtk(self.h, os.fsencode(path), 1 if ascii else 0)
+
+    def is_full(self):
+        return bool(self.L.is_full(self.h))
+
+    def is_parallel(self):
+        return bool(self.L.is_parallel(self.h))
+
+    def ghost_layers(self):
+        return self.L.ghost_layers(self.h)
 
     def __del__(self):
         try:
@@ -331,6 +359,22 @@ def Oracle(dim, coords, conn) -> CpuMesh:
 def Reference(dim, coords, conn, serial=False) -> CpuMesh:
     return CpuMesh(_lib(REF_SERIAL_SO if serial else REF_OMP_SO, "refd_"),
                    dim, coords, conn)
+
+
+def reference_read_vtk(path, variant="serial") -> CpuMesh:
+    """read_mesh_vtk of the reference; variant "serial", "omp" or "zlib"."""
+    so = {"serial": REF_SERIAL_SO, "omp": REF_OMP_SO, "zlib": REF_ZLIB_SO}[variant]
+    lib = _lib(so, "refd_")
+    return CpuMesh.adopt(lib, lib.read_vtk(os.fsencode(path)))
+
+
+def reference_lib(variant="serial") -> _Lib:
+    so = {"serial": REF_SERIAL_SO, "omp": REF_OMP_SO, "zlib": REF_ZLIB_SO}[variant]
+    return _lib(so, "refd_")
+
+
+def ReferenceVariant(dim, coords, conn, variant="serial") -> CpuMesh:
+    return CpuMesh(reference_lib(variant), dim, coords, conn)
 
 
 # -- seeded synthetic inputs ---------------------------------------------------

@@ -38,6 +38,7 @@
 #include "swap_qualities.hpp"
 #include "tables.hpp"
 #include "tag.hpp"
+#include "vtk_io.hpp"
 #include "warp_to_limit.hpp"
 
 using namespace omega_h;
@@ -68,6 +69,19 @@ void refd_derive_model_full(void* p)
 }
 
 void refd_make_parallel(void* p) { mesh_make_parallel(M(p)); }
+
+// read_mesh_vtk / write_mesh_vtk_opts (vtk_io.cpp:787-826); ascii selects
+// VTK_ASCII, else VTK_BINARY (zlib-compressed in the USE_ZLIB=1 build)
+void* refd_read_vtk(char const* path) { return read_mesh_vtk(path); }
+
+void refd_write_vtk(void* p, char const* path, unsigned ascii)
+{
+  write_mesh_vtk_opts(M(p), path, ascii ? VTK_ASCII : VTK_BINARY);
+}
+
+unsigned refd_is_full(void* p) { return mesh_get_rep(M(p)) == MESH_FULL; }
+unsigned refd_is_parallel(void* p) { return mesh_is_parallel(M(p)); }
+unsigned refd_ghost_layers(void* p) { return mesh_ghost_layers(M(p)); }
 
 void refd_free(void* p) { free_mesh(M(p)); }
 

@@ -103,8 +103,8 @@ def test_getters_and_small_entry_points():
     L.osh_b200_copy_to_host(r.ctypes.data_as(C.c_void_p), pr, r.nbytes)
     L.osh_b200_copy_to_host(i.ctypes.data_as(C.c_void_p), pi, i.nbytes)
     assert not r.any() and np.array_equal(i, np.arange(o.count(0)))
-    # VTU I/O is outside this build: reported, not aborted
+    # a missing VTU file is reported (OSH_B200_E_IO), not aborted on
     L.osh_read_vtk.restype = C.c_void_p
     assert not L.osh_read_vtk(b"missing.vtu")
-    assert L.osh_b200_last_error() == 6
+    assert L.osh_b200_last_error() == 9
     L.osh_b200_clear_error()
