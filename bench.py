@@ -41,10 +41,15 @@ N_BOX = 48
 H0, H1 = 0.01, 0.04
 SIZE_FLOOR, GOOD_QUAL, NLAYERS, MAX_OPS = 1.0 / 3.0, 0.3, 4, 50
 L2_BYTES = 126 * 2 ** 20
-# DRAM bytes (read + write) per launch of the reflect_down kernels over one
-# adapt of this workload, from the ncu capture summarised in
-# profiles/k_reflect_down_box48_adapt.md (mean over the adapt's 37 launches)
-REFLECT_TRAFFIC_PER_LAUNCH = 75.3e6
+# DRAM bytes (read + write) per launch of a probed kernel over one adapt of
+# this workload, from the ncu captures summarised in profiles/ (mean over
+# the adapt's launches of that kernel); None where no capture exists
+TRAFFIC_PER_LAUNCH = {
+    "carry_up": 119.1e6,      # profiles/k_carry_up_box48_adapt.md
+}
+# the kernel whose roofline the bench line reports: the one with the largest
+# share of the adapt's time in the live probe
+DEFAULT_PROBE = "carry_up"
 
 
 def workload_config():
@@ -270,7 +275,10 @@ def run_ours(args, world, rank, local):
         L.osh_free(copies[i])
     torch.cuda.synchronize()
     # the probe of the dominant kernel runs live inside the timed region
-    probe_id = args.probe
+    names = [L.osh_b200_probe_name(i).decode() for i in range(L.osh_b200_probe_count())]
+    if args.probe not in names:
+        raise SystemExit("unknown probe %r (have %s)" % (args.probe, ", ".join(names)))
+    probe_id = names.index(args.probe)
     L.osh_b200_probe_reset()
     L.osh_b200_probe_enable(1 << probe_id)
     launches0 = L.osh_b200_launch_count()
@@ -314,7 +322,7 @@ def run_ours(args, world, rank, local):
                 "launches": plaunch.value, "avg_launch_us": round(avg_ms * 1e3, 2),
                 "algorithmic_bytes_per_launch": round(avg_bytes),
                 "traffic": args.traffic if args.traffic is not None else
-                (REFLECT_TRAFFIC_PER_LAUNCH if probe_id == 0 else None)}
+                TRAFFIC_PER_LAUNCH.get(args.probe)}
     base.close()
     return {
         "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world,
@@ -878,8 +886,8 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--probe", type=int, default=int(os.environ.get("OSH_BENCH_PROBE", "0")),
-                    help="probe id of the kernel whose roofline is reported")
+    ap.add_argument("--probe", default=os.environ.get("OSH_BENCH_PROBE", DEFAULT_PROBE),
+                    help="probe name of the kernel whose roofline is reported")
     ap.add_argument("--traffic", type=float, default=None,
                     help="DRAM bytes per launch of that kernel from an ncu capture")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")

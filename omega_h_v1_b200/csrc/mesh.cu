@@ -192,6 +192,8 @@ void Mesh::overwrite(Mesh* with)
       up[h][l] = with->up[h][l];
       have_up[h][l] = with->have_up[h][l];
       up_sorted[h][l] = with->up_sorted[h][l];
+      used_up[h][l] = false;
+      used_down[h][l] = false;
       star[h][l] = with->star[h][l];
       have_star[h][l] = with->have_star[h][l];
       with->down[h][l] = nullptr;
@@ -939,30 +941,58 @@ void Mesh::reflect_range(u32 high, u32 low, u32 first, u32* out)
 }
 
 // new ids of a surviving high entity's lows: its old lows through the lows'
-// survivor offsets (a surviving entity's lows all survive)
-__global__ void k_carry_down(u32 nh_old, u32 lph, u32 const* __restrict__ same_h,
+// survivor offsets (a surviving entity's lows all survive). A thread takes
+// CARRY_UNROLL entries a block apart (reads and writes stay coalesced) and
+// issues all their loads before it uses any: the gather through same_l is
+// the one random access, and a single entry per thread left the kernel
+// waiting on two dependent loads per entry.
+constexpr u32 CARRY_UNROLL = 4;
+
+template <u32 LPH>
+__global__ void __launch_bounds__(BLOCK) k_carry_down(u32 n, u32 const* __restrict__ same_h,
     u32 const* __restrict__ same_l, u32 const* __restrict__ old_down, u32* __restrict__ out)
 {
-  u32 t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= nh_old * lph) return;
-  u32 i = t / lph, k = t - i * lph;
-  u32 ni = same_h[i];
-  if (same_h[i + 1] == ni) return;
-  out[(size_t)ni * lph + k] = same_l[old_down[t]];
+  u32 base = blockIdx.x * (BLOCK * CARRY_UNROLL) + threadIdx.x;
+  u32 od[CARRY_UNROLL], ni[CARRY_UNROLL], nn[CARRY_UNROLL];
+#pragma unroll
+  for (u32 k = 0; k < CARRY_UNROLL; ++k) {
+    u32 t = base + k * BLOCK;
+    od[k] = 0;
+    ni[k] = nn[k] = 0;
+    if (t < n) {
+      u32 i = t / LPH;
+      ni[k] = same_h[i];
+      nn[k] = same_h[i + 1];
+      od[k] = old_down[t];
+    }
+  }
+#pragma unroll
+  for (u32 k = 0; k < CARRY_UNROLL; ++k) {
+    u32 t = base + k * BLOCK;
+    if (t < n && nn[k] != ni[k]) out[(size_t)ni[k] * LPH + t % LPH] = same_l[od[k]];
+  }
 }
 
 void carry_down(Mesh& m, Mesh& out, u32 high, u32 low, u32 const* same_h, u32 nsame,
     u32 const* same_l)
 {
-  if (!m.down[high][low] || out.down[high][low] || !out.has_dim(high) || !out.has_dim(low))
+  if (!m.down[high][low] || !m.used_down[high][low] || out.down[high][low] ||
+      !out.has_dim(high) || !out.has_dim(low))
     return;
   cudaStream_t s = out.s;
   u32 nh_old = m.counts[high], nh = out.count(high), lph = deg(high, low);
   out.count(low);
   u32* dn = dalloc<u32>((size_t)nh * lph, s);
   if (nh_old) {
-    k_carry_down<<<grid_for((u64)nh_old * lph), BLOCK, 0, s>>>(nh_old, lph, same_h, same_l,
-        m.down[high][low], dn);
+    u32 n = nh_old * lph;
+    u32 g = (u32)ceil_div((u64)n, (u64)BLOCK * CARRY_UNROLL);
+    PROBE(P_CARRY, s, 4.0 * (nh_old + 1) + 12.0 * n);
+    if (lph == 3)
+      k_carry_down<3><<<g, BLOCK, 0, s>>>(n, same_h, same_l, m.down[high][low], dn);
+    else if (lph == 4)
+      k_carry_down<4><<<g, BLOCK, 0, s>>>(n, same_h, same_l, m.down[high][low], dn);
+    else
+      k_carry_down<6><<<g, BLOCK, 0, s>>>(n, same_h, same_l, m.down[high][low], dn);
     CK_LAUNCH();
   }
   // the survivors come first; the entities the pass made are searched
@@ -974,19 +1004,35 @@ void carry_down(Mesh& m, Mesh& out, u32 high, u32 low, u32 const* same_h, u32 ns
 // its old row whose high entity survived, in the old order, mapped to new
 // ids, followed by the uses of the entities the pass made; a low the pass
 // made has only such uses (a surviving high entity's lows all survive).
+// One thread walks one old row, four uses at a time with their loads issued
+// together; newid_h holds each old high entity's new id or INV, one gather
+// per use. (Measured alternatives: a lane group per row left too few rows in
+// flight and ran at half the speed; a warp per 32 rows reading their uses
+// coalesced ran at the same speed as this.)
+__global__ void k_new_ids(u32 n, u32 const* __restrict__ same, u32* __restrict__ newid)
+{
+  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  u32 a = same[i];
+  newid[i] = same[i + 1] != a ? a : INV;
+}
+
 __global__ void k_up_surv_count(u32 nl_old, u32 const* __restrict__ same_l,
-    u32 const* __restrict__ same_h, u32 const* __restrict__ offs, u32 const* __restrict__ adj,
+    u32 const* __restrict__ newid_h, u32 const* __restrict__ offs, u32 const* __restrict__ adj,
     u32* __restrict__ cnt, u32* __restrict__ surv)
 {
   u32 j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= nl_old) return;
   u32 nj = same_l[j];
   if (same_l[j + 1] == nj) return;
+  u32 r = offs[j], e = offs[j + 1];
   u32 c = 0;
-  for (u32 r = offs[j]; r < offs[j + 1]; ++r) {
-    u32 a = adj[r];
-    c += same_h[a + 1] != same_h[a] ? 1u : 0u;
+  for (; r + 4 <= e; r += 4) {
+    u32 a0 = adj[r], a1 = adj[r + 1], a2 = adj[r + 2], a3 = adj[r + 3];
+    u32 n0 = newid_h[a0], n1 = newid_h[a1], n2 = newid_h[a2], n3 = newid_h[a3];
+    c += (n0 != INV) + (n1 != INV) + (n2 != INV) + (n3 != INV);
   }
+  for (; r < e; ++r) c += newid_h[adj[r]] != INV;
   cnt[nj] = c;
   surv[nj] = c;
 }
@@ -999,7 +1045,7 @@ __global__ void k_up_gen_count(u32 first, u32 nuses, u32 const* __restrict__ loh
 }
 
 __global__ void k_up_surv_fill(u32 nl_old, u32 const* __restrict__ same_l,
-    u32 const* __restrict__ same_h, u32 const* __restrict__ offs_old,
+    u32 const* __restrict__ newid_h, u32 const* __restrict__ offs_old,
     u32 const* __restrict__ adj_old, u32 const* __restrict__ dirs_old,
     u32 const* __restrict__ offs, u32* __restrict__ adj, u32* __restrict__ dirs)
 {
@@ -1008,9 +1054,27 @@ __global__ void k_up_surv_fill(u32 nl_old, u32 const* __restrict__ same_l,
   u32 nj = same_l[j];
   if (same_l[j + 1] == nj) return;
   u32 w = offs[nj];
-  for (u32 r = offs_old[j]; r < offs_old[j + 1]; ++r) {
-    u32 a = adj_old[r], na = same_h[a];
-    if (same_h[a + 1] == na) continue;
+  u32 r = offs_old[j], e = offs_old[j + 1];
+  for (; r + 4 <= e; r += 4) {
+    u32 a[4], d[4], na[4];
+#pragma unroll
+    for (u32 k = 0; k < 4; ++k) {
+      a[k] = adj_old[r + k];
+      d[k] = dirs_old[r + k];
+    }
+#pragma unroll
+    for (u32 k = 0; k < 4; ++k) na[k] = newid_h[a[k]];
+#pragma unroll
+    for (u32 k = 0; k < 4; ++k)
+      if (na[k] != INV) {
+        adj[w] = na[k];
+        dirs[w] = d[k];
+        ++w;
+      }
+  }
+  for (; r < e; ++r) {
+    u32 na = newid_h[adj_old[r]];
+    if (na == INV) continue;
     adj[w] = na;
     dirs[w] = dirs_old[r];
     ++w;
@@ -1031,7 +1095,7 @@ __global__ void k_up_gen_fill(u32 first, u32 nuses, u32 lph, u32 const* __restri
 void carry_up(Mesh& m, Mesh& out, u32 low, u32 high, u32 const* same_l, u32 const* same_h,
     u32 nsame_h)
 {
-  if (!m.have_up[low][high] || out.have_up[low][high]) return;
+  if (!m.have_up[low][high] || !m.used_up[low][high] || out.have_up[low][high]) return;
   if (!out.has_dim(high) || !out.has_dim(low)) return;
   if (low > 0 && !out.down[high][low]) return;  // its search is not worth it here
   cudaStream_t s = out.s;
@@ -1039,12 +1103,20 @@ void carry_up(Mesh& m, Mesh& out, u32 low, u32 high, u32 const* same_l, u32 cons
   u32 lph = deg(high, low), nuses = nh * lph, first = nsame_h * lph;
   u32 const* loh = out.ask_down(high, low);
   UpAdj const& old = m.up[low][high];
+  u32 nh_old = m.counts[high];
+  u32* newid_h = dalloc<u32>(nh_old ? nh_old : 1, s);
+  if (nh_old) {
+    k_new_ids<<<grid_for(nh_old), BLOCK, 0, s>>>(nh_old, same_h, newid_h);
+    CK_LAUNCH();
+  }
   u32* cnt = dalloc<u32>((size_t)nl + 1, s);
   u32* surv = dalloc<u32>((size_t)nl + 1, s);
   CK(cudaMemsetAsync(cnt, 0, sizeof(u32) * ((size_t)nl + 1), s));
   CK(cudaMemsetAsync(surv, 0, sizeof(u32) * ((size_t)nl + 1), s));
+  u32 nuses_old = m.counts[high] * lph;
   if (nl_old) {
-    k_up_surv_count<<<grid_for(nl_old), BLOCK, 0, s>>>(nl_old, same_l, same_h, old.offs,
+    PROBE(P_CARRY_UP, s, 8.0 * (nl_old + 1) + 4.0 * nuses_old + 8.0 * nuses_old + 8.0 * nl);
+    k_up_surv_count<<<grid_for(nl_old), BLOCK, 0, s>>>(nl_old, same_l, newid_h, old.offs,
         old.adj, cnt, surv);
     CK_LAUNCH();
   }
@@ -1062,8 +1134,9 @@ void carry_up(Mesh& m, Mesh& out, u32 low, u32 high, u32 const* same_l, u32 cons
   u.adj = dalloc<u32>(nuses, s);
   u.dirs = dalloc<u32>(nuses, s);
   if (nl_old) {
-    k_up_surv_fill<<<grid_for(nl_old), BLOCK, 0, s>>>(nl_old, same_l, same_h, old.offs, old.adj,
-        old.dirs, u.offs, u.adj, u.dirs);
+    PROBE(P_CARRY_UP, s, 8.0 * (nl_old + 1) + 12.0 * nuses_old + 8.0 * nuses_old + 4.0 * nl);
+    k_up_surv_fill<<<grid_for(nl_old), BLOCK, 0, s>>>(nl_old, same_l, newid_h, old.offs,
+        old.adj, old.dirs, u.offs, u.adj, u.dirs);
     CK_LAUNCH();
   }
   if (nuses > first) {
@@ -1073,6 +1146,7 @@ void carry_up(Mesh& m, Mesh& out, u32 low, u32 high, u32 const* same_l, u32 cons
     CK_LAUNCH();
   }
   dev_free(cnt, s);
+  dev_free(newid_h, s);
   if (m.up_sorted[low][high]) {
     u.pre = surv;
     u.npre = first;
@@ -1086,6 +1160,7 @@ void carry_up(Mesh& m, Mesh& out, u32 low, u32 high, u32 const* same_l, u32 cons
 
 u32 const* Mesh::ask_down(u32 high, u32 low)
 {
+  used_down[high][low] = true;
   if (down[high][low]) return down[high][low];
   if (low == high) {
     u32 n = counts[high];
@@ -1143,6 +1218,7 @@ u32 const* Mesh::ask_down(u32 high, u32 low)
 
 UpAdj const& Mesh::ask_up(u32 low, u32 high, bool sorted)
 {
+  used_up[low][high] = true;
   if (have_up[low][high]) {
     if (sorted && !up_sorted[low][high]) {
       sort_up_rows(high, low, counts[high], counts[low], up[low][high], s);

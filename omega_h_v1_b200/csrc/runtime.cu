@@ -83,7 +83,7 @@ ProbeState& probes()
 char const* const g_probe_names[P_NPROBES] = {"reflect_down", "up_count", "up_fill",
     "up_rank", "exscan", "elem_quality", "refine_candidates", "refine_quality",
     "indset_round", "coarsen_quality", "swap_quality", "refine_topology",
-    "collapse_to_ent", "expand"};
+    "collapse_to_ent", "expand", "carry_down", "carry_up"};
 }  // namespace
 
 char const* probe_name(u32 id) { return id < P_NPROBES ? g_probe_names[id] : nullptr; }
@@ -312,8 +312,11 @@ void Mailbox::fetch(cudaStream_t s, u32 nslots)
 // prefix. The walk is bounded: after SCAN_SPIN_LIMIT empty polls it records
 // E_TIMEOUT in the error word and stops instead of spinning forever.
 
-constexpr int SCAN_THREADS = 256;
-constexpr int SCAN_ITEMS = 8;
+// 8192-element tiles: a 2M-element scan has 256 tiles, so a tile's
+// look-back meets a published prefix within a few steps (with 2048-element
+// tiles the chain of look-backs, not bandwidth, set the time)
+constexpr int SCAN_THREADS = 512;
+constexpr int SCAN_ITEMS = 16;
 constexpr int SCAN_TILE = SCAN_THREADS * SCAN_ITEMS;
 constexpr int SCAN_WARPS = SCAN_THREADS / 32;
 constexpr unsigned long long FLAG_AGG = 1ull << 62;

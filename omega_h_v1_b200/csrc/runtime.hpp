@@ -65,6 +65,8 @@ enum ProbeId {
   P_REFINE_TOPOLOGY,
   P_COLLAPSE_TO_ENT,
   P_EXPAND,
+  P_CARRY,
+  P_CARRY_UP,
   P_NPROBES
 };
 char const* probe_name(u32 id);
