@@ -192,8 +192,6 @@ void Mesh::overwrite(Mesh* with)
       up[h][l] = with->up[h][l];
       have_up[h][l] = with->have_up[h][l];
       up_sorted[h][l] = with->up_sorted[h][l];
-      used_up[h][l] = false;
-      used_down[h][l] = false;
       star[h][l] = with->star[h][l];
       have_star[h][l] = with->have_star[h][l];
       with->down[h][l] = nullptr;
@@ -976,8 +974,7 @@ __global__ void __launch_bounds__(BLOCK) k_carry_down(u32 n, u32 const* __restri
 void carry_down(Mesh& m, Mesh& out, u32 high, u32 low, u32 const* same_h, u32 nsame,
     u32 const* same_l)
 {
-  if (!m.down[high][low] || !m.used_down[high][low] || out.down[high][low] ||
-      !out.has_dim(high) || !out.has_dim(low))
+  if (!m.down[high][low] || out.down[high][low] || !out.has_dim(high) || !out.has_dim(low))
     return;
   cudaStream_t s = out.s;
   u32 nh_old = m.counts[high], nh = out.count(high), lph = deg(high, low);
@@ -1095,7 +1092,7 @@ __global__ void k_up_gen_fill(u32 first, u32 nuses, u32 lph, u32 const* __restri
 void carry_up(Mesh& m, Mesh& out, u32 low, u32 high, u32 const* same_l, u32 const* same_h,
     u32 nsame_h)
 {
-  if (!m.have_up[low][high] || !m.used_up[low][high] || out.have_up[low][high]) return;
+  if (!m.have_up[low][high] || out.have_up[low][high]) return;
   if (!out.has_dim(high) || !out.has_dim(low)) return;
   if (low > 0 && !out.down[high][low]) return;  // its search is not worth it here
   cudaStream_t s = out.s;
@@ -1160,7 +1157,6 @@ void carry_up(Mesh& m, Mesh& out, u32 low, u32 high, u32 const* same_l, u32 cons
 
 u32 const* Mesh::ask_down(u32 high, u32 low)
 {
-  used_down[high][low] = true;
   if (down[high][low]) return down[high][low];
   if (low == high) {
     u32 n = counts[high];
@@ -1218,7 +1214,6 @@ u32 const* Mesh::ask_down(u32 high, u32 low)
 
 UpAdj const& Mesh::ask_up(u32 low, u32 high, bool sorted)
 {
-  used_up[low][high] = true;
   if (have_up[low][high]) {
     if (sorted && !up_sorted[low][high]) {
       sort_up_rows(high, low, counts[high], counts[low], up[low][high], s);

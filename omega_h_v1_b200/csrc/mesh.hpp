@@ -78,11 +78,6 @@ struct Mesh {
   bool up_sorted[4][4] = {};  // rows in use-index order (the reference's)
   Graph star[4][4] = {};
   bool have_star[4][4] = {};
-  // adjacency asked for since this mesh state was made: a pass carries into
-  // the mesh it builds only what its input was asked for (the next pass of
-  // the same kind asks for the same), the rest is derived if ever asked
-  bool used_up[4][4] = {};
-  bool used_down[4][4] = {};
   u32* dual = nullptr;
   // reflect_down's search rows: every edge (1) / triangle (2) listed once, in
   // the row of its smallest vertex, as (other vertices..., id) records:
