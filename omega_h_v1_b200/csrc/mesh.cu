@@ -1421,9 +1421,10 @@ double Mesh::min_quality()
 {
   double const* q = qualities();
   u32 ne = count(dim);
-  unsigned long long k;
-  CK(cudaMemcpyAsync(&k, q + ne, sizeof(k), cudaMemcpyDeviceToHost, s));
+  unsigned long long* hk = static_cast<unsigned long long*>(pinned_scratch());
+  CK(cudaMemcpyAsync(hk, q + ne, sizeof(*hk), cudaMemcpyDeviceToHost, s));
   stream_sync(s);
+  unsigned long long k = *hk;
   if (k == ~0ull) return DBL_MAX;
   return from_order_key(k);
 }

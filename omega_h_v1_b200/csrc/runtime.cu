@@ -260,20 +260,40 @@ void dev_free(void* p, cudaStream_t s)
   if (p) CK(cudaFreeAsync(p, s));
 }
 
+namespace {
+// a pinned word per host thread for read_u32: a copy into pageable memory
+// goes through the driver's staging buffer and takes several times longer
+struct PinnedWord {
+  u32* p = nullptr;
+  ~PinnedWord()
+  {
+    if (p) cudaFreeHost(p);
+  }
+  u32* get()
+  {
+    if (!p) CK(cudaMallocHost(&p, 64));
+    return p;
+  }
+};
+thread_local PinnedWord t_word;
+}  // namespace
+
+void* pinned_scratch() { return t_word.get(); }
+
 u32 read_u32(u32 const* d, cudaStream_t s)
 {
-  u32 v = 0;
-  CK(cudaMemcpyAsync(&v, d, sizeof(u32), cudaMemcpyDeviceToHost, s));
+  u32* h = t_word.get();
+  CK(cudaMemcpyAsync(h, d, sizeof(u32), cudaMemcpyDeviceToHost, s));
   stream_sync(s);
-  return v;
+  return *h;
 }
 
 double read_f64(double const* d, cudaStream_t s)
 {
-  double v = 0;
-  CK(cudaMemcpyAsync(&v, d, sizeof(double), cudaMemcpyDeviceToHost, s));
+  double* h = static_cast<double*>(pinned_scratch());
+  CK(cudaMemcpyAsync(h, d, sizeof(double), cudaMemcpyDeviceToHost, s));
   stream_sync(s);
-  return v;
+  return *h;
 }
 
 void Mailbox::init(cudaStream_t s)

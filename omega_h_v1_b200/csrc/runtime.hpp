@@ -96,6 +96,9 @@ struct ProbeScope {
 unsigned long long launch_count();
 unsigned long long sync_count();
 void stream_sync(cudaStream_t s);
+// 64 bytes of pinned host memory owned by the calling host thread, for small
+// device-to-host reads (a read into pageable memory is staged by the driver)
+void* pinned_scratch();
 
 // small pinned host mailbox for reading several device scalars at once
 struct Mailbox {
