@@ -310,6 +310,9 @@ def run_ours(args, world, rank, local):
     e2e = None
     if not args.no_e2e:
         e2e = e2e_leg(G, L, base, args, world, stream, stream_ptr)
+    fp32 = None
+    if not args.no_fp32:
+        fp32 = fp32_leg(G, L, base, args, world, stream, stream_ptr, ms_local)
     peak, peak_kind = measured_peak()
     roof = None
     if plaunch.value:
@@ -332,11 +335,59 @@ def run_ours(args, world, rank, local):
         "config": workload_config(),
         "roofline": roof,
         "e2e": e2e,
+        "fp32_filter": fp32,
         "gpu_launches": int(launches),
         "clocks": clk,
         "tets_in": tets_in,
         "passes_per_step": npass[0] if npass else None,
     }
+
+
+def fp32_leg(G, L, base, args, world, stream, stream_ptr, plain_ms):
+    """The same adapts with the single-precision filter (candidate lengths
+    and qualities decided on an FP32 estimate with an error bound, FP64
+    recheck near every threshold), timed the same way after the plain leg;
+    the adapted mesh's device digest must equal the plain path's."""
+    import torch
+    def fresh(filt):
+        h = L.osh_b200_clone(base.h)
+        G.check()
+        L.osh_b200_set_stream(h, C.c_void_p(stream_ptr))
+        L.osh_b200_set_fp32_filter(h, 1 if filt else 0)
+        return h
+    digests = []
+    for filt in (False, True):
+        h = fresh(filt)
+        L.osh_adapt(h, SIZE_FLOOR, GOOD_QUAL, NLAYERS, MAX_OPS)
+        G.check()
+        digests.append(L.osh_b200_digest(h))
+        L.osh_free(h)
+    copies = [fresh(True) for _ in range(args.steps)]
+    L.osh_b200_fp32_stats_reset()
+    torch.cuda.synchronize()
+    barrier(world)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    units = 0.0
+    for h in copies:
+        L.osh_adapt(h, SIZE_FLOOR, GOOD_QUAL, NLAYERS, MAX_OPS)
+        G.check()
+        passes, e = C.c_uint(), C.c_double()
+        L.osh_b200_adapt_stats(C.byref(passes), C.byref(e))
+        units += e.value
+        L.osh_free(h)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    ms_local = e0.elapsed_time(e1)
+    value, ms, _ = replica_throughput(units, ms_local, world)
+    fs = G.fp32_stats()
+    return {"value": round(value, 1), "unit": UNIT, "ms_per_step": round(ms / args.steps, 3),
+            "vs_plain_fp64": round(plain_ms / ms_local, 3),
+            "identical_to_plain": bool(digests[0] == digests[1]),
+            "decided_single": fs["decided"], "rechecked_double": fs["rechecked"],
+            "max_fp32_error": fs["max_error"], "bound_exceeded": fs["bound_exceeded"]}
 
 
 def e2e_leg(G, L, base, args, world, stream, stream_ptr):
@@ -892,6 +943,8 @@ def main():
                     help="DRAM bytes per launch of that kernel from an ncu capture")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling)")
+    ap.add_argument("--no-fp32", action="store_true",
+                    help="skip the single-precision filter leg of the box48 workload")
     ap.add_argument("--workload", default="box48",
                     choices=["box48", "batched", "serving", "warp"],
                     help="box48: the 48^3 radial-size adapt; batched: 512 uneven boxes, "

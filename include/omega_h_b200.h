@@ -258,6 +258,10 @@ void osh_b200_adapt_stats(unsigned* passes, double* elems_in) OSH_PUBLIC;
    waited for the device (stream synchronisations) */
 unsigned long long osh_b200_launch_count(void) OSH_PUBLIC;
 unsigned long long osh_b200_sync_count(void) OSH_PUBLIC;
+/* device allocations made by this library so far, and the host seconds its
+   stream synchronisations spent waiting for the device (diagnostics of the
+   host side of a pass) */
+void osh_b200_host_stats(unsigned long long* allocs, double* sync_wait_seconds) OSH_PUBLIC;
 /* run all further work of mesh m on the CUDA stream `stream` (a
    cudaStream_t; 0 is the legacy default stream); the caller keeps it alive */
 void osh_b200_set_stream(osh_t m, void* stream) OSH_PUBLIC;

@@ -170,6 +170,7 @@ def lib():
     f("osh_b200_server_times", None, vp, *([C.POINTER(C.c_double)] * 4))
     f("osh_b200_launch_count", C.c_ulonglong)
     f("osh_b200_sync_count", C.c_ulonglong)
+    f("osh_b200_host_stats", None, C.POINTER(C.c_ulonglong), C.POINTER(C.c_double))
     f("osh_b200_probe_enable", None, C.c_uint)
     f("osh_b200_probe_reset", None)
     f("osh_b200_probe_count", C.c_uint)

@@ -1095,6 +1095,10 @@ void osh_b200_adapt_stats(unsigned* passes, double* elems_in)
 
 unsigned long long osh_b200_launch_count(void) { return osh::launch_count(); }
 unsigned long long osh_b200_sync_count(void) { return osh::sync_count(); }
+void osh_b200_host_stats(unsigned long long* allocs, double* sync_wait_seconds)
+{
+  osh::host_stats(allocs, sync_wait_seconds);
+}
 
 void osh_b200_set_stream(osh_t h, void* stream)
 {

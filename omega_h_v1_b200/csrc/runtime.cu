@@ -1,5 +1,6 @@
 // Device runtime for the adaptation pass: error state, stream-ordered
 // allocation, the decoupled look-back exclusive scan and small array kernels.
+#include <chrono>
 #include <cstdio>
 #include <cstring>
 #include <atomic>
@@ -51,12 +52,23 @@ unsigned long long launch_count() { return g_launches.load(); }
 
 namespace {
 std::atomic<unsigned long long> g_syncs{0};
+std::atomic<unsigned long long> g_sync_ns{0};
+std::atomic<unsigned long long> g_allocs{0};
 }
 unsigned long long sync_count() { return g_syncs.load(); }
 void stream_sync(cudaStream_t s)
 {
   g_syncs.fetch_add(1, std::memory_order_relaxed);
+  auto t0 = std::chrono::steady_clock::now();
   CK(cudaStreamSynchronize(s));
+  auto dt = std::chrono::steady_clock::now() - t0;
+  g_sync_ns.fetch_add((unsigned long long)std::chrono::duration_cast<std::chrono::nanoseconds>(
+      dt).count(), std::memory_order_relaxed);
+}
+void host_stats(unsigned long long* allocs, double* sync_seconds)
+{
+  if (allocs) *allocs = g_allocs.load();
+  if (sync_seconds) *sync_seconds = g_sync_ns.load() * 1e-9;
 }
 
 // ---------------------------------------------------------------------------
@@ -210,6 +222,7 @@ void* dev_alloc(size_t bytes, cudaStream_t s)
   setup_pool();
   void* p = nullptr;
   if (bytes < 16) bytes = 16;
+  g_allocs.fetch_add(1, std::memory_order_relaxed);
   cudaError_t e = cudaMallocAsync(&p, bytes, s);
   if (e != cudaSuccess) {
     cudaGetLastError();

@@ -95,6 +95,9 @@ struct ProbeScope {
 // times it waited for the device
 unsigned long long launch_count();
 unsigned long long sync_count();
+// device allocations made so far, and host seconds spent waiting in stream
+// synchronisations
+void host_stats(unsigned long long* allocs, double* sync_seconds);
 void stream_sync(cudaStream_t s);
 // 64 bytes of pinned host memory owned by the calling host thread, for small
 // device-to-host reads (a read into pageable memory is staged by the driver)
