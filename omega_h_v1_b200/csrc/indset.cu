@@ -151,7 +151,10 @@ u32* find_indset(Mesh& m, u32 ent_dim, u32 const* filter, double const* good)
       std::swap(a, b);
       ++rounds;
     }
-    if (!read_u32(flag, m.s)) done = true;
+    // slots 1-3 come back too: a caller that left flags there reads them
+    // after this call without a read-back of its own
+    m.mb->fetch(m.s, 4);
+    if (!m.mb->host[0]) done = true;
   }
   dev_free(b, m.s);
   last_pass_stats().indset_rounds = rounds;

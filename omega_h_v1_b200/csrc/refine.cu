@@ -250,37 +250,15 @@ struct Splits {
   u32 nsplit = 0;
 };
 
-static void refine_build(Mesh& m, u32 const* gen_offs, u32 nsplit)
+// returns the number of split edges (read back with the domain counts)
+static u32 refine_build(Mesh& m, u32 const* gen_offs)
 {
   cudaStream_t s = m.s;
   u32 dim = m.dim, src = 1;
   u32 nv = m.count(0), ns = m.count(src);
   Mesh* out = m.spawn();
-  // refine_verts (refine_common.cpp:29-54)
-  u32 nv_out = nv + nsplit;
-  out->set_ents(0, nv_out, nullptr);
-  u32 const* voe1 = m.ask_down(1, 0);
-  for (auto const& t : m.tags[0]) {
-    if (t.type != T_F64) continue;
-    double* d = dalloc<double>((size_t)nv_out * t.ncomps, s);
-    CK(cudaMemcpyAsync(d, t.data, sizeof(double) * nv * t.ncomps, cudaMemcpyDeviceToDevice, s));
-    if (ns) {
-      k_refine_nodal<<<grid_for(ns), BLOCK, 0, s>>>(ns, nv, voe1, gen_offs, t.ncomps,
-          static_cast<double const*>(t.data), d);
-      CK_LAUNCH();
-    }
-    out->add_tag(0, T_F64, t.name.c_str(), t.ncomps, X_NOT, d);
-  }
-  if (m.parallel) inherit_globals(*out, 0, nv_out);
-  if (m.seg) {
-    out->seg = dalloc<u32>(nv_out, s);
-    CK(cudaMemcpyAsync(out->seg, m.seg, sizeof(u32) * nv, cudaMemcpyDeviceToDevice, s));
-    if (ns) {
-      k_refine_seg<<<grid_for(ns), BLOCK, 0, s>>>(ns, nv, voe1, gen_offs, m.seg, out->seg);
-      CK_LAUNCH();
-    }
-  }
-  // splits_to_domains for every domain dimension
+  // splits_to_domains for every domain dimension; the edges' count is the
+  // number of split edges, so one read-back sizes everything below
   Splits sp[4];
   u32* zero_v = dalloc<u32>((size_t)nv + 1, s);
   fill_u32(zero_v, nv + 1, 0, s);
@@ -305,6 +283,31 @@ static void refine_build(Mesh& m, u32 const* gen_offs, u32 nsplit)
   m.mb->fetch(s, 16);
   for (u32 dd = 1; dd <= dim; ++dd)
     if (m.has_dim(dd)) sp[dd].nsplit = m.mb->host[8 + dd];
+  u32 nsplit = sp[1].nsplit;
+  // refine_verts (refine_common.cpp:29-54)
+  u32 nv_out = nv + nsplit;
+  out->set_ents(0, nv_out, nullptr);
+  u32 const* voe1 = m.ask_down(1, 0);
+  for (auto const& t : m.tags[0]) {
+    if (t.type != T_F64) continue;
+    double* d = dalloc<double>((size_t)nv_out * t.ncomps, s);
+    CK(cudaMemcpyAsync(d, t.data, sizeof(double) * nv * t.ncomps, cudaMemcpyDeviceToDevice, s));
+    if (ns) {
+      k_refine_nodal<<<grid_for(ns), BLOCK, 0, s>>>(ns, nv, voe1, gen_offs, t.ncomps,
+          static_cast<double const*>(t.data), d);
+      CK_LAUNCH();
+    }
+    out->add_tag(0, T_F64, t.name.c_str(), t.ncomps, X_NOT, d);
+  }
+  if (m.parallel) inherit_globals(*out, 0, nv_out);
+  if (m.seg) {
+    out->seg = dalloc<u32>(nv_out, s);
+    CK(cudaMemcpyAsync(out->seg, m.seg, sizeof(u32) * nv, cudaMemcpyDeviceToDevice, s));
+    if (ns) {
+      k_refine_seg<<<grid_for(ns), BLOCK, 0, s>>>(ns, nv, voe1, gen_offs, m.seg, out->seg);
+      CK_LAUNCH();
+    }
+  }
   // products of every dimension (refine_common.cpp:90-123, inherit.cpp:104-138)
   u32* same_of[4] = {nullptr, nullptr, nullptr, nullptr};
   u32 nsame_of[4] = {0, 0, 0, 0};
@@ -385,6 +388,7 @@ static void refine_build(Mesh& m, u32 const* gen_offs, u32 nsplit)
     dev_free(sp[dd].vert, s);
   }
   m.overwrite(out);
+  return nsplit;
 }
 
 // choose_refinement_indset (refine_common.cpp:131-160) on a candidate array
@@ -414,10 +418,15 @@ static u32* choose_refinement(Mesh& m, u32* cand, double qual_floor, double** qu
           m.fp32_filter ? fp32_stats_dev() : nullptr, cand, q, any, inverted);
       CK_LAUNCH();
     }
-    m.mb->fetch(s, 4);
   } else {
     m.mb->host[1] = max_u32(cand, ne, s) ? 1 : 0;
   }
+  // The independent set runs without first reading back "any good
+  // candidate": with none it settles in its first batch of rounds to the
+  // empty set, and its first read-back brings the flags of mailbox slots
+  // 1-3 with it (one host wait fewer per pass).
+  u32* ind = ne ? find_indset(m, 1, cand, q) : nullptr;
+  if (!ne) m.mb->host[1] = m.mb->host[3] = 0;
   // choose_refinement_indset (refine_common.cpp:131-160) ghosts a parallel
   // mesh, and exchanges the edge qualities once any edge is a candidate
   if (m.parallel && !m.seg) {
@@ -425,18 +434,15 @@ static u32* choose_refinement(Mesh& m, u32* cand, double qual_floor, double** qu
     bool any_cand = uniform ? ne > 0 : dim >= 2 ? m.mb->host[3] != 0 : m.mb->host[1] != 0;
     if (any_cand) m.note_exchange(1);
   }
-  if (!m.mb->host[1]) {
-    if (quals_out)
-      *quals_out = q;
-    else
-      dev_free(q, s);
-    return nullptr;
-  }
-  u32* ind = find_indset(m, 1, cand, q);
   if (quals_out)
     *quals_out = q;
   else
     dev_free(q, s);
+  if (!m.mb->host[1]) {
+    dev_free(ind, s);
+    last_pass_stats().indset_rounds = 0;
+    return nullptr;
+  }
   return ind;
 }
 
@@ -453,8 +459,7 @@ static u32 refine_common(Mesh& m, u32* cand, double qual_floor, bool uniform)
   seg_tally(m, 1, ind);
   u32* gen_offs = exscan_new(ind, ne, s);
   dev_free(ind, s);
-  u32 nsplit = read_u32(gen_offs + ne, s);
-  refine_build(m, gen_offs, nsplit);
+  u32 nsplit = refine_build(m, gen_offs);
   dev_free(gen_offs, s);
   st.nselected = nsplit;
   st.elems_out = m.count(m.dim);
