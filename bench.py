@@ -911,6 +911,71 @@ def cpu_reference_run(nsteps_total, ntimed):
             % (len(times), passes.value, elems.value), 1e3 * t / len(times))
 
 
+def gpu_reference_run(nadapts=2):
+    """Times the reference built in its own CUDA loop mode (loop_cuda.hpp
+    and Thrust, compiled for sm_100a from its sources into
+    oracle/_ref/libosh_ref_cuda.so) on the same workload: returns a dict, or
+    None when that build or a GPU is missing."""
+    from oracle import oracle as O
+    so = os.path.join(os.path.dirname(O.__file__), "_ref", "libosh_ref_cuda.so")
+    if not os.path.exists(so):
+        return None
+    try:
+        import torch
+        if not torch.cuda.is_available():
+            return None
+    except Exception:
+        return None
+    L = C.CDLL(so)
+    vp = C.c_void_p
+    if L.refc_ready() != 0:
+        return None
+    L.refc_new_reduced.restype = vp
+    L.refc_new_reduced.argtypes = [C.c_uint, C.c_uint, O._f64p, C.c_uint, O._u32p]
+    L.refc_derive_model_full.argtypes = [vp]
+    L.refc_free.argtypes = [vp]
+    L.refc_add_vertex_field.argtypes = [vp, C.c_char_p, O._f64p]
+    L.refc_adapt.restype = C.c_uint
+    L.refc_adapt.argtypes = [vp, C.c_double, C.c_double, C.c_uint, C.c_uint]
+    L.refc_adapt_counted.restype = C.c_uint
+    L.refc_adapt_counted.argtypes = [vp, C.c_double, C.c_double, C.c_uint, C.c_uint,
+                                     C.POINTER(C.c_uint), C.POINTER(C.c_double)]
+    L.refc_count.restype = C.c_uint
+    L.refc_count.argtypes = [vp, C.c_uint]
+    coords, conn, center = O.box(N_BOX, 0, 0.1)
+    h = O.radial_size(coords, center, H0, H1)
+
+    def fresh():
+        m = L.refc_new_reduced(3, coords.size // 3, coords, conn.size // 4, conn)
+        L.refc_derive_model_full(m)
+        L.refc_add_vertex_field(m, b"adapt_size", h)
+        return m
+
+    m = fresh()
+    passes, elems = C.c_uint(), C.c_double()
+    with _Quiet():
+        L.refc_adapt_counted(m, SIZE_FLOOR, GOOD_QUAL, NLAYERS, MAX_OPS,
+                             C.byref(passes), C.byref(elems))
+    tets_out = L.refc_count(m, 3)
+    L.refc_free(m)
+    times = []
+    for _ in range(nadapts):
+        m = fresh()
+        with _Quiet():
+            t0 = time.perf_counter()
+            L.refc_adapt(m, SIZE_FLOOR, GOOD_QUAL, NLAYERS, MAX_OPS)
+            t1 = time.perf_counter()
+        L.refc_free(m)
+        times.append(t1 - t0)
+    t = float(sum(times))
+    return {"value": round(elems.value * len(times) / t, 1), "unit": UNIT,
+            "ms_per_step": round(1e3 * t / len(times), 1), "tets_out": int(tets_out),
+            "passes": passes.value,
+            "build": "the reference's CUDA loop mode (loop_cuda.hpp, Thrust) compiled for "
+                     "sm_100a from its own sources, NDEBUG",
+            "sample": "%d full mesh_adapt runs of the 48^3 workload on one B200" % len(times)}
+
+
 def run_reference(args, world, rank):
     if rank != 0:
         return None
@@ -928,7 +993,8 @@ def run_reference(args, world, rank):
             "cpu_baseline": {"value": round(value, 1), "unit": UNIT, "cores": cores,
                              "kind": "reference", "sample": sample},
             "e2e": {"value": round(value, 1), "unit": UNIT, "h2d_bytes_per_step": 0,
-                    "d2h_bytes_per_step": 0}}
+                    "d2h_bytes_per_step": 0},
+            "reference_gpu": None if args.no_ref_gpu else gpu_reference_run()}
 
 
 def main():
@@ -943,6 +1009,8 @@ def main():
                     help="DRAM bytes per launch of that kernel from an ncu capture")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling)")
+    ap.add_argument("--no-ref-gpu", action="store_true",
+                    help="reference arm: skip timing the reference's own CUDA build")
     ap.add_argument("--no-fp32", action="store_true",
                     help="skip the single-precision filter leg of the box48 workload")
     ap.add_argument("--workload", default="box48",
