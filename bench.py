@@ -423,6 +423,7 @@ def e2e_leg(G, L, base, args, world, stream, stream_ptr):
 
 BATCH_CHUNK_EST_TETS = 60e6     # estimated output tets per adapt_batch call
 BATCH_UNION_ELEMS = 1000000     # current elements per union inside a call
+CONCURRENT_THREADS = 4   # host threads (streams) of the concurrent leg
 
 
 def reserve_pool(G, fraction=0.5):
@@ -524,6 +525,22 @@ def run_batched(args, world, rank, local):
                 L.osh_free(hs[i])
         return digests, elems, unions, upasses
 
+    def concurrent_leg(hs, chunk_list, nthreads=CONCURRENT_THREADS):
+        digests, elems = {}, 0.0
+        for idx in chunk_list:
+            arr = (C.c_void_p * len(idx))(*[hs[i] for i in idx])
+            rc = L.osh_b200_adapt_concurrent(arr, len(idx), SIZE_FLOOR, GOOD_QUAL, NLAYERS,
+                                             MAX_OPS, nthreads, 0, None, None)
+            if rc:
+                G.check()
+            for k, i in enumerate(idx):
+                p, e = C.c_uint(), C.c_double()
+                L.osh_b200_batch_mesh_stats(k, C.byref(p), C.byref(e))
+                elems += e.value
+                digests[i] = L.osh_b200_digest(hs[i])
+                L.osh_free(hs[i])
+        return digests, elems
+
     # warm-up on the smallest meshes through both paths (untimed)
     warm = chunks[0][:16]
     hs = clones()
@@ -533,6 +550,11 @@ def run_batched(args, world, rank, local):
             L.osh_free(hs[i])
     hs = clones()
     batch_leg(hs, [warm])
+    for i in range(len(hs)):
+        if i not in warm:
+            L.osh_free(hs[i])
+    hs = clones()
+    concurrent_leg(hs, [warm])
     for i in range(len(hs)):
         if i not in warm:
             L.osh_free(hs[i])
@@ -557,6 +579,13 @@ def run_batched(args, world, rank, local):
     torch.cuda.synchronize()
     (bd64, be64, _, _), batch64_ms = timed(lambda: batch_leg(hs, chunks))
     secs64 = dict(batch_secs)
+    # concurrent streams, double and with the filter
+    hs = clones()
+    torch.cuda.synchronize()
+    (cd64, ce64), conc64_ms = timed(lambda: concurrent_leg(hs, chunks))
+    hs = clones(fp32=True)
+    torch.cuda.synchronize()
+    (cd32, ce32), conc32_ms = timed(lambda: concurrent_leg(hs, chunks))
     # the batched path with the single-precision filter (double recheck)
     hs = clones(fp32=True)
     torch.cuda.synchronize()
@@ -568,6 +597,7 @@ def run_batched(args, world, rank, local):
     clk = clocks.stop()
     fs = G.fp32_stats()
     same = all(pd[i] == bd[i] == bd64[i] for i in range(len(jobs)))
+    same_conc = all(pd[i] == cd64[i] == cd32[i] for i in range(len(jobs)))
     for b in bases:
         b.close()
     value = be / (batch_ms / 1e3)
@@ -591,6 +621,17 @@ def run_batched(args, world, rank, local):
                   "path": "one mesh_adapt per mesh, double"},
         "batched_fp64": {"value": round(be64 / (batch64_ms / 1e3), 1),
                          "ms": round(batch64_ms, 3), "union_secs": secs64},
+        "concurrent_fp64": {"value": round(ce64 / (conc64_ms / 1e3), 1),
+                            "ms": round(conc64_ms, 3), "threads": CONCURRENT_THREADS,
+                            "speedup_vs_plain": round(plain_ms / conc64_ms, 3),
+                            "path": "osh_b200_adapt_concurrent: unchanged mesh_adapt per "
+                                    "mesh, host threads on streams of their own"},
+        "concurrent_fp32": {"value": round(ce32 / (conc32_ms / 1e3), 1),
+                            "ms": round(conc32_ms, 3), "threads": CONCURRENT_THREADS,
+                            "speedup_vs_plain": round(plain_ms / conc32_ms, 3),
+                            "path": "concurrent streams with the single-precision filter"},
+        "identical_concurrent": bool(same_conc and abs(pe - ce64) < 0.5
+                                     and abs(pe - ce32) < 0.5),
         "speedup_vs_plain": round(plain_ms / batch_ms, 3),
         "identical_to_plain": bool(same and abs(pe - be) < 0.5 and abs(pe - be64) < 0.5),
         "fp32": {"decided_single": fs["decided"], "rechecked_double": fs["rechecked"],

@@ -71,6 +71,19 @@ void osh_b200_last_pass(unsigned* op, unsigned* elems_in, unsigned* elems_out,
 int osh_b200_adapt_batch(osh_t* meshes, unsigned nmeshes, double size_ratio_floor,
     double good_qual, unsigned nsliver_layers, unsigned max_passes,
     unsigned long long max_union_elems, unsigned* changed, int* status) OSH_PUBLIC;
+/* No single counterpart in the reference: mesh_adapt (adapt.cpp:82-94) of
+   every mesh, unchanged, by nthreads host threads (0 = 4) each issuing on a
+   CUDA stream of its own, so that the passes of different meshes overlap on
+   the device (one mesh's host read-backs and launch gaps are filled by
+   another's kernels). Meshes start largest first while the device-memory
+   estimates of the meshes in flight fit budget_bytes (0 = 70% of the free
+   device memory; a mesh larger than the budget runs alone). Each mesh ends
+   exactly as osh_adapt leaves it, on the stream it had. changed / status as
+   for osh_b200_adapt_batch; per-mesh statistics through
+   osh_b200_batch_mesh_stats. Meshes need not share dimension or tags. */
+int osh_b200_adapt_concurrent(osh_t* meshes, unsigned nmeshes, double size_ratio_floor,
+    double good_qual, unsigned nsliver_layers, unsigned max_passes, unsigned nthreads,
+    unsigned long long budget_bytes, unsigned* changed, int* status) OSH_PUBLIC;
 /* statistics of the last osh_b200_adapt_batch on this thread: unions,
    scheduling steps, passes over whole unions, passes that changed a mesh
    (summed over meshes) and the elements entering those passes */

@@ -133,6 +133,8 @@ def lib():
     f("osh_b200_adapt_stats", None, C.POINTER(C.c_uint), C.POINTER(C.c_double))
     f("osh_b200_adapt_batch", C.c_int, C.POINTER(vp), C.c_uint, C.c_double, C.c_double,
       C.c_uint, C.c_uint, C.c_ulonglong, C.POINTER(C.c_uint), C.POINTER(C.c_int))
+    f("osh_b200_adapt_concurrent", C.c_int, C.POINTER(vp), C.c_uint, C.c_double, C.c_double,
+      C.c_uint, C.c_uint, C.c_uint, C.c_ulonglong, C.POINTER(C.c_uint), C.POINTER(C.c_int))
     f("osh_b200_batch_stats", None, *([C.POINTER(C.c_uint)] * 4), C.POINTER(C.c_double))
     f("osh_b200_batch_mesh_stats", None, C.c_uint, C.POINTER(C.c_uint), C.POINTER(C.c_double))
     f("osh_b200_batch_times", None, *([C.POINTER(C.c_double)] * 3))
@@ -567,6 +569,30 @@ def adapt_batch(meshes, size_floor, good_qual, nlayers, max_ops, max_union_elems
     stats = dict(unions=u.value, steps=st.value, union_passes=up.value,
                  mesh_passes=mp.value, elems_in=e.value, per_mesh=per)
     return list(changed[:n]), list(status[:n]), stats
+
+
+def adapt_concurrent(meshes, size_floor, good_qual, nlayers, max_ops, nthreads=0,
+                     budget_bytes=0):
+    """mesh_adapt of every mesh, unchanged, by ``nthreads`` host threads on
+    streams of their own (0 = 4), largest first within a device-memory
+    budget (0 = 70% of free memory). Returns (changed, status) per mesh and
+    the per-mesh (passes, elements in)."""
+    L = lib()
+    n = len(meshes)
+    hs = (C.c_void_p * max(n, 1))(*[m.h for m in meshes])
+    changed = (C.c_uint * max(n, 1))()
+    status = (C.c_int * max(n, 1))()
+    rc = L.osh_b200_adapt_concurrent(hs, n, size_floor, good_qual, nlayers, max_ops,
+                                     nthreads, budget_bytes, changed, status)
+    if rc:
+        check()
+        raise OshError(rc, "osh_b200_adapt_concurrent failed")
+    per = []
+    for i in range(n):
+        p, ei = C.c_uint(), C.c_double()
+        L.osh_b200_batch_mesh_stats(i, C.byref(p), C.byref(ei))
+        per.append((p.value, ei.value))
+    return list(changed[:n]), list(status[:n]), per
 
 
 class Server:

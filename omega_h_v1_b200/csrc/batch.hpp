@@ -131,4 +131,11 @@ void adapt_batch(std::vector<Mesh*> const& ms, double size_floor, double good_qu
     u32 nlayers, u32 max_ops, unsigned long long max_union_elems,
     std::vector<BatchMeshResult>& res);
 
+// mesh_adapt of every mesh, unchanged, by `nthreads` host threads (0 = 4)
+// each issuing on a stream of its own; meshes start largest first while the
+// device-memory estimates of those in flight fit `budget` bytes (0 = 70% of
+// the device's free memory); each mesh ends exactly as osh_adapt leaves it
+void adapt_concurrent(std::vector<Mesh*> const& ms, AdaptParams const& ap, u32 nthreads,
+    unsigned long long budget, std::vector<BatchMeshResult>& res);
+
 }  // namespace osh

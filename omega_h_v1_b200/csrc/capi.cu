@@ -551,6 +551,30 @@ int osh_b200_adapt_batch(osh_t* meshes, unsigned n, double sf, double gq, unsign
   API_CATCH(osh::last_error())
 }
 
+int osh_b200_adapt_concurrent(osh_t* meshes, unsigned n, double sf, double gq, unsigned nl,
+    unsigned mo, unsigned nthreads, unsigned long long budget_bytes, unsigned* changed,
+    int* status)
+{
+  API_TRY
+  need(meshes != nullptr || n == 0, "meshes is NULL");
+  std::vector<Mesh*> ms(n);
+  for (unsigned i = 0; i < n; ++i) {
+    need(meshes[i] != nullptr, "a mesh handle is NULL");
+    ms[i] = M(meshes[i]);
+    for (unsigned j = 0; j < i; ++j) need(ms[j] != ms[i], "a mesh appears twice");
+  }
+  t_batch_res.clear();
+  osh::AdaptParams ap{sf, gq, nl, mo};
+  osh::adapt_concurrent(ms, ap, nthreads, budget_bytes, t_batch_res);
+  for (unsigned i = 0; i < n; ++i) {
+    if (changed) changed[i] = t_batch_res[i].changed;
+    if (status) status[i] = t_batch_res[i].status;
+    sync(ms[i]);
+  }
+  return 0;
+  API_CATCH(osh::last_error())
+}
+
 #define SV(h) reinterpret_cast<osh::Server*>(h)
 
 osh_b200_server_t osh_b200_server_new(double sf, double gq, unsigned nl, unsigned mo,
