@@ -1,0 +1,42 @@
+"""Records the SHA-256 of every VTU step the reference's 2D warp test
+(test_warp.cpp) writes, run through the reference's own library
+(oracle/_ref, oracle/Makefile) with tests/warp2d_flow.py:
+`python tests/golden/make_warp2d_golden.py`. The GPU test compares this
+library's files with these digests (and with a live reference run where
+oracle/_ref is present)."""
+import hashlib
+import json
+import os
+import sys
+import tempfile
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "tests"))
+sys.path.insert(0, HERE)
+
+import warp2d_flow as W  # noqa: E402
+from make_golden import Quiet  # noqa: E402
+from oracle import oracle as O  # noqa: E402
+
+
+def quiet(f, *a):
+    with Quiet():
+        return f(*a)
+
+
+def main():
+    m = O.ReferenceVariant(2, W.BOX_2D_COORDS, W.BOX_2D_CONN, "serial")
+    m.derive_model_full()
+    with tempfile.TemporaryDirectory() as d:
+        files = W.run(m, d, adapt=quiet)
+        out = {os.path.basename(f): hashlib.sha256(open(f, "rb").read()).hexdigest()
+               for f in files}
+    json.dump(out, open(os.path.join(HERE, "warp2d_sha256.json"), "w"), indent=1,
+              sort_keys=True)
+    print(len(out), "steps")
+
+
+if __name__ == "__main__":
+    main()

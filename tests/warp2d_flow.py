@@ -1,0 +1,128 @@
+"""The reference's 2D warp test (test_warp.cpp:23-153) as one flow that runs
+on either library: the reference driven through oracle/ref_driver.cpp, or
+this library on the GPU. Both expose the same mesh methods, so the same
+calls produce the VTU steps the reference's test writes (warp_0000.vtu,
+...), and the two sets of files can be compared byte for byte, as the
+reference's own run_tests.sh compares warp_0008.vtu with its gold copy.
+
+Vertex fields are evaluated on the host with Python's math module, which
+calls the same C library functions (atan2, cos, sin, sqrt) as the
+reference's eval_field, in the reference's operation order."""
+import math
+import os
+
+import numpy as np
+
+PI = 3.14159265359                    # algebra.hpp:8
+WARP_QUAL_FLOOR = 0.1                 # test_warp.cpp:20-24
+GOOD_QUAL_FLOOR = 0.4
+SIZE_FLOOR = 1. / 3.
+NSLIVER_LAYERS = 0
+MAX_OPS = 50
+
+BOX_2D_COORDS = np.array([0, 0, 0, 1, 0, 0, 1, 1, 0, 0, 1, 0], np.float64)  # tables.cpp:22-27
+BOX_2D_CONN = np.array([0, 1, 2, 2, 3, 0], np.uint32)                      # tables.cpp:17-20
+X_NOT = 0
+
+
+def _norm3(x):
+    d = 0.0
+    for k in range(3):
+        d += x[k] * x[k]
+    return math.sqrt(d)
+
+
+def dye_fun(c):
+    """test_warp.cpp:53-70"""
+    l, r = (.25, .5, 0.0), (.75, .5, 0.0)
+    d = 1.0
+    x = [c[k] - l[k] for k in range(3)]
+    if _norm3(x) > .25:
+        d = -1.0
+        x = [c[k] - r[k] for k in range(3)]
+    if _norm3(x) > .25:
+        return [0.0]
+    return [4 * d * (.25 - _norm3(x))]
+
+
+def warp_fun(c, rotation):
+    """test_warp.cpp:34-51"""
+    mid = (.5, .5, 0.0)
+    x = [c[k] - mid[k] for k in range(3)]
+    polar_a = math.atan2(x[1], x[0])
+    polar_r = _norm3(x)
+    rot_a = 0.0
+    if polar_r < .5:
+        rot_a = rotation * (2 * (.5 - polar_r))
+    dest_a = polar_a + rot_a
+    dst = [math.cos(dest_a) * polar_r, math.sin(dest_a) * polar_r, 0.0]
+    return [dst[k] - x[k] for k in range(3)]
+
+
+def _coords(m):
+    for t in m.tags(0):
+        if t.name == "coordinates":
+            return t.data.reshape(-1, 3)
+    raise KeyError("coordinates")
+
+
+def eval_field(m, name, ncomps, fun):
+    """mesh_eval_field (eval_field.cpp:34-40): fun at every vertex"""
+    x = _coords(m)
+    out = np.empty((x.shape[0], ncomps), np.float64)
+    for i in range(x.shape[0]):
+        out[i] = fun([float(x[i, 0]), float(x[i, 1]), float(x[i, 2])])
+    m.add_field(0, name, out.ravel(), ncomps, X_NOT)
+
+
+def set_size_field(m):
+    """test_warp.cpp:72-85"""
+    dim = 2
+    m.free_tag(0, "adapt_size")
+    m.element_gradients("dye")
+    m.recover_by_volume("grad_dye")
+    m.free_tag(dim, "grad_dye")
+    m.element_gradients("grad_dye")
+    m.free_tag(0, "grad_dye")
+    m.recover_by_volume("grad_grad_dye")
+    m.free_tag(dim, "grad_grad_dye")
+    m.size_from_hessian("grad_grad_dye", [0.075 / 100.0], 0.025, 0.1)
+    m.free_tag(0, "grad_grad_dye")
+
+
+def run(m, outdir, adapt=None):
+    """main() and warped_adapt() of test_warp.cpp on mesh m (the 2D box,
+    already made full and classified); writes outdir/warp_%04u.vtu as
+    write_vtk_step does and returns the file names. `adapt` wraps calls that
+    print (the reference's passes)."""
+    call = adapt or (lambda f, *a: f(*a))
+    files = []
+
+    def step():
+        name = os.path.join(outdir, "warp_%04u.vtu" % len(files))
+        m.write_vtk(name)
+        files.append(name)
+
+    eval_field(m, "adapt_size", 1, lambda c: [0.1])
+    while call(m.refine_by_size, 0.0):
+        pass
+    eval_field(m, "dye", 1, dye_fun)
+    set_size_field(m)
+    step()
+    call(m.adapt, SIZE_FLOOR, GOOD_QUAL_FLOOR, NSLIVER_LAYERS, MAX_OPS)
+    rotation = PI / 4.
+    for _ in range(2):
+        for _ in range(4):
+            eval_field(m, "warp", 3, lambda c: warp_fun(c, rotation))
+            for it in range(3):
+                done = m.warp_to_limit(WARP_QUAL_FLOOR)
+                set_size_field(m)
+                step()
+                call(m.adapt, SIZE_FLOOR, GOOD_QUAL_FLOOR, NSLIVER_LAYERS, MAX_OPS)
+                if done:
+                    break
+            else:
+                raise RuntimeError("warped_adapt still not done after 3 iters")
+            m.free_tag(0, "warp")
+        rotation = -rotation
+    return files
