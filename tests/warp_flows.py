@@ -1,4 +1,5 @@
-"""The reference's 2D warp test (test_warp.cpp:23-153) as one flow that runs
+"""The reference's 2D and 3D warp tests (test_warp.cpp, test_warp_3d.cpp) as
+flows that run
 on either library: the reference driven through oracle/ref_driver.cpp, or
 this library on the GPU. Both expose the same mesh methods, so the same
 calls produce the VTU steps the reference's test writes (warp_0000.vtu,
@@ -123,6 +124,93 @@ def run(m, outdir, adapt=None):
                     break
             else:
                 raise RuntimeError("warped_adapt still not done after 3 iters")
+            m.free_tag(0, "warp")
+        rotation = -rotation
+    return files
+
+
+# ---------------------------------------------------------------------------
+# test_warp_3d.cpp
+
+BOX_3D_COORDS = np.array([0, 0, 0, 1, 0, 0, 1, 1, 0, 0, 1, 0,
+                          0, 0, 1, 1, 0, 1, 1, 1, 1, 0, 1, 1], np.float64)  # tables.cpp:38-47
+BOX_3D_CONN = np.array([0, 1, 2, 6, 2, 3, 0, 6, 0, 3, 7, 6,
+                        7, 4, 0, 6, 0, 4, 5, 6, 5, 1, 0, 6], np.uint32)     # tables.cpp:29-36
+X_CONSERVE, X_POINTWISE = 2, 1
+
+
+def dye_fun_3d(c):
+    """test_warp_3d.cpp:57-74"""
+    l, r = (.25, .5, .5), (.75, .5, .5)
+    d = 1.0
+    x = [c[k] - l[k] for k in range(3)]
+    if _norm3(x) > .25:
+        d = -1.0
+        x = [c[k] - r[k] for k in range(3)]
+    if _norm3(x) > .25:
+        return [0.0]
+    return [4 * d * (.25 - _norm3(x))]
+
+
+def warp_fun_3d(c, rotation):
+    """test_warp_3d.cpp:36-55 (rotation about the z axis)"""
+    mid = (.5, .5, 0.0)
+    x = [c[k] - mid[k] for k in range(3)]
+    x[2] = 0.0
+    polar_a = math.atan2(x[1], x[0])
+    polar_r = _norm3(x)
+    rot_a = 0.0
+    if polar_r < .5:
+        rot_a = rotation * (2 * (.5 - polar_r))
+    dest_a = polar_a + rot_a
+    dst = [math.cos(dest_a) * polar_r, math.sin(dest_a) * polar_r, 0.0]
+    return [dst[k] - x[k] for k in range(3)]
+
+
+def element_centroids(m):
+    """mesh_interp_to_elems of the coordinates (element_field.cpp:9-44):
+    the vertices' sum in element order, divided by the vertex count"""
+    x = _coords(m)
+    c = m.down(3, 0).reshape(-1, 4)
+    s = np.zeros((c.shape[0], 3))
+    for j in range(4):
+        s = s + x[c[:, j]]
+    return s / 4
+
+
+def run3d(m, outdir, adapt=None):
+    """main() and warped_adapt() of test_warp_3d.cpp on the 3D box (already
+    full and classified); returns the VTU steps written."""
+    call = adapt or (lambda f, *a: f(*a))
+    files = []
+
+    def step():
+        name = os.path.join(outdir, "warp_%04u.vtu" % len(files))
+        m.write_vtk(name)
+        files.append(name)
+
+    eval_field(m, "adapt_size", 1, lambda c: [0.2])
+    while call(m.refine_by_size, 0.0):
+        pass
+    eval_field(m, "dye", 1, dye_fun_3d)
+    ec = element_centroids(m)
+    nel = ec.shape[0]
+    mass = np.where(ec[:, 0] > 0.5, 1.0 / nel, 0.0)
+    m.add_field(3, "mass", mass, 1, X_CONSERVE)
+    m.add_field(3, "pointwise", ec.ravel().copy(), 3, X_POINTWISE)
+    step()
+    rotation = PI / 4
+    for _ in range(2):
+        for _ in range(4):
+            eval_field(m, "warp", 3, lambda c: warp_fun_3d(c, rotation))
+            for it in range(6):
+                done = m.warp_to_limit(0.2)
+                call(m.adapt, 1. / 3., 0.3, 4, 50)
+                step()
+                if done:
+                    break
+            else:
+                raise RuntimeError("warped_adapt still not done after 6 iters")
             m.free_tag(0, "warp")
         rotation = -rotation
     return files
