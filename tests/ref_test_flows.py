@@ -214,3 +214,107 @@ def run3d(m, outdir, adapt=None):
             m.free_tag(0, "warp")
         rotation = -rotation
     return files
+
+
+# ---------------------------------------------------------------------------
+# test_refine_by_size.cpp, test_coarsen_by_size.cpp, test_box.cpp, test_grad.cpp
+
+def _radial_size(fine):
+    """size_fun of test_refine_by_size.cpp:13-20 / fine_fun of
+    test_coarsen_by_size.cpp:15-22"""
+    def f(c):
+        coarse = 0.5
+        radius = _norm3(c)
+        d = abs(radius - 0.5)
+        return [coarse * d + fine * (1 - d)]
+    return f
+
+
+def _write(m, outdir, name, files):
+    p = os.path.join(outdir, name)
+    m.write_vtk(p)
+    files.append(p)
+
+
+def run_refine_by_size(m, outdir, adapt=None):
+    """test_refine_by_size.cpp on the 2D box (full, classified)"""
+    call = adapt or (lambda f, *a: f(*a))
+    files = []
+    size = _radial_size(0.1)
+    eval_field(m, "adapt_size", 1, size)
+    nel = m.count(2)
+    m.add_field(2, "mass", np.full(nel, 1.0 / nel), 1, X_NOT)
+    _write(m, outdir, "out_0.vtu", files)
+    it = 1
+    while call(m.refine_by_size, 0.0):
+        _write(m, outdir, "out_%u.vtu" % it, files)
+        it += 1
+        m.free_tag(0, "adapt_size")
+        eval_field(m, "adapt_size", 1, size)
+    return files
+
+
+def run_coarsen_by_size(m, outdir, adapt=None):
+    """test_coarsen_by_size.cpp on the 2D box (full, classified)"""
+    call = adapt or (lambda f, *a: f(*a))
+    files = []
+    fine = _radial_size(0.2)
+    eval_field(m, "adapt_size", 1, fine)
+    nel = m.count(2)
+    m.add_field(2, "mass", np.full(nel, 1.0 / nel), 1, X_NOT)
+    it = 0
+    while call(m.refine_by_size, 0.0):
+        _write(m, outdir, "ref_%u.vtu" % it, files)
+        it += 1
+        m.free_tag(0, "adapt_size")
+        eval_field(m, "adapt_size", 1, fine)
+    m.free_tag(0, "adapt_size")
+    eval_field(m, "adapt_size", 1, lambda c: [4.0])
+    it = 0
+    while call(m.coarsen_by_size, 0.1, 0.5):
+        _write(m, outdir, "cor_%u.vtu" % it, files)
+        it += 1
+    return files
+
+
+def run_box(m, outdir, nrefs, adapt=None):
+    """test_box.cpp: uniformly_refine nrefs times, write box.vtu"""
+    call = adapt or (lambda f, *a: f(*a))
+    for _ in range(nrefs):
+        call(m.uniformly_refine)
+    files = []
+    _write(m, outdir, "box.vtu", files)
+    return files
+
+
+def run_grad(m, outdir, adapt=None):
+    """test_grad.cpp on the 3D box (reduced, unclassified)"""
+    call = adapt or (lambda f, *a: f(*a))
+    eval_field(m, "adapt_size", 1, lambda c: [0.1])
+    while call(m.refine_by_size, 0.0):
+        pass
+    eval_field(m, "dye", 1, dye_fun_3d)
+    m.element_gradients("dye")
+    m.recover_by_volume("grad_dye")
+    m.element_gradients("grad_dye")
+    m.recover_by_volume("grad_grad_dye")
+    m.free_tag(0, "adapt_size")
+    m.size_from_hessian("grad_grad_dye", [0.05 / 75.0], 0.05, 0.1)
+    files = []
+    _write(m, outdir, "grad.vtu", files)
+    return files
+
+
+# name -> (dim, flow, box coordinates, box connectivity, classified full mesh)
+CASES = {
+    "warp_2d": (2, run, BOX_2D_COORDS, BOX_2D_CONN, True),
+    "warp_3d": (3, run3d, BOX_3D_COORDS, BOX_3D_CONN, True),
+    "refine_by_size_2d": (2, run_refine_by_size, BOX_2D_COORDS, BOX_2D_CONN, True),
+    "coarsen_by_size_2d": (2, run_coarsen_by_size, BOX_2D_COORDS, BOX_2D_CONN, True),
+    # run_tests.sh: box.exe --dim 2 --refinements 6
+    "box_2d_6": (2, lambda m, d, adapt=None: run_box(m, d, 6, adapt), BOX_2D_COORDS,
+                 BOX_2D_CONN, True),
+    "box_3d_3": (3, lambda m, d, adapt=None: run_box(m, d, 3, adapt), BOX_3D_COORDS,
+                 BOX_3D_CONN, True),
+    "grad_3d": (3, run_grad, BOX_3D_COORDS, BOX_3D_CONN, False),
+}
