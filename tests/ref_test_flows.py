@@ -305,6 +305,51 @@ def run_grad(m, outdir, adapt=None):
     return files
 
 
+# ---------------------------------------------------------------------------
+# test_one_refine.cpp, test_one_coarsen.cpp on a parallel mesh read from a
+# .pvtu, as run_tests.sh chains them (split -> one_ref -> two_ref, split ->
+# one_cor -> two_cor), on one rank
+
+def _read_like(m, path):
+    """read_mesh_vtk in the library m belongs to"""
+    if type(m).__name__ == "CpuMesh":
+        from oracle import oracle as O
+        return O.CpuMesh.adopt(m.L, m.L.read_vtk(os.fsencode(path)))
+    return type(m).read_vtk(path)
+
+
+def _pvtu_files(outdir, stem):
+    return [os.path.join(outdir, stem + ".pvtu"), os.path.join(outdir, stem + ".vtu")]
+
+
+def run_one_ops(m, outdir, adapt=None):
+    """the 2D box refined uniformly three times and made parallel is the
+    split mesh; then one_refine twice and one_coarsen twice from it"""
+    call = adapt or (lambda f, *a: f(*a))
+    for _ in range(3):
+        call(m.uniformly_refine)
+    m.make_parallel()
+    m.write_vtk(os.path.join(outdir, "split.pvtu"))
+    files = _pvtu_files(outdir, "split")
+    src = "split"
+    for stem in ("one_ref", "two_ref"):
+        r = _read_like(m, os.path.join(outdir, src + ".pvtu"))
+        call(r.uniformly_refine)
+        r.write_vtk(os.path.join(outdir, stem + ".pvtu"))
+        files += _pvtu_files(outdir, stem)
+        src = stem
+    src = "split"
+    for stem in ("one_cor", "two_cor"):
+        c = _read_like(m, os.path.join(outdir, src + ".pvtu"))
+        c.add_field(0, "adapt_size", np.full(c.count(0), 2.0), 1, X_NOT)
+        call(c.coarsen_by_size, 0.1, 0.7)
+        c.free_tag(0, "adapt_size")
+        c.write_vtk(os.path.join(outdir, stem + ".pvtu"))
+        files += _pvtu_files(outdir, stem)
+        src = stem
+    return files
+
+
 # name -> (dim, flow, box coordinates, box connectivity, classified full mesh)
 CASES = {
     "warp_2d": (2, run, BOX_2D_COORDS, BOX_2D_CONN, True),
@@ -317,4 +362,5 @@ CASES = {
     "box_3d_3": (3, lambda m, d, adapt=None: run_box(m, d, 3, adapt), BOX_3D_COORDS,
                  BOX_3D_CONN, True),
     "grad_3d": (3, run_grad, BOX_3D_COORDS, BOX_3D_CONN, False),
+    "one_ops_pvtu_2d": (2, run_one_ops, BOX_2D_COORDS, BOX_2D_CONN, True),
 }

@@ -4,7 +4,9 @@ test_warp_3d.cpp (3D: conserved and pointwise element fields, warps with
 sliver layers), test_refine_by_size.cpp and test_coarsen_by_size.cpp (2D,
 radial size fields), test_box.cpp (uniform refinement, the arguments of
 run_tests.sh) and test_grad.cpp (3D unclassified mesh, gradient recovery,
-size from Hessian). Every VTU file a flow writes must equal, byte for byte,
+size from Hessian), test_one_refine.cpp and test_one_coarsen.cpp (a
+parallel mesh through .pvtu files). Every VTU file a flow writes must
+equal, byte for byte,
 the file the reference writes on the same calls (the reference's own
 run_tests.sh diffs warp_0008.vtu against a gold copy): against digests
 recorded from the reference (tests/golden/make_ref_test_golden.py), and
