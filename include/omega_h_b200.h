@@ -150,6 +150,11 @@ void osh_b200_pool_stats(unsigned long long* reserved, unsigned long long* used,
    (the reference's USE_ZLIB build). osh_read_vtk reads all three. */
 void osh_b200_write_vtk_opts(osh_t m, char const* filename, int ascii, int compress) OSH_PUBLIC;
 
+/* mesh_has_dim (mesh.cpp:295-298): whether the mesh holds entities of
+   dimension dim (vertices always; others once set or derived), without
+   deriving them */
+unsigned osh_b200_has_dim(osh_t m, unsigned dim) OSH_PUBLIC;
+
 /* order-sensitive 64-bit digest of a mesh (connectivity of every dimension,
    tag names, kinds and data, global numbers), computed on the device; equal
    meshes give equal digests. No counterpart in the reference. */

@@ -139,6 +139,7 @@ def lib():
     f("osh_b200_batch_mesh_stats", None, C.c_uint, C.POINTER(C.c_uint), C.POINTER(C.c_double))
     f("osh_b200_batch_times", None, *([C.POINTER(C.c_double)] * 3))
     f("osh_b200_digest", C.c_ulonglong, vp)
+    f("osh_b200_has_dim", C.c_uint, vp, C.c_uint)
     f("osh_ghost", None, vp, C.c_uint)
     f("osh_num_ghost_layers", C.c_uint, vp)
     f("osh_read_vtk", vp, C.c_char_p)
@@ -322,6 +323,10 @@ class Mesh:
         else:
             self.L.osh_write_vtk(self.h, os.fsencode(path))
         self._chk()
+
+    def has_dim(self, dim):
+        """mesh_has_dim: entities of dimension dim are held (not derived)"""
+        return bool(self._chk(self.L.osh_b200_has_dim(self.h, dim)))
 
     def digest(self):
         """Order-sensitive 64-bit hash of every array of the mesh (device)."""

@@ -789,6 +789,15 @@ void osh_b200_write_vtk_opts(osh_t h, char const* filename, int ascii, int compr
   API_CATCH_VOID
 }
 
+unsigned osh_b200_has_dim(osh_t h, unsigned dim)
+{
+  API_TRY
+  need(h != nullptr, "mesh is NULL");
+  Mesh* m = M(h);
+  return dim <= m->dim && m->has_dim(dim) ? 1u : 0u;
+  API_CATCH(0)
+}
+
 unsigned long long osh_b200_digest(osh_t h)
 {
   API_TRY

@@ -752,10 +752,13 @@ static void coarsen_build(Mesh& m, CoarsenSel const& sel)
     for (u32 l = 1; l < h; ++l)
       if (same_of[h] && same_of[l])
         carry_down(m, *out, h, l, same_of[h], nsame_of[h], same_of[l]);
-  for (u32 h = 1; h <= dim; ++h)
+  for (u32 h = 1; h <= dim; ++h) {
+    u32* newid = nullptr;
     for (u32 l = 0; l < h; ++l)
       if (same_of[h] && same_of[l])
-        carry_up(m, *out, l, h, same_of[l], same_of[h], nsame_of[h]);
+        carry_up(m, *out, l, h, same_of[l], same_of[h], nsame_of[h], &newid);
+    dev_free(newid, s);
+  }
   for (u32 d = 0; d < 4; ++d) {
     dev_free(fused[d], s);
     dev_free(same_of[d], s);

@@ -1089,8 +1089,18 @@ __global__ void k_up_gen_fill(u32 first, u32 nuses, u32 lph, u32 const* __restri
   dirs[slot] = u % lph;
 }
 
+u32* carry_new_ids(u32 const* same, u32 n, cudaStream_t s)
+{
+  u32* newid = dalloc<u32>(n ? n : 1, s);
+  if (n) {
+    k_new_ids<<<grid_for(n), BLOCK, 0, s>>>(n, same, newid);
+    CK_LAUNCH();
+  }
+  return newid;
+}
+
 void carry_up(Mesh& m, Mesh& out, u32 low, u32 high, u32 const* same_l, u32 const* same_h,
-    u32 nsame_h)
+    u32 nsame_h, u32** newid_cache)
 {
   if (!m.have_up[low][high] || out.have_up[low][high]) return;
   if (!out.has_dim(high) || !out.has_dim(low)) return;
@@ -1101,10 +1111,19 @@ void carry_up(Mesh& m, Mesh& out, u32 low, u32 high, u32 const* same_l, u32 cons
   u32 const* loh = out.ask_down(high, low);
   UpAdj const& old = m.up[low][high];
   u32 nh_old = m.counts[high];
-  u32* newid_h = dalloc<u32>(nh_old ? nh_old : 1, s);
-  if (nh_old) {
-    k_new_ids<<<grid_for(nh_old), BLOCK, 0, s>>>(nh_old, same_h, newid_h);
-    CK_LAUNCH();
+  // each old high entity's new id (INV when it did not survive), shared by
+  // the carries of one high dimension through *newid_cache
+  u32* own_newid = nullptr;
+  u32 const* newid_h;
+  if (newid_cache && *newid_cache) {
+    newid_h = *newid_cache;
+  } else {
+    own_newid = carry_new_ids(same_h, nh_old, s);
+    newid_h = own_newid;
+    if (newid_cache) {
+      *newid_cache = own_newid;
+      own_newid = nullptr;
+    }
   }
   u32* cnt = dalloc<u32>((size_t)nl + 1, s);
   u32* surv = dalloc<u32>((size_t)nl + 1, s);
@@ -1143,7 +1162,7 @@ void carry_up(Mesh& m, Mesh& out, u32 low, u32 high, u32 const* same_l, u32 cons
     CK_LAUNCH();
   }
   dev_free(cnt, s);
-  dev_free(newid_h, s);
+  dev_free(own_newid, s);
   if (m.up_sorted[low][high]) {
     u.pre = surv;
     u.npre = first;

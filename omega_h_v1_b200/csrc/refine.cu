@@ -377,10 +377,13 @@ static u32 refine_build(Mesh& m, u32 const* gen_offs)
     for (u32 l = 1; l < h; ++l)
       if (same_of[h] && same_of[l])
         carry_down(m, *out, h, l, same_of[h], nsame_of[h], same_of[l]);
-  for (u32 h = 1; h <= dim; ++h)
+  for (u32 h = 1; h <= dim; ++h) {
+    u32* newid = nullptr;
     for (u32 l = 0; l < h; ++l)
       if (same_of[h] && same_of[l])
-        carry_up(m, *out, l, h, same_of[l], same_of[h], nsame_of[h]);
+        carry_up(m, *out, l, h, same_of[l], same_of[h], nsame_of[h], &newid);
+    dev_free(newid, s);
+  }
   for (u32 dd = 0; dd <= dim; ++dd) {
     dev_free(same_of[dd], s);
     dev_free(sp[dd].offs, s);
