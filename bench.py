@@ -230,13 +230,18 @@ def e2e_step(G, L, inp, stream_ptr):
     L.osh_b200_adapt_stats(C.byref(passes), C.byref(elems))
     nt = L.osh_count(m, 3)
     nvo = L.osh_count(m, 0)
-    out_conn = np.empty(nt * 4, np.uint32)
-    out_x = np.empty(nvo * 3, np.float64)
-    L.osh_b200_copy_to_host(out_conn.ctypes.data_as(C.c_void_p), L.osh_down(m, 3, 0),
-                            out_conn.nbytes)
-    L.osh_b200_copy_to_host(out_x.ctypes.data_as(C.c_void_p), L.osh_coords(m), out_x.nbytes)
+    # the result read into pinned host buffers (grown when a step needs more)
+    import torch
+    if inp.get("out_conn") is None or inp["out_conn"].numel() < nt * 4:
+        inp["out_conn"] = torch.empty(nt * 4, dtype=torch.int32, pin_memory=True)
+    if inp.get("out_x") is None or inp["out_x"].numel() < nvo * 3:
+        inp["out_x"] = torch.empty(nvo * 3, dtype=torch.float64, pin_memory=True)
+    L.osh_b200_copy_to_host(C.c_void_p(inp["out_conn"].data_ptr()), L.osh_down(m, 3, 0),
+                            nt * 4 * 4)
+    L.osh_b200_copy_to_host(C.c_void_p(inp["out_x"].data_ptr()), L.osh_coords(m),
+                            nvo * 3 * 8)
     G.check()
-    d2h = out_conn.nbytes + out_x.nbytes
+    d2h = nt * 4 * 4 + nvo * 3 * 8
     L.osh_free(m)
     return elems.value, h2d, d2h
 
