@@ -151,8 +151,10 @@ void adapt_concurrent(std::vector<Mesh*> const& ms, AdaptParams const& ap, u32 n
         inflight += est[k];
       }
       Mesh& m = *ms[k];
+      // a mesh on a stream of its own keeps it; one on a stream it may share
+      // (the legacy default stream, a caller's stream) runs on the worker's
       cudaStream_t orig = m.s;
-      m.s = st;
+      if (!m.own_stream) m.s = st;
       BatchMeshResult& r = res[k];
       try {
         r.changed = mesh_adapt(m, ap.size_floor, ap.good_qual, ap.nlayers, ap.max_ops);
@@ -175,7 +177,7 @@ void adapt_concurrent(std::vector<Mesh*> const& ms, AdaptParams const& ap, u32 n
       }
       r.passes = last_adapt_stats().passes;
       r.elems_in = last_adapt_stats().elems_in;
-      cudaStreamSynchronize(st);
+      cudaStreamSynchronize(m.s);
       m.s = orig;
       {
         std::lock_guard<std::mutex> g(mu);

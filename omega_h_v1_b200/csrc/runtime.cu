@@ -275,16 +275,36 @@ void dev_free(void* p, cudaStream_t s)
 
 namespace {
 // a pinned word per host thread for read_u32: a copy into pageable memory
-// goes through the driver's staging buffer and takes several times longer
+// goes through the driver's staging buffer and takes several times longer.
+// Words go back to a process-wide free list when their thread ends (pinning
+// and unpinning memory each take a driver call that can wait for the
+// device, which short-lived worker threads would pay every time).
+std::mutex g_words_mu;
+std::vector<u32*>& free_words()
+{
+  static std::vector<u32*>* v = new std::vector<u32*>();  // lives to exit
+  return *v;
+}
 struct PinnedWord {
   u32* p = nullptr;
   ~PinnedWord()
   {
-    if (p) cudaFreeHost(p);
+    if (!p) return;
+    std::lock_guard<std::mutex> g(g_words_mu);
+    free_words().push_back(p);
   }
   u32* get()
   {
-    if (!p) CK(cudaMallocHost(&p, 64));
+    if (p) return p;
+    {
+      std::lock_guard<std::mutex> g(g_words_mu);
+      if (!free_words().empty()) {
+        p = free_words().back();
+        free_words().pop_back();
+        return p;
+      }
+    }
+    CK(cudaMallocHost(&p, 64));
     return p;
   }
 };
