@@ -4,6 +4,7 @@
 #include <cstdio>
 #include <cstring>
 #include <atomic>
+#include <map>
 #include <mutex>
 #include <vector>
 
@@ -488,9 +489,74 @@ k_exscan(u32 const* __restrict__ in, u32* __restrict__ out, u32 n, u32 ntiles,
     if (gi < n) out[gi] = s_buf[li + (li >> 5)];
   }
   if (tile == ntiles - 1 && threadIdx.x == 0) out[n] = s_prefix + total;
+  // The last tile to finish returns the scratch to zero for the next scan
+  // on the stream: every other tile has counted itself done, so no look-back
+  // reads a status word any more.
+  __shared__ u32 s_last;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    s_last = atomicAdd(&ticket_and_err[2], 1u) == ntiles - 1 ? 1u : 0u;
+  }
+  __syncthreads();
+  if (s_last) {
+    for (u32 t = threadIdx.x; t < ntiles; t += blockDim.x) status[t] = 0ull;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      ticket_and_err[0] = 0;
+      ticket_and_err[2] = 0;
+      __threadfence();
+    }
+  }
 }
 
 __global__ void k_set_zero_total(u32* out) { out[0] = 0; }
+
+namespace {
+// Scratch of the scans issued on each stream ([ticket, error, done, pad]
+// then two words per tile), zero between scans: the scan kernel's last tile
+// clears it, so no scan pays for a memset. Scans on one stream run one
+// after another; each stream has its own.
+struct ScanScratch {
+  u32* p = nullptr;
+  size_t words = 0;
+};
+std::mutex g_scan_mu;
+std::map<std::pair<int, cudaStream_t>, ScanScratch>& scan_scratches()
+{
+  static auto* m = new std::map<std::pair<int, cudaStream_t>, ScanScratch>();
+  return *m;
+}
+
+u32* stream_scan_scratch(size_t words, cudaStream_t s)
+{
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> g(g_scan_mu);
+  auto& all = scan_scratches();
+  if (all.size() > 1024 && !all.count({dev, s})) {
+    // streams come and go (one per mesh that owns its stream): past 1024
+    // entries, wait for the device and return every other stream's scratch
+    CK(cudaDeviceSynchronize());
+    for (auto& kv : all)
+      if (kv.second.p) cudaFree(kv.second.p);
+    all.clear();
+  }
+  ScanScratch& sc = all[{dev, s}];
+  if (sc.words < words) {
+    size_t want = std::max(words, (size_t)4096);
+    if (sc.p) CK(cudaFreeAsync(sc.p, s));
+    sc.p = nullptr;
+    sc.words = 0;
+    void* q = nullptr;
+    CK(cudaMallocAsync(&q, want * sizeof(u32), s));
+    CK(cudaMemsetAsync(q, 0, want * sizeof(u32), s));
+    sc.p = static_cast<u32*>(q);
+    sc.words = want;
+  }
+  return sc.p;
+}
+}  // namespace
 
 void exscan_u32(u32 const* in, u32* out, u32 n, cudaStream_t s)
 {
@@ -500,17 +566,14 @@ void exscan_u32(u32 const* in, u32* out, u32 n, cudaStream_t s)
     return;
   }
   u32 ntiles = ceil_div(n, SCAN_TILE);
-  // [ticket, error, pad, pad][status per tile]
-  size_t words = 4 + 2 * (size_t)ntiles;
-  u32* scratch = dalloc<u32>(words, s);
-  CK(cudaMemsetAsync(scratch, 0, words * sizeof(u32), s));
+  // [ticket, error, done, pad][status per tile], zero on entry
+  u32* scratch = stream_scan_scratch(4 + 2 * (size_t)ntiles, s);
   {
     PROBE(P_EXSCAN, s, 4.0 * n + 4.0 * (n + 1));
     k_exscan<0><<<ntiles, SCAN_THREADS, 0, s>>>(in, out, n, ntiles,
         reinterpret_cast<unsigned long long*>(scratch + 4), scratch);
     CK_LAUNCH();
   }
-  dev_free(scratch, s);
 }
 
 void check_device_timeouts(cudaStream_t s)
@@ -565,16 +628,13 @@ u32* negate_offsets(u32 const* offs, u32 n, cudaStream_t s)
     return o;
   }
   u32 ntiles = ceil_div(n, SCAN_TILE);
-  size_t words = 4 + 2 * (size_t)ntiles;
-  u32* scratch = dalloc<u32>(words, s);
-  CK(cudaMemsetAsync(scratch, 0, words * sizeof(u32), s));
+  u32* scratch = stream_scan_scratch(4 + 2 * (size_t)ntiles, s);
   {
     PROBE(P_EXSCAN, s, 4.0 * (n + 1) + 4.0 * (n + 1));
     k_exscan<1><<<ntiles, SCAN_THREADS, 0, s>>>(offs, o, n, ntiles,
         reinterpret_cast<unsigned long long*>(scratch + 4), scratch);
     CK_LAUNCH();
   }
-  dev_free(scratch, s);
   return o;
 }
 
