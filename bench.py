@@ -722,7 +722,9 @@ def run_serving(args, world, rank, local):
         "data": "synthetic (seeded Poisson stream of box jobs)",
         "config": {"workload": "serving_poisson", "jobs": len(jobs), "rate_per_s": args.rate,
                    "tets": "log-uniform in [2e3, 2e6] per job, seed 2",
-                   "size": "half uniform U[1.0/n, 1.6/n], half radial 0.8/n (1 + 4|x-c|)",
+                   "size": "half uniform U[1.0/n, 1.6/n], half the recovered Hessian of "
+                           "tanh(50(x-o-0.1 sin 2 pi y)), o~U[0.3,0.7], sizes 0.5/n..2/n, "
+                           "weight (2/n-0.5/n)/2000 (computed on the GPU before the stream)",
                    "tets_in": int(tets_in), "budget_bytes": budget,
                    "adapt": "mesh_adapt(1/3, 0.3, 4, 50) per job",
                    "l2": "inputs larger than L2 (hundreds of MB resident)"},

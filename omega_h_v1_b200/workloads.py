@@ -6,8 +6,11 @@ them; every draw comes from a splitmix64 stream of the stated seed).
   perturbed by up to 0.1 h0 with its index as the perturbation seed;
 * serving stream: Poisson arrivals of adaptation jobs (rate `rate` per
   second) whose tet count is log-uniform in [2e3, 2e6] (n = round((tets/6)^(1/3))),
-  half with a uniform size h in [1.0/n, 1.6/n], half with a radial size
-  0.8/n (1 + 4 |x - c|) around a centre drawn in [0.3, 0.7]^3.
+  half with a uniform size h in [1.0/n, 1.6/n], half with the anisotropic-front
+  workload's size field: the recovered Hessian of u = tanh(50(x - o - 0.1
+  sin 2 pi y)) with the front offset o drawn in [0.3, 0.7], sizes between
+  min_h = 0.5/n and max_h = 2/n and weight (max_h - min_h) / 2000 (the
+  Frobenius norm of the exact Hessian peaks near 2000 at the front).
 """
 from __future__ import annotations
 
@@ -44,6 +47,7 @@ class BoxJob:
     seed: int          # perturbation seed
     radial: tuple | None = None   # (h0, h1, cx, cy, cz) for h0 + h1 |x - c|
     arrival: float = 0.0          # seconds from the start of a serving run
+    front: tuple | None = None    # (offset, weight, min_h, max_h): tanh-front Hessian size
 
     @property
     def tets(self) -> int:
@@ -52,6 +56,10 @@ class BoxJob:
     def estimated_output_tets(self) -> float:
         """Rough size after adaptation (fit of mesh_adapt on uniform boxes:
         about 6.9 / (h n)^3 times the input); used only to plan memory."""
+        if self.front is not None:
+            # a band at min_h = 0.5/n in a field of up to 2/n: about the
+            # output of a uniform size 1/n
+            return self.tets * 6.9
         if self.radial is None:
             c = self.size * self.n
             return self.tets * max(6.9 / c ** 3, 0.5)
@@ -86,14 +94,21 @@ def serving_stream(count=200, seed=2, rate=200.0, tmin=2e3, tmax=2e6):
             out.append(BoxJob(i, n, h, i, None, t))
         else:
             c = tuple(0.3 + 0.4 * rng.uniform() for _ in range(3))
-            h0 = 0.8 / n
-            out.append(BoxJob(i, n, 0.0, i, (h0, 4.0 * h0) + c, t))
+            min_h, max_h = 0.5 / n, 2.0 / n
+            out.append(BoxJob(i, n, 0.0, i, None, t,
+                              (c[0], (max_h - min_h) / 2000.0, min_h, max_h)))
     return out
 
 
 def build_job_mesh(G, job: BoxJob, pert=0.1):
     """The job's classified full-topology box on the current GPU with its
     adapt_size field (input preparation)."""
+    if job.front is not None:
+        coords, conn, h = job_host_input(G, job, pert)
+        m = G.Mesh.reduced(3, coords, conn)
+        m.derive_model_full()
+        m.add_field(0, "adapt_size", h)
+        return m
     coords, conn, _ = G.box(job.n, job.seed, pert)
     m = G.Mesh.reduced(3, coords, conn)
     m.derive_model_full()
@@ -109,9 +124,20 @@ def build_job_mesh(G, job: BoxJob, pert=0.1):
 
 
 def job_host_input(G, job: BoxJob, pert=0.1):
-    """Host arrays of the job's input for the CPU checkers: coords, conn, h."""
+    """Host arrays of the job's input: coords, conn, h. A front job's size
+    field comes from the library's size-field chain on the GPU (element
+    gradients, volume recovery twice, size from Hessian)."""
     coords, conn, _ = G.box(job.n, job.seed, pert)
     nv = coords.size // 3
+    if job.front is not None:
+        offset, weight, min_h, max_h = job.front
+        m = G.Mesh.reduced(3, coords, conn)
+        m.derive_model_full()
+        m.add_field(0, "dye", front_field(coords, offset))
+        hessian_size_field(m, "dye", weight, min_h, max_h)
+        h = next(t.data for t in m.tags(0) if t.name == "adapt_size").copy()
+        m.close()
+        return coords, conn, h
     if job.radial is None:
         h = np.full(nv, job.size)
     else:

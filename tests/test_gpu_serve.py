@@ -19,7 +19,9 @@ def _jobs():
     jobs = [W.BoxJob(0, 4, 0.2, 0), W.BoxJob(1, 6, 0.12, 1),
             W.BoxJob(2, 5, 0.0, 2, (0.05, 0.2, 0.4, 0.5, 0.6)),
             W.BoxJob(3, 3, 0.09, 3), W.BoxJob(4, 7, 0.3, 4),
-            W.BoxJob(5, 6, 0.0, 5, (0.08, 0.3, 0.6, 0.4, 0.5))]
+            W.BoxJob(5, 6, 0.0, 5, (0.08, 0.3, 0.6, 0.4, 0.5)),
+            # the front's Hessian size field, computed on the GPU
+            W.BoxJob(6, 8, 0.0, 6, None, 0.0, (0.45, (2 / 8 - 0.5 / 8) / 2000, 0.5 / 8, 2 / 8))]
     return [(j,) + W.job_host_input(G, j) for j in jobs]
 
 
@@ -58,7 +60,7 @@ def test_results_equal_alone_and_in_the_mix():
     from oracle import oracle as O
     inputs = _jobs()
     alone = [_alone(c, k, h) for _, c, k, h in inputs]
-    sv, out, info, max_active = _serve(inputs, 1 << 40, [2, 1, 3])
+    sv, out, info, max_active = _serve(inputs, 1 << 40, [2, 1, 4])
     assert max_active >= 3, "jobs should overlap on the device"
     for i, (m, r) in enumerate(alone):
         g = out[i]
@@ -67,7 +69,7 @@ def test_results_equal_alone_and_in_the_mix():
         assert not errs, "job %d: %s" % (i, errs[:5])
         assert g.digest() == m.digest(), "job %d digest" % i
     # each job alone in its own server gives the same result
-    for i in (1, 2):
+    for i in (1, 2, 6):
         _, out1, _, _ = _serve([inputs[i]], 1 << 40, [1])
         assert out1[0].digest() == out[i].digest()
     sv.close()
