@@ -690,6 +690,13 @@ static void coarsen_build(Mesh& m, CoarsenSel const& sel)
   u32* fused[4] = {nullptr, nullptr, nullptr, nullptr};
   u32* same_of[4] = {nullptr, nullptr, nullptr, nullptr};
   u32 nsame_of[4] = {0, 0, 0, 0};
+  // the products and survivors of every dimension are counted first (the
+  // fused sides pass from each dimension to the next on the device), their
+  // totals landing in mailbox slots 16 + 2 (ed - 1) and 17 + 2 (ed - 1), so
+  // one read-back serves all dimensions
+  u32* gen_offs_of[4] = {nullptr, nullptr, nullptr, nullptr};
+  u32* gvert_of[4] = {nullptr, nullptr, nullptr, nullptr};
+  u32* gdir_of[4] = {nullptr, nullptr, nullptr, nullptr};
   for (u32 dd = 0; dd < dim; ++dd) {
     u32 ed = dim - dd;
     u32 n = m.count(ed), vpe = deg(ed, 0);
@@ -700,23 +707,30 @@ static void coarsen_build(Mesh& m, CoarsenSel const& sel)
     CK(cudaMemsetAsync(fused[ed - 1], 0, sizeof(u32) * nsides, s));
     u32* is_same = dalloc<u32>(n, s);
     u32* will_gen = dalloc<u32>(n, s);
-    u32* gvert = dalloc<u32>(n, s);
-    u32* gdir = dalloc<u32>(n, s);
+    gvert_of[ed] = dalloc<u32>(n, s);
+    gdir_of[ed] = dalloc<u32>(n, s);
     if (n) {
       PROBE(P_COLLAPSE_TO_ENT, s, 4.0 * (vpe + deg(ed, ed - 1)) * n + 8.0 * (nv + 1) +
           4.0 * n * 4 + 4.0 * nsides);
       k_collapse_to_ent<<<grid_for(n), BLOCK, 0, s>>>(ed, n, voe, soe, gen_offs_v,
-          sel.gen_vert, fused[ed], is_same, fused[ed - 1], will_gen, gvert, gdir);
+          sel.gen_vert, fused[ed], is_same, fused[ed - 1], will_gen, gvert_of[ed], gdir_of[ed]);
       CK_LAUNCH();
     }
-    u32* gen_offs = exscan_new(will_gen, n, s);
-    u32* same_e = exscan_new(is_same, n, s);
+    gen_offs_of[ed] = exscan_new(will_gen, n, s, m.mb->dev + 16 + 2 * (ed - 1));
+    same_of[ed] = exscan_new(is_same, n, s, m.mb->dev + 17 + 2 * (ed - 1));
     dev_free(will_gen, s);
     dev_free(is_same, s);
-    CK(cudaMemcpyAsync(m.mb->dev + 16, gen_offs + n, sizeof(u32), cudaMemcpyDeviceToDevice, s));
-    CK(cudaMemcpyAsync(m.mb->dev + 17, same_e + n, sizeof(u32), cudaMemcpyDeviceToDevice, s));
-    m.mb->fetch(s, 18);
-    u32 ngen = m.mb->host[16], nsame = m.mb->host[17];
+  }
+  m.mb->fetch(s, 22);
+  for (u32 dd = 0; dd < dim; ++dd) {
+    u32 ed = dim - dd;
+    u32 n = m.count(ed), vpe = deg(ed, 0);
+    u32 const* voe = m.ask_down(ed, 0);
+    u32 ngen = m.mb->host[16 + 2 * (ed - 1)], nsame = m.mb->host[17 + 2 * (ed - 1)];
+    u32* gen_offs = gen_offs_of[ed];
+    u32* same_e = same_of[ed];
+    u32* gvert = gvert_of[ed];
+    u32* gdir = gdir_of[ed];
     u32 nout = nsame + ngen;
     u32* conn = dalloc<u32>((size_t)nout * vpe, s);
     if (n) {
@@ -742,7 +756,6 @@ static void coarsen_build(Mesh& m, CoarsenSel const& sel)
     if (m.parallel) inherit_globals(*out, ed, nout);
     if (ed == dim) coarsen_transfer(m, *out, gen_offs_v, gen_offs, same_e, nsame, ngen);
     dev_free(gen_offs, s);
-    same_of[ed] = same_e;
     nsame_of[ed] = nsame;
   }
   same_of[0] = same_v;
@@ -756,7 +769,7 @@ static void coarsen_build(Mesh& m, CoarsenSel const& sel)
     u32* newid = nullptr;
     for (u32 l = 0; l < h; ++l)
       if (same_of[h] && same_of[l])
-        carry_up(m, *out, l, h, same_of[l], same_of[h], nsame_of[h], &newid);
+        carry_up(m, *out, l, h, same_of[l], nsame_of[l], same_of[h], nsame_of[h], &newid);
     dev_free(newid, s);
   }
   for (u32 d = 0; d < 4; ++d) {

@@ -343,13 +343,16 @@ __global__ void k_count_lows(u32 const* __restrict__ loh, u32 nuses, u32* cnt)
   if (i < nuses) atomicAdd(&cnt[loh[i]], 1u);
 }
 
+// cnt holds each row's count: a row's uses take its slots from the end down
+// (their order is arbitrary either way; the rows are ranked or marked
+// unsorted afterwards), so no cursor array is zeroed for the fill
 __global__ void k_fill_uses(u32 const* __restrict__ loh, u32 nuses,
-    u32 const* __restrict__ offs, u32* cur, u32* __restrict__ tmp)
+    u32 const* __restrict__ offs, u32* cnt, u32* __restrict__ tmp)
 {
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nuses) return;
   u32 l = loh[i];
-  u32 slot = atomicAdd(&cur[l], 1u);
+  u32 slot = atomicSub(&cnt[l], 1u) - 1u;
   tmp[offs[l] + slot] = i;
 }
 
@@ -470,13 +473,14 @@ static void rank_rows(u32 const* offs, u32 const* pre, u32 const* tmp, u32 nrows
   else launch_sort_rows<32, 4>(offs, pre, tmp, nrows, lph, adj, dirs, s);
 }
 
+// as k_fill_uses, the row's slots taken from its end down
 __global__ void k_fill_uses_split(u32 const* __restrict__ loh, u32 nuses, u32 lph,
-    u32 const* __restrict__ offs, u32* cur, u32* __restrict__ adj, u32* __restrict__ dirs)
+    u32 const* __restrict__ offs, u32* cnt, u32* __restrict__ adj, u32* __restrict__ dirs)
 {
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nuses) return;
   u32 l = loh[i];
-  u32 slot = offs[l] + atomicAdd(&cur[l], 1u);
+  u32 slot = offs[l] + atomicSub(&cnt[l], 1u) - 1u;
   adj[slot] = i / lph;
   dirs[slot] = i % lph;
 }
@@ -501,7 +505,6 @@ void up_from_down_unsorted(u32 high, u32 low, u32 nhighs, u32 nlows, u32 const* 
     CK_LAUNCH();
   }
   out.offs = exscan_new(cnt, nlows, s);
-  CK(cudaMemsetAsync(cnt, 0, sizeof(u32) * ((size_t)nlows + 1), s));
   out.adj = dalloc<u32>(nuses, s);
   out.dirs = dalloc<u32>(nuses, s);
   if (nuses) {
@@ -543,7 +546,6 @@ void up_from_down(u32 high, u32 low, u32 nhighs, u32 nlows, u32 const* loh,
     CK_LAUNCH();
   }
   out.offs = exscan_new(cnt, nlows, s);
-  CK(cudaMemsetAsync(cnt, 0, sizeof(u32) * ((size_t)nlows + 1), s));
   u32* tmp = dalloc<u32>(nuses, s);
   out.adj = dalloc<u32>(nuses, s);
   out.dirs = dalloc<u32>(nuses, s);
@@ -588,7 +590,6 @@ void up_from_down_scratch(u32 high, u32 low, u32 nhighs, u32 nlows, u32 const* l
     CK_LAUNCH();
   }
   exscan_u32_scratch(cnt, out.offs, nlows, scan, s);
-  CK(cudaMemsetAsync(cnt, 0, sizeof(u32) * ((size_t)nlows + 1), s));
   if (nuses) {
     k_fill_uses<<<grid_for(nuses), BLOCK, 0, s>>>(loh, nuses, out.offs, cnt, tmp);
     CK_LAUNCH();
@@ -627,15 +628,17 @@ __global__ void k_count_min_vert(u32 low, u32 nl, u32 const* __restrict__ vol, u
   atomicAdd(&cnt[m], 1u);
 }
 
+// cnt holds each vertex's row count; a row's records take its slots from the
+// end down (the search reads a whole row, so their order does not matter)
 __global__ void k_fill_min_vert(u32 low, u32 nl, u32 const* __restrict__ vol,
-    u32 const* __restrict__ offs, u32* cur, u32* __restrict__ rows)
+    u32 const* __restrict__ offs, u32* cnt, u32* __restrict__ rows)
 {
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nl) return;
   u32 vpl = low + 1, w[3];
   for (u32 k = 0; k < vpl; ++k) w[k] = vol[(size_t)i * vpl + k];
   sort_small(w, vpl);
-  u32 slot = offs[w[0]] + atomicAdd(&cur[w[0]], 1u);
+  u32 slot = offs[w[0]] + atomicSub(&cnt[w[0]], 1u) - 1u;
   if (low == 1)
     reinterpret_cast<uint2*>(rows)[slot] = make_uint2(w[1], i);
   else
@@ -904,7 +907,6 @@ void Mesh::build_low_rows(u32 low)
     CK_LAUNCH();
   }
   low_row_offs[low] = exscan_new(cnt, nv, s);
-  CK(cudaMemsetAsync(cnt, 0, sizeof(u32) * ((size_t)nv + 1), s));
   low_rows[low] = dalloc<u32>((size_t)nl * (low == 1 ? 2 : 4), s);
   if (nl) {
     k_fill_min_vert<<<grid_for(nl), BLOCK, 0, s>>>(low, nl, vol, low_row_offs[low], cnt,
@@ -1014,12 +1016,22 @@ __global__ void k_new_ids(u32 n, u32 const* __restrict__ same, u32* __restrict__
   newid[i] = same[i + 1] != a ? a : INV;
 }
 
-__global__ void k_up_surv_count(u32 nl_old, u32 const* __restrict__ same_l,
-    u32 const* __restrict__ newid_h, u32 const* __restrict__ offs, u32 const* __restrict__ adj,
-    u32* __restrict__ cnt, u32* __restrict__ surv)
+// threads past the old rows zero the counts of the rows the pass made (and
+// the entry after the last row), so no memset precedes the launch
+__global__ void k_up_surv_count(u32 nl_old, u32 nsame_l, u32 ntail,
+    u32 const* __restrict__ same_l, u32 const* __restrict__ newid_h,
+    u32 const* __restrict__ offs, u32 const* __restrict__ adj, u32* __restrict__ cnt,
+    u32* __restrict__ surv)
 {
   u32 j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= nl_old) return;
+  if (j >= nl_old) {
+    if (j - nl_old < ntail) {
+      u32 r = nsame_l + (j - nl_old);
+      cnt[r] = 0;
+      if (surv) surv[r] = 0;
+    }
+    return;
+  }
   u32 nj = same_l[j];
   if (same_l[j + 1] == nj) return;
   u32 r = offs[j], e = offs[j + 1];
@@ -1031,7 +1043,7 @@ __global__ void k_up_surv_count(u32 nl_old, u32 const* __restrict__ same_l,
   }
   for (; r < e; ++r) c += newid_h[adj[r]] != INV;
   cnt[nj] = c;
-  surv[nj] = c;
+  if (surv) surv[nj] = c;
 }
 
 __global__ void k_up_gen_count(u32 first, u32 nuses, u32 const* __restrict__ loh,
@@ -1078,13 +1090,16 @@ __global__ void k_up_surv_fill(u32 nl_old, u32 const* __restrict__ same_l,
   }
 }
 
+// cnt holds each row's kept + generated uses: the generated ones take the
+// slots after the kept ones, from the row's end down (their order within a
+// row is arbitrary either way: the rows are marked unsorted)
 __global__ void k_up_gen_fill(u32 first, u32 nuses, u32 lph, u32 const* __restrict__ loh,
-    u32 const* __restrict__ offs, u32* cur, u32* __restrict__ adj, u32* __restrict__ dirs)
+    u32 const* __restrict__ offs, u32* cnt, u32* __restrict__ adj, u32* __restrict__ dirs)
 {
   u32 u = first + blockIdx.x * blockDim.x + threadIdx.x;
   if (u >= nuses) return;
   u32 l = loh[u];
-  u32 slot = offs[l] + atomicAdd(&cur[l], 1u);
+  u32 slot = offs[l] + atomicSub(&cnt[l], 1u) - 1u;
   adj[slot] = u / lph;
   dirs[slot] = u % lph;
 }
@@ -1099,14 +1114,15 @@ u32* carry_new_ids(u32 const* same, u32 n, cudaStream_t s)
   return newid;
 }
 
-void carry_up(Mesh& m, Mesh& out, u32 low, u32 high, u32 const* same_l, u32 const* same_h,
-    u32 nsame_h, u32** newid_cache)
+void carry_up(Mesh& m, Mesh& out, u32 low, u32 high, u32 const* same_l, u32 nsame_l,
+    u32 const* same_h, u32 nsame_h, u32** newid_cache)
 {
   if (!m.have_up[low][high] || out.have_up[low][high]) return;
   if (!out.has_dim(high) || !out.has_dim(low)) return;
   if (low > 0 && !out.down[high][low]) return;  // its search is not worth it here
   cudaStream_t s = out.s;
   u32 nl_old = m.counts[low], nl = out.count(low), nh = out.count(high);
+  if (nsame_l > nl || nsame_l > nl_old) throw Failure(E_ARG, "carry_up: survivor count");
   u32 lph = deg(high, low), nuses = nh * lph, first = nsame_h * lph;
   u32 const* loh = out.ask_down(high, low);
   UpAdj const& old = m.up[low][high];
@@ -1125,15 +1141,16 @@ void carry_up(Mesh& m, Mesh& out, u32 low, u32 high, u32 const* same_l, u32 cons
       own_newid = nullptr;
     }
   }
+  // cnt: kept + generated uses per new row; surv (kept only when the old
+  // rows were sorted): each row's count of leading uses, in order
   u32* cnt = dalloc<u32>((size_t)nl + 1, s);
-  u32* surv = dalloc<u32>((size_t)nl + 1, s);
-  CK(cudaMemsetAsync(cnt, 0, sizeof(u32) * ((size_t)nl + 1), s));
-  CK(cudaMemsetAsync(surv, 0, sizeof(u32) * ((size_t)nl + 1), s));
+  u32* surv = m.up_sorted[low][high] ? dalloc<u32>((size_t)nl + 1, s) : nullptr;
   u32 nuses_old = m.counts[high] * lph;
-  if (nl_old) {
+  {
+    u32 ntail = nl + 1 - nsame_l;
     PROBE(P_CARRY_UP, s, 8.0 * (nl_old + 1) + 4.0 * nuses_old + 8.0 * nuses_old + 8.0 * nl);
-    k_up_surv_count<<<grid_for(nl_old), BLOCK, 0, s>>>(nl_old, same_l, newid_h, old.offs,
-        old.adj, cnt, surv);
+    k_up_surv_count<<<grid_for((u64)nl_old + ntail), BLOCK, 0, s>>>(nl_old, nsame_l, ntail,
+        same_l, newid_h, old.offs, old.adj, cnt, surv);
     CK_LAUNCH();
   }
   if (nuses > first) {
@@ -1143,10 +1160,6 @@ void carry_up(Mesh& m, Mesh& out, u32 low, u32 high, u32 const* same_l, u32 cons
   }
   UpAdj u;
   u.offs = exscan_new(cnt, nl, s);
-  // cnt becomes the fill cursor (starting after each row's survivors); surv
-  // stays as the count of each row's leading uses, in order when the old
-  // rows were
-  CK(cudaMemcpyAsync(cnt, surv, sizeof(u32) * ((size_t)nl + 1), cudaMemcpyDeviceToDevice, s));
   u.adj = dalloc<u32>(nuses, s);
   u.dirs = dalloc<u32>(nuses, s);
   if (nl_old) {
@@ -1163,11 +1176,9 @@ void carry_up(Mesh& m, Mesh& out, u32 low, u32 high, u32 const* same_l, u32 cons
   }
   dev_free(cnt, s);
   dev_free(own_newid, s);
-  if (m.up_sorted[low][high]) {
+  if (surv) {
     u.pre = surv;
     u.npre = first;
-  } else {
-    dev_free(surv, s);
   }
   out.up[low][high] = u;
   out.have_up[low][high] = true;

@@ -275,10 +275,8 @@ static u32 refine_build(Mesh& m, u32 const* gen_offs)
           will, sp[dd].dir, sp[dd].vert);
       CK_LAUNCH();
     }
-    sp[dd].offs = exscan_new(will, nd, s);
+    sp[dd].offs = exscan_new(will, nd, s, m.mb->dev + 8 + dd);
     dev_free(will, s);
-    CK(cudaMemcpyAsync(m.mb->dev + 8 + dd, sp[dd].offs + nd, sizeof(u32),
-        cudaMemcpyDeviceToDevice, s));
   }
   m.mb->fetch(s, 16);
   for (u32 dd = 1; dd <= dim; ++dd)
@@ -381,7 +379,7 @@ static u32 refine_build(Mesh& m, u32 const* gen_offs)
     u32* newid = nullptr;
     for (u32 l = 0; l < h; ++l)
       if (same_of[h] && same_of[l])
-        carry_up(m, *out, l, h, same_of[l], same_of[h], nsame_of[h], &newid);
+        carry_up(m, *out, l, h, same_of[l], nsame_of[l], same_of[h], nsame_of[h], &newid);
     dev_free(newid, s);
   }
   for (u32 dd = 0; dd <= dim; ++dd) {

@@ -385,7 +385,7 @@ __device__ u32 d_wait_timeouts;
 template <int MODE>
 __global__ void __launch_bounds__(SCAN_THREADS)
 k_exscan(u32 const* __restrict__ in, u32* __restrict__ out, u32 n, u32 ntiles,
-    unsigned long long* status, u32* ticket_and_err)
+    unsigned long long* status, u32* ticket_and_err, u32* total_to)
 {
   __shared__ u32 s_tile;
   __shared__ u32 s_warp[SCAN_WARPS];
@@ -488,7 +488,10 @@ k_exscan(u32 const* __restrict__ in, u32* __restrict__ out, u32 n, u32 ntiles,
     size_t gi = base + li;
     if (gi < n) out[gi] = s_buf[li + (li >> 5)];
   }
-  if (tile == ntiles - 1 && threadIdx.x == 0) out[n] = s_prefix + total;
+  if (tile == ntiles - 1 && threadIdx.x == 0) {
+    out[n] = s_prefix + total;
+    if (total_to) *total_to = s_prefix + total;
+  }
   // The last tile to finish returns the scratch to zero for the next scan
   // on the stream: every other tile has counted itself done, so no look-back
   // reads a status word any more.
@@ -510,7 +513,11 @@ k_exscan(u32 const* __restrict__ in, u32* __restrict__ out, u32 n, u32 ntiles,
   }
 }
 
-__global__ void k_set_zero_total(u32* out) { out[0] = 0; }
+__global__ void k_set_zero_total(u32* out, u32* total_to)
+{
+  out[0] = 0;
+  if (total_to) *total_to = 0;
+}
 
 namespace {
 // Scratch of the scans issued on each stream ([ticket, error, done, pad]
@@ -558,10 +565,10 @@ u32* stream_scan_scratch(size_t words, cudaStream_t s)
 }
 }  // namespace
 
-void exscan_u32(u32 const* in, u32* out, u32 n, cudaStream_t s)
+void exscan_u32(u32 const* in, u32* out, u32 n, cudaStream_t s, u32* total_to)
 {
   if (n == 0) {
-    k_set_zero_total<<<1, 1, 0, s>>>(out);
+    k_set_zero_total<<<1, 1, 0, s>>>(out, total_to);
     CK_LAUNCH();
     return;
   }
@@ -571,7 +578,7 @@ void exscan_u32(u32 const* in, u32* out, u32 n, cudaStream_t s)
   {
     PROBE(P_EXSCAN, s, 4.0 * n + 4.0 * (n + 1));
     k_exscan<0><<<ntiles, SCAN_THREADS, 0, s>>>(in, out, n, ntiles,
-        reinterpret_cast<unsigned long long*>(scratch + 4), scratch);
+        reinterpret_cast<unsigned long long*>(scratch + 4), scratch, total_to);
     CK_LAUNCH();
   }
 }
@@ -601,21 +608,21 @@ void exscan_u32_scratch(u32 const* in, u32* out, u32 n, u32* scratch, cudaStream
   if (reinterpret_cast<uintptr_t>(scratch) % 16 != 0)
     throw Failure(E_ARG, "scan scratch must start on a 16-byte boundary");
   if (n == 0) {
-    k_set_zero_total<<<1, 1, 0, s>>>(out);
+    k_set_zero_total<<<1, 1, 0, s>>>(out, nullptr);
     CK_LAUNCH();
     return;
   }
   u32 ntiles = ceil_div(n, SCAN_TILE);
   CK(cudaMemsetAsync(scratch, 0, exscan_scratch_words(n) * sizeof(u32), s));
   k_exscan<0><<<ntiles, SCAN_THREADS, 0, s>>>(in, out, n, ntiles,
-      reinterpret_cast<unsigned long long*>(scratch + 4), scratch);
+      reinterpret_cast<unsigned long long*>(scratch + 4), scratch, nullptr);
   CK_LAUNCH();
 }
 
-u32* exscan_new(u32 const* in, u32 n, cudaStream_t s)
+u32* exscan_new(u32 const* in, u32 n, cudaStream_t s, u32* total_to)
 {
   u32* out = dalloc<u32>((size_t)n + 1, s);
-  exscan_u32(in, out, n, s);
+  exscan_u32(in, out, n, s, total_to);
   return out;
 }
 
@@ -623,7 +630,7 @@ u32* negate_offsets(u32 const* offs, u32 n, cudaStream_t s)
 {
   u32* o = dalloc<u32>((size_t)n + 1, s);
   if (n == 0) {
-    k_set_zero_total<<<1, 1, 0, s>>>(o);
+    k_set_zero_total<<<1, 1, 0, s>>>(o, nullptr);
     CK_LAUNCH();
     return o;
   }
@@ -632,7 +639,7 @@ u32* negate_offsets(u32 const* offs, u32 n, cudaStream_t s)
   {
     PROBE(P_EXSCAN, s, 4.0 * (n + 1) + 4.0 * (n + 1));
     k_exscan<1><<<ntiles, SCAN_THREADS, 0, s>>>(offs, o, n, ntiles,
-        reinterpret_cast<unsigned long long*>(scratch + 4), scratch);
+        reinterpret_cast<unsigned long long*>(scratch + 4), scratch, nullptr);
     CK_LAUNCH();
   }
   return o;

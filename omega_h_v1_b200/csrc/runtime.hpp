@@ -14,8 +14,10 @@ void clear_error();
 
 // Exclusive scan with the total appended: out has n+1 entries and
 // out[n] = sum(in). Single-pass decoupled look-back (uints_exscan, ints.cpp).
-void exscan_u32(u32 const* in, u32* out, u32 n, cudaStream_t s);
-u32* exscan_new(u32 const* in, u32 n, cudaStream_t s);
+// total_to (optional, device): receives out[n] as well (a mailbox slot the
+// host reads back with other flags, instead of a copy of its own)
+void exscan_u32(u32 const* in, u32* out, u32 n, cudaStream_t s, u32* total_to = nullptr);
+u32* exscan_new(u32 const* in, u32 n, cudaStream_t s, u32* total_to = nullptr);
 
 // The same scan with caller-provided scratch of at least
 // exscan_scratch_words(n) 32-bit words (zeroed here); allocates nothing.

@@ -513,23 +513,32 @@ static void swap_build(Mesh& m, SwapSel const& sel)
   u32* cnt = dalloc<u32>(ne, s);
   u32* same_of[4] = {nullptr, nullptr, nullptr, nullptr};
   u32 nsame_of[4] = {0, 0, 0, 0};
-  for (u32 ed = m.full ? 1u : dim; ed <= dim; ++ed) {
-    u32 n = m.count(ed), vpe = deg(ed, 0);
+  // the products and survivors of every dimension are counted first, their
+  // totals landing in mailbox slots 20 + 2 (ed - 1) and 21 + 2 (ed - 1), so
+  // one read-back serves all dimensions
+  u32 const ed0 = m.full ? 1u : dim;
+  u32* gen_offs_of[4] = {nullptr, nullptr, nullptr, nullptr};
+  for (u32 ed = ed0; ed <= dim; ++ed) {
+    u32 n = m.count(ed);
     k_swap_counts<<<grid_for(ne), BLOCK, 0, s>>>(ne, ed, sel.ind, sel.rs, cnt);
     CK_LAUNCH();
-    u32* gen_offs = exscan_new(cnt, ne, s);
+    gen_offs_of[ed] = exscan_new(cnt, ne, s, m.mb->dev + 20 + 2 * (ed - 1));
     u32* same = dalloc<u32>(n, s);
     if (n) {
       k_swap_same<<<grid_for(n), BLOCK, 0, s>>>(n, deg(ed, 1), ed == 1 ? nullptr : m.ask_down(ed, 1),
           sel.ind, same);
       CK_LAUNCH();
     }
-    u32* same_offs = exscan_new(same, n, s);
+    same_of[ed] = exscan_new(same, n, s, m.mb->dev + 21 + 2 * (ed - 1));
     dev_free(same, s);
-    CK(cudaMemcpyAsync(m.mb->dev + 20, gen_offs + ne, sizeof(u32), cudaMemcpyDeviceToDevice, s));
-    CK(cudaMemcpyAsync(m.mb->dev + 21, same_offs + n, sizeof(u32), cudaMemcpyDeviceToDevice, s));
-    m.mb->fetch(s, 22);
-    u32 ngen = m.mb->host[20], nsame = m.mb->host[21];
+  }
+  dev_free(cnt, s);
+  m.mb->fetch(s, 26);
+  for (u32 ed = ed0; ed <= dim; ++ed) {
+    u32 n = m.count(ed), vpe = deg(ed, 0);
+    u32 ngen = m.mb->host[20 + 2 * (ed - 1)], nsame = m.mb->host[21 + 2 * (ed - 1)];
+    u32* gen_offs = gen_offs_of[ed];
+    u32* same_offs = same_of[ed];
     u32* conn = dalloc<u32>((size_t)(nsame + ngen) * vpe, s);
     expand_scaled(m.ask_down(ed, 0), same_offs, 1, n, vpe, 4, conn, s);
     k_swap_cavity<<<ceil_div(ne, 128), 128, 0, s>>>(ne, ed, sel.ind, sel.codes, gen_offs, te.offs,
@@ -580,10 +589,8 @@ static void swap_build(Mesh& m, SwapSel const& sel)
       }
     }
     dev_free(gen_offs, s);
-    same_of[ed] = same_offs;
     nsame_of[ed] = nsame;
   }
-  dev_free(cnt, s);
   same_of[0] = dalloc<u32>((size_t)nv + 1, s);  // vertices all survive, in order
   iota_u32(same_of[0], nv + 1, 1, s);
   nsame_of[0] = nv;
@@ -596,7 +603,7 @@ static void swap_build(Mesh& m, SwapSel const& sel)
     u32* newid = nullptr;
     for (u32 l = 0; l < h; ++l)
       if (same_of[h] && same_of[l])
-        carry_up(m, *out, l, h, same_of[l], same_of[h], nsame_of[h], &newid);
+        carry_up(m, *out, l, h, same_of[l], nsame_of[l], same_of[h], nsame_of[h], &newid);
     dev_free(newid, s);
   }
   for (u32 d = 0; d < 4; ++d) dev_free(same_of[d], s);
