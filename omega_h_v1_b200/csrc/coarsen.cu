@@ -223,12 +223,15 @@ __global__ void k_coarsen_quality(u32 dim, u32 const* __restrict__ list,
   }
 }
 
-// ids of the entities with a nonzero flag, in no particular order
-__global__ void k_list_nonzero(u32 n, u32 const* __restrict__ flags, u32* __restrict__ list,
-    u32* count)
+// the candidate edges listed (a warp's candidates take consecutive slots,
+// warps in any order) and every edge's two collapse qualities zeroed (the
+// quality kernel writes the kept ones)
+__global__ void k_list_candidates(u32 n, u32 const* __restrict__ flags, u32* __restrict__ list,
+    u32* count, double2* __restrict__ q2)
 {
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   bool on = i < n && flags[i] != 0;
+  if (i < n) q2[i] = make_double2(0.0, 0.0);
   u32 mask = __ballot_sync(0xffffffffu, on);
   if (!mask) return;
   u32 lane = threadIdx.x & 31, leader = __ffs(mask) - 1;
@@ -593,35 +596,27 @@ static bool coarsen_select(Mesh& m, u32* codes, double qual_floor, bool require_
     CK(cudaMemcpyAsync(codes_class_out, codes, sizeof(u32) * ne, cudaMemcpyDeviceToDevice, s));
   if (codes_qual_out)
     CK(cudaMemcpyAsync(codes_qual_out, codes, sizeof(u32) * ne, cudaMemcpyDeviceToDevice, s));
-  // the candidate edges, listed (this read-back also tells whether any is left)
+  // the candidate edges, listed, and the qualities of their collapses; one
+  // read-back (mailbox slots 4 and 7) tells whether any edge was a candidate
+  // and whether any collapse survived
   u32* clist = dalloc<u32>(ne ? ne : 1, s);
+  sel.q2 = dalloc<double>((size_t)ne * 2, s);
+  u32* any = m.mb->dev + 4;
   u32* ncand = m.mb->dev + 7;
-  CK(cudaMemsetAsync(ncand, 0, sizeof(u32), s));
+  CK(cudaMemsetAsync(any, 0, 4 * sizeof(u32), s));  // slots 4-7
   if (ne) {
-    k_list_nonzero<<<grid_for(ne), BLOCK, 0, s>>>(ne, codes, clist, ncand);
+    k_list_candidates<<<grid_for(ne), BLOCK, 0, s>>>(ne, codes, clist, ncand,
+        reinterpret_cast<double2*>(sel.q2));
     CK_LAUNCH();
   }
-  m.mb->fetch(s, 8);
-  u32 nc = m.mb->host[7];
-  if (!nc) {
-    dev_free(clist, s);
-    return false;
-  }
-  // check_coarsen_quality (coarsen_common.cpp:139-180) ghosts a parallel
-  // mesh and exchanges the collapse codes whatever it then finds
-  m.ensure_ghosting(1);
-  m.note_exchange(1);
-  sel.q2 = dalloc<double>((size_t)ne * 2, s);
-  CK(cudaMemsetAsync(sel.q2, 0, sizeof(double) * ne * 2, s));
-  u32* any = m.mb->dev + 4;
-  CK(cudaMemsetAsync(any, 0, sizeof(u32), s));
-  if (dim >= 2) {
+  if (dim >= 2 && ne) {
     double const* eq = require_better ? m.qualities() : nullptr;
     UpAdj const& ev = m.ask_up(0, dim, false);
     double nel = m.counts[dim];
     PROBE(P_COARSEN_QUALITY, s, 4.0 * (nv + 1) + 8.0 * deg(dim, 0) * nel + 8.0 * ne +
         4.0 * deg(dim, 0) * nel + 24.0 * nv + 8.0 * ne + 16.0 * ne);
-    u32 blocks = (u32)std::min<u64>(ceil_div((u64)nc * 32, BLOCK), 148u * 64u);
+    // a warp per listed edge; the list's length is read on the device
+    u32 blocks = (u32)std::min<u64>(ceil_div((u64)ne * 32, BLOCK), 148u * 16u);
     k_coarsen_quality<<<blocks, BLOCK, 0, s>>>(dim, clist, ncand, voe1, m.ask_down(dim, 0),
         ev.offs, ev.adj, ev.dirs, m.coords(), eq, qual_floor, m.segview(),
         m.fp32_filter ? fp32_stats_dev() : nullptr, codes, sel.q2, any);
@@ -630,7 +625,13 @@ static bool coarsen_select(Mesh& m, u32* codes, double qual_floor, bool require_
   dev_free(clist, s);
   if (codes_qual_out)
     CK(cudaMemcpyAsync(codes_qual_out, codes, sizeof(u32) * ne, cudaMemcpyDeviceToDevice, s));
-  if (!read_u32(any, s)) return false;
+  m.mb->fetch(s, 8);
+  if (!m.mb->host[7]) return false;
+  // check_coarsen_quality (coarsen_common.cpp:139-180) ghosts a parallel
+  // mesh and exchanges the collapse codes whatever it then finds
+  m.ensure_ghosting(1);
+  m.note_exchange(1);
+  if (!m.mb->host[4]) return false;
   UpAdj const& ue = m.ask_up(0, 1);
   sel.cand = dalloc<u32>(nv, s);
   sel.colq = dalloc<double>(nv, s);
@@ -655,38 +656,9 @@ static void coarsen_build(Mesh& m, CoarsenSel const& sel)
   cudaStream_t s = m.s;
   u32 dim = m.dim, nv = m.count(0);
   u32* gen_offs_v = exscan_new(sel.ind, nv, s);
-  u32* same_v = negate_offsets(gen_offs_v, nv, s);
-  u32 nv_out = read_u32(same_v + nv, s);
-  last_pass_stats().nselected = nv - nv_out;
-  Mesh* out = m.spawn();
-  out->set_ents(0, nv_out, nullptr);
-  // tags_subset (subset.cpp:15-43): every vertex tag survives (one launch)
-  std::vector<ExpandJob> vjobs;
-  for (auto const& t : m.tags[0]) {
-    u32 esz = tag_esz(t.type);
-    void* d = dev_alloc((size_t)nv_out * t.ncomps * esz, s);
-    ExpandJob jb;
-    jb.in = t.data;
-    jb.offs = same_v;
-    jb.out = d;
-    jb.n = nv;
-    jb.width = t.ncomps;
-    jb.esz = esz;
-    vjobs.push_back(jb);
-    out->add_tag(0, t.type, t.name.c_str(), t.ncomps, t.transfer, d);
-  }
-  if (m.seg) {
-    out->seg = dalloc<u32>(nv_out, s);
-    ExpandJob jb;
-    jb.in = m.seg;
-    jb.offs = same_v;
-    jb.out = out->seg;
-    jb.n = nv;
-    jb.width = 1;
-    vjobs.push_back(jb);
-  }
-  expand_many(vjobs, s);
-  if (m.parallel) inherit_globals(*out, 0, nv_out);
+  // the surviving vertices' count lands in mailbox slot 22, read back with
+  // the other dimensions' counts
+  u32* same_v = negate_offsets(gen_offs_v, nv, s, m.mb->dev + 22);
   u32* fused[4] = {nullptr, nullptr, nullptr, nullptr};
   u32* same_of[4] = {nullptr, nullptr, nullptr, nullptr};
   u32 nsame_of[4] = {0, 0, 0, 0};
@@ -721,7 +693,38 @@ static void coarsen_build(Mesh& m, CoarsenSel const& sel)
     dev_free(will_gen, s);
     dev_free(is_same, s);
   }
-  m.mb->fetch(s, 22);
+  m.mb->fetch(s, 23);
+  u32 nv_out = m.mb->host[22];
+  last_pass_stats().nselected = nv - nv_out;
+  Mesh* out = m.spawn();
+  out->set_ents(0, nv_out, nullptr);
+  // tags_subset (subset.cpp:15-43): every vertex tag survives (one launch)
+  std::vector<ExpandJob> vjobs;
+  for (auto const& t : m.tags[0]) {
+    u32 esz = tag_esz(t.type);
+    void* d = dev_alloc((size_t)nv_out * t.ncomps * esz, s);
+    ExpandJob jb;
+    jb.in = t.data;
+    jb.offs = same_v;
+    jb.out = d;
+    jb.n = nv;
+    jb.width = t.ncomps;
+    jb.esz = esz;
+    vjobs.push_back(jb);
+    out->add_tag(0, t.type, t.name.c_str(), t.ncomps, t.transfer, d);
+  }
+  if (m.seg) {
+    out->seg = dalloc<u32>(nv_out, s);
+    ExpandJob jb;
+    jb.in = m.seg;
+    jb.offs = same_v;
+    jb.out = out->seg;
+    jb.n = nv;
+    jb.width = 1;
+    vjobs.push_back(jb);
+  }
+  expand_many(vjobs, s);
+  if (m.parallel) inherit_globals(*out, 0, nv_out);
   for (u32 dd = 0; dd < dim; ++dd) {
     u32 ed = dim - dd;
     u32 n = m.count(ed), vpe = deg(ed, 0);
@@ -810,8 +813,10 @@ u32 coarsen_by_size(Mesh& m, double qual_floor, double size_floor)
   Tag* h = m.find_tag(0, "adapt_size");
   if (!h) throw Failure(E_ARG, "mesh has no adapt_size vertex field");
   u32* codes = dalloc<u32>(ne, s);
+  // the codes kernel's "any code" flag (slot 5) is not read: with no code,
+  // the candidate list of coarsen_select comes back empty in its one
+  // read-back
   u32* any = m.mb->dev + 5;
-  CK(cudaMemsetAsync(any, 0, sizeof(u32), s));
   if (ne) {
     k_coarsen_size_codes<<<grid_for(ne), BLOCK, 0, s>>>(ne, m.ask_down(1, 0), m.coords(),
         static_cast<double const*>(h->data), size_floor, m.segview(),
@@ -820,7 +825,7 @@ u32 coarsen_by_size(Mesh& m, double qual_floor, double size_floor)
   }
   u32 r = 0;
   try {
-    if (read_u32(any, s)) r = coarsen_common(m, codes, qual_floor, false);
+    r = coarsen_common(m, codes, qual_floor, false);
   } catch (...) {
     dev_free(codes, s);
     throw;
@@ -846,8 +851,7 @@ u32 coarsen_slivers(Mesh& m, double qual_floor, u32 nlayers)
   m.note_exchange(0);
   dev_free(sl, s);
   u32* codes = dalloc<u32>(ne, s);
-  u32* any = m.mb->dev + 5;
-  CK(cudaMemsetAsync(any, 0, sizeof(u32), s));
+  u32* any = m.mb->dev + 5;  // not read (as in coarsen_by_size)
   if (ne) {
     k_coarsen_sliver_codes<<<grid_for(ne), BLOCK, 0, s>>>(ne, m.ask_down(1, 0), mv, codes, any);
     CK_LAUNCH();
@@ -855,7 +859,7 @@ u32 coarsen_slivers(Mesh& m, double qual_floor, u32 nlayers)
   dev_free(mv, s);
   u32 r = 0;
   try {
-    if (read_u32(any, s)) r = coarsen_common(m, codes, 0.0, true);
+    r = coarsen_common(m, codes, 0.0, true);
   } catch (...) {
     dev_free(codes, s);
     throw;

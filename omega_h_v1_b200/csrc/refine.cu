@@ -148,6 +148,7 @@ __global__ void k_refine_quality(u32 dim, u32 ne, u32 const* __restrict__ voe1,
     }
     }
   }
+  if (i < ne && !keep) out[i] = 0.0;  // every edge's goodness is written here
   if (__any_sync(0xffffffffu, keep) && (threadIdx.x & 31) == 0) atomicOr(any, 1u);
 }
 
@@ -403,7 +404,7 @@ static u32* choose_refinement(Mesh& m, u32* cand, double qual_floor, double** qu
   cudaStream_t s = m.s;
   u32 ne = m.count(1), dim = m.dim;
   double* q = dalloc<double>(ne, s);
-  CK(cudaMemsetAsync(q, 0, sizeof(double) * ne, s));
+  if (dim < 2) CK(cudaMemsetAsync(q, 0, sizeof(double) * ne, s));
   u32* any = m.mb->dev + 1;
   u32* inverted = m.mb->dev + 2;
   CK(cudaMemsetAsync(any, 0, 2 * sizeof(u32), s));

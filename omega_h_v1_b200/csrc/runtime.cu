@@ -626,11 +626,11 @@ u32* exscan_new(u32 const* in, u32 n, cudaStream_t s, u32* total_to)
   return out;
 }
 
-u32* negate_offsets(u32 const* offs, u32 n, cudaStream_t s)
+u32* negate_offsets(u32 const* offs, u32 n, cudaStream_t s, u32* total_to)
 {
   u32* o = dalloc<u32>((size_t)n + 1, s);
   if (n == 0) {
-    k_set_zero_total<<<1, 1, 0, s>>>(o, nullptr);
+    k_set_zero_total<<<1, 1, 0, s>>>(o, total_to);
     CK_LAUNCH();
     return o;
   }
@@ -639,7 +639,7 @@ u32* negate_offsets(u32 const* offs, u32 n, cudaStream_t s)
   {
     PROBE(P_EXSCAN, s, 4.0 * (n + 1) + 4.0 * (n + 1));
     k_exscan<1><<<ntiles, SCAN_THREADS, 0, s>>>(offs, o, n, ntiles,
-        reinterpret_cast<unsigned long long*>(scratch + 4), scratch, nullptr);
+        reinterpret_cast<unsigned long long*>(scratch + 4), scratch, total_to);
     CK_LAUNCH();
   }
   return o;

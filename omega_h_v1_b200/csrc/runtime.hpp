@@ -28,7 +28,7 @@ void exscan_u32_scratch(u32 const* in, u32* out, u32 n, u32* scratch, cudaStream
 void check_device_timeouts(cudaStream_t s);
 
 // out[i] = !(offs[i+1] - offs[i]) scanned (uints_negate_offsets, ints.cpp:227)
-u32* negate_offsets(u32 const* offs, u32 n, cudaStream_t s);
+u32* negate_offsets(u32 const* offs, u32 n, cudaStream_t s, u32* total_to = nullptr);
 
 void fill_u32(u32* a, u32 n, u32 v, cudaStream_t s);
 

@@ -301,6 +301,10 @@ __global__ void k_swap_quality(u32 ne, u32 const* __restrict__ te_offs,
       }
     }
   }
+  if (i < ne && !keep) {  // every edge's goodness and ring size is written here
+    quals[i] = 0.0;
+    ring_sizes[i] = 0;
+  }
   if (__any_sync(0xffffffffu, keep) && (threadIdx.x & 31) == 0) atomicOr(any, 1u);
 }
 
@@ -451,27 +455,22 @@ static bool swap_select(Mesh& m, double gq, u32 nlayers, SwapSel& sel, u32* sliv
   dev_free(sl, s);
   if (cand_out)
     CK(cudaMemcpyAsync(cand_out, sel.cand, sizeof(u32) * ne, cudaMemcpyDeviceToDevice, s));
-  if (!max_u32(sel.cand, ne, s)) {
-    if (interior_out)
-      CK(cudaMemcpyAsync(interior_out, sel.cand, sizeof(u32) * ne, cudaMemcpyDeviceToDevice, s));
-    return false;
-  }
+  if (!ne) return false;
   Tag* cd = m.find_tag(1, "class_dim");
   if (!cd) throw Failure(E_ARG, "swapping needs class_dim on edges");
+  // no read-back between the stages: an edge that is no candidate (no
+  // sliver, or on the boundary) is skipped by the quality kernel, whose
+  // "any swap kept" flag (mailbox slot 6) is the one read
   u32* any = m.mb->dev + 6;
-  CK(cudaMemsetAsync(any, 0, sizeof(u32), s));
+  CK(cudaMemsetAsync(m.mb->dev + 5, 0, 2 * sizeof(u32), s));  // slots 5-6
   k_unmark_boundary<<<grid_for(ne), BLOCK, 0, s>>>(ne, m.dim, static_cast<u32 const*>(cd->data),
-      sel.cand, any);
+      sel.cand, m.mb->dev + 5);
   CK_LAUNCH();
   if (interior_out)
     CK(cudaMemcpyAsync(interior_out, sel.cand, sizeof(u32) * ne, cudaMemcpyDeviceToDevice, s));
-  if (!read_u32(any, s)) return false;
   sel.quals = dalloc<double>(ne, s);
   sel.rs = dalloc<u32>(ne, s);
   sel.codes = dalloc<u32>(ne, s);
-  CK(cudaMemsetAsync(sel.quals, 0, sizeof(double) * ne, s));
-  CK(cudaMemsetAsync(sel.rs, 0, sizeof(u32) * ne, s));
-  CK(cudaMemsetAsync(any, 0, sizeof(u32), s));
   UpAdj const& te = m.ask_up(1, 3);
   double const* eq = m.qualities();
   PROBE(P_SWAP_QUALITY, s, 4.0 * (ne + 1) + 8.0 * 6.0 * m.counts[3] + 8.0 * ne +
