@@ -20,9 +20,12 @@ PassStats& last_pass_stats()
   return s;
 }
 
-__global__ void k_indset_init(u32 n, u32 const* __restrict__ filter, u32* __restrict__ st)
+// also zeroes the first round's "anything left" flag
+__global__ void k_indset_init(u32 n, u32 const* __restrict__ filter, u32* __restrict__ st,
+    u32* first_flag)
 {
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i == 0) *first_flag = 0;
   if (i < n) st[i] = filter[i] ? (u32)UNKNOWN : (u32)NOT_IN_SET;
 }
 
@@ -57,11 +60,14 @@ __device__ inline bool for_nbrs(Nbrs const& g, u32 i, F&& f)
 }
 
 // one round of indset_at_vert (indset.cpp:55-84) over all entities
+// unknown_left: this round's flag; next_flag: the next round's, zeroed here
+// (rounds alternate between two mailbox slots, so no memset precedes one)
 __global__ void k_indset_round(u32 n, Nbrs g, u32 const* __restrict__ old_st,
     u32* __restrict__ st, double const* __restrict__ good,
-    u64 const* __restrict__ glob, u32* unknown_left)
+    u64 const* __restrict__ glob, u32* unknown_left, u32* next_flag)
 {
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i == 0) *next_flag = 0;
   if (i >= n) return;
   u32 s0 = old_st[i];
   if (s0 != UNKNOWN) {
@@ -125,9 +131,10 @@ u32* find_indset(Mesh& m, u32 ent_dim, u32 const* filter, double const* good)
   double via_bytes = ent_dim == 0 ? 8.0 * m.counts[1] : 4.0 * g.per * m.counts[m.dim];
   u32* a = dalloc<u32>(n, m.s);
   u32* b = dalloc<u32>(n, m.s);
-  u32* flag = m.mb->dev + 0;
+  // the "anything left" flags of even and odd rounds (mailbox slots 0, 40)
+  u32 const flag_slot[2] = {0, 40};
   if (n) {
-    k_indset_init<<<grid_for(n), BLOCK, 0, m.s>>>(n, filter, a);
+    k_indset_init<<<grid_for(n), BLOCK, 0, m.s>>>(n, filter, a, m.mb->dev + flag_slot[0]);
     CK_LAUNCH();
   }
   // Rounds are issued in batches and the "anything left" flag is read once
@@ -140,21 +147,21 @@ u32* find_indset(Mesh& m, u32 ent_dim, u32 const* filter, double const* good)
     u32 batch = rounds == 0 ? 3u : 1u;
     if (rounds + batch > MAX_INDSET_ROUNDS) batch = MAX_INDSET_ROUNDS - rounds;
     for (u32 r = 0; r < batch; ++r) {
-      if (r + 1 == batch) CK(cudaMemsetAsync(flag, 0, sizeof(u32), m.s));
       // offsets, upward lists, the via-entities' down lists, states,
       // goodness and (parallel) globals read once; states written once
       double nuse = (double)read_cached_uses(m, ent_dim);
       PROBE(P_INDSET_ROUND, m.s, 4.0 * (n + 1.0) + 4.0 * nuse + via_bytes +
           4.0 * n + 8.0 * n + (glob ? 8.0 * n : 0.0) + 4.0 * n);
-      k_indset_round<<<grid_for(n), BLOCK, 0, m.s>>>(n, g, a, b, good, glob, flag);
+      k_indset_round<<<grid_for(n), BLOCK, 0, m.s>>>(n, g, a, b, good, glob,
+          m.mb->dev + flag_slot[rounds % 2], m.mb->dev + flag_slot[(rounds + 1) % 2]);
       CK_LAUNCH();
       std::swap(a, b);
       ++rounds;
     }
     // slots 1-3 come back too: a caller that left flags there reads them
     // after this call without a read-back of its own
-    m.mb->fetch(m.s, 4);
-    if (!m.mb->host[0]) done = true;
+    m.mb->fetch(m.s, 41);
+    if (!m.mb->host[flag_slot[(rounds - 1) % 2]]) done = true;
   }
   dev_free(b, m.s);
   last_pass_stats().indset_rounds = rounds;
