@@ -93,6 +93,8 @@ def serving_stream(count=200, seed=2, rate=200.0, tmin=2e3, tmax=2e6):
             h = (1.0 + 0.6 * rng.uniform()) / n
             out.append(BoxJob(i, n, h, i, None, t))
         else:
+            # the front offset is the first of three draws (the other two
+            # are unused; every non-uniform job takes three)
             c = tuple(0.3 + 0.4 * rng.uniform() for _ in range(3))
             min_h, max_h = 0.5 / n, 2.0 / n
             out.append(BoxJob(i, n, 0.0, i, None, t,
