@@ -669,6 +669,9 @@ static void coarsen_build(Mesh& m, CoarsenSel const& sel)
   u32* gen_offs_of[4] = {nullptr, nullptr, nullptr, nullptr};
   u32* gvert_of[4] = {nullptr, nullptr, nullptr, nullptr};
   u32* gdir_of[4] = {nullptr, nullptr, nullptr, nullptr};
+  // each kept entity's new id, written by the survivors' scan for the
+  // dimensions whose upward adjacency is carried
+  u32* newid_of[4] = {nullptr, nullptr, nullptr, nullptr};
   for (u32 dd = 0; dd < dim; ++dd) {
     u32 ed = dim - dd;
     u32 n = m.count(ed), vpe = deg(ed, 0);
@@ -689,7 +692,8 @@ static void coarsen_build(Mesh& m, CoarsenSel const& sel)
       CK_LAUNCH();
     }
     gen_offs_of[ed] = exscan_new(will_gen, n, s, m.mb->dev + 16 + 2 * (ed - 1));
-    same_of[ed] = exscan_new(is_same, n, s, m.mb->dev + 17 + 2 * (ed - 1));
+    if (carried_high(m, ed)) newid_of[ed] = dalloc<u32>(n ? n : 1, s);
+    same_of[ed] = exscan_new(is_same, n, s, m.mb->dev + 17 + 2 * (ed - 1), newid_of[ed]);
     dev_free(will_gen, s);
     dev_free(is_same, s);
   }
@@ -769,7 +773,7 @@ static void coarsen_build(Mesh& m, CoarsenSel const& sel)
       if (same_of[h] && same_of[l])
         carry_down(m, *out, h, l, same_of[h], nsame_of[h], same_of[l]);
   for (u32 h = 1; h <= dim; ++h) {
-    u32* newid = nullptr;
+    u32* newid = newid_of[h];
     for (u32 l = 0; l < h; ++l)
       if (same_of[h] && same_of[l])
         carry_up(m, *out, l, h, same_of[l], nsame_of[l], same_of[h], nsame_of[h], &newid);

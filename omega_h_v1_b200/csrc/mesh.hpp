@@ -204,6 +204,15 @@ void carry_up(Mesh& m, Mesh& out, u32 low, u32 high, u32 const* same_l, u32 nsam
     u32 const* same_h, u32 nsame_h, u32** newid_cache = nullptr);
 // new id of every old entity, or INV where it did not survive (caller frees)
 u32* carry_new_ids(u32 const* same, u32 n, cudaStream_t s);
+// whether a pass over m carries some upward adjacency of dimension `high`
+// (and so wants the new ids of its kept entities)
+inline bool carried_high(Mesh const& m, u32 high)
+{
+  if (high == 0 || high > 3) return false;
+  for (u32 l = 0; l < high; ++l)
+    if (m.have_up[l][high]) return true;
+  return false;
+}
 
 // derivation helpers (mesh.cu)
 void up_from_down(u32 high, u32 low, u32 nhighs, u32 nlows, u32 const* lows_of_highs,

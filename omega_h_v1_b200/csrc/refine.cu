@@ -310,11 +310,15 @@ static u32 refine_build(Mesh& m, u32 const* gen_offs)
   // products of every dimension (refine_common.cpp:90-123, inherit.cpp:104-138)
   u32* same_of[4] = {nullptr, nullptr, nullptr, nullptr};
   u32 nsame_of[4] = {0, 0, 0, 0};
+  // each kept entity's new id, written by the survivors' scan for the
+  // dimensions whose upward adjacency is carried
+  u32* newid_of[4] = {nullptr, nullptr, nullptr, nullptr};
   for (u32 prod = 0; prod <= dim; ++prod) {
     if (!m.full && 0 < prod && prod < dim) continue;
     u32 np = m.count(prod);
     Doms d;
-    u32* same = negate_offsets(sp[prod].offs, np, s);
+    if (carried_high(m, prod)) newid_of[prod] = dalloc<u32>(np ? np : 1, s);
+    u32* same = negate_offsets(sp[prod].offs, np, s, nullptr, newid_of[prod]);
     d.ndoms[0] = np;
     d.offs[0] = same;
     d.scale[0] = 1;
@@ -377,7 +381,7 @@ static u32 refine_build(Mesh& m, u32 const* gen_offs)
       if (same_of[h] && same_of[l])
         carry_down(m, *out, h, l, same_of[h], nsame_of[h], same_of[l]);
   for (u32 h = 1; h <= dim; ++h) {
-    u32* newid = nullptr;
+    u32* newid = newid_of[h];
     for (u32 l = 0; l < h; ++l)
       if (same_of[h] && same_of[l])
         carry_up(m, *out, l, h, same_of[l], nsame_of[l], same_of[h], nsame_of[h], &newid);

@@ -381,11 +381,14 @@ constexpr u32 SCAN_SPIN_LIMIT = 1u << 24;
 __device__ u32 d_wait_timeouts;
 
 // mode 0 scans in[i]; mode 1 scans (in[i + 1] == in[i]), i.e. the
-// survivors of an offsets array (uints_negate_offsets, ints.cpp:227-235)
+// survivors of an offsets array (uints_negate_offsets, ints.cpp:227-235).
+// newid (optional, for 0/1 items): out[i] where item i is 1, INV where 0 --
+// each old entity's new id when the items mark survivors
+
 template <int MODE>
 __global__ void __launch_bounds__(SCAN_THREADS)
 k_exscan(u32 const* __restrict__ in, u32* __restrict__ out, u32 n, u32 ntiles,
-    unsigned long long* status, u32* ticket_and_err, u32* total_to)
+    unsigned long long* status, u32* ticket_and_err, u32* total_to, u32* __restrict__ newid)
 {
   __shared__ u32 s_tile;
   __shared__ u32 s_warp[SCAN_WARPS];
@@ -486,7 +489,14 @@ k_exscan(u32 const* __restrict__ in, u32* __restrict__ out, u32 n, u32 ntiles,
   for (int k = 0; k < SCAN_ITEMS; ++k) {
     u32 li = k * SCAN_THREADS + threadIdx.x;
     size_t gi = base + li;
-    if (gi < n) out[gi] = s_buf[li + (li >> 5)];
+    if (gi < n) {
+      u32 const o = s_buf[li + (li >> 5)];
+      out[gi] = o;
+      if (newid) {
+        bool const on = MODE == 0 ? in[gi] != 0 : in[gi + 1] == in[gi];
+        newid[gi] = on ? o : INV;
+      }
+    }
   }
   if (tile == ntiles - 1 && threadIdx.x == 0) {
     out[n] = s_prefix + total;
@@ -565,7 +575,7 @@ u32* stream_scan_scratch(size_t words, cudaStream_t s)
 }
 }  // namespace
 
-void exscan_u32(u32 const* in, u32* out, u32 n, cudaStream_t s, u32* total_to)
+void exscan_u32(u32 const* in, u32* out, u32 n, cudaStream_t s, u32* total_to, u32* newid)
 {
   if (n == 0) {
     k_set_zero_total<<<1, 1, 0, s>>>(out, total_to);
@@ -578,7 +588,7 @@ void exscan_u32(u32 const* in, u32* out, u32 n, cudaStream_t s, u32* total_to)
   {
     PROBE(P_EXSCAN, s, 4.0 * n + 4.0 * (n + 1));
     k_exscan<0><<<ntiles, SCAN_THREADS, 0, s>>>(in, out, n, ntiles,
-        reinterpret_cast<unsigned long long*>(scratch + 4), scratch, total_to);
+        reinterpret_cast<unsigned long long*>(scratch + 4), scratch, total_to, newid);
     CK_LAUNCH();
   }
 }
@@ -615,18 +625,18 @@ void exscan_u32_scratch(u32 const* in, u32* out, u32 n, u32* scratch, cudaStream
   u32 ntiles = ceil_div(n, SCAN_TILE);
   CK(cudaMemsetAsync(scratch, 0, exscan_scratch_words(n) * sizeof(u32), s));
   k_exscan<0><<<ntiles, SCAN_THREADS, 0, s>>>(in, out, n, ntiles,
-      reinterpret_cast<unsigned long long*>(scratch + 4), scratch, nullptr);
+      reinterpret_cast<unsigned long long*>(scratch + 4), scratch, nullptr, nullptr);
   CK_LAUNCH();
 }
 
-u32* exscan_new(u32 const* in, u32 n, cudaStream_t s, u32* total_to)
+u32* exscan_new(u32 const* in, u32 n, cudaStream_t s, u32* total_to, u32* newid)
 {
   u32* out = dalloc<u32>((size_t)n + 1, s);
-  exscan_u32(in, out, n, s, total_to);
+  exscan_u32(in, out, n, s, total_to, newid);
   return out;
 }
 
-u32* negate_offsets(u32 const* offs, u32 n, cudaStream_t s, u32* total_to)
+u32* negate_offsets(u32 const* offs, u32 n, cudaStream_t s, u32* total_to, u32* newid)
 {
   u32* o = dalloc<u32>((size_t)n + 1, s);
   if (n == 0) {
@@ -639,7 +649,7 @@ u32* negate_offsets(u32 const* offs, u32 n, cudaStream_t s, u32* total_to)
   {
     PROBE(P_EXSCAN, s, 4.0 * (n + 1) + 4.0 * (n + 1));
     k_exscan<1><<<ntiles, SCAN_THREADS, 0, s>>>(offs, o, n, ntiles,
-        reinterpret_cast<unsigned long long*>(scratch + 4), scratch, total_to);
+        reinterpret_cast<unsigned long long*>(scratch + 4), scratch, total_to, newid);
     CK_LAUNCH();
   }
   return o;

@@ -16,8 +16,12 @@ void clear_error();
 // out[n] = sum(in). Single-pass decoupled look-back (uints_exscan, ints.cpp).
 // total_to (optional, device): receives out[n] as well (a mailbox slot the
 // host reads back with other flags, instead of a copy of its own)
-void exscan_u32(u32 const* in, u32* out, u32 n, cudaStream_t s, u32* total_to = nullptr);
-u32* exscan_new(u32 const* in, u32 n, cudaStream_t s, u32* total_to = nullptr);
+// newid (optional, device, n entries; for 0/1 inputs): out[i] where in[i]
+// is 1, INV where 0 -- the new id of each entity the flags mark as kept
+void exscan_u32(u32 const* in, u32* out, u32 n, cudaStream_t s, u32* total_to = nullptr,
+    u32* newid = nullptr);
+u32* exscan_new(u32 const* in, u32 n, cudaStream_t s, u32* total_to = nullptr,
+    u32* newid = nullptr);
 
 // The same scan with caller-provided scratch of at least
 // exscan_scratch_words(n) 32-bit words (zeroed here); allocates nothing.
@@ -28,7 +32,9 @@ void exscan_u32_scratch(u32 const* in, u32* out, u32 n, u32* scratch, cudaStream
 void check_device_timeouts(cudaStream_t s);
 
 // out[i] = !(offs[i+1] - offs[i]) scanned (uints_negate_offsets, ints.cpp:227)
-u32* negate_offsets(u32 const* offs, u32 n, cudaStream_t s, u32* total_to = nullptr);
+// newid (optional): out[i] where entity i is kept, INV where it is not
+u32* negate_offsets(u32 const* offs, u32 n, cudaStream_t s, u32* total_to = nullptr,
+    u32* newid = nullptr);
 
 void fill_u32(u32* a, u32 n, u32 v, cudaStream_t s);
 

@@ -517,6 +517,9 @@ static void swap_build(Mesh& m, SwapSel const& sel)
   // one read-back serves all dimensions
   u32 const ed0 = m.full ? 1u : dim;
   u32* gen_offs_of[4] = {nullptr, nullptr, nullptr, nullptr};
+  // each kept entity's new id, written by the survivors' scan for the
+  // dimensions whose upward adjacency is carried
+  u32* newid_of[4] = {nullptr, nullptr, nullptr, nullptr};
   for (u32 ed = ed0; ed <= dim; ++ed) {
     u32 n = m.count(ed);
     k_swap_counts<<<grid_for(ne), BLOCK, 0, s>>>(ne, ed, sel.ind, sel.rs, cnt);
@@ -528,7 +531,8 @@ static void swap_build(Mesh& m, SwapSel const& sel)
           sel.ind, same);
       CK_LAUNCH();
     }
-    same_of[ed] = exscan_new(same, n, s, m.mb->dev + 21 + 2 * (ed - 1));
+    if (carried_high(m, ed)) newid_of[ed] = dalloc<u32>(n ? n : 1, s);
+    same_of[ed] = exscan_new(same, n, s, m.mb->dev + 21 + 2 * (ed - 1), newid_of[ed]);
     dev_free(same, s);
   }
   dev_free(cnt, s);
@@ -599,7 +603,7 @@ static void swap_build(Mesh& m, SwapSel const& sel)
       if (same_of[h] && same_of[l])
         carry_down(m, *out, h, l, same_of[h], nsame_of[h], same_of[l]);
   for (u32 h = 1; h <= dim; ++h) {
-    u32* newid = nullptr;
+    u32* newid = newid_of[h];
     for (u32 l = 0; l < h; ++l)
       if (same_of[h] && same_of[l])
         carry_up(m, *out, l, h, same_of[l], nsame_of[l], same_of[h], nsame_of[h], &newid);
