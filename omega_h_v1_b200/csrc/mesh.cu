@@ -1090,6 +1090,79 @@ __global__ void k_up_surv_fill(u32 nl_old, u32 const* __restrict__ same_l,
   }
 }
 
+// The same two kernels for long rows (vertex rows, 8 or more uses on
+// average): a group of CARRY_GROUP lanes walks one row, each lane one use,
+// so a row's uses are read and written by consecutive lanes; a ballot over
+// the group gives each kept use its place, in the old order. (One thread
+// per long row issues loads whose lanes are a row apart and fills the
+// load/store queue.) Groups never straddle a warp; a group's lanes share
+// their row, so they loop and leave together.
+constexpr u32 CARRY_GROUP = 8;
+
+__global__ void k_up_surv_count_grouped(u32 nl_old, u32 nsame_l, u32 ntail,
+    u32 const* __restrict__ same_l, u32 const* __restrict__ newid_h,
+    u32 const* __restrict__ offs, u32 const* __restrict__ adj, u32* __restrict__ cnt,
+    u32* __restrict__ surv)
+{
+  u32 const t = blockIdx.x * blockDim.x + threadIdx.x;
+  u32 const j = t / CARRY_GROUP, g = t % CARRY_GROUP;
+  if (j >= nl_old) {
+    if (g == 0 && j - nl_old < ntail) {
+      u32 r = nsame_l + (j - nl_old);
+      cnt[r] = 0;
+      if (surv) surv[r] = 0;
+    }
+    return;
+  }
+  u32 const nj = same_l[j];
+  if (same_l[j + 1] == nj) return;
+  u32 const gbase = (threadIdx.x & 31) & ~(CARRY_GROUP - 1);
+  u32 const gmask = ((1u << CARRY_GROUP) - 1u) << gbase;
+  u32 const e = offs[j + 1];
+  u32 c = 0;
+  for (u32 base = offs[j]; base < e; base += CARRY_GROUP) {
+    u32 const u = base + g;
+    bool const keep = u < e && newid_h[adj[u]] != INV;
+    c += __popc(__ballot_sync(gmask, keep) & gmask);
+  }
+  if (g == 0) {
+    cnt[nj] = c;
+    if (surv) surv[nj] = c;
+  }
+}
+
+__global__ void k_up_surv_fill_grouped(u32 nl_old, u32 const* __restrict__ same_l,
+    u32 const* __restrict__ newid_h, u32 const* __restrict__ offs_old,
+    u32 const* __restrict__ adj_old, u32 const* __restrict__ dirs_old,
+    u32 const* __restrict__ offs, u32* __restrict__ adj, u32* __restrict__ dirs)
+{
+  u32 const t = blockIdx.x * blockDim.x + threadIdx.x;
+  u32 const j = t / CARRY_GROUP, g = t % CARRY_GROUP;
+  if (j >= nl_old) return;
+  u32 const nj = same_l[j];
+  if (same_l[j + 1] == nj) return;
+  u32 const gbase = (threadIdx.x & 31) & ~(CARRY_GROUP - 1);
+  u32 const gmask = ((1u << CARRY_GROUP) - 1u) << gbase;
+  u32 const below = (1u << g) - 1u;
+  u32 w = offs[nj];
+  u32 const e = offs_old[j + 1];
+  for (u32 base = offs_old[j]; base < e; base += CARRY_GROUP) {
+    u32 const u = base + g;
+    u32 na = INV, d = 0;
+    if (u < e) {
+      na = newid_h[adj_old[u]];
+      d = dirs_old[u];
+    }
+    u32 const kept = (__ballot_sync(gmask, na != INV) & gmask) >> gbase;
+    if (na != INV) {
+      u32 const pos = w + __popc(kept & below);
+      adj[pos] = na;
+      dirs[pos] = d;
+    }
+    w += __popc(kept);
+  }
+}
+
 // cnt holds each row's kept + generated uses: the generated ones take the
 // slots after the kept ones, from the row's end down (their order within a
 // row is arbitrary either way: the rows are marked unsorted)
@@ -1146,11 +1219,17 @@ void carry_up(Mesh& m, Mesh& out, u32 low, u32 high, u32 const* same_l, u32 nsam
   u32* cnt = dalloc<u32>((size_t)nl + 1, s);
   u32* surv = m.up_sorted[low][high] ? dalloc<u32>((size_t)nl + 1, s) : nullptr;
   u32 nuses_old = m.counts[high] * lph;
+  // rows of 8 or more uses on average (vertex rows) take a lane group each
+  bool const long_rows = nl_old && (u64)nuses_old >= (u64)CARRY_GROUP * nl_old;
   {
     u32 ntail = nl + 1 - nsame_l;
     PROBE(P_CARRY_UP, s, 8.0 * (nl_old + 1) + 4.0 * nuses_old + 8.0 * nuses_old + 8.0 * nl);
-    k_up_surv_count<<<grid_for((u64)nl_old + ntail), BLOCK, 0, s>>>(nl_old, nsame_l, ntail,
-        same_l, newid_h, old.offs, old.adj, cnt, surv);
+    if (long_rows)
+      k_up_surv_count_grouped<<<grid_for(((u64)nl_old + ntail) * CARRY_GROUP), BLOCK, 0, s>>>(
+          nl_old, nsame_l, ntail, same_l, newid_h, old.offs, old.adj, cnt, surv);
+    else
+      k_up_surv_count<<<grid_for((u64)nl_old + ntail), BLOCK, 0, s>>>(nl_old, nsame_l, ntail,
+          same_l, newid_h, old.offs, old.adj, cnt, surv);
     CK_LAUNCH();
   }
   if (nuses > first) {
@@ -1164,8 +1243,12 @@ void carry_up(Mesh& m, Mesh& out, u32 low, u32 high, u32 const* same_l, u32 nsam
   u.dirs = dalloc<u32>(nuses, s);
   if (nl_old) {
     PROBE(P_CARRY_UP, s, 8.0 * (nl_old + 1) + 12.0 * nuses_old + 8.0 * nuses_old + 4.0 * nl);
-    k_up_surv_fill<<<grid_for(nl_old), BLOCK, 0, s>>>(nl_old, same_l, newid_h, old.offs,
-        old.adj, old.dirs, u.offs, u.adj, u.dirs);
+    if (long_rows)
+      k_up_surv_fill_grouped<<<grid_for((u64)nl_old * CARRY_GROUP), BLOCK, 0, s>>>(nl_old,
+          same_l, newid_h, old.offs, old.adj, old.dirs, u.offs, u.adj, u.dirs);
+    else
+      k_up_surv_fill<<<grid_for(nl_old), BLOCK, 0, s>>>(nl_old, same_l, newid_h, old.offs,
+          old.adj, old.dirs, u.offs, u.adj, u.dirs);
     CK_LAUNCH();
   }
   if (nuses > first) {
