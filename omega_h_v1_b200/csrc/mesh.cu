@@ -1003,11 +1003,13 @@ void carry_down(Mesh& m, Mesh& out, u32 high, u32 low, u32 const* same_h, u32 ns
 // its old row whose high entity survived, in the old order, mapped to new
 // ids, followed by the uses of the entities the pass made; a low the pass
 // made has only such uses (a surviving high entity's lows all survive).
-// One thread walks one old row, four uses at a time with their loads issued
-// together; newid_h holds each old high entity's new id or INV, one gather
-// per use. (Measured alternatives: a lane group per row left too few rows in
-// flight and ran at half the speed; a warp per 32 rows reading their uses
-// coalesced ran at the same speed as this.)
+// On short rows (edges, faces) one thread walks one old row, four uses at a
+// time with their loads issued together; long rows (vertices) take a lane
+// group each (the _grouped kernels below). newid_h holds each old high
+// entity's new id or INV, one gather per use. (Measured alternatives: a
+// lane group for every row left too few short rows in flight and ran at
+// half the speed; a warp per 32 rows reading their uses coalesced ran at
+// the same speed as a thread per row.)
 __global__ void k_new_ids(u32 n, u32 const* __restrict__ same, u32* __restrict__ newid)
 {
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
