@@ -111,7 +111,21 @@ void stream_sync(cudaStream_t s);
 // device-to-host reads (a read into pageable memory is staged by the driver)
 void* pinned_scratch();
 
-// small pinned host mailbox for reading several device scalars at once
+// small pinned host mailbox for reading several device scalars at once.
+// Slots, by the step that writes them (steps of one mesh run one at a time,
+// so steps that never overlap share slots):
+//   0, 40   independent-set rounds' "anything left" flags (even, odd rounds)
+//   1-3     refinement: any good candidate, any inverted child, any candidate
+//   4-7     coarsening selection: any collapse kept (4), codes flag (5, not
+//           read), listed candidates (7); swap selection: interior
+//           candidates (5, not read), any swap kept (6)
+//   8-11    refinement build: split entities per domain dimension
+//   16-22   coarsening build: products and survivors per dimension, kept
+//           vertices (22)
+//   20-25   swap build: products and survivors per dimension
+//   24-25   classification (derive_model)
+//   30-31   size fields (a 64-bit word)
+//   60-61   adjacency derivation error flags
 struct Mailbox {
   u32* host = nullptr;   // pinned
   u32* dev = nullptr;    // device, 64 slots
