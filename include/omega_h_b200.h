@@ -280,6 +280,13 @@ unsigned long long osh_b200_sync_count(void) OSH_PUBLIC;
    stream synchronisations spent waiting for the device (diagnostics of the
    host side of a pass) */
 void osh_b200_host_stats(unsigned long long* allocs, double* sync_wait_seconds) OSH_PUBLIC;
+/* self-test of the scans' bounded wait (no counterpart in the reference,
+   whose Thrust scan has none): runs one scan whose second tile waits for a
+   first tile that never publishes, with a wait limit of spin_limit polls.
+   Returns OSH_B200_E_TIMEOUT when the wait gave up and was reported (the
+   expected result), 0 if it did not, or another error code; the device
+   stays usable afterwards. */
+int osh_b200_selftest_scan_wait(unsigned spin_limit) OSH_PUBLIC;
 /* run all further work of mesh m on the CUDA stream `stream` (a
    cudaStream_t; 0 is the legacy default stream); the caller keeps it alive */
 void osh_b200_set_stream(osh_t m, void* stream) OSH_PUBLIC;
@@ -296,25 +303,29 @@ void osh_b200_probe_read(unsigned id, unsigned* launches, double* total_ms,
 
 /* ---- upward adjacency without device allocation -------------------------- */
 /* No counterpart in the reference. For callers that cannot allocate device
-   memory when they need it: work issued while a stream is captured into a
-   CUDA graph, host callbacks and real-time loops that must not wait on the
-   allocator, and host codes that give the GPU a fixed memory budget.
+   memory when they need the adjacency: host callbacks and real-time loops
+   that must not wait on the allocator, and host codes that give the GPU a
+   fixed memory budget and own every byte of it.
    Computes the same upward adjacency as osh_up_offs / osh_up / osh_up_dirs
    (rows sorted by use index) from a device array lows_of_highs of
-   nhighs * deg(high_dim, low_dim) entries into caller-allocated device arrays
-   offsets[nlows + 1], highs_of_lows[nuses] and directions[nuses], enqueued
-   on `stream` (a cudaStream_t, 0 = legacy default stream) without
-   synchronising. It calls no allocator: its scratch is one fixed device
-   array inside the library (about 8.4 MB, held by every GPU that loads the
-   library until the process exits), so the sizes are capped at
-   OSH_B200_NOALLOC_MAX_USES uses and OSH_B200_NOALLOC_MAX_LOWS rows; larger
-   requests return OSH_B200_E_ARG without launching anything. The first call
-   on each device looks up the array's device address, so make it before any
-   stream capture on that device. Every call shares the one array and each
-   clears what it needs, so calls that may run at the same time on the GPU
-   (different streams, no ordering between them) race and must not be
-   issued. Returns 0, or the error code also recorded for
-   osh_b200_last_error(). */
+   nuses = nhighs * deg(high_dim, low_dim) entries into caller-allocated
+   device arrays offsets[nlows + 1], highs_of_lows[nuses] and
+   directions[nuses], enqueued on `stream` (a cudaStream_t, 0 = legacy
+   default stream) without synchronising. It calls no allocator: its scratch
+   is one fixed device array inside the library (about 8.4 MB, held by every
+   GPU that loads the library until the process exits), so the sizes are
+   capped at OSH_B200_NOALLOC_MAX_USES uses and OSH_B200_NOALLOC_MAX_LOWS
+   rows; larger requests return OSH_B200_E_ARG without launching anything.
+   The first call on each device looks up the array's device address (with
+   that device current), so make it before any stream capture on that
+   device. Every call shares the one array and clears what it needs; calls
+   that may run at the same time on the GPU (different streams, no ordering
+   between them) race and must not be issued. Failures found on the device
+   (an entry of lows_of_highs not below nlows, a bounded wait that gave up)
+   write nothing through a computed index and leave 0xffffffff in
+   offsets[nlows], which holds nuses after a successful call: read it once
+   the stream's work is done. Returns 0, or the error code also recorded
+   for osh_b200_last_error(). */
 #define OSH_B200_NOALLOC_MAX_USES (1u << 20)
 #define OSH_B200_NOALLOC_MAX_LOWS (1u << 20)
 int osh_b200_up_from_down_noalloc(unsigned high_dim, unsigned low_dim,

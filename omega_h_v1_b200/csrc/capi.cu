@@ -614,9 +614,7 @@ int osh_b200_server_step(osh_b200_server_t sv)
 {
   API_TRY
   need(sv != nullptr, "server is NULL");
-  u32 r = osh::server_step(SV(sv));
-  osh::check_device_timeouts(nullptr);
-  return (int)r;
+  return (int)osh::server_step(SV(sv));
   API_CATCH(-1)
 }
 
@@ -1131,6 +1129,13 @@ unsigned long long osh_b200_sync_count(void) { return osh::sync_count(); }
 void osh_b200_host_stats(unsigned long long* allocs, double* sync_wait_seconds)
 {
   osh::host_stats(allocs, sync_wait_seconds);
+}
+
+int osh_b200_selftest_scan_wait(unsigned spin_limit)
+{
+  API_TRY
+  return osh::selftest_scan_wait(spin_limit);
+  API_CATCH(osh::last_error())
 }
 
 void osh_b200_set_stream(osh_t h, void* stream)

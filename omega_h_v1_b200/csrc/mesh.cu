@@ -564,42 +564,6 @@ void up_from_down(u32 high, u32 low, u32 nhighs, u32 nlows, u32 const* loh,
   dev_free(cnt, s);
 }
 
-// word offsets of the scratch regions, each starting on a 256-byte boundary
-// (the scan's tile status is read and written as 64-bit words)
-static size_t align64w(size_t w) { return (w + 63) & ~(size_t)63; }
-
-size_t up_from_down_scratch_words(u32 nuses, u32 nlows)
-{
-  // counts (nlows + 1), the unsorted rows (nuses), the scan's scratch
-  size_t tmp = align64w((size_t)nlows + 1);
-  size_t scan = align64w(tmp + nuses);
-  return scan + exscan_scratch_words(nlows);
-}
-
-void up_from_down_scratch(u32 high, u32 low, u32 nhighs, u32 nlows, u32 const* loh,
-    UpAdj const& out, u32* scratch, cudaStream_t s)
-{
-  u32 lph = deg(high, low);
-  u32 nuses = nhighs * lph;
-  u32* cnt = scratch;
-  u32* tmp = scratch + align64w((size_t)nlows + 1);
-  u32* scan = scratch + align64w(align64w((size_t)nlows + 1) + nuses);
-  CK(cudaMemsetAsync(cnt, 0, sizeof(u32) * ((size_t)nlows + 1), s));
-  if (nuses) {
-    k_count_lows<<<grid_for(nuses), BLOCK, 0, s>>>(loh, nuses, cnt);
-    CK_LAUNCH();
-  }
-  exscan_u32_scratch(cnt, out.offs, nlows, scan, s);
-  if (nuses) {
-    k_fill_uses<<<grid_for(nuses), BLOCK, 0, s>>>(loh, nuses, out.offs, cnt, tmp);
-    CK_LAUNCH();
-    u64 threads = (u64)nlows * 32;
-    k_rank_rows<<<grid_for(threads), BLOCK, 0, s>>>(out.offs, tmp, nlows, lph, out.adj,
-        out.dirs);
-    CK_LAUNCH();
-  }
-}
-
 // ---------------------------------------------------------------------------
 // downward adjacency by search (reflect_down.cpp:13-81)
 

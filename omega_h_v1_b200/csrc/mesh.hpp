@@ -224,10 +224,4 @@ void up_from_down_unsorted(u32 high, u32 low, u32 nhighs, u32 nlows,
 void sort_up_rows(u32 high, u32 low, u32 nhighs, u32 nlows, UpAdj const& u,
     cudaStream_t s);
 
-// up_from_down into caller-provided outputs, with caller-provided scratch of
-// up_from_down_scratch_words(nuses, nlows) 32-bit words; allocates nothing
-size_t up_from_down_scratch_words(u32 nuses, u32 nlows);
-void up_from_down_scratch(u32 high, u32 low, u32 nhighs, u32 nlows,
-    u32 const* lows_of_highs, UpAdj const& out, u32* scratch, cudaStream_t s);
-
 }  // namespace osh

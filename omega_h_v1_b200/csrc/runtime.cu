@@ -363,8 +363,10 @@ void Mailbox::fetch(cudaStream_t s, u32 nslots)
 // Tiles are claimed through an atomic ticket, so every tile a block waits on
 // was claimed (and is running or done) before it. Each tile publishes its
 // aggregate, then walks back over predecessors until it meets an inclusive
-// prefix. The walk is bounded: after SCAN_SPIN_LIMIT empty polls it records
-// E_TIMEOUT in the error word and stops instead of spinning forever.
+// prefix. The walk is bounded: after spin_limit empty polls (SCAN_SPIN_LIMIT
+// in every scan the passes issue) it sets the scratch's error word, which
+// the host reads for that stream (check_device_timeouts), and stops instead
+// of spinning forever.
 
 // 8192-element tiles: a 2M-element scan has 256 tiles, so a tile's
 // look-back meets a published prefix within a few steps (with 2048-element
@@ -377,9 +379,6 @@ constexpr unsigned long long FLAG_AGG = 1ull << 62;
 constexpr unsigned long long FLAG_PRE = 2ull << 62;
 constexpr u32 SCAN_SPIN_LIMIT = 1u << 24;
 
-// set by any bounded device wait that gave up; read by check_device_timeouts
-__device__ u32 d_wait_timeouts;
-
 // mode 0 scans in[i]; mode 1 scans (in[i + 1] == in[i]), i.e. the
 // survivors of an offsets array (uints_negate_offsets, ints.cpp:227-235).
 // newid (optional, for 0/1 items): out[i] where item i is 1, INV where 0 --
@@ -388,7 +387,8 @@ __device__ u32 d_wait_timeouts;
 template <int MODE>
 __global__ void __launch_bounds__(SCAN_THREADS)
 k_exscan(u32 const* __restrict__ in, u32* __restrict__ out, u32 n, u32 ntiles,
-    unsigned long long* status, u32* ticket_and_err, u32* total_to, u32* __restrict__ newid)
+    unsigned long long* status, u32* ticket_and_err, u32* total_to, u32* __restrict__ newid,
+    u32 spin_limit)
 {
   __shared__ u32 s_tile;
   __shared__ u32 s_warp[SCAN_WARPS];
@@ -453,14 +453,14 @@ k_exscan(u32 const* __restrict__ in, u32* __restrict__ out, u32 n, u32 ntiles,
         unsigned long long st = FLAG_PRE;  // before tile 0: an empty prefix
         if (idx >= 0) st = *((volatile unsigned long long*)&status[idx]);
         while (__any_sync(0xffffffffu, (st >> 62) == 0)) {
-          if (++spins > SCAN_SPIN_LIMIT) {
+          if (++spins > spin_limit) {
             gave_up = true;
             break;
           }
           if (idx >= 0 && (st >> 62) == 0) st = *((volatile unsigned long long*)&status[idx]);
         }
         if (gave_up) {
-          if (lane == 0) atomicOr(&d_wait_timeouts, 1u);
+          if (lane == 0) atomicOr(&ticket_and_err[1], 1u);
           break;
         }
         u32 pre = __ballot_sync(0xffffffffu, (st & (3ull << 62)) == FLAG_PRE);
@@ -588,24 +588,65 @@ void exscan_u32(u32 const* in, u32* out, u32 n, cudaStream_t s, u32* total_to, u
   {
     PROBE(P_EXSCAN, s, 4.0 * n + 4.0 * (n + 1));
     k_exscan<0><<<ntiles, SCAN_THREADS, 0, s>>>(in, out, n, ntiles,
-        reinterpret_cast<unsigned long long*>(scratch + 4), scratch, total_to, newid);
+        reinterpret_cast<unsigned long long*>(scratch + 4), scratch, total_to, newid,
+        SCAN_SPIN_LIMIT);
     CK_LAUNCH();
   }
 }
 
+// The scans of one stream record a look-back that gave up in word 1 of that
+// stream's scratch (the last tile clears words 0 and 2 only), so a stream's
+// check sees its own scans' timeouts and no other stream's.
 void check_device_timeouts(cudaStream_t s)
 {
-  u32 v = 0;
-  CK(cudaMemcpyFromSymbolAsync(&v, d_wait_timeouts, sizeof(u32), 0,
-      cudaMemcpyDeviceToHost, s));
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  u32* p = nullptr;
+  {
+    std::lock_guard<std::mutex> g(g_scan_mu);
+    auto& all = scan_scratches();
+    auto it = all.find({dev, s});
+    if (it != all.end()) p = it->second.p;
+  }
+  if (!p) return;
+  u32* h = static_cast<u32*>(pinned_scratch());
+  CK(cudaMemcpyAsync(h, p + 1, sizeof(u32), cudaMemcpyDeviceToHost, s));
   stream_sync(s);
-  if (v) {
-    u32 zero = 0;
-    CK(cudaMemcpyToSymbolAsync(d_wait_timeouts, &zero, sizeof(u32), 0,
-        cudaMemcpyHostToDevice, s));
+  if (*h) {
+    CK(cudaMemsetAsync(p + 1, 0, sizeof(u32), s));
     stream_sync(s);
     throw Failure(E_TIMEOUT, "a bounded device wait gave up (scan look-back)");
   }
+}
+
+int selftest_scan_wait(u32 spin_limit)
+{
+  // Two tiles, the ticket counter starting at 1: the block that takes tile
+  // 1 waits for tile 0, which no block takes, until spin_limit polls have
+  // gone by; the block that takes ticket 2 has no tile and returns.
+  cudaStream_t s = nullptr;
+  CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  u32 const n = 2 * SCAN_TILE, ntiles = 2;
+  size_t words = (size_t)(n + 1) * 2 + 4 + 2 * ntiles + 4;  // + alignment room
+  u32* buf = nullptr;
+  CK(cudaMalloc(&buf, words * sizeof(u32)));
+  u32* in = buf;
+  u32* out = buf + n + 1;
+  u32* scratch = buf + 2 * (size_t)(n + 1);
+  scratch += (4 - (reinterpret_cast<uintptr_t>(scratch) / 4) % 4) % 4;  // 16-byte aligned
+  CK(cudaMemsetAsync(buf, 0, words * sizeof(u32), s));
+  u32 one = 1;
+  CK(cudaMemcpyAsync(scratch, &one, sizeof(u32), cudaMemcpyHostToDevice, s));
+  k_exscan<0><<<ntiles, SCAN_THREADS, 0, s>>>(in, out, n, ntiles,
+      reinterpret_cast<unsigned long long*>(scratch + 4), scratch, nullptr, nullptr,
+      spin_limit);
+  CK_LAUNCH();
+  u32 err = 0;
+  CK(cudaMemcpyAsync(&err, scratch + 1, sizeof(u32), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  CK(cudaFree(buf));
+  CK(cudaStreamDestroy(s));
+  return err ? E_TIMEOUT : E_OK;
 }
 
 size_t exscan_scratch_words(u32 n)
@@ -625,7 +666,8 @@ void exscan_u32_scratch(u32 const* in, u32* out, u32 n, u32* scratch, cudaStream
   u32 ntiles = ceil_div(n, SCAN_TILE);
   CK(cudaMemsetAsync(scratch, 0, exscan_scratch_words(n) * sizeof(u32), s));
   k_exscan<0><<<ntiles, SCAN_THREADS, 0, s>>>(in, out, n, ntiles,
-      reinterpret_cast<unsigned long long*>(scratch + 4), scratch, nullptr, nullptr);
+      reinterpret_cast<unsigned long long*>(scratch + 4), scratch, nullptr, nullptr,
+      SCAN_SPIN_LIMIT);
   CK_LAUNCH();
 }
 
@@ -649,7 +691,8 @@ u32* negate_offsets(u32 const* offs, u32 n, cudaStream_t s, u32* total_to, u32* 
   {
     PROBE(P_EXSCAN, s, 4.0 * (n + 1) + 4.0 * (n + 1));
     k_exscan<1><<<ntiles, SCAN_THREADS, 0, s>>>(offs, o, n, ntiles,
-        reinterpret_cast<unsigned long long*>(scratch + 4), scratch, total_to, newid);
+        reinterpret_cast<unsigned long long*>(scratch + 4), scratch, total_to, newid,
+        SCAN_SPIN_LIMIT);
     CK_LAUNCH();
   }
   return o;

@@ -30,6 +30,9 @@ void exscan_u32_scratch(u32 const* in, u32* out, u32 n, u32* scratch, cudaStream
 
 // throws E_TIMEOUT if a bounded device-side wait gave up since the last check
 void check_device_timeouts(cudaStream_t s);
+// one scan whose second tile waits for a first tile that never publishes,
+// with a wait limit of spin_limit polls: E_TIMEOUT when the wait gave up
+int selftest_scan_wait(u32 spin_limit);
 
 // out[i] = !(offs[i+1] - offs[i]) scanned (uints_negate_offsets, ints.cpp:227)
 // newid (optional): out[i] where entity i is kept, INV where it is not

@@ -219,6 +219,7 @@ struct Server {
     steps += 1;
     u32 u0 = last_batch_stats().unions;
     run.step(ms, st, owned);
+    check_device_timeouts(run.s);
     unions += last_batch_stats().unions - u0;
     double t_c = now_s();
     secs_passes += t_c - t_b;

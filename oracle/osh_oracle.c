@@ -18,7 +18,7 @@
  * doubles_min skips element 0, doubles.cpp:111-118), this restatement follows
  * the OpenMP/CUDA semantics: the minimum over all elements.
  *
- * Parity pin: tests/test_oracle_pin.py runs this restatement and the
+ * Parity pin: tests/test_oracle.py runs this restatement and the
  * reference itself (compiled from its own sources into oracle/_ref/ by
  * oracle/Makefile) on the same seeded inputs and requires identical meshes.
  */
