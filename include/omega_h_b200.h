@@ -131,6 +131,26 @@ void osh_b200_set_fp32_filter(osh_t m, int on) OSH_PUBLIC;
 void osh_b200_fp32_stats(unsigned long long* decided, unsigned long long* rechecked,
     double* max_error, unsigned* bound_exceeded) OSH_PUBLIC;
 void osh_b200_fp32_stats_reset(void) OSH_PUBLIC;
+/* Audit mode (device-wide, off by default; for tests): every decision the
+   filter takes on an estimate is also taken in double, and every estimate
+   whose double value is computed is checked against its bound. Counters:
+   decisions audited, audited decisions the double path takes differently
+   (always 0 when the bound holds), estimates checked (bound_exceeded of
+   osh_b200_fp32_stats then covers all of them). */
+void osh_b200_set_fp32_audit(int on) OSH_PUBLIC;
+void osh_b200_fp32_audit_stats(unsigned long long* audited, unsigned long long* flips,
+    unsigned long long* checked) OSH_PUBLIC;
+/* The filter's device estimates for caller-given inputs, beside the double
+   values the passes compute (host arrays). Tets: 12 coordinates each (four
+   vertices); est / err: the single-precision quality and its bound (+inf:
+   no bound), q64: tet_quality (quality.hpp:68-89). Edges: 6 coordinates and
+   2 sizes each; side: +1 / -1 when the estimate places the metric length
+   (size.cpp:57-69) above / below thr, 0 undecided; ratio64: the double
+   metric length. */
+void osh_b200_fp32_probe_tets(unsigned n, double const* host_x, float* host_est,
+    float* host_err, double* host_q64) OSH_PUBLIC;
+void osh_b200_fp32_probe_edges(unsigned n, double const* host_x, double const* host_h,
+    double thr, int* host_side, double* host_ratio64) OSH_PUBLIC;
 
 /* ---- device memory -------------------------------------------------------- */
 /* All device memory of this library comes from the current device's default

@@ -156,6 +156,13 @@ def lib():
     f("osh_b200_fp32_stats", None, C.POINTER(C.c_ulonglong), C.POINTER(C.c_ulonglong),
       C.POINTER(C.c_double), C.POINTER(C.c_uint))
     f("osh_b200_fp32_stats_reset", None)
+    f("osh_b200_set_fp32_audit", None, C.c_int)
+    f("osh_b200_fp32_audit_stats", None, *([C.POINTER(C.c_ulonglong)] * 3))
+    f("osh_b200_fp32_probe_tets", None, C.c_uint, _f64p, np.ctypeslib.ndpointer(np.float32),
+      np.ctypeslib.ndpointer(np.float32), _f64p)
+    f("osh_b200_fp32_probe_edges", None, C.c_uint, _f64p, _f64p, C.c_double,
+      np.ctypeslib.ndpointer(np.int32), _f64p)
+    f("osh_b200_selftest_scan_wait", C.c_int, C.c_uint)
     f("osh_b200_server_new", vp, C.c_double, C.c_double, C.c_uint, C.c_uint, C.c_ulonglong)
     f("osh_b200_server_free", None, vp)
     f("osh_b200_server_submit", C.c_int, vp, C.c_uint, C.c_uint, _f64p, C.c_uint, _u32p, _f64p)
@@ -533,6 +540,49 @@ def fp32_stats(reset=False):
         L.osh_b200_fp32_stats_reset()
         check()
     return dict(decided=d.value, rechecked=r.value, max_error=e.value, bound_exceeded=b.value)
+
+
+def set_fp32_audit(on=True):
+    """Audit mode of the filter (device-wide): every decision taken on an
+    estimate is also taken in double and compared."""
+    lib().osh_b200_set_fp32_audit(1 if on else 0)
+    check()
+
+
+def fp32_audit_stats():
+    """(decisions audited, audited decisions the double path takes
+    differently, estimates checked against their double value)."""
+    L = lib()
+    a, f, c = C.c_ulonglong(), C.c_ulonglong(), C.c_ulonglong()
+    L.osh_b200_fp32_audit_stats(C.byref(a), C.byref(f), C.byref(c))
+    check()
+    return dict(audited=a.value, flips=f.value, checked=c.value)
+
+
+def fp32_probe_tets(tets_xyz):
+    """Device estimates for tets given as an (n, 4, 3) array: (estimate,
+    bound, double quality)."""
+    x = np.ascontiguousarray(tets_xyz, dtype=np.float64).reshape(-1)
+    n = x.size // 12
+    est = np.empty(n, np.float32)
+    err = np.empty(n, np.float32)
+    q64 = np.empty(n, np.float64)
+    lib().osh_b200_fp32_probe_tets(n, x, est, err, q64)
+    check()
+    return est, err, q64
+
+
+def fp32_probe_edges(ends_xyz, sizes, thr):
+    """Device side decisions for edges given as an (n, 2, 3) array of end
+    points and (n, 2) sizes: (side, double metric length)."""
+    x = np.ascontiguousarray(ends_xyz, dtype=np.float64).reshape(-1)
+    h = np.ascontiguousarray(sizes, dtype=np.float64).reshape(-1)
+    n = x.size // 6
+    side = np.empty(n, np.int32)
+    r64 = np.empty(n, np.float64)
+    lib().osh_b200_fp32_probe_edges(n, x, h, float(thr), side, r64)
+    check()
+    return side, r64
 
 
 def pool_reserve(nbytes):

@@ -51,6 +51,7 @@ template <class T>
 __global__ void k_concat(u32 nm, T const* const* __restrict__ src, u32 const* __restrict__ offs,
     u32 width, T const* __restrict__ add, T* __restrict__ out)
 {
+  pdl_wait();
   u64 total = (u64)offs[nm] * width;
   for (u64 j = blockIdx.x * (u64)blockDim.x + threadIdx.x; j < total;
        j += (u64)gridDim.x * blockDim.x) {
@@ -66,6 +67,7 @@ __global__ void k_concat(u32 nm, T const* const* __restrict__ src, u32 const* __
 __global__ void k_seg_concat(u32 nm, u32 const* __restrict__ offs,
     u32 const* const* __restrict__ src, u32 const* __restrict__ base, u32* __restrict__ out)
 {
+  pdl_wait();
   u32 total = offs[nm];
   for (u32 j = blockIdx.x * blockDim.x + threadIdx.x; j < total; j += gridDim.x * blockDim.x) {
     u32 k = find_seg(nm, offs, j);
@@ -78,6 +80,7 @@ __global__ void k_seg_concat(u32 nm, u32 const* __restrict__ offs,
 __global__ void k_ent_seg(u32 n, u32 const* __restrict__ voe, u32 vpe,
     u32 const* __restrict__ seg, u32* __restrict__ out)
 {
+  pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) out[i] = seg[voe[(size_t)i * vpe]];
 }
@@ -86,6 +89,7 @@ __global__ void k_ent_seg(u32 n, u32 const* __restrict__ voe, u32 vpe,
 // stored segment-major: hist[seg * ntiles + tile]
 __global__ void k_tile_hist(u32 n, u32 const* __restrict__ es, u32 ntiles, u32* __restrict__ hist)
 {
+  pdl_wait();
   u32 tile = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   if (tile >= ntiles) return;
   u32 base = tile * SPLIT_TILE;
@@ -108,6 +112,7 @@ __global__ void k_tile_hist(u32 n, u32 const* __restrict__ es, u32 ntiles, u32* 
 __global__ void k_tile_scatter(u32 n, u32 const* __restrict__ es, u32 ntiles, u32* __restrict__ run,
     u32* __restrict__ perm)
 {
+  pdl_wait();
   u32 tile = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   if (tile >= ntiles) return;
   u32 base = tile * SPLIT_TILE;
@@ -136,6 +141,7 @@ __global__ void k_tile_scatter(u32 n, u32 const* __restrict__ es, u32 ntiles, u3
 __global__ void k_seg_bases(u32 nseg, u32 ntiles, u32 const* __restrict__ scan,
     u32* __restrict__ out)
 {
+  pdl_wait();
   u32 s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s <= nseg) out[s] = scan[(size_t)s * ntiles];
 }
@@ -143,6 +149,7 @@ __global__ void k_seg_bases(u32 nseg, u32 ntiles, u32 const* __restrict__ scan,
 __global__ void k_local_ids(u32 n, u32 const* __restrict__ es, u32 const* __restrict__ perm,
     u32 const* __restrict__ bases, u32* __restrict__ out)
 {
+  pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) out[i] = perm[i] - bases[es[i]];
 }
@@ -154,6 +161,7 @@ __global__ void k_scatter_meshes(u32 n, u32 width, T const* __restrict__ in,
     u32 const* __restrict__ es, u32 const* __restrict__ local, u32 const* __restrict__ vloc,
     T* const* __restrict__ dst)
 {
+  pdl_wait();
   u64 total = (u64)n * width;
   for (u64 j = blockIdx.x * (u64)blockDim.x + threadIdx.x; j < total;
        j += (u64)gridDim.x * blockDim.x) {
@@ -170,6 +178,7 @@ __global__ void k_scatter_meshes(u32 n, u32 width, T const* __restrict__ in,
 __global__ void k_scatter_iota64(u32 n, u32 const* __restrict__ es,
     u32 const* __restrict__ local, u64* const* __restrict__ dst)
 {
+  pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   u64* d = dst[es[i]];
@@ -181,6 +190,7 @@ __global__ void k_seg_min_quality(u32 n, double const* __restrict__ q,
     u32 const* __restrict__ voe, u32 vpe, u32 const* __restrict__ seg,
     unsigned long long* __restrict__ out)
 {
+  pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   bool on = i < n;
   u32 mask = __ballot_sync(FULL_MASK, on);
@@ -203,6 +213,7 @@ __global__ void k_seg_min_quality(u32 n, double const* __restrict__ q,
 __global__ void k_seg_count(u32 n, u32 const* __restrict__ voe, u32 vpe,
     u32 const* __restrict__ seg, u32* __restrict__ out)
 {
+  pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   bool on = i < n;
   u32 mask = __ballot_sync(FULL_MASK, on);
@@ -253,8 +264,8 @@ void launch_concat(u32 nm, Meta const& meta, size_t src_at, size_t offs_at, u32 
     T const* add, u64 total, void* out, cudaStream_t s)
 {
   if (!total) return;
-  k_concat<T><<<capped_grid(total), BLOCK, 0, s>>>(nm, meta.at<T const* const>(src_at),
-      meta.at<u32 const>(offs_at), width, add, static_cast<T*>(out));
+  CK(launch_kernel(k_concat<T>, dim3(capped_grid(total)), dim3(BLOCK), 0, s, nm, meta.at<T const* const>(src_at),
+      meta.at<u32 const>(offs_at), width, add, static_cast<T*>(out)));
   CK_LAUNCH();
 }
 
@@ -264,8 +275,8 @@ void launch_scatter(u32 n, u32 width, void const* in, u32 const* es, u32 const* 
 {
   u64 total = (u64)n * width;
   if (!total) return;
-  k_scatter_meshes<T><<<capped_grid(total), BLOCK, 0, s>>>(n, width, static_cast<T const*>(in),
-      es, local, vloc, meta.at<T* const>(dst_at));
+  CK(launch_kernel(k_scatter_meshes<T>, dim3(capped_grid(total)), dim3(BLOCK), 0, s, n, width, static_cast<T const*>(in),
+      es, local, vloc, meta.at<T* const>(dst_at)));
   CK_LAUNCH();
 }
 
@@ -437,8 +448,8 @@ Mesh* concat_meshes(std::vector<Mesh*> const& ms, cudaStream_t stream)
     u32 nv = offs[0][nm];
     u->seg = dalloc<u32>(nv, s);
     if (nv) {
-      k_seg_concat<<<capped_grid(nv), BLOCK, 0, s>>>(nm, meta.at<u32 const>(offs_at[0]),
-          meta.at<u32 const* const>(segsrc_at), meta.at<u32 const>(segbase_at), u->seg);
+      CK(launch_kernel(k_seg_concat, dim3(capped_grid(nv)), dim3(BLOCK), 0, s, nm, meta.at<u32 const>(offs_at[0]),
+          meta.at<u32 const* const>(segsrc_at), meta.at<u32 const>(segbase_at), u->seg));
       CK_LAUNCH();
     }
     dev_free(meta.dev, s);
@@ -476,7 +487,7 @@ std::vector<Mesh*> split_union(Mesh& u, cudaStream_t stream, std::vector<char> c
       if (d) {
         es[d] = dalloc<u32>(n ? n : 1, s);
         if (n) {
-          k_ent_seg<<<grid_for(n), BLOCK, 0, s>>>(n, u.ask_down(d, 0), deg(d, 0), u.seg, es[d]);
+          CK(launch_kernel(k_ent_seg, dim3(grid_for(n)), dim3(BLOCK), 0, s, n, u.ask_down(d, 0), deg(d, 0), u.seg, es[d]));
           CK_LAUNCH();
         }
       } else {
@@ -489,24 +500,24 @@ std::vector<Mesh*> split_union(Mesh& u, cudaStream_t stream, std::vector<char> c
       CK(cudaMemsetAsync(hist, 0, sizeof(u32) * nh, s));
       u32 warps_per_block = BLOCK / 32;
       if (n) {
-        k_tile_hist<<<ceil_div(ntiles, warps_per_block), BLOCK, 0, s>>>(n, es[d], ntiles, hist);
+        CK(launch_kernel(k_tile_hist, dim3(ceil_div(ntiles, warps_per_block)), dim3(BLOCK), 0, s, n, es[d], ntiles, hist));
         CK_LAUNCH();
       }
       u32* scan = exscan_new(hist, (u32)nh, s);
       dev_free(hist, s);
       u32* bases = dalloc<u32>(nm + 1, s);
-      k_seg_bases<<<grid_for(nm + 1), BLOCK, 0, s>>>(nm, ntiles, scan, bases);
+      CK(launch_kernel(k_seg_bases, dim3(grid_for(nm + 1)), dim3(BLOCK), 0, s, nm, ntiles, scan, bases));
       CK_LAUNCH();
       u32* perm = dalloc<u32>(n ? n : 1, s);
       if (n) {
-        k_tile_scatter<<<ceil_div(ntiles, warps_per_block), BLOCK, 0, s>>>(n, es[d], ntiles,
-            scan, perm);
+        CK(launch_kernel(k_tile_scatter, dim3(ceil_div(ntiles, warps_per_block)), dim3(BLOCK), 0, s, n, es[d], ntiles,
+            scan, perm));
         CK_LAUNCH();
       }
       dev_free(scan, s);
       local[d] = dalloc<u32>(n ? n : 1, s);
       if (n) {
-        k_local_ids<<<grid_for(n), BLOCK, 0, s>>>(n, es[d], perm, bases, local[d]);
+        CK(launch_kernel(k_local_ids, dim3(grid_for(n)), dim3(BLOCK), 0, s, n, es[d], perm, bases, local[d]));
         CK_LAUNCH();
       }
       dev_free(perm, s);
@@ -584,8 +595,8 @@ std::vector<Mesh*> split_union(Mesh& u, cudaStream_t stream, std::vector<char> c
               tag_at[d][t], s);
       }
       if (u.parallel && u.globals[d] && n) {
-        k_scatter_iota64<<<grid_for(n), BLOCK, 0, s>>>(n, es[d], local[d],
-            meta.at<u64* const>(glob_at[d]));
+        CK(launch_kernel(k_scatter_iota64, dim3(grid_for(n)), dim3(BLOCK), 0, s, n, es[d], local[d],
+            meta.at<u64* const>(glob_at[d])));
         CK_LAUNCH();
       }
     }
@@ -649,8 +660,8 @@ std::vector<double> UnionCtl::min_quality()
   double const* q = u.qualities();
   CK(cudaMemsetAsync(minkey, 0xff, sizeof(unsigned long long) * nm, s));
   if (ne) {
-    k_seg_min_quality<<<grid_for(ne), BLOCK, 0, s>>>(ne, q, u.ask_down(u.dim, 0),
-        deg(u.dim, 0), u.seg, minkey);
+    CK(launch_kernel(k_seg_min_quality, dim3(grid_for(ne)), dim3(BLOCK), 0, s, ne, q, u.ask_down(u.dim, 0),
+        deg(u.dim, 0), u.seg, minkey));
     CK_LAUNCH();
   }
   CK(cudaMemcpyAsync(h_key, minkey, sizeof(unsigned long long) * nm, cudaMemcpyDeviceToHost, s));
@@ -674,8 +685,8 @@ void UnionCtl::run(u32 op, std::vector<u32> const& group, std::vector<double> co
   CK(cudaMemsetAsync(elems, 0, sizeof(u32) * nm, s));
   u32 ne = u.count(u.dim);
   if (ne) {
-    k_seg_count<<<grid_for(ne), BLOCK, 0, s>>>(ne, u.ask_down(u.dim, 0), deg(u.dim, 0), u.seg,
-        elems);
+    CK(launch_kernel(k_seg_count, dim3(grid_for(ne)), dim3(BLOCK), 0, s, ne, u.ask_down(u.dim, 0), deg(u.dim, 0), u.seg,
+        elems));
     CK_LAUNCH();
   }
   ctl.active = active;
@@ -941,6 +952,7 @@ __device__ inline u64 mix64(u64 z)
 // sum over words of mix(word, position, salt); wraps modulo 2^64
 __global__ void k_digest(u64 nwords, u32 const* __restrict__ w, u64 salt, u64* out)
 {
+  pdl_wait();
   u64 acc = 0;
   for (u64 j = blockIdx.x * (u64)blockDim.x + threadIdx.x; j < nwords;
        j += (u64)gridDim.x * blockDim.x)
@@ -977,7 +989,7 @@ u64 mesh_digest(Mesh& m)
     salt = host_mix(salt + 1);
     u64 nw = bytes / 4;
     if (nw) {
-      k_digest<<<capped_grid(nw), BLOCK, 0, s>>>(nw, static_cast<u32 const*>(p), salt, acc);
+      CK(launch_kernel(k_digest, dim3(capped_grid(nw)), dim3(BLOCK), 0, s, nw, static_cast<u32 const*>(p), salt, acc));
       CK_LAUNCH();
     }
     // a trailing partial word (u8 tags) enters through the host

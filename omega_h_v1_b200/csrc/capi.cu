@@ -52,6 +52,9 @@ void swap_table_host(u32 rs, u32* ntri, u32* nmesh, u32* nint, u32* tris, u32* i
     return;                                              \
   }
 
+using osh::launch_kernel;
+using osh::pdl_wait;
+
 namespace {
 
 void need(bool ok, char const* what)
@@ -68,6 +71,7 @@ void sync(Mesh* m)
 __global__ void k_mark_classified(u32 n, u32 const* __restrict__ cd,
     u32 const* __restrict__ cid, u32 target_dim, u32 target_id, u32* __restrict__ marked)
 {
+  pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   // mark_class_kern + mark_or_kern (mark.cpp:149-167, omega_h.cpp:890-896)
@@ -78,6 +82,7 @@ __global__ void k_mark_classified(u32 n, u32 const* __restrict__ cd,
 __global__ void k_identity_size(u32 nv, u32 const* __restrict__ offs,
     u32 const* __restrict__ adj, double const* __restrict__ x, double* __restrict__ out)
 {
+  pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nv) return;
   double xi[3];
@@ -419,9 +424,9 @@ void osh_mark_classified(osh_t h, unsigned ent_dim, unsigned class_dim, unsigned
   need(class_id == osh::INV || ci != nullptr, "no class_id label");
   u32 n = m->count(ent_dim);
   if (n) {
-    k_mark_classified<<<osh::grid_for(n), osh::BLOCK, 0, m->s>>>(n,
+    CK(launch_kernel(k_mark_classified, dim3(osh::grid_for(n)), dim3(osh::BLOCK), 0, m->s, n,
         static_cast<u32 const*>(cd->data), ci ? static_cast<u32 const*>(ci->data) : nullptr,
-        class_dim, class_id, marked);
+        class_dim, class_id, marked));
     CK_LAUNCH();
   }
   sync(m);
@@ -463,8 +468,8 @@ void osh_identity_size(osh_t h, char const* name)
   osh::Graph const& g = m->ask_star(0, 1);
   double* out = osh::dalloc<double>(nv, m->s);
   if (nv) {
-    k_identity_size<<<osh::grid_for(nv), osh::BLOCK, 0, m->s>>>(nv, g.offs, g.adj,
-        m->coords(), out);
+    CK(launch_kernel(k_identity_size, dim3(osh::grid_for(nv)), dim3(osh::BLOCK), 0, m->s, nv, g.offs, g.adj,
+        m->coords(), out));
     CK_LAUNCH();
   }
   m->add_tag(0, osh::T_F64, name, 1, osh::X_NOT, out);
@@ -761,6 +766,39 @@ void osh_b200_fp32_stats_reset(void)
 {
   API_TRY
   osh::fp32_stats_reset();
+  API_CATCH_VOID
+}
+
+void osh_b200_set_fp32_audit(int on)
+{
+  API_TRY
+  osh::fp32_set_audit(on != 0);
+  API_CATCH_VOID
+}
+
+void osh_b200_fp32_audit_stats(unsigned long long* audited, unsigned long long* flips,
+    unsigned long long* checked)
+{
+  API_TRY
+  osh::fp32_audit_read(audited, flips, checked);
+  API_CATCH_VOID
+}
+
+void osh_b200_fp32_probe_tets(unsigned n, double const* host_x, float* host_est,
+    float* host_err, double* host_q64)
+{
+  API_TRY
+  need(n == 0 || (host_x && host_est && host_err && host_q64), "null array");
+  osh::fp32_probe_tets(n, host_x, host_est, host_err, host_q64);
+  API_CATCH_VOID
+}
+
+void osh_b200_fp32_probe_edges(unsigned n, double const* host_x, double const* host_h,
+    double thr, int* host_side, double* host_ratio64)
+{
+  API_TRY
+  need(n == 0 || (host_x && host_h && host_side && host_ratio64), "null array");
+  osh::fp32_probe_edges(n, host_x, host_h, thr, host_side, host_ratio64);
   API_CATCH_VOID
 }
 

@@ -15,27 +15,33 @@ __global__ void k_coarsen_size_codes(u32 ne, u32 const* __restrict__ voe,
     double const* __restrict__ x, double const* __restrict__ h, double size_floor,
     SegView sv, Fp32Stats* fs, u32* __restrict__ codes, u32* any)
 {
+  pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   u32 c = 0;
+  bool decided = false, rechecked = false, flipped = false;
   if (i < ne) {
     u32 a = voe[i * 2], b = voe[i * 2 + 1];
     double xa[3], xb[3];
     load3(x, a, xa);
     load3(x, b, xb);
     int r32 = fs ? edge_ratio_side_f32(xa, xb, h[a], h[b], size_floor) : 0;
-    bool shorter;
+    bool shorter = false;
     if (r32) {
-      atomicAdd(&fs->decided, 1ull);
+      decided = true;
       shorter = r32 < 0;
-    } else {
-      if (fs) atomicAdd(&fs->rechecked, 1ull);
+    }
+    if (!r32 || fs->audit) {
+      rechecked = !r32;
       double len = sqrt(sqdist3(xb, xa));
       double want = (h[a] + h[b]) / 2;
-      shorter = (len / want) < size_floor;
+      bool s64 = (len / want) < size_floor;
+      flipped = r32 && s64 != shorter;
+      shorter = s64;
     }
     c = (shorter && seg_acts(sv, a)) ? (u32)COLLAPSE_BOTH : (u32)DONT_COLLAPSE;
     codes[i] = c;
   }
+  if (fs) fp32_count_warp(fs, decided, rechecked, decided && fs->audit, flipped);
   if (__any_sync(0xffffffffu, c) && (threadIdx.x & 31) == 0) atomicOr(any, 1u);
 }
 
@@ -43,6 +49,7 @@ __global__ void k_coarsen_size_codes(u32 ne, u32 const* __restrict__ voe,
 __global__ void k_coarsen_sliver_codes(u32 ne, u32 const* __restrict__ voe,
     u32 const* __restrict__ marked, u32* __restrict__ codes, u32* any)
 {
+  pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   u32 c = 0;
   if (i < ne) {
@@ -57,6 +64,7 @@ __global__ void k_coarsen_sliver_codes(u32 ne, u32 const* __restrict__ voe,
 __global__ void k_check_basic_class(u32 ne, u32 const* __restrict__ voe,
     u32 const* __restrict__ cdv, u32 const* __restrict__ cde, u32* __restrict__ codes)
 {
+  pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= ne) return;
   u32 code = codes[i];
@@ -77,6 +85,7 @@ __global__ void k_check_exposed_sides(u32 ed, u32 ne, u32 const* __restrict__ u_
     u32 const* __restrict__ vot, u32 const* __restrict__ voe, u32 const* __restrict__ sot,
     u32 const* __restrict__ cdt, u32 const* __restrict__ cds, u32* __restrict__ codes)
 {
+  pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= ne) return;
   u32 code = codes[i];
@@ -147,11 +156,13 @@ __global__ void k_coarsen_quality(u32 dim, u32 const* __restrict__ list,
     double const* __restrict__ eq, double floor_q, SegView sv, Fp32Stats* fs,
     u32* __restrict__ codes, double* __restrict__ out, u32* any)
 {
+  pdl_wait();
   u32 lane = threadIdx.x & 31;
   u32 n = *nlist;
   u32 vpe = deg(dim, 0);
   double const perfect = dim == 3 ? perfect_tet_quality() : perfect_tri_quality();
   bool const use32 = fs && dim == 3;
+  float const k6 = tet_k6_f32();
   for (u32 w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < n;
        w += (gridDim.x * blockDim.x) >> 5) {
     u32 i = list[w];
@@ -167,10 +178,62 @@ __global__ void k_coarsen_quality(u32 dim, u32 const* __restrict__ list,
       if (eq)
         for (u32 k = f + lane; k < e; k += 32) first_min_add(om, eq[ev[k]], k - f + 1);
       double old_minq = warp_first_min(om);
-      float upper = 1.0f;
+      // with the filter: the cavity's estimates first; the direction is
+      // rejected on them when the worst element is surely below the floor or
+      // surely no better than before; otherwise only the elements whose
+      // lower bound reaches the lowest upper bound (they alone can hold the
+      // minimum) are computed in double
+      bool rejected32 = false, filtered = false;
+      unsigned long long need = 0;   // this lane's elements, by visit index
+      bool all = true;
       if (use32) {
-        // reject on the estimate when the cavity's worst element is surely
-        // below the floor, or surely no better than before
+        float upper = 1.0f;
+        all = (e - f) > 64 * 32;
+        u32 c = 0;
+        for (u32 k = f + lane; k < e; k += 32, ++c) {
+          u32 const* ve = voe + (size_t)ev[k] * vpe;
+          bool adjacent = false;
+          for (u32 l = 0; l < vpe; ++l) adjacent = adjacent || ve[l] == gen;
+          if (adjacent) continue;
+          u32 base = opp(dim, 0, ev_dirs[k]);
+          for (u32 l = 0; l + 1 < vpe; ++l) load3(x, ve[canon(dim, dim - 1, 0, base, l)], ex[l]);
+          Q32 q = tet_quality_f32(ex, k6);
+          upper = fminf(upper, q32_hi(q));
+          if (!all && q32_lo(q) <= upper) need |= 1ull << c;
+        }
+        upper = warp_minf(upper);
+        filtered = true;
+        rejected32 = (double)upper < fq || (eq && (double)upper <= old_minq);
+        if (lane == 0) {
+          if (rejected32)
+            atomicAdd(&fs->decided, 1ull);
+          else
+            atomicAdd(&fs->rechecked, 1ull);
+        }
+      }
+      double minq = 1.0;
+      if (!rejected32) {
+        FirstMin mm{1.0, 0};
+        u32 c = 0;
+        for (u32 k = f + lane; k < e; k += 32, ++c) {
+          if (filtered && !all && !((need >> c) & 1ull)) continue;
+          u32 const* ve = voe + (size_t)ev[k] * vpe;
+          bool adjacent = false;
+          for (u32 l = 0; l < vpe; ++l) adjacent = adjacent || ve[l] == gen;
+          if (adjacent) continue;
+          u32 base = opp(dim, 0, ev_dirs[k]);
+          for (u32 l = 0; l + 1 < vpe; ++l) load3(x, ve[canon(dim, dim - 1, 0, base, l)], ex[l]);
+          double q = dim == 3 ? tet_quality(ex, perfect) : tri_quality(ex, 1, perfect);
+          if (filtered && fs->audit) fp32_note_error(fs, tet_quality_f32(ex, k6), q);
+          first_min_add(mm, q, k - f + 1);
+        }
+        minq = warp_first_min(mm);
+      }
+      bool drop = rejected32 || minq < fq || (eq && minq <= old_minq);
+      if (filtered && fs->audit) {
+        // the double path's result over the whole cavity, and every
+        // estimate against its double value
+        FirstMin m64{1.0, 0};
         for (u32 k = f + lane; k < e; k += 32) {
           u32 const* ve = voe + (size_t)ev[k] * vpe;
           bool adjacent = false;
@@ -178,40 +241,19 @@ __global__ void k_coarsen_quality(u32 dim, u32 const* __restrict__ list,
           if (adjacent) continue;
           u32 base = opp(dim, 0, ev_dirs[k]);
           for (u32 l = 0; l + 1 < vpe; ++l) load3(x, ve[canon(dim, dim - 1, 0, base, l)], ex[l]);
-          Q32 q = tet_quality_f32(ex, (float)perfect);
-          upper = fminf(upper, q.q + q.err);
-        }
-        upper = warp_minf(upper);
-        if ((double)upper < fq || (eq && (double)upper <= old_minq)) {
-          if (lane == 0) atomicAdd(&fs->decided, 1ull);
-          code &= ~(1u << j);
-          continue;
-        }
-        if (lane == 0) atomicAdd(&fs->rechecked, 1ull);
-      }
-      FirstMin mm{1.0, 0};
-      for (u32 k = f + lane; k < e; k += 32) {
-        u32 const* ve = voe + (size_t)ev[k] * vpe;
-        bool adjacent = false;
-        for (u32 l = 0; l < vpe; ++l) adjacent = adjacent || ve[l] == gen;
-        if (adjacent) continue;
-        u32 base = opp(dim, 0, ev_dirs[k]);
-        for (u32 l = 0; l + 1 < vpe; ++l) load3(x, ve[canon(dim, dim - 1, 0, base, l)], ex[l]);
-        if (use32) {
-          // only an element whose estimate - bound reaches `upper` can hold
-          // the minimum; the others are not computed in double
-          Q32 q32 = tet_quality_f32(ex, (float)perfect);
-          if ((double)q32.q - (double)q32.err > (double)upper) continue;
           double q = tet_quality(ex, perfect);
-          fp32_note_error(fs, q32, q);
-          first_min_add(mm, q, k - f + 1);
-        } else {
-          first_min_add(mm, dim == 3 ? tet_quality(ex, perfect) : tri_quality(ex, 1, perfect),
-              k - f + 1);
+          fp32_note_error(fs, tet_quality_f32(ex, k6), q);
+          first_min_add(m64, q, k - f + 1);
+        }
+        double q64 = warp_first_min(m64);
+        bool drop64 = q64 < fq || (eq && q64 <= old_minq);
+        bool flip = drop64 != drop || (!drop && q64 != minq);
+        if (lane == 0) {
+          atomicAdd(&fs->audited, 1ull);
+          if (flip) atomicAdd(&fs->flips, 1ull);
         }
       }
-      double minq = warp_first_min(mm);
-      if (minq < fq || (eq && minq <= old_minq))
+      if (drop)
         code &= ~(1u << j);
       else if (lane == 0)
         out[i * 2 + j] = minq;
@@ -229,6 +271,7 @@ __global__ void k_coarsen_quality(u32 dim, u32 const* __restrict__ list,
 __global__ void k_list_candidates(u32 n, u32 const* __restrict__ flags, u32* __restrict__ list,
     u32* count, double2* __restrict__ q2)
 {
+  pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   bool on = i < n && flags[i] != 0;
   if (i < n) q2[i] = make_double2(0.0, 0.0);
@@ -247,6 +290,7 @@ __global__ void k_collapses_to_verts(u32 nv, u32 const* __restrict__ ue_offs,
     u32 const* __restrict__ codes, double const* __restrict__ q2, u32* __restrict__ cand,
     double* __restrict__ colq)
 {
+  pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nv) return;
   double maxq = 0;
@@ -274,6 +318,7 @@ __global__ void k_vertex_dest(u32 nv, u32 const* __restrict__ ue_offs,
     double const* __restrict__ colq, u32 const* __restrict__ codes,
     double const* __restrict__ q2, u32* __restrict__ gen_vert)
 {
+  pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nv) return;
   u32 g = INV;
@@ -294,6 +339,87 @@ __global__ void k_vertex_dest(u32 nv, u32 const* __restrict__ ue_offs,
   gen_vert[i] = g;
 }
 
+// The two vertex kernels with a group of VERT_GROUP lanes per vertex row
+// (rows of about 13.5 edges): lane l takes the row's entries l, l + 8, ...,
+// and shuffles within the group combine the lanes' results. The best
+// collapse keeps the first entry (in upward order) of greatest quality, as
+// the reference's loop does, so lanes combine (quality, position) pairs;
+// the destination is the first entry whose quality equals the best.
+constexpr u32 VERT_GROUP = 8;
+
+__global__ void k_collapses_to_verts_grouped(u32 nv, u32 const* __restrict__ ue_offs,
+    u32 const* __restrict__ ue, u32 const* __restrict__ ue_dirs,
+    u32 const* __restrict__ codes, double const* __restrict__ q2, u32* __restrict__ cand,
+    double* __restrict__ colq)
+{
+  pdl_wait();
+  u32 const t = blockIdx.x * blockDim.x + threadIdx.x;
+  u32 const i = t / VERT_GROUP, lg = t % VERT_GROUP;
+  if (i >= nv) return;  // a group shares i: it leaves together
+  u32 const gbase = (threadIdx.x & 31) & ~(VERT_GROUP - 1);
+  u32 const gmask = ((1u << VERT_GROUP) - 1u) << gbase;
+  double maxq = 0;
+  u32 pos = INV;  // position of the lane's best entry; INV: no collapse seen
+  for (u32 j = ue_offs[i] + lg; j < ue_offs[i + 1]; j += VERT_GROUP) {
+    u32 e = ue[j], d = ue_dirs[j];
+    if (!collapses(codes[e], d)) continue;
+    double q = q2[e * 2 + d];
+    if (pos == INV || q > maxq) {
+      maxq = q;
+      pos = j;
+    }
+  }
+  for (u32 o = VERT_GROUP / 2; o; o >>= 1) {
+    double oq = __shfl_xor_sync(gmask, maxq, o);
+    u32 op = __shfl_xor_sync(gmask, pos, o);
+    if (op != INV && (pos == INV || oq > maxq || (oq == maxq && op < pos))) {
+      maxq = oq;
+      pos = op;
+    }
+  }
+  if (lg == 0) {
+    cand[i] = pos != INV;
+    colq[i] = pos != INV ? maxq : 0.0;
+  }
+}
+
+__global__ void k_vertex_dest_grouped(u32 nv, u32 const* __restrict__ ue_offs,
+    u32 const* __restrict__ ue, u32 const* __restrict__ ue_dirs,
+    u32 const* __restrict__ voe1, u32 const* __restrict__ ind,
+    double const* __restrict__ colq, u32 const* __restrict__ codes,
+    double const* __restrict__ q2, u32* __restrict__ gen_vert)
+{
+  pdl_wait();
+  u32 const t = blockIdx.x * blockDim.x + threadIdx.x;
+  u32 const i = t / VERT_GROUP, lg = t % VERT_GROUP;
+  if (i >= nv) return;
+  u32 const gbase = (threadIdx.x & 31) & ~(VERT_GROUP - 1);
+  u32 const gmask = ((1u << VERT_GROUP) - 1u) << gbase;
+  if (!ind[i]) {
+    if (lg == 0) gen_vert[i] = INV;
+    return;
+  }
+  double maxq = colq[i];
+  if (maxq == 1e10) maxq = -1e10;
+  u32 first = INV;
+  for (u32 j = ue_offs[i] + lg; j < ue_offs[i + 1]; j += VERT_GROUP) {
+    u32 e = ue[j], d = ue_dirs[j];
+    if (!collapses(codes[e], d)) continue;
+    double q = q2[e * 2 + d];
+    if (q == 1e10) q = -1e10;
+    if (q == maxq) {
+      first = j;
+      break;
+    }
+  }
+  for (u32 o = VERT_GROUP / 2; o; o >>= 1) first = min(first, __shfl_xor_sync(gmask, first, o));
+  if (lg == 0) {
+    u32 g = INV;
+    if (first != INV) g = voe1[ue[first] * 2 + (1 - ue_dirs[first])];
+    gen_vert[i] = g;
+  }
+}
+
 // collapse_to_ent (collapses_to_ents.cpp:11-64)
 __global__ void k_collapse_to_ent(u32 ed, u32 n, u32 const* __restrict__ voe,
     u32 const* __restrict__ soe, u32 const* __restrict__ gen_offs_v,
@@ -301,6 +427,7 @@ __global__ void k_collapse_to_ent(u32 ed, u32 n, u32 const* __restrict__ voe,
     u32* __restrict__ is_same, u32* __restrict__ fused_sides, u32* __restrict__ will_gen,
     u32* __restrict__ gen_vert, u32* __restrict__ gen_dir)
 {
+  pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   u32 vpe = deg(ed, 0), spe = deg(ed, ed - 1);
@@ -339,6 +466,7 @@ __global__ void k_coarsen_topology(u32 ed, u32 n, u32 const* __restrict__ voe,
     u32 const* __restrict__ gen_dir, u32 const* __restrict__ same_v,
     u32* __restrict__ out)
 {
+  pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n || gen_offs[i] == gen_offs[i + 1]) return;
   u32 vpe = deg(ed, 0);
@@ -353,6 +481,7 @@ __global__ void k_coarsen_topology(u32 ed, u32 n, u32 const* __restrict__ voe,
 __global__ void k_same_conn(u32 n, u32 vpe, u32 const* __restrict__ voe,
     u32 const* __restrict__ same_e, u32 const* __restrict__ same_v, u32* __restrict__ out)
 {
+  pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n || same_e[i] == same_e[i + 1]) return;
   u32 o = same_e[i];
@@ -366,6 +495,7 @@ __global__ void k_coarsen_conserve(u32 nv, u32 nc, u32 nsame,
     double const* __restrict__ in, double const* __restrict__ sizes,
     double* __restrict__ gen)
 {
+  pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nv || gen_offs_v[i] == gen_offs_v[i + 1]) return;
   u32 f = ev_offs[i], e = ev_offs[i + 1];
@@ -451,6 +581,7 @@ __global__ void k_coarsen_fit(u32 nv, u32 nc, u32 nsame, u32 const* __restrict__
     double const* __restrict__ newx, double const* __restrict__ in,
     double* __restrict__ gen)
 {
+  pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nv || gen_offs_v[i] == gen_offs_v[i + 1]) return;
   u32 f = ev_offs[i], e = ev_offs[i + 1];
@@ -518,9 +649,9 @@ static void coarsen_transfer(Mesh& m, Mesh& out, u32 const* gen_offs_v,
       double* data = dalloc<double>((size_t)(nsame + ngen) * nc, s);
       expand_scaled(t.data, same_e, 1, ne, nc, 8, data, s);
       if (nv) {
-        k_coarsen_conserve<<<grid_for(nv), BLOCK, 0, s>>>(nv, nc, nsame, gen_offs_v,
+        CK(launch_kernel(k_coarsen_conserve, dim3(grid_for(nv)), dim3(BLOCK), 0, s, nv, nc, nsame, gen_offs_v,
             gen_offs_e, ev.offs, ev.adj, static_cast<double const*>(t.data), sizes,
-            data + (size_t)nsame * nc);
+            data + (size_t)nsame * nc));
         CK_LAUNCH();
       }
       out.add_tag(dim, T_F64, t.name.c_str(), nc, t.transfer, data);
@@ -538,9 +669,9 @@ static void coarsen_transfer(Mesh& m, Mesh& out, u32 const* gen_offs_v,
     double* data = dalloc<double>((size_t)(nsame + ngen) * nc, s);
     expand_scaled(t.data, same_e, 1, ne, nc, 8, data, s);
     if (nv) {
-      k_coarsen_fit<<<ceil_div(nv, 128), 128, 0, s>>>(nv, nc, nsame, gen_offs_v, gen_offs_e,
+      CK(launch_kernel(k_coarsen_fit, dim3(ceil_div(nv, 128)), dim3(128), 0, s, nv, nc, nsame, gen_offs_v, gen_offs_e,
           ev.offs, ev.adj, oldx, newx, static_cast<double const*>(t.data),
-          data + (size_t)nsame * nc);
+          data + (size_t)nsame * nc));
       CK_LAUNCH();
     }
     out.add_tag(dim, T_F64, t.name.c_str(), nc, t.transfer, data);
@@ -576,8 +707,8 @@ static bool coarsen_select(Mesh& m, u32* codes, double qual_floor, bool require_
   if (!cdv || !cde) throw Failure(E_ARG, "coarsening needs class_dim on every dimension");
   u32 const* voe1 = m.ask_down(1, 0);
   if (ne) {
-    k_check_basic_class<<<grid_for(ne), BLOCK, 0, s>>>(ne, voe1,
-        static_cast<u32 const*>(cdv->data), static_cast<u32 const*>(cde->data), codes);
+    CK(launch_kernel(k_check_basic_class, dim3(grid_for(ne)), dim3(BLOCK), 0, s, ne, voe1,
+        static_cast<u32 const*>(cdv->data), static_cast<u32 const*>(cde->data), codes));
     CK_LAUNCH();
   }
   for (u32 ed = 2; ed <= dim; ++ed) {
@@ -586,9 +717,9 @@ static bool coarsen_select(Mesh& m, u32* codes, double qual_floor, bool require_
     Tag* cds = m.find_tag(ed - 1, "class_dim");
     if (!cdt || !cds) throw Failure(E_ARG, "coarsening needs class_dim on every dimension");
     if (ne) {
-      k_check_exposed_sides<<<grid_for(ne), BLOCK, 0, s>>>(ed, ne, u.offs, u.adj, u.dirs,
+      CK(launch_kernel(k_check_exposed_sides, dim3(grid_for(ne)), dim3(BLOCK), 0, s, ed, ne, u.offs, u.adj, u.dirs,
           m.ask_down(ed, 0), voe1, m.ask_down(ed, ed - 1),
-          static_cast<u32 const*>(cdt->data), static_cast<u32 const*>(cds->data), codes);
+          static_cast<u32 const*>(cdt->data), static_cast<u32 const*>(cds->data), codes));
       CK_LAUNCH();
     }
   }
@@ -605,8 +736,8 @@ static bool coarsen_select(Mesh& m, u32* codes, double qual_floor, bool require_
   u32* ncand = m.mb->dev + 7;
   CK(cudaMemsetAsync(any, 0, 4 * sizeof(u32), s));  // slots 4-7
   if (ne) {
-    k_list_candidates<<<grid_for(ne), BLOCK, 0, s>>>(ne, codes, clist, ncand,
-        reinterpret_cast<double2*>(sel.q2));
+    CK(launch_kernel(k_list_candidates, dim3(grid_for(ne)), dim3(BLOCK), 0, s, ne, codes, clist, ncand,
+        reinterpret_cast<double2*>(sel.q2)));
     CK_LAUNCH();
   }
   if (dim >= 2 && ne) {
@@ -617,9 +748,9 @@ static bool coarsen_select(Mesh& m, u32* codes, double qual_floor, bool require_
         4.0 * deg(dim, 0) * nel + 24.0 * nv + 8.0 * ne + 16.0 * ne);
     // a warp per listed edge; the list's length is read on the device
     u32 blocks = (u32)std::min<u64>(ceil_div((u64)ne * 32, BLOCK), 148u * 16u);
-    k_coarsen_quality<<<blocks, BLOCK, 0, s>>>(dim, clist, ncand, voe1, m.ask_down(dim, 0),
+    CK(launch_kernel(k_coarsen_quality, dim3(blocks), dim3(BLOCK), 0, s, dim, clist, ncand, voe1, m.ask_down(dim, 0),
         ev.offs, ev.adj, ev.dirs, m.coords(), eq, qual_floor, m.segview(),
-        m.fp32_filter ? fp32_stats_dev() : nullptr, codes, sel.q2, any);
+        m.fp32_filter ? fp32_stats_dev() : nullptr, codes, sel.q2, any));
     CK_LAUNCH();
   }
   dev_free(clist, s);
@@ -636,15 +767,15 @@ static bool coarsen_select(Mesh& m, u32* codes, double qual_floor, bool require_
   sel.cand = dalloc<u32>(nv, s);
   sel.colq = dalloc<double>(nv, s);
   if (nv) {
-    k_collapses_to_verts<<<grid_for(nv), BLOCK, 0, s>>>(nv, ue.offs, ue.adj, ue.dirs, codes,
-        sel.q2, sel.cand, sel.colq);
+    CK(launch_kernel(k_collapses_to_verts_grouped, dim3(grid_for((u64)nv * VERT_GROUP)), dim3(BLOCK), 0, s, nv, ue.offs,
+        ue.adj, ue.dirs, codes, sel.q2, sel.cand, sel.colq));
     CK_LAUNCH();
   }
   sel.ind = find_indset(m, 0, sel.cand, sel.colq);
   sel.gen_vert = dalloc<u32>(nv, s);
   if (nv) {
-    k_vertex_dest<<<grid_for(nv), BLOCK, 0, s>>>(nv, ue.offs, ue.adj, ue.dirs, voe1, sel.ind,
-        sel.colq, codes, sel.q2, sel.gen_vert);
+    CK(launch_kernel(k_vertex_dest_grouped, dim3(grid_for((u64)nv * VERT_GROUP)), dim3(BLOCK), 0, s, nv, ue.offs,
+        ue.adj, ue.dirs, voe1, sel.ind, sel.colq, codes, sel.q2, sel.gen_vert));
     CK_LAUNCH();
   }
   return true;
@@ -687,8 +818,8 @@ static void coarsen_build(Mesh& m, CoarsenSel const& sel)
     if (n) {
       PROBE(P_COLLAPSE_TO_ENT, s, 4.0 * (vpe + deg(ed, ed - 1)) * n + 8.0 * (nv + 1) +
           4.0 * n * 4 + 4.0 * nsides);
-      k_collapse_to_ent<<<grid_for(n), BLOCK, 0, s>>>(ed, n, voe, soe, gen_offs_v,
-          sel.gen_vert, fused[ed], is_same, fused[ed - 1], will_gen, gvert_of[ed], gdir_of[ed]);
+      CK(launch_kernel(k_collapse_to_ent, dim3(grid_for(n)), dim3(BLOCK), 0, s, ed, n, voe, soe, gen_offs_v,
+          sel.gen_vert, fused[ed], is_same, fused[ed - 1], will_gen, gvert_of[ed], gdir_of[ed]));
       CK_LAUNCH();
     }
     gen_offs_of[ed] = exscan_new(will_gen, n, s, m.mb->dev + 16 + 2 * (ed - 1));
@@ -741,10 +872,10 @@ static void coarsen_build(Mesh& m, CoarsenSel const& sel)
     u32 nout = nsame + ngen;
     u32* conn = dalloc<u32>((size_t)nout * vpe, s);
     if (n) {
-      k_same_conn<<<grid_for(n), BLOCK, 0, s>>>(n, vpe, voe, same_e, same_v, conn);
+      CK(launch_kernel(k_same_conn, dim3(grid_for(n)), dim3(BLOCK), 0, s, n, vpe, voe, same_e, same_v, conn));
       CK_LAUNCH();
-      k_coarsen_topology<<<grid_for(n), BLOCK, 0, s>>>(ed, n, voe, gen_offs, gvert, gdir,
-          same_v, conn + (size_t)nsame * vpe);
+      CK(launch_kernel(k_coarsen_topology, dim3(grid_for(n)), dim3(BLOCK), 0, s, ed, n, voe, gen_offs, gvert, gdir,
+          same_v, conn + (size_t)nsame * vpe));
       CK_LAUNCH();
     }
     dev_free(gvert, s);
@@ -822,9 +953,9 @@ u32 coarsen_by_size(Mesh& m, double qual_floor, double size_floor)
   // read-back
   u32* any = m.mb->dev + 5;
   if (ne) {
-    k_coarsen_size_codes<<<grid_for(ne), BLOCK, 0, s>>>(ne, m.ask_down(1, 0), m.coords(),
+    CK(launch_kernel(k_coarsen_size_codes, dim3(grid_for(ne)), dim3(BLOCK), 0, s, ne, m.ask_down(1, 0), m.coords(),
         static_cast<double const*>(h->data), size_floor, m.segview(),
-        m.fp32_filter ? fp32_stats_dev() : nullptr, codes, any);
+        m.fp32_filter ? fp32_stats_dev() : nullptr, codes, any));
     CK_LAUNCH();
   }
   u32 r = 0;
@@ -857,7 +988,7 @@ u32 coarsen_slivers(Mesh& m, double qual_floor, u32 nlayers)
   u32* codes = dalloc<u32>(ne, s);
   u32* any = m.mb->dev + 5;  // not read (as in coarsen_by_size)
   if (ne) {
-    k_coarsen_sliver_codes<<<grid_for(ne), BLOCK, 0, s>>>(ne, m.ask_down(1, 0), mv, codes, any);
+    CK(launch_kernel(k_coarsen_sliver_codes, dim3(grid_for(ne)), dim3(BLOCK), 0, s, ne, m.ask_down(1, 0), mv, codes, any));
     CK_LAUNCH();
   }
   dev_free(mv, s);
@@ -888,9 +1019,9 @@ u32 coarsen_sets(Mesh& m, double qual_floor, double size_floor, u32* codes_size,
   CK(cudaMemsetAsync(indset, 0, sizeof(u32) * nv, s));
   CK(cudaMemsetAsync(gen_vert, 0xff, sizeof(u32) * nv, s));
   if (ne) {
-    k_coarsen_size_codes<<<grid_for(ne), BLOCK, 0, s>>>(ne, m.ask_down(1, 0), m.coords(),
+    CK(launch_kernel(k_coarsen_size_codes, dim3(grid_for(ne)), dim3(BLOCK), 0, s, ne, m.ask_down(1, 0), m.coords(),
         static_cast<double const*>(h->data), size_floor, m.segview(),
-        m.fp32_filter ? fp32_stats_dev() : nullptr, codes_size, any);
+        m.fp32_filter ? fp32_stats_dev() : nullptr, codes_size, any));
     CK_LAUNCH();
   }
   u32* codes = dalloc<u32>(ne, s);

@@ -62,6 +62,36 @@ void count_launch();
 
 inline u32 ceil_div(u64 a, u64 b) { return (u32)((a + b - 1) / b); }
 
+// Programmatic dependent launch. Every kernel of the library starts with
+// pdl_wait(), which returns once the kernels before it on the stream have
+// finished and their writes are visible (a no-op for a kernel launched
+// without the attribute), and every launch goes through launch_kernel,
+// which sets the attribute: the next kernel's blocks are scheduled while
+// the previous kernel's last blocks drain, instead of after a full launch
+// gap. The launches are the same kernels with the same arguments in the
+// same order; OSH_B200_PDL=0 in the environment launches without the
+// attribute.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
+bool pdl_enabled();
+
+template <class... KArgs, class... Args>
+cudaError_t launch_kernel(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem,
+    cudaStream_t stream, Args&&... args)
+{
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = pdl_enabled() ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+}
+
 // order-preserving 64-bit key of a double (min of keys = min of values)
 __device__ inline unsigned long long order_key(double x)
 {
@@ -234,19 +264,52 @@ __host__ __device__ inline double perfect_tet_quality()
   return (sqrt(2.0) / 12.0) / (s * s * s);
 }
 
-// Single-precision filter for quality decisions. The estimate is formed
-// from coordinates relative to the first vertex (each difference taken in
-// double, then rounded), with a running bound on its error: the triple
-// product and the face areas are each off by at most a few float epsilons
-// of the products of the edge lengths that form them, which the bound
-// scales by the same normalisation as the quality. A candidate is rejected
-// on the estimate only when estimate + bound is already below the
-// threshold; every other decision, and every value that is kept, comes from
-// the double computation, so all decisions equal the double path's.
+// Single-precision filter for quality and edge-length decisions.
+//
+// Each estimate comes with a rigorous bound on its distance from the value
+// the double path computes, so a decision taken on the estimate is the
+// double path's decision. The derivation (standard rounding-error analysis,
+// u = 2^-24, gamma_n = n u / (1 - n u), no fused multiply-add since every
+// unit is built with -fmad=false, IEEE float division and square root):
+//
+//  * inputs: d_k = fl32(fl64(x_k - x_0)) differs from the exact difference
+//    D_k by a factor (1 + a), |a| <= u + 2^-53 + 2^-77, per component;
+//  * volume: the triple product fl(fl(d0 x d1) . d2) is within
+//    gamma_5 Pi(d) of det(d0, d1, d2), where Pi is the sum of the absolute
+//    values of the six terms of the determinant, and det(d) within
+//    3.0002 u Pi(d) of det(D); Pi(d) <= sqrt(2) |d0||d1||d2|, and |d_k| <=
+//    sqrt(n_k)(1 + 1.51 u) for the computed squared lengths n_k, so
+//    |V6 - det(D)| <= 12 u sqrt(n0 n1 n2);
+//  * faces: each cross product c_i (of two edge vectors, formed from the
+//    d_k with at most one more subtraction) is within 8.85 u lmax^2 of the
+//    exact one (rounding of the cross product: gamma_2 sqrt(2) |a||b|;
+//    edge vectors off by at most 3.0001 u lmax), and lmax^2 <= (1 + 9.01 u)
+//    times the computed largest squared edge length lmax2: eps = 9 u lmax2;
+//  * the sum S of the four |c_i|^2 (a sum of non-negative terms: gamma_6)
+//    is within T = 7 u S + 4 eps sqrt(S) + 4 eps^2 of the exact one
+//    (| |c|^2 - |C|^2 | <= |c - C| (2 |c| + |c - C|), sum |c_i| <= 2 sqrt(S));
+//    delta = T / S;
+//  * the denominator (S/16)^(3/4) 6 perfect, formed by two square roots,
+//    three products and the rounded constant 6 perfect, is within a factor
+//    1 +- rho_den of the exact one, rho_den = (delta + 9 u)(1 + 10 u), using
+//    (1 + delta)^(3/4) <= 1 + delta and (1 - delta)^(3/4) >= 1 - delta;
+//  * the quotient: with rho = rho_den (1 + 2u) + u and
+//    E = 13 u sqrt(n0 n1 n2) / den, |q - q_exact| <= (rho |q| + E) / (1 - rho);
+//  * the double path (the same operations with unit roundoff 2^-53 and
+//    constants at most 1.2 times these) is within 2^-27 of that bound of
+//    q_exact, which the factor (1 + 2^-20) covers; 2^-60 covers underflow
+//    of products (every edge is at least 2^-20 long by the guard below).
+//
+// The bound is evaluated with every operation rounded upward (and 1 - rho
+// downward), so it is at least the real bound. It is +inf (no decision on
+// the estimate) when lmax2 is outside [2^-40, 2^40], delta > 1/8, rho > 1/4,
+// the bound exceeds 1, or anything is not finite.
 struct Q32 {
   float q;    // estimate of tet_quality
-  float err;  // bound on |estimate - tet_quality|; inf when unbounded
+  float err;  // bound on |estimate - tet_quality in double|; +inf when none
 };
+
+constexpr float F32_U = 5.9604644775390625e-08f;  // 2^-24
 
 __device__ inline float3 f3sub(float3 a, float3 b) { return make_float3(a.x - b.x, a.y - b.y, a.z - b.z); }
 __device__ inline float3 f3cross(float3 a, float3 b)
@@ -254,9 +317,11 @@ __device__ inline float3 f3cross(float3 a, float3 b)
   return make_float3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
 }
 __device__ inline float f3dot(float3 a, float3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
-__device__ inline float f3norm(float3 a) { return sqrtf(f3dot(a, a)); }
 
-__device__ inline Q32 tet_quality_f32(double const (*x)[3], float perfect)
+// 6 * perfect_tet_quality(), formed in double and rounded once to float
+__host__ __device__ inline float tet_k6_f32() { return (float)(6.0 * perfect_tet_quality()); }
+
+__device__ inline Q32 tet_quality_f32(double const (*x)[3], float k6)
 {
   float3 d0 = make_float3((float)(x[1][0] - x[0][0]), (float)(x[1][1] - x[0][1]),
       (float)(x[1][2] - x[0][2]));
@@ -265,57 +330,119 @@ __device__ inline Q32 tet_quality_f32(double const (*x)[3], float perfect)
   float3 d2 = make_float3((float)(x[3][0] - x[0][0]), (float)(x[3][1] - x[0][1]),
       (float)(x[3][2] - x[0][2]));
   float3 e12 = f3sub(d1, d0), e13 = f3sub(d2, d0), e23 = f3sub(d2, d1);
+  // faces {0,1,2}, {1,0,3}, {2,1,3}, {0,2,3} as cross products of two edges
   float3 c0 = f3cross(d0, d1), c1 = f3cross(d0, e13), c2 = f3cross(e12, e23), c3 = f3cross(d1, d2);
-  float sum_asq = 0.25f * (f3dot(c0, c0) + f3dot(c1, c1) + f3dot(c2, c2) + f3dot(c3, c3));
-  float arms = sqrtf(sum_asq * 0.25f);
-  float v = f3dot(c0, d2) * (1.0f / 6.0f);
+  float s = f3dot(c0, c0) + f3dot(c1, c1);
+  s = s + f3dot(c2, c2);
+  s = s + f3dot(c3, c3);
+  float arms = sqrtf(s * 0.0625f);
   float r = sqrtf(arms);
-  float den = r * r * r * perfect;
+  float den = r * r * r * k6;
+  float v6 = f3dot(c0, d2);
   Q32 out;
-  out.q = v / den;
-  // the triple product is off by at most 64 eps |d0||d1||d2|; each face
-  // area by 12 eps of the square of the longest edge, so the denominator by
-  // 24 eps lmax^2 / A_rms relative; the divisions and roots add 32 eps
+  out.q = v6 / den;
+  out.err = __int_as_float(0x7f800000);
   float n0 = f3dot(d0, d0), n1 = f3dot(d1, d1), n2 = f3dot(d2, d2);
   float lmax2 = fmaxf(fmaxf(fmaxf(n0, n1), fmaxf(n2, f3dot(e12, e12))),
       fmaxf(f3dot(e13, e13), f3dot(e23, e23)));
-  float eps = 5.9604645e-08f;
-  out.err = 64.0f * eps * (sqrtf(n0) * sqrtf(n1) * sqrtf(n2) / 6.0f) / den +
-      fabsf(out.q) * eps * (32.0f + 24.0f * lmax2 / arms) + 1e-30f;
-  if (!(den > 0.0f) || !isfinite(out.q) || !isfinite(out.err)) out.err = __int_as_float(0x7f800000);
+  if (!(lmax2 >= 0x1p-40f && lmax2 <= 0x1p40f) || !(den > 0.0f) || !(s > 0.0f) ||
+      !isfinite(out.q))
+    return out;
+  float const u = F32_U;
+  float eps = __fmul_ru(9.0f * u, lmax2);
+  float t = __fadd_ru(__fadd_ru(__fmul_ru(7.0f * u, s),
+      __fmul_ru(__fmul_ru(4.0f, eps), __fsqrt_ru(s))), __fmul_ru(__fmul_ru(4.0f, eps), eps));
+  float delta = __fdiv_ru(t, s);
+  // (1 + 10u and 1 + 2u are floats; 1 + 9u and 1 + u are not)
+  float rho = __fmul_ru(__fadd_ru(delta, 9.0f * u), 1.0f + 10.0f * u);
+  rho = __fadd_ru(__fmul_ru(rho, 1.0f + 2.0f * u), u);
+  float e = __fdiv_ru(__fmul_ru(13.0f * u, __fsqrt_ru(__fmul_ru(__fmul_ru(n0, n1), n2))), den);
+  float b = __fdiv_ru(__fadd_ru(__fmul_ru(rho, fabsf(out.q)), e), __fadd_rd(1.0f, -rho));
+  b = __fadd_ru(__fmul_ru(b, 1.0f + 0x1p-20f), 0x1p-60f);
+  if (delta <= 0.125f && rho <= 0.25f && b <= 1.0f) out.err = b;
   return out;
 }
 
-// which side of `thr` the metric edge length |xb - xa| / ((ha + hb) / 2)
-// lies on, from a single-precision estimate: +1 above, -1 below, 0 when the
-// estimate is within 64 float epsilons (relative) of the threshold
+// bounds of the interval the double value lies in (rounded outward)
+__device__ inline float q32_lo(Q32 e) { return __fadd_rd(e.q, -e.err); }
+__device__ inline float q32_hi(Q32 e) { return __fadd_ru(e.q, e.err); }
+
+// Which side of `thr` the metric edge length |xb - xa| / ((ha + hb) / 2),
+// as the double path computes it, lies on, from a single-precision estimate:
+// +1 above, -1 below, 0 undecided. The estimate (differences rounded to
+// float, a float dot product, square root, the mean size rounded to float,
+// one division) is within 5.5001 u relative of the exact ratio and the
+// double path within 4.6 * 2^-53, so an estimate with est (1 - 6u) > thr
+// (formed in double: the product's rounding costs 2^-53) is above for both,
+// and est (1 + 6u) < thr below. Undecided when the squared length or the
+// mean size is outside [2^-100, 2^100] or the estimate is not finite.
 __device__ inline int edge_ratio_side_f32(double const* xa, double const* xb, double ha,
     double hb, double thr)
 {
   float3 d = make_float3((float)(xb[0] - xa[0]), (float)(xb[1] - xa[1]), (float)(xb[2] - xa[2]));
-  float r = sqrtf(f3dot(d, d)) / (float)((ha + hb) / 2);
-  float t = (float)thr, band = 64.0f * 5.9604645e-08f * t;
-  if (!isfinite(r)) return 0;
-  if (r > t + band) return 1;
-  if (r < t - band) return -1;
+  float s = f3dot(d, d);
+  float hv = (float)((ha + hb) / 2);
+  if (!(s >= 0x1p-100f && s <= 0x1p100f && hv >= 0x1p-100f && hv <= 0x1p100f)) return 0;
+  float r = sqrtf(s) / hv;
+  double const u = 0x1p-24;
+  if ((double)r * (1.0 - 6.0 * u) > thr) return 1;
+  if ((double)r * (1.0 + 6.0 * u) < thr) return -1;
   return 0;
 }
 
-// device counters of the filter: candidates rejected on the estimate,
-// candidates recomputed in double, the largest |estimate - double| seen and
-// the number of times that exceeded the bound
+// device counters of the filter. decided / rechecked: decisions taken on
+// the estimate and candidates that needed double values; max_err_bits /
+// bound_exceeded: the largest |estimate - double| among estimates whose
+// double value was computed, and how many exceeded their bound. With
+// `audit` set (by the host, for tests), every decision taken on the
+// estimate is also taken in double: audited counts them, flips counts those
+// the double path takes differently, checked counts the estimates compared
+// with their double value (bound_exceeded then covers all of them).
 struct Fp32Stats {
   unsigned long long decided;
   unsigned long long rechecked;
   unsigned int max_err_bits;
   unsigned int bound_exceeded;
+  unsigned int audit;
+  unsigned int pad;
+  unsigned long long audited;
+  unsigned long long flips;
+  unsigned long long checked;
 };
 
+// one estimate against its double value; lanes of the calling warp that are
+// active here aggregate before touching the counters
 __device__ inline void fp32_note_error(Fp32Stats* st, Q32 e, double q64)
 {
-  float diff = fabsf((float)(q64 - (double)e.q));
-  atomicMax(&st->max_err_bits, __float_as_uint(diff));
-  if ((double)diff > (double)e.err) atomicAdd(&st->bound_exceeded, 1u);
+  double d = fabs(q64 - (double)e.q);
+  float diff = __double2float_ru(d);
+  bool over = d > (double)e.err;
+  unsigned m = __activemask();
+  unsigned lead = __ffs(m) - 1;
+  unsigned mx = __reduce_max_sync(m, __float_as_uint(diff));
+  unsigned nover = __popc(__ballot_sync(m, over));
+  if ((threadIdx.x & 31) == lead) {
+    atomicMax(&st->max_err_bits, mx);
+    if (nover) atomicAdd(&st->bound_exceeded, nover);
+    if (st->audit) atomicAdd(&st->checked, (unsigned long long)__popc(m));
+  }
+}
+
+// per-warp sums of the decided / rechecked / audited / flipped flags; every
+// lane of the warp must call it
+__device__ inline void fp32_count_warp(Fp32Stats* st, bool decided, bool rechecked,
+    bool audited, bool flipped)
+{
+  unsigned nd = __popc(__ballot_sync(0xffffffffu, decided));
+  unsigned nr = __popc(__ballot_sync(0xffffffffu, rechecked));
+  unsigned na = __popc(__ballot_sync(0xffffffffu, audited));
+  unsigned nf = __popc(__ballot_sync(0xffffffffu, flipped));
+  if ((threadIdx.x & 31) == 0) {
+    if (nd) atomicAdd(&st->decided, (unsigned long long)nd);
+    if (nr) atomicAdd(&st->rechecked, (unsigned long long)nr);
+    if (na) atomicAdd(&st->audited, (unsigned long long)na);
+    if (nf) atomicAdd(&st->flips, (unsigned long long)nf);
+  }
 }
 
 // tet_quality (quality.hpp:68-89): Shewchuk's V / A_rms^(3/2), normalised

@@ -28,6 +28,7 @@ namespace {
 __global__ void k_estimate_elements(u32 dim, u32 ne, u32 const* __restrict__ voe,
     double const* __restrict__ x, double const* __restrict__ h, double* out)
 {
+  pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   double r = 0;
   if (i < ne) {
@@ -68,8 +69,8 @@ unsigned long long estimate_bytes(Mesh& m)
   if (h && ne && m.dim >= 2) {
     double* sum = dalloc<double>(1, m.s);
     CK(cudaMemsetAsync(sum, 0, sizeof(double), m.s));
-    k_estimate_elements<<<grid_for(ne), BLOCK, 0, m.s>>>(m.dim, ne, m.ask_down(m.dim, 0),
-        m.coords(), static_cast<double const*>(h->data), sum);
+    CK(launch_kernel(k_estimate_elements, dim3(grid_for(ne)), dim3(BLOCK), 0, m.s, m.dim, ne, m.ask_down(m.dim, 0),
+        m.coords(), static_cast<double const*>(h->data), sum));
     CK_LAUNCH();
     est = std::max(est, read_f64(sum, m.s));
     dev_free(sum, m.s);

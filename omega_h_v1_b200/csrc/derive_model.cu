@@ -29,6 +29,7 @@ constexpr u32 UF_CAP = 1u << 24;  // bound on any union-find walk or retry loop
 __global__ void k_side_class(u32 ns, u32 D, u32 const* __restrict__ offs,
     u32* __restrict__ bside, u32* __restrict__ scd)
 {
+  pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= ns) return;
   u32 b = (offs[i + 1] - offs[i]) < 2 ? 1u : 0u;
@@ -41,6 +42,7 @@ __global__ void k_side_class(u32 ns, u32 D, u32 const* __restrict__ offs,
 __global__ void k_side_normals(u32 ns, u32 D, u32 const* __restrict__ vos,
     double const* __restrict__ x, u32 const* __restrict__ bside, double* __restrict__ nrm)
 {
+  pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= ns) return;
   double nn[3] = {0.0, 0.0, 0.0};
@@ -75,6 +77,7 @@ __global__ void k_hinge_class(u32 nh, u32 const* __restrict__ offs, u32 const* _
     double cos_hi, u32* __restrict__ bh, u32* __restrict__ crease, double* __restrict__ dots,
     u32* __restrict__ namb, u32* __restrict__ amb)
 {
+  pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nh) return;
   u32 a[2] = {0, 0}, na = 0;
@@ -99,6 +102,7 @@ __global__ void k_hinge_class(u32 nh, u32 const* __restrict__ offs, u32 const* _
 __global__ void k_set_flags(u32 n, u32 const* __restrict__ idx, u32 const* __restrict__ val,
     u32* __restrict__ out)
 {
+  pdl_wait();
   u32 k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k < n) out[idx[k]] = val[k];
 }
@@ -106,6 +110,7 @@ __global__ void k_set_flags(u32 n, u32 const* __restrict__ idx, u32 const* __res
 __global__ void k_hinge_cd(u32 nh, u32 D, u32 const* __restrict__ bh,
     u32 const* __restrict__ crease, u32* __restrict__ hcd)
 {
+  pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < nh) hcd[i] = D - bh[i] - crease[i];
 }
@@ -115,6 +120,7 @@ __global__ void k_hinge_cd(u32 nh, u32 D, u32 const* __restrict__ bh,
 __global__ void k_vertex_class(u32 nv, u32 const* __restrict__ offs, u32 const* __restrict__ adj,
     u32 const* __restrict__ crease, u32 const* __restrict__ hcd, u32* __restrict__ vcd)
 {
+  pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nv) return;
   u32 nin = 0, d = 3;
@@ -128,6 +134,7 @@ __global__ void k_vertex_class(u32 nv, u32 const* __restrict__ offs, u32 const* 
 
 __global__ void k_is_value(u32 n, u32 const* __restrict__ a, u32 v, u32* __restrict__ out)
 {
+  pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) out[i] = a[i] == v ? 1u : 0u;
 }
@@ -135,6 +142,7 @@ __global__ void k_is_value(u32 n, u32 const* __restrict__ a, u32 v, u32* __restr
 __global__ void k_vertex_ids(u32 n, u32 const* __restrict__ cd, u32 const* __restrict__ scan,
     u32* __restrict__ cid)
 {
+  pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) cid[i] = cd[i] == 0 ? scan[i] : INV;
 }
@@ -154,6 +162,7 @@ __device__ u32 uf_find(u32* parent, u32 x, u32* fail)
 
 __global__ void k_cc_init(u32 n, u32 const* __restrict__ cd, u32 d, u32* __restrict__ parent)
 {
+  pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) parent[i] = cd[i] == d ? i : INV;
 }
@@ -164,6 +173,7 @@ __global__ void k_cc_hook(u32 n, u32 spd, u32 const* __restrict__ sod,
     u32 const* __restrict__ cds, u32 const* __restrict__ offs, u32 const* __restrict__ adj,
     u32 const* __restrict__ cdd, u32 d, u32* parent, u32* fail)
 {
+  pdl_wait();
   u32 t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n * spd) return;
   u32 u = t / spd;
@@ -195,6 +205,7 @@ __global__ void k_cc_hook(u32 n, u32 spd, u32 const* __restrict__ sod,
 
 __global__ void k_cc_flatten(u32 n, u32* parent, u32* __restrict__ is_root, u32* fail)
 {
+  pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   u32 p = parent[i];
@@ -210,6 +221,7 @@ __global__ void k_cc_flatten(u32 n, u32* parent, u32* __restrict__ is_root, u32*
 __global__ void k_cc_ids(u32 n, u32 const* __restrict__ parent, u32 const* __restrict__ scan,
     u32* __restrict__ cid)
 {
+  pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   u32 p = parent[i];
@@ -222,6 +234,7 @@ __global__ void k_project_ids(u32 n, u32 const* __restrict__ offs, u32 const* __
     u32 const* __restrict__ cd_hi, u32 const* __restrict__ cid_hi,
     u32 const* __restrict__ cd_lo, u32* __restrict__ cid_lo)
 {
+  pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   u32 c = cd_lo[i], id = cid_lo[i];
@@ -248,14 +261,14 @@ void Mesh::derive_model(double crease_angle)
   u32* bside = dalloc<u32>(ns, s);
   cd[D - 1] = dalloc<u32>(ns, s);
   if (ns) {
-    k_side_class<<<grid_for(ns), BLOCK, 0, s>>>(ns, D, es.offs, bside, cd[D - 1]);
+    CK(launch_kernel(k_side_class, dim3(grid_for(ns)), dim3(BLOCK), 0, s, ns, D, es.offs, bside, cd[D - 1]));
     CK_LAUNCH();
   }
   add_tag(D - 1, T_U32, "class_dim", 1, X_NOT, cd[D - 1]);
   double* nrm = dalloc<double>((size_t)ns * 3, s);
   if (ns) {
-    k_side_normals<<<grid_for(ns), BLOCK, 0, s>>>(ns, D, ask_down(D - 1, 0), coords(), bside,
-        nrm);
+    CK(launch_kernel(k_side_normals, dim3(grid_for(ns)), dim3(BLOCK), 0, s, ns, D, ask_down(D - 1, 0), coords(), bside,
+        nrm));
     CK_LAUNCH();
   }
   // hinges
@@ -269,8 +282,8 @@ void Mesh::derive_model(double crease_angle)
   CK(cudaMemsetAsync(namb, 0, sizeof(u32), s));
   double cc = std::cos(crease_angle);
   if (nh) {
-    k_hinge_class<<<grid_for(nh), BLOCK, 0, s>>>(nh, sh.offs, sh.adj, bside, nrm, cc - 1e-9,
-        cc + 1e-9, bh, crease, dots, namb, amb);
+    CK(launch_kernel(k_hinge_class, dim3(grid_for(nh)), dim3(BLOCK), 0, s, nh, sh.offs, sh.adj, bside, nrm, cc - 1e-9,
+        cc + 1e-9, bh, crease, dots, namb, amb));
     CK_LAUNCH();
   }
   mb->fetch(s, 25);
@@ -291,7 +304,7 @@ void Mesh::derive_model(double crease_angle)
     u32* di = dalloc<u32>(2 * (size_t)na, s);
     CK(cudaMemcpyAsync(di, idx.data(), sizeof(u32) * na, cudaMemcpyHostToDevice, s));
     CK(cudaMemcpyAsync(di + na, val.data(), sizeof(u32) * na, cudaMemcpyHostToDevice, s));
-    k_set_flags<<<grid_for(na), BLOCK, 0, s>>>(na, di, di + na, crease);
+    CK(launch_kernel(k_set_flags, dim3(grid_for(na)), dim3(BLOCK), 0, s, na, di, di + na, crease));
     CK_LAUNCH();
     stream_sync(s);
     dev_free(di, s);
@@ -301,7 +314,7 @@ void Mesh::derive_model(double crease_angle)
   dev_free(nrm, s);
   cd[D - 2] = dalloc<u32>(nh, s);
   if (nh) {
-    k_hinge_cd<<<grid_for(nh), BLOCK, 0, s>>>(nh, D, bh, crease, cd[D - 2]);
+    CK(launch_kernel(k_hinge_cd, dim3(grid_for(nh)), dim3(BLOCK), 0, s, nh, D, bh, crease, cd[D - 2]));
     CK_LAUNCH();
   }
   add_tag(D - 2, T_U32, "class_dim", 1, X_NOT, cd[D - 2]);
@@ -310,8 +323,8 @@ void Mesh::derive_model(double crease_angle)
     UpAdj const& ev = ask_up(0, 1, false);
     cd[0] = dalloc<u32>(nv, s);
     if (nv) {
-      k_vertex_class<<<grid_for(nv), BLOCK, 0, s>>>(nv, ev.offs, ev.adj, crease, cd[D - 2],
-          cd[0]);
+      CK(launch_kernel(k_vertex_class, dim3(grid_for(nv)), dim3(BLOCK), 0, s, nv, ev.offs, ev.adj, crease, cd[D - 2],
+          cd[0]));
       CK_LAUNCH();
     }
     add_tag(0, T_U32, "class_dim", 1, X_NOT, cd[0]);
@@ -325,13 +338,13 @@ void Mesh::derive_model(double crease_angle)
     u32 nv = count(0);
     u32* f = dalloc<u32>(nv ? nv : 1, s);
     if (nv) {
-      k_is_value<<<grid_for(nv), BLOCK, 0, s>>>(nv, cd[0], 0, f);
+      CK(launch_kernel(k_is_value, dim3(grid_for(nv)), dim3(BLOCK), 0, s, nv, cd[0], 0, f));
       CK_LAUNCH();
     }
     u32* sc = exscan_new(f, nv, s);
     cid[0] = dalloc<u32>(nv, s);
     if (nv) {
-      k_vertex_ids<<<grid_for(nv), BLOCK, 0, s>>>(nv, cd[0], sc, cid[0]);
+      CK(launch_kernel(k_vertex_ids, dim3(grid_for(nv)), dim3(BLOCK), 0, s, nv, cd[0], sc, cid[0]));
       CK_LAUNCH();
     }
     dev_free(sc, s);
@@ -346,17 +359,17 @@ void Mesh::derive_model(double crease_angle)
     cid[d] = dalloc<u32>(n, s);
     u32* roots = dalloc<u32>(n ? n : 1, s);
     if (n) {
-      k_cc_init<<<grid_for(n), BLOCK, 0, s>>>(n, cd[d], d, cid[d]);
+      CK(launch_kernel(k_cc_init, dim3(grid_for(n)), dim3(BLOCK), 0, s, n, cd[d], d, cid[d]));
       CK_LAUNCH();
-      k_cc_hook<<<grid_for((u64)n * spd), BLOCK, 0, s>>>(n, spd, sod, cd[d - 1], dos.offs,
-          dos.adj, cd[d], d, cid[d], fail);
+      CK(launch_kernel(k_cc_hook, dim3(grid_for((u64)n * spd)), dim3(BLOCK), 0, s, n, spd, sod, cd[d - 1], dos.offs,
+          dos.adj, cd[d], d, cid[d], fail));
       CK_LAUNCH();
-      k_cc_flatten<<<grid_for(n), BLOCK, 0, s>>>(n, cid[d], roots, fail);
+      CK(launch_kernel(k_cc_flatten, dim3(grid_for(n)), dim3(BLOCK), 0, s, n, cid[d], roots, fail));
       CK_LAUNCH();
     }
     u32* sc = exscan_new(roots, n, s);
     if (n) {
-      k_cc_ids<<<grid_for(n), BLOCK, 0, s>>>(n, cid[d], sc, cid[d]);
+      CK(launch_kernel(k_cc_ids, dim3(grid_for(n)), dim3(BLOCK), 0, s, n, cid[d], sc, cid[d]));
       CK_LAUNCH();
     }
     dev_free(sc, s);
@@ -371,8 +384,8 @@ void Mesh::derive_model(double crease_angle)
     u32 d = D - dd, nl = count(d);
     UpAdj const& u = ask_up(d, d + 1, true);
     if (nl) {
-      k_project_ids<<<grid_for(nl), BLOCK, 0, s>>>(nl, u.offs, u.adj, cd[d + 1], cid[d + 1],
-          cd[d], cid[d]);
+      CK(launch_kernel(k_project_ids, dim3(grid_for(nl)), dim3(BLOCK), 0, s, nl, u.offs, u.adj, cd[d + 1], cid[d + 1],
+          cd[d], cid[d]));
       CK_LAUNCH();
     }
   }

@@ -71,6 +71,7 @@ __global__ void k_element_gradients(u32 dim, u32 ne, u32 const* __restrict__ voe
     double const* __restrict__ x, u32 nc, double const* __restrict__ f,
     double* __restrict__ out)
 {
+  pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= ne) return;
   u32 vpe = dim + 1;
@@ -97,6 +98,7 @@ __global__ void k_recover_by_volume(u32 nv, u32 const* __restrict__ offs,
     u32 const* __restrict__ adj, double const* __restrict__ sizes, u32 nc,
     double const* __restrict__ f, double* __restrict__ out)
 {
+  pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nv) return;
   double* o = out + (size_t)i * nc;
@@ -115,6 +117,7 @@ __global__ void k_size_from_hessian(u32 nv, u32 nhc, double const* __restrict__ 
     double const* __restrict__ w, u32 nsol, double min_h, double max_h,
     double* __restrict__ out)
 {
+  pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nv) return;
   double const* hs = hess + (size_t)i * nhc;
@@ -134,6 +137,7 @@ __global__ void k_size_from_hessian(u32 nv, u32 nhc, double const* __restrict__ 
 __global__ void k_axpy(u32 n, double a, double const* __restrict__ x,
     double const* __restrict__ y, double* __restrict__ out)
 {
+  pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) out[i] = a * x[i] + y[i];
 }
@@ -141,6 +145,7 @@ __global__ void k_axpy(u32 n, double a, double const* __restrict__ x,
 __global__ void k_min_quality(u32 dim, u32 ne, u32 const* __restrict__ voe,
     double const* __restrict__ x, unsigned long long* minkey)
 {
+  pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   unsigned long long key = ~0ull;
   if (i < ne) {
@@ -167,8 +172,8 @@ void element_gradients(Mesh& m, char const* name)
   u32 dim = m.dim, ne = m.count(dim), nc = t->ncomps;
   double* out = dalloc<double>((size_t)ne * nc * 3, s);
   if (ne) {
-    k_element_gradients<<<grid_for(ne), BLOCK, 0, s>>>(dim, ne, m.ask_down(dim, 0), m.coords(),
-        nc, static_cast<double const*>(t->data), out);
+    CK(launch_kernel(k_element_gradients, dim3(grid_for(ne)), dim3(BLOCK), 0, s, dim, ne, m.ask_down(dim, 0), m.coords(),
+        nc, static_cast<double const*>(t->data), out));
     CK_LAUNCH();
   }
   m.add_tag(dim, T_F64, (std::string("grad_") + name).c_str(), nc * 3, X_NOT, out);
@@ -185,8 +190,8 @@ void recover_by_volume(Mesh& m, char const* name)
   double* sizes = m.element_sizes();
   double* out = dalloc<double>((size_t)nv * nc, s);
   if (nv) {
-    k_recover_by_volume<<<grid_for(nv), BLOCK, 0, s>>>(nv, ve.offs, ve.adj, sizes, nc,
-        static_cast<double const*>(m.find_tag(dim, name)->data), out);
+    CK(launch_kernel(k_recover_by_volume, dim3(grid_for(nv)), dim3(BLOCK), 0, s, nv, ve.offs, ve.adj, sizes, nc,
+        static_cast<double const*>(m.find_tag(dim, name)->data), out));
     CK_LAUNCH();
   }
   dev_free(sizes, s);
@@ -211,8 +216,8 @@ void size_from_hessian(Mesh& m, char const* hess_name, double const* weights, do
   }
   double* out = dalloc<double>(nv, s);
   if (nv) {
-    k_size_from_hessian<<<grid_for(nv), BLOCK, 0, s>>>(nv, t->ncomps,
-        static_cast<double const*>(t->data), w, nsol, min_h, max_h, out);
+    CK(launch_kernel(k_size_from_hessian, dim3(grid_for(nv)), dim3(BLOCK), 0, s, nv, t->ncomps,
+        static_cast<double const*>(t->data), w, nsol, min_h, max_h, out));
     CK_LAUNCH();
   }
   stream_sync(s);
@@ -227,7 +232,7 @@ static double min_quality_of(Mesh& m, double const* x)
   unsigned long long* mk = reinterpret_cast<unsigned long long*>(m.mb->dev + 30);
   CK(cudaMemsetAsync(mk, 0xff, sizeof(unsigned long long), s));
   if (ne) {
-    k_min_quality<<<grid_for(ne), BLOCK, 0, s>>>(m.dim, ne, m.ask_down(m.dim, 0), x, mk);
+    CK(launch_kernel(k_min_quality, dim3(grid_for(ne)), dim3(BLOCK), 0, s, m.dim, ne, m.ask_down(m.dim, 0), x, mk));
     CK_LAUNCH();
   }
   m.mb->fetch(s, 32);
@@ -250,7 +255,7 @@ u32 warp_to_limit(Mesh& m, double qual_floor)
   u32 hit = 0;
   auto apply = [&]() {
     if (n) {
-      k_axpy<<<grid_for(n), BLOCK, 0, s>>>(n, factor, w, x, xo);
+      CK(launch_kernel(k_axpy, dim3(grid_for(n)), dim3(BLOCK), 0, s, n, factor, w, x, xo));
       CK_LAUNCH();
     }
   };
@@ -265,7 +270,7 @@ u32 warp_to_limit(Mesh& m, double qual_floor)
   }
   double* wo = dalloc<double>(n, s);
   if (n) {
-    k_axpy<<<grid_for(n), BLOCK, 0, s>>>(n, -factor, w, w, wo);
+    CK(launch_kernel(k_axpy, dim3(grid_for(n)), dim3(BLOCK), 0, s, n, -factor, w, w, wo));
     CK_LAUNCH();
   }
   m.remove_tag(0, "coordinates");

@@ -24,6 +24,7 @@ PassStats& last_pass_stats()
 __global__ void k_indset_init(u32 n, u32 const* __restrict__ filter, u32* __restrict__ st,
     u32* first_flag)
 {
+  pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i == 0) *first_flag = 0;
   if (i < n) st[i] = filter[i] ? (u32)UNKNOWN : (u32)NOT_IN_SET;
@@ -66,6 +67,7 @@ __global__ void k_indset_round(u32 n, Nbrs g, u32 const* __restrict__ old_st,
     u32* __restrict__ st, double const* __restrict__ good,
     u64 const* __restrict__ glob, u32* unknown_left, u32* next_flag)
 {
+  pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i == 0) *next_flag = 0;
   if (i >= n) return;
@@ -95,6 +97,83 @@ __global__ void k_indset_round(u32 n, Nbrs g, u32 const* __restrict__ old_st,
     st[i] = UNKNOWN;
     *unknown_left = 1;
   }
+}
+
+// The same round with a group of G lanes per entity (G divides 32, so a
+// group never straddles a warp): lane l of a group walks the entity's
+// upward entries l, l + G, ..., each lane folds its neighbours into two
+// flags, and two ballots over the group give "a neighbour is in the set" and
+// "no neighbour beats me". The rule depends on the neighbour set only, so
+// the walk order does not matter. (One thread per long row issues loads
+// whose lanes are a row apart and fills the load/store queue.)
+template <int G>
+__global__ void k_indset_round_grouped(u32 n, Nbrs g, u32 const* __restrict__ old_st,
+    u32* __restrict__ st, double const* __restrict__ good,
+    u64 const* __restrict__ glob, u32* unknown_left, u32* next_flag)
+{
+  pdl_wait();
+  u32 const t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t == 0) *next_flag = 0;
+  u32 const i = t / G, lg = t % G;
+  if (i >= n) return;  // a group shares i: it leaves together
+  u32 const gbase = (threadIdx.x & 31) & ~(u32)(G - 1);
+  u32 const gmask = (G == 32 ? 0xffffffffu : ((1u << G) - 1u)) << gbase;
+  u32 const s0 = old_st[i];
+  if (s0 != UNKNOWN) {
+    if (lg == 0) st[i] = s0;
+    return;
+  }
+  u32 const b = g.offs[i], e = g.offs[i + 1];
+  double const myg = good[i];
+  u64 const myid = glob ? glob[i] : (u64)i;
+  bool in_set = false, beaten = false;
+  auto visit = [&](u32 o) {
+    u32 so = old_st[o];
+    if (so == IN_SET) in_set = true;
+    if (so == NOT_IN_SET) return;
+    double og = good[o];
+    u64 oid = glob ? glob[o] : (u64)o;
+    if ((myg == og && oid < myid) || myg < og) beaten = true;
+  };
+  for (u32 j = b + lg; j < e; j += G) {
+    if (g.mode == 0) {
+      visit(g.down[g.adj[j] * 2 + (1 - g.dirs[j])]);
+    } else {
+      u32 const* ds = g.down + (size_t)g.adj[j] * g.per;
+      for (u32 k = 0; k < g.per; ++k)
+        if (ds[k] != i) visit(ds[k]);
+    }
+  }
+  bool const any_in = (__ballot_sync(gmask, in_set) & gmask) != 0;
+  bool const lost = (__ballot_sync(gmask, beaten) & gmask) != 0;
+  if (lg == 0) {
+    if (any_in) {
+      st[i] = NOT_IN_SET;
+    } else if (!lost) {
+      st[i] = IN_SET;
+    } else {
+      st[i] = UNKNOWN;
+      *unknown_left = 1;
+    }
+  }
+}
+
+static void launch_indset_round(u32 n, Nbrs const& g, double avg_row, u32 const* old_st,
+    u32* st, double const* good, u64 const* glob, u32* flag, u32* next_flag, cudaStream_t s)
+{
+  // lanes per entity from the mean upward row length: vertex rows (about
+  // 13.5 edges) take 8, edge rows in 3D (about 5 tets) 4, 2D rows 2
+  if (avg_row >= 8.0) {
+    CK(launch_kernel(k_indset_round_grouped<8>, dim3(grid_for((u64)n * 8)), dim3(BLOCK), 0, s, n, g, old_st, st, good,
+        glob, flag, next_flag));
+  } else if (avg_row >= 3.0) {
+    CK(launch_kernel(k_indset_round_grouped<4>, dim3(grid_for((u64)n * 4)), dim3(BLOCK), 0, s, n, g, old_st, st, good,
+        glob, flag, next_flag));
+  } else {
+    CK(launch_kernel(k_indset_round_grouped<2>, dim3(grid_for((u64)n * 2)), dim3(BLOCK), 0, s, n, g, old_st, st, good,
+        glob, flag, next_flag));
+  }
+  CK_LAUNCH();
 }
 
 // number of upward uses walked per round (edges of vertices / elements of
@@ -134,7 +213,7 @@ u32* find_indset(Mesh& m, u32 ent_dim, u32 const* filter, double const* good)
   // the "anything left" flags of even and odd rounds (mailbox slots 0, 40)
   u32 const flag_slot[2] = {0, 40};
   if (n) {
-    k_indset_init<<<grid_for(n), BLOCK, 0, m.s>>>(n, filter, a, m.mb->dev + flag_slot[0]);
+    CK(launch_kernel(k_indset_init, dim3(grid_for(n)), dim3(BLOCK), 0, m.s, n, filter, a, m.mb->dev + flag_slot[0]));
     CK_LAUNCH();
   }
   // Rounds are issued in batches and the "anything left" flag is read once
@@ -152,9 +231,8 @@ u32* find_indset(Mesh& m, u32 ent_dim, u32 const* filter, double const* good)
       double nuse = (double)read_cached_uses(m, ent_dim);
       PROBE(P_INDSET_ROUND, m.s, 4.0 * (n + 1.0) + 4.0 * nuse + via_bytes +
           4.0 * n + 8.0 * n + (glob ? 8.0 * n : 0.0) + 4.0 * n);
-      k_indset_round<<<grid_for(n), BLOCK, 0, m.s>>>(n, g, a, b, good, glob,
-          m.mb->dev + flag_slot[rounds % 2], m.mb->dev + flag_slot[(rounds + 1) % 2]);
-      CK_LAUNCH();
+      launch_indset_round(n, g, n ? nuse / n : 0.0, a, b, good, glob,
+          m.mb->dev + flag_slot[rounds % 2], m.mb->dev + flag_slot[(rounds + 1) % 2], m.s);
       std::swap(a, b);
       ++rounds;
     }
@@ -179,6 +257,7 @@ template <class T>
 __global__ void k_expand_scaled(T const* __restrict__ in, u32 const* __restrict__ offs,
     u32 k, u32 n, u32 width, T* __restrict__ out)
 {
+  pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   u32 f = offs[i] * k, e = offs[i + 1] * k;
@@ -192,14 +271,14 @@ void expand_scaled(void const* in, u32 const* offs, u32 k, u32 n, u32 width,
   if (!n || !width || !k) return;
   PROBE(P_EXPAND, s, 4.0 * (n + 1) + 2.0 * (double)n * width * esz * k);
   if (esz == 1)
-    k_expand_scaled<unsigned char><<<grid_for(n), BLOCK, 0, s>>>(
-        (unsigned char const*)in, offs, k, n, width, (unsigned char*)out);
+    CK(launch_kernel(k_expand_scaled<unsigned char>, dim3(grid_for(n)), dim3(BLOCK), 0, s, 
+        (unsigned char const*)in, offs, k, n, width, (unsigned char*)out));
   else if (esz == 4)
-    k_expand_scaled<u32><<<grid_for(n), BLOCK, 0, s>>>(
-        (u32 const*)in, offs, k, n, width, (u32*)out);
+    CK(launch_kernel(k_expand_scaled<u32>, dim3(grid_for(n)), dim3(BLOCK), 0, s, 
+        (u32 const*)in, offs, k, n, width, (u32*)out));
   else
-    k_expand_scaled<unsigned long long><<<grid_for(n), BLOCK, 0, s>>>(
-        (unsigned long long const*)in, offs, k, n, width, (unsigned long long*)out);
+    CK(launch_kernel(k_expand_scaled<unsigned long long>, dim3(grid_for(n)), dim3(BLOCK), 0, s, 
+        (unsigned long long const*)in, offs, k, n, width, (unsigned long long*)out));
   CK_LAUNCH();
 }
 
@@ -211,6 +290,7 @@ struct ExpandJobs {
 
 __global__ void k_expand_many(ExpandJobs jobs)
 {
+  pdl_wait();
   ExpandJob const jb = jobs.j[blockIdx.y];
   for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < jb.n; i += gridDim.x * blockDim.x) {
     u32 f = jb.offs[i] * jb.k, e = jb.offs[i + 1] * jb.k;
@@ -250,7 +330,7 @@ void expand_many(std::vector<ExpandJob> const& jobs, cudaStream_t s)
     }
     PROBE(P_EXPAND, s, bytes);
     dim3 grid(std::min<u32>(grid_for(nmax), 148u * 16u), cnt);
-    k_expand_many<<<grid, BLOCK, 0, s>>>(pack);
+    CK(launch_kernel(k_expand_many, dim3(grid), dim3(BLOCK), 0, s, pack));
     CK_LAUNCH();
   }
 }
@@ -299,6 +379,7 @@ void inherit_globals(Mesh& out, u32 d, u32 n)
 __global__ void k_interp_coords(u32 ne, u32 vpe, u32 const* __restrict__ voe,
     double const* __restrict__ x, double* __restrict__ out)
 {
+  pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= ne) return;
   // average_element_field (element_field.hpp:9-25)
@@ -319,8 +400,8 @@ void interp_coords_to_elems(Mesh& m)
   u32 ne = m.count(m.dim), vpe = deg(m.dim, 0);
   double* out = dalloc<double>((size_t)ne * 3, m.s);
   if (ne) {
-    k_interp_coords<<<grid_for(ne), BLOCK, 0, m.s>>>(ne, vpe, m.ask_down(m.dim, 0),
-        m.coords(), out);
+    CK(launch_kernel(k_interp_coords, dim3(grid_for(ne)), dim3(BLOCK), 0, m.s, ne, vpe, m.ask_down(m.dim, 0),
+        m.coords(), out));
     CK_LAUNCH();
   }
   m.add_tag(m.dim, T_F64, "coordinates", 3, X_NOT, out);
@@ -332,6 +413,7 @@ void interp_coords_to_elems(Mesh& m)
 __global__ void k_mark_down(u32 n, u32 const* __restrict__ offs, u32 const* __restrict__ adj,
     u32 const* __restrict__ marked, u32* __restrict__ out)
 {
+  pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   u32 r = 0;
@@ -349,7 +431,7 @@ u32* mark_down(Mesh& m, u32 high, u32 low, u32 const* marked)
   UpAdj const& u = m.ask_up(low, high, false);
   u32* out = dalloc<u32>(n, m.s);
   if (n) {
-    k_mark_down<<<grid_for(n), BLOCK, 0, m.s>>>(n, u.offs, u.adj, marked, out);
+    CK(launch_kernel(k_mark_down, dim3(grid_for(n)), dim3(BLOCK), 0, m.s, n, u.offs, u.adj, marked, out));
     CK_LAUNCH();
   }
   return out;
@@ -358,6 +440,7 @@ u32* mark_down(Mesh& m, u32 high, u32 low, u32 const* marked)
 __global__ void k_mark_up(u32 n, u32 lph, u32 const* __restrict__ loh,
     u32 const* __restrict__ marked, u32* __restrict__ out)
 {
+  pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   u32 r = 0;
@@ -374,8 +457,8 @@ u32* mark_up(Mesh& m, u32 low, u32 high, u32 const* marked)
   u32 n = m.count(high);
   u32* out = dalloc<u32>(n, m.s);
   if (n) {
-    k_mark_up<<<grid_for(n), BLOCK, 0, m.s>>>(n, deg(high, low), m.ask_down(high, low),
-        marked, out);
+    CK(launch_kernel(k_mark_up, dim3(grid_for(n)), dim3(BLOCK), 0, m.s, n, deg(high, low), m.ask_down(high, low),
+        marked, out));
     CK_LAUNCH();
   }
   return out;
@@ -384,6 +467,7 @@ u32* mark_up(Mesh& m, u32 low, u32 high, u32 const* marked)
 __global__ void k_mark_slivers(u32 n, double const* __restrict__ q, double gq,
     u32 const* __restrict__ voe, u32 vpe, SegView sv, u32* __restrict__ out)
 {
+  pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) out[i] = (q[i] < gq && (!sv.active || seg_acts(sv, voe[(size_t)i * vpe]))) ? 1u : 0u;
 }
@@ -392,6 +476,7 @@ __global__ void k_mark_slivers(u32 n, double const* __restrict__ q, double gq,
 __global__ void k_seg_tally(u32 n, u32 const* __restrict__ flags, u32 const* __restrict__ voe,
     u32 vpe, u32 const* __restrict__ seg, u32* __restrict__ out)
 {
+  pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   bool on = i < n && flags[i] != 0;
   u32 mask = __ballot_sync(0xffffffffu, on);
@@ -407,14 +492,15 @@ void seg_tally(Mesh& m, u32 ent_dim, u32 const* flags)
   u32 n = m.count(ent_dim);
   if (!n) return;
   u32 const* voe = ent_dim ? m.ask_down(ent_dim, 0) : nullptr;
-  k_seg_tally<<<grid_for(n), BLOCK, 0, m.s>>>(n, flags, voe, deg(ent_dim, 0), m.seg,
-      m.ctl->selected);
+  CK(launch_kernel(k_seg_tally, dim3(grid_for(n)), dim3(BLOCK), 0, m.s, n, flags, voe, deg(ent_dim, 0), m.seg,
+      m.ctl->selected));
   CK_LAUNCH();
 }
 
 __global__ void k_dual_layer(u32 n, u32 degr, u32 const* __restrict__ dual,
     u32 const* __restrict__ in, u32* __restrict__ out)
 {
+  pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   u32 r = in[i];
@@ -433,8 +519,8 @@ u32* mark_slivers(Mesh& m, double gq, u32 nlayers)
   u32* a = dalloc<u32>(n, m.s);
   if (n) {
     SegView sv = m.segview();
-    k_mark_slivers<<<grid_for(n), BLOCK, 0, m.s>>>(n, q, gq,
-        sv.active ? m.ask_down(m.dim, 0) : nullptr, deg(m.dim, 0), sv, a);
+    CK(launch_kernel(k_mark_slivers, dim3(grid_for(n)), dim3(BLOCK), 0, m.s, n, q, gq,
+        sv.active ? m.ask_down(m.dim, 0) : nullptr, deg(m.dim, 0), sv, a));
     CK_LAUNCH();
   }
   if (!nlayers) return a;
@@ -443,7 +529,7 @@ u32* mark_slivers(Mesh& m, double gq, u32 nlayers)
   u32 degr = deg(m.dim, m.dim - 1);
   for (u32 l = 0; l < nlayers; ++l) {
     if (n) {
-      k_dual_layer<<<grid_for(n), BLOCK, 0, m.s>>>(n, degr, du, a, b);
+      CK(launch_kernel(k_dual_layer, dim3(grid_for(n)), dim3(BLOCK), 0, m.s, n, degr, du, a, b));
       CK_LAUNCH();
     }
     std::swap(a, b);

@@ -339,6 +339,7 @@ void Mesh::make_parallel()
 
 __global__ void k_count_lows(u32 const* __restrict__ loh, u32 nuses, u32* cnt)
 {
+  pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < nuses) atomicAdd(&cnt[loh[i]], 1u);
 }
@@ -349,6 +350,7 @@ __global__ void k_count_lows(u32 const* __restrict__ loh, u32 nuses, u32* cnt)
 __global__ void k_fill_uses(u32 const* __restrict__ loh, u32 nuses,
     u32 const* __restrict__ offs, u32* cnt, u32* __restrict__ tmp)
 {
+  pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nuses) return;
   u32 l = loh[i];
@@ -361,6 +363,7 @@ __global__ void k_fill_uses(u32 const* __restrict__ loh, u32 nuses,
 __global__ void k_rank_rows(u32 const* __restrict__ offs, u32 const* __restrict__ tmp,
     u32 nrows, u32 lph, u32* __restrict__ adj, u32* __restrict__ dirs)
 {
+  pdl_wait();
   u32 row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   u32 lane = threadIdx.x & 31;
   if (row >= nrows) return;
@@ -396,6 +399,7 @@ k_sort_rows(u32 const* __restrict__ offs, u32 const* __restrict__ pre,
     u32 const* __restrict__ tmp, u32 nrows, u32 lph, u32* __restrict__ adj,
     u32* __restrict__ dirs)
 {
+  pdl_wait();
   constexpr int N = G * K;
   u32 row = (blockIdx.x * blockDim.x + threadIdx.x) / G;
   u32 l = threadIdx.x % G;
@@ -453,7 +457,7 @@ static void launch_sort_rows(u32 const* offs, u32 const* pre, u32 const* tmp, u3
     u32 lph, u32* adj, u32* dirs, cudaStream_t s)
 {
   u64 threads = (u64)nrows * G;
-  k_sort_rows<G, K><<<grid_for(threads), 256, 0, s>>>(offs, pre, tmp, nrows, lph, adj, dirs);
+  CK(launch_kernel(k_sort_rows<G, K>, dim3(grid_for(threads)), dim3(256), 0, s, offs, pre, tmp, nrows, lph, adj, dirs));
   CK_LAUNCH();
 }
 
@@ -477,6 +481,7 @@ static void rank_rows(u32 const* offs, u32 const* pre, u32 const* tmp, u32 nrows
 __global__ void k_fill_uses_split(u32 const* __restrict__ loh, u32 nuses, u32 lph,
     u32 const* __restrict__ offs, u32* cnt, u32* __restrict__ adj, u32* __restrict__ dirs)
 {
+  pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nuses) return;
   u32 l = loh[i];
@@ -488,6 +493,7 @@ __global__ void k_fill_uses_split(u32 const* __restrict__ loh, u32 nuses, u32 lp
 __global__ void k_join_uses(u32 n, u32 lph, u32 const* __restrict__ adj,
     u32 const* __restrict__ dirs, u32* __restrict__ uses)
 {
+  pdl_wait();
   u32 j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j < n) uses[j] = adj[j] * lph + dirs[j];
 }
@@ -501,7 +507,7 @@ void up_from_down_unsorted(u32 high, u32 low, u32 nhighs, u32 nlows, u32 const* 
   CK(cudaMemsetAsync(cnt, 0, sizeof(u32) * ((size_t)nlows + 1), s));
   if (nuses) {
     PROBE(P_UP_COUNT, s, 4.0 * nuses + 4.0 * nlows);
-    k_count_lows<<<grid_for(nuses), BLOCK, 0, s>>>(loh, nuses, cnt);
+    CK(launch_kernel(k_count_lows, dim3(grid_for(nuses)), dim3(BLOCK), 0, s, loh, nuses, cnt));
     CK_LAUNCH();
   }
   out.offs = exscan_new(cnt, nlows, s);
@@ -509,8 +515,8 @@ void up_from_down_unsorted(u32 high, u32 low, u32 nhighs, u32 nlows, u32 const* 
   out.dirs = dalloc<u32>(nuses, s);
   if (nuses) {
     PROBE(P_UP_FILL, s, 4.0 * nuses + 4.0 * (nlows + 1.0) + 4.0 * nlows + 8.0 * nuses);
-    k_fill_uses_split<<<grid_for(nuses), BLOCK, 0, s>>>(loh, nuses, lph, out.offs, cnt,
-        out.adj, out.dirs);
+    CK(launch_kernel(k_fill_uses_split, dim3(grid_for(nuses)), dim3(BLOCK), 0, s, loh, nuses, lph, out.offs, cnt,
+        out.adj, out.dirs));
     CK_LAUNCH();
   }
   dev_free(cnt, s);
@@ -523,7 +529,7 @@ void sort_up_rows(u32 high, u32 low, u32 nhighs, u32 nlows, UpAdj const& u,
   u32 nuses = nhighs * lph;
   if (!nuses || !nlows) return;
   u32* uses = dalloc<u32>(nuses, s);
-  k_join_uses<<<grid_for(nuses), BLOCK, 0, s>>>(nuses, lph, u.adj, u.dirs, uses);
+  CK(launch_kernel(k_join_uses, dim3(grid_for(nuses)), dim3(BLOCK), 0, s, nuses, lph, u.adj, u.dirs, uses));
   CK_LAUNCH();
   {
     u32 nsort = u.pre ? nuses - u.npre : nuses;
@@ -542,7 +548,7 @@ void up_from_down(u32 high, u32 low, u32 nhighs, u32 nlows, u32 const* loh,
   CK(cudaMemsetAsync(cnt, 0, sizeof(u32) * ((size_t)nlows + 1), s));
   if (nuses) {
     PROBE(P_UP_COUNT, s, 4.0 * nuses + 4.0 * nlows);
-    k_count_lows<<<grid_for(nuses), BLOCK, 0, s>>>(loh, nuses, cnt);
+    CK(launch_kernel(k_count_lows, dim3(grid_for(nuses)), dim3(BLOCK), 0, s, loh, nuses, cnt));
     CK_LAUNCH();
   }
   out.offs = exscan_new(cnt, nlows, s);
@@ -552,7 +558,7 @@ void up_from_down(u32 high, u32 low, u32 nhighs, u32 nlows, u32 const* loh,
   if (nuses) {
     {
       PROBE(P_UP_FILL, s, 8.0 * nuses + 4.0 * (nlows + 1.0) + 4.0 * nlows);
-      k_fill_uses<<<grid_for(nuses), BLOCK, 0, s>>>(loh, nuses, out.offs, cnt, tmp);
+      CK(launch_kernel(k_fill_uses, dim3(grid_for(nuses)), dim3(BLOCK), 0, s, loh, nuses, out.offs, cnt, tmp));
       CK_LAUNCH();
     }
     if (nlows) {
@@ -585,6 +591,7 @@ __device__ inline void sort_small(u32* w, u32 n)
 
 __global__ void k_count_min_vert(u32 low, u32 nl, u32 const* __restrict__ vol, u32* cnt)
 {
+  pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nl) return;
   u32 vpl = low + 1, m = vol[(size_t)i * vpl];
@@ -597,6 +604,7 @@ __global__ void k_count_min_vert(u32 low, u32 nl, u32 const* __restrict__ vol, u
 __global__ void k_fill_min_vert(u32 low, u32 nl, u32 const* __restrict__ vol,
     u32 const* __restrict__ offs, u32* cnt, u32* __restrict__ rows)
 {
+  pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nl) return;
   u32 vpl = low + 1, w[3];
@@ -616,6 +624,7 @@ template <u32 HIGH, u32 LOW>
 __global__ void k_reflect_grouped(u32 first, u32 nh, u32 const* __restrict__ voh,
     u32 const* __restrict__ offs, u32 const* __restrict__ rows, u32* __restrict__ out)
 {
+  pdl_wait();
   constexpr u32 LPH = HIGH == 3 ? (LOW == 1 ? 6 : 4) : 3;
   constexpr u32 VPH = HIGH + 1, VPL = LOW + 1;
   u32 i = first + blockIdx.x * blockDim.x + threadIdx.x;
@@ -676,6 +685,7 @@ __global__ void k_reflect_grouped(u32 first, u32 nh, u32 const* __restrict__ voh
 __global__ void k_vertex_edge_star(u32 nadj, u32 const* __restrict__ adj,
     u32 const* __restrict__ dirs, u32 const* __restrict__ voe, u32* __restrict__ star)
 {
+  pdl_wait();
   u32 j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j < nadj) star[j] = voe[adj[j] * 2 + (1 - dirs[j])];
 }
@@ -683,6 +693,7 @@ __global__ void k_vertex_edge_star(u32 nadj, u32 const* __restrict__ adj,
 __global__ void k_scale_offsets(u32 const* __restrict__ in, u32 n1, u32 k,
     u32* __restrict__ out)
 {
+  pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n1) out[i] = in[i] * k;
 }
@@ -690,6 +701,7 @@ __global__ void k_scale_offsets(u32 const* __restrict__ in, u32 n1, u32 k,
 __global__ void k_edge_tri_star(u32 nadj, u32 const* __restrict__ adj,
     u32 const* __restrict__ dirs, u32 const* __restrict__ eot, u32* __restrict__ star)
 {
+  pdl_wait();
   u32 j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= nadj) return;
   u32 t = adj[j], d = dirs[j];
@@ -700,6 +712,7 @@ __global__ void k_edge_tri_star(u32 nadj, u32 const* __restrict__ adj,
 __global__ void k_sum_degrees(u32 n, u32 const* __restrict__ a, u32 const* __restrict__ b,
     u32* __restrict__ deg_out)
 {
+  pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) deg_out[i] = (a[i + 1] - a[i]) + (b[i + 1] - b[i]);
 }
@@ -709,6 +722,7 @@ __global__ void k_edge_tet_star(u32 n, u32 const* __restrict__ so,
     u32 const* __restrict__ roe_offs, u32 const* __restrict__ roe,
     u32 const* __restrict__ roe_dirs, u32 const* __restrict__ eor, u32* __restrict__ star)
 {
+  pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   u32 o = so[i];
@@ -725,6 +739,7 @@ __global__ void k_star_general(u32 n, u32 const* __restrict__ hl_offs,
     u32 const* __restrict__ star_offs, u32* __restrict__ deg_out,
     u32* __restrict__ star, u32* err)
 {
+  pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   u32 buf[STAR_BUF];
@@ -760,6 +775,7 @@ __global__ void k_star_general(u32 n, u32 const* __restrict__ hl_offs,
 __global__ void k_dual_from_sides(u32 ne, u32 spe, u32 const* __restrict__ soe,
     u32 const* __restrict__ es_offs, u32 const* __restrict__ es, u32* __restrict__ out)
 {
+  pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= ne) return;
   for (u32 j = 0; j < spe; ++j) {
@@ -778,6 +794,7 @@ __global__ void k_dual_from_verts(u32 dim, u32 ne, u32 const* __restrict__ voe,
     u32 const* __restrict__ ev_offs, u32 const* __restrict__ ev,
     u32* __restrict__ out, u32* err)
 {
+  pdl_wait();
   u32 spe = deg(dim, dim - 1), vpe = deg(dim, 0), vps = deg(dim - 1, 0);
   u32 idx = blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= ne * spe) return;
@@ -817,6 +834,7 @@ __global__ void k_dual_from_verts(u32 dim, u32 ne, u32 const* __restrict__ voe,
 __global__ void k_bridge_degree(u32 n, u32 const* __restrict__ offs, u32 stride,
     u32 const* __restrict__ adj, u32* __restrict__ degree)
 {
+  pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   u32 f = offs ? offs[i] : i * stride, e = offs ? offs[i + 1] : (i + 1) * stride;
@@ -829,6 +847,7 @@ __global__ void k_bridge_degree(u32 n, u32 const* __restrict__ offs, u32 stride,
 __global__ void k_bridge_edges(u32 n, u32 const* __restrict__ offs,
     u32 const* __restrict__ adj, u32 const* __restrict__ bo, u32* __restrict__ voe)
 {
+  pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   u32 e = bo[i];
@@ -844,6 +863,7 @@ __global__ void k_bridge_edges(u32 n, u32 const* __restrict__ offs,
 __global__ void k_derive_sides(u32 dim, u32 ne, u32 const* __restrict__ dual,
     u32 const* __restrict__ bo, u32 const* __restrict__ voe, u32* __restrict__ vos)
 {
+  pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= ne) return;
   u32 spe = deg(dim, dim - 1), vpe = deg(dim, 0), vps = deg(dim - 1, 0);
@@ -867,14 +887,14 @@ void Mesh::build_low_rows(u32 low)
   u32* cnt = dalloc<u32>((size_t)nv + 1, s);
   CK(cudaMemsetAsync(cnt, 0, sizeof(u32) * ((size_t)nv + 1), s));
   if (nl) {
-    k_count_min_vert<<<grid_for(nl), BLOCK, 0, s>>>(low, nl, vol, cnt);
+    CK(launch_kernel(k_count_min_vert, dim3(grid_for(nl)), dim3(BLOCK), 0, s, low, nl, vol, cnt));
     CK_LAUNCH();
   }
   low_row_offs[low] = exscan_new(cnt, nv, s);
   low_rows[low] = dalloc<u32>((size_t)nl * (low == 1 ? 2 : 4), s);
   if (nl) {
-    k_fill_min_vert<<<grid_for(nl), BLOCK, 0, s>>>(low, nl, vol, low_row_offs[low], cnt,
-        low_rows[low]);
+    CK(launch_kernel(k_fill_min_vert, dim3(grid_for(nl)), dim3(BLOCK), 0, s, low, nl, vol, low_row_offs[low], cnt,
+        low_rows[low]));
     CK_LAUNCH();
   }
   dev_free(cnt, s);
@@ -893,14 +913,14 @@ void Mesh::reflect_range(u32 high, u32 low, u32 first, u32* out)
       rec * nld + 4.0 * n);
   u32 g = grid_for(nh - first);
   if (high == 3 && low == 2)
-    k_reflect_grouped<3, 2><<<g, BLOCK, 0, s>>>(first, nh, voh, low_row_offs[low],
-        low_rows[low], out);
+    CK(launch_kernel(k_reflect_grouped<3, 2>, dim3(g), dim3(BLOCK), 0, s, first, nh, voh, low_row_offs[low],
+        low_rows[low], out));
   else if (high == 3)
-    k_reflect_grouped<3, 1><<<g, BLOCK, 0, s>>>(first, nh, voh, low_row_offs[low],
-        low_rows[low], out);
+    CK(launch_kernel(k_reflect_grouped<3, 1>, dim3(g), dim3(BLOCK), 0, s, first, nh, voh, low_row_offs[low],
+        low_rows[low], out));
   else
-    k_reflect_grouped<2, 1><<<g, BLOCK, 0, s>>>(first, nh, voh, low_row_offs[low],
-        low_rows[low], out);
+    CK(launch_kernel(k_reflect_grouped<2, 1>, dim3(g), dim3(BLOCK), 0, s, first, nh, voh, low_row_offs[low],
+        low_rows[low], out));
   CK_LAUNCH();
 }
 
@@ -916,6 +936,7 @@ template <u32 LPH>
 __global__ void __launch_bounds__(BLOCK) k_carry_down(u32 n, u32 const* __restrict__ same_h,
     u32 const* __restrict__ same_l, u32 const* __restrict__ old_down, u32* __restrict__ out)
 {
+  pdl_wait();
   u32 base = blockIdx.x * (BLOCK * CARRY_UNROLL) + threadIdx.x;
   u32 od[CARRY_UNROLL], ni[CARRY_UNROLL], nn[CARRY_UNROLL];
 #pragma unroll
@@ -951,11 +972,11 @@ void carry_down(Mesh& m, Mesh& out, u32 high, u32 low, u32 const* same_h, u32 ns
     u32 g = (u32)ceil_div((u64)n, (u64)BLOCK * CARRY_UNROLL);
     PROBE(P_CARRY, s, 4.0 * (nh_old + 1) + 12.0 * n);
     if (lph == 3)
-      k_carry_down<3><<<g, BLOCK, 0, s>>>(n, same_h, same_l, m.down[high][low], dn);
+      CK(launch_kernel(k_carry_down<3>, dim3(g), dim3(BLOCK), 0, s, n, same_h, same_l, m.down[high][low], dn));
     else if (lph == 4)
-      k_carry_down<4><<<g, BLOCK, 0, s>>>(n, same_h, same_l, m.down[high][low], dn);
+      CK(launch_kernel(k_carry_down<4>, dim3(g), dim3(BLOCK), 0, s, n, same_h, same_l, m.down[high][low], dn));
     else
-      k_carry_down<6><<<g, BLOCK, 0, s>>>(n, same_h, same_l, m.down[high][low], dn);
+      CK(launch_kernel(k_carry_down<6>, dim3(g), dim3(BLOCK), 0, s, n, same_h, same_l, m.down[high][low], dn));
     CK_LAUNCH();
   }
   // the survivors come first; the entities the pass made are searched
@@ -976,6 +997,7 @@ void carry_down(Mesh& m, Mesh& out, u32 high, u32 low, u32 const* same_h, u32 ns
 // the same speed as a thread per row.)
 __global__ void k_new_ids(u32 n, u32 const* __restrict__ same, u32* __restrict__ newid)
 {
+  pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   u32 a = same[i];
@@ -989,6 +1011,7 @@ __global__ void k_up_surv_count(u32 nl_old, u32 nsame_l, u32 ntail,
     u32 const* __restrict__ offs, u32 const* __restrict__ adj, u32* __restrict__ cnt,
     u32* __restrict__ surv)
 {
+  pdl_wait();
   u32 j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= nl_old) {
     if (j - nl_old < ntail) {
@@ -1015,6 +1038,7 @@ __global__ void k_up_surv_count(u32 nl_old, u32 nsame_l, u32 ntail,
 __global__ void k_up_gen_count(u32 first, u32 nuses, u32 const* __restrict__ loh,
     u32* __restrict__ cnt)
 {
+  pdl_wait();
   u32 u = first + blockIdx.x * blockDim.x + threadIdx.x;
   if (u < nuses) atomicAdd(&cnt[loh[u]], 1u);
 }
@@ -1024,6 +1048,7 @@ __global__ void k_up_surv_fill(u32 nl_old, u32 const* __restrict__ same_l,
     u32 const* __restrict__ adj_old, u32 const* __restrict__ dirs_old,
     u32 const* __restrict__ offs, u32* __restrict__ adj, u32* __restrict__ dirs)
 {
+  pdl_wait();
   u32 j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= nl_old) return;
   u32 nj = same_l[j];
@@ -1070,6 +1095,7 @@ __global__ void k_up_surv_count_grouped(u32 nl_old, u32 nsame_l, u32 ntail,
     u32 const* __restrict__ offs, u32 const* __restrict__ adj, u32* __restrict__ cnt,
     u32* __restrict__ surv)
 {
+  pdl_wait();
   u32 const t = blockIdx.x * blockDim.x + threadIdx.x;
   u32 const j = t / CARRY_GROUP, g = t % CARRY_GROUP;
   if (j >= nl_old) {
@@ -1102,6 +1128,7 @@ __global__ void k_up_surv_fill_grouped(u32 nl_old, u32 const* __restrict__ same_
     u32 const* __restrict__ adj_old, u32 const* __restrict__ dirs_old,
     u32 const* __restrict__ offs, u32* __restrict__ adj, u32* __restrict__ dirs)
 {
+  pdl_wait();
   u32 const t = blockIdx.x * blockDim.x + threadIdx.x;
   u32 const j = t / CARRY_GROUP, g = t % CARRY_GROUP;
   if (j >= nl_old) return;
@@ -1135,6 +1162,7 @@ __global__ void k_up_surv_fill_grouped(u32 nl_old, u32 const* __restrict__ same_
 __global__ void k_up_gen_fill(u32 first, u32 nuses, u32 lph, u32 const* __restrict__ loh,
     u32 const* __restrict__ offs, u32* cnt, u32* __restrict__ adj, u32* __restrict__ dirs)
 {
+  pdl_wait();
   u32 u = first + blockIdx.x * blockDim.x + threadIdx.x;
   if (u >= nuses) return;
   u32 l = loh[u];
@@ -1147,7 +1175,7 @@ u32* carry_new_ids(u32 const* same, u32 n, cudaStream_t s)
 {
   u32* newid = dalloc<u32>(n ? n : 1, s);
   if (n) {
-    k_new_ids<<<grid_for(n), BLOCK, 0, s>>>(n, same, newid);
+    CK(launch_kernel(k_new_ids, dim3(grid_for(n)), dim3(BLOCK), 0, s, n, same, newid));
     CK_LAUNCH();
   }
   return newid;
@@ -1189,18 +1217,20 @@ void carry_up(Mesh& m, Mesh& out, u32 low, u32 high, u32 const* same_l, u32 nsam
   bool const long_rows = nl_old && (u64)nuses_old >= (u64)CARRY_GROUP * nl_old;
   {
     u32 ntail = nl + 1 - nsame_l;
-    PROBE(P_CARRY_UP, s, 8.0 * (nl_old + 1) + 4.0 * nuses_old + 8.0 * nuses_old + 8.0 * nl);
+    // each array once: same_l and the old offsets, the old rows' highs, the
+    // highs' new ids, the new counts
+    PROBE(P_CARRY_UP, s, 8.0 * (nl_old + 1) + 4.0 * nuses_old + 4.0 * nh_old + 4.0 * nl);
     if (long_rows)
-      k_up_surv_count_grouped<<<grid_for(((u64)nl_old + ntail) * CARRY_GROUP), BLOCK, 0, s>>>(
-          nl_old, nsame_l, ntail, same_l, newid_h, old.offs, old.adj, cnt, surv);
+      CK(launch_kernel(k_up_surv_count_grouped, dim3(grid_for(((u64)nl_old + ntail) * CARRY_GROUP)), dim3(BLOCK), 0, s, 
+          nl_old, nsame_l, ntail, same_l, newid_h, old.offs, old.adj, cnt, surv));
     else
-      k_up_surv_count<<<grid_for((u64)nl_old + ntail), BLOCK, 0, s>>>(nl_old, nsame_l, ntail,
-          same_l, newid_h, old.offs, old.adj, cnt, surv);
+      CK(launch_kernel(k_up_surv_count, dim3(grid_for((u64)nl_old + ntail)), dim3(BLOCK), 0, s, nl_old, nsame_l, ntail,
+          same_l, newid_h, old.offs, old.adj, cnt, surv));
     CK_LAUNCH();
   }
   if (nuses > first) {
     PROBE(P_UP_COUNT, s, 4.0 * (nuses - first) + 4.0 * nl);
-    k_up_gen_count<<<grid_for(nuses - first), BLOCK, 0, s>>>(first, nuses, loh, cnt);
+    CK(launch_kernel(k_up_gen_count, dim3(grid_for(nuses - first)), dim3(BLOCK), 0, s, first, nuses, loh, cnt));
     CK_LAUNCH();
   }
   UpAdj u;
@@ -1208,19 +1238,23 @@ void carry_up(Mesh& m, Mesh& out, u32 low, u32 high, u32 const* same_l, u32 nsam
   u.adj = dalloc<u32>(nuses, s);
   u.dirs = dalloc<u32>(nuses, s);
   if (nl_old) {
-    PROBE(P_CARRY_UP, s, 8.0 * (nl_old + 1) + 12.0 * nuses_old + 8.0 * nuses_old + 4.0 * nl);
+    // each array once: same_l and the old offsets, the old rows' highs and
+    // directions, the highs' new ids, the new offsets, the kept uses (first)
+    // written as highs and directions
+    PROBE(P_CARRY_UP, s, 8.0 * (nl_old + 1) + 8.0 * nuses_old + 4.0 * nh_old + 4.0 * (nl + 1) +
+        8.0 * first);
     if (long_rows)
-      k_up_surv_fill_grouped<<<grid_for((u64)nl_old * CARRY_GROUP), BLOCK, 0, s>>>(nl_old,
-          same_l, newid_h, old.offs, old.adj, old.dirs, u.offs, u.adj, u.dirs);
+      CK(launch_kernel(k_up_surv_fill_grouped, dim3(grid_for((u64)nl_old * CARRY_GROUP)), dim3(BLOCK), 0, s, nl_old,
+          same_l, newid_h, old.offs, old.adj, old.dirs, u.offs, u.adj, u.dirs));
     else
-      k_up_surv_fill<<<grid_for(nl_old), BLOCK, 0, s>>>(nl_old, same_l, newid_h, old.offs,
-          old.adj, old.dirs, u.offs, u.adj, u.dirs);
+      CK(launch_kernel(k_up_surv_fill, dim3(grid_for(nl_old)), dim3(BLOCK), 0, s, nl_old, same_l, newid_h, old.offs,
+          old.adj, old.dirs, u.offs, u.adj, u.dirs));
     CK_LAUNCH();
   }
   if (nuses > first) {
     PROBE(P_UP_FILL, s, 4.0 * (nuses - first) + 8.0 * nl + 8.0 * (nuses - first));
-    k_up_gen_fill<<<grid_for(nuses - first), BLOCK, 0, s>>>(first, nuses, lph, loh, u.offs,
-        cnt, u.adj, u.dirs);
+    CK(launch_kernel(k_up_gen_fill, dim3(grid_for(nuses - first)), dim3(BLOCK), 0, s, first, nuses, lph, loh, u.offs,
+        cnt, u.adj, u.dirs));
     CK_LAUNCH();
   }
   dev_free(cnt, s);
@@ -1253,7 +1287,7 @@ u32 const* Mesh::ask_down(u32 high, u32 low)
     u32 nv = counts[0];
     u32* degree = dalloc<u32>(nv, s);
     if (nv) {
-      k_bridge_degree<<<grid_for(nv), BLOCK, 0, s>>>(nv, vv.offs, 0, vv.adj, degree);
+      CK(launch_kernel(k_bridge_degree, dim3(grid_for(nv)), dim3(BLOCK), 0, s, nv, vv.offs, 0, vv.adj, degree));
       CK_LAUNCH();
     }
     u32* bo = exscan_new(degree, nv, s);
@@ -1261,7 +1295,7 @@ u32 const* Mesh::ask_down(u32 high, u32 low)
     u32 ne = read_u32(bo + nv, s);
     u32* voe = dalloc<u32>((size_t)ne * 2, s);
     if (nv) {
-      k_bridge_edges<<<grid_for(nv), BLOCK, 0, s>>>(nv, vv.offs, vv.adj, bo, voe);
+      CK(launch_kernel(k_bridge_edges, dim3(grid_for(nv)), dim3(BLOCK), 0, s, nv, vv.offs, vv.adj, bo, voe));
       CK_LAUNCH();
     }
     dev_free(bo, s);
@@ -1273,7 +1307,7 @@ u32 const* Mesh::ask_down(u32 high, u32 low)
     u32 spe = deg(dim, dim - 1);
     u32* degree = dalloc<u32>(nel, s);
     if (nel) {
-      k_bridge_degree<<<grid_for(nel), BLOCK, 0, s>>>(nel, nullptr, spe, du, degree);
+      CK(launch_kernel(k_bridge_degree, dim3(grid_for(nel)), dim3(BLOCK), 0, s, nel, nullptr, spe, du, degree));
       CK_LAUNCH();
     }
     u32* bo = exscan_new(degree, nel, s);
@@ -1282,7 +1316,7 @@ u32 const* Mesh::ask_down(u32 high, u32 low)
     u32 vps = deg(dim - 1, 0);
     u32* vos = dalloc<u32>((size_t)ns * vps, s);
     if (nel) {
-      k_derive_sides<<<grid_for(nel), BLOCK, 0, s>>>(dim, nel, du, bo, down[dim][0], vos);
+      CK(launch_kernel(k_derive_sides, dim3(grid_for(nel)), dim3(BLOCK), 0, s, dim, nel, du, bo, down[dim][0], vos));
       CK_LAUNCH();
     }
     dev_free(bo, s);
@@ -1355,7 +1389,7 @@ Graph const& Mesh::ask_star(u32 low, u32 high)
     CK(cudaMemcpyAsync(g.offs, ev.offs, sizeof(u32) * (n + 1), cudaMemcpyDeviceToDevice, s));
     g.adj = dalloc<u32>(g.nadj, s);
     if (g.nadj) {
-      k_vertex_edge_star<<<grid_for(g.nadj), BLOCK, 0, s>>>(g.nadj, ev.adj, ev.dirs, voe, g.adj);
+      CK(launch_kernel(k_vertex_edge_star, dim3(grid_for(g.nadj)), dim3(BLOCK), 0, s, g.nadj, ev.adj, ev.dirs, voe, g.adj));
       CK_LAUNCH();
     }
   } else if (low == 1 && high == 2) {
@@ -1366,11 +1400,11 @@ Graph const& Mesh::ask_star(u32 low, u32 high)
     u32 nuse = counts[2] * 3;
     g.nadj = nuse * 2;
     g.offs = dalloc<u32>((size_t)n + 1, s);
-    k_scale_offsets<<<grid_for(n + 1), BLOCK, 0, s>>>(te.offs, n + 1, 2, g.offs);
+    CK(launch_kernel(k_scale_offsets, dim3(grid_for(n + 1)), dim3(BLOCK), 0, s, te.offs, n + 1, 2, g.offs));
     CK_LAUNCH();
     g.adj = dalloc<u32>(g.nadj, s);
     if (nuse) {
-      k_edge_tri_star<<<grid_for(nuse), BLOCK, 0, s>>>(nuse, te.adj, te.dirs, eot, g.adj);
+      CK(launch_kernel(k_edge_tri_star, dim3(grid_for(nuse)), dim3(BLOCK), 0, s, nuse, te.adj, te.dirs, eot, g.adj));
       CK_LAUNCH();
     }
   } else if (low == 1 && high == 3 && has_dim(2)) {
@@ -1381,7 +1415,7 @@ Graph const& Mesh::ask_star(u32 low, u32 high)
     UpAdj const& re = ask_up(1, 3);
     u32* degree = dalloc<u32>(n, s);
     if (n) {
-      k_sum_degrees<<<grid_for(n), BLOCK, 0, s>>>(n, ts.offs, re.offs, degree);
+      CK(launch_kernel(k_sum_degrees, dim3(grid_for(n)), dim3(BLOCK), 0, s, n, ts.offs, re.offs, degree));
       CK_LAUNCH();
     }
     g.offs = exscan_new(degree, n, s);
@@ -1389,8 +1423,8 @@ Graph const& Mesh::ask_star(u32 low, u32 high)
     g.nadj = ts.nadj + counts[3] * 6;
     g.adj = dalloc<u32>(g.nadj, s);
     if (n) {
-      k_edge_tet_star<<<grid_for(n), BLOCK, 0, s>>>(n, g.offs, ts.offs, ts.adj, re.offs,
-          re.adj, re.dirs, eor, g.adj);
+      CK(launch_kernel(k_edge_tet_star, dim3(grid_for(n)), dim3(BLOCK), 0, s, n, g.offs, ts.offs, ts.adj, re.offs,
+          re.adj, re.dirs, eor, g.adj));
       CK_LAUNCH();
     }
   } else {
@@ -1403,8 +1437,8 @@ Graph const& Mesh::ask_star(u32 low, u32 high)
     u32* err = mb->dev + 60;
     CK(cudaMemsetAsync(err, 0, sizeof(u32), s));
     if (n) {
-      k_star_general<<<grid_for(n), BLOCK, 0, s>>>(n, hl.offs, hl.adj, loh, lph,
-          nullptr, degree, nullptr, err);
+      CK(launch_kernel(k_star_general, dim3(grid_for(n)), dim3(BLOCK), 0, s, n, hl.offs, hl.adj, loh, lph,
+          nullptr, degree, nullptr, err));
       CK_LAUNCH();
     }
     g.offs = exscan_new(degree, n, s);
@@ -1412,8 +1446,8 @@ Graph const& Mesh::ask_star(u32 low, u32 high)
     g.nadj = read_u32(g.offs + n, s);
     g.adj = dalloc<u32>(g.nadj, s);
     if (n) {
-      k_star_general<<<grid_for(n), BLOCK, 0, s>>>(n, hl.offs, hl.adj, loh, lph, g.offs,
-          nullptr, g.adj, err);
+      CK(launch_kernel(k_star_general, dim3(grid_for(n)), dim3(BLOCK), 0, s, n, hl.offs, hl.adj, loh, lph, g.offs,
+          nullptr, g.adj, err));
       CK_LAUNCH();
     }
     if (read_u32(err, s)) throw Failure(E_ARG, "star wider than 256 entries");
@@ -1432,7 +1466,7 @@ u32 const* Mesh::ask_dual()
     u32 const* soe = ask_down(dim, dim - 1);
     UpAdj const& es = ask_up(dim - 1, dim, false);
     if (nel) {
-      k_dual_from_sides<<<grid_for(nel), BLOCK, 0, s>>>(nel, spe, soe, es.offs, es.adj, out);
+      CK(launch_kernel(k_dual_from_sides, dim3(grid_for(nel)), dim3(BLOCK), 0, s, nel, spe, soe, es.offs, es.adj, out));
       CK_LAUNCH();
     }
   } else {
@@ -1441,8 +1475,8 @@ u32 const* Mesh::ask_dual()
     u32* err = mb->dev + 61;
     CK(cudaMemsetAsync(err, 0, sizeof(u32), s));
     if (nel) {
-      k_dual_from_verts<<<grid_for((u64)nel * spe), BLOCK, 0, s>>>(dim, nel, voe, ev.offs,
-          ev.adj, out, err);
+      CK(launch_kernel(k_dual_from_verts, dim3(grid_for((u64)nel * spe)), dim3(BLOCK), 0, s, dim, nel, voe, ev.offs,
+          ev.adj, out, err));
       CK_LAUNCH();
     }
     if (read_u32(err, s)) throw Failure(E_ARG, "vertex with more than 256 elements");
@@ -1459,6 +1493,7 @@ __global__ void k_elem_quality(u32 dim, u32 ne, u32 const* __restrict__ voe,
     double const* __restrict__ x, double* __restrict__ q,
     unsigned long long* minkey)
 {
+  pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   double qi = DBL_MAX;
   if (i < ne) {
@@ -1488,8 +1523,8 @@ double const* Mesh::qualities()
   CK(cudaMemsetAsync(mk, 0xff, sizeof(unsigned long long), s));
   if (ne) {
     PROBE(P_ELEM_QUALITY, s, 4.0 * deg(dim, 0) * ne + 24.0 * counts[0] + 8.0 * ne);
-    k_elem_quality<<<grid_for(ne), BLOCK, 0, s>>>(dim, ne, ask_down(dim, 0), coords(),
-        qual_cache, mk);
+    CK(launch_kernel(k_elem_quality, dim3(grid_for(ne)), dim3(BLOCK), 0, s, dim, ne, ask_down(dim, 0), coords(),
+        qual_cache, mk));
     CK_LAUNCH();
   }
   return qual_cache;
@@ -1511,6 +1546,7 @@ double Mesh::min_quality()
 __global__ void k_elem_size(u32 dim, u32 ne, u32 const* __restrict__ voe,
     double const* __restrict__ x, double* __restrict__ out)
 {
+  pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= ne) return;
   u32 vpe = deg(dim, 0);
@@ -1531,7 +1567,7 @@ double* Mesh::element_sizes()
   u32 ne = count(dim);
   double* out = dalloc<double>(ne, s);
   if (ne) {
-    k_elem_size<<<grid_for(ne), BLOCK, 0, s>>>(dim, ne, ask_down(dim, 0), coords(), out);
+    CK(launch_kernel(k_elem_size, dim3(grid_for(ne)), dim3(BLOCK), 0, s, dim, ne, ask_down(dim, 0), coords(), out));
     CK_LAUNCH();
   }
   return out;
@@ -1540,6 +1576,7 @@ double* Mesh::element_sizes()
 __global__ void k_measure_edges(u32 ne, u32 const* __restrict__ voe,
     double const* __restrict__ x, double const* __restrict__ h, double* __restrict__ out)
 {
+  pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= ne) return;
   u32 a = voe[i * 2], b = voe[i * 2 + 1];
@@ -1558,8 +1595,8 @@ double* Mesh::measure_edges()
   if (!t) throw Failure(E_ARG, "mesh has no adapt_size vertex field");
   double* out = dalloc<double>(ne, s);
   if (ne) {
-    k_measure_edges<<<grid_for(ne), BLOCK, 0, s>>>(ne, ask_down(1, 0), coords(),
-        static_cast<double const*>(t->data), out);
+    CK(launch_kernel(k_measure_edges, dim3(grid_for(ne)), dim3(BLOCK), 0, s, ne, ask_down(1, 0), coords(),
+        static_cast<double const*>(t->data), out));
     CK_LAUNCH();
   }
   return out;

@@ -78,6 +78,7 @@ u32* scratch_address()
 __global__ void k_na_count(u32 const* __restrict__ loh, u32 nuses, u32 nlows,
     u32* __restrict__ cnt, u32* status)
 {
+  pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nuses) return;
   u32 l = loh[i];
@@ -94,6 +95,7 @@ __global__ void k_na_fill(u32 const* __restrict__ loh, u32 nuses, u32 nlows,
     u32 const* __restrict__ offs, u32* __restrict__ cnt, u32* __restrict__ rows,
     u32* status, u32 const* scan_err)
 {
+  pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nuses) return;
   if (*(volatile u32*)status || *(volatile u32 const*)scan_err) {
@@ -115,6 +117,7 @@ __global__ void k_na_rank(u32 const* __restrict__ offs, u32 const* __restrict__ 
     u32 nrows, u32 nuses, u32 lph, u32* __restrict__ adj, u32* __restrict__ dirs,
     u32 const* status)
 {
+  pdl_wait();
   u32 row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   u32 lane = threadIdx.x & 31;
   if (row >= nrows || *(volatile u32 const*)status) return;
@@ -143,6 +146,7 @@ __global__ void k_na_rank(u32 const* __restrict__ offs, u32 const* __restrict__ 
 // a failed call says so in offsets[nlows], whose value is nuses otherwise
 __global__ void k_na_finish(u32 nlows, u32* offs, u32 const* status, u32 const* scan_err)
 {
+  pdl_wait();
   if (*(volatile u32 const*)status || *(volatile u32 const*)scan_err) offs[nlows] = INV;
 }
 
@@ -180,7 +184,7 @@ extern "C" int osh_b200_up_from_down_noalloc(unsigned high_dim, unsigned low_dim
     CK(cudaMemsetAsync(scratch, 0, sizeof(u32) * (NA_COUNTS + (size_t)nlows + 1), s));
     u32 const n = (u32)nuses;
     if (n) {
-      k_na_count<<<grid_for(n), BLOCK, 0, s>>>(lows_of_highs, n, nlows, cnt, status);
+      CK(launch_kernel(k_na_count, dim3(grid_for(n)), dim3(BLOCK), 0, s, lows_of_highs, n, nlows, cnt, status));
       CK_LAUNCH();
     }
     // clears its own scratch (word 1 of which records a wait that gave up);
@@ -188,15 +192,15 @@ extern "C" int osh_b200_up_from_down_noalloc(unsigned high_dim, unsigned low_dim
     if (!nlows) CK(cudaMemsetAsync(scan, 0, 4 * sizeof(u32), s));
     exscan_u32_scratch(cnt, offsets, nlows, scan, s);
     if (n) {
-      k_na_fill<<<grid_for(n), BLOCK, 0, s>>>(lows_of_highs, n, nlows, offsets, cnt, rows,
-          status, scan + 1);
+      CK(launch_kernel(k_na_fill, dim3(grid_for(n)), dim3(BLOCK), 0, s, lows_of_highs, n, nlows, offsets, cnt, rows,
+          status, scan + 1));
       CK_LAUNCH();
       u64 threads = (u64)nlows * 32;
-      k_na_rank<<<grid_for(threads), BLOCK, 0, s>>>(offsets, rows, nlows, n, lph,
-          highs_of_lows, directions, status);
+      CK(launch_kernel(k_na_rank, dim3(grid_for(threads)), dim3(BLOCK), 0, s, offsets, rows, nlows, n, lph,
+          highs_of_lows, directions, status));
       CK_LAUNCH();
     }
-    k_na_finish<<<1, 1, 0, s>>>(nlows, offsets, status, scan + 1);
+    CK(launch_kernel(k_na_finish, dim3(1), dim3(1), 0, s, nlows, offsets, status, scan + 1));
     CK_LAUNCH();
     return 0;
   } catch (Failure const& f) {

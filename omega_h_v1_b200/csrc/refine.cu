@@ -16,8 +16,10 @@ __global__ void k_refine_candidates(u32 ne, u32 const* __restrict__ voe,
     double const* __restrict__ x, double const* __restrict__ h, SegView sv,
     Fp32Stats* fs, u32* __restrict__ cand, u32* any)
 {
+  pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   u32 c = 0;
+  bool decided = false, rechecked = false, flipped = false;
   if (i < ne) {
     u32 a = voe[i * 2], b = voe[i * 2 + 1];
     double xa[3], xb[3];
@@ -25,30 +27,54 @@ __global__ void k_refine_candidates(u32 ne, u32 const* __restrict__ voe,
     load3(x, b, xb);
     int r32 = fs ? edge_ratio_side_f32(xa, xb, h[a], h[b], 1.0) : 0;
     if (r32) {
-      atomicAdd(&fs->decided, 1ull);
+      decided = true;
       c = r32 > 0;
-    } else {
-      if (fs) atomicAdd(&fs->rechecked, 1ull);
+    }
+    if (!r32 || fs->audit) {
+      rechecked = !r32;
       double len = sqrt(sqdist3(xb, xa));
       double want = (h[a] + h[b]) / 2;
-      c = (len / want) > 1.0;
+      u32 c64 = (len / want) > 1.0;
+      flipped = r32 && c64 != c;
+      c = c64;
     }
     c = c && seg_acts(sv, a);
     cand[i] = c;
   }
+  if (fs) fp32_count_warp(fs, decided, rechecked, decided && fs->audit, flipped);
   if (__any_sync(0xffffffffu, c) && (threadIdx.x & 31) == 0) atomicOr(any, 1u);
 }
 
+// the two children of element e (split at its edge of direction dir)
+// around the midpoint `split`, in the reference's order
+__device__ inline void refine_child(u32 dim, u32 const* __restrict__ ve, u32 dir, u32 k,
+    double const* __restrict__ x, double const* split, double (*ex)[3])
+{
+  u32 vpe = deg(dim, 0);
+  u32 o = canon(dim, 1, 0, dir, k);
+  u32 base = opp(dim, 0, o);
+  for (u32 l = 0; l + 1 < vpe; ++l) load3(x, ve[canon(dim, dim - 1, 0, base, l)], ex[l]);
+  ex[vpe - 1][0] = split[0];
+  ex[vpe - 1][1] = split[1];
+  ex[vpe - 1][2] = split[2];
+}
+
 // refine_quality (refine_qualities.cpp:16-82) for edges, require_better = 0:
-// the worst child of every element around the edge, split at its midpoint
+// the worst child of every element around the edge, split at its midpoint.
+// With the filter: the children's estimates first; the edge is rejected on
+// them when every child is surely upright and the worst surely below the
+// floor; otherwise only the children whose lower bound reaches the lowest
+// upper bound seen (they alone can hold the minimum) are computed in double.
 __global__ void k_refine_quality(u32 dim, u32 ne, u32 const* __restrict__ voe1,
     u32 const* __restrict__ voe, u32 const* __restrict__ eo_offs,
     u32 const* __restrict__ eo, u32 const* __restrict__ eo_dirs,
     double const* __restrict__ x, double qual_floor, SegView sv, Fp32Stats* fs,
     u32* __restrict__ cand, double* __restrict__ out, u32* any, u32* inverted)
 {
+  pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   u32 keep = 0;
+  bool decided = false, rechecked = false, audited = false, flipped = false;
   if (i < ne && cand[i]) {
     u32 vpe = deg(dim, 0);
     double const perfect = dim == 3 ? perfect_tet_quality() : perfect_tri_quality();
@@ -62,93 +88,88 @@ __global__ void k_refine_quality(u32 dim, u32 ne, u32 const* __restrict__ voe1,
       split[c] = acc / 2u;
     }
     double const fl = seg_floor(sv, a, qual_floor);
-    bool filtered = false;
+    u32 const f = eo_offs[i], e = eo_offs[i + 1];
+    // filtered: 0 = no decision on estimates, 1 = rejected on them,
+    // 2 = minimum over the children that can hold it
+    int filtered = 0;
+    double minq = 1;
     if (fs && dim == 3) {
-      // reject on the estimate only when every child is surely upright and
-      // the worst child is surely below the floor
+      float const k6 = tet_k6_f32();
       float upper = 1.0f;
       bool upright = true;
-      for (u32 j = eo_offs[i]; j < eo_offs[i + 1]; ++j) {
-        u32 dir = eo_dirs[j], e = eo[j];
-        u32 const* ve = voe + (size_t)e * vpe;
+      unsigned long long need = 0;  // children (2 per element) that can hold the minimum
+      bool all = 2 * (e - f) > 64;
+      for (u32 j = f; j < e; ++j) {
+        u32 const* ve = voe + (size_t)eo[j] * vpe;
         for (u32 k = 0; k < 2; ++k) {
-          u32 o = canon(dim, 1, 0, dir, k);
-          u32 base = opp(dim, 0, o);
           double ex[4][3];
-          for (u32 l = 0; l + 1 < vpe; ++l) load3(x, ve[canon(dim, dim - 1, 0, base, l)], ex[l]);
-          ex[3][0] = split[0];
-          ex[3][1] = split[1];
-          ex[3][2] = split[2];
-          Q32 q = tet_quality_f32(ex, (float)perfect);
-          upright = upright && (q.q - q.err > 0.0f);
-          upper = fminf(upper, q.q + q.err);
+          refine_child(dim, ve, eo_dirs[j], k, x, split, ex);
+          Q32 q = tet_quality_f32(ex, k6);
+          float lo = q32_lo(q);
+          upright = upright && lo > 0.0f;
+          upper = fminf(upper, q32_hi(q));
+          if (lo <= upper && !all) need |= 1ull << (2 * (j - f) + k);
         }
       }
       if (upright && (double)upper < fl) {
-        filtered = true;
-        atomicAdd(&fs->decided, 1ull);
-        cand[i] = 0;
+        filtered = 1;
+        decided = true;
       } else if (upright) {
-        // the worst child has estimate - bound <= upper: only such children
-        // are computed in double, in order, and their minimum is exact
-        atomicAdd(&fs->rechecked, 1ull);
-        filtered = true;
-        double minq = 1;
-        for (u32 j = eo_offs[i]; j < eo_offs[i + 1]; ++j) {
-          u32 dir = eo_dirs[j], e = eo[j];
-          u32 const* ve = voe + (size_t)e * vpe;
+        filtered = 2;
+        rechecked = true;
+        for (u32 j = f; j < e; ++j) {
+          u32 const* ve = voe + (size_t)eo[j] * vpe;
           for (u32 k = 0; k < 2; ++k) {
-            u32 o = canon(dim, 1, 0, dir, k);
-            u32 base = opp(dim, 0, o);
+            if (!all && !((need >> (2 * (j - f) + k)) & 1ull)) continue;
             double ex[4][3];
-            for (u32 l = 0; l + 1 < vpe; ++l) load3(x, ve[canon(dim, dim - 1, 0, base, l)], ex[l]);
-            ex[3][0] = split[0];
-            ex[3][1] = split[1];
-            ex[3][2] = split[2];
-            Q32 q32 = tet_quality_f32(ex, (float)perfect);
-            if ((double)q32.q - (double)q32.err > (double)upper) continue;
+            refine_child(dim, ve, eo_dirs[j], k, x, split, ex);
             double q = tet_quality(ex, perfect);
-            fp32_note_error(fs, q32, q);
+            if (fs->audit) fp32_note_error(fs, tet_quality_f32(ex, k6), q);
             if (q < minq) minq = q;
           }
         }
-        if (minq < fl) {
-          cand[i] = 0;
-        } else {
-          out[i] = minq;
-          keep = 1;
+      }
+      if (filtered && fs->audit) {
+        // the double path's result, every child in order, and every
+        // estimate against its double value
+        audited = true;
+        double m64 = 1;
+        for (u32 j = f; j < e; ++j) {
+          u32 const* ve = voe + (size_t)eo[j] * vpe;
+          for (u32 k = 0; k < 2; ++k) {
+            double ex[4][3];
+            refine_child(dim, ve, eo_dirs[j], k, x, split, ex);
+            double q = tet_quality(ex, perfect);
+            fp32_note_error(fs, tet_quality_f32(ex, k6), q);
+            if (q < m64) m64 = q;
+          }
         }
-      } else {
-        atomicAdd(&fs->rechecked, 1ull);
+        bool keep64 = !(m64 < fl);
+        flipped = filtered == 1 ? keep64
+                                : (keep64 != !(minq < fl) || (keep64 && m64 != minq));
       }
     }
-    double minq = 1;
     if (!filtered) {
-    for (u32 j = eo_offs[i]; j < eo_offs[i + 1]; ++j) {
-      u32 dir = eo_dirs[j], e = eo[j];
-      u32 const* ve = voe + (size_t)e * vpe;
-      for (u32 k = 0; k < 2; ++k) {
-        u32 o = canon(dim, 1, 0, dir, k);
-        u32 base = opp(dim, 0, o);
-        double ex[4][3];
-        for (u32 l = 0; l + 1 < vpe; ++l) load3(x, ve[canon(dim, dim - 1, 0, base, l)], ex[l]);
-        ex[vpe - 1][0] = split[0];
-        ex[vpe - 1][1] = split[1];
-        ex[vpe - 1][2] = split[2];
-        double q = dim == 3 ? tet_quality(ex, perfect) : tri_quality(ex, 0, perfect);
-        if (!(q > 0)) atomicOr(inverted, 1u);
-        if (q < minq) minq = q;
+      for (u32 j = f; j < e; ++j) {
+        u32 const* ve = voe + (size_t)eo[j] * vpe;
+        for (u32 k = 0; k < 2; ++k) {
+          double ex[4][3];
+          refine_child(dim, ve, eo_dirs[j], k, x, split, ex);
+          double q = dim == 3 ? tet_quality(ex, perfect) : tri_quality(ex, 0, perfect);
+          if (!(q > 0)) atomicOr(inverted, 1u);
+          if (q < minq) minq = q;
+        }
       }
     }
-    if (minq < fl) {
+    if (filtered == 1 || minq < fl) {
       cand[i] = 0;
     } else {
       out[i] = minq;
       keep = 1;
     }
-    }
   }
   if (i < ne && !keep) out[i] = 0.0;  // every edge's goodness is written here
+  if (fs && dim == 3) fp32_count_warp(fs, decided, rechecked, audited, flipped);
   if (__any_sync(0xffffffffu, keep) && (threadIdx.x & 31) == 0) atomicOr(any, 1u);
 }
 
@@ -157,6 +178,7 @@ __global__ void k_refine_nodal(u32 ne, u32 nv, u32 const* __restrict__ voe,
     u32 const* __restrict__ gen_offs, u32 nc, double const* __restrict__ f,
     double* __restrict__ out)
 {
+  pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= ne || gen_offs[i] == gen_offs[i + 1]) return;
   u32 a = voe[i * 2], b = voe[i * 2 + 1];
@@ -173,6 +195,7 @@ __global__ void k_refine_nodal(u32 ne, u32 nv, u32 const* __restrict__ voe,
 __global__ void k_refine_seg(u32 ne, u32 nv, u32 const* __restrict__ voe,
     u32 const* __restrict__ gen_offs, u32 const* __restrict__ seg, u32* __restrict__ out)
 {
+  pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= ne || gen_offs[i] == gen_offs[i + 1]) return;
   out[nv + gen_offs[i]] = seg[voe[i * 2]];
@@ -184,6 +207,7 @@ __global__ void k_split_to_domain(u32 nd, u32 spd, u32 const* __restrict__ sod,
     u32 const* __restrict__ gen_offs, u32 nv, u32* __restrict__ will,
     u32* __restrict__ dir, u32* __restrict__ vert)
 {
+  pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nd) return;
   u32 w = 0, d = INV, v = INV;
@@ -205,6 +229,7 @@ __global__ void k_refine_topology(u32 dd, u32 prod, u32 nd, u32 const* __restric
     u32 const* __restrict__ offs, u32 const* __restrict__ dir,
     u32 const* __restrict__ vert, u32* __restrict__ out)
 {
+  pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nd || offs[i] == offs[i + 1]) return;
   u32 base_dim = prod - 1, opp_dim = dd - 1 - base_dim;
@@ -226,6 +251,7 @@ __global__ void k_refine_topology(u32 dd, u32 prod, u32 nd, u32 const* __restric
 __global__ void k_refine_elem_field(u32 n, u32 const* __restrict__ offs, u32 k,
     u32 nc, int conserve, double const* __restrict__ in, double* __restrict__ out)
 {
+  pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   u32 f = offs[i] * k, e = offs[i + 1] * k;
@@ -272,8 +298,8 @@ static u32 refine_build(Mesh& m, u32 const* gen_offs)
     sp[dd].dir = dalloc<u32>(nd, s);
     sp[dd].vert = dalloc<u32>(nd, s);
     if (nd) {
-      k_split_to_domain<<<grid_for(nd), BLOCK, 0, s>>>(nd, deg(dd, 1), sod, gen_offs, nv,
-          will, sp[dd].dir, sp[dd].vert);
+      CK(launch_kernel(k_split_to_domain, dim3(grid_for(nd)), dim3(BLOCK), 0, s, nd, deg(dd, 1), sod, gen_offs, nv,
+          will, sp[dd].dir, sp[dd].vert));
       CK_LAUNCH();
     }
     sp[dd].offs = exscan_new(will, nd, s, m.mb->dev + 8 + dd);
@@ -292,8 +318,8 @@ static u32 refine_build(Mesh& m, u32 const* gen_offs)
     double* d = dalloc<double>((size_t)nv_out * t.ncomps, s);
     CK(cudaMemcpyAsync(d, t.data, sizeof(double) * nv * t.ncomps, cudaMemcpyDeviceToDevice, s));
     if (ns) {
-      k_refine_nodal<<<grid_for(ns), BLOCK, 0, s>>>(ns, nv, voe1, gen_offs, t.ncomps,
-          static_cast<double const*>(t.data), d);
+      CK(launch_kernel(k_refine_nodal, dim3(grid_for(ns)), dim3(BLOCK), 0, s, ns, nv, voe1, gen_offs, t.ncomps,
+          static_cast<double const*>(t.data), d));
       CK_LAUNCH();
     }
     out->add_tag(0, T_F64, t.name.c_str(), t.ncomps, X_NOT, d);
@@ -303,7 +329,7 @@ static u32 refine_build(Mesh& m, u32 const* gen_offs)
     out->seg = dalloc<u32>(nv_out, s);
     CK(cudaMemcpyAsync(out->seg, m.seg, sizeof(u32) * nv, cudaMemcpyDeviceToDevice, s));
     if (ns) {
-      k_refine_seg<<<grid_for(ns), BLOCK, 0, s>>>(ns, nv, voe1, gen_offs, m.seg, out->seg);
+      CK(launch_kernel(k_refine_seg, dim3(grid_for(ns)), dim3(BLOCK), 0, s, ns, nv, voe1, gen_offs, m.seg, out->seg));
       CK_LAUNCH();
     }
   }
@@ -346,8 +372,8 @@ static u32 refine_build(Mesh& m, u32 const* gen_offs)
         u32 nd = d.ndoms[dd];
         PROBE(P_REFINE_TOPOLOGY, s, 4.0 * deg(dd, 0) * nd + 12.0 * nd + 4.0 * (nd + 1) +
             4.0 * vpp * (double)d.ngen[dd]);
-        k_refine_topology<<<grid_for(nd), BLOCK, 0, s>>>(dd, prod, nd, m.ask_down(dd, 0),
-            sp[dd].offs, sp[dd].dir, sp[dd].vert, conn + (size_t)d.ngo[dd] * vpp);
+        CK(launch_kernel(k_refine_topology, dim3(grid_for(nd)), dim3(BLOCK), 0, s, dd, prod, nd, m.ask_down(dd, 0),
+            sp[dd].offs, sp[dd].dir, sp[dd].vert, conn + (size_t)d.ngo[dd] * vpp));
         CK_LAUNCH();
       }
       out->set_ents(prod, nout, conn);
@@ -363,9 +389,9 @@ static u32 refine_build(Mesh& m, u32 const* gen_offs)
           double* data = dalloc<double>((size_t)d.ngo[4] * nc, s);
           expand_scaled(t.data, same, 1, np, nc, 8, data, s);
           if (d.ngen[dim]) {
-            k_refine_elem_field<<<grid_for(np), BLOCK, 0, s>>>(np, sp[dim].offs,
+            CK(launch_kernel(k_refine_elem_field, dim3(grid_for(np)), dim3(BLOCK), 0, s, np, sp[dim].offs,
                 d.scale[dim], nc, pass == 0, static_cast<double const*>(t.data),
-                data + (size_t)d.ngo[dim] * nc);
+                data + (size_t)d.ngo[dim] * nc));
             CK_LAUNCH();
           }
           out->add_tag(dim, T_F64, t.name.c_str(), nc, t.transfer, data);
@@ -419,9 +445,9 @@ static u32* choose_refinement(Mesh& m, u32* cand, double qual_floor, double** qu
       double nel = m.counts[dim];
       PROBE(P_REFINE_QUALITY, s, 4.0 * (ne + 1) + 8.0 * deg(dim, 1) * nel + 8.0 * ne +
           4.0 * deg(dim, 0) * nel + 24.0 * m.counts[0] + 8.0 * ne + 8.0 * ne);
-      k_refine_quality<<<grid_for(ne), BLOCK, 0, s>>>(dim, ne, m.ask_down(1, 0),
+      CK(launch_kernel(k_refine_quality, dim3(grid_for(ne)), dim3(BLOCK), 0, s, dim, ne, m.ask_down(1, 0),
           m.ask_down(dim, 0), eo.offs, eo.adj, eo.dirs, m.coords(), qual_floor, m.segview(),
-          m.fp32_filter ? fp32_stats_dev() : nullptr, cand, q, any, inverted);
+          m.fp32_filter ? fp32_stats_dev() : nullptr, cand, q, any, inverted));
       CK_LAUNCH();
     }
   } else {
@@ -483,9 +509,9 @@ u32 refine_by_size(Mesh& m, double qual_floor)
   CK(cudaMemsetAsync(any, 0, sizeof(u32), s));
   if (ne) {
     PROBE(P_REFINE_CANDIDATES, s, 8.0 * ne + 32.0 * m.counts[0] + 4.0 * ne);
-    k_refine_candidates<<<grid_for(ne), BLOCK, 0, s>>>(ne, m.ask_down(1, 0), m.coords(),
+    CK(launch_kernel(k_refine_candidates, dim3(grid_for(ne)), dim3(BLOCK), 0, s, ne, m.ask_down(1, 0), m.coords(),
         static_cast<double const*>(h->data), m.segview(),
-        m.fp32_filter ? fp32_stats_dev() : nullptr, cand, any);
+        m.fp32_filter ? fp32_stats_dev() : nullptr, cand, any));
     CK_LAUNCH();
   }
   // no separate check for "any candidate": with none, the quality kernel
@@ -515,9 +541,9 @@ u32 refine_sets(Mesh& m, double qual_floor, u32* cand_out, u32* good_out,
   CK(cudaMemsetAsync(any, 0, sizeof(u32), s));
   CK(cudaMemsetAsync(indset_out, 0, sizeof(u32) * ne, s));
   if (ne) {
-    k_refine_candidates<<<grid_for(ne), BLOCK, 0, s>>>(ne, m.ask_down(1, 0), m.coords(),
+    CK(launch_kernel(k_refine_candidates, dim3(grid_for(ne)), dim3(BLOCK), 0, s, ne, m.ask_down(1, 0), m.coords(),
         static_cast<double const*>(h->data), m.segview(),
-        m.fp32_filter ? fp32_stats_dev() : nullptr, cand_out, any);
+        m.fp32_filter ? fp32_stats_dev() : nullptr, cand_out, any));
     CK_LAUNCH();
   }
   CK(cudaMemcpyAsync(good_out, cand_out, sizeof(u32) * ne, cudaMemcpyDeviceToDevice, s));

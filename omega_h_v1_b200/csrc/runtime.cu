@@ -1,5 +1,6 @@
 // Device runtime for the adaptation pass: error state, stream-ordered
 // allocation, the decoupled look-back exclusive scan and small array kernels.
+#include <cstdlib>
 #include <chrono>
 #include <cstdio>
 #include <cstring>
@@ -11,6 +12,16 @@
 #include "runtime.hpp"
 
 namespace osh {
+
+bool pdl_enabled()
+{
+  static bool const on = [] {
+    char const* e = std::getenv("OSH_B200_PDL");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
+
 
 // ---------------------------------------------------------------------------
 // errors
@@ -134,10 +145,35 @@ void fp32_stats_read(unsigned long long* decided, unsigned long long* rechecked,
   if (bound_exceeded) *bound_exceeded = h.bound_exceeded;
 }
 
+void fp32_audit_read(unsigned long long* audited, unsigned long long* flips,
+    unsigned long long* checked)
+{
+  Fp32Stats h;
+  CK(cudaDeviceSynchronize());
+  CK(cudaMemcpy(&h, fp32_stats_dev(), sizeof(h), cudaMemcpyDeviceToHost));
+  if (audited) *audited = h.audited;
+  if (flips) *flips = h.flips;
+  if (checked) *checked = h.checked;
+}
+
+// the counters return to zero; the audit switch is kept
 void fp32_stats_reset()
 {
   CK(cudaDeviceSynchronize());
-  CK(cudaMemset(fp32_stats_dev(), 0, sizeof(Fp32Stats)));
+  Fp32Stats* d = fp32_stats_dev();
+  unsigned audit = 0;
+  CK(cudaMemcpy(&audit, &d->audit, sizeof(audit), cudaMemcpyDeviceToHost));
+  Fp32Stats z;
+  std::memset(&z, 0, sizeof(z));
+  z.audit = audit;
+  CK(cudaMemcpy(d, &z, sizeof(z), cudaMemcpyHostToDevice));
+}
+
+void fp32_set_audit(bool on)
+{
+  CK(cudaDeviceSynchronize());
+  unsigned v = on ? 1u : 0u;
+  CK(cudaMemcpy(&fp32_stats_dev()->audit, &v, sizeof(v), cudaMemcpyHostToDevice));
 }
 
 void probe_enable(u32 mask) { probes().mask = mask; }
@@ -390,6 +426,7 @@ k_exscan(u32 const* __restrict__ in, u32* __restrict__ out, u32 n, u32 ntiles,
     unsigned long long* status, u32* ticket_and_err, u32* total_to, u32* __restrict__ newid,
     u32 spin_limit)
 {
+  pdl_wait();
   __shared__ u32 s_tile;
   __shared__ u32 s_warp[SCAN_WARPS];
   __shared__ u32 s_prefix;
@@ -525,6 +562,7 @@ k_exscan(u32 const* __restrict__ in, u32* __restrict__ out, u32 n, u32 ntiles,
 
 __global__ void k_set_zero_total(u32* out, u32* total_to)
 {
+  pdl_wait();
   out[0] = 0;
   if (total_to) *total_to = 0;
 }
@@ -578,7 +616,7 @@ u32* stream_scan_scratch(size_t words, cudaStream_t s)
 void exscan_u32(u32 const* in, u32* out, u32 n, cudaStream_t s, u32* total_to, u32* newid)
 {
   if (n == 0) {
-    k_set_zero_total<<<1, 1, 0, s>>>(out, total_to);
+    CK(launch_kernel(k_set_zero_total, dim3(1), dim3(1), 0, s, out, total_to));
     CK_LAUNCH();
     return;
   }
@@ -587,9 +625,9 @@ void exscan_u32(u32 const* in, u32* out, u32 n, cudaStream_t s, u32* total_to, u
   u32* scratch = stream_scan_scratch(4 + 2 * (size_t)ntiles, s);
   {
     PROBE(P_EXSCAN, s, 4.0 * n + 4.0 * (n + 1));
-    k_exscan<0><<<ntiles, SCAN_THREADS, 0, s>>>(in, out, n, ntiles,
+    CK(launch_kernel(k_exscan<0>, dim3(ntiles), dim3(SCAN_THREADS), 0, s, in, out, n, ntiles,
         reinterpret_cast<unsigned long long*>(scratch + 4), scratch, total_to, newid,
-        SCAN_SPIN_LIMIT);
+        SCAN_SPIN_LIMIT));
     CK_LAUNCH();
   }
 }
@@ -637,9 +675,9 @@ int selftest_scan_wait(u32 spin_limit)
   CK(cudaMemsetAsync(buf, 0, words * sizeof(u32), s));
   u32 one = 1;
   CK(cudaMemcpyAsync(scratch, &one, sizeof(u32), cudaMemcpyHostToDevice, s));
-  k_exscan<0><<<ntiles, SCAN_THREADS, 0, s>>>(in, out, n, ntiles,
+  CK(launch_kernel(k_exscan<0>, dim3(ntiles), dim3(SCAN_THREADS), 0, s, in, out, n, ntiles,
       reinterpret_cast<unsigned long long*>(scratch + 4), scratch, nullptr, nullptr,
-      spin_limit);
+      spin_limit));
   CK_LAUNCH();
   u32 err = 0;
   CK(cudaMemcpyAsync(&err, scratch + 1, sizeof(u32), cudaMemcpyDeviceToHost, s));
@@ -659,15 +697,15 @@ void exscan_u32_scratch(u32 const* in, u32* out, u32 n, u32* scratch, cudaStream
   if (reinterpret_cast<uintptr_t>(scratch) % 16 != 0)
     throw Failure(E_ARG, "scan scratch must start on a 16-byte boundary");
   if (n == 0) {
-    k_set_zero_total<<<1, 1, 0, s>>>(out, nullptr);
+    CK(launch_kernel(k_set_zero_total, dim3(1), dim3(1), 0, s, out, nullptr));
     CK_LAUNCH();
     return;
   }
   u32 ntiles = ceil_div(n, SCAN_TILE);
   CK(cudaMemsetAsync(scratch, 0, exscan_scratch_words(n) * sizeof(u32), s));
-  k_exscan<0><<<ntiles, SCAN_THREADS, 0, s>>>(in, out, n, ntiles,
+  CK(launch_kernel(k_exscan<0>, dim3(ntiles), dim3(SCAN_THREADS), 0, s, in, out, n, ntiles,
       reinterpret_cast<unsigned long long*>(scratch + 4), scratch, nullptr, nullptr,
-      SCAN_SPIN_LIMIT);
+      SCAN_SPIN_LIMIT));
   CK_LAUNCH();
 }
 
@@ -682,7 +720,7 @@ u32* negate_offsets(u32 const* offs, u32 n, cudaStream_t s, u32* total_to, u32* 
 {
   u32* o = dalloc<u32>((size_t)n + 1, s);
   if (n == 0) {
-    k_set_zero_total<<<1, 1, 0, s>>>(o, total_to);
+    CK(launch_kernel(k_set_zero_total, dim3(1), dim3(1), 0, s, o, total_to));
     CK_LAUNCH();
     return o;
   }
@@ -690,9 +728,9 @@ u32* negate_offsets(u32 const* offs, u32 n, cudaStream_t s, u32* total_to, u32* 
   u32* scratch = stream_scan_scratch(4 + 2 * (size_t)ntiles, s);
   {
     PROBE(P_EXSCAN, s, 4.0 * (n + 1) + 4.0 * (n + 1));
-    k_exscan<1><<<ntiles, SCAN_THREADS, 0, s>>>(offs, o, n, ntiles,
+    CK(launch_kernel(k_exscan<1>, dim3(ntiles), dim3(SCAN_THREADS), 0, s, offs, o, n, ntiles,
         reinterpret_cast<unsigned long long*>(scratch + 4), scratch, total_to, newid,
-        SCAN_SPIN_LIMIT);
+        SCAN_SPIN_LIMIT));
     CK_LAUNCH();
   }
   return o;
@@ -700,6 +738,7 @@ u32* negate_offsets(u32 const* offs, u32 n, cudaStream_t s, u32* total_to, u32* 
 
 __global__ void k_fill(u32* a, u32 n, u32 v)
 {
+  pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) a[i] = v;
 }
@@ -707,12 +746,13 @@ __global__ void k_fill(u32* a, u32 n, u32 v)
 void fill_u32(u32* a, u32 n, u32 v, cudaStream_t s)
 {
   if (!n) return;
-  k_fill<<<grid_for(n), BLOCK, 0, s>>>(a, n, v);
+  CK(launch_kernel(k_fill, dim3(grid_for(n)), dim3(BLOCK), 0, s, a, n, v));
   CK_LAUNCH();
 }
 
 __global__ void k_iota(u32* a, u32 n, u32 stride)
 {
+  pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) a[i] = i * stride;
 }
@@ -720,12 +760,13 @@ __global__ void k_iota(u32* a, u32 n, u32 stride)
 void iota_u32(u32* a, u32 n, u32 stride, cudaStream_t s)
 {
   if (!n) return;
-  k_iota<<<grid_for(n), BLOCK, 0, s>>>(a, n, stride);
+  CK(launch_kernel(k_iota, dim3(grid_for(n)), dim3(BLOCK), 0, s, a, n, stride));
   CK_LAUNCH();
 }
 
 __global__ void k_iota64(u64* a, u32 n)
 {
+  pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) a[i] = i;
 }
@@ -733,7 +774,7 @@ __global__ void k_iota64(u64* a, u32 n)
 void iota_u64(u64* a, u32 n, cudaStream_t s)
 {
   if (!n) return;
-  k_iota64<<<grid_for(n), BLOCK, 0, s>>>(a, n);
+  CK(launch_kernel(k_iota64, dim3(grid_for(n)), dim3(BLOCK), 0, s, a, n));
   CK_LAUNCH();
 }
 
@@ -741,6 +782,7 @@ template <class T>
 __global__ void k_expand(T const* __restrict__ in, u32 const* __restrict__ offs,
     u32 n, u32 width, T* __restrict__ out)
 {
+  pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   u32 f = offs[i], e = offs[i + 1];
@@ -755,15 +797,15 @@ void expand_rows(void const* in, u32 const* offs, u32 n, u32 width, u32 esz,
   PROBE(P_EXPAND, s, 4.0 * (n + 1) + 2.0 * (double)n * width * esz);
   switch (esz) {
     case 1:
-      k_expand<unsigned char><<<grid_for(n), BLOCK, 0, s>>>(
-          (unsigned char const*)in, offs, n, width, (unsigned char*)out);
+      CK(launch_kernel(k_expand<unsigned char>, dim3(grid_for(n)), dim3(BLOCK), 0, s, 
+          (unsigned char const*)in, offs, n, width, (unsigned char*)out));
       break;
     case 4:
-      k_expand<u32><<<grid_for(n), BLOCK, 0, s>>>((u32 const*)in, offs, n, width, (u32*)out);
+      CK(launch_kernel(k_expand<u32>, dim3(grid_for(n)), dim3(BLOCK), 0, s, (u32 const*)in, offs, n, width, (u32*)out));
       break;
     default:
-      k_expand<unsigned long long><<<grid_for(n), BLOCK, 0, s>>>(
-          (unsigned long long const*)in, offs, n, width, (unsigned long long*)out);
+      CK(launch_kernel(k_expand<unsigned long long>, dim3(grid_for(n)), dim3(BLOCK), 0, s, 
+          (unsigned long long const*)in, offs, n, width, (unsigned long long*)out));
       break;
   }
   CK_LAUNCH();
@@ -771,6 +813,7 @@ void expand_rows(void const* in, u32 const* offs, u32 n, u32 width, u32 esz,
 
 __global__ void k_max_u32(u32 const* __restrict__ a, u32 n, u32* out)
 {
+  pdl_wait();
   u32 m = 0;
   for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
     m = max(m, a[i]);
@@ -785,7 +828,7 @@ u32 max_u32(u32 const* a, u32 n, cudaStream_t s)
   CK(cudaMemsetAsync(d, 0, sizeof(u32), s));
   u32 g = grid_for(n);
   if (g > 4096) g = 4096;
-  k_max_u32<<<g, BLOCK, 0, s>>>(a, n, d);
+  CK(launch_kernel(k_max_u32, dim3(g), dim3(BLOCK), 0, s, a, n, d));
   CK_LAUNCH();
   u32 v = read_u32(d, s);
   dev_free(d, s);

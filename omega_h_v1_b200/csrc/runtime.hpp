@@ -87,6 +87,16 @@ Fp32Stats* fp32_stats_dev();
 void fp32_stats_read(unsigned long long* decided, unsigned long long* rechecked,
     double* max_err, unsigned* bound_exceeded);
 void fp32_stats_reset();
+// audit mode (every decision taken on an estimate also taken in double) and
+// its counters
+void fp32_set_audit(bool on);
+void fp32_audit_read(unsigned long long* audited, unsigned long long* flips,
+    unsigned long long* checked);
+// the filter's estimates for n given tets (12 coordinates each) and edges
+// (6 coordinates and 2 sizes each), with the double values (filter.cu)
+void fp32_probe_tets(u32 n, double const* host_x, float* est, float* err, double* q64);
+void fp32_probe_edges(u32 n, double const* host_x, double const* host_h, double thr,
+    int* side, double* ratio64);
 
 void probe_enable(u32 mask);
 void probe_reset();

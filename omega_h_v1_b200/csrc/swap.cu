@@ -197,9 +197,10 @@ __device__ void choose_edge_swap(u32 rs, double const (*ex)[3], double const (*r
 
 // Upper bound, from single-precision estimates, on the best triangulation's
 // worst tet as choose_edge_swap would find it, valid whenever that value is
-// positive (a triangulation it stops early on has a negative value).
+// positive (a triangulation it stops early on has a negative value). With
+// `audit`, every estimate is also compared with its double value.
 __device__ float best_swap_upper_f32(u32 rs, double const (*ex)[3], double const (*rx)[3],
-    float perfect)
+    float k6, Fp32Stats* audit)
 {
   float cache[35];
   unsigned long long cached = 0;
@@ -222,8 +223,9 @@ __device__ float best_swap_upper_f32(u32 rs, double const (*ex)[3], double const
           tx[3][0] = ex[1 - k][0];
           tx[3][1] = ex[1 - k][1];
           tx[3][2] = ex[1 - k][2];
-          Q32 q = tet_quality_f32(tx, perfect);
-          tri_upper = fminf(tri_upper, q.q + q.err);
+          Q32 q = tet_quality_f32(tx, k6);
+          if (audit) fp32_note_error(audit, q, tet_quality(tx, perfect_tet_quality()));
+          tri_upper = fminf(tri_upper, q32_hi(q));
           for (u32 c = 0; c < 3; ++c) {
             double tmp = tx[0][c];
             tx[0][c] = tx[1][c];
@@ -244,6 +246,7 @@ __device__ float best_swap_upper_f32(u32 rs, double const (*ex)[3], double const
 __global__ void k_unmark_boundary(u32 n, u32 dim, u32 const* __restrict__ cd,
     u32* __restrict__ marked, u32* any)
 {
+  pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   u32 keep = 0;
   if (i < n) {
@@ -261,8 +264,10 @@ __global__ void k_swap_quality(u32 ne, u32 const* __restrict__ te_offs,
     u32* __restrict__ cand, double* __restrict__ quals, u32* __restrict__ ring_sizes,
     u32* __restrict__ codes, u32* any)
 {
+  pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   u32 keep = 0;
+  bool decided = false, rechecked = false, audited = false, flipped = false;
   if (i < ne && cand[i]) {
     double old_minq = 1;
     for (u32 j = te_offs[i]; j < te_offs[i + 1]; ++j)
@@ -282,12 +287,19 @@ __global__ void k_swap_quality(u32 ne, u32 const* __restrict__ te_offs,
       // an upper bound at or below it settles the rejection
       bool filtered = false;
       if (fs && old_minq > 0) {
-        float ub = best_swap_upper_f32(rs, ex, rx, (float)perfect_tet_quality());
+        float ub = best_swap_upper_f32(rs, ex, rx, tet_k6_f32(), fs->audit ? fs : nullptr);
         if ((double)ub <= old_minq) {
           filtered = true;
-          atomicAdd(&fs->decided, 1ull);
+          decided = true;
+          if (fs->audit) {
+            u32 c64;
+            double q64;
+            choose_edge_swap(rs, ex, rx, perfect_tet_quality(), &c64, &q64);
+            audited = true;
+            flipped = q64 > old_minq;
+          }
         } else {
-          atomicAdd(&fs->rechecked, 1ull);
+          rechecked = true;
         }
       }
       if (!filtered) choose_edge_swap(rs, ex, rx, perfect_tet_quality(), &code, &q);
@@ -305,6 +317,7 @@ __global__ void k_swap_quality(u32 ne, u32 const* __restrict__ te_offs,
     quals[i] = 0.0;
     ring_sizes[i] = 0;
   }
+  if (fs) fp32_count_warp(fs, decided, rechecked, audited, flipped);
   if (__any_sync(0xffffffffu, keep) && (threadIdx.x & 31) == 0) atomicOr(any, 1u);
 }
 
@@ -318,6 +331,7 @@ __device__ inline u32 count_swap_ents(u32 rs, u32 dim)
 __global__ void k_swap_counts(u32 ne, u32 dim, u32 const* __restrict__ ind,
     u32 const* __restrict__ rs, u32* __restrict__ cnt)
 {
+  pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < ne) cnt[i] = ind[i] ? count_swap_ents(rs[i], dim) : 0u;
 }
@@ -329,6 +343,7 @@ __global__ void k_swap_cavity(u32 ne, u32 dim, u32 const* __restrict__ ind,
     u32 const* __restrict__ te_dirs, u32 const* __restrict__ voe1,
     u32 const* __restrict__ vot, u32* __restrict__ out)
 {
+  pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= ne || !ind[i]) return;
   u32 ev[2], rv[MAX_EDGE_SWAP];
@@ -371,6 +386,7 @@ __global__ void k_swap_cavity(u32 ne, u32 dim, u32 const* __restrict__ ind,
 __global__ void k_swap_same(u32 n, u32 lph, u32 const* __restrict__ loh,
     u32 const* __restrict__ ind, u32* __restrict__ same)
 {
+  pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   u32 r = 1;
@@ -388,6 +404,7 @@ __global__ void k_swap_conserve(u32 ne, u32 nc, u32 nsame, u32 const* __restrict
     double const* __restrict__ sizes, double const* __restrict__ in,
     double* __restrict__ gen)
 {
+  pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= ne || gen_offs[i] == gen_offs[i + 1]) return;
   double sum[MAX_NCOMPS];
@@ -408,6 +425,7 @@ __global__ void k_swap_fit(u32 ne, u32 nc, u32 const* __restrict__ gen_offs,
     u32 const* __restrict__ te_offs, u32 const* __restrict__ te,
     double const* __restrict__ in, double* __restrict__ gen)
 {
+  pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= ne || gen_offs[i] == gen_offs[i + 1]) return;
   u32 f = te_offs[i], e = te_offs[i + 1];
@@ -463,8 +481,8 @@ static bool swap_select(Mesh& m, double gq, u32 nlayers, SwapSel& sel, u32* sliv
   // "any swap kept" flag (mailbox slot 6) is the one read
   u32* any = m.mb->dev + 6;
   CK(cudaMemsetAsync(m.mb->dev + 5, 0, 2 * sizeof(u32), s));  // slots 5-6
-  k_unmark_boundary<<<grid_for(ne), BLOCK, 0, s>>>(ne, m.dim, static_cast<u32 const*>(cd->data),
-      sel.cand, m.mb->dev + 5);
+  CK(launch_kernel(k_unmark_boundary, dim3(grid_for(ne)), dim3(BLOCK), 0, s, ne, m.dim, static_cast<u32 const*>(cd->data),
+      sel.cand, m.mb->dev + 5));
   CK_LAUNCH();
   if (interior_out)
     CK(cudaMemcpyAsync(interior_out, sel.cand, sizeof(u32) * ne, cudaMemcpyDeviceToDevice, s));
@@ -475,9 +493,9 @@ static bool swap_select(Mesh& m, double gq, u32 nlayers, SwapSel& sel, u32* sliv
   double const* eq = m.qualities();
   PROBE(P_SWAP_QUALITY, s, 4.0 * (ne + 1) + 8.0 * 6.0 * m.counts[3] + 8.0 * ne +
       16.0 * m.counts[3] + 24.0 * m.counts[0] + 8.0 * m.counts[3] + 4.0 * ne + 16.0 * ne);
-  k_swap_quality<<<ceil_div(ne, 128), 128, 0, s>>>(ne, te.offs, te.adj, te.dirs, m.ask_down(1, 0),
+  CK(launch_kernel(k_swap_quality, dim3(ceil_div(ne, 128)), dim3(128), 0, s, ne, te.offs, te.adj, te.dirs, m.ask_down(1, 0),
       m.ask_down(3, 0), m.coords(), eq, m.fp32_filter ? fp32_stats_dev() : nullptr, sel.cand,
-      sel.quals, sel.rs, sel.codes, any);
+      sel.quals, sel.rs, sel.codes, any));
   CK_LAUNCH();
   if (!read_u32(any, s)) return false;
   sel.ind = find_indset(m, 1, sel.cand, sel.quals);
@@ -522,13 +540,13 @@ static void swap_build(Mesh& m, SwapSel const& sel)
   u32* newid_of[4] = {nullptr, nullptr, nullptr, nullptr};
   for (u32 ed = ed0; ed <= dim; ++ed) {
     u32 n = m.count(ed);
-    k_swap_counts<<<grid_for(ne), BLOCK, 0, s>>>(ne, ed, sel.ind, sel.rs, cnt);
+    CK(launch_kernel(k_swap_counts, dim3(grid_for(ne)), dim3(BLOCK), 0, s, ne, ed, sel.ind, sel.rs, cnt));
     CK_LAUNCH();
     gen_offs_of[ed] = exscan_new(cnt, ne, s, m.mb->dev + 20 + 2 * (ed - 1));
     u32* same = dalloc<u32>(n, s);
     if (n) {
-      k_swap_same<<<grid_for(n), BLOCK, 0, s>>>(n, deg(ed, 1), ed == 1 ? nullptr : m.ask_down(ed, 1),
-          sel.ind, same);
+      CK(launch_kernel(k_swap_same, dim3(grid_for(n)), dim3(BLOCK), 0, s, n, deg(ed, 1), ed == 1 ? nullptr : m.ask_down(ed, 1),
+          sel.ind, same));
       CK_LAUNCH();
     }
     if (carried_high(m, ed)) newid_of[ed] = dalloc<u32>(n ? n : 1, s);
@@ -544,8 +562,8 @@ static void swap_build(Mesh& m, SwapSel const& sel)
     u32* same_offs = same_of[ed];
     u32* conn = dalloc<u32>((size_t)(nsame + ngen) * vpe, s);
     expand_scaled(m.ask_down(ed, 0), same_offs, 1, n, vpe, 4, conn, s);
-    k_swap_cavity<<<ceil_div(ne, 128), 128, 0, s>>>(ne, ed, sel.ind, sel.codes, gen_offs, te.offs,
-        te.adj, te.dirs, voe1, vot, conn + (size_t)nsame * vpe);
+    CK(launch_kernel(k_swap_cavity, dim3(ceil_div(ne, 128)), dim3(128), 0, s, ne, ed, sel.ind, sel.codes, gen_offs, te.offs,
+        te.adj, te.dirs, voe1, vot, conn + (size_t)nsame * vpe));
     CK_LAUNCH();
     out->set_ents(ed, nsame + ngen, conn);
     if (m.full) {
@@ -573,8 +591,8 @@ static void swap_build(Mesh& m, SwapSel const& sel)
           if (nc > MAX_NCOMPS) throw Failure(E_ARG, "conserved field wider than 32");
           double* data = dalloc<double>((size_t)(nsame + ngen) * nc, s);
           expand_scaled(t.data, same_offs, 1, n, nc, 8, data, s);
-          k_swap_conserve<<<grid_for(ne), BLOCK, 0, s>>>(ne, nc, nsame, gen_offs, te.offs,
-              te.adj, sizes, static_cast<double const*>(t.data), data + (size_t)nsame * nc);
+          CK(launch_kernel(k_swap_conserve, dim3(grid_for(ne)), dim3(BLOCK), 0, s, ne, nc, nsame, gen_offs, te.offs,
+              te.adj, sizes, static_cast<double const*>(t.data), data + (size_t)nsame * nc));
           CK_LAUNCH();
           out->add_tag(ed, T_F64, t.name.c_str(), nc, t.transfer, data);
         }
@@ -585,8 +603,8 @@ static void swap_build(Mesh& m, SwapSel const& sel)
         u32 nc = t.ncomps;
         double* data = dalloc<double>((size_t)(nsame + ngen) * nc, s);
         expand_scaled(t.data, same_offs, 1, n, nc, 8, data, s);
-        k_swap_fit<<<grid_for(ne), BLOCK, 0, s>>>(ne, nc, gen_offs, te.offs, te.adj,
-            static_cast<double const*>(t.data), data + (size_t)nsame * nc);
+        CK(launch_kernel(k_swap_fit, dim3(grid_for(ne)), dim3(BLOCK), 0, s, ne, nc, gen_offs, te.offs, te.adj,
+            static_cast<double const*>(t.data), data + (size_t)nsame * nc));
         CK_LAUNCH();
         out->add_tag(ed, T_F64, t.name.c_str(), nc, t.transfer, data);
       }

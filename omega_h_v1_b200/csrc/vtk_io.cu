@@ -67,6 +67,7 @@ __host__ __device__ inline u32 b64_value(u32 c)
 __global__ void k_b64_encode(unsigned char const* __restrict__ in, u64 nbytes,
     char4* __restrict__ out)
 {
+  pdl_wait();
   u64 u = blockIdx.x * (u64)blockDim.x + threadIdx.x;
   u64 b = u * 3;
   if (b >= nbytes) return;
@@ -87,6 +88,7 @@ __global__ void k_b64_encode(unsigned char const* __restrict__ in, u64 nbytes,
 __global__ void k_b64_decode(char const* __restrict__ in, u64 nbytes,
     unsigned char* __restrict__ out, u32* bad)
 {
+  pdl_wait();
   u64 u = blockIdx.x * (u64)blockDim.x + threadIdx.x;
   u64 b = u * 3;
   if (b >= nbytes) return;
@@ -108,6 +110,7 @@ __global__ void k_b64_decode(char const* __restrict__ in, u64 nbytes,
 // reverse the bytes of every `width`-byte value (generic_swap_if_needed)
 __global__ void k_swap_bytes(unsigned char* a, u64 n, u32 width)
 {
+  pdl_wait();
   u64 i = blockIdx.x * (u64)blockDim.x + threadIdx.x;
   if (i >= n) return;
   unsigned char* p = a + i * width;
@@ -122,6 +125,7 @@ __global__ void k_swap_bytes(unsigned char* a, u64 n, u32 width)
 __global__ void k_cell_arrays(u32 n, u32 vpe, u32* __restrict__ offs, unsigned char* types,
     unsigned char type)
 {
+  pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   offs[i] = (i + 1) * vpe;
@@ -342,12 +346,12 @@ struct Reader {
         if (nbytes) {
           to_device();
           CK(cudaMemsetAsync(dbad, 0, sizeof(u32), s));
-          k_b64_decode<<<encode_grid(nbytes), BLOCK, 0, s>>>(dtext + pos + head, nbytes,
-              static_cast<unsigned char*>(out), dbad);
+          CK(launch_kernel(k_b64_decode, dim3(encode_grid(nbytes)), dim3(BLOCK), 0, s, dtext + pos + head, nbytes,
+              static_cast<unsigned char*>(out), dbad));
           CK_LAUNCH();
           if (swap && esz > 1) {
-            k_swap_bytes<<<grid_for(nvals), BLOCK, 0, s>>>(static_cast<unsigned char*>(out),
-                nvals, esz);
+            CK(launch_kernel(k_swap_bytes, dim3(grid_for(nvals)), dim3(BLOCK), 0, s, static_cast<unsigned char*>(out),
+                nvals, esz));
             CK_LAUNCH();
           }
           u32 bad = 0;
@@ -637,8 +641,8 @@ struct Writer {
           dtext = dalloc<char>(nch, s);
           dcap = nch;
         }
-        k_b64_encode<<<encode_grid(nbytes), BLOCK, 0, s>>>(
-            static_cast<unsigned char const*>(d), nbytes, reinterpret_cast<char4*>(dtext));
+        CK(launch_kernel(k_b64_encode, dim3(encode_grid(nbytes)), dim3(BLOCK), 0, s, 
+            static_cast<unsigned char const*>(d), nbytes, reinterpret_cast<char4*>(dtext)));
         CK_LAUNCH();
         char* h = static_cast<char*>(host_staging(nch));
         CK(cudaMemcpyAsync(h, dtext, nch, cudaMemcpyDeviceToHost, s));
@@ -773,8 +777,8 @@ void write_vtu(Mesh& m, char const* path, bool ascii, bool compress)
     u32* offs = dalloc<u32>(nelems ? nelems : 1, m.s);
     unsigned char* types = dalloc<unsigned char>(nelems ? nelems : 1, m.s);
     if (nelems) {
-      k_cell_arrays<<<grid_for(nelems), BLOCK, 0, m.s>>>(nelems, deg(dim, 0), offs, types,
-          CELL_TYPES[dim]);
+      CK(launch_kernel(k_cell_arrays, dim3(grid_for(nelems)), dim3(BLOCK), 0, m.s, nelems, deg(dim, 0), offs, types,
+          CELL_TYPES[dim]));
       CK_LAUNCH();
     }
     try {

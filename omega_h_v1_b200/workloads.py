@@ -69,6 +69,21 @@ class BoxJob:
         return self.tets * max(6.9 / c ** 3, 0.5)
 
 
+def place_jobs(jobs, nbins):
+    """Whole jobs onto nbins GPUs by greedy bin packing on estimated output
+    tets: largest job first (ties by index) onto the least-loaded bin (ties
+    by the lower bin). Returns one ascending list of job positions per bin.
+    Jobs never share data, so the bins need no exchange."""
+    order = sorted(range(len(jobs)), key=lambda i: (-jobs[i].estimated_output_tets(), i))
+    load = [0.0] * nbins
+    bins = [[] for _ in range(nbins)]
+    for i in order:
+        b = min(range(nbins), key=lambda k: (load[k], k))
+        bins[b].append(i)
+        load[b] += jobs[i].estimated_output_tets()
+    return [sorted(b) for b in bins]
+
+
 def batched_boxes(count=512, seed=1, nmin=4, nmax=40):
     rng = SplitMix64(seed)
     out = []

@@ -1,7 +1,9 @@
-"""World-size-2 checks of the replica plumbing bench.py uses on N GPUs, run
-as two gloo ranks on the CPU: every rank takes the same collective steps,
-throughput is all ranks' units over the slowest rank's time, and the CPU
-reference arm runs on rank 0 only."""
+"""World-size-2 checks of the multi-GPU plumbing bench.py uses on N GPUs,
+run as two gloo ranks on the CPU: every rank takes the same collective
+steps, throughput is all ranks' units over the slowest rank's time, the CPU
+reference arm runs on rank 0 only, and meshes placed whole on the ranks by
+bin packing (each rank adapting its own with the oracle) end as they do on
+one rank."""
 import os
 import socket
 
@@ -74,3 +76,70 @@ def test_reference_arm_runs_on_rank0_only():
     out = mgr.dict()
     mp.spawn(_ref_worker, args=(world, _free_port(), out), nprocs=world, join=True)
     assert out[1] is None
+
+
+def _adapt_worker(rank, world, port, out):
+    """Each rank adapts the meshes placed on it (the oracle on the CPU
+    stands in for a GPU) and reports their digests; the ranks exchange only
+    the final counts, as bench.py's batched legs do."""
+    import datetime
+    import sys
+    import torch.distributed as dist
+    sys.path.insert(0, ROOT)
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=120))
+    import bench
+    import large_flows as F
+    from oracle import oracle as O
+    from omega_h_v1_b200 import workloads as W
+    jobs = W.batched_boxes(12, seed=5, nmax=5)
+    mine = W.place_jobs(jobs, world)[rank]
+    digests, tets = {}, 0.0
+    for i in mine:
+        m = F.box_job_mesh(O.Oracle, O.box, jobs[i])
+        m.adapt(*F.BOX_ADAPT)
+        digests[i] = O.snapshot_digest(m.snapshot())
+        tets += m.count(3)
+        m.close()
+    total = bench.sum_over_ranks(tets, world)
+    out[rank] = (mine, digests, total)
+    dist.destroy_process_group()
+
+
+def test_meshes_placed_on_two_ranks_adapt_as_on_one():
+    import sys
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import large_flows as F
+    from oracle import oracle as O
+    from omega_h_v1_b200 import workloads as W
+    world = 2
+    mgr = mp.Manager()
+    out = mgr.dict()
+    mp.spawn(_adapt_worker, args=(world, _free_port(), out), nprocs=world, join=True)
+    jobs = W.batched_boxes(12, seed=5, nmax=5)
+    placed = sorted(out[0][0] + out[1][0])
+    assert placed == list(range(len(jobs)))           # every mesh placed once
+    want, tets = {}, 0
+    for i, j in enumerate(jobs):
+        m = F.box_job_mesh(O.Oracle, O.box, j)
+        m.adapt(*F.BOX_ADAPT)
+        want[i] = O.snapshot_digest(m.snapshot())
+        tets += m.count(3)
+        m.close()
+    for r in range(world):
+        for i, d in out[r][1].items():
+            assert d == want[i], (r, i)
+        assert out[r][2] == tets
+
+
+def test_placement_balances_estimated_work():
+    from omega_h_v1_b200 import workloads as W
+    jobs = W.batched_boxes()
+    for nb in (1, 2, 4, 8):
+        bins = W.place_jobs(jobs, nb)
+        assert sorted(i for b in bins for i in b) == list(range(len(jobs)))
+        loads = [sum(jobs[i].estimated_output_tets() for i in b) for b in bins]
+        biggest = max(j.estimated_output_tets() for j in jobs)
+        # greedy largest-first: no bin exceeds the mean by more than one job
+        assert max(loads) <= sum(loads) / nb + biggest
