@@ -311,6 +311,22 @@ int osh_b200_selftest_scan_wait(unsigned spin_limit) OSH_PUBLIC;
    cudaStream_t; 0 is the legacy default stream); the caller keeps it alive */
 void osh_b200_set_stream(osh_t m, void* stream) OSH_PUBLIC;
 
+/* ---- launch shapes (tuning table) ------------------------------------------ */
+/* No counterpart in the reference (its loops launch 256 threads per block,
+   loop_cuda.hpp:28-53). Lanes per row of the long-row kernels, threads per
+   block and scan tile sizes come from a table: defaults, overridden once at
+   load by the file named by OSH_B200_TUNING or else tuning.txt beside the
+   library ("name value" lines, written by omega_h_v1_b200/tune.py, which
+   times each candidate with CUDA events on the GPU it runs on). Every allowed
+   value gives the same meshes. get/set/load return 0 or OSH_B200_E_ARG
+   (unknown name, a value the key does not allow, or a bad line in the file:
+   then nothing of the file is applied) / OSH_B200_E_IO (unreadable file). */
+unsigned osh_b200_tuning_count(void) OSH_PUBLIC;
+char const* osh_b200_tuning_name(unsigned i) OSH_PUBLIC;
+int osh_b200_tuning_get(char const* name, unsigned* value) OSH_PUBLIC;
+int osh_b200_tuning_set(char const* name, unsigned value) OSH_PUBLIC;
+int osh_b200_tuning_load(char const* path) OSH_PUBLIC;
+
 /* ---- per-kernel event probes (bench instrumentation) -------------------- */
 /* Bit i of mask enables probe i: each launch of that kernel is bracketed by
    CUDA events on its stream and credited with its algorithmic bytes. */

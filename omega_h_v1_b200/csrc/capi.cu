@@ -1169,6 +1169,12 @@ void osh_b200_host_stats(unsigned long long* allocs, double* sync_wait_seconds)
   osh::host_stats(allocs, sync_wait_seconds);
 }
 
+unsigned osh_b200_tuning_count(void) { return osh::TK_NKEYS; }
+char const* osh_b200_tuning_name(unsigned i) { return osh::tune_name(i); }
+int osh_b200_tuning_get(char const* name, unsigned* value) { return osh::tune_get(name, value); }
+int osh_b200_tuning_set(char const* name, unsigned value) { return osh::tune_set(name, value); }
+int osh_b200_tuning_load(char const* path) { return osh::tune_load(path); }
+
 int osh_b200_selftest_scan_wait(unsigned spin_limit)
 {
   API_TRY

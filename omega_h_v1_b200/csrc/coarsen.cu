@@ -339,14 +339,15 @@ __global__ void k_vertex_dest(u32 nv, u32 const* __restrict__ ue_offs,
   gen_vert[i] = g;
 }
 
-// The two vertex kernels with a group of VERT_GROUP lanes per vertex row
-// (rows of about 13.5 edges): lane l takes the row's entries l, l + 8, ...,
-// and shuffles within the group combine the lanes' results. The best
-// collapse keeps the first entry (in upward order) of greatest quality, as
-// the reference's loop does, so lanes combine (quality, position) pairs;
-// the destination is the first entry whose quality equals the best.
-constexpr u32 VERT_GROUP = 8;
+// The two vertex kernels with a group of VG lanes per vertex row (rows of
+// about 13.5 edges; VG is the tuning table's vert_group): lane l takes the
+// row's entries l, l + VG, ..., and shuffles within the group combine the
+// lanes' results. The best collapse keeps the first entry (in upward order)
+// of greatest quality, as the reference's loop does, so lanes combine
+// (quality, position) pairs; the destination is the first entry whose
+// quality equals the best.
 
+template <u32 VG>
 __global__ void k_collapses_to_verts_grouped(u32 nv, u32 const* __restrict__ ue_offs,
     u32 const* __restrict__ ue, u32 const* __restrict__ ue_dirs,
     u32 const* __restrict__ codes, double const* __restrict__ q2, u32* __restrict__ cand,
@@ -354,13 +355,13 @@ __global__ void k_collapses_to_verts_grouped(u32 nv, u32 const* __restrict__ ue_
 {
   pdl_wait();
   u32 const t = blockIdx.x * blockDim.x + threadIdx.x;
-  u32 const i = t / VERT_GROUP, lg = t % VERT_GROUP;
+  u32 const i = t / VG, lg = t % VG;
   if (i >= nv) return;  // a group shares i: it leaves together
-  u32 const gbase = (threadIdx.x & 31) & ~(VERT_GROUP - 1);
-  u32 const gmask = ((1u << VERT_GROUP) - 1u) << gbase;
+  u32 const gbase = (threadIdx.x & 31) & ~(VG - 1);
+  u32 const gmask = ((1u << VG) - 1u) << gbase;
   double maxq = 0;
   u32 pos = INV;  // position of the lane's best entry; INV: no collapse seen
-  for (u32 j = ue_offs[i] + lg; j < ue_offs[i + 1]; j += VERT_GROUP) {
+  for (u32 j = ue_offs[i] + lg; j < ue_offs[i + 1]; j += VG) {
     u32 e = ue[j], d = ue_dirs[j];
     if (!collapses(codes[e], d)) continue;
     double q = q2[e * 2 + d];
@@ -369,7 +370,7 @@ __global__ void k_collapses_to_verts_grouped(u32 nv, u32 const* __restrict__ ue_
       pos = j;
     }
   }
-  for (u32 o = VERT_GROUP / 2; o; o >>= 1) {
+  for (u32 o = VG / 2; o; o >>= 1) {
     double oq = __shfl_xor_sync(gmask, maxq, o);
     u32 op = __shfl_xor_sync(gmask, pos, o);
     if (op != INV && (pos == INV || oq > maxq || (oq == maxq && op < pos))) {
@@ -383,6 +384,7 @@ __global__ void k_collapses_to_verts_grouped(u32 nv, u32 const* __restrict__ ue_
   }
 }
 
+template <u32 VG>
 __global__ void k_vertex_dest_grouped(u32 nv, u32 const* __restrict__ ue_offs,
     u32 const* __restrict__ ue, u32 const* __restrict__ ue_dirs,
     u32 const* __restrict__ voe1, u32 const* __restrict__ ind,
@@ -391,10 +393,10 @@ __global__ void k_vertex_dest_grouped(u32 nv, u32 const* __restrict__ ue_offs,
 {
   pdl_wait();
   u32 const t = blockIdx.x * blockDim.x + threadIdx.x;
-  u32 const i = t / VERT_GROUP, lg = t % VERT_GROUP;
+  u32 const i = t / VG, lg = t % VG;
   if (i >= nv) return;
-  u32 const gbase = (threadIdx.x & 31) & ~(VERT_GROUP - 1);
-  u32 const gmask = ((1u << VERT_GROUP) - 1u) << gbase;
+  u32 const gbase = (threadIdx.x & 31) & ~(VG - 1);
+  u32 const gmask = ((1u << VG) - 1u) << gbase;
   if (!ind[i]) {
     if (lg == 0) gen_vert[i] = INV;
     return;
@@ -402,7 +404,7 @@ __global__ void k_vertex_dest_grouped(u32 nv, u32 const* __restrict__ ue_offs,
   double maxq = colq[i];
   if (maxq == 1e10) maxq = -1e10;
   u32 first = INV;
-  for (u32 j = ue_offs[i] + lg; j < ue_offs[i + 1]; j += VERT_GROUP) {
+  for (u32 j = ue_offs[i] + lg; j < ue_offs[i + 1]; j += VG) {
     u32 e = ue[j], d = ue_dirs[j];
     if (!collapses(codes[e], d)) continue;
     double q = q2[e * 2 + d];
@@ -412,7 +414,7 @@ __global__ void k_vertex_dest_grouped(u32 nv, u32 const* __restrict__ ue_offs,
       break;
     }
   }
-  for (u32 o = VERT_GROUP / 2; o; o >>= 1) first = min(first, __shfl_xor_sync(gmask, first, o));
+  for (u32 o = VG / 2; o; o >>= 1) first = min(first, __shfl_xor_sync(gmask, first, o));
   if (lg == 0) {
     u32 g = INV;
     if (first != INV) g = voe1[ue[first] * 2 + (1 - ue_dirs[first])];
@@ -747,8 +749,9 @@ static bool coarsen_select(Mesh& m, u32* codes, double qual_floor, bool require_
     PROBE(P_COARSEN_QUALITY, s, 4.0 * (nv + 1) + 8.0 * deg(dim, 0) * nel + 8.0 * ne +
         4.0 * deg(dim, 0) * nel + 24.0 * nv + 8.0 * ne + 16.0 * ne);
     // a warp per listed edge; the list's length is read on the device
-    u32 blocks = (u32)std::min<u64>(ceil_div((u64)ne * 32, BLOCK), 148u * 16u);
-    CK(launch_kernel(k_coarsen_quality, dim3(blocks), dim3(BLOCK), 0, s, dim, clist, ncand, voe1, m.ask_down(dim, 0),
+    u32 const qb = tuned(TK_QUALITY_BLOCK);
+    u32 blocks = (u32)std::min<u64>(ceil_div((u64)ne * 32, qb), 148u * 16u * 256u / qb);
+    CK(launch_kernel(k_coarsen_quality, dim3(blocks), dim3(qb), 0, s, dim, clist, ncand, voe1, m.ask_down(dim, 0),
         ev.offs, ev.adj, ev.dirs, m.coords(), eq, qual_floor, m.segview(),
         m.fp32_filter ? fp32_stats_dev() : nullptr, codes, sel.q2, any));
     CK_LAUNCH();
@@ -767,15 +770,21 @@ static bool coarsen_select(Mesh& m, u32* codes, double qual_floor, bool require_
   sel.cand = dalloc<u32>(nv, s);
   sel.colq = dalloc<double>(nv, s);
   if (nv) {
-    CK(launch_kernel(k_collapses_to_verts_grouped, dim3(grid_for((u64)nv * VERT_GROUP)), dim3(BLOCK), 0, s, nv, ue.offs,
-        ue.adj, ue.dirs, codes, sel.q2, sel.cand, sel.colq));
+    u32 const vg = tuned(TK_VERT_GROUP);
+    auto k = vg == 4 ? k_collapses_to_verts_grouped<4>
+           : vg == 16 ? k_collapses_to_verts_grouped<16> : k_collapses_to_verts_grouped<8>;
+    CK(launch_kernel(k, dim3(grid_for((u64)nv * vg)), dim3(BLOCK), 0, s, nv, ue.offs, ue.adj,
+        ue.dirs, codes, sel.q2, sel.cand, sel.colq));
     CK_LAUNCH();
   }
   sel.ind = find_indset(m, 0, sel.cand, sel.colq);
   sel.gen_vert = dalloc<u32>(nv, s);
   if (nv) {
-    CK(launch_kernel(k_vertex_dest_grouped, dim3(grid_for((u64)nv * VERT_GROUP)), dim3(BLOCK), 0, s, nv, ue.offs,
-        ue.adj, ue.dirs, voe1, sel.ind, sel.colq, codes, sel.q2, sel.gen_vert));
+    u32 const vg = tuned(TK_VERT_GROUP);
+    auto k = vg == 4 ? k_vertex_dest_grouped<4>
+           : vg == 16 ? k_vertex_dest_grouped<16> : k_vertex_dest_grouped<8>;
+    CK(launch_kernel(k, dim3(grid_for((u64)nv * vg)), dim3(BLOCK), 0, s, nv, ue.offs, ue.adj,
+        ue.dirs, voe1, sel.ind, sel.colq, codes, sel.q2, sel.gen_vert));
     CK_LAUNCH();
   }
   return true;

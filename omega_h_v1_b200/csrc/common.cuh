@@ -109,6 +109,8 @@ __host__ inline double from_order_key(unsigned long long k)
 
 constexpr int BLOCK = 256;
 inline u32 grid_for(u64 n) { return n ? ceil_div(n, BLOCK) : 1; }
+// blocks of `block` threads covering n threads (at least one block)
+inline u32 grid_for(u64 n, u32 block) { return n ? ceil_div(n, block) : 1; }
 
 // ---------------------------------------------------------------------------
 // entity tables (tables.cpp:77-193)

@@ -20,13 +20,16 @@ PassStats& last_pass_stats()
   return s;
 }
 
-// also zeroes the first round's "anything left" flag
+// control words of the single-launch rounds (mailbox slots 44-50)
+constexpr u32 COOP_CTL_SLOT = 44, COOP_CTL_WORDS = 7;
+
+// also zeroes the control words of the rounds
 __global__ void k_indset_init(u32 n, u32 const* __restrict__ filter, u32* __restrict__ st,
-    u32* first_flag)
+    u32* ctl)
 {
   pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i == 0) *first_flag = 0;
+  if (i < COOP_CTL_WORDS) ctl[i] = 0;
   if (i < n) st[i] = filter[i] ? (u32)UNKNOWN : (u32)NOT_IN_SET;
 }
 
@@ -41,140 +44,156 @@ struct Nbrs {
   u32 per;           // entities per via-entity
 };
 
-template <class F>
-__device__ inline bool for_nbrs(Nbrs const& g, u32 i, F&& f)
+// one round of indset_at_vert (indset.cpp:55-84) for entity i: in the set
+// if no neighbour is in the set and no undecided neighbour beats it (higher
+// goodness, or equal goodness and a lower global id), out of it if a
+// neighbour is in the set, undecided otherwise. A group of G lanes (G
+// divides 32, so a group never straddles a warp) walks the entity's upward
+// entries l, l + G, ...; each lane folds its neighbours into two flags and
+// two ballots over the group combine them. The rule depends on the
+// neighbour set only, so the walk order does not matter. (One thread per
+// long row issues loads whose lanes are a row apart and fills the
+// load/store queue.)
+//
+// All rounds run in one launch: a cooperative grid (every block resident)
+// runs the rounds over a grid-stride loop, separated by a grid barrier,
+// until a round leaves no entity undecided or 100 rounds have run. Control words (zeroed by k_indset_init): [0] barrier arrivals,
+// [1] barrier generation, [2..4] "anything left" of rounds r = 0, 1, 2 mod 3
+// (round r zeroes the flag of round r + 1, last read before the barrier of
+// round r - 1 that every block has passed), [5] rounds run, [6] a barrier
+// wait gave up. States are read past L1 (another block wrote them in the
+// previous round). The barrier's wait is bounded: after COOP_SPIN_LIMIT
+// polls it sets [6] and every block leaves.
+constexpr u32 COOP_SPIN_LIMIT = 1u << 24;
+
+__device__ inline bool coop_barrier(u32* ctl)
 {
-  u32 b = g.offs[i], e = g.offs[i + 1];
-  if (g.mode == 0) {
-    for (u32 j = b; j < e; ++j)
-      if (!f(g.down[g.adj[j] * 2 + (1 - g.dirs[j])])) return false;
-  } else {
-    for (u32 j = b; j < e; ++j) {
-      u32 const* ds = g.down + (size_t)g.adj[j] * g.per;
-      for (u32 k = 0; k < g.per; ++k) {
-        u32 o = ds[k];
-        if (o != i && !f(o)) return false;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    u32 const g0 = *(volatile u32*)&ctl[1];
+    __threadfence();
+    if (atomicAdd(&ctl[0], 1u) + 1u == gridDim.x) {
+      *(volatile u32*)&ctl[0] = 0;
+      __threadfence();
+      atomicAdd(&ctl[1], 1u);
+    } else {
+      u32 spins = 0;
+      while (*(volatile u32*)&ctl[1] == g0) {
+        if (++spins > COOP_SPIN_LIMIT) {
+          atomicOr(&ctl[6], 1u);
+          break;
+        }
+        __nanosleep(64);
       }
     }
+    __threadfence();
   }
-  return true;
+  __syncthreads();
+  return *(volatile u32*)&ctl[6] == 0;
 }
 
-// one round of indset_at_vert (indset.cpp:55-84) over all entities
-// unknown_left: this round's flag; next_flag: the next round's, zeroed here
-// (rounds alternate between two mailbox slots, so no memset precedes one)
-__global__ void k_indset_round(u32 n, Nbrs g, u32 const* __restrict__ old_st,
-    u32* __restrict__ st, double const* __restrict__ good,
-    u64 const* __restrict__ glob, u32* unknown_left, u32* next_flag)
-{
-  pdl_wait();
-  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i == 0) *next_flag = 0;
-  if (i >= n) return;
-  u32 s0 = old_st[i];
-  if (s0 != UNKNOWN) {
-    st[i] = s0;
-    return;
-  }
-  bool any_in = !for_nbrs(g, i, [&](u32 o) { return old_st[o] != IN_SET; });
-  if (any_in) {
-    st[i] = NOT_IN_SET;
-    return;
-  }
-  double myg = good[i];
-  u64 myid = glob ? glob[i] : (u64)i;
-  bool win = for_nbrs(g, i, [&](u32 o) {
-    if (old_st[o] == NOT_IN_SET) return true;
-    double og = good[o];
-    u64 oid = glob ? glob[o] : (u64)o;
-    if (myg == og && oid < myid) return false;
-    if (myg < og) return false;
-    return true;
-  });
-  if (win) {
-    st[i] = IN_SET;
-  } else {
-    st[i] = UNKNOWN;
-    *unknown_left = 1;
-  }
-}
-
-// The same round with a group of G lanes per entity (G divides 32, so a
-// group never straddles a warp): lane l of a group walks the entity's
-// upward entries l, l + G, ..., each lane folds its neighbours into two
-// flags, and two ballots over the group give "a neighbour is in the set" and
-// "no neighbour beats me". The rule depends on the neighbour set only, so
-// the walk order does not matter. (One thread per long row issues loads
-// whose lanes are a row apart and fills the load/store queue.)
 template <int G>
-__global__ void k_indset_round_grouped(u32 n, Nbrs g, u32 const* __restrict__ old_st,
-    u32* __restrict__ st, double const* __restrict__ good,
-    u64 const* __restrict__ glob, u32* unknown_left, u32* next_flag)
+__global__ void __launch_bounds__(BLOCK) k_indset_coop(u32 n, Nbrs g, u32* a, u32* b,
+    double const* __restrict__ good, u64 const* __restrict__ glob, u32* ctl)
 {
-  pdl_wait();
-  u32 const t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t == 0) *next_flag = 0;
-  u32 const i = t / G, lg = t % G;
-  if (i >= n) return;  // a group shares i: it leaves together
+  u32 const lg = threadIdx.x % G;
   u32 const gbase = (threadIdx.x & 31) & ~(u32)(G - 1);
   u32 const gmask = (G == 32 ? 0xffffffffu : ((1u << G) - 1u)) << gbase;
-  u32 const s0 = old_st[i];
-  if (s0 != UNKNOWN) {
-    if (lg == 0) st[i] = s0;
-    return;
-  }
-  u32 const b = g.offs[i], e = g.offs[i + 1];
-  double const myg = good[i];
-  u64 const myid = glob ? glob[i] : (u64)i;
-  bool in_set = false, beaten = false;
-  auto visit = [&](u32 o) {
-    u32 so = old_st[o];
-    if (so == IN_SET) in_set = true;
-    if (so == NOT_IN_SET) return;
-    double og = good[o];
-    u64 oid = glob ? glob[o] : (u64)o;
-    if ((myg == og && oid < myid) || myg < og) beaten = true;
-  };
-  for (u32 j = b + lg; j < e; j += G) {
-    if (g.mode == 0) {
-      visit(g.down[g.adj[j] * 2 + (1 - g.dirs[j])]);
-    } else {
-      u32 const* ds = g.down + (size_t)g.adj[j] * g.per;
-      for (u32 k = 0; k < g.per; ++k)
-        if (ds[k] != i) visit(ds[k]);
+  u32 const stride = gridDim.x * blockDim.x;
+  for (u32 r = 0; r < MAX_INDSET_ROUNDS; ++r) {
+    u32 const* old_st = (r % 2 == 0) ? a : b;
+    u32* st = (r % 2 == 0) ? b : a;
+    if (blockIdx.x == 0 && threadIdx.x == 0) ctl[2 + (r + 1) % 3] = 0;
+    bool left = false;
+    for (u64 t = (u64)blockIdx.x * blockDim.x + threadIdx.x; t < (u64)n * G; t += stride) {
+      u32 const i = (u32)(t / G);
+      u32 const s0 = __ldcg(&old_st[i]);
+      if (s0 != UNKNOWN) {
+        if (lg == 0) st[i] = s0;
+        continue;
+      }
+      u32 const rb = g.offs[i], re = g.offs[i + 1];
+      double const myg = good[i];
+      u64 const myid = glob ? glob[i] : (u64)i;
+      bool in_set = false, beaten = false;
+      auto visit = [&](u32 o) {
+        u32 so = __ldcg(&old_st[o]);
+        if (so == IN_SET) in_set = true;
+        if (so == NOT_IN_SET) return;
+        double og = good[o];
+        u64 oid = glob ? glob[o] : (u64)o;
+        if ((myg == og && oid < myid) || myg < og) beaten = true;
+      };
+      for (u32 j = rb + lg; j < re; j += G) {
+        if (g.mode == 0) {
+          visit(g.down[g.adj[j] * 2 + (1 - g.dirs[j])]);
+        } else {
+          u32 const* ds = g.down + (size_t)g.adj[j] * g.per;
+          for (u32 k = 0; k < g.per; ++k)
+            if (ds[k] != i) visit(ds[k]);
+        }
+      }
+      bool const any_in = (__ballot_sync(gmask, in_set) & gmask) != 0;
+      bool const lost = (__ballot_sync(gmask, beaten) & gmask) != 0;
+      if (lg == 0) {
+        if (any_in) {
+          st[i] = NOT_IN_SET;
+        } else if (!lost) {
+          st[i] = IN_SET;
+        } else {
+          st[i] = UNKNOWN;
+          left = true;
+        }
+      }
+    }
+    if (__syncthreads_or(left) && threadIdx.x == 0) atomicOr(&ctl[2 + r % 3], 1u);
+    __threadfence();
+    if (!coop_barrier(ctl)) return;
+    if (*(volatile u32*)&ctl[2 + r % 3] == 0) {
+      if (blockIdx.x == 0 && threadIdx.x == 0) ctl[5] = r + 1;
+      return;
     }
   }
-  bool const any_in = (__ballot_sync(gmask, in_set) & gmask) != 0;
-  bool const lost = (__ballot_sync(gmask, beaten) & gmask) != 0;
-  if (lg == 0) {
-    if (any_in) {
-      st[i] = NOT_IN_SET;
-    } else if (!lost) {
-      st[i] = IN_SET;
-    } else {
-      st[i] = UNKNOWN;
-      *unknown_left = 1;
-    }
-  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) ctl[5] = MAX_INDSET_ROUNDS;
 }
 
-static void launch_indset_round(u32 n, Nbrs const& g, double avg_row, u32 const* old_st,
-    u32* st, double const* good, u64 const* glob, u32* flag, u32* next_flag, cudaStream_t s)
+namespace {
+// resident blocks of BLOCK threads a cooperative launch may use on this device
+template <int G>
+u32 coop_blocks()
 {
-  // lanes per entity from the mean upward row length: vertex rows (about
-  // 13.5 edges) take 8, edge rows in 3D (about 5 tets) 4, 2D rows 2
-  if (avg_row >= 8.0) {
-    CK(launch_kernel(k_indset_round_grouped<8>, dim3(grid_for((u64)n * 8)), dim3(BLOCK), 0, s, n, g, old_st, st, good,
-        glob, flag, next_flag));
-  } else if (avg_row >= 3.0) {
-    CK(launch_kernel(k_indset_round_grouped<4>, dim3(grid_for((u64)n * 4)), dim3(BLOCK), 0, s, n, g, old_st, st, good,
-        glob, flag, next_flag));
-  } else {
-    CK(launch_kernel(k_indset_round_grouped<2>, dim3(grid_for((u64)n * 2)), dim3(BLOCK), 0, s, n, g, old_st, st, good,
-        glob, flag, next_flag));
+  static u32 cached[64] = {};
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return 0;
+  if (!cached[dev]) {
+    int per_sm = 0, sms = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_indset_coop<G>, BLOCK, 0));
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    cached[dev] = (u32)(per_sm * sms);
   }
+  return cached[dev];
+}
+
+template <int G>
+void launch_coop(u32 n, Nbrs const& g, u32* a, u32* b, double const* good, u64 const* glob,
+    u32* ctl, cudaStream_t s)
+{
+  u32 blocks = std::min<u32>(grid_for((u64)n * G), coop_blocks<G>());
+  if (!blocks) throw Failure(E_CUDA, "independent set: no resident blocks");
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(blocks);
+  cfg.blockDim = dim3(BLOCK);
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  CK(cudaLaunchKernelEx(&cfg, k_indset_coop<G>, n, g, a, b, good, glob, ctl));
   CK_LAUNCH();
 }
+}  // namespace
 
 // number of upward uses walked per round (edges of vertices / elements of
 // edges), for the probe's byte count
@@ -207,39 +226,39 @@ u32* find_indset(Mesh& m, u32 ent_dim, u32 const* filter, double const* good)
     throw Failure(E_ARG, "independent sets are built on vertices or edges");
   }
   u64 const* glob = (m.parallel && m.globals[ent_dim]) ? m.globals[ent_dim] : nullptr;
-  double via_bytes = ent_dim == 0 ? 8.0 * m.counts[1] : 4.0 * g.per * m.counts[m.dim];
   u32* a = dalloc<u32>(n, m.s);
   u32* b = dalloc<u32>(n, m.s);
-  // the "anything left" flags of even and odd rounds (mailbox slots 0, 40)
-  u32 const flag_slot[2] = {0, 40};
   if (n) {
-    CK(launch_kernel(k_indset_init, dim3(grid_for(n)), dim3(BLOCK), 0, m.s, n, filter, a, m.mb->dev + flag_slot[0]));
+    CK(launch_kernel(k_indset_init, dim3(grid_for(std::max<u32>(n, COOP_CTL_WORDS))),
+        dim3(BLOCK), 0, m.s, n, filter, a, m.mb->dev + COOP_CTL_SLOT));
     CK_LAUNCH();
   }
-  // Rounds are issued in batches and the "anything left" flag is read once
-  // per batch: a round applied to a settled state leaves it unchanged, so
-  // the extra rounds of a batch cannot alter the result, and the total stays
-  // capped at 100 rounds as in the reference.
+  // All rounds run in one cooperative launch; its control words (mailbox
+  // slots COOP_CTL_SLOT..) come back with slots 1-3, which a caller that
+  // left flags there reads after this call without a read-back of its own.
   u32 rounds = 0;
   bool done = (n == 0);
-  while (!done && rounds < MAX_INDSET_ROUNDS) {
-    u32 batch = rounds == 0 ? 3u : 1u;
-    if (rounds + batch > MAX_INDSET_ROUNDS) batch = MAX_INDSET_ROUNDS - rounds;
-    for (u32 r = 0; r < batch; ++r) {
-      // offsets, upward lists, the via-entities' down lists, states,
-      // goodness and (parallel) globals read once; states written once
-      double nuse = (double)read_cached_uses(m, ent_dim);
-      PROBE(P_INDSET_ROUND, m.s, 4.0 * (n + 1.0) + 4.0 * nuse + via_bytes +
-          4.0 * n + 8.0 * n + (glob ? 8.0 * n : 0.0) + 4.0 * n);
-      launch_indset_round(n, g, n ? nuse / n : 0.0, a, b, good, glob,
-          m.mb->dev + flag_slot[rounds % 2], m.mb->dev + flag_slot[(rounds + 1) % 2], m.s);
-      std::swap(a, b);
-      ++rounds;
+  if (!done) {
+    u32* ctl = m.mb->dev + COOP_CTL_SLOT;
+    double nuse = (double)read_cached_uses(m, ent_dim);
+    double avg_row = nuse / n;
+    u32 lanes = avg_row >= 8.0 ? tuned(TK_INDSET_VERT_GROUP)
+              : avg_row >= 3.0 ? tuned(TK_INDSET_EDGE_GROUP) : 2u;
+    if (lanes == 16) launch_coop<16>(n, g, a, b, good, glob, ctl, m.s);
+    else if (lanes == 8) launch_coop<8>(n, g, a, b, good, glob, ctl, m.s);
+    else if (lanes == 4) launch_coop<4>(n, g, a, b, good, glob, ctl, m.s);
+    else launch_coop<2>(n, g, a, b, good, glob, ctl, m.s);
+    m.mb->fetch(m.s, COOP_CTL_SLOT + COOP_CTL_WORDS);
+    u32 const* hc = m.mb->host + COOP_CTL_SLOT;
+    if (hc[6]) {
+      dev_free(a, m.s);
+      dev_free(b, m.s);
+      throw Failure(E_TIMEOUT, "independent set: a grid barrier wait gave up");
     }
-    // slots 1-3 come back too: a caller that left flags there reads them
-    // after this call without a read-back of its own
-    m.mb->fetch(m.s, 41);
-    if (!m.mb->host[flag_slot[(rounds - 1) % 2]]) done = true;
+    rounds = hc[5];
+    done = rounds > 0 && hc[2 + (rounds - 1) % 3] == 0;
+    // round r writes b when r is even: the result is in b after an odd count
+    if (rounds % 2 == 1) std::swap(a, b);
   }
   dev_free(b, m.s);
   last_pass_stats().indset_rounds = rounds;
@@ -270,14 +289,15 @@ void expand_scaled(void const* in, u32 const* offs, u32 k, u32 n, u32 width,
 {
   if (!n || !width || !k) return;
   PROBE(P_EXPAND, s, 4.0 * (n + 1) + 2.0 * (double)n * width * esz * k);
+  u32 const gb = tuned(TK_GATHER_BLOCK);
   if (esz == 1)
-    CK(launch_kernel(k_expand_scaled<unsigned char>, dim3(grid_for(n)), dim3(BLOCK), 0, s, 
+    CK(launch_kernel(k_expand_scaled<unsigned char>, dim3(grid_for(n, gb)), dim3(gb), 0, s,
         (unsigned char const*)in, offs, k, n, width, (unsigned char*)out));
   else if (esz == 4)
-    CK(launch_kernel(k_expand_scaled<u32>, dim3(grid_for(n)), dim3(BLOCK), 0, s, 
+    CK(launch_kernel(k_expand_scaled<u32>, dim3(grid_for(n, gb)), dim3(gb), 0, s,
         (u32 const*)in, offs, k, n, width, (u32*)out));
   else
-    CK(launch_kernel(k_expand_scaled<unsigned long long>, dim3(grid_for(n)), dim3(BLOCK), 0, s, 
+    CK(launch_kernel(k_expand_scaled<unsigned long long>, dim3(grid_for(n, gb)), dim3(gb), 0, s,
         (unsigned long long const*)in, offs, k, n, width, (unsigned long long*)out));
   CK_LAUNCH();
 }
@@ -329,8 +349,9 @@ void expand_many(std::vector<ExpandJob> const& jobs, cudaStream_t s)
           2.0 * (double)pack.j[q].n * pack.j[q].width * pack.j[q].esz * pack.j[q].k;
     }
     PROBE(P_EXPAND, s, bytes);
-    dim3 grid(std::min<u32>(grid_for(nmax), 148u * 16u), cnt);
-    CK(launch_kernel(k_expand_many, dim3(grid), dim3(BLOCK), 0, s, pack));
+    u32 const gb = tuned(TK_GATHER_BLOCK);
+    dim3 grid(std::min<u32>(grid_for(nmax, gb), 148u * 16u * 256u / gb), cnt);
+    CK(launch_kernel(k_expand_many, dim3(grid), dim3(gb), 0, s, pack));
     CK_LAUNCH();
   }
 }

@@ -911,16 +911,12 @@ void Mesh::reflect_range(u32 high, u32 low, u32 first, u32* out)
   double nld = nl, rec = low == 1 ? 8.0 : 16.0;
   PROBE(P_REFLECT_DOWN, s, 4.0 * deg(high, 0) * (nh - first) + 4.0 * (counts[0] + 1.0) +
       rec * nld + 4.0 * n);
-  u32 g = grid_for(nh - first);
-  if (high == 3 && low == 2)
-    CK(launch_kernel(k_reflect_grouped<3, 2>, dim3(g), dim3(BLOCK), 0, s, first, nh, voh, low_row_offs[low],
-        low_rows[low], out));
-  else if (high == 3)
-    CK(launch_kernel(k_reflect_grouped<3, 1>, dim3(g), dim3(BLOCK), 0, s, first, nh, voh, low_row_offs[low],
-        low_rows[low], out));
-  else
-    CK(launch_kernel(k_reflect_grouped<2, 1>, dim3(g), dim3(BLOCK), 0, s, first, nh, voh, low_row_offs[low],
-        low_rows[low], out));
+  u32 const gb = tuned(TK_GATHER_BLOCK);
+  u32 g = grid_for(nh - first, gb);
+  auto k = high == 3 && low == 2 ? k_reflect_grouped<3, 2>
+         : high == 3 ? k_reflect_grouped<3, 1> : k_reflect_grouped<2, 1>;
+  CK(launch_kernel(k, dim3(g), dim3(gb), 0, s, first, nh, voh, low_row_offs[low], low_rows[low],
+      out));
   CK_LAUNCH();
 }
 
@@ -933,15 +929,16 @@ void Mesh::reflect_range(u32 high, u32 low, u32 first, u32* out)
 constexpr u32 CARRY_UNROLL = 4;
 
 template <u32 LPH>
-__global__ void __launch_bounds__(BLOCK) k_carry_down(u32 n, u32 const* __restrict__ same_h,
+__global__ void __launch_bounds__(512) k_carry_down(u32 n, u32 const* __restrict__ same_h,
     u32 const* __restrict__ same_l, u32 const* __restrict__ old_down, u32* __restrict__ out)
 {
   pdl_wait();
-  u32 base = blockIdx.x * (BLOCK * CARRY_UNROLL) + threadIdx.x;
+  u32 const bs = blockDim.x;
+  u32 base = blockIdx.x * (bs * CARRY_UNROLL) + threadIdx.x;
   u32 od[CARRY_UNROLL], ni[CARRY_UNROLL], nn[CARRY_UNROLL];
 #pragma unroll
   for (u32 k = 0; k < CARRY_UNROLL; ++k) {
-    u32 t = base + k * BLOCK;
+    u32 t = base + k * bs;
     od[k] = 0;
     ni[k] = nn[k] = 0;
     if (t < n) {
@@ -953,7 +950,7 @@ __global__ void __launch_bounds__(BLOCK) k_carry_down(u32 n, u32 const* __restri
   }
 #pragma unroll
   for (u32 k = 0; k < CARRY_UNROLL; ++k) {
-    u32 t = base + k * BLOCK;
+    u32 t = base + k * bs;
     if (t < n && nn[k] != ni[k]) out[(size_t)ni[k] * LPH + t % LPH] = same_l[od[k]];
   }
 }
@@ -969,14 +966,11 @@ void carry_down(Mesh& m, Mesh& out, u32 high, u32 low, u32 const* same_h, u32 ns
   u32* dn = dalloc<u32>((size_t)nh * lph, s);
   if (nh_old) {
     u32 n = nh_old * lph;
-    u32 g = (u32)ceil_div((u64)n, (u64)BLOCK * CARRY_UNROLL);
+    u32 const gb = tuned(TK_GATHER_BLOCK);
+    u32 g = (u32)ceil_div((u64)n, (u64)gb * CARRY_UNROLL);
     PROBE(P_CARRY, s, 4.0 * (nh_old + 1) + 12.0 * n);
-    if (lph == 3)
-      CK(launch_kernel(k_carry_down<3>, dim3(g), dim3(BLOCK), 0, s, n, same_h, same_l, m.down[high][low], dn));
-    else if (lph == 4)
-      CK(launch_kernel(k_carry_down<4>, dim3(g), dim3(BLOCK), 0, s, n, same_h, same_l, m.down[high][low], dn));
-    else
-      CK(launch_kernel(k_carry_down<6>, dim3(g), dim3(BLOCK), 0, s, n, same_h, same_l, m.down[high][low], dn));
+    auto k = lph == 3 ? k_carry_down<3> : lph == 4 ? k_carry_down<4> : k_carry_down<6>;
+    CK(launch_kernel(k, dim3(g), dim3(gb), 0, s, n, same_h, same_l, m.down[high][low], dn));
     CK_LAUNCH();
   }
   // the survivors come first; the entities the pass made are searched
@@ -1082,14 +1076,15 @@ __global__ void k_up_surv_fill(u32 nl_old, u32 const* __restrict__ same_l,
 }
 
 // The same two kernels for long rows (vertex rows, 8 or more uses on
-// average): a group of CARRY_GROUP lanes walks one row, each lane one use,
-// so a row's uses are read and written by consecutive lanes; a ballot over
-// the group gives each kept use its place, in the old order. (One thread
-// per long row issues loads whose lanes are a row apart and fills the
-// load/store queue.) Groups never straddle a warp; a group's lanes share
-// their row, so they loop and leave together.
-constexpr u32 CARRY_GROUP = 8;
+// average): a group of CG lanes (the tuning table's carry_group) walks one
+// row, each lane one use, so a row's uses are read and written by
+// consecutive lanes; a ballot over the group gives each kept use its place,
+// in the old order. (One thread per long row issues loads whose lanes are a
+// row apart and fills the load/store queue.) Groups never straddle a warp;
+// a group's lanes share their row, so they loop and leave together.
+constexpr u32 LONG_ROW_USES = 8;
 
+template <u32 CG>
 __global__ void k_up_surv_count_grouped(u32 nl_old, u32 nsame_l, u32 ntail,
     u32 const* __restrict__ same_l, u32 const* __restrict__ newid_h,
     u32 const* __restrict__ offs, u32 const* __restrict__ adj, u32* __restrict__ cnt,
@@ -1097,7 +1092,7 @@ __global__ void k_up_surv_count_grouped(u32 nl_old, u32 nsame_l, u32 ntail,
 {
   pdl_wait();
   u32 const t = blockIdx.x * blockDim.x + threadIdx.x;
-  u32 const j = t / CARRY_GROUP, g = t % CARRY_GROUP;
+  u32 const j = t / CG, g = t % CG;
   if (j >= nl_old) {
     if (g == 0 && j - nl_old < ntail) {
       u32 r = nsame_l + (j - nl_old);
@@ -1108,11 +1103,11 @@ __global__ void k_up_surv_count_grouped(u32 nl_old, u32 nsame_l, u32 ntail,
   }
   u32 const nj = same_l[j];
   if (same_l[j + 1] == nj) return;
-  u32 const gbase = (threadIdx.x & 31) & ~(CARRY_GROUP - 1);
-  u32 const gmask = ((1u << CARRY_GROUP) - 1u) << gbase;
+  u32 const gbase = (threadIdx.x & 31) & ~(CG - 1);
+  u32 const gmask = ((1u << CG) - 1u) << gbase;
   u32 const e = offs[j + 1];
   u32 c = 0;
-  for (u32 base = offs[j]; base < e; base += CARRY_GROUP) {
+  for (u32 base = offs[j]; base < e; base += CG) {
     u32 const u = base + g;
     bool const keep = u < e && newid_h[adj[u]] != INV;
     c += __popc(__ballot_sync(gmask, keep) & gmask);
@@ -1123,6 +1118,7 @@ __global__ void k_up_surv_count_grouped(u32 nl_old, u32 nsame_l, u32 ntail,
   }
 }
 
+template <u32 CG>
 __global__ void k_up_surv_fill_grouped(u32 nl_old, u32 const* __restrict__ same_l,
     u32 const* __restrict__ newid_h, u32 const* __restrict__ offs_old,
     u32 const* __restrict__ adj_old, u32 const* __restrict__ dirs_old,
@@ -1130,16 +1126,16 @@ __global__ void k_up_surv_fill_grouped(u32 nl_old, u32 const* __restrict__ same_
 {
   pdl_wait();
   u32 const t = blockIdx.x * blockDim.x + threadIdx.x;
-  u32 const j = t / CARRY_GROUP, g = t % CARRY_GROUP;
+  u32 const j = t / CG, g = t % CG;
   if (j >= nl_old) return;
   u32 const nj = same_l[j];
   if (same_l[j + 1] == nj) return;
-  u32 const gbase = (threadIdx.x & 31) & ~(CARRY_GROUP - 1);
-  u32 const gmask = ((1u << CARRY_GROUP) - 1u) << gbase;
+  u32 const gbase = (threadIdx.x & 31) & ~(CG - 1);
+  u32 const gmask = ((1u << CG) - 1u) << gbase;
   u32 const below = (1u << g) - 1u;
   u32 w = offs[nj];
   u32 const e = offs_old[j + 1];
-  for (u32 base = offs_old[j]; base < e; base += CARRY_GROUP) {
+  for (u32 base = offs_old[j]; base < e; base += CG) {
     u32 const u = base + g;
     u32 na = INV, d = 0;
     if (u < e) {
@@ -1214,23 +1210,28 @@ void carry_up(Mesh& m, Mesh& out, u32 low, u32 high, u32 const* same_l, u32 nsam
   u32* surv = m.up_sorted[low][high] ? dalloc<u32>((size_t)nl + 1, s) : nullptr;
   u32 nuses_old = m.counts[high] * lph;
   // rows of 8 or more uses on average (vertex rows) take a lane group each
-  bool const long_rows = nl_old && (u64)nuses_old >= (u64)CARRY_GROUP * nl_old;
+  bool const long_rows = nl_old && (u64)nuses_old >= (u64)LONG_ROW_USES * nl_old;
+  u32 const cg = tuned(TK_CARRY_GROUP), gb = tuned(TK_GATHER_BLOCK);
   {
     u32 ntail = nl + 1 - nsame_l;
     // each array once: same_l and the old offsets, the old rows' highs, the
     // highs' new ids, the new counts
     PROBE(P_CARRY_UP, s, 8.0 * (nl_old + 1) + 4.0 * nuses_old + 4.0 * nh_old + 4.0 * nl);
-    if (long_rows)
-      CK(launch_kernel(k_up_surv_count_grouped, dim3(grid_for(((u64)nl_old + ntail) * CARRY_GROUP)), dim3(BLOCK), 0, s, 
+    if (long_rows) {
+      auto kc = cg == 4 ? k_up_surv_count_grouped<4>
+              : cg == 16 ? k_up_surv_count_grouped<16> : k_up_surv_count_grouped<8>;
+      CK(launch_kernel(kc, dim3(grid_for(((u64)nl_old + ntail) * cg, gb)), dim3(gb), 0, s,
           nl_old, nsame_l, ntail, same_l, newid_h, old.offs, old.adj, cnt, surv));
-    else
-      CK(launch_kernel(k_up_surv_count, dim3(grid_for((u64)nl_old + ntail)), dim3(BLOCK), 0, s, nl_old, nsame_l, ntail,
-          same_l, newid_h, old.offs, old.adj, cnt, surv));
+    } else {
+      CK(launch_kernel(k_up_surv_count, dim3(grid_for((u64)nl_old + ntail, gb)), dim3(gb), 0, s,
+          nl_old, nsame_l, ntail, same_l, newid_h, old.offs, old.adj, cnt, surv));
+    }
     CK_LAUNCH();
   }
   if (nuses > first) {
     PROBE(P_UP_COUNT, s, 4.0 * (nuses - first) + 4.0 * nl);
-    CK(launch_kernel(k_up_gen_count, dim3(grid_for(nuses - first)), dim3(BLOCK), 0, s, first, nuses, loh, cnt));
+    CK(launch_kernel(k_up_gen_count, dim3(grid_for(nuses - first, gb)), dim3(gb), 0, s, first,
+        nuses, loh, cnt));
     CK_LAUNCH();
   }
   UpAdj u;
@@ -1243,18 +1244,21 @@ void carry_up(Mesh& m, Mesh& out, u32 low, u32 high, u32 const* same_l, u32 nsam
     // written as highs and directions
     PROBE(P_CARRY_UP, s, 8.0 * (nl_old + 1) + 8.0 * nuses_old + 4.0 * nh_old + 4.0 * (nl + 1) +
         8.0 * first);
-    if (long_rows)
-      CK(launch_kernel(k_up_surv_fill_grouped, dim3(grid_for((u64)nl_old * CARRY_GROUP)), dim3(BLOCK), 0, s, nl_old,
+    if (long_rows) {
+      auto kf = cg == 4 ? k_up_surv_fill_grouped<4>
+              : cg == 16 ? k_up_surv_fill_grouped<16> : k_up_surv_fill_grouped<8>;
+      CK(launch_kernel(kf, dim3(grid_for((u64)nl_old * cg, gb)), dim3(gb), 0, s, nl_old,
           same_l, newid_h, old.offs, old.adj, old.dirs, u.offs, u.adj, u.dirs));
-    else
-      CK(launch_kernel(k_up_surv_fill, dim3(grid_for(nl_old)), dim3(BLOCK), 0, s, nl_old, same_l, newid_h, old.offs,
-          old.adj, old.dirs, u.offs, u.adj, u.dirs));
+    } else {
+      CK(launch_kernel(k_up_surv_fill, dim3(grid_for(nl_old, gb)), dim3(gb), 0, s, nl_old, same_l,
+          newid_h, old.offs, old.adj, old.dirs, u.offs, u.adj, u.dirs));
+    }
     CK_LAUNCH();
   }
   if (nuses > first) {
     PROBE(P_UP_FILL, s, 4.0 * (nuses - first) + 8.0 * nl + 8.0 * (nuses - first));
-    CK(launch_kernel(k_up_gen_fill, dim3(grid_for(nuses - first)), dim3(BLOCK), 0, s, first, nuses, lph, loh, u.offs,
-        cnt, u.adj, u.dirs));
+    CK(launch_kernel(k_up_gen_fill, dim3(grid_for(nuses - first, gb)), dim3(gb), 0, s, first,
+        nuses, lph, loh, u.offs, cnt, u.adj, u.dirs));
     CK_LAUNCH();
   }
   dev_free(cnt, s);
@@ -1523,8 +1527,9 @@ double const* Mesh::qualities()
   CK(cudaMemsetAsync(mk, 0xff, sizeof(unsigned long long), s));
   if (ne) {
     PROBE(P_ELEM_QUALITY, s, 4.0 * deg(dim, 0) * ne + 24.0 * counts[0] + 8.0 * ne);
-    CK(launch_kernel(k_elem_quality, dim3(grid_for(ne)), dim3(BLOCK), 0, s, dim, ne, ask_down(dim, 0), coords(),
-        qual_cache, mk));
+    u32 const qb = tuned(TK_QUALITY_BLOCK);
+    CK(launch_kernel(k_elem_quality, dim3(grid_for(ne, qb)), dim3(qb), 0, s, dim, ne,
+        ask_down(dim, 0), coords(), qual_cache, mk));
     CK_LAUNCH();
   }
   return qual_cache;

@@ -445,7 +445,9 @@ static u32* choose_refinement(Mesh& m, u32* cand, double qual_floor, double** qu
       double nel = m.counts[dim];
       PROBE(P_REFINE_QUALITY, s, 4.0 * (ne + 1) + 8.0 * deg(dim, 1) * nel + 8.0 * ne +
           4.0 * deg(dim, 0) * nel + 24.0 * m.counts[0] + 8.0 * ne + 8.0 * ne);
-      CK(launch_kernel(k_refine_quality, dim3(grid_for(ne)), dim3(BLOCK), 0, s, dim, ne, m.ask_down(1, 0),
+      u32 const qb = tuned(TK_QUALITY_BLOCK);
+      CK(launch_kernel(k_refine_quality, dim3(grid_for(ne, qb)), dim3(qb), 0, s, dim, ne,
+          m.ask_down(1, 0),
           m.ask_down(dim, 0), eo.offs, eo.adj, eo.dirs, m.coords(), qual_floor, m.segview(),
           m.fp32_filter ? fp32_stats_dev() : nullptr, cand, q, any, inverted));
       CK_LAUNCH();

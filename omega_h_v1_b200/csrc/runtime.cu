@@ -1,6 +1,8 @@
 // Device runtime for the adaptation pass: error state, stream-ordered
 // allocation, the decoupled look-back exclusive scan and small array kernels.
 #include <cstdlib>
+#include <dlfcn.h>
+#include <string>
 #include <chrono>
 #include <cstdio>
 #include <cstring>
@@ -12,6 +14,122 @@
 #include "runtime.hpp"
 
 namespace osh {
+
+namespace {
+
+struct TuneSpec {
+  char const* name;
+  u32 def;
+  u32 allowed[4];
+};
+TuneSpec const g_tune_spec[TK_NKEYS] = {
+    {"carry_group", 8, {4, 8, 16, 0}},
+    {"vert_group", 8, {4, 8, 16, 0}},
+    {"indset_vert_group", 8, {4, 8, 16, 0}},
+    {"indset_edge_group", 4, {2, 4, 8, 0}},
+    {"quality_block", 256, {64, 128, 256, 512}},
+    {"gather_block", 256, {128, 256, 512, 0}},
+    {"scan_items", 16, {8, 16, 0, 0}},
+};
+std::atomic<u32> g_tune[TK_NKEYS];
+std::once_flag g_tune_once;
+
+bool tune_allowed(u32 k, u32 v)
+{
+  for (u32 a : g_tune_spec[k].allowed)
+    if (a && a == v) return true;
+  return false;
+}
+
+int tune_find(char const* name)
+{
+  if (!name) return -1;
+  for (u32 k = 0; k < TK_NKEYS; ++k)
+    if (std::strcmp(name, g_tune_spec[k].name) == 0) return (int)k;
+  return -1;
+}
+
+int tune_read_file(char const* path, bool apply)
+{
+  FILE* f = std::fopen(path, "r");
+  if (!f) return E_IO;
+  std::vector<std::pair<u32, u32>> sets;
+  char line[256];
+  int rc = E_OK;
+  while (std::fgets(line, sizeof line, f)) {
+    char* h = std::strchr(line, '#');
+    if (h) *h = 0;
+    char name[64];
+    unsigned v = 0;
+    char extra[8];
+    int got = std::sscanf(line, "%63s %u %7s", name, &v, extra);
+    if (got <= 0) continue;  // blank or comment
+    int k = got == 2 ? tune_find(name) : -1;
+    if (k < 0 || !tune_allowed((u32)k, v)) {
+      rc = E_ARG;
+      break;
+    }
+    sets.emplace_back((u32)k, (u32)v);
+  }
+  std::fclose(f);
+  if (rc == E_OK && apply)
+    for (auto const& kv : sets) g_tune[kv.first].store(kv.second);
+  return rc;
+}
+
+void tune_init()
+{
+  std::call_once(g_tune_once, [] {
+    for (u32 k = 0; k < TK_NKEYS; ++k) g_tune[k].store(g_tune_spec[k].def);
+    char const* env = std::getenv("OSH_B200_TUNING");
+    if (env && *env) {
+      tune_read_file(env, true);
+      return;
+    }
+    Dl_info info;
+    if (dladdr(reinterpret_cast<void*>(&tune_init), &info) && info.dli_fname) {
+      std::string p(info.dli_fname);
+      size_t slash = p.rfind('/');
+      p = (slash == std::string::npos ? std::string(".") : p.substr(0, slash)) + "/tuning.txt";
+      tune_read_file(p.c_str(), true);
+    }
+  });
+}
+
+}  // namespace
+
+u32 tuned(TuneKey k)
+{
+  tune_init();
+  return g_tune[k].load(std::memory_order_relaxed);
+}
+
+char const* tune_name(u32 k) { return k < TK_NKEYS ? g_tune_spec[k].name : nullptr; }
+
+int tune_set(char const* name, u32 value)
+{
+  tune_init();
+  int k = tune_find(name);
+  if (k < 0 || !tune_allowed((u32)k, value)) return E_ARG;
+  g_tune[k].store(value);
+  return E_OK;
+}
+
+int tune_get(char const* name, u32* value)
+{
+  tune_init();
+  int k = tune_find(name);
+  if (k < 0) return E_ARG;
+  if (value) *value = g_tune[k].load();
+  return E_OK;
+}
+
+int tune_load(char const* path)
+{
+  tune_init();
+  if (!path) return E_ARG;
+  return tune_read_file(path, true);
+}
 
 bool pdl_enabled()
 {
@@ -408,8 +526,9 @@ void Mailbox::fetch(cudaStream_t s, u32 nslots)
 // look-back meets a published prefix within a few steps (with 2048-element
 // tiles the chain of look-backs, not bandwidth, set the time)
 constexpr int SCAN_THREADS = 512;
-constexpr int SCAN_ITEMS = 16;
-constexpr int SCAN_TILE = SCAN_THREADS * SCAN_ITEMS;
+// items per thread: the tuning table's scan_items (8 or 16); scratch is
+// sized for the smaller tile, so either fits
+constexpr int SCAN_MIN_TILE = SCAN_THREADS * 8;
 constexpr int SCAN_WARPS = SCAN_THREADS / 32;
 constexpr unsigned long long FLAG_AGG = 1ull << 62;
 constexpr unsigned long long FLAG_PRE = 2ull << 62;
@@ -420,7 +539,7 @@ constexpr u32 SCAN_SPIN_LIMIT = 1u << 24;
 // newid (optional, for 0/1 items): out[i] where item i is 1, INV where 0 --
 // each old entity's new id when the items mark survivors
 
-template <int MODE>
+template <int MODE, int SCAN_ITEMS>
 __global__ void __launch_bounds__(SCAN_THREADS)
 k_exscan(u32 const* __restrict__ in, u32* __restrict__ out, u32 n, u32 ntiles,
     unsigned long long* status, u32* ticket_and_err, u32* total_to, u32* __restrict__ newid,
@@ -430,6 +549,7 @@ k_exscan(u32 const* __restrict__ in, u32* __restrict__ out, u32 n, u32 ntiles,
   __shared__ u32 s_tile;
   __shared__ u32 s_warp[SCAN_WARPS];
   __shared__ u32 s_prefix;
+  constexpr int SCAN_TILE = SCAN_THREADS * SCAN_ITEMS;
   __shared__ u32 s_buf[SCAN_TILE + SCAN_TILE / 32];
   if (threadIdx.x == 0) s_tile = atomicAdd(ticket_and_err, 1u);
   __syncthreads();
@@ -620,12 +740,14 @@ void exscan_u32(u32 const* in, u32* out, u32 n, cudaStream_t s, u32* total_to, u
     CK_LAUNCH();
     return;
   }
-  u32 ntiles = ceil_div(n, SCAN_TILE);
+  u32 const items = tuned(TK_SCAN_ITEMS);
+  u32 ntiles = ceil_div(n, (u64)SCAN_THREADS * items);
   // [ticket, error, done, pad][status per tile], zero on entry
   u32* scratch = stream_scan_scratch(4 + 2 * (size_t)ntiles, s);
   {
     PROBE(P_EXSCAN, s, 4.0 * n + 4.0 * (n + 1));
-    CK(launch_kernel(k_exscan<0>, dim3(ntiles), dim3(SCAN_THREADS), 0, s, in, out, n, ntiles,
+    CK(launch_kernel(items == 8 ? k_exscan<0, 8> : k_exscan<0, 16>, dim3(ntiles),
+        dim3(SCAN_THREADS), 0, s, in, out, n, ntiles,
         reinterpret_cast<unsigned long long*>(scratch + 4), scratch, total_to, newid,
         SCAN_SPIN_LIMIT));
     CK_LAUNCH();
@@ -664,7 +786,7 @@ int selftest_scan_wait(u32 spin_limit)
   // gone by; the block that takes ticket 2 has no tile and returns.
   cudaStream_t s = nullptr;
   CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
-  u32 const n = 2 * SCAN_TILE, ntiles = 2;
+  u32 const n = 2 * SCAN_THREADS * 16, ntiles = 2;
   size_t words = (size_t)(n + 1) * 2 + 4 + 2 * ntiles + 4;  // + alignment room
   u32* buf = nullptr;
   CK(cudaMalloc(&buf, words * sizeof(u32)));
@@ -675,7 +797,7 @@ int selftest_scan_wait(u32 spin_limit)
   CK(cudaMemsetAsync(buf, 0, words * sizeof(u32), s));
   u32 one = 1;
   CK(cudaMemcpyAsync(scratch, &one, sizeof(u32), cudaMemcpyHostToDevice, s));
-  CK(launch_kernel(k_exscan<0>, dim3(ntiles), dim3(SCAN_THREADS), 0, s, in, out, n, ntiles,
+  CK(launch_kernel(k_exscan<0, 16>, dim3(ntiles), dim3(SCAN_THREADS), 0, s, in, out, n, ntiles,
       reinterpret_cast<unsigned long long*>(scratch + 4), scratch, nullptr, nullptr,
       spin_limit));
   CK_LAUNCH();
@@ -689,7 +811,7 @@ int selftest_scan_wait(u32 spin_limit)
 
 size_t exscan_scratch_words(u32 n)
 {
-  return 4 + 2 * (size_t)ceil_div(n ? n : 1, SCAN_TILE);
+  return 4 + 2 * (size_t)ceil_div(n ? n : 1, SCAN_MIN_TILE);
 }
 
 void exscan_u32_scratch(u32 const* in, u32* out, u32 n, u32* scratch, cudaStream_t s)
@@ -701,9 +823,11 @@ void exscan_u32_scratch(u32 const* in, u32* out, u32 n, u32* scratch, cudaStream
     CK_LAUNCH();
     return;
   }
-  u32 ntiles = ceil_div(n, SCAN_TILE);
+  u32 const items = tuned(TK_SCAN_ITEMS);
+  u32 ntiles = ceil_div(n, (u64)SCAN_THREADS * items);
   CK(cudaMemsetAsync(scratch, 0, exscan_scratch_words(n) * sizeof(u32), s));
-  CK(launch_kernel(k_exscan<0>, dim3(ntiles), dim3(SCAN_THREADS), 0, s, in, out, n, ntiles,
+  CK(launch_kernel(items == 8 ? k_exscan<0, 8> : k_exscan<0, 16>, dim3(ntiles),
+      dim3(SCAN_THREADS), 0, s, in, out, n, ntiles,
       reinterpret_cast<unsigned long long*>(scratch + 4), scratch, nullptr, nullptr,
       SCAN_SPIN_LIMIT));
   CK_LAUNCH();
@@ -724,11 +848,13 @@ u32* negate_offsets(u32 const* offs, u32 n, cudaStream_t s, u32* total_to, u32* 
     CK_LAUNCH();
     return o;
   }
-  u32 ntiles = ceil_div(n, SCAN_TILE);
+  u32 const items = tuned(TK_SCAN_ITEMS);
+  u32 ntiles = ceil_div(n, (u64)SCAN_THREADS * items);
   u32* scratch = stream_scan_scratch(4 + 2 * (size_t)ntiles, s);
   {
     PROBE(P_EXSCAN, s, 4.0 * (n + 1) + 4.0 * (n + 1));
-    CK(launch_kernel(k_exscan<1>, dim3(ntiles), dim3(SCAN_THREADS), 0, s, offs, o, n, ntiles,
+    CK(launch_kernel(items == 8 ? k_exscan<1, 8> : k_exscan<1, 16>, dim3(ntiles),
+        dim3(SCAN_THREADS), 0, s, offs, o, n, ntiles,
         reinterpret_cast<unsigned long long*>(scratch + 4), scratch, total_to, newid,
         SCAN_SPIN_LIMIT));
     CK_LAUNCH();

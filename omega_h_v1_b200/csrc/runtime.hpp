@@ -6,6 +6,30 @@
 
 namespace osh {
 
+// Launch shapes chosen by the tuner (omega_h_v1_b200/tune.py, which times
+// each candidate with CUDA events on a mid-size adapt and writes the table).
+// Every key has a default and a set of allowed values; the table is read
+// once, from the file named by OSH_B200_TUNING or else tuning.txt beside
+// the library ("name value" lines, # comments). Any allowed value gives the
+// same meshes: only the launch shapes change.
+enum TuneKey : u32 {
+  TK_CARRY_GROUP = 0,    // lanes per long carried upward row: 4, 8, 16
+  TK_VERT_GROUP,         // lanes per vertex row, coarsening vertex kernels: 4, 8, 16
+  TK_INDSET_VERT_GROUP,  // lanes per vertex, independent-set rounds: 4, 8, 16
+  TK_INDSET_EDGE_GROUP,  // lanes per edge (3D), independent-set rounds: 2, 4, 8
+  TK_QUALITY_BLOCK,      // threads per block, quality kernels: 64, 128, 256, 512
+  TK_GATHER_BLOCK,       // threads per block, carry / search / copy kernels: 128, 256, 512
+  TK_SCAN_ITEMS,         // items per thread of a 512-thread scan tile: 8, 16
+  TK_NKEYS
+};
+u32 tuned(TuneKey k);
+char const* tune_name(u32 k);
+// 0, or E_ARG for an unknown name or a value the key does not allow
+int tune_set(char const* name, u32 value);
+int tune_get(char const* name, u32* value);
+// reads a table file; 0, E_IO (unreadable) or E_ARG (a bad line: nothing set)
+int tune_load(char const* path);
+
 // thread-local error state behind osh_b200_last_error()
 void set_error(int code, char const* msg);
 int last_error();
@@ -127,7 +151,8 @@ void* pinned_scratch();
 // small pinned host mailbox for reading several device scalars at once.
 // Slots, by the step that writes them (steps of one mesh run one at a time,
 // so steps that never overlap share slots):
-//   0, 40   independent-set rounds' "anything left" flags (even, odd rounds)
+//   44-50   independent-set rounds: grid barrier, "anything left" flags,
+//           rounds run, barrier error (one launch runs every round)
 //   1-3     refinement: any good candidate, any inverted child, any candidate
 //   4-7     coarsening selection: any collapse kept (4), codes flag (5, not
 //           read), listed candidates (7); swap selection: interior

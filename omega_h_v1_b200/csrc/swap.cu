@@ -493,7 +493,8 @@ static bool swap_select(Mesh& m, double gq, u32 nlayers, SwapSel& sel, u32* sliv
   double const* eq = m.qualities();
   PROBE(P_SWAP_QUALITY, s, 4.0 * (ne + 1) + 8.0 * 6.0 * m.counts[3] + 8.0 * ne +
       16.0 * m.counts[3] + 24.0 * m.counts[0] + 8.0 * m.counts[3] + 4.0 * ne + 16.0 * ne);
-  CK(launch_kernel(k_swap_quality, dim3(ceil_div(ne, 128)), dim3(128), 0, s, ne, te.offs, te.adj, te.dirs, m.ask_down(1, 0),
+  u32 const qb = std::min<u32>(tuned(TK_QUALITY_BLOCK), 128u);
+  CK(launch_kernel(k_swap_quality, dim3(grid_for(ne, qb)), dim3(qb), 0, s, ne, te.offs, te.adj, te.dirs, m.ask_down(1, 0),
       m.ask_down(3, 0), m.coords(), eq, m.fp32_filter ? fp32_stats_dev() : nullptr, sel.cand,
       sel.quals, sel.rs, sel.codes, any));
   CK_LAUNCH();

@@ -84,6 +84,20 @@ def place_jobs(jobs, nbins):
     return [sorted(b) for b in bins]
 
 
+def route_stream(jobs, nbins):
+    """Jobs of an arrival stream routed to nbins GPUs as they arrive: each
+    job, in arrival order, to the GPU that has been given the least estimated
+    output tets so far (ties by the lower GPU). Returns one list of job
+    positions per GPU, in arrival order."""
+    load = [0.0] * nbins
+    bins = [[] for _ in range(nbins)]
+    for i in sorted(range(len(jobs)), key=lambda k: (jobs[k].arrival, k)):
+        b = min(range(nbins), key=lambda k: (load[k], k))
+        bins[b].append(i)
+        load[b] += jobs[i].estimated_output_tets()
+    return bins
+
+
 def batched_boxes(count=512, seed=1, nmin=4, nmax=40):
     rng = SplitMix64(seed)
     out = []

@@ -60,3 +60,16 @@ def test_front_field_zero_level():
     left = W.front_field(on - [0.05, 0.0, 0.0], offset)
     right = W.front_field(on + [0.05, 0.0, 0.0], offset)
     assert np.all(left < -0.9) and np.all(right > 0.9)
+
+
+def test_serving_routing_assigns_every_job_once_in_arrival_order():
+    from omega_h_v1_b200 import workloads as W
+    jobs = W.serving_stream(200, seed=2, rate=200.0)
+    for nb in (1, 2, 4, 8):
+        bins = W.route_stream(jobs, nb)
+        assert sorted(i for b in bins for i in b) == list(range(len(jobs)))
+        for b in bins:
+            assert [jobs[i].arrival for i in b] == sorted(jobs[i].arrival for i in b)
+        loads = [sum(jobs[i].estimated_output_tets() for i in b) for b in bins]
+        biggest = max(j.estimated_output_tets() for j in jobs)
+        assert max(loads) - min(loads) <= biggest
