@@ -798,7 +798,14 @@ static void coarsen_build(Mesh& m, CoarsenSel const& sel)
   u32* gen_offs_v = exscan_new(sel.ind, nv, s);
   // the surviving vertices' count lands in mailbox slot 22, read back with
   // the other dimensions' counts
-  u32* same_v = negate_offsets(gen_offs_v, nv, s, m.mb->dev + 22);
+  u32* same_v = dalloc<u32>((size_t)nv + 1, s);
+  // the scans below are independent of one another and of the collapse
+  // kernels after them: they run together in one launch after the loop
+  ScanJob sj[7];
+  u32 nsj = 0;
+  sj[nsj++] = ScanJob{gen_offs_v, same_v, m.mb->dev + 22, nullptr, nv, 1};
+  u32* scan_in[6] = {};
+  u32 nscan_in = 0;
   u32* fused[4] = {nullptr, nullptr, nullptr, nullptr};
   u32* same_of[4] = {nullptr, nullptr, nullptr, nullptr};
   u32 nsame_of[4] = {0, 0, 0, 0};
@@ -831,12 +838,16 @@ static void coarsen_build(Mesh& m, CoarsenSel const& sel)
           sel.gen_vert, fused[ed], is_same, fused[ed - 1], will_gen, gvert_of[ed], gdir_of[ed]));
       CK_LAUNCH();
     }
-    gen_offs_of[ed] = exscan_new(will_gen, n, s, m.mb->dev + 16 + 2 * (ed - 1));
+    gen_offs_of[ed] = dalloc<u32>((size_t)n + 1, s);
+    sj[nsj++] = ScanJob{will_gen, gen_offs_of[ed], m.mb->dev + 16 + 2 * (ed - 1), nullptr, n, 0};
     if (carried_high(m, ed)) newid_of[ed] = dalloc<u32>(n ? n : 1, s);
-    same_of[ed] = exscan_new(is_same, n, s, m.mb->dev + 17 + 2 * (ed - 1), newid_of[ed]);
-    dev_free(will_gen, s);
-    dev_free(is_same, s);
+    same_of[ed] = dalloc<u32>((size_t)n + 1, s);
+    sj[nsj++] = ScanJob{is_same, same_of[ed], m.mb->dev + 17 + 2 * (ed - 1), newid_of[ed], n, 0};
+    scan_in[nscan_in++] = will_gen;
+    scan_in[nscan_in++] = is_same;
   }
+  exscan_jobs(sj, nsj, s);
+  for (u32 k = 0; k < nscan_in; ++k) dev_free(scan_in[k], s);
   m.mb->fetch(s, 23);
   u32 nv_out = m.mb->host[22];
   last_pass_stats().nselected = nv - nv_out;
@@ -912,13 +923,8 @@ static void coarsen_build(Mesh& m, CoarsenSel const& sel)
     for (u32 l = 1; l < h; ++l)
       if (same_of[h] && same_of[l])
         carry_down(m, *out, h, l, same_of[h], nsame_of[h], same_of[l]);
-  for (u32 h = 1; h <= dim; ++h) {
-    u32* newid = newid_of[h];
-    for (u32 l = 0; l < h; ++l)
-      if (same_of[h] && same_of[l])
-        carry_up(m, *out, l, h, same_of[l], nsame_of[l], same_of[h], nsame_of[h], &newid);
-    dev_free(newid, s);
-  }
+  carry_up_all(m, *out, same_of, nsame_of, newid_of);
+  for (u32 h = 0; h <= dim; ++h) dev_free(newid_of[h], s);
   for (u32 d = 0; d < 4; ++d) {
     dev_free(fused[d], s);
     dev_free(same_of[d], s);

@@ -349,8 +349,10 @@ void expand_many(std::vector<ExpandJob> const& jobs, cudaStream_t s)
           2.0 * (double)pack.j[q].n * pack.j[q].width * pack.j[q].esz * pack.j[q].k;
     }
     PROBE(P_EXPAND, s, bytes);
+    // a thread per row: a grid-stride loop over several rows per thread
+    // chains their dependent loads (offsets, then the row) one after another
     u32 const gb = tuned(TK_GATHER_BLOCK);
-    dim3 grid(std::min<u32>(grid_for(nmax, gb), 148u * 16u * 256u / gb), cnt);
+    dim3 grid(grid_for(nmax, gb), cnt);
     CK(launch_kernel(k_expand_many, dim3(grid), dim3(gb), 0, s, pack));
     CK_LAUNCH();
   }

@@ -1177,99 +1177,152 @@ u32* carry_new_ids(u32 const* same, u32 n, cudaStream_t s)
   return newid;
 }
 
-void carry_up(Mesh& m, Mesh& out, u32 low, u32 high, u32 const* same_l, u32 nsame_l,
-    u32 const* same_h, u32 nsame_h, u32** newid_cache)
+namespace {
+
+// one carried upward adjacency between its count and its fill (the counts
+// of every carried pair are scanned together in one launch)
+struct UpCarry {
+  u32 low = 0, high = 0;
+  u32 nl_old = 0, nl = 0, nsame_l = 0, nh_old = 0, nuses = 0, nuses_old = 0, first = 0, lph = 0;
+  bool long_rows = false;
+  u32 const* same_l = nullptr;
+  u32 const* newid_h = nullptr;
+  u32 const* loh = nullptr;
+  u32* cnt = nullptr;
+  u32* surv = nullptr;
+  UpAdj u;
+};
+
+// everything up to the counts: false when the pair is not carried
+bool carry_up_count(Mesh& m, Mesh& out, u32 low, u32 high, u32 const* same_l, u32 nsame_l,
+    u32 nsame_h, u32 const* newid_h, UpCarry& c)
 {
-  if (!m.have_up[low][high] || out.have_up[low][high]) return;
-  if (!out.has_dim(high) || !out.has_dim(low)) return;
-  if (low > 0 && !out.down[high][low]) return;  // its search is not worth it here
+  if (!m.have_up[low][high] || out.have_up[low][high]) return false;
+  if (!out.has_dim(high) || !out.has_dim(low)) return false;
+  if (low > 0 && !out.down[high][low]) return false;  // its search is not worth it here
   cudaStream_t s = out.s;
-  u32 nl_old = m.counts[low], nl = out.count(low), nh = out.count(high);
-  if (nsame_l > nl || nsame_l > nl_old) throw Failure(E_ARG, "carry_up: survivor count");
-  u32 lph = deg(high, low), nuses = nh * lph, first = nsame_h * lph;
-  u32 const* loh = out.ask_down(high, low);
+  c.low = low;
+  c.high = high;
+  c.nl_old = m.counts[low];
+  c.nl = out.count(low);
+  u32 nh = out.count(high);
+  if (nsame_l > c.nl || nsame_l > c.nl_old) throw Failure(E_ARG, "carry_up: survivor count");
+  c.nsame_l = nsame_l;
+  c.same_l = same_l;
+  c.newid_h = newid_h;
+  c.lph = deg(high, low);
+  c.nuses = nh * c.lph;
+  c.first = nsame_h * c.lph;
+  c.loh = out.ask_down(high, low);
   UpAdj const& old = m.up[low][high];
-  u32 nh_old = m.counts[high];
-  // each old high entity's new id (INV when it did not survive), shared by
-  // the carries of one high dimension through *newid_cache
-  u32* own_newid = nullptr;
-  u32 const* newid_h;
-  if (newid_cache && *newid_cache) {
-    newid_h = *newid_cache;
-  } else {
-    own_newid = carry_new_ids(same_h, nh_old, s);
-    newid_h = own_newid;
-    if (newid_cache) {
-      *newid_cache = own_newid;
-      own_newid = nullptr;
-    }
-  }
+  c.nh_old = m.counts[high];
   // cnt: kept + generated uses per new row; surv (kept only when the old
   // rows were sorted): each row's count of leading uses, in order
-  u32* cnt = dalloc<u32>((size_t)nl + 1, s);
-  u32* surv = m.up_sorted[low][high] ? dalloc<u32>((size_t)nl + 1, s) : nullptr;
-  u32 nuses_old = m.counts[high] * lph;
+  c.cnt = dalloc<u32>((size_t)c.nl + 1, s);
+  c.surv = m.up_sorted[low][high] ? dalloc<u32>((size_t)c.nl + 1, s) : nullptr;
+  c.nuses_old = m.counts[high] * c.lph;
   // rows of 8 or more uses on average (vertex rows) take a lane group each
-  bool const long_rows = nl_old && (u64)nuses_old >= (u64)LONG_ROW_USES * nl_old;
+  c.long_rows = c.nl_old && (u64)c.nuses_old >= (u64)LONG_ROW_USES * c.nl_old;
   u32 const cg = tuned(TK_CARRY_GROUP), gb = tuned(TK_GATHER_BLOCK);
   {
-    u32 ntail = nl + 1 - nsame_l;
+    u32 ntail = c.nl + 1 - nsame_l;
     // each array once: same_l and the old offsets, the old rows' highs, the
     // highs' new ids, the new counts
-    PROBE(P_CARRY_UP, s, 8.0 * (nl_old + 1) + 4.0 * nuses_old + 4.0 * nh_old + 4.0 * nl);
-    if (long_rows) {
+    PROBE(P_CARRY_UP, s, 8.0 * (c.nl_old + 1) + 4.0 * c.nuses_old + 4.0 * c.nh_old +
+        4.0 * c.nl);
+    if (c.long_rows) {
       auto kc = cg == 4 ? k_up_surv_count_grouped<4>
               : cg == 16 ? k_up_surv_count_grouped<16> : k_up_surv_count_grouped<8>;
-      CK(launch_kernel(kc, dim3(grid_for(((u64)nl_old + ntail) * cg, gb)), dim3(gb), 0, s,
-          nl_old, nsame_l, ntail, same_l, newid_h, old.offs, old.adj, cnt, surv));
+      CK(launch_kernel(kc, dim3(grid_for(((u64)c.nl_old + ntail) * cg, gb)), dim3(gb), 0, s,
+          c.nl_old, nsame_l, ntail, same_l, newid_h, old.offs, old.adj, c.cnt, c.surv));
     } else {
-      CK(launch_kernel(k_up_surv_count, dim3(grid_for((u64)nl_old + ntail, gb)), dim3(gb), 0, s,
-          nl_old, nsame_l, ntail, same_l, newid_h, old.offs, old.adj, cnt, surv));
+      CK(launch_kernel(k_up_surv_count, dim3(grid_for((u64)c.nl_old + ntail, gb)), dim3(gb), 0,
+          s, c.nl_old, nsame_l, ntail, same_l, newid_h, old.offs, old.adj, c.cnt, c.surv));
     }
     CK_LAUNCH();
   }
-  if (nuses > first) {
-    PROBE(P_UP_COUNT, s, 4.0 * (nuses - first) + 4.0 * nl);
-    CK(launch_kernel(k_up_gen_count, dim3(grid_for(nuses - first, gb)), dim3(gb), 0, s, first,
-        nuses, loh, cnt));
+  if (c.nuses > c.first) {
+    PROBE(P_UP_COUNT, s, 4.0 * (c.nuses - c.first) + 4.0 * c.nl);
+    CK(launch_kernel(k_up_gen_count, dim3(grid_for(c.nuses - c.first, gb)), dim3(gb), 0, s,
+        c.first, c.nuses, c.loh, c.cnt));
     CK_LAUNCH();
   }
-  UpAdj u;
-  u.offs = exscan_new(cnt, nl, s);
-  u.adj = dalloc<u32>(nuses, s);
-  u.dirs = dalloc<u32>(nuses, s);
-  if (nl_old) {
+  c.u.offs = dalloc<u32>((size_t)c.nl + 1, s);
+  return true;
+}
+
+// after the scan of the counts: the rows' fill, and the adjacency installed
+void carry_up_fill(Mesh& m, Mesh& out, UpCarry& c)
+{
+  cudaStream_t s = out.s;
+  UpAdj const& old = m.up[c.low][c.high];
+  UpAdj& u = c.u;
+  u.adj = dalloc<u32>(c.nuses, s);
+  u.dirs = dalloc<u32>(c.nuses, s);
+  u32 const cg = tuned(TK_CARRY_GROUP), gb = tuned(TK_GATHER_BLOCK);
+  if (c.nl_old) {
     // each array once: same_l and the old offsets, the old rows' highs and
     // directions, the highs' new ids, the new offsets, the kept uses (first)
     // written as highs and directions
-    PROBE(P_CARRY_UP, s, 8.0 * (nl_old + 1) + 8.0 * nuses_old + 4.0 * nh_old + 4.0 * (nl + 1) +
-        8.0 * first);
-    if (long_rows) {
+    PROBE(P_CARRY_UP, s, 8.0 * (c.nl_old + 1) + 8.0 * c.nuses_old + 4.0 * c.nh_old +
+        4.0 * (c.nl + 1) + 8.0 * c.first);
+    if (c.long_rows) {
       auto kf = cg == 4 ? k_up_surv_fill_grouped<4>
               : cg == 16 ? k_up_surv_fill_grouped<16> : k_up_surv_fill_grouped<8>;
-      CK(launch_kernel(kf, dim3(grid_for((u64)nl_old * cg, gb)), dim3(gb), 0, s, nl_old,
-          same_l, newid_h, old.offs, old.adj, old.dirs, u.offs, u.adj, u.dirs));
+      CK(launch_kernel(kf, dim3(grid_for((u64)c.nl_old * cg, gb)), dim3(gb), 0, s, c.nl_old,
+          c.same_l, c.newid_h, old.offs, old.adj, old.dirs, u.offs, u.adj, u.dirs));
     } else {
-      CK(launch_kernel(k_up_surv_fill, dim3(grid_for(nl_old, gb)), dim3(gb), 0, s, nl_old, same_l,
-          newid_h, old.offs, old.adj, old.dirs, u.offs, u.adj, u.dirs));
+      CK(launch_kernel(k_up_surv_fill, dim3(grid_for(c.nl_old, gb)), dim3(gb), 0, s, c.nl_old,
+          c.same_l, c.newid_h, old.offs, old.adj, old.dirs, u.offs, u.adj, u.dirs));
     }
     CK_LAUNCH();
   }
-  if (nuses > first) {
-    PROBE(P_UP_FILL, s, 4.0 * (nuses - first) + 8.0 * nl + 8.0 * (nuses - first));
-    CK(launch_kernel(k_up_gen_fill, dim3(grid_for(nuses - first, gb)), dim3(gb), 0, s, first,
-        nuses, lph, loh, u.offs, cnt, u.adj, u.dirs));
+  if (c.nuses > c.first) {
+    PROBE(P_UP_FILL, s, 4.0 * (c.nuses - c.first) + 8.0 * c.nl + 8.0 * (c.nuses - c.first));
+    CK(launch_kernel(k_up_gen_fill, dim3(grid_for(c.nuses - c.first, gb)), dim3(gb), 0, s,
+        c.first, c.nuses, c.lph, c.loh, u.offs, c.cnt, u.adj, u.dirs));
     CK_LAUNCH();
   }
-  dev_free(cnt, s);
-  dev_free(own_newid, s);
-  if (surv) {
-    u.pre = surv;
-    u.npre = first;
+  dev_free(c.cnt, s);
+  if (c.surv) {
+    u.pre = c.surv;
+    u.npre = c.first;
   }
-  out.up[low][high] = u;
-  out.have_up[low][high] = true;
-  out.up_sorted[low][high] = false;
+  out.up[c.low][c.high] = u;
+  out.have_up[c.low][c.high] = true;
+  out.up_sorted[c.low][c.high] = false;
+}
+
+}  // namespace
+
+void carry_up_all(Mesh& m, Mesh& out, u32* const* same_of, u32 const* nsame_of,
+    u32* const* newid_of)
+{
+  cudaStream_t s = out.s;
+  UpCarry cs[6];
+  u32 nc = 0;
+  // each old high entity's new id (INV when it did not survive): from the
+  // survivors' scan where it wrote them, else computed here, once per
+  // high dimension
+  u32* own_newid[4] = {nullptr, nullptr, nullptr, nullptr};
+  for (u32 h = 1; h <= m.dim; ++h)
+    for (u32 l = 0; l < h; ++l) {
+      if (!same_of[h] || !same_of[l]) continue;
+      if (!m.have_up[l][h] || out.have_up[l][h]) continue;
+      u32 const* newid_h = newid_of[h];
+      if (!newid_h) {
+        if (!own_newid[h]) own_newid[h] = carry_new_ids(same_of[h], m.counts[h], s);
+        newid_h = own_newid[h];
+      }
+      if (carry_up_count(m, out, l, h, same_of[l], nsame_of[l], nsame_of[h], newid_h, cs[nc]))
+        ++nc;
+    }
+  ScanJob jobs[6];
+  for (u32 k = 0; k < nc; ++k) jobs[k] = ScanJob{cs[k].cnt, cs[k].u.offs, nullptr, nullptr,
+      cs[k].nl, 0};
+  exscan_jobs(jobs, nc, s);
+  for (u32 k = 0; k < nc; ++k) carry_up_fill(m, out, cs[k]);
+  for (u32 h = 0; h < 4; ++h) dev_free(own_newid[h], s);
 }
 
 u32 const* Mesh::ask_down(u32 high, u32 low)

@@ -193,15 +193,16 @@ struct Mesh {
 void carry_down(Mesh& m, Mesh& out, u32 high, u32 low, u32 const* same_h, u32 nsame,
     u32 const* same_l);
 
-// up(low, high) of `out` when m has it: surviving lows keep their old rows'
-// uses by surviving highs (mapped, in order), then the uses of the entities
-// the pass made are added; rows come out unsorted
-// (same_l / same_h: survivor offsets of m's lows / highs, nsame_l / nsame_h
-// survivors, numbered first in out)
-// newid_cache (optional): holds the high dimension's new-id array between
-// the carries of one high dimension (computed on first use; caller frees)
-void carry_up(Mesh& m, Mesh& out, u32 low, u32 high, u32 const* same_l, u32 nsame_l,
-    u32 const* same_h, u32 nsame_h, u32** newid_cache = nullptr);
+// up(low, high) of `out` for every pair m has: surviving lows keep their
+// old rows' uses by surviving highs (mapped, in order), then the uses of the
+// entities the pass made are added; rows come out unsorted. Every pair's
+// counts are scanned together in one launch.
+// (same_of[d]: survivor offsets of m's entities of dimension d, nullptr
+// for a dimension the pass does not keep; nsame_of[d] survivors, numbered
+// first in out; newid_of[d] (optional): each old entity's new id, INV for
+// the ones that do not survive)
+void carry_up_all(Mesh& m, Mesh& out, u32* const* same_of, u32 const* nsame_of,
+    u32* const* newid_of);
 // new id of every old entity, or INV where it did not survive (caller frees)
 u32* carry_new_ids(u32 const* same, u32 n, cudaStream_t s);
 // whether a pass over m carries some upward adjacency of dimension `high`

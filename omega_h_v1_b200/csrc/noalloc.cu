@@ -187,9 +187,7 @@ extern "C" int osh_b200_up_from_down_noalloc(unsigned high_dim, unsigned low_dim
       CK(launch_kernel(k_na_count, dim3(grid_for(n)), dim3(BLOCK), 0, s, lows_of_highs, n, nlows, cnt, status));
       CK_LAUNCH();
     }
-    // clears its own scratch (word 1 of which records a wait that gave up);
-    // with no rows it launches no scan, so the word is cleared here
-    if (!nlows) CK(cudaMemsetAsync(scan, 0, 4 * sizeof(u32), s));
+    // clears its own scratch (word 1 of which records a wait that gave up)
     exscan_u32_scratch(cnt, offsets, nlows, scan, s);
     if (n) {
       CK(launch_kernel(k_na_fill, dim3(grid_for(n)), dim3(BLOCK), 0, s, lows_of_highs, n, nlows, offsets, cnt, rows,

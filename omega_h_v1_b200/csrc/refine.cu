@@ -290,21 +290,27 @@ static u32 refine_build(Mesh& m, u32 const* gen_offs)
   u32* zero_v = dalloc<u32>((size_t)nv + 1, s);
   fill_u32(zero_v, nv + 1, 0, s);
   sp[0].offs = zero_v;
+  u32* will[4] = {nullptr, nullptr, nullptr, nullptr};
+  ScanJob jobs[4];
+  u32 njobs = 0;
   for (u32 dd = 1; dd <= dim; ++dd) {
     if (!m.has_dim(dd)) continue;
     u32 nd = m.count(dd);
     u32 const* sod = dd == 1 ? nullptr : m.ask_down(dd, 1);
-    u32* will = dalloc<u32>(nd, s);
+    will[dd] = dalloc<u32>(nd, s);
     sp[dd].dir = dalloc<u32>(nd, s);
     sp[dd].vert = dalloc<u32>(nd, s);
     if (nd) {
-      CK(launch_kernel(k_split_to_domain, dim3(grid_for(nd)), dim3(BLOCK), 0, s, nd, deg(dd, 1), sod, gen_offs, nv,
-          will, sp[dd].dir, sp[dd].vert));
+      CK(launch_kernel(k_split_to_domain, dim3(grid_for(nd)), dim3(BLOCK), 0, s, nd,
+          deg(dd, 1), sod, gen_offs, nv, will[dd], sp[dd].dir, sp[dd].vert));
       CK_LAUNCH();
     }
-    sp[dd].offs = exscan_new(will, nd, s, m.mb->dev + 8 + dd);
-    dev_free(will, s);
+    sp[dd].offs = dalloc<u32>((size_t)nd + 1, s);
+    jobs[njobs++] = ScanJob{will[dd], sp[dd].offs, m.mb->dev + 8 + dd, nullptr, nd, 0};
   }
+  // the domains' scans in one launch
+  exscan_jobs(jobs, njobs, s);
+  for (u32 dd = 1; dd <= dim; ++dd) dev_free(will[dd], s);
   m.mb->fetch(s, 16);
   for (u32 dd = 1; dd <= dim; ++dd)
     if (m.has_dim(dd)) sp[dd].nsplit = m.mb->host[8 + dd];
@@ -339,12 +345,24 @@ static u32 refine_build(Mesh& m, u32 const* gen_offs)
   // each kept entity's new id, written by the survivors' scan for the
   // dimensions whose upward adjacency is carried
   u32* newid_of[4] = {nullptr, nullptr, nullptr, nullptr};
+  // the survivors of every product dimension, scanned in one launch
+  {
+    ScanJob sj[4];
+    u32 nsj = 0;
+    for (u32 prod = 0; prod <= dim; ++prod) {
+      if (!m.full && 0 < prod && prod < dim) continue;
+      u32 np = m.count(prod);
+      if (carried_high(m, prod)) newid_of[prod] = dalloc<u32>(np ? np : 1, s);
+      same_of[prod] = dalloc<u32>((size_t)np + 1, s);
+      sj[nsj++] = ScanJob{sp[prod].offs, same_of[prod], nullptr, newid_of[prod], np, 1};
+    }
+    exscan_jobs(sj, nsj, s);
+  }
   for (u32 prod = 0; prod <= dim; ++prod) {
     if (!m.full && 0 < prod && prod < dim) continue;
     u32 np = m.count(prod);
     Doms d;
-    if (carried_high(m, prod)) newid_of[prod] = dalloc<u32>(np ? np : 1, s);
-    u32* same = negate_offsets(sp[prod].offs, np, s, nullptr, newid_of[prod]);
+    u32* same = same_of[prod];
     d.ndoms[0] = np;
     d.offs[0] = same;
     d.scale[0] = 1;
@@ -406,13 +424,8 @@ static u32 refine_build(Mesh& m, u32 const* gen_offs)
     for (u32 l = 1; l < h; ++l)
       if (same_of[h] && same_of[l])
         carry_down(m, *out, h, l, same_of[h], nsame_of[h], same_of[l]);
-  for (u32 h = 1; h <= dim; ++h) {
-    u32* newid = newid_of[h];
-    for (u32 l = 0; l < h; ++l)
-      if (same_of[h] && same_of[l])
-        carry_up(m, *out, l, h, same_of[l], nsame_of[l], same_of[h], nsame_of[h], &newid);
-    dev_free(newid, s);
-  }
+  carry_up_all(m, *out, same_of, nsame_of, newid_of);
+  for (u32 h = 0; h <= dim; ++h) dev_free(newid_of[h], s);
   for (u32 dd = 0; dd <= dim; ++dd) {
     dev_free(same_of[dd], s);
     dev_free(sp[dd].offs, s);

@@ -534,16 +534,19 @@ constexpr unsigned long long FLAG_AGG = 1ull << 62;
 constexpr unsigned long long FLAG_PRE = 2ull << 62;
 constexpr u32 SCAN_SPIN_LIMIT = 1u << 24;
 
-// mode 0 scans in[i]; mode 1 scans (in[i + 1] == in[i]), i.e. the
-// survivors of an offsets array (uints_negate_offsets, ints.cpp:227-235).
-// newid (optional, for 0/1 items): out[i] where item i is 1, INV where 0 --
-// each old entity's new id when the items mark survivors
-
-template <int MODE, int SCAN_ITEMS>
+// Several independent scans in one launch. Job j scans its `in` (mode 0)
+// or the survivors of an offsets array, (in[i + 1] == in[i]) (mode 1,
+// uints_negate_offsets, ints.cpp:227-235), into out[0..n] with the total at
+// out[n] (and in *total_to when given); newid (optional, for 0/1 items)
+// receives out[i] where item i is 1 and INV where it is 0 -- each old
+// entity's new id when the items mark survivors. Tiles are numbered across
+// the jobs (job j owns tiles tile0[j] .. tile0[j + 1] - 1, one at least) and
+// claimed through one ticket, so a look-back, which stops at its job's
+// first tile, only waits on tiles claimed before it. Independent scans of a
+// pass share a launch, and their look-back chains overlap.
+template <int SCAN_ITEMS>
 __global__ void __launch_bounds__(SCAN_THREADS)
-k_exscan(u32 const* __restrict__ in, u32* __restrict__ out, u32 n, u32 ntiles,
-    unsigned long long* status, u32* ticket_and_err, u32* total_to, u32* __restrict__ newid,
-    u32 spin_limit)
+k_exscan(ScanJobs jobs, unsigned long long* status, u32* ticket_and_err, u32 spin_limit)
 {
   pdl_wait();
   __shared__ u32 s_tile;
@@ -554,15 +557,23 @@ k_exscan(u32 const* __restrict__ in, u32* __restrict__ out, u32 n, u32 ntiles,
   if (threadIdx.x == 0) s_tile = atomicAdd(ticket_and_err, 1u);
   __syncthreads();
   u32 const tile = s_tile;
+  u32 const ntiles = jobs.tile0[jobs.njobs];
   if (tile >= ntiles) return;
-  size_t const base = (size_t)tile * SCAN_TILE;
+  u32 jn = 0;
+  while (jn + 1 < jobs.njobs && tile >= jobs.tile0[jn + 1]) ++jn;
+  ScanJob const job = jobs.j[jn];
+  u32 const first = jobs.tile0[jn], last = jobs.tile0[jn + 1] - 1;
+  u32 const* __restrict__ in = job.in;
+  u32 const n = job.n;
+  bool const mode1 = job.mode != 0;
+  size_t const base = (size_t)(tile - first) * SCAN_TILE;
   // coalesced load into shared memory (padded to avoid bank conflicts)
 #pragma unroll
   for (int k = 0; k < SCAN_ITEMS; ++k) {
     u32 li = k * SCAN_THREADS + threadIdx.x;
     size_t gi = base + li;
     u32 v = 0;
-    if (gi < n) v = MODE == 0 ? in[gi] : (in[gi + 1] == in[gi] ? 1u : 0u);
+    if (gi < n) v = !mode1 ? in[gi] : (in[gi + 1] == in[gi] ? 1u : 0u);
     s_buf[li + (li >> 5)] = v;
   }
   __syncthreads();
@@ -598,8 +609,8 @@ k_exscan(u32 const* __restrict__ in, u32* __restrict__ out, u32 n, u32 ntiles,
   if (warp == 0) {
     // warp-cooperative look-back: lane l inspects tile (p - l)
     u32 prefix = 0;
-    if (tile == 0) {
-      if (lane == 0) atomicExch(&status[0], FLAG_PRE | (unsigned long long)total);
+    if (tile == first) {
+      if (lane == 0) atomicExch(&status[tile], FLAG_PRE | (unsigned long long)total);
     } else {
       if (lane == 0) atomicExch(&status[tile], FLAG_AGG | (unsigned long long)total);
       int p = (int)tile - 1;
@@ -607,14 +618,15 @@ k_exscan(u32 const* __restrict__ in, u32* __restrict__ out, u32 n, u32 ntiles,
       bool gave_up = false;
       for (;;) {
         int idx = p - (int)lane;
-        unsigned long long st = FLAG_PRE;  // before tile 0: an empty prefix
-        if (idx >= 0) st = *((volatile unsigned long long*)&status[idx]);
+        unsigned long long st = FLAG_PRE;  // before the job's first tile: empty
+        if (idx >= (int)first) st = *((volatile unsigned long long*)&status[idx]);
         while (__any_sync(0xffffffffu, (st >> 62) == 0)) {
           if (++spins > spin_limit) {
             gave_up = true;
             break;
           }
-          if (idx >= 0 && (st >> 62) == 0) st = *((volatile unsigned long long*)&status[idx]);
+          if (idx >= (int)first && (st >> 62) == 0)
+            st = *((volatile unsigned long long*)&status[idx]);
         }
         if (gave_up) {
           if (lane == 0) atomicOr(&ticket_and_err[1], 1u);
@@ -642,6 +654,8 @@ k_exscan(u32 const* __restrict__ in, u32* __restrict__ out, u32 n, u32 ntiles,
     run += v[k];
   }
   __syncthreads();
+  u32* __restrict__ out = job.out;
+  u32* __restrict__ newid = job.newid;
 #pragma unroll
   for (int k = 0; k < SCAN_ITEMS; ++k) {
     u32 li = k * SCAN_THREADS + threadIdx.x;
@@ -650,14 +664,14 @@ k_exscan(u32 const* __restrict__ in, u32* __restrict__ out, u32 n, u32 ntiles,
       u32 const o = s_buf[li + (li >> 5)];
       out[gi] = o;
       if (newid) {
-        bool const on = MODE == 0 ? in[gi] != 0 : in[gi + 1] == in[gi];
+        bool const on = !mode1 ? in[gi] != 0 : in[gi + 1] == in[gi];
         newid[gi] = on ? o : INV;
       }
     }
   }
-  if (tile == ntiles - 1 && threadIdx.x == 0) {
+  if (tile == last && threadIdx.x == 0) {
     out[n] = s_prefix + total;
-    if (total_to) *total_to = s_prefix + total;
+    if (job.total_to) *job.total_to = s_prefix + total;
   }
   // The last tile to finish returns the scratch to zero for the next scan
   // on the stream: every other tile has counted itself done, so no look-back
@@ -678,13 +692,6 @@ k_exscan(u32 const* __restrict__ in, u32* __restrict__ out, u32 n, u32 ntiles,
       __threadfence();
     }
   }
-}
-
-__global__ void k_set_zero_total(u32* out, u32* total_to)
-{
-  pdl_wait();
-  out[0] = 0;
-  if (total_to) *total_to = 0;
 }
 
 namespace {
@@ -733,25 +740,44 @@ u32* stream_scan_scratch(size_t words, cudaStream_t s)
 }
 }  // namespace
 
+namespace {
+// tiles of a job (one at least: an empty scan still writes out[0] = 0)
+u32 job_tiles(u32 n, u32 items) { return n ? ceil_div(n, (u64)SCAN_THREADS * items) : 1u; }
+
+void launch_scan_jobs(ScanJobs const& jobs, u32 items, u32* scratch, u32 spin_limit,
+    cudaStream_t s)
+{
+  u32 const ntiles = jobs.tile0[jobs.njobs];
+  CK(launch_kernel(items == 8 ? k_exscan<8> : k_exscan<16>, dim3(ntiles), dim3(SCAN_THREADS),
+      0, s, jobs, reinterpret_cast<unsigned long long*>(scratch + 4), scratch, spin_limit));
+  CK_LAUNCH();
+}
+}  // namespace
+
+void exscan_jobs(ScanJob const* jobs, u32 njobs, cudaStream_t s)
+{
+  u32 const items = tuned(TK_SCAN_ITEMS);
+  for (u32 at = 0; at < njobs; at += MAX_SCAN_JOBS) {
+    ScanJobs pack;
+    pack.njobs = std::min<u32>(MAX_SCAN_JOBS, njobs - at);
+    pack.tile0[0] = 0;
+    double bytes = 0;
+    for (u32 q = 0; q < pack.njobs; ++q) {
+      pack.j[q] = jobs[at + q];
+      pack.tile0[q + 1] = pack.tile0[q] + job_tiles(pack.j[q].n, items);
+      bytes += 8.0 * pack.j[q].n + 4.0 + (pack.j[q].newid ? 4.0 * pack.j[q].n : 0.0);
+    }
+    // [ticket, error, done, pad][status per tile], zero on entry
+    u32* scratch = stream_scan_scratch(4 + 2 * (size_t)pack.tile0[pack.njobs], s);
+    PROBE(P_EXSCAN, s, bytes);
+    launch_scan_jobs(pack, items, scratch, SCAN_SPIN_LIMIT, s);
+  }
+}
+
 void exscan_u32(u32 const* in, u32* out, u32 n, cudaStream_t s, u32* total_to, u32* newid)
 {
-  if (n == 0) {
-    CK(launch_kernel(k_set_zero_total, dim3(1), dim3(1), 0, s, out, total_to));
-    CK_LAUNCH();
-    return;
-  }
-  u32 const items = tuned(TK_SCAN_ITEMS);
-  u32 ntiles = ceil_div(n, (u64)SCAN_THREADS * items);
-  // [ticket, error, done, pad][status per tile], zero on entry
-  u32* scratch = stream_scan_scratch(4 + 2 * (size_t)ntiles, s);
-  {
-    PROBE(P_EXSCAN, s, 4.0 * n + 4.0 * (n + 1));
-    CK(launch_kernel(items == 8 ? k_exscan<0, 8> : k_exscan<0, 16>, dim3(ntiles),
-        dim3(SCAN_THREADS), 0, s, in, out, n, ntiles,
-        reinterpret_cast<unsigned long long*>(scratch + 4), scratch, total_to, newid,
-        SCAN_SPIN_LIMIT));
-    CK_LAUNCH();
-  }
+  ScanJob j{in, out, total_to, newid, n, 0};
+  exscan_jobs(&j, 1, s);
 }
 
 // The scans of one stream record a look-back that gave up in word 1 of that
@@ -797,10 +823,12 @@ int selftest_scan_wait(u32 spin_limit)
   CK(cudaMemsetAsync(buf, 0, words * sizeof(u32), s));
   u32 one = 1;
   CK(cudaMemcpyAsync(scratch, &one, sizeof(u32), cudaMemcpyHostToDevice, s));
-  CK(launch_kernel(k_exscan<0, 16>, dim3(ntiles), dim3(SCAN_THREADS), 0, s, in, out, n, ntiles,
-      reinterpret_cast<unsigned long long*>(scratch + 4), scratch, nullptr, nullptr,
-      spin_limit));
-  CK_LAUNCH();
+  ScanJobs pack;
+  pack.njobs = 1;
+  pack.tile0[0] = 0;
+  pack.tile0[1] = ntiles;
+  pack.j[0] = ScanJob{in, out, nullptr, nullptr, n, 0};
+  launch_scan_jobs(pack, 16, scratch, spin_limit, s);
   u32 err = 0;
   CK(cudaMemcpyAsync(&err, scratch + 1, sizeof(u32), cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
@@ -818,19 +846,14 @@ void exscan_u32_scratch(u32 const* in, u32* out, u32 n, u32* scratch, cudaStream
 {
   if (reinterpret_cast<uintptr_t>(scratch) % 16 != 0)
     throw Failure(E_ARG, "scan scratch must start on a 16-byte boundary");
-  if (n == 0) {
-    CK(launch_kernel(k_set_zero_total, dim3(1), dim3(1), 0, s, out, nullptr));
-    CK_LAUNCH();
-    return;
-  }
   u32 const items = tuned(TK_SCAN_ITEMS);
-  u32 ntiles = ceil_div(n, (u64)SCAN_THREADS * items);
   CK(cudaMemsetAsync(scratch, 0, exscan_scratch_words(n) * sizeof(u32), s));
-  CK(launch_kernel(items == 8 ? k_exscan<0, 8> : k_exscan<0, 16>, dim3(ntiles),
-      dim3(SCAN_THREADS), 0, s, in, out, n, ntiles,
-      reinterpret_cast<unsigned long long*>(scratch + 4), scratch, nullptr, nullptr,
-      SCAN_SPIN_LIMIT));
-  CK_LAUNCH();
+  ScanJobs pack;
+  pack.njobs = 1;
+  pack.tile0[0] = 0;
+  pack.tile0[1] = job_tiles(n, items);
+  pack.j[0] = ScanJob{in, out, nullptr, nullptr, n, 0};
+  launch_scan_jobs(pack, items, scratch, SCAN_SPIN_LIMIT, s);
 }
 
 u32* exscan_new(u32 const* in, u32 n, cudaStream_t s, u32* total_to, u32* newid)
@@ -843,22 +866,8 @@ u32* exscan_new(u32 const* in, u32 n, cudaStream_t s, u32* total_to, u32* newid)
 u32* negate_offsets(u32 const* offs, u32 n, cudaStream_t s, u32* total_to, u32* newid)
 {
   u32* o = dalloc<u32>((size_t)n + 1, s);
-  if (n == 0) {
-    CK(launch_kernel(k_set_zero_total, dim3(1), dim3(1), 0, s, o, total_to));
-    CK_LAUNCH();
-    return o;
-  }
-  u32 const items = tuned(TK_SCAN_ITEMS);
-  u32 ntiles = ceil_div(n, (u64)SCAN_THREADS * items);
-  u32* scratch = stream_scan_scratch(4 + 2 * (size_t)ntiles, s);
-  {
-    PROBE(P_EXSCAN, s, 4.0 * (n + 1) + 4.0 * (n + 1));
-    CK(launch_kernel(items == 8 ? k_exscan<1, 8> : k_exscan<1, 16>, dim3(ntiles),
-        dim3(SCAN_THREADS), 0, s, offs, o, n, ntiles,
-        reinterpret_cast<unsigned long long*>(scratch + 4), scratch, total_to, newid,
-        SCAN_SPIN_LIMIT));
-    CK_LAUNCH();
-  }
+  ScanJob j{offs, o, total_to, newid, n, 1};
+  exscan_jobs(&j, 1, s);
   return o;
 }
 

@@ -47,6 +47,26 @@ void exscan_u32(u32 const* in, u32* out, u32 n, cudaStream_t s, u32* total_to = 
 u32* exscan_new(u32 const* in, u32 n, cudaStream_t s, u32* total_to = nullptr,
     u32* newid = nullptr);
 
+// Independent scans in one launch (their look-back chains overlap): job j
+// scans `in` (mode 0) or the survivors of an offsets array in[0..n]
+// (mode 1: in[i + 1] == in[i], uints_negate_offsets) into out[0..n], with
+// total_to and newid as above. Jobs are launched MAX_SCAN_JOBS at a time.
+constexpr u32 MAX_SCAN_JOBS = 8;
+struct ScanJob {
+  u32 const* in;
+  u32* out;
+  u32* total_to;
+  u32* newid;
+  u32 n;
+  u32 mode;
+};
+struct ScanJobs {
+  u32 njobs;
+  u32 tile0[MAX_SCAN_JOBS + 1];
+  ScanJob j[MAX_SCAN_JOBS];
+};
+void exscan_jobs(ScanJob const* jobs, u32 njobs, cudaStream_t s);
+
 // The same scan with caller-provided scratch of at least
 // exscan_scratch_words(n) 32-bit words (zeroed here); allocates nothing.
 size_t exscan_scratch_words(u32 n);

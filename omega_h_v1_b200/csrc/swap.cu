@@ -528,7 +528,6 @@ static void swap_build(Mesh& m, SwapSel const& sel)
   UpAdj const& te = m.ask_up(1, 3);
   u32 const* voe1 = m.ask_down(1, 0);
   u32 const* vot = m.ask_down(3, 0);
-  u32* cnt = dalloc<u32>(ne, s);
   u32* same_of[4] = {nullptr, nullptr, nullptr, nullptr};
   u32 nsame_of[4] = {0, 0, 0, 0};
   // the products and survivors of every dimension are counted first, their
@@ -539,22 +538,32 @@ static void swap_build(Mesh& m, SwapSel const& sel)
   // each kept entity's new id, written by the survivors' scan for the
   // dimensions whose upward adjacency is carried
   u32* newid_of[4] = {nullptr, nullptr, nullptr, nullptr};
+  // every dimension's two scans run together in one launch
+  ScanJob sj[6];
+  u32 nsj = 0;
+  u32* scan_in[6] = {};
   for (u32 ed = ed0; ed <= dim; ++ed) {
     u32 n = m.count(ed);
-    CK(launch_kernel(k_swap_counts, dim3(grid_for(ne)), dim3(BLOCK), 0, s, ne, ed, sel.ind, sel.rs, cnt));
+    u32* cnt = dalloc<u32>(ne, s);
+    CK(launch_kernel(k_swap_counts, dim3(grid_for(ne)), dim3(BLOCK), 0, s, ne, ed, sel.ind,
+        sel.rs, cnt));
     CK_LAUNCH();
-    gen_offs_of[ed] = exscan_new(cnt, ne, s, m.mb->dev + 20 + 2 * (ed - 1));
+    gen_offs_of[ed] = dalloc<u32>((size_t)ne + 1, s);
+    scan_in[nsj] = cnt;
+    sj[nsj++] = ScanJob{cnt, gen_offs_of[ed], m.mb->dev + 20 + 2 * (ed - 1), nullptr, ne, 0};
     u32* same = dalloc<u32>(n, s);
     if (n) {
-      CK(launch_kernel(k_swap_same, dim3(grid_for(n)), dim3(BLOCK), 0, s, n, deg(ed, 1), ed == 1 ? nullptr : m.ask_down(ed, 1),
-          sel.ind, same));
+      CK(launch_kernel(k_swap_same, dim3(grid_for(n)), dim3(BLOCK), 0, s, n, deg(ed, 1),
+          ed == 1 ? nullptr : m.ask_down(ed, 1), sel.ind, same));
       CK_LAUNCH();
     }
     if (carried_high(m, ed)) newid_of[ed] = dalloc<u32>(n ? n : 1, s);
-    same_of[ed] = exscan_new(same, n, s, m.mb->dev + 21 + 2 * (ed - 1), newid_of[ed]);
-    dev_free(same, s);
+    same_of[ed] = dalloc<u32>((size_t)n + 1, s);
+    scan_in[nsj] = same;
+    sj[nsj++] = ScanJob{same, same_of[ed], m.mb->dev + 21 + 2 * (ed - 1), newid_of[ed], n, 0};
   }
-  dev_free(cnt, s);
+  exscan_jobs(sj, nsj, s);
+  for (u32 k = 0; k < nsj; ++k) dev_free(scan_in[k], s);
   m.mb->fetch(s, 26);
   for (u32 ed = ed0; ed <= dim; ++ed) {
     u32 n = m.count(ed), vpe = deg(ed, 0);
@@ -621,13 +630,8 @@ static void swap_build(Mesh& m, SwapSel const& sel)
     for (u32 l = 1; l < h; ++l)
       if (same_of[h] && same_of[l])
         carry_down(m, *out, h, l, same_of[h], nsame_of[h], same_of[l]);
-  for (u32 h = 1; h <= dim; ++h) {
-    u32* newid = newid_of[h];
-    for (u32 l = 0; l < h; ++l)
-      if (same_of[h] && same_of[l])
-        carry_up(m, *out, l, h, same_of[l], nsame_of[l], same_of[h], nsame_of[h], &newid);
-    dev_free(newid, s);
-  }
+  carry_up_all(m, *out, same_of, nsame_of, newid_of);
+  for (u32 h = 0; h <= dim; ++h) dev_free(newid_of[h], s);
   for (u32 d = 0; d < 4; ++d) dev_free(same_of[d], s);
   m.overwrite(out);
 }
