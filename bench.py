@@ -294,6 +294,7 @@ def run_ours(args, world, rank, local):
     L.osh_b200_probe_reset()
     L.osh_b200_probe_enable(1 << probe_id)
     launches0 = L.osh_b200_launch_count()
+    syncs0 = L.osh_b200_sync_count()
     clocks = Clocks(local)
     barrier(world)
     torch.cuda.synchronize()
@@ -313,6 +314,7 @@ def run_ours(args, world, rank, local):
     barrier(world)
     clk = clocks.stop()
     launches = L.osh_b200_launch_count() - launches0
+    syncs = L.osh_b200_sync_count() - syncs0
     L.osh_b200_probe_enable(0)
     ms_local = ev0.elapsed_time(ev1)
     plaunch, pms, pbytes = C.c_uint(), C.c_double(), C.c_double()
@@ -358,6 +360,8 @@ def run_ours(args, world, rank, local):
         "e2e": e2e,
         "fp32_filter": fp32,
         "gpu_launches": int(launches),
+        "per_adapt": {"launches": round(launches / args.steps, 1),
+                      "host_waits": round(syncs / args.steps, 1)},
         "clocks": clk,
         "tets_in": tets_in,
         "passes_per_step": npass[0] if npass else None,
@@ -412,8 +416,8 @@ def fp32_leg(G, L, base, args, world, stream, stream_ptr, plain_ms):
     G.check()
     audited_digest = L.osh_b200_digest(h)
     L.osh_free(h)
-    fa = G.fp32_stats(reset=True)
     au = G.fp32_audit_stats()
+    fa = G.fp32_stats(reset=True)
     G.set_fp32_audit(False)
     return {"value": round(value, 1), "unit": UNIT, "ms_per_step": round(ms / args.steps, 3),
             "vs_plain_fp64": round(plain_ms / ms_local, 3),

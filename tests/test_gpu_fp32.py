@@ -26,8 +26,8 @@ def audit_on():
 
 def _audit_clean():
     import omega_h_v1_b200 as G
-    st = G.fp32_stats(reset=True)
     au = G.fp32_audit_stats()
+    st = G.fp32_stats(reset=True)
     assert au["flips"] == 0, au
     assert st["bound_exceeded"] == 0, st
     return st, au
