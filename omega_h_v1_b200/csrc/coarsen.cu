@@ -423,20 +423,31 @@ __global__ void k_vertex_dest_grouped(u32 nv, u32 const* __restrict__ ue_offs,
 }
 
 // collapse_to_ent (collapses_to_ents.cpp:11-64)
-__global__ void k_collapse_to_ent(u32 ed, u32 n, u32 const* __restrict__ voe,
+// (ED: the entities' dimension at compile time, so the loads of all their
+// vertices are issued before any is used)
+template <u32 ED>
+__global__ void k_collapse_to_ent(u32 n, u32 const* __restrict__ voe,
     u32 const* __restrict__ soe, u32 const* __restrict__ gen_offs_v,
     u32 const* __restrict__ gen_vert_v, u32 const* __restrict__ fused_ents,
     u32* __restrict__ is_same, u32* __restrict__ fused_sides, u32* __restrict__ will_gen,
     u32* __restrict__ gen_vert, u32* __restrict__ gen_dir)
 {
   pdl_wait();
+  constexpr u32 VPE = ED + 1, SPE = ED + 1;
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  u32 vpe = deg(ed, 0), spe = deg(ed, ed - 1);
-  u32 const* v = voe + (size_t)i * vpe;
+  u32 v[VPE], a[VPE], b[VPE];
+#pragma unroll
+  for (u32 j = 0; j < VPE; ++j) v[j] = voe[(size_t)i * VPE + j];
+#pragma unroll
+  for (u32 j = 0; j < VPE; ++j) {
+    a[j] = gen_offs_v[v[j]];
+    b[j] = gen_offs_v[v[j] + 1];
+  }
   u32 col = INV, dir = INV;
-  for (u32 j = 0; j < vpe; ++j)
-    if (gen_offs_v[v[j]] != gen_offs_v[v[j] + 1]) {
+#pragma unroll
+  for (u32 j = 0; j < VPE; ++j)
+    if (a[j] != b[j]) {  // the last collapsing vertex in local order wins
       col = v[j];
       dir = j;
     }
@@ -448,10 +459,11 @@ __global__ void k_collapse_to_ent(u32 ed, u32 n, u32 const* __restrict__ voe,
   }
   is_same[i] = 0;
   u32 gv = gen_vert_v[col], gd = INV;
-  for (u32 j = 0; j < vpe; ++j)
+#pragma unroll
+  for (u32 j = 0; j < VPE; ++j)
     if (v[j] == gv) gd = j;
   if (gd != INV) {
-    fused_sides[soe[(size_t)i * spe + opp(ed, 0, gd)]] = 1;
+    fused_sides[soe[(size_t)i * SPE + opp(ED, 0, gd)]] = 1;
   } else if (!(fused_ents && fused_ents[i])) {
     wg = 1;
     gen_vert[i] = gv;
@@ -480,14 +492,18 @@ __global__ void k_coarsen_topology(u32 ed, u32 n, u32 const* __restrict__ voe,
 }
 
 // expansion of the surviving entities' vertices, renumbered
-__global__ void k_same_conn(u32 n, u32 vpe, u32 const* __restrict__ voe,
-    u32 const* __restrict__ same_e, u32 const* __restrict__ same_v, u32* __restrict__ out)
+template <u32 VPE>
+__global__ void k_same_conn(u32 n, u32 const* __restrict__ voe, u32 const* __restrict__ same_e,
+    u32 const* __restrict__ same_v, u32* __restrict__ out)
 {
   pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n || same_e[i] == same_e[i + 1]) return;
-  u32 o = same_e[i];
-  for (u32 j = 0; j < vpe; ++j) out[(size_t)o * vpe + j] = same_v[voe[(size_t)i * vpe + j]];
+  u32 o = same_e[i], v[VPE];
+#pragma unroll
+  for (u32 j = 0; j < VPE; ++j) v[j] = voe[(size_t)i * VPE + j];
+#pragma unroll
+  for (u32 j = 0; j < VPE; ++j) out[(size_t)o * VPE + j] = same_v[v[j]];
 }
 
 // coarsen_conserve_cavity (coarsen_conserve.cpp:15-55)
@@ -699,8 +715,10 @@ struct CoarsenSel {
   }
 };
 
+// deferred: no read-back here (the candidate flags and the set's outcome
+// come back with coarsen_build's), so it always returns true
 static bool coarsen_select(Mesh& m, u32* codes, double qual_floor, bool require_better,
-    CoarsenSel& sel, u32* codes_class_out, u32* codes_qual_out)
+    CoarsenSel& sel, u32* codes_class_out, u32* codes_qual_out, bool deferred = false)
 {
   cudaStream_t s = m.s;
   u32 dim = m.dim, ne = m.count(1), nv = m.count(0);
@@ -759,13 +777,15 @@ static bool coarsen_select(Mesh& m, u32* codes, double qual_floor, bool require_
   dev_free(clist, s);
   if (codes_qual_out)
     CK(cudaMemcpyAsync(codes_qual_out, codes, sizeof(u32) * ne, cudaMemcpyDeviceToDevice, s));
-  m.mb->fetch(s, 8);
-  if (!m.mb->host[7]) return false;
-  // check_coarsen_quality (coarsen_common.cpp:139-180) ghosts a parallel
-  // mesh and exchanges the collapse codes whatever it then finds
-  m.ensure_ghosting(1);
-  m.note_exchange(1);
-  if (!m.mb->host[4]) return false;
+  if (!deferred) {
+    m.mb->fetch(s, 8);
+    if (!m.mb->host[7]) return false;
+    // check_coarsen_quality (coarsen_common.cpp:139-180) ghosts a parallel
+    // mesh and exchanges the collapse codes whatever it then finds
+    m.ensure_ghosting(1);
+    m.note_exchange(1);
+    if (!m.mb->host[4]) return false;
+  }
   UpAdj const& ue = m.ask_up(0, 1);
   sel.cand = dalloc<u32>(nv, s);
   sel.colq = dalloc<double>(nv, s);
@@ -777,7 +797,7 @@ static bool coarsen_select(Mesh& m, u32* codes, double qual_floor, bool require_
         ue.dirs, codes, sel.q2, sel.cand, sel.colq));
     CK_LAUNCH();
   }
-  sel.ind = find_indset(m, 0, sel.cand, sel.colq);
+  sel.ind = find_indset(m, 0, sel.cand, sel.colq, !deferred);
   sel.gen_vert = dalloc<u32>(nv, s);
   if (nv) {
     u32 const vg = tuned(TK_VERT_GROUP);
@@ -791,7 +811,9 @@ static bool coarsen_select(Mesh& m, u32* codes, double qual_floor, bool require_
 }
 
 // coarsen_interior + coarsen_all_ents (coarsen_common.cpp:35-219)
-static void coarsen_build(Mesh& m, CoarsenSel const& sel)
+// deferred: the selection's flags and the set's outcome come back with the
+// counts; with no collapse kept it frees what it made and returns false
+static bool coarsen_build(Mesh& m, CoarsenSel const& sel, bool deferred)
 {
   cudaStream_t s = m.s;
   u32 dim = m.dim, nv = m.count(0);
@@ -834,8 +856,11 @@ static void coarsen_build(Mesh& m, CoarsenSel const& sel)
     if (n) {
       PROBE(P_COLLAPSE_TO_ENT, s, 4.0 * (vpe + deg(ed, ed - 1)) * n + 8.0 * (nv + 1) +
           4.0 * n * 4 + 4.0 * nsides);
-      CK(launch_kernel(k_collapse_to_ent, dim3(grid_for(n)), dim3(BLOCK), 0, s, ed, n, voe, soe, gen_offs_v,
-          sel.gen_vert, fused[ed], is_same, fused[ed - 1], will_gen, gvert_of[ed], gdir_of[ed]));
+      auto k = ed == 1 ? k_collapse_to_ent<1> : ed == 2 ? k_collapse_to_ent<2>
+                                                        : k_collapse_to_ent<3>;
+      CK(launch_kernel(k, dim3(grid_for(n)), dim3(BLOCK), 0, s, n, voe, soe, gen_offs_v,
+          sel.gen_vert, fused[ed], is_same, fused[ed - 1], will_gen, gvert_of[ed],
+          gdir_of[ed]));
       CK_LAUNCH();
     }
     gen_offs_of[ed] = dalloc<u32>((size_t)n + 1, s);
@@ -848,7 +873,32 @@ static void coarsen_build(Mesh& m, CoarsenSel const& sel)
   }
   exscan_jobs(sj, nsj, s);
   for (u32 k = 0; k < nscan_in; ++k) dev_free(scan_in[k], s);
-  m.mb->fetch(s, 23);
+  m.mb->fetch(s, deferred ? INDSET_FETCH_SLOTS : 23);
+  if (deferred) {
+    auto abandon = [&] {
+      for (u32 d = 0; d < 4; ++d) {
+        dev_free(fused[d], s);
+        dev_free(same_of[d], s);
+        dev_free(gen_offs_of[d], s);
+        dev_free(gvert_of[d], s);
+        dev_free(gdir_of[d], s);
+        dev_free(newid_of[d], s);
+      }
+      dev_free(same_v, s);
+      dev_free(gen_offs_v, s);
+    };
+    try {
+      indset_check(m);
+    } catch (...) {
+      abandon();
+      throw;
+    }
+    if (!m.mb->host[7] || !m.mb->host[4]) {  // no candidate, or no collapse kept
+      abandon();
+      last_pass_stats().indset_rounds = 0;
+      return false;
+    }
+  }
   u32 nv_out = m.mb->host[22];
   last_pass_stats().nselected = nv - nv_out;
   Mesh* out = m.spawn();
@@ -892,7 +942,8 @@ static void coarsen_build(Mesh& m, CoarsenSel const& sel)
     u32 nout = nsame + ngen;
     u32* conn = dalloc<u32>((size_t)nout * vpe, s);
     if (n) {
-      CK(launch_kernel(k_same_conn, dim3(grid_for(n)), dim3(BLOCK), 0, s, n, vpe, voe, same_e, same_v, conn));
+      auto k = vpe == 2 ? k_same_conn<2> : vpe == 3 ? k_same_conn<3> : k_same_conn<4>;
+      CK(launch_kernel(k, dim3(grid_for(n)), dim3(BLOCK), 0, s, n, voe, same_e, same_v, conn));
       CK_LAUNCH();
       CK(launch_kernel(k_coarsen_topology, dim3(grid_for(n)), dim3(BLOCK), 0, s, ed, n, voe, gen_offs, gvert, gdir,
           same_v, conn + (size_t)nsame * vpe));
@@ -931,17 +982,27 @@ static void coarsen_build(Mesh& m, CoarsenSel const& sel)
   }
   dev_free(gen_offs_v, s);
   m.overwrite(out);
+  return true;
+}
+
+// For a serial mesh outside a batch (no ghosting state, no segments to
+// tally) the selection's flags and the set's outcome come back with the
+// build's first read-back: two host waits fewer per pass.
+static bool coarsen_deferred(Mesh& m)
+{
+  return m.dim >= 2 && !m.parallel && !m.seg;
 }
 
 static u32 coarsen_common(Mesh& m, u32* codes, double qual_floor, bool require_better)
 {
   CoarsenSel sel;
   bool ok = false;
+  bool const deferred = coarsen_deferred(m);
   try {
-    ok = coarsen_select(m, codes, qual_floor, require_better, sel, nullptr, nullptr);
+    ok = coarsen_select(m, codes, qual_floor, require_better, sel, nullptr, nullptr, deferred);
     if (ok) {
       seg_tally(m, 0, sel.ind);
-      coarsen_build(m, sel);
+      ok = coarsen_build(m, sel, deferred);
     }
   } catch (...) {
     sel.free(m.s);

@@ -22,6 +22,7 @@ PassStats& last_pass_stats()
 
 // control words of the single-launch rounds (mailbox slots 44-50)
 constexpr u32 COOP_CTL_SLOT = 44, COOP_CTL_WORDS = 7;
+static_assert(COOP_CTL_SLOT + COOP_CTL_WORDS == INDSET_FETCH_SLOTS, "mailbox slots");
 
 // also zeroes the control words of the rounds
 __global__ void k_indset_init(u32 n, u32 const* __restrict__ filter, u32* __restrict__ st,
@@ -151,9 +152,15 @@ __global__ void __launch_bounds__(BLOCK) k_indset_coop(u32 n, Nbrs g, u32* a, u3
     if (!coop_barrier(ctl)) return;
     if (*(volatile u32*)&ctl[2 + r % 3] == 0) {
       if (blockIdx.x == 0 && threadIdx.x == 0) ctl[5] = r + 1;
+      // the result always ends in a: an even round wrote b, which every
+      // block now copies its share of (b is settled: no round writes it)
+      if (r % 2 == 0)
+        for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+          a[i] = __ldcg(&b[i]);
       return;
     }
   }
+  // 100 rounds: the last (an odd round) wrote a
   if (blockIdx.x == 0 && threadIdx.x == 0) ctl[5] = MAX_INDSET_ROUNDS;
 }
 
@@ -202,7 +209,7 @@ static u32 read_cached_uses(Mesh& m, u32 ent_dim)
   return ent_dim == 0 ? 2u * m.counts[1] : deg(m.dim, 1) * m.counts[m.dim];
 }
 
-u32* find_indset(Mesh& m, u32 ent_dim, u32 const* filter, double const* good)
+u32* find_indset(Mesh& m, u32 ent_dim, u32 const* filter, double const* good, bool check)
 {
   u32 n = m.count(ent_dim);
   Nbrs g{};
@@ -228,17 +235,15 @@ u32* find_indset(Mesh& m, u32 ent_dim, u32 const* filter, double const* good)
   u64 const* glob = (m.parallel && m.globals[ent_dim]) ? m.globals[ent_dim] : nullptr;
   u32* a = dalloc<u32>(n, m.s);
   u32* b = dalloc<u32>(n, m.s);
+  // zeroes the control words even with no entity (rounds run = 0 then)
+  CK(launch_kernel(k_indset_init, dim3(grid_for(std::max<u32>(n, COOP_CTL_WORDS))),
+      dim3(BLOCK), 0, m.s, n, filter, a, m.mb->dev + COOP_CTL_SLOT));
+  CK_LAUNCH();
+  // All rounds run in one cooperative launch that leaves the set in a; its
+  // control words (mailbox slots COOP_CTL_SLOT..) come back with slots 1-3,
+  // which a caller that left flags there reads after this call without a
+  // read-back of its own
   if (n) {
-    CK(launch_kernel(k_indset_init, dim3(grid_for(std::max<u32>(n, COOP_CTL_WORDS))),
-        dim3(BLOCK), 0, m.s, n, filter, a, m.mb->dev + COOP_CTL_SLOT));
-    CK_LAUNCH();
-  }
-  // All rounds run in one cooperative launch; its control words (mailbox
-  // slots COOP_CTL_SLOT..) come back with slots 1-3, which a caller that
-  // left flags there reads after this call without a read-back of its own.
-  u32 rounds = 0;
-  bool done = (n == 0);
-  if (!done) {
     u32* ctl = m.mb->dev + COOP_CTL_SLOT;
     double nuse = (double)read_cached_uses(m, ent_dim);
     double avg_row = nuse / n;
@@ -248,25 +253,29 @@ u32* find_indset(Mesh& m, u32 ent_dim, u32 const* filter, double const* good)
     else if (lanes == 8) launch_coop<8>(n, g, a, b, good, glob, ctl, m.s);
     else if (lanes == 4) launch_coop<4>(n, g, a, b, good, glob, ctl, m.s);
     else launch_coop<2>(n, g, a, b, good, glob, ctl, m.s);
-    m.mb->fetch(m.s, COOP_CTL_SLOT + COOP_CTL_WORDS);
-    u32 const* hc = m.mb->host + COOP_CTL_SLOT;
-    if (hc[6]) {
-      dev_free(a, m.s);
-      dev_free(b, m.s);
-      throw Failure(E_TIMEOUT, "independent set: a grid barrier wait gave up");
-    }
-    rounds = hc[5];
-    done = rounds > 0 && hc[2 + (rounds - 1) % 3] == 0;
-    // round r writes b when r is even: the result is in b after an odd count
-    if (rounds % 2 == 1) std::swap(a, b);
   }
   dev_free(b, m.s);
-  last_pass_stats().indset_rounds = rounds;
-  if (!done) {
-    dev_free(a, m.s);
-    throw Failure(E_NOCONVERGE, "independent set did not settle in 100 rounds");
+  if (check) {
+    m.mb->fetch(m.s, INDSET_FETCH_SLOTS);
+    try {
+      indset_check(m);
+    } catch (...) {
+      dev_free(a, m.s);
+      throw;
+    }
   }
   return a;
+}
+
+void indset_check(Mesh& m)
+{
+  u32 const* hc = m.mb->host + COOP_CTL_SLOT;
+  if (hc[6]) throw Failure(E_TIMEOUT, "independent set: a grid barrier wait gave up");
+  u32 rounds = hc[5];
+  last_pass_stats().indset_rounds = rounds;
+  // settled: no entity, or the last round left none undecided
+  bool done = rounds == 0 || hc[2 + (rounds - 1) % 3] == 0;
+  if (!done) throw Failure(E_NOCONVERGE, "independent set did not settle in 100 rounds");
 }
 
 // ---------------------------------------------------------------------------
@@ -360,12 +369,17 @@ void expand_many(std::vector<ExpandJob> const& jobs, cudaStream_t s)
 
 // class_dim / class_id of the products: every domain of both labels in one
 // launch
-void inherit_class(Mesh& m, Mesh& out, u32 prod, Doms const& d)
+void inherit_class(Mesh& m, Mesh& out, u32 prod, Doms const& d,
+    std::vector<ExpandJob> const* also)
 {
-  if (!m.find_tag(0, "class_dim")) return;
+  if (!m.find_tag(0, "class_dim")) {
+    if (also) expand_many(*also, m.s);
+    return;
+  }
   char const* names[2] = {"class_dim", "class_id"};
   u32 nnames = m.find_tag(0, "class_id") ? 2 : 1;
   std::vector<ExpandJob> jobs;
+  if (also) jobs = *also;
   u32* data[2] = {nullptr, nullptr};
   u32 nc[2] = {1, 1};
   for (u32 q = 0; q < nnames; ++q) {

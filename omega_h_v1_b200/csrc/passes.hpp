@@ -26,7 +26,13 @@ void seg_tally(Mesh& m, u32 ent_dim, u32 const* flags);
 // Luby independent set over the star graph of `ent_dim` entities
 // (mesh_find_indset, indset.cpp:119-139). filter and goodness are device
 // arrays; returns a device state array (1 = in set) or throws E_NOCONVERGE.
-u32* find_indset(Mesh& m, u32 ent_dim, u32 const* filter, double const* goodness);
+// With check = false the outcome is not read back here: the caller fetches
+// at least INDSET_FETCH_SLOTS mailbox slots later (with its own read-back)
+// and calls indset_check, which throws as find_indset would have.
+constexpr u32 INDSET_FETCH_SLOTS = 51;
+u32* find_indset(Mesh& m, u32 ent_dim, u32 const* filter, double const* goodness,
+    bool check = true);
+void indset_check(Mesh& m);
 
 // copy rows of `width` elements: out[j] = in[i] for j in
 // [offs[i]*k, offs[i+1]*k), for T of 1, 4 or 8 bytes
@@ -62,7 +68,9 @@ struct Doms {
 
 // class_dim / class_id of the products of `prod_dim` (inherit_class,
 // inherit.cpp:217-232)
-void inherit_class(Mesh& m, Mesh& out, u32 prod_dim, Doms const& d);
+// `also` (optional): further row expansions launched with the labels' copies
+void inherit_class(Mesh& m, Mesh& out, u32 prod_dim, Doms const& d,
+    std::vector<ExpandJob> const* also = nullptr);
 
 // u64 global numbering of a single-rank parallel mesh after a pass
 // (inherit_globals, parallel_modify.cpp:79-111): survivors keep their order,

@@ -203,44 +203,68 @@ __global__ void k_refine_seg(u32 ne, u32 nv, u32 const* __restrict__ voe,
 
 // split_to_domain (splits_to_domains.cpp:13-31): first split edge of each
 // domain, in the domain's local edge order
-__global__ void k_split_to_domain(u32 nd, u32 spd, u32 const* __restrict__ sod,
+// (SPD edges per domain entity, a compile-time count: the loads of all of
+// them are issued before any is used)
+template <u32 SPD>
+__global__ void k_split_to_domain(u32 nd, u32 const* __restrict__ sod,
     u32 const* __restrict__ gen_offs, u32 nv, u32* __restrict__ will,
     u32* __restrict__ dir, u32* __restrict__ vert)
 {
   pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nd) return;
-  u32 w = 0, d = INV, v = INV;
-  for (u32 j = 0; j < spd; ++j) {
-    u32 s = sod ? sod[(size_t)i * spd + j] : i;
-    if (gen_offs[s] == gen_offs[s + 1]) continue;
-    w = 1;
-    d = j;
-    v = nv + gen_offs[s];
-    break;
+  u32 sv[SPD], a[SPD], b[SPD];
+#pragma unroll
+  for (u32 j = 0; j < SPD; ++j) sv[j] = sod ? sod[(size_t)i * SPD + j] : i;
+#pragma unroll
+  for (u32 j = 0; j < SPD; ++j) {
+    a[j] = gen_offs[sv[j]];
+    b[j] = gen_offs[sv[j] + 1];
   }
+  u32 w = 0, d = INV, v = INV;
+#pragma unroll
+  for (u32 j = SPD; j-- > 0;)
+    if (a[j] != b[j]) {  // the first split edge in local order wins
+      w = 1;
+      d = j;
+      v = nv + a[j];
+    }
   will[i] = w;
   dir[i] = d;
   vert[i] = v;
 }
 
-// refine_domain_entity (refine_topology.cpp:26-64)
-__global__ void k_refine_topology(u32 dd, u32 prod, u32 nd, u32 const* __restrict__ vod,
-    u32 const* __restrict__ offs, u32 const* __restrict__ dir,
-    u32 const* __restrict__ vert, u32* __restrict__ out)
+// refine_domain_entity (refine_topology.cpp:26-64), for every domain
+// dimension of one product dimension in one launch (blockIdx.y: the domain
+// dimension's job)
+struct TopoJob {
+  u32 dd, nd;
+  u32 const* vod;
+  u32 const* offs;
+  u32 const* dir;
+  u32 const* vert;
+  u32* out;
+};
+struct TopoJobs {
+  TopoJob j[3];
+};
+
+__global__ void k_refine_topology(TopoJobs jobs, u32 prod)
 {
   pdl_wait();
+  TopoJob const jb = jobs.j[blockIdx.y];
+  u32 const dd = jb.dd;
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= nd || offs[i] == offs[i + 1]) return;
+  if (i >= jb.nd || jb.offs[i] == jb.offs[i + 1]) return;
   u32 base_dim = prod - 1, opp_dim = dd - 1 - base_dim;
   u32 ops = deg(1, opp_dim), vpp = deg(prod, 0), vpb = vpp - 1, vpd = deg(dd, 0);
-  u32* p = out + (size_t)offs[i] * ops * vpp;
-  u32 di = dir[i];
+  u32* p = jb.out + (size_t)jb.offs[i] * ops * vpp;
+  u32 di = jb.dir[i];
   for (u32 j = 0; j < ops; ++j) {
     u32 o = canon(dd, 1, opp_dim, di, j);
     u32 b = opp(dd, opp_dim, o);
-    for (u32 k = 0; k < vpb; ++k) p[k] = vod[(size_t)i * vpd + canon(dd, base_dim, 0, b, k)];
-    p[vpb] = vert[i];
+    for (u32 k = 0; k < vpb; ++k) p[k] = jb.vod[(size_t)i * vpd + canon(dd, base_dim, 0, b, k)];
+    p[vpb] = jb.vert[i];
     p += vpp;
   }
 }
@@ -277,8 +301,10 @@ struct Splits {
   u32 nsplit = 0;
 };
 
-// returns the number of split edges (read back with the domain counts)
-static u32 refine_build(Mesh& m, u32 const* gen_offs)
+// returns the number of split edges (read back with the domain counts).
+// deferred: the independent set's outcome comes back with the same
+// read-back; nothing to split (or a failed set) leaves the mesh unchanged.
+static u32 refine_build(Mesh& m, u32 const* gen_offs, bool deferred)
 {
   cudaStream_t s = m.s;
   u32 dim = m.dim, src = 1;
@@ -301,8 +327,11 @@ static u32 refine_build(Mesh& m, u32 const* gen_offs)
     sp[dd].dir = dalloc<u32>(nd, s);
     sp[dd].vert = dalloc<u32>(nd, s);
     if (nd) {
-      CK(launch_kernel(k_split_to_domain, dim3(grid_for(nd)), dim3(BLOCK), 0, s, nd,
-          deg(dd, 1), sod, gen_offs, nv, will[dd], sp[dd].dir, sp[dd].vert));
+      u32 const spd = deg(dd, 1);
+      auto k = spd == 1 ? k_split_to_domain<1> : spd == 3 ? k_split_to_domain<3>
+                                                           : k_split_to_domain<6>;
+      CK(launch_kernel(k, dim3(grid_for(nd)), dim3(BLOCK), 0, s, nd, sod, gen_offs, nv,
+          will[dd], sp[dd].dir, sp[dd].vert));
       CK_LAUNCH();
     }
     sp[dd].offs = dalloc<u32>((size_t)nd + 1, s);
@@ -311,7 +340,28 @@ static u32 refine_build(Mesh& m, u32 const* gen_offs)
   // the domains' scans in one launch
   exscan_jobs(jobs, njobs, s);
   for (u32 dd = 1; dd <= dim; ++dd) dev_free(will[dd], s);
-  m.mb->fetch(s, 16);
+  m.mb->fetch(s, deferred ? INDSET_FETCH_SLOTS : 16);
+  if (deferred) {
+    auto abandon = [&] {
+      delete out;
+      for (u32 dd = 0; dd <= dim; ++dd) {
+        dev_free(sp[dd].offs, s);
+        dev_free(sp[dd].dir, s);
+        dev_free(sp[dd].vert, s);
+      }
+    };
+    try {
+      indset_check(m);
+    } catch (...) {
+      abandon();
+      throw;
+    }
+    if (!m.mb->host[1]) {  // no good candidate: the set is empty
+      abandon();
+      last_pass_stats().indset_rounds = 0;
+      return 0;
+    }
+  }
   for (u32 dd = 1; dd <= dim; ++dd)
     if (m.has_dim(dd)) sp[dd].nsplit = m.mb->host[8 + dd];
   u32 nsplit = sp[1].nsplit;
@@ -363,6 +413,7 @@ static u32 refine_build(Mesh& m, u32 const* gen_offs)
     u32 np = m.count(prod);
     Doms d;
     u32* same = same_of[prod];
+    std::vector<ExpandJob> conn_job;
     d.ndoms[0] = np;
     d.offs[0] = same;
     d.scale[0] = 1;
@@ -384,20 +435,37 @@ static u32 refine_build(Mesh& m, u32 const* gen_offs)
     if (prod) {
       u32 vpp = deg(prod, 0), nout = d.ngo[4];
       u32* conn = dalloc<u32>((size_t)nout * vpp, s);
-      expand_scaled(m.ask_down(prod, 0), same, 1, np, vpp, 4, conn, s);
+      // the survivors' connectivity is copied with the class labels' copies
+      ExpandJob cj;
+      cj.in = m.ask_down(prod, 0);
+      cj.offs = same;
+      cj.out = conn;
+      cj.k = 1;
+      cj.n = np;
+      cj.width = vpp;
+      cj.esz = 4;
+      conn_job.push_back(cj);
+      TopoJobs tj;
+      u32 ntj = 0, ndmax = 0;
+      double bytes = 0;
       for (u32 dd = first; dd <= last; ++dd) {
         if (!d.ndoms[dd] || !d.scale[dd] || !sp[dd].nsplit) continue;
         u32 nd = d.ndoms[dd];
-        PROBE(P_REFINE_TOPOLOGY, s, 4.0 * deg(dd, 0) * nd + 12.0 * nd + 4.0 * (nd + 1) +
-            4.0 * vpp * (double)d.ngen[dd]);
-        CK(launch_kernel(k_refine_topology, dim3(grid_for(nd)), dim3(BLOCK), 0, s, dd, prod, nd, m.ask_down(dd, 0),
-            sp[dd].offs, sp[dd].dir, sp[dd].vert, conn + (size_t)d.ngo[dd] * vpp));
+        tj.j[ntj++] = TopoJob{dd, nd, m.ask_down(dd, 0), sp[dd].offs, sp[dd].dir, sp[dd].vert,
+            conn + (size_t)d.ngo[dd] * vpp};
+        ndmax = std::max(ndmax, nd);
+        bytes += 4.0 * deg(dd, 0) * nd + 12.0 * nd + 4.0 * (nd + 1) + 4.0 * vpp * (double)d.ngen[dd];
+      }
+      if (ntj) {
+        PROBE(P_REFINE_TOPOLOGY, s, bytes);
+        CK(launch_kernel(k_refine_topology, dim3(grid_for(ndmax), ntj), dim3(BLOCK), 0, s, tj,
+            prod));
         CK_LAUNCH();
       }
       out->set_ents(prod, nout, conn);
       if (m.parallel) inherit_globals(*out, prod, nout);
     }
-    inherit_class(m, *out, prod, d);
+    inherit_class(m, *out, prod, d, &conn_job);
     if (prod == dim) {
       for (int pass = 0; pass < 2; ++pass) {
         u32 want = pass == 0 ? X_CONSERVE : X_POINTWISE;
@@ -441,8 +509,10 @@ static u32 refine_build(Mesh& m, u32 const* gen_offs)
 // qualifies. quals_out (optional) receives the goodness.
 // uniform: every edge is a candidate; otherwise the candidate kernel of
 // refine_by_size / refine_sets left "any candidate" in mailbox slot 3
+// deferred (see refine_deferred): the set is returned unchecked, and the
+// build's read-back brings its outcome and the flags
 static u32* choose_refinement(Mesh& m, u32* cand, double qual_floor, double** quals_out,
-    bool uniform)
+    bool uniform, bool deferred = false)
 {
   cudaStream_t s = m.s;
   u32 ne = m.count(1), dim = m.dim;
@@ -472,7 +542,11 @@ static u32* choose_refinement(Mesh& m, u32* cand, double qual_floor, double** qu
   // candidate": with none it settles in its first batch of rounds to the
   // empty set, and its first read-back brings the flags of mailbox slots
   // 1-3 with it (one host wait fewer per pass).
-  u32* ind = ne ? find_indset(m, 1, cand, q) : nullptr;
+  u32* ind = ne ? find_indset(m, 1, cand, q, !deferred) : nullptr;
+  if (deferred) {
+    dev_free(q, s);
+    return ind;
+  }
   if (!ne) m.mb->host[1] = m.mb->host[3] = 0;
   // choose_refinement_indset (refine_common.cpp:131-160) ghosts a parallel
   // mesh, and exchanges the edge qualities once any edge is a candidate
@@ -493,6 +567,15 @@ static u32* choose_refinement(Mesh& m, u32* cand, double qual_floor, double** qu
   return ind;
 }
 
+// The independent set's outcome need not be read back on its own: for a
+// serial mesh outside a batch (whose passes keep no ghosting state and tally
+// no segments) it comes back with the build's first read-back, one host
+// wait fewer per pass.
+static bool refine_deferred(Mesh& m)
+{
+  return m.count(1) && m.dim >= 2 && !m.parallel && !m.seg;
+}
+
 static u32 refine_common(Mesh& m, u32* cand, double qual_floor, bool uniform)
 {
   cudaStream_t s = m.s;
@@ -501,13 +584,21 @@ static u32 refine_common(Mesh& m, u32* cand, double qual_floor, bool uniform)
   st.op = 1;
   st.elems_in = m.count(m.dim);
   u32 ne = m.count(1);
-  u32* ind = choose_refinement(m, cand, qual_floor, nullptr, uniform);
+  bool const deferred = refine_deferred(m);
+  u32* ind = choose_refinement(m, cand, qual_floor, nullptr, uniform, deferred);
   if (!ind) return 0;
   seg_tally(m, 1, ind);
   u32* gen_offs = exscan_new(ind, ne, s);
   dev_free(ind, s);
-  u32 nsplit = refine_build(m, gen_offs);
+  u32 nsplit = 0;
+  try {
+    nsplit = refine_build(m, gen_offs, deferred);
+  } catch (...) {
+    dev_free(gen_offs, s);
+    throw;
+  }
   dev_free(gen_offs, s);
+  if (!nsplit) return 0;  // a deferred set that came back empty
   st.nselected = nsplit;
   st.elems_out = m.count(m.dim);
   return 1;

@@ -383,18 +383,23 @@ __global__ void k_swap_cavity(u32 ne, u32 dim, u32 const* __restrict__ ind,
 }
 
 // entities not adjacent to a swapped edge survive (swap.cpp:39-43)
-__global__ void k_swap_same(u32 n, u32 lph, u32 const* __restrict__ loh,
-    u32 const* __restrict__ ind, u32* __restrict__ same)
+// (LPH edges per entity at compile time: their loads are issued together)
+template <u32 LPH>
+__global__ void k_swap_same(u32 n, u32 const* __restrict__ loh, u32 const* __restrict__ ind,
+    u32* __restrict__ same)
 {
   pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
+  u32 e[LPH], f[LPH];
+#pragma unroll
+  for (u32 j = 0; j < LPH; ++j) e[j] = loh ? loh[(size_t)i * LPH + j] : i;
+#pragma unroll
+  for (u32 j = 0; j < LPH; ++j) f[j] = ind[e[j]];
   u32 r = 1;
-  for (u32 j = 0; j < lph; ++j)
-    if (ind[loh ? loh[(size_t)i * lph + j] : i]) {
-      r = 0;
-      break;
-    }
+#pragma unroll
+  for (u32 j = 0; j < LPH; ++j)
+    if (f[j]) r = 0;
   same[i] = r;
 }
 
@@ -455,8 +460,10 @@ struct SwapSel {
 
 // marks through the independent set (swap_slivers + swap_common,
 // swap.cpp:99-154); the optional outputs record each stage
+// deferred: no read-back here (the "any swap kept" flag and the set's
+// outcome come back with swap_build's)
 static bool swap_select(Mesh& m, double gq, u32 nlayers, SwapSel& sel, u32* slivers_out,
-    u32* cand_out, u32* interior_out)
+    u32* cand_out, u32* interior_out, bool deferred = false)
 {
   cudaStream_t s = m.s;
   ensure_swap_tables();
@@ -498,13 +505,15 @@ static bool swap_select(Mesh& m, double gq, u32 nlayers, SwapSel& sel, u32* sliv
       m.ask_down(3, 0), m.coords(), eq, m.fp32_filter ? fp32_stats_dev() : nullptr, sel.cand,
       sel.quals, sel.rs, sel.codes, any));
   CK_LAUNCH();
-  if (!read_u32(any, s)) return false;
-  sel.ind = find_indset(m, 1, sel.cand, sel.quals);
+  if (!deferred && !read_u32(any, s)) return false;
+  sel.ind = find_indset(m, 1, sel.cand, sel.quals, !deferred);
   return true;
 }
 
 // swap_interior + swap_ents (swap.cpp:27-97)
-static void swap_build(Mesh& m, SwapSel const& sel)
+// deferred: the selection's flag and the set's outcome come back with the
+// counts; with no swap kept it frees what it made and returns false
+static bool swap_build(Mesh& m, SwapSel const& sel, bool deferred)
 {
   cudaStream_t s = m.s;
   u32 ne = m.count(1), nv = m.count(0), dim = m.dim;
@@ -553,7 +562,9 @@ static void swap_build(Mesh& m, SwapSel const& sel)
     sj[nsj++] = ScanJob{cnt, gen_offs_of[ed], m.mb->dev + 20 + 2 * (ed - 1), nullptr, ne, 0};
     u32* same = dalloc<u32>(n, s);
     if (n) {
-      CK(launch_kernel(k_swap_same, dim3(grid_for(n)), dim3(BLOCK), 0, s, n, deg(ed, 1),
+      u32 const lph = deg(ed, 1);
+      auto k = lph == 1 ? k_swap_same<1> : lph == 3 ? k_swap_same<3> : k_swap_same<6>;
+      CK(launch_kernel(k, dim3(grid_for(n)), dim3(BLOCK), 0, s, n,
           ed == 1 ? nullptr : m.ask_down(ed, 1), sel.ind, same));
       CK_LAUNCH();
     }
@@ -564,7 +575,28 @@ static void swap_build(Mesh& m, SwapSel const& sel)
   }
   exscan_jobs(sj, nsj, s);
   for (u32 k = 0; k < nsj; ++k) dev_free(scan_in[k], s);
-  m.mb->fetch(s, 26);
+  m.mb->fetch(s, deferred ? INDSET_FETCH_SLOTS : 26);
+  if (deferred) {
+    auto abandon = [&] {
+      delete out;
+      for (u32 d = 0; d < 4; ++d) {
+        dev_free(same_of[d], s);
+        dev_free(gen_offs_of[d], s);
+        dev_free(newid_of[d], s);
+      }
+    };
+    try {
+      indset_check(m);
+    } catch (...) {
+      abandon();
+      throw;
+    }
+    if (!m.mb->host[6]) {  // no swap kept: the set is empty
+      abandon();
+      last_pass_stats().indset_rounds = 0;
+      return false;
+    }
+  }
   for (u32 ed = ed0; ed <= dim; ++ed) {
     u32 n = m.count(ed), vpe = deg(ed, 0);
     u32 ngen = m.mb->host[20 + 2 * (ed - 1)], nsame = m.mb->host[21 + 2 * (ed - 1)];
@@ -634,6 +666,7 @@ static void swap_build(Mesh& m, SwapSel const& sel)
   for (u32 h = 0; h <= dim; ++h) dev_free(newid_of[h], s);
   for (u32 d = 0; d < 4; ++d) dev_free(same_of[d], s);
   m.overwrite(out);
+  return true;
 }
 
 u32 swap_slivers(Mesh& m, double gq, u32 nlayers)
@@ -645,13 +678,17 @@ u32 swap_slivers(Mesh& m, double gq, u32 nlayers)
   st.elems_in = m.count(3);
   SwapSel sel;
   bool ok = false;
+  // a serial mesh outside a batch (no ghosting state, no segments to tally)
+  // reads the selection's flag and the set's outcome with the build's
+  // first read-back: two host waits fewer per pass
+  bool const deferred = !m.parallel && !m.seg;
   try {
-    ok = swap_select(m, gq, nlayers, sel, nullptr, nullptr, nullptr);
+    ok = swap_select(m, gq, nlayers, sel, nullptr, nullptr, nullptr, deferred);
     if (ok) {
       seg_tally(m, 1, sel.ind);
       st.nselected = 0;
-      swap_build(m, sel);
-      st.elems_out = m.count(3);
+      ok = swap_build(m, sel, deferred);
+      if (ok) st.elems_out = m.count(3);
     }
   } catch (...) {
     sel.free(m.s);
