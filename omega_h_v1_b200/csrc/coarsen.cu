@@ -896,6 +896,12 @@ static bool coarsen_build(Mesh& m, CoarsenSel const& sel, bool deferred)
     if (!m.mb->host[7] || !m.mb->host[4]) {  // no candidate, or no collapse kept
       abandon();
       last_pass_stats().indset_rounds = 0;
+      // check_coarsen_quality ghosts a parallel mesh and exchanges the
+      // collapse codes once any edge was a candidate
+      if (m.mb->host[7]) {
+        m.ensure_ghosting(1);
+        m.note_exchange(1);
+      }
       return false;
     }
   }
@@ -985,12 +991,13 @@ static bool coarsen_build(Mesh& m, CoarsenSel const& sel, bool deferred)
   return true;
 }
 
-// For a serial mesh outside a batch (no ghosting state, no segments to
-// tally) the selection's flags and the set's outcome come back with the
-// build's first read-back: two host waits fewer per pass.
+// The selection's flags and the set's outcome come back with the build's
+// first read-back: two host waits fewer per pass. (A parallel mesh's
+// ghosting state that depends on the flags is set after that read-back: a
+// pass that changes the mesh replaces that state anyway.)
 static bool coarsen_deferred(Mesh& m)
 {
-  return m.dim >= 2 && !m.parallel && !m.seg;
+  return m.dim >= 2;
 }
 
 static u32 coarsen_common(Mesh& m, u32* codes, double qual_floor, bool require_better)

@@ -304,7 +304,7 @@ struct Splits {
 // returns the number of split edges (read back with the domain counts).
 // deferred: the independent set's outcome comes back with the same
 // read-back; nothing to split (or a failed set) leaves the mesh unchanged.
-static u32 refine_build(Mesh& m, u32 const* gen_offs, bool deferred)
+static u32 refine_build(Mesh& m, u32 const* gen_offs, bool deferred, bool uniform)
 {
   cudaStream_t s = m.s;
   u32 dim = m.dim, src = 1;
@@ -359,6 +359,9 @@ static u32 refine_build(Mesh& m, u32 const* gen_offs, bool deferred)
     if (!m.mb->host[1]) {  // no good candidate: the set is empty
       abandon();
       last_pass_stats().indset_rounds = 0;
+      // choose_refinement_indset exchanges the edge qualities of a parallel
+      // mesh once any edge is a candidate
+      if (m.parallel && !m.seg && (uniform || m.mb->host[3])) m.note_exchange(1);
       return 0;
     }
   }
@@ -544,6 +547,7 @@ static u32* choose_refinement(Mesh& m, u32* cand, double qual_floor, double** qu
   // 1-3 with it (one host wait fewer per pass).
   u32* ind = ne ? find_indset(m, 1, cand, q, !deferred) : nullptr;
   if (deferred) {
+    if (m.parallel && !m.seg) m.ensure_ghosting(1);
     dev_free(q, s);
     return ind;
   }
@@ -567,13 +571,13 @@ static u32* choose_refinement(Mesh& m, u32* cand, double qual_floor, double** qu
   return ind;
 }
 
-// The independent set's outcome need not be read back on its own: for a
-// serial mesh outside a batch (whose passes keep no ghosting state and tally
-// no segments) it comes back with the build's first read-back, one host
-// wait fewer per pass.
+// The independent set's outcome need not be read back on its own: it comes
+// back with the build's first read-back, one host wait fewer per pass. (A
+// parallel mesh's ghosting state that depends on the flags is set after
+// that read-back: a pass that changes the mesh replaces that state anyway.)
 static bool refine_deferred(Mesh& m)
 {
-  return m.count(1) && m.dim >= 2 && !m.parallel && !m.seg;
+  return m.count(1) && m.dim >= 2;
 }
 
 static u32 refine_common(Mesh& m, u32* cand, double qual_floor, bool uniform)
@@ -592,7 +596,7 @@ static u32 refine_common(Mesh& m, u32* cand, double qual_floor, bool uniform)
   dev_free(ind, s);
   u32 nsplit = 0;
   try {
-    nsplit = refine_build(m, gen_offs, deferred);
+    nsplit = refine_build(m, gen_offs, deferred, uniform);
   } catch (...) {
     dev_free(gen_offs, s);
     throw;

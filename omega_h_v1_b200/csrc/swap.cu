@@ -678,10 +678,9 @@ u32 swap_slivers(Mesh& m, double gq, u32 nlayers)
   st.elems_in = m.count(3);
   SwapSel sel;
   bool ok = false;
-  // a serial mesh outside a batch (no ghosting state, no segments to tally)
-  // reads the selection's flag and the set's outcome with the build's
+  // the selection's flag and the set's outcome come back with the build's
   // first read-back: two host waits fewer per pass
-  bool const deferred = !m.parallel && !m.seg;
+  bool const deferred = true;
   try {
     ok = swap_select(m, gq, nlayers, sel, nullptr, nullptr, nullptr, deferred);
     if (ok) {
