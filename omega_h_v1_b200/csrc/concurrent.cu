@@ -60,6 +60,10 @@ __global__ void k_estimate_elements(u32 dim, u32 ne, u32 const* __restrict__ voe
 }
 
 constexpr double BYTES_PER_ELEMENT = 900.0;  // as the server's admission
+// a group of small meshes: at most this many estimated elements, adapted in
+// unions of at most SMALL_UNION_ELEMS current elements
+constexpr double SMALL_GROUP_ELEMS = 4.0e6;
+constexpr unsigned long long SMALL_UNION_ELEMS = 1000000ull;
 
 unsigned long long estimate_bytes(Mesh& m)
 {
@@ -101,6 +105,57 @@ void adapt_concurrent(std::vector<Mesh*> const& ms, AdaptParams const& ap, u32 n
   for (u32 i = 0; i < n; ++i) order[i] = i;
   std::stable_sort(order.begin(), order.end(),
       [&](u32 a, u32 b) { return est[a] > est[b]; });
+  // Work items, largest first: a large mesh is an item of its own; meshes
+  // estimated below the tuning table's small_mesh_elems, whose passes are
+  // all launch latency, are grouped (up to SMALL_GROUP_ELEMS estimated
+  // elements a group, each group batchable: same dimension, entities and
+  // tags) and adapted together by adapt_batch, one launch per stage for the
+  // group. Every mesh still ends exactly as osh_adapt leaves it.
+  std::vector<std::vector<u32>> items;
+  std::vector<unsigned long long> item_est;
+  {
+    double const small = tuned(TK_SMALL_MESH_ELEMS);
+    double const cap = SMALL_GROUP_ELEMS;
+    std::vector<u32> group;
+    double group_elems = 0;
+    auto close_group = [&]() {
+      if (group.empty()) return;
+      unsigned long long e = 0;
+      for (u32 k : group) e += est[k];
+      items.push_back(group);
+      item_est.push_back(e);
+      group.clear();
+      group_elems = 0;
+    };
+    for (u32 k : order) {
+      double elems = (double)est[k] / BYTES_PER_ELEMENT;
+      bool fits = elems < small;
+      if (fits && !group.empty()) {
+        try {
+          check_batchable({ms[group[0]], ms[k]});
+        } catch (Failure const&) {
+          fits = false;
+        }
+      } else if (fits) {
+        try {
+          check_batchable({ms[k]});
+        } catch (Failure const&) {
+          fits = false;
+        }
+      }
+      if (!fits) {
+        items.push_back({k});
+        item_est.push_back(est[k]);
+        continue;
+      }
+      if (group_elems + elems > cap) close_group();
+      group.push_back(k);
+      group_elems += elems;
+    }
+    close_group();
+  }
+  u32 const nitems = (u32)items.size();
+  nthreads = std::min(nthreads, nitems);
   // a mailbox shared by two of the meshes is replaced for the call: their
   // passes would otherwise read back each other's flags
   std::vector<std::shared_ptr<Mailbox>> saved_mb(n);
@@ -141,16 +196,55 @@ void adapt_concurrent(std::vector<Mesh*> const& ms, AdaptParams const& ap, u32 n
       return;
     }
     for (;;) {
-      u32 k;
+      u32 it;
       {
         std::unique_lock<std::mutex> g(mu);
         cv.wait(g, [&]() {
-          return next >= n || inflight == 0 || inflight + est[order[next]] <= budget;
+          return next >= nitems || inflight == 0 || inflight + item_est[next] <= budget;
         });
-        if (next >= n) break;
-        k = order[next++];
-        inflight += est[k];
+        if (next >= nitems) break;
+        it = next++;
+        inflight += item_est[it];
       }
+      if (items[it].size() > 1) {
+        // a group of small meshes through the batched path
+        std::vector<Mesh*> gm;
+        std::vector<cudaStream_t> orig;
+        for (u32 k : items[it]) {
+          gm.push_back(ms[k]);
+          orig.push_back(ms[k]->s);
+          if (!ms[k]->own_stream) ms[k]->s = st;
+        }
+        std::vector<BatchMeshResult> gr;
+        try {
+          adapt_batch(gm, ap.size_floor, ap.good_qual, ap.nlayers, ap.max_ops,
+              SMALL_UNION_ELEMS, gr);
+          for (size_t j = 0; j < gm.size(); ++j) res[items[it][j]] = gr[j];
+        } catch (Failure const& f) {
+          std::lock_guard<std::mutex> g(mu);
+          if (!first_error) {
+            first_error = f.code;
+            first_msg = f.what();
+          }
+        } catch (std::exception const& e) {
+          std::lock_guard<std::mutex> g(mu);
+          if (!first_error) {
+            first_error = E_CUDA;
+            first_msg = e.what();
+          }
+        }
+        for (size_t j = 0; j < gm.size(); ++j) {
+          cudaStreamSynchronize(gm[j]->s);
+          gm[j]->s = orig[j];
+        }
+        {
+          std::lock_guard<std::mutex> g(mu);
+          inflight -= item_est[it];
+        }
+        cv.notify_all();
+        continue;
+      }
+      u32 const k = items[it][0];
       Mesh& m = *ms[k];
       // a mesh on a stream of its own keeps it; one on a stream it may share
       // (the legacy default stream, a caller's stream) runs on the worker's
@@ -182,7 +276,7 @@ void adapt_concurrent(std::vector<Mesh*> const& ms, AdaptParams const& ap, u32 n
       m.s = orig;
       {
         std::lock_guard<std::mutex> g(mu);
-        inflight -= est[k];
+        inflight -= item_est[it];
       }
       cv.notify_all();
     }

@@ -20,24 +20,29 @@ namespace {
 struct TuneSpec {
   char const* name;
   u32 def;
-  u32 allowed[4];
+  u32 allowed[5];
 };
 TuneSpec const g_tune_spec[TK_NKEYS] = {
-    {"carry_group", 8, {4, 8, 16, 0}},
-    {"vert_group", 8, {4, 8, 16, 0}},
-    {"indset_vert_group", 8, {4, 8, 16, 0}},
-    {"indset_edge_group", 4, {2, 4, 8, 0}},
-    {"quality_block", 256, {64, 128, 256, 512}},
-    {"gather_block", 256, {128, 256, 512, 0}},
-    {"scan_items", 16, {8, 16, 0, 0}},
+    {"carry_group", 8, {4, 8, 16, 0, 0}},
+    {"vert_group", 8, {4, 8, 16, 0, 0}},
+    {"indset_vert_group", 8, {4, 8, 16, 0, 0}},
+    {"indset_edge_group", 4, {2, 4, 8, 0, 0}},
+    {"quality_block", 256, {64, 128, 256, 512, 0}},
+    {"gather_block", 256, {128, 256, 512, 0, 0}},
+    {"scan_items", 16, {8, 16, 0, 0, 0}},
+    {"small_mesh_elems", 0, {0, 25000, 50000, 100000, 200000}},
 };
 std::atomic<u32> g_tune[TK_NKEYS];
 std::once_flag g_tune_once;
 
 bool tune_allowed(u32 k, u32 v)
 {
-  for (u32 a : g_tune_spec[k].allowed)
-    if (a && a == v) return true;
+  // the list ends at the first 0 after its first entry (0 may be a value)
+  TuneSpec const& t = g_tune_spec[k];
+  for (u32 i = 0; i < 5; ++i) {
+    if (i > 0 && t.allowed[i] == 0) break;
+    if (t.allowed[i] == v) return true;
+  }
   return false;
 }
 

@@ -20,6 +20,9 @@ enum TuneKey : u32 {
   TK_QUALITY_BLOCK,      // threads per block, quality kernels: 64, 128, 256, 512
   TK_GATHER_BLOCK,       // threads per block, carry / search / copy kernels: 128, 256, 512
   TK_SCAN_ITEMS,         // items per thread of a 512-thread scan tile: 8, 16
+  TK_SMALL_MESH_ELEMS,   // concurrent many-mesh adapt: meshes estimated below this
+                         // many elements are adapted together in batch unions
+                         // (0: none): 0, 25000, 50000, 100000, 200000
   TK_NKEYS
 };
 u32 tuned(TuneKey k);

@@ -40,6 +40,11 @@ CANDIDATES = {
     "gather_block": (128, 256, 512),
     "scan_items": (8, 16),
 }
+# keys the single-mesh sweep does not tune (they only act in the
+# concurrent many-mesh driver): their allowed values
+OTHER_KEYS = {
+    "small_mesh_elems": (0, 25000, 50000, 100000, 200000),
+}
 
 
 def table(L):

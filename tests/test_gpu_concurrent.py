@@ -72,3 +72,22 @@ def test_concurrent_rejects_a_mesh_twice():
         G.adapt_concurrent([a, a], *ARGS)
     assert e.value.code == 4
     G.lib().osh_b200_clear_error()
+
+
+@pytest.mark.parametrize("small", [25000, 200000])
+def test_concurrent_with_small_meshes_grouped_into_unions(small):
+    """Meshes estimated below small_mesh_elems run through the batched path
+    inside the concurrent driver; each still ends as osh_adapt alone."""
+    import omega_h_v1_b200 as G
+    from omega_h_v1_b200 import tune
+    L = tune._lib(G)
+    before = tune.table(L)["small_mesh_elems"]
+    assert L.osh_b200_tuning_set(b"small_mesh_elems", small) == 0
+    try:
+        _check(_cases(14, seed=7, nmin=3, nmax=14), 3)
+        cases = [dict(n=12, seed=4, pert=0.25, size=1 / 12.),
+                 dict(n=6, seed=0, pert=0.3, size=1 / 6.),
+                 dict(n=5, seed=2, pert=0.1, size=0.08)]
+        _check(cases, 2, fields=True, parallel=True)
+    finally:
+        L.osh_b200_tuning_set(b"small_mesh_elems", before)

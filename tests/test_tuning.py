@@ -13,8 +13,8 @@ def _L():
 def test_every_key_has_its_stated_values():
     L = _L()
     names = [L.osh_b200_tuning_name(i).decode() for i in range(L.osh_b200_tuning_count())]
-    assert names == list(tune.CANDIDATES)
-    for name, values in tune.CANDIDATES.items():
+    assert names == list(tune.CANDIDATES) + list(tune.OTHER_KEYS)
+    for name, values in list(tune.CANDIDATES.items()) + list(tune.OTHER_KEYS.items()):
         v = C.c_uint()
         assert L.osh_b200_tuning_get(name.encode(), C.byref(v)) == 0
         assert v.value in values
