@@ -54,9 +54,10 @@ def recorded_traffic(probe):
         return (float(rec["bytes_per_launch"]), rec.get("command")) if rec else (None, None)
     except (OSError, ValueError, KeyError, TypeError):
         return None, None
-# the kernel whose roofline the bench line reports: the one with the largest
-# share of the adapt's time in the live probe
-DEFAULT_PROBE = "carry_up"
+# the kernel whose roofline the bench line reports: the fill of the carried
+# upward rows of edges and faces, the largest single kernel of the adapt
+# after the label copies (one launch per carried pair and pass)
+DEFAULT_PROBE = "carry_up_fill"
 
 
 def workload_config():
@@ -342,9 +343,10 @@ def run_ours(args, world, rank, local):
                 "launches": plaunch.value, "avg_launch_us": round(avg_ms * 1e3, 2),
                 "algorithmic_bytes_per_launch": round(avg_bytes),
                 "bytes_rule": "each array read once and each output written once per "
-                              "launch (count: same_l, old offsets, old rows' highs, the "
-                              "highs' new ids, new counts; fill: the same plus old "
-                              "directions, new offsets, kept uses written twice)",
+                              "launch: same_l and the old offsets 8(rows+1), the old "
+                              "rows' highs and directions 8 uses, the highs' new ids "
+                              "4 highs, the new offsets 4(rows+1), the kept uses "
+                              "written as highs and directions 8 kept",
                 "traffic": traffic,
                 "dram_frac": (round(traffic / (avg_ms / 1e3) / 1e9 / peak, 4)
                               if traffic else None),

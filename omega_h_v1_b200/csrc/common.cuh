@@ -302,10 +302,12 @@ __host__ __device__ inline double perfect_tet_quality()
 //    q_exact, which the factor (1 + 2^-20) covers; 2^-60 covers underflow
 //    of products (every edge is at least 2^-20 long by the guard below).
 //
-// The bound is evaluated with every operation rounded upward (and 1 - rho
-// downward), so it is at least the real bound. It is +inf (no decision on
-// the estimate) when lmax2 is outside [2^-40, 2^40], delta > 1/8, rho > 1/4,
-// the bound exceeds 1, or anything is not finite.
+// The bound is evaluated with every sum and product rounded upward (and
+// 1 - rho downward), and every quotient and root through div_up / sqrt_up,
+// which return a value at least the exact one, so it is at least the real
+// bound. It is +inf (no decision on the estimate) when lmax2 is outside
+// [2^-40, 2^40], S or the denominator is below 2^-120, delta > 1/8,
+// rho > 1/4, the bound exceeds 1, or anything is not finite.
 struct Q32 {
   float q;    // estimate of tet_quality
   float err;  // bound on |estimate - tet_quality in double|; +inf when none
@@ -322,6 +324,18 @@ __device__ inline float f3dot(float3 a, float3 b) { return a.x * b.x + a.y * b.y
 
 // 6 * perfect_tet_quality(), formed in double and rounded once to float
 __host__ __device__ inline float tet_k6_f32() { return (float)(6.0 * perfect_tet_quality()); }
+
+// Upper bounds of a quotient and a square root from fast operations (the
+// bound needs no correctly rounded result, only one that is not below the
+// exact value): __fdividef is within 2 ulp of a / b for b in [2^-126, 2^126]
+// (CUDA math API), so a / b <= q (1 + 8u); sqrtf is correctly rounded, so
+// sqrt(x) <= r (1 + 2u); the product is rounded upward. Callers keep b and x
+// in range (their guards).
+__device__ inline float div_up(float a, float b)
+{
+  return __fmul_ru(__fdividef(a, b), 1.0f + 8.0f * F32_U);
+}
+__device__ inline float sqrt_up(float x) { return __fmul_ru(sqrtf(x), 1.0f + 2.0f * F32_U); }
 
 __device__ inline Q32 tet_quality_f32(double const (*x)[3], float k6)
 {
@@ -347,19 +361,19 @@ __device__ inline Q32 tet_quality_f32(double const (*x)[3], float k6)
   float n0 = f3dot(d0, d0), n1 = f3dot(d1, d1), n2 = f3dot(d2, d2);
   float lmax2 = fmaxf(fmaxf(fmaxf(n0, n1), fmaxf(n2, f3dot(e12, e12))),
       fmaxf(f3dot(e13, e13), f3dot(e23, e23)));
-  if (!(lmax2 >= 0x1p-40f && lmax2 <= 0x1p40f) || !(den > 0.0f) || !(s > 0.0f) ||
+  if (!(lmax2 >= 0x1p-40f && lmax2 <= 0x1p40f) || !(den >= 0x1p-120f) || !(s >= 0x1p-120f) ||
       !isfinite(out.q))
     return out;
   float const u = F32_U;
   float eps = __fmul_ru(9.0f * u, lmax2);
   float t = __fadd_ru(__fadd_ru(__fmul_ru(7.0f * u, s),
-      __fmul_ru(__fmul_ru(4.0f, eps), __fsqrt_ru(s))), __fmul_ru(__fmul_ru(4.0f, eps), eps));
-  float delta = __fdiv_ru(t, s);
+      __fmul_ru(__fmul_ru(4.0f, eps), sqrt_up(s))), __fmul_ru(__fmul_ru(4.0f, eps), eps));
+  float delta = div_up(t, s);
   // (1 + 10u and 1 + 2u are floats; 1 + 9u and 1 + u are not)
   float rho = __fmul_ru(__fadd_ru(delta, 9.0f * u), 1.0f + 10.0f * u);
   rho = __fadd_ru(__fmul_ru(rho, 1.0f + 2.0f * u), u);
-  float e = __fdiv_ru(__fmul_ru(13.0f * u, __fsqrt_ru(__fmul_ru(__fmul_ru(n0, n1), n2))), den);
-  float b = __fdiv_ru(__fadd_ru(__fmul_ru(rho, fabsf(out.q)), e), __fadd_rd(1.0f, -rho));
+  float e = div_up(__fmul_ru(13.0f * u, sqrt_up(__fmul_ru(__fmul_ru(n0, n1), n2))), den);
+  float b = div_up(__fadd_ru(__fmul_ru(rho, fabsf(out.q)), e), __fadd_rd(1.0f, -rho));
   b = __fadd_ru(__fmul_ru(b, 1.0f + 0x1p-20f), 0x1p-60f);
   if (delta <= 0.125f && rho <= 0.25f && b <= 1.0f) out.err = b;
   return out;

@@ -22,6 +22,8 @@ PassStats& last_pass_stats()
 
 // control words of the single-launch rounds (mailbox slots 44-50)
 constexpr u32 COOP_CTL_SLOT = 44, COOP_CTL_WORDS = 7;
+// (what the rounds read back: the words below; the control words' layout
+// is given at k_indset_coop)
 static_assert(COOP_CTL_SLOT + COOP_CTL_WORDS == INDSET_FETCH_SLOTS, "mailbox slots");
 
 // also zeroes the control words of the rounds
@@ -45,26 +47,38 @@ struct Nbrs {
   u32 per;           // entities per via-entity
 };
 
-// one round of indset_at_vert (indset.cpp:55-84) for entity i: in the set
-// if no neighbour is in the set and no undecided neighbour beats it (higher
-// goodness, or equal goodness and a lower global id), out of it if a
-// neighbour is in the set, undecided otherwise. A group of G lanes (G
-// divides 32, so a group never straddles a warp) walks the entity's upward
-// entries l, l + G, ...; each lane folds its neighbours into two flags and
-// two ballots over the group combine them. The rule depends on the
-// neighbour set only, so the walk order does not matter. (One thread per
-// long row issues loads whose lanes are a row apart and fills the
-// load/store queue.)
+// indset_at_vert (indset.cpp:55-84) for entity i: out of the set if a
+// neighbour is in it; in the set if no undecided neighbour beats it (higher
+// goodness, or equal goodness and a lower global id); undecided otherwise.
+// The rounds here update one state array in place and keep a list of the
+// entities still undecided, so a round's work is the undecided entities,
+// not all of them. The set is the same as the reference's synchronous
+// rounds give: states only ever change from undecided to decided, so a
+// state read during a round is either the one of the round before or the
+// final one, and an entity that joins sees every better neighbour decided
+// out -- the lexicographically first independent set in goodness order,
+// whatever the timing. (A state read from the round before only delays a
+// decision to a later round.)
+//
+// A group of G lanes (G divides 32, so a group never straddles a warp)
+// walks the entity's upward entries l, l + G, ...; each lane folds its
+// neighbours into two flags, and two ballots over the group combine them.
+// (One thread per long row issues loads whose lanes are a row apart and
+// fills the load/store queue.)
 //
 // All rounds run in one launch: a cooperative grid (every block resident)
-// runs the rounds over a grid-stride loop, separated by a grid barrier,
-// until a round leaves no entity undecided or 100 rounds have run. Control words (zeroed by k_indset_init): [0] barrier arrivals,
-// [1] barrier generation, [2..4] "anything left" of rounds r = 0, 1, 2 mod 3
-// (round r zeroes the flag of round r + 1, last read before the barrier of
-// round r - 1 that every block has passed), [5] rounds run, [6] a barrier
-// wait gave up. States are read past L1 (another block wrote them in the
-// previous round). The barrier's wait is bounded: after COOP_SPIN_LIMIT
-// polls it sets [6] and every block leaves.
+// runs round 0 over every entity and later rounds over the list the round
+// before left, separated by a grid barrier, until a round leaves no entity
+// undecided or 100 rounds have run. Control words (zeroed by
+// k_indset_init): [0] barrier arrivals, [1] barrier generation, [2..4]
+// length of the list round r builds for round r + 1, r + 1 = 0, 1, 2 mod 3
+// (round r zeroes the counter of round r + 2, last read after the barrier
+// of round r - 2 that every block has passed), [5] rounds run, [6] a barrier
+// wait gave up. States are read past L1 (L1 may keep a line another block
+// has since rewritten; a stale undecided state would only delay the
+// decision, but a line kept stale for good would never let it end). The
+// barrier's wait is bounded: after COOP_SPIN_LIMIT polls it sets [6] and
+// every block leaves.
 constexpr u32 COOP_SPIN_LIMIT = 1u << 24;
 
 __device__ inline bool coop_barrier(u32* ctl)
@@ -94,73 +108,77 @@ __device__ inline bool coop_barrier(u32* ctl)
 }
 
 template <int G>
-__global__ void __launch_bounds__(BLOCK) k_indset_coop(u32 n, Nbrs g, u32* a, u32* b,
-    double const* __restrict__ good, u64 const* __restrict__ glob, u32* ctl)
+__global__ void __launch_bounds__(BLOCK) k_indset_coop(u32 n, Nbrs g, u32* st, u32* wl0,
+    u32* wl1, double const* __restrict__ good, u64 const* __restrict__ glob, u32* ctl)
 {
   u32 const lg = threadIdx.x % G;
   u32 const gbase = (threadIdx.x & 31) & ~(u32)(G - 1);
   u32 const gmask = (G == 32 ? 0xffffffffu : ((1u << G) - 1u)) << gbase;
+  u32 const lane = threadIdx.x & 31;
   u32 const stride = gridDim.x * blockDim.x;
   for (u32 r = 0; r < MAX_INDSET_ROUNDS; ++r) {
-    u32 const* old_st = (r % 2 == 0) ? a : b;
-    u32* st = (r % 2 == 0) ? b : a;
-    if (blockIdx.x == 0 && threadIdx.x == 0) ctl[2 + (r + 1) % 3] = 0;
-    bool left = false;
-    for (u64 t = (u64)blockIdx.x * blockDim.x + threadIdx.x; t < (u64)n * G; t += stride) {
-      u32 const i = (u32)(t / G);
-      u32 const s0 = __ldcg(&old_st[i]);
-      if (s0 != UNKNOWN) {
-        if (lg == 0) st[i] = s0;
-        continue;
-      }
-      u32 const rb = g.offs[i], re = g.offs[i + 1];
-      double const myg = good[i];
-      u64 const myid = glob ? glob[i] : (u64)i;
-      bool in_set = false, beaten = false;
-      auto visit = [&](u32 o) {
-        u32 so = __ldcg(&old_st[o]);
-        if (so == IN_SET) in_set = true;
-        if (so == NOT_IN_SET) return;
-        double og = good[o];
-        u64 oid = glob ? glob[o] : (u64)o;
-        if ((myg == og && oid < myid) || myg < og) beaten = true;
-      };
-      for (u32 j = rb + lg; j < re; j += G) {
-        if (g.mode == 0) {
-          visit(g.down[g.adj[j] * 2 + (1 - g.dirs[j])]);
-        } else {
-          u32 const* ds = g.down + (size_t)g.adj[j] * g.per;
-          for (u32 k = 0; k < g.per; ++k)
-            if (ds[k] != i) visit(ds[k]);
+    // round 0 walks every entity; round r > 0 the list round r - 1 left
+    u32 const len = r == 0 ? n : *(volatile u32*)&ctl[2 + r % 3];
+    u32 const* list = (r % 2 == 1) ? wl0 : wl1;
+    u32* next = (r % 2 == 0) ? wl0 : wl1;
+    u32* next_len = &ctl[2 + (r + 1) % 3];
+    if (blockIdx.x == 0 && threadIdx.x == 0) ctl[2 + (r + 2) % 3] = 0;
+    for (u64 t = (u64)blockIdx.x * blockDim.x + threadIdx.x; t < (u64)len * G; t += stride) {
+      u32 const i = r == 0 ? (u32)(t / G) : list[t / G];
+      u32 const s0 = __ldcg(&st[i]);
+      bool undecided = false;
+      if (s0 == UNKNOWN) {
+        u32 const rb = g.offs[i], re = g.offs[i + 1];
+        double const myg = good[i];
+        u64 const myid = glob ? glob[i] : (u64)i;
+        bool in_set = false, beaten = false;
+        auto visit = [&](u32 o) {
+          u32 so = __ldcg(&st[o]);
+          if (so == IN_SET) in_set = true;
+          if (so == NOT_IN_SET) return;
+          double og = good[o];
+          u64 oid = glob ? glob[o] : (u64)o;
+          if ((myg == og && oid < myid) || myg < og) beaten = true;
+        };
+        for (u32 j = rb + lg; j < re; j += G) {
+          if (g.mode == 0) {
+            visit(g.down[g.adj[j] * 2 + (1 - g.dirs[j])]);
+          } else {
+            u32 const* ds = g.down + (size_t)g.adj[j] * g.per;
+            for (u32 k = 0; k < g.per; ++k)
+              if (ds[k] != i) visit(ds[k]);
+          }
+        }
+        bool const any_in = (__ballot_sync(gmask, in_set) & gmask) != 0;
+        bool const lost = (__ballot_sync(gmask, beaten) & gmask) != 0;
+        if (lg == 0) {
+          if (any_in)
+            __stcg(&st[i], (u32)NOT_IN_SET);
+          else if (!lost)
+            __stcg(&st[i], (u32)IN_SET);
+          else
+            undecided = true;
         }
       }
-      bool const any_in = (__ballot_sync(gmask, in_set) & gmask) != 0;
-      bool const lost = (__ballot_sync(gmask, beaten) & gmask) != 0;
-      if (lg == 0) {
-        if (any_in) {
-          st[i] = NOT_IN_SET;
-        } else if (!lost) {
-          st[i] = IN_SET;
-        } else {
-          st[i] = UNKNOWN;
-          left = true;
-        }
+      // the undecided entities of this pass of the loop, appended to the
+      // next list: one counter update per warp
+      unsigned const act = __activemask();
+      unsigned const want = __ballot_sync(act, undecided);
+      if (want) {
+        u32 const leader = __ffs(want) - 1;
+        u32 base = 0;
+        if (lane == leader) base = atomicAdd(next_len, (u32)__popc(want));
+        base = __shfl_sync(act, base, leader);
+        if (undecided) next[base + __popc(want & ((1u << lane) - 1u))] = i;
       }
     }
-    if (__syncthreads_or(left) && threadIdx.x == 0) atomicOr(&ctl[2 + r % 3], 1u);
     __threadfence();
     if (!coop_barrier(ctl)) return;
-    if (*(volatile u32*)&ctl[2 + r % 3] == 0) {
+    if (*(volatile u32*)next_len == 0) {
       if (blockIdx.x == 0 && threadIdx.x == 0) ctl[5] = r + 1;
-      // the result always ends in a: an even round wrote b, which every
-      // block now copies its share of (b is settled: no round writes it)
-      if (r % 2 == 0)
-        for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
-          a[i] = __ldcg(&b[i]);
       return;
     }
   }
-  // 100 rounds: the last (an odd round) wrote a
   if (blockIdx.x == 0 && threadIdx.x == 0) ctl[5] = MAX_INDSET_ROUNDS;
 }
 
@@ -183,7 +201,7 @@ u32 coop_blocks()
 }
 
 template <int G>
-void launch_coop(u32 n, Nbrs const& g, u32* a, u32* b, double const* good, u64 const* glob,
+void launch_coop(u32 n, Nbrs const& g, u32* st, u32* wl, double const* good, u64 const* glob,
     u32* ctl, cudaStream_t s)
 {
   u32 blocks = std::min<u32>(grid_for((u64)n * G), coop_blocks<G>());
@@ -197,7 +215,7 @@ void launch_coop(u32 n, Nbrs const& g, u32* a, u32* b, double const* good, u64 c
   attr[0].val.cooperative = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  CK(cudaLaunchKernelEx(&cfg, k_indset_coop<G>, n, g, a, b, good, glob, ctl));
+  CK(cudaLaunchKernelEx(&cfg, k_indset_coop<G>, n, g, st, wl, wl + n, good, glob, ctl));
   CK_LAUNCH();
 }
 }  // namespace
@@ -234,12 +252,12 @@ u32* find_indset(Mesh& m, u32 ent_dim, u32 const* filter, double const* good, bo
   }
   u64 const* glob = (m.parallel && m.globals[ent_dim]) ? m.globals[ent_dim] : nullptr;
   u32* a = dalloc<u32>(n, m.s);
-  u32* b = dalloc<u32>(n, m.s);
+  u32* b = dalloc<u32>(2 * (size_t)n, m.s);  // the two lists of undecided entities
   // zeroes the control words even with no entity (rounds run = 0 then)
   CK(launch_kernel(k_indset_init, dim3(grid_for(std::max<u32>(n, COOP_CTL_WORDS))),
       dim3(BLOCK), 0, m.s, n, filter, a, m.mb->dev + COOP_CTL_SLOT));
   CK_LAUNCH();
-  // All rounds run in one cooperative launch that leaves the set in a; its
+  // All rounds run in one cooperative launch that updates a in place; its
   // control words (mailbox slots COOP_CTL_SLOT..) come back with slots 1-3,
   // which a caller that left flags there reads after this call without a
   // read-back of its own
@@ -274,7 +292,8 @@ void indset_check(Mesh& m)
   u32 rounds = hc[5];
   last_pass_stats().indset_rounds = rounds;
   // settled: no entity, or the last round left none undecided
-  bool done = rounds == 0 || hc[2 + (rounds - 1) % 3] == 0;
+  // the last round left an empty list for the round after it
+  bool done = rounds == 0 || hc[2 + rounds % 3] == 0;
   if (!done) throw Failure(E_NOCONVERGE, "independent set did not settle in 100 rounds");
 }
 
@@ -358,10 +377,10 @@ void expand_many(std::vector<ExpandJob> const& jobs, cudaStream_t s)
           2.0 * (double)pack.j[q].n * pack.j[q].width * pack.j[q].esz * pack.j[q].k;
     }
     PROBE(P_EXPAND, s, bytes);
-    // a thread per row: a grid-stride loop over several rows per thread
-    // chains their dependent loads (offsets, then the row) one after another
+    // a grid-stride loop over at most 16 blocks of 256 threads per SM
+    // (measured: a block per 256 rows was twice as slow on the 48^3 adapt)
     u32 const gb = tuned(TK_GATHER_BLOCK);
-    dim3 grid(grid_for(nmax, gb), cnt);
+    dim3 grid(std::min<u32>(grid_for(nmax, gb), 148u * 16u * 256u / gb), cnt);
     CK(launch_kernel(k_expand_many, dim3(grid), dim3(gb), 0, s, pack));
     CK_LAUNCH();
   }

@@ -1264,8 +1264,10 @@ void carry_up_fill(Mesh& m, Mesh& out, UpCarry& c)
     // each array once: same_l and the old offsets, the old rows' highs and
     // directions, the highs' new ids, the new offsets, the kept uses (first)
     // written as highs and directions
-    PROBE(P_CARRY_UP, s, 8.0 * (c.nl_old + 1) + 8.0 * c.nuses_old + 4.0 * c.nh_old +
-        4.0 * (c.nl + 1) + 8.0 * c.first);
+    // (the fill of edge and face rows, the largest single kernel of an
+    // adapt, is probed on its own: carry_up_fill)
+    PROBE(c.long_rows ? P_CARRY_UP : P_CARRY_UP_FILL, s, 8.0 * (c.nl_old + 1) +
+        8.0 * c.nuses_old + 4.0 * c.nh_old + 4.0 * (c.nl + 1) + 8.0 * c.first);
     if (c.long_rows) {
       auto kf = cg == 4 ? k_up_surv_fill_grouped<4>
               : cg == 16 ? k_up_surv_fill_grouped<16> : k_up_surv_fill_grouped<8>;

@@ -30,7 +30,7 @@ TuneSpec const g_tune_spec[TK_NKEYS] = {
     {"quality_block", 256, {64, 128, 256, 512, 0}},
     {"gather_block", 256, {128, 256, 512, 0, 0}},
     {"scan_items", 16, {8, 16, 0, 0, 0}},
-    {"small_mesh_elems", 0, {0, 25000, 50000, 100000, 200000}},
+    {"small_mesh_elems", 50000, {0, 25000, 50000, 100000, 200000}},
 };
 std::atomic<u32> g_tune[TK_NKEYS];
 std::once_flag g_tune_once;
@@ -230,7 +230,7 @@ ProbeState& probes()
 char const* const g_probe_names[P_NPROBES] = {"reflect_down", "up_count", "up_fill",
     "up_rank", "exscan", "elem_quality", "refine_candidates", "refine_quality",
     "indset_round", "coarsen_quality", "swap_quality", "refine_topology",
-    "collapse_to_ent", "expand", "carry_down", "carry_up"};
+    "collapse_to_ent", "expand", "carry_down", "carry_up", "carry_up_fill"};
 }  // namespace
 
 char const* probe_name(u32 id) { return id < P_NPROBES ? g_probe_names[id] : nullptr; }

@@ -22,7 +22,7 @@ enum TuneKey : u32 {
   TK_SCAN_ITEMS,         // items per thread of a 512-thread scan tile: 8, 16
   TK_SMALL_MESH_ELEMS,   // concurrent many-mesh adapt: meshes estimated below this
                          // many elements are adapted together in batch unions
-                         // (0: none): 0, 25000, 50000, 100000, 200000
+                         // (0: none): 0, 25000, 50000 (default), 100000, 200000
   TK_NKEYS
 };
 u32 tuned(TuneKey k);
@@ -125,6 +125,7 @@ enum ProbeId {
   P_EXPAND,
   P_CARRY,
   P_CARRY_UP,
+  P_CARRY_UP_FILL,
   P_NPROBES
 };
 char const* probe_name(u32 id);
