@@ -336,27 +336,32 @@ struct ExpandJobs {
   ExpandJob j[8];
 };
 
+template <class T>
+__device__ inline void copy_rows(void const* in, void* out, u32 i, u32 f, u32 e, u32 width)
+{
+  T const* src = static_cast<T const*>(in) + (size_t)i * width;
+  for (u32 j = f; j < e; ++j) {
+    T* dst = static_cast<T*>(out) + (size_t)j * width;
+    for (u32 c = 0; c < width; ++c) dst[c] = src[c];
+  }
+}
+
 __global__ void k_expand_many(ExpandJobs jobs)
 {
   pdl_wait();
   ExpandJob const jb = jobs.j[blockIdx.y];
-  for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < jb.n; i += gridDim.x * blockDim.x) {
+  for (u32 t = blockIdx.x * blockDim.x + threadIdx.x; t < jb.n; t += gridDim.x * blockDim.x) {
+    u32 const i = jb.list ? jb.list[t] : t;
     u32 f = jb.offs[i] * jb.k, e = jb.offs[i + 1] * jb.k;
-    for (u32 j = f; j < e; ++j) {
-      if (jb.esz == 4) {
-        u32 const* in = static_cast<u32 const*>(jb.in) + (size_t)i * jb.width;
-        u32* out = static_cast<u32*>(jb.out) + (size_t)j * jb.width;
-        for (u32 c = 0; c < jb.width; ++c) out[c] = in[c];
-      } else if (jb.esz == 8) {
-        unsigned long long const* in =
-            static_cast<unsigned long long const*>(jb.in) + (size_t)i * jb.width;
-        unsigned long long* out = static_cast<unsigned long long*>(jb.out) + (size_t)j * jb.width;
-        for (u32 c = 0; c < jb.width; ++c) out[c] = in[c];
-      } else {
-        unsigned char const* in = static_cast<unsigned char const*>(jb.in) + (size_t)i * jb.width;
-        unsigned char* out = static_cast<unsigned char*>(jb.out) + (size_t)j * jb.width;
-        for (u32 c = 0; c < jb.width; ++c) out[c] = in[c];
-      }
+    if (jb.esz == 4) {
+      copy_rows<u32>(jb.in, jb.out, i, f, e, jb.width);
+      if (jb.in2) copy_rows<u32>(jb.in2, jb.out2, i, f, e, jb.width);
+    } else if (jb.esz == 8) {
+      copy_rows<unsigned long long>(jb.in, jb.out, i, f, e, jb.width);
+      if (jb.in2) copy_rows<unsigned long long>(jb.in2, jb.out2, i, f, e, jb.width);
+    } else {
+      copy_rows<unsigned char>(jb.in, jb.out, i, f, e, jb.width);
+      if (jb.in2) copy_rows<unsigned char>(jb.in2, jb.out2, i, f, e, jb.width);
     }
   }
 }
@@ -373,8 +378,8 @@ void expand_many(std::vector<ExpandJob> const& jobs, cudaStream_t s)
     for (u32 q = 0; q < cnt; ++q) {
       pack.j[q] = live[at + q];
       nmax = std::max(nmax, pack.j[q].n);
-      bytes += 4.0 * (pack.j[q].n + 1) +
-          2.0 * (double)pack.j[q].n * pack.j[q].width * pack.j[q].esz * pack.j[q].k;
+      bytes += 4.0 * (pack.j[q].n + 1) + (pack.j[q].in2 ? 4.0 : 2.0) *
+          (double)pack.j[q].n * pack.j[q].width * pack.j[q].esz * pack.j[q].k;
     }
     PROBE(P_EXPAND, s, bytes);
     // a grid-stride loop over at most 16 blocks of 256 threads per SM
@@ -401,14 +406,21 @@ void inherit_class(Mesh& m, Mesh& out, u32 prod, Doms const& d,
   if (also) jobs = *also;
   u32* data[2] = {nullptr, nullptr};
   u32 nc[2] = {1, 1};
+  Tag* t[2] = {nullptr, nullptr};
   for (u32 q = 0; q < nnames; ++q) {
-    Tag* t = m.find_tag(prod, names[q]);
-    if (!t) throw Failure(E_ARG, std::string("missing tag ") + names[q]);
-    nc[q] = t->ncomps;
+    t[q] = m.find_tag(prod, names[q]);
+    if (!t[q]) throw Failure(E_ARG, std::string("missing tag ") + names[q]);
+    nc[q] = t[q]->ncomps;
     data[q] = dalloc<u32>((size_t)d.ngo[4] * nc[q], m.s);
-    for (u32 k = 0; k < 4; ++k) {
-      if (!d.ndoms[k] || !d.offs[k] || !d.ngen[k]) continue;
-      Tag* tk = (k == 0) ? t : m.find_tag(k, names[q]);
+  }
+  // both labels of a domain dimension in one job when they have the same
+  // width (the domain offsets are read once); a domain with a list of its
+  // producing entities walks only those
+  bool const paired = nnames == 2 && nc[0] == nc[1];
+  for (u32 k = 0; k < 4; ++k) {
+    if (!d.ndoms[k] || !d.offs[k] || !d.ngen[k]) continue;
+    for (u32 q = 0; q < nnames; ++q) {
+      Tag* tk = (k == 0) ? t[q] : m.find_tag(k, names[q]);
       if (!tk) continue;
       ExpandJob jb;
       jb.in = tk->data;
@@ -416,8 +428,21 @@ void inherit_class(Mesh& m, Mesh& out, u32 prod, Doms const& d,
       jb.out = data[q] + (size_t)d.ngo[k] * nc[q];
       jb.k = d.scale[k];
       jb.n = d.ndoms[k];
+      if (d.list[k]) {
+        jb.list = d.list[k];
+        jb.n = d.nlist[k];
+      }
       jb.width = nc[q];
       jb.esz = 4;
+      if (paired && q == 0) {
+        Tag* tk2 = (k == 0) ? t[1] : m.find_tag(k, names[1]);
+        if (tk2) {
+          jb.in2 = tk2->data;
+          jb.out2 = data[1] + (size_t)d.ngo[k] * nc[1];
+          jobs.push_back(jb);
+          break;  // the second label goes with the first
+        }
+      }
       jobs.push_back(jb);
     }
   }

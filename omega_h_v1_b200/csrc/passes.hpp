@@ -40,12 +40,17 @@ void expand_scaled(void const* in, u32 const* offs, u32 k, u32 n, u32 width,
     u32 esz, void* out, cudaStream_t s);
 
 // one row expansion (as expand_scaled); expand_many runs up to eight per
-// launch
+// launch. list (optional): the rows that produce anything, n of them (the
+// others are skipped without reading their offsets); in2 / out2 (optional):
+// a second array copied with the same offsets
 struct ExpandJob {
   void const* in = nullptr;
   u32 const* offs = nullptr;
   void* out = nullptr;
   u32 k = 1, n = 0, width = 0, esz = 4;
+  u32 const* list = nullptr;
+  void const* in2 = nullptr;
+  void* out2 = nullptr;
 };
 void expand_many(std::vector<ExpandJob> const& jobs, cudaStream_t s);
 
@@ -56,6 +61,9 @@ void expand_many(std::vector<ExpandJob> const& jobs, cudaStream_t s);
 struct Doms {
   u32 ndoms[4] = {0, 0, 0, 0};
   u32 const* offs[4] = {nullptr, nullptr, nullptr, nullptr};
+  // (optional) the domains that produce anything, in order, and their count
+  u32 const* list[4] = {nullptr, nullptr, nullptr, nullptr};
+  u32 nlist[4] = {0, 0, 0, 0};
   u32 scale[4] = {1, 1, 1, 1};
   u32 ngen[4] = {0, 0, 0, 0};  // host copy of each domain's product count
   u32 ngo[5] = {0, 0, 0, 0, 0};

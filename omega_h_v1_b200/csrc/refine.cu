@@ -298,6 +298,7 @@ struct Splits {
   u32* offs = nullptr;
   u32* dir = nullptr;
   u32* vert = nullptr;
+  u32* list = nullptr;  // the split entities, in order (nsplit of them)
   u32 nsplit = 0;
 };
 
@@ -335,7 +336,9 @@ static u32 refine_build(Mesh& m, u32 const* gen_offs, bool deferred, bool unifor
       CK_LAUNCH();
     }
     sp[dd].offs = dalloc<u32>((size_t)nd + 1, s);
-    jobs[njobs++] = ScanJob{will[dd], sp[dd].offs, m.mb->dev + 8 + dd, nullptr, nd, 0};
+    sp[dd].list = dalloc<u32>(nd ? nd : 1, s);
+    jobs[njobs++] = ScanJob{will[dd], sp[dd].offs, m.mb->dev + 8 + dd, nullptr, nd, 0,
+        sp[dd].list};
   }
   // the domains' scans in one launch
   exscan_jobs(jobs, njobs, s);
@@ -348,6 +351,7 @@ static u32 refine_build(Mesh& m, u32 const* gen_offs, bool deferred, bool unifor
         dev_free(sp[dd].offs, s);
         dev_free(sp[dd].dir, s);
         dev_free(sp[dd].vert, s);
+        dev_free(sp[dd].list, s);
       }
     };
     try {
@@ -432,6 +436,8 @@ static u32 refine_build(Mesh& m, u32 const* gen_offs, bool deferred, bool unifor
       d.offs[dd] = sp[dd].offs;
       d.scale[dd] = prods_per_dom(dd, src, prod);
       d.ngen[dd] = sp[dd].nsplit * d.scale[dd];
+      d.list[dd] = sp[dd].list;
+      d.nlist[dd] = sp[dd].nsplit;
     }
     d.ngen[0] = np - sp[prod].nsplit;
     d.finish();
@@ -502,6 +508,7 @@ static u32 refine_build(Mesh& m, u32 const* gen_offs, bool deferred, bool unifor
     dev_free(sp[dd].offs, s);
     dev_free(sp[dd].dir, s);
     dev_free(sp[dd].vert, s);
+    dev_free(sp[dd].list, s);
   }
   m.overwrite(out);
   return nsplit;

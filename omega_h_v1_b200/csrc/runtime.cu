@@ -661,6 +661,7 @@ k_exscan(ScanJobs jobs, unsigned long long* status, u32* ticket_and_err, u32 spi
   __syncthreads();
   u32* __restrict__ out = job.out;
   u32* __restrict__ newid = job.newid;
+  u32* __restrict__ list = job.list;
 #pragma unroll
   for (int k = 0; k < SCAN_ITEMS; ++k) {
     u32 li = k * SCAN_THREADS + threadIdx.x;
@@ -668,9 +669,10 @@ k_exscan(ScanJobs jobs, unsigned long long* status, u32* ticket_and_err, u32 spi
     if (gi < n) {
       u32 const o = s_buf[li + (li >> 5)];
       out[gi] = o;
-      if (newid) {
+      if (newid || list) {
         bool const on = !mode1 ? in[gi] != 0 : in[gi + 1] == in[gi];
-        newid[gi] = on ? o : INV;
+        if (newid) newid[gi] = on ? o : INV;
+        if (list && on) list[o] = (u32)gi;
       }
     }
   }

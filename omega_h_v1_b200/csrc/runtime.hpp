@@ -62,6 +62,9 @@ struct ScanJob {
   u32* newid;
   u32 n;
   u32 mode;
+  // (optional, mode 0 with 0/1 items) list[out[i]] = i where item i is 1:
+  // the marked items in order
+  u32* list = nullptr;
 };
 struct ScanJobs {
   u32 njobs;
