@@ -836,6 +836,7 @@ static bool coarsen_build(Mesh& m, CoarsenSel const& sel, bool deferred)
   // totals landing in mailbox slots 16 + 2 (ed - 1) and 17 + 2 (ed - 1), so
   // one read-back serves all dimensions
   u32* gen_offs_of[4] = {nullptr, nullptr, nullptr, nullptr};
+  u32* gen_list_of[4] = {nullptr, nullptr, nullptr, nullptr};  // the generating entities
   u32* gvert_of[4] = {nullptr, nullptr, nullptr, nullptr};
   u32* gdir_of[4] = {nullptr, nullptr, nullptr, nullptr};
   // each kept entity's new id, written by the survivors' scan for the
@@ -864,7 +865,9 @@ static bool coarsen_build(Mesh& m, CoarsenSel const& sel, bool deferred)
       CK_LAUNCH();
     }
     gen_offs_of[ed] = dalloc<u32>((size_t)n + 1, s);
-    sj[nsj++] = ScanJob{will_gen, gen_offs_of[ed], m.mb->dev + 16 + 2 * (ed - 1), nullptr, n, 0};
+    gen_list_of[ed] = dalloc<u32>(n ? n : 1, s);
+    sj[nsj++] = ScanJob{will_gen, gen_offs_of[ed], m.mb->dev + 16 + 2 * (ed - 1), nullptr, n, 0,
+        gen_list_of[ed]};
     if (carried_high(m, ed)) newid_of[ed] = dalloc<u32>(n ? n : 1, s);
     same_of[ed] = dalloc<u32>((size_t)n + 1, s);
     sj[nsj++] = ScanJob{is_same, same_of[ed], m.mb->dev + 17 + 2 * (ed - 1), newid_of[ed], n, 0};
@@ -880,6 +883,7 @@ static bool coarsen_build(Mesh& m, CoarsenSel const& sel, bool deferred)
         dev_free(fused[d], s);
         dev_free(same_of[d], s);
         dev_free(gen_offs_of[d], s);
+        dev_free(gen_list_of[d], s);
         dev_free(gvert_of[d], s);
         dev_free(gdir_of[d], s);
         dev_free(newid_of[d], s);
@@ -966,8 +970,11 @@ static bool coarsen_build(Mesh& m, CoarsenSel const& sel, bool deferred)
     d.ndoms[ed] = n;
     d.offs[ed] = gen_offs;
     d.ngen[ed] = ngen;
+    d.list[ed] = gen_list_of[ed];
+    d.nlist[ed] = ngen;
     d.finish();
     inherit_class(m, *out, ed, d);
+    dev_free(gen_list_of[ed], s);
     if (m.parallel) inherit_globals(*out, ed, nout);
     if (ed == dim) coarsen_transfer(m, *out, gen_offs_v, gen_offs, same_e, nsame, ngen);
     dev_free(gen_offs, s);
