@@ -266,11 +266,12 @@ u32* find_indset(Mesh& m, u32 ent_dim, u32 const* filter, double const* good, bo
     double nuse = (double)read_cached_uses(m, ent_dim);
     double avg_row = nuse / n;
     u32 lanes = avg_row >= 8.0 ? tuned(TK_INDSET_VERT_GROUP)
-              : avg_row >= 3.0 ? tuned(TK_INDSET_EDGE_GROUP) : 2u;
+              : avg_row >= 3.0 ? tuned(TK_INDSET_EDGE_GROUP) : 1u;
     if (lanes == 16) launch_coop<16>(n, g, a, b, good, glob, ctl, m.s);
     else if (lanes == 8) launch_coop<8>(n, g, a, b, good, glob, ctl, m.s);
     else if (lanes == 4) launch_coop<4>(n, g, a, b, good, glob, ctl, m.s);
-    else launch_coop<2>(n, g, a, b, good, glob, ctl, m.s);
+    else if (lanes == 2) launch_coop<2>(n, g, a, b, good, glob, ctl, m.s);
+    else launch_coop<1>(n, g, a, b, good, glob, ctl, m.s);
   }
   dev_free(b, m.s);
   if (check) {

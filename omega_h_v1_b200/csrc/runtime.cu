@@ -26,7 +26,7 @@ TuneSpec const g_tune_spec[TK_NKEYS] = {
     {"carry_group", 8, {4, 8, 16, 0, 0}},
     {"vert_group", 8, {4, 8, 16, 0, 0}},
     {"indset_vert_group", 8, {4, 8, 16, 0, 0}},
-    {"indset_edge_group", 4, {2, 4, 8, 0, 0}},
+    {"indset_edge_group", 1, {1, 2, 4, 8, 0}},
     {"quality_block", 256, {64, 128, 256, 512, 0}},
     {"gather_block", 256, {128, 256, 512, 0, 0}},
     {"scan_items", 16, {8, 16, 0, 0, 0}},

@@ -16,7 +16,7 @@ enum TuneKey : u32 {
   TK_CARRY_GROUP = 0,    // lanes per long carried upward row: 4, 8, 16
   TK_VERT_GROUP,         // lanes per vertex row, coarsening vertex kernels: 4, 8, 16
   TK_INDSET_VERT_GROUP,  // lanes per vertex, independent-set rounds: 4, 8, 16
-  TK_INDSET_EDGE_GROUP,  // lanes per edge (3D), independent-set rounds: 2, 4, 8
+  TK_INDSET_EDGE_GROUP,  // lanes per edge (3D), independent-set rounds: 1, 2, 4, 8
   TK_QUALITY_BLOCK,      // threads per block, quality kernels: 64, 128, 256, 512
   TK_GATHER_BLOCK,       // threads per block, carry / search / copy kernels: 128, 256, 512
   TK_SCAN_ITEMS,         // items per thread of a 512-thread scan tile: 8, 16

@@ -35,7 +35,7 @@ CANDIDATES = {
     "carry_group": (4, 8, 16),
     "vert_group": (4, 8, 16),
     "indset_vert_group": (4, 8, 16),
-    "indset_edge_group": (2, 4, 8),
+    "indset_edge_group": (1, 2, 4, 8),
     "quality_block": (64, 128, 256, 512),
     "gather_block": (128, 256, 512),
     "scan_items": (8, 16),
