@@ -307,6 +307,15 @@ void osh_b200_host_stats(unsigned long long* allocs, double* sync_wait_seconds) 
    expected result), 0 if it did not, or another error code; the device
    stays usable afterwards. */
 int osh_b200_selftest_scan_wait(unsigned spin_limit) OSH_PUBLIC;
+/* the passes' exclusive scan over device arrays (replaces uints_exscan,
+   ints.cpp:45-59, a Thrust scan there): out[0..n] with out[0] = 0 and
+   out[n] the total of in[0..n), 32-bit wrap-around sums, queued on `stream`
+   (a cudaStream_t; 0 is the legacy default stream). With check != 0 the
+   call waits for the stream and returns OSH_B200_E_TIMEOUT if a bounded
+   look-back wait gave up; with check == 0 it returns once the scan is
+   queued. in and out may not overlap. Returns 0 or an error code. */
+int osh_b200_exscan_u32(unsigned const* in, unsigned* out, unsigned n, void* stream,
+    int check) OSH_PUBLIC;
 /* run all further work of mesh m on the CUDA stream `stream` (a
    cudaStream_t; 0 is the legacy default stream); the caller keeps it alive */
 void osh_b200_set_stream(osh_t m, void* stream) OSH_PUBLIC;

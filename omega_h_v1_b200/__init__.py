@@ -163,6 +163,7 @@ def lib():
     f("osh_b200_fp32_probe_edges", None, C.c_uint, _f64p, _f64p, C.c_double,
       np.ctypeslib.ndpointer(np.int32), _f64p)
     f("osh_b200_selftest_scan_wait", C.c_int, C.c_uint)
+    f("osh_b200_exscan_u32", C.c_int, vp, vp, C.c_uint, vp, C.c_int)
     f("osh_b200_server_new", vp, C.c_double, C.c_double, C.c_uint, C.c_uint, C.c_ulonglong)
     f("osh_b200_server_free", None, vp)
     f("osh_b200_server_submit", C.c_int, vp, C.c_uint, C.c_uint, _f64p, C.c_uint, _u32p, _f64p)

@@ -1182,6 +1182,19 @@ int osh_b200_selftest_scan_wait(unsigned spin_limit)
   API_CATCH(osh::last_error())
 }
 
+int osh_b200_exscan_u32(unsigned const* in, unsigned* out, unsigned n, void* stream, int check)
+{
+  API_TRY
+  need(out != nullptr && (in != nullptr || n == 0), "exscan: null array");
+  uintptr_t const a = reinterpret_cast<uintptr_t>(in), b = reinterpret_cast<uintptr_t>(out);
+  need(n == 0 || b + 4ull * ((u64)n + 1) <= a || a + 4ull * n <= b, "exscan: in and out overlap");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  osh::exscan_u32(in, out, n, s, nullptr, nullptr);
+  if (check) osh::check_device_timeouts(s);
+  return 0;
+  API_CATCH(osh::last_error())
+}
+
 void osh_b200_set_stream(osh_t h, void* stream)
 {
   API_TRY

@@ -8,6 +8,7 @@
 // That is exactly the neighbour set of the reference's star(1,3) /
 // star(0,1) (star.cpp:135-293); the selection rule depends only on that set.
 #include <algorithm>
+#include <atomic>
 #include <vector>
 
 #include "passes.hpp"
@@ -107,8 +108,10 @@ __device__ inline bool coop_barrier(u32* ctl)
   return *(volatile u32*)&ctl[6] == 0;
 }
 
+// (at least 4 blocks per SM: without a minimum the compiler held the
+// kernel to 32 registers and spilled)
 template <int G>
-__global__ void __launch_bounds__(BLOCK) k_indset_coop(u32 n, Nbrs g, u32* st, u32* wl0,
+__global__ void __launch_bounds__(BLOCK, 4) k_indset_coop(u32 n, Nbrs g, u32* st, u32* wl0,
     u32* wl1, double const* __restrict__ good, u64 const* __restrict__ glob, u32* ctl)
 {
   u32 const lg = threadIdx.x % G;
@@ -183,21 +186,26 @@ __global__ void __launch_bounds__(BLOCK) k_indset_coop(u32 n, Nbrs g, u32* st, u
 }
 
 namespace {
-// resident blocks of BLOCK threads a cooperative launch may use on this device
+// blocks of BLOCK threads a cooperative launch uses on this device: the
+// tuning table's indset_blocks per SM, at most as many as are resident
 template <int G>
 u32 coop_blocks()
 {
-  static u32 cached[64] = {};
+  static std::atomic<u32> per_sm_of[64];
+  static std::atomic<u32> sms_of[64];
   int dev = 0;
   CK(cudaGetDevice(&dev));
   if (dev < 0 || dev >= 64) return 0;
-  if (!cached[dev]) {
+  if (!sms_of[dev].load()) {
     int per_sm = 0, sms = 0;
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_indset_coop<G>, BLOCK, 0));
     CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    cached[dev] = (u32)(per_sm * sms);
+    per_sm_of[dev].store((u32)per_sm);
+    sms_of[dev].store((u32)sms);
   }
-  return cached[dev];
+  u32 per_sm = per_sm_of[dev].load(), want = tuned(TK_INDSET_BLOCKS);
+  if (want && want < per_sm) per_sm = want;
+  return per_sm * sms_of[dev].load();
 }
 
 template <int G>

@@ -575,9 +575,18 @@ void up_from_down(u32 high, u32 low, u32 nhighs, u32 nlows, u32 const* loh,
 
 // reflect_down_entity / find_by_verts (reflect_down.cpp:13-38,
 // find_by_verts.hpp:14-76): the low entity with the wanted vertices is
-// unique, so it is found in the row of its smallest vertex, where every low
-// entity is listed once with its other vertices (half the records of the
-// vertices' upward adjacency, and one contiguous row to scan).
+// unique, so it is found among the entities that share its smallest vertex,
+// where every low entity is listed once with its other vertices. Each
+// vertex's entities are split over SUB sub-rows by a hash of their other
+// vertices (4 for edges, 8 for triangles), so a search reads about 1/SUB of
+// the vertex's row: the vertices a refinement left with the lowest ids are
+// the smallest vertex of most entities around them, and a single
+// tet-to-triangle search of a refined 2M-tet mesh took 254 us scanning their
+// whole rows. Consecutive entities mostly share their smallest vertex, so
+// the fill's writes stay close together (a hash of the whole tuple over all
+// buckets scattered them and made the fill slower than the search it
+// saved). A row's order does not matter: a search reads a whole sub-row and
+// the key is unique.
 
 __device__ inline void sort_small(u32* w, u32 n)
 {
@@ -589,39 +598,67 @@ __device__ inline void sort_small(u32* w, u32 n)
     }
 }
 
-__global__ void k_count_min_vert(u32 low, u32 nl, u32 const* __restrict__ vol, u32* cnt)
+template <u32 VPL>
+struct KeyRows {
+  static constexpr u32 SUB = VPL == 2 ? 4 : 8;
+};
+
+// sub-row of a sorted tuple: its smallest vertex's SUB sub-rows, picked by
+// murmur3's 32-bit finaliser over the other vertices
+template <u32 VPL>
+__device__ inline u32 key_row(u32 const* w)
+{
+  u32 h = w[1] * 0x9e3779b1u + (VPL == 3 ? w[2] * 0x85ebca77u : 0u);
+  h ^= h >> 16;
+  h *= 0x85ebca6bu;
+  h ^= h >> 13;
+  h *= 0xc2b2ae35u;
+  h ^= h >> 16;
+  return w[0] * KeyRows<VPL>::SUB + (h & (KeyRows<VPL>::SUB - 1));
+}
+
+template <u32 VPL>
+__device__ inline void low_key(u32 const* __restrict__ vol, u32 i, u32* w)
+{
+#pragma unroll
+  for (u32 k = 0; k < VPL; ++k) w[k] = vol[(size_t)i * VPL + k];
+  sort_small(w, VPL);
+}
+
+template <u32 VPL>
+__global__ void k_count_key_rows(u32 nl, u32 const* __restrict__ vol, u32* cnt)
 {
   pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nl) return;
-  u32 vpl = low + 1, m = vol[(size_t)i * vpl];
-  for (u32 k = 1; k < vpl; ++k) m = min(m, vol[(size_t)i * vpl + k]);
-  atomicAdd(&cnt[m], 1u);
+  u32 w[VPL];
+  low_key<VPL>(vol, i, w);
+  atomicAdd(&cnt[key_row<VPL>(w)], 1u);
 }
 
-// cnt holds each vertex's row count; a row's records take its slots from the
-// end down (the search reads a whole row, so their order does not matter)
-__global__ void k_fill_min_vert(u32 low, u32 nl, u32 const* __restrict__ vol,
+// cnt holds each sub-row's count; a row's records take its slots from the
+// end down: uint2 {v1, id} for edges, uint4 {v1, v2, id, 0} for triangles
+template <u32 VPL>
+__global__ void k_fill_key_rows(u32 nl, u32 const* __restrict__ vol,
     u32 const* __restrict__ offs, u32* cnt, u32* __restrict__ rows)
 {
   pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nl) return;
-  u32 vpl = low + 1, w[3];
-  for (u32 k = 0; k < vpl; ++k) w[k] = vol[(size_t)i * vpl + k];
-  sort_small(w, vpl);
-  u32 slot = offs[w[0]] + atomicSub(&cnt[w[0]], 1u) - 1u;
-  if (low == 1)
+  u32 w[VPL];
+  low_key<VPL>(vol, i, w);
+  u32 b = key_row<VPL>(w);
+  u32 slot = offs[b] + atomicSub(&cnt[b], 1u) - 1u;
+  if (VPL == 2)
     reinterpret_cast<uint2*>(rows)[slot] = make_uint2(w[1], i);
   else
-    reinterpret_cast<uint4*>(rows)[slot] = make_uint4(w[1], w[2], i, 0u);
+    reinterpret_cast<uint4*>(rows)[slot] = make_uint4(w[1], w[VPL - 1], i, 0u);
 }
 
-// One thread per high entity: its low entities are looked up grouped by
-// their smallest vertex, so each row is scanned once for every wanted entity
-// it holds (a tet's four triangles live in two rows, its six edges in three).
+// One thread per high entity: every wanted low's sub-row bounds are loaded
+// together, then each sub-row is read four records at a time.
 template <u32 HIGH, u32 LOW>
-__global__ void k_reflect_grouped(u32 first, u32 nh, u32 const* __restrict__ voh,
+__global__ void k_reflect_keyed(u32 first, u32 nh, u32 const* __restrict__ voh,
     u32 const* __restrict__ offs, u32 const* __restrict__ rows, u32* __restrict__ out)
 {
   pdl_wait();
@@ -632,51 +669,44 @@ __global__ void k_reflect_grouped(u32 first, u32 nh, u32 const* __restrict__ voh
   u32 v[VPH];
 #pragma unroll
   for (u32 k = 0; k < VPH; ++k) v[k] = voh[(size_t)i * VPH + k];
-  u32 t[LPH][VPL], found[LPH];
+  u32 t[LPH][VPL], f[LPH], e[LPH];
 #pragma unroll
   for (u32 j = 0; j < LPH; ++j) {
 #pragma unroll
     for (u32 k = 0; k < VPL; ++k) t[j][k] = v[canon(HIGH, LOW, 0, j, k)];
     sort_small(t[j], VPL);
-    found[j] = INV;
   }
 #pragma unroll
   for (u32 j = 0; j < LPH; ++j) {
-    if (found[j] != INV) continue;
-    u32 m = t[j][0];
-    u32 f = offs[m], e = offs[m + 1];
-    bool pending = true;
-    for (u32 k = f; k < e && pending; k += 4) {
+    u32 b = key_row<VPL>(t[j]);
+    f[j] = offs[b];
+    e[j] = offs[b + 1];
+  }
+#pragma unroll
+  for (u32 j = 0; j < LPH; ++j) {
+    u32 found = INV;
+    for (u32 k = f[j]; k < e[j] && found == INV; k += 4) {
       if (LOW == 1) {
         uint2 x[4];
         uint2 const* r = reinterpret_cast<uint2 const*>(rows);
 #pragma unroll
-        for (u32 q = 0; q < 4; ++q) x[q] = k + q < e ? __ldg(r + k + q) : make_uint2(INV, INV);
+        for (u32 q = 0; q < 4; ++q) x[q] = k + q < e[j] ? __ldg(r + k + q) : make_uint2(INV, INV);
 #pragma unroll
         for (u32 q = 0; q < 4; ++q)
-#pragma unroll
-          for (u32 l = j; l < LPH; ++l)
-            if (found[l] == INV && t[l][0] == m && x[q].x == t[l][1]) found[l] = x[q].y;
+          if (x[q].x == t[j][1]) found = x[q].y;
       } else {
         uint4 x[4];
         uint4 const* r = reinterpret_cast<uint4 const*>(rows);
 #pragma unroll
         for (u32 q = 0; q < 4; ++q)
-          x[q] = k + q < e ? __ldg(r + k + q) : make_uint4(INV, INV, INV, INV);
+          x[q] = k + q < e[j] ? __ldg(r + k + q) : make_uint4(INV, INV, INV, INV);
 #pragma unroll
         for (u32 q = 0; q < 4; ++q)
-#pragma unroll
-          for (u32 l = j; l < LPH; ++l)
-            if (found[l] == INV && t[l][0] == m && x[q].x == t[l][1] && x[q].y == t[l][2])
-              found[l] = x[q].z;
+          if (x[q].x == t[j][1] && x[q].y == t[j][VPL - 1]) found = x[q].z;
       }
-      pending = false;
-#pragma unroll
-      for (u32 l = j; l < LPH; ++l) pending = pending || (found[l] == INV && t[l][0] == m);
     }
+    out[(size_t)i * LPH + j] = found;
   }
-#pragma unroll
-  for (u32 j = 0; j < LPH; ++j) out[(size_t)i * LPH + j] = found[j];
 }
 
 // ---------------------------------------------------------------------------
@@ -883,17 +913,21 @@ void Mesh::build_low_rows(u32 low)
 {
   if (low_rows[low]) return;
   u32 const* vol = ask_down(low, 0);
-  u32 nl = counts[low], nv = counts[0];
-  u32* cnt = dalloc<u32>((size_t)nv + 1, s);
-  CK(cudaMemsetAsync(cnt, 0, sizeof(u32) * ((size_t)nv + 1), s));
+  u32 nl = counts[low];
+  size_t nb = (size_t)counts[0] * (low == 1 ? KeyRows<2>::SUB : KeyRows<3>::SUB);
+  if (nb >= 0xffffffffull) throw Failure(E_ARG, "reflect_down: too many vertices");
+  u32* cnt = dalloc<u32>(nb + 1, s);
+  CK(cudaMemsetAsync(cnt, 0, sizeof(u32) * (nb + 1), s));
   if (nl) {
-    CK(launch_kernel(k_count_min_vert, dim3(grid_for(nl)), dim3(BLOCK), 0, s, low, nl, vol, cnt));
+    auto k = low == 1 ? k_count_key_rows<2> : k_count_key_rows<3>;
+    CK(launch_kernel(k, dim3(grid_for(nl)), dim3(BLOCK), 0, s, nl, vol, cnt));
     CK_LAUNCH();
   }
-  low_row_offs[low] = exscan_new(cnt, nv, s);
+  low_row_offs[low] = exscan_new(cnt, (u32)nb, s);
   low_rows[low] = dalloc<u32>((size_t)nl * (low == 1 ? 2 : 4), s);
   if (nl) {
-    CK(launch_kernel(k_fill_min_vert, dim3(grid_for(nl)), dim3(BLOCK), 0, s, low, nl, vol, low_row_offs[low], cnt,
+    auto k = low == 1 ? k_fill_key_rows<2> : k_fill_key_rows<3>;
+    CK(launch_kernel(k, dim3(grid_for(nl)), dim3(BLOCK), 0, s, nl, vol, low_row_offs[low], cnt,
         low_rows[low]));
     CK_LAUNCH();
   }
@@ -906,17 +940,17 @@ void Mesh::reflect_range(u32 high, u32 low, u32 first, u32* out)
   if (first >= nh) return;
   u32 const* voh = ask_down(high, 0);
   build_low_rows(low);
-  u32 nl = counts[low], n = (nh - first) * deg(high, low);
-  // voh once, the row offsets and every row record once, out once
-  double nld = nl, rec = low == 1 ? 8.0 : 16.0;
-  PROBE(P_REFLECT_DOWN, s, 4.0 * deg(high, 0) * (nh - first) + 4.0 * (counts[0] + 1.0) +
-      rec * nld + 4.0 * n);
+  u32 n = (nh - first) * deg(high, low);
+  // voh once, each wanted low's sub-row bounds and its records (a few of
+  // 8 / 16 bytes) once, out once
+  double rec = low == 1 ? 8.0 : 16.0;
+  PROBE(P_REFLECT_DOWN, s, 4.0 * deg(high, 0) * (nh - first) + (8.0 + 4.0 * rec) * n + 4.0 * n);
   u32 const gb = tuned(TK_GATHER_BLOCK);
   u32 g = grid_for(nh - first, gb);
-  auto k = high == 3 && low == 2 ? k_reflect_grouped<3, 2>
-         : high == 3 ? k_reflect_grouped<3, 1> : k_reflect_grouped<2, 1>;
-  CK(launch_kernel(k, dim3(g), dim3(gb), 0, s, first, nh, voh, low_row_offs[low], low_rows[low],
-      out));
+  auto k = high == 3 && low == 2 ? k_reflect_keyed<3, 2>
+         : high == 3 ? k_reflect_keyed<3, 1> : k_reflect_keyed<2, 1>;
+  CK(launch_kernel(k, dim3(g), dim3(gb), 0, s, first, nh, voh, low_row_offs[low],
+      low_rows[low], out));
   CK_LAUNCH();
 }
 

@@ -80,7 +80,8 @@ struct Mesh {
   bool have_star[4][4] = {};
   u32* dual = nullptr;
   // reflect_down's search rows: every edge (1) / triangle (2) listed once, in
-  // the row of its smallest vertex, as (other vertices..., id) records:
+  // one of its smallest vertex's sub-rows (4 / 8 per vertex, picked by a
+  // hash of its other vertices), as (other vertices..., id) records:
   // uint2 {v1, id} for edges, uint4 {v1, v2, id, 0} for triangles
   u32* low_row_offs[3] = {nullptr, nullptr, nullptr};
   u32* low_rows[3] = {nullptr, nullptr, nullptr};

@@ -26,10 +26,12 @@ TuneSpec const g_tune_spec[TK_NKEYS] = {
     {"carry_group", 8, {4, 8, 16, 0, 0}},
     {"vert_group", 8, {4, 8, 16, 0, 0}},
     {"indset_vert_group", 8, {4, 8, 16, 0, 0}},
-    {"indset_edge_group", 1, {1, 2, 4, 8, 0}},
+    {"indset_edge_group", 4, {1, 2, 4, 8, 0}},
     {"quality_block", 256, {64, 128, 256, 512, 0}},
     {"gather_block", 256, {128, 256, 512, 0, 0}},
     {"scan_items", 16, {8, 16, 0, 0, 0}},
+    {"scan_threads", 512, {256, 512, 0, 0, 0}},
+    {"indset_blocks", 0, {0, 1, 2, 4, 0}},
     {"small_mesh_elems", 50000, {0, 25000, 50000, 100000, 200000}},
 };
 std::atomic<u32> g_tune[TK_NKEYS];
@@ -527,14 +529,13 @@ void Mailbox::fetch(cudaStream_t s, u32 nslots)
 // the host reads for that stream (check_device_timeouts), and stops instead
 // of spinning forever.
 
-// 8192-element tiles: a 2M-element scan has 256 tiles, so a tile's
-// look-back meets a published prefix within a few steps (with 2048-element
-// tiles the chain of look-backs, not bandwidth, set the time)
-constexpr int SCAN_THREADS = 512;
-// items per thread: the tuning table's scan_items (8 or 16); scratch is
-// sized for the smaller tile, so either fits
-constexpr int SCAN_MIN_TILE = SCAN_THREADS * 8;
-constexpr int SCAN_WARPS = SCAN_THREADS / 32;
+// Tiles of SCAN_T threads (the tuning table's scan_threads, 256 or 512)
+// times SCAN_ITEMS items (scan_items, 8 or 16). With 8192-element tiles a
+// 2M-element scan has 256 tiles, so a tile's look-back meets a published
+// prefix within a few steps (with 2048-element tiles the chain of
+// look-backs, not bandwidth, set the time of the adapt's scans). Scratch
+// is sized for the smallest tile, so every shape fits.
+constexpr int SCAN_MIN_TILE = 256 * 8;
 constexpr unsigned long long FLAG_AGG = 1ull << 62;
 constexpr unsigned long long FLAG_PRE = 2ull << 62;
 constexpr u32 SCAN_SPIN_LIMIT = 1u << 24;
@@ -549,11 +550,12 @@ constexpr u32 SCAN_SPIN_LIMIT = 1u << 24;
 // claimed through one ticket, so a look-back, which stops at its job's
 // first tile, only waits on tiles claimed before it. Independent scans of a
 // pass share a launch, and their look-back chains overlap.
-template <int SCAN_ITEMS>
-__global__ void __launch_bounds__(SCAN_THREADS)
+template <int SCAN_T, int SCAN_ITEMS>
+__global__ void __launch_bounds__(SCAN_T)
 k_exscan(ScanJobs jobs, unsigned long long* status, u32* ticket_and_err, u32 spin_limit)
 {
   pdl_wait();
+  constexpr int SCAN_THREADS = SCAN_T, SCAN_WARPS = SCAN_T / 32;
   __shared__ u32 s_tile;
   __shared__ u32 s_warp[SCAN_WARPS];
   __shared__ u32 s_prefix;
@@ -749,21 +751,31 @@ u32* stream_scan_scratch(size_t words, cudaStream_t s)
 
 namespace {
 // tiles of a job (one at least: an empty scan still writes out[0] = 0)
-u32 job_tiles(u32 n, u32 items) { return n ? ceil_div(n, (u64)SCAN_THREADS * items) : 1u; }
+u32 job_tiles(u32 n, u32 tile) { return n ? ceil_div(n, (u64)tile) : 1u; }
 
-void launch_scan_jobs(ScanJobs const& jobs, u32 items, u32* scratch, u32 spin_limit,
+// a tile's shape: threads (256 or 512) x items per thread (8 or 16)
+struct ScanShape {
+  u32 threads, items;
+  u32 tile() const { return threads * items; }
+};
+ScanShape tuned_scan_shape() { return {tuned(TK_SCAN_THREADS), tuned(TK_SCAN_ITEMS)}; }
+
+void launch_scan_jobs(ScanJobs const& jobs, ScanShape sh, u32* scratch, u32 spin_limit,
     cudaStream_t s)
 {
   u32 const ntiles = jobs.tile0[jobs.njobs];
-  CK(launch_kernel(items == 8 ? k_exscan<8> : k_exscan<16>, dim3(ntiles), dim3(SCAN_THREADS),
-      0, s, jobs, reinterpret_cast<unsigned long long*>(scratch + 4), scratch, spin_limit));
+  auto k = sh.threads == 256 ? (sh.items == 8 ? k_exscan<256, 8> : k_exscan<256, 16>)
+                             : (sh.items == 8 ? k_exscan<512, 8> : k_exscan<512, 16>);
+  CK(launch_kernel(k, dim3(ntiles), dim3(sh.threads), 0, s, jobs,
+      reinterpret_cast<unsigned long long*>(scratch + 4), scratch, spin_limit));
   CK_LAUNCH();
 }
 }  // namespace
 
 void exscan_jobs(ScanJob const* jobs, u32 njobs, cudaStream_t s)
 {
-  u32 const items = tuned(TK_SCAN_ITEMS);
+  ScanShape const sh = tuned_scan_shape();
+  u32 const tile = sh.tile();
   for (u32 at = 0; at < njobs; at += MAX_SCAN_JOBS) {
     ScanJobs pack;
     pack.njobs = std::min<u32>(MAX_SCAN_JOBS, njobs - at);
@@ -771,13 +783,13 @@ void exscan_jobs(ScanJob const* jobs, u32 njobs, cudaStream_t s)
     double bytes = 0;
     for (u32 q = 0; q < pack.njobs; ++q) {
       pack.j[q] = jobs[at + q];
-      pack.tile0[q + 1] = pack.tile0[q] + job_tiles(pack.j[q].n, items);
+      pack.tile0[q + 1] = pack.tile0[q] + job_tiles(pack.j[q].n, tile);
       bytes += 8.0 * pack.j[q].n + 4.0 + (pack.j[q].newid ? 4.0 * pack.j[q].n : 0.0);
     }
     // [ticket, error, done, pad][status per tile], zero on entry
     u32* scratch = stream_scan_scratch(4 + 2 * (size_t)pack.tile0[pack.njobs], s);
     PROBE(P_EXSCAN, s, bytes);
-    launch_scan_jobs(pack, items, scratch, SCAN_SPIN_LIMIT, s);
+    launch_scan_jobs(pack, sh, scratch, SCAN_SPIN_LIMIT, s);
   }
 }
 
@@ -819,7 +831,7 @@ int selftest_scan_wait(u32 spin_limit)
   // gone by; the block that takes ticket 2 has no tile and returns.
   cudaStream_t s = nullptr;
   CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
-  u32 const n = 2 * SCAN_THREADS * 16, ntiles = 2;
+  u32 const n = 2 * 512 * 16, ntiles = 2;
   size_t words = (size_t)(n + 1) * 2 + 4 + 2 * ntiles + 4;  // + alignment room
   u32* buf = nullptr;
   CK(cudaMalloc(&buf, words * sizeof(u32)));
@@ -835,7 +847,7 @@ int selftest_scan_wait(u32 spin_limit)
   pack.tile0[0] = 0;
   pack.tile0[1] = ntiles;
   pack.j[0] = ScanJob{in, out, nullptr, nullptr, n, 0};
-  launch_scan_jobs(pack, 16, scratch, spin_limit, s);
+  launch_scan_jobs(pack, ScanShape{512, 16}, scratch, spin_limit, s);
   u32 err = 0;
   CK(cudaMemcpyAsync(&err, scratch + 1, sizeof(u32), cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
@@ -853,14 +865,14 @@ void exscan_u32_scratch(u32 const* in, u32* out, u32 n, u32* scratch, cudaStream
 {
   if (reinterpret_cast<uintptr_t>(scratch) % 16 != 0)
     throw Failure(E_ARG, "scan scratch must start on a 16-byte boundary");
-  u32 const items = tuned(TK_SCAN_ITEMS);
+  ScanShape const sh = tuned_scan_shape();
   CK(cudaMemsetAsync(scratch, 0, exscan_scratch_words(n) * sizeof(u32), s));
   ScanJobs pack;
   pack.njobs = 1;
   pack.tile0[0] = 0;
-  pack.tile0[1] = job_tiles(n, items);
+  pack.tile0[1] = job_tiles(n, sh.tile());
   pack.j[0] = ScanJob{in, out, nullptr, nullptr, n, 0};
-  launch_scan_jobs(pack, items, scratch, SCAN_SPIN_LIMIT, s);
+  launch_scan_jobs(pack, sh, scratch, SCAN_SPIN_LIMIT, s);
 }
 
 u32* exscan_new(u32 const* in, u32 n, cudaStream_t s, u32* total_to, u32* newid)

@@ -19,7 +19,11 @@ enum TuneKey : u32 {
   TK_INDSET_EDGE_GROUP,  // lanes per edge (3D), independent-set rounds: 1, 2, 4, 8
   TK_QUALITY_BLOCK,      // threads per block, quality kernels: 64, 128, 256, 512
   TK_GATHER_BLOCK,       // threads per block, carry / search / copy kernels: 128, 256, 512
-  TK_SCAN_ITEMS,         // items per thread of a 512-thread scan tile: 8, 16
+  TK_SCAN_ITEMS,         // items per thread of a scan tile: 8, 16
+  TK_SCAN_THREADS,       // threads per scan tile: 256, 512
+  TK_INDSET_BLOCKS,      // blocks per SM of the one-launch independent set (each
+                         // round ends in a grid barrier that every block joins;
+                         // 0: as many as fit): 0, 1, 2, 4
   TK_SMALL_MESH_ELEMS,   // concurrent many-mesh adapt: meshes estimated below this
                          // many elements are adapted together in batch unions
                          // (0: none): 0, 25000, 50000 (default), 100000, 200000

@@ -39,6 +39,8 @@ CANDIDATES = {
     "quality_block": (64, 128, 256, 512),
     "gather_block": (128, 256, 512),
     "scan_items": (8, 16),
+    "scan_threads": (256, 512),
+    "indset_blocks": (0, 1, 2, 4),
 }
 # keys the single-mesh sweep does not tune (they only act in the
 # concurrent many-mesh driver): their allowed values
