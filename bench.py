@@ -346,7 +346,9 @@ def run_ours(args, world, rank, local):
                               "launch: same_l and the old offsets 8(rows+1), the old "
                               "rows' highs and directions 8 uses, the highs' new ids "
                               "4 highs, the new offsets 4(rows+1), the kept uses "
-                              "written as highs and directions 8 kept",
+                              "written as highs and directions 8 kept, and per use "
+                              "of the entities the pass made (filled in the same "
+                              "launch) its low, the row's count and the use written 20",
                 "traffic": traffic,
                 "dram_frac": (round(traffic / (avg_ms / 1e3) / 1e9 / peak, 4)
                               if traffic else None),

@@ -149,7 +149,8 @@ __device__ inline float warp_minf(float v)
   return v;
 }
 
-__global__ void k_coarsen_quality(u32 dim, u32 const* __restrict__ list,
+template <u32 DIM>
+__global__ void k_coarsen_quality(u32 const* __restrict__ list,
     u32 const* __restrict__ nlist, u32 const* __restrict__ voe1, u32 const* __restrict__ voe,
     u32 const* __restrict__ ev_offs, u32 const* __restrict__ ev,
     u32 const* __restrict__ ev_dirs, double const* __restrict__ x,
@@ -157,9 +158,10 @@ __global__ void k_coarsen_quality(u32 dim, u32 const* __restrict__ list,
     u32* __restrict__ codes, double* __restrict__ out, u32* any)
 {
   pdl_wait();
+  constexpr u32 dim = DIM;  // element dimension: corner loops unroll into registers
   u32 lane = threadIdx.x & 31;
   u32 n = *nlist;
-  u32 vpe = deg(dim, 0);
+  constexpr u32 vpe = deg(dim, 0);
   double const perfect = dim == 3 ? perfect_tet_quality() : perfect_tri_quality();
   bool const use32 = fs && dim == 3;
   float const k6 = tet_k6_f32();
@@ -475,16 +477,19 @@ __global__ void k_collapse_to_ent(u32 n, u32 const* __restrict__ voe,
 // coarsen_elem (coarsen_topology.cpp:9-34) writing straight into the new
 // connectivity after the same entities, with remap_conn applied
 // (coarsen_common.cpp:29-33)
-__global__ void k_coarsen_topology(u32 ed, u32 n, u32 const* __restrict__ voe,
-    u32 const* __restrict__ gen_offs, u32 const* __restrict__ gen_vert,
+// a thread per generating entity, from their list in order (the t-th
+// generates the t-th product)
+__global__ void k_coarsen_topology(u32 ed, u32 ngen, u32 const* __restrict__ gen_list,
+    u32 const* __restrict__ voe, u32 const* __restrict__ gen_vert,
     u32 const* __restrict__ gen_dir, u32 const* __restrict__ same_v,
     u32* __restrict__ out)
 {
   pdl_wait();
-  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n || gen_offs[i] == gen_offs[i + 1]) return;
+  u32 t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= ngen) return;
+  u32 const i = gen_list[t];
   u32 vpe = deg(ed, 0);
-  u32* o = out + (size_t)gen_offs[i] * vpe;
+  u32* o = out + (size_t)t * vpe;
   u32 b = opp(ed, 0, gen_dir[i]);
   for (u32 j = 0; j + 1 < vpe; ++j)
     o[j] = same_v[voe[(size_t)i * vpe + canon(ed, ed - 1, 0, b, j)]];
@@ -769,7 +774,8 @@ static bool coarsen_select(Mesh& m, u32* codes, double qual_floor, bool require_
     // a warp per listed edge; the list's length is read on the device
     u32 const qb = tuned(TK_QUALITY_BLOCK);
     u32 blocks = (u32)std::min<u64>(ceil_div((u64)ne * 32, qb), 148u * 16u * 256u / qb);
-    CK(launch_kernel(k_coarsen_quality, dim3(blocks), dim3(qb), 0, s, dim, clist, ncand, voe1, m.ask_down(dim, 0),
+    CK(launch_kernel(dim == 3 ? k_coarsen_quality<3> : k_coarsen_quality<2>, dim3(blocks),
+        dim3(qb), 0, s, clist, ncand, voe1, m.ask_down(dim, 0),
         ev.offs, ev.adj, ev.dirs, m.coords(), eq, qual_floor, m.segview(),
         m.fp32_filter ? fp32_stats_dev() : nullptr, codes, sel.q2, any));
     CK_LAUNCH();
@@ -955,9 +961,11 @@ static bool coarsen_build(Mesh& m, CoarsenSel const& sel, bool deferred)
       auto k = vpe == 2 ? k_same_conn<2> : vpe == 3 ? k_same_conn<3> : k_same_conn<4>;
       CK(launch_kernel(k, dim3(grid_for(n)), dim3(BLOCK), 0, s, n, voe, same_e, same_v, conn));
       CK_LAUNCH();
-      CK(launch_kernel(k_coarsen_topology, dim3(grid_for(n)), dim3(BLOCK), 0, s, ed, n, voe, gen_offs, gvert, gdir,
-          same_v, conn + (size_t)nsame * vpe));
-      CK_LAUNCH();
+      if (ngen) {
+        CK(launch_kernel(k_coarsen_topology, dim3(grid_for(ngen)), dim3(BLOCK), 0, s, ed, ngen,
+            gen_list_of[ed], voe, gvert, gdir, same_v, conn + (size_t)nsame * vpe));
+        CK_LAUNCH();
+      }
     }
     dev_free(gvert, s);
     dev_free(gdir, s);
@@ -983,10 +991,7 @@ static bool coarsen_build(Mesh& m, CoarsenSel const& sel, bool deferred)
   same_of[0] = same_v;
   nsame_of[0] = nv_out;
   // downward adjacency of the survivors carries over; the products are searched
-  for (u32 h = 2; h <= dim; ++h)
-    for (u32 l = 1; l < h; ++l)
-      if (same_of[h] && same_of[l])
-        carry_down(m, *out, h, l, same_of[h], nsame_of[h], same_of[l]);
+  carry_down_all(m, *out, same_of, nsame_of);
   carry_up_all(m, *out, same_of, nsame_of, newid_of);
   for (u32 h = 0; h <= dim; ++h) dev_free(newid_of[h], s);
   for (u32 d = 0; d < 4; ++d) {

@@ -340,7 +340,7 @@ void expand_scaled(void const* in, u32 const* offs, u32 k, u32 n, u32 width,
 }
 
 // Several row expansions in one launch: blockIdx.y picks the job, the x
-// blocks stride over its rows (the same copy as k_expand_scaled)
+// blocks stride over its rows (the same copy as k_expand_scaled).
 struct ExpandJobs {
   ExpandJob j[8];
 };
@@ -355,11 +355,88 @@ __device__ inline void copy_rows(void const* in, void* out, u32 i, u32 f, u32 e,
   }
 }
 
-__global__ void k_expand_many(ExpandJobs jobs)
+// Jobs over every row with k = 1 -- the survivors' copy, one output row or
+// none per row, in order: a stream compaction -- of rows of W 32-bit words
+// go by warps: a warp takes EXPAND_CHUNKS runs of 32 consecutive rows,
+// loads their offsets (one per lane) and their words coalesced, all before
+// any store, and stores each word at its row's place, the row's offsets
+// coming by shuffle; the kept rows' words stay consecutive, so the stores
+// are coalesced too. (A thread per row read and wrote rows of 2-4 words a
+// row apart per lane, with one or two loads in flight: a third of DRAM
+// peak.)
+constexpr u32 EXPAND_CHUNKS = 2;
+
+template <u32 W>
+__device__ inline void expand_same_rows(ExpandJob const& jb, u32 warp, u32 nwarps)
+{
+  u32 const lane = threadIdx.x & 31;
+  u32 const* __restrict__ in = static_cast<u32 const*>(jb.in);
+  u32 const* __restrict__ in2 = static_cast<u32 const*>(jb.in2);
+  u32* __restrict__ out = static_cast<u32*>(jb.out);
+  u32* __restrict__ out2 = static_cast<u32*>(jb.out2);
+  bool const two = in2 != nullptr;
+  for (u32 base = warp * 32 * EXPAND_CHUNKS; base < jb.n; base += nwarps * 32 * EXPAND_CHUNKS) {
+    u32 o0[EXPAND_CHUNKS], o1[EXPAND_CHUNKS], a[EXPAND_CHUNKS][W], b[EXPAND_CHUNKS][W];
+#pragma unroll
+    for (u32 ch = 0; ch < EXPAND_CHUNKS; ++ch) {
+      u32 const cb = base + ch * 32;
+      u32 const nrows = cb < jb.n ? min(32u, jb.n - cb) : 0u, nw = nrows * W;
+      o0[ch] = o1[ch] = 0;
+      if (lane < nrows) {
+        o0[ch] = jb.offs[cb + lane];
+        o1[ch] = jb.offs[cb + lane + 1];
+      }
+#pragma unroll
+      for (u32 it = 0; it < W; ++it) {
+        u32 const q = it * 32 + lane;
+        if (q < nw) {
+          a[ch][it] = in[(size_t)cb * W + q];
+          if (two) b[ch][it] = in2[(size_t)cb * W + q];
+        }
+      }
+    }
+#pragma unroll
+    for (u32 ch = 0; ch < EXPAND_CHUNKS; ++ch) {
+      u32 const cb = base + ch * 32;
+      u32 const nw = (cb < jb.n ? min(32u, jb.n - cb) : 0u) * W;
+#pragma unroll
+      for (u32 it = 0; it < W; ++it) {
+        u32 const q = it * 32 + lane;
+        u32 const row = q / W, c = q - row * W;
+        u32 const f = __shfl_sync(0xffffffffu, o0[ch], row & 31);
+        u32 const e = __shfl_sync(0xffffffffu, o1[ch], row & 31);
+        if (q < nw)
+          for (u32 j = f; j < e; ++j) {  // (a row of the survivors' copy has one)
+            out[(size_t)j * W + c] = a[ch][it];
+            if (two) out2[(size_t)j * W + c] = b[ch][it];
+          }
+      }
+    }
+  }
+}
+
+// Other jobs (a list of rows, k > 1, wider rows, 1-byte elements): a
+// thread per row. (At least three blocks of 512 per SM: at 56 registers
+// only four blocks of 256 fit, too few warps to keep the loads in flight.)
+__global__ void __launch_bounds__(512, 3) k_expand_many(ExpandJobs jobs)
 {
   pdl_wait();
   ExpandJob const jb = jobs.j[blockIdx.y];
-  for (u32 t = blockIdx.x * blockDim.x + threadIdx.x; t < jb.n; t += gridDim.x * blockDim.x) {
+  u32 const t0 = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+  u32 const words = jb.esz == 4 ? jb.width : jb.esz == 8 ? 2 * jb.width : 0;
+  if (words && words <= 4 && !jb.list && jb.k == 1) {
+    u32 const warp = t0 / 32, nwarps = stride / 32;
+    if (words == 1)
+      expand_same_rows<1>(jb, warp, nwarps);
+    else if (words == 2)
+      expand_same_rows<2>(jb, warp, nwarps);
+    else if (words == 3)
+      expand_same_rows<3>(jb, warp, nwarps);
+    else
+      expand_same_rows<4>(jb, warp, nwarps);
+    return;
+  }
+  for (u32 t = t0; t < jb.n; t += stride) {
     u32 const i = jb.list ? jb.list[t] : t;
     u32 f = jb.offs[i] * jb.k, e = jb.offs[i + 1] * jb.k;
     if (jb.esz == 4) {

@@ -163,6 +163,8 @@ void Mesh::clear_contents()
     low_row_offs[d] = nullptr;
     low_rows[d] = nullptr;
   }
+  dev_free(search_marks, s);
+  search_marks = nullptr;
   for (u32 d = 0; d < 4; ++d) {
     for (auto& t : tags[d]) dev_free(t.data, s);
     tags[d].clear();
@@ -206,6 +208,8 @@ void Mesh::overwrite(Mesh* with)
     with->low_row_offs[d] = nullptr;
     with->low_rows[d] = nullptr;
   }
+  search_marks = with->search_marks;
+  with->search_marks = nullptr;
   for (u32 d = 0; d < 4; ++d) {
     counts[d] = with->counts[d];
     tags[d].swap(with->tags[d]);
@@ -625,14 +629,17 @@ __device__ inline void low_key(u32 const* __restrict__ vol, u32 i, u32* w)
   sort_small(w, VPL);
 }
 
+// marks (optional): only entities whose smallest vertex is marked are listed
 template <u32 VPL>
-__global__ void k_count_key_rows(u32 nl, u32 const* __restrict__ vol, u32* cnt)
+__global__ void k_count_key_rows(u32 nl, u32 const* __restrict__ vol,
+    u32 const* __restrict__ marks, u32* cnt)
 {
   pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nl) return;
   u32 w[VPL];
   low_key<VPL>(vol, i, w);
+  if (marks && !marks[w[0]]) return;
   atomicAdd(&cnt[key_row<VPL>(w)], 1u);
 }
 
@@ -640,13 +647,15 @@ __global__ void k_count_key_rows(u32 nl, u32 const* __restrict__ vol, u32* cnt)
 // end down: uint2 {v1, id} for edges, uint4 {v1, v2, id, 0} for triangles
 template <u32 VPL>
 __global__ void k_fill_key_rows(u32 nl, u32 const* __restrict__ vol,
-    u32 const* __restrict__ offs, u32* cnt, u32* __restrict__ rows)
+    u32 const* __restrict__ marks, u32 const* __restrict__ offs, u32* cnt,
+    u32* __restrict__ rows)
 {
   pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nl) return;
   u32 w[VPL];
   low_key<VPL>(vol, i, w);
+  if (marks && !marks[w[0]]) return;
   u32 b = key_row<VPL>(w);
   u32 slot = offs[b] + atomicSub(&cnt[b], 1u) - 1u;
   if (VPL == 2)
@@ -909,6 +918,63 @@ __global__ void k_derive_sides(u32 dim, u32 ne, u32 const* __restrict__ dual,
 // ---------------------------------------------------------------------------
 // Mesh::ask_* (mesh.cpp:136-261)
 
+// the vertices of high entities first..nh-1 of up to two dimensions
+// (blockIdx.y picks one)
+struct MarkRange {
+  u32 first, nh, vph;
+  u32 const* voh;
+};
+struct MarkRanges {
+  MarkRange r[2];
+};
+
+__global__ void k_mark_verts(MarkRanges rs, u32* __restrict__ marks)
+{
+  pdl_wait();
+  MarkRange const r = rs.r[blockIdx.y];
+  u32 i = r.first + blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= r.nh) return;
+  for (u32 k = 0; k < r.vph; ++k) marks[r.voh[(size_t)i * r.vph + k]] = 1;
+}
+
+// Search rows limited to what a pass's products need: the vertices of the
+// high entities from first[h] on (h = 2, 3) are marked, and the rows list
+// only the low entities whose smallest vertex is marked (a product's lows
+// all have one of its vertices as their smallest). They serve those
+// searches only, so drop_search_rows discards them afterwards.
+void Mesh::mark_search_verts(u32 const* first)
+{
+  u32 nv = counts[0];
+  search_marks = dalloc<u32>(nv ? nv : 1, s);
+  CK(cudaMemsetAsync(search_marks, 0, sizeof(u32) * (nv ? nv : 1), s));
+  MarkRanges rs;
+  u32 nr = 0, most = 0;
+  for (u32 h = 2; h <= dim; ++h) {
+    u32 nh = count(h);
+    if (first[h] >= nh) continue;
+    rs.r[nr++] = MarkRange{first[h], nh, deg(h, 0), ask_down(h, 0)};
+    most = std::max(most, nh - first[h]);
+  }
+  if (nr) {
+    CK(launch_kernel(k_mark_verts, dim3(grid_for(most), nr), dim3(BLOCK), 0, s, rs,
+        search_marks));
+    CK_LAUNCH();
+  }
+}
+
+void Mesh::drop_search_rows()
+{
+  if (!search_marks) return;
+  for (u32 d = 1; d < 3; ++d) {
+    dev_free(low_row_offs[d], s);
+    dev_free(low_rows[d], s);
+    low_row_offs[d] = nullptr;
+    low_rows[d] = nullptr;
+  }
+  dev_free(search_marks, s);
+  search_marks = nullptr;
+}
+
 void Mesh::build_low_rows(u32 low)
 {
   if (low_rows[low]) return;
@@ -920,15 +986,15 @@ void Mesh::build_low_rows(u32 low)
   CK(cudaMemsetAsync(cnt, 0, sizeof(u32) * (nb + 1), s));
   if (nl) {
     auto k = low == 1 ? k_count_key_rows<2> : k_count_key_rows<3>;
-    CK(launch_kernel(k, dim3(grid_for(nl)), dim3(BLOCK), 0, s, nl, vol, cnt));
+    CK(launch_kernel(k, dim3(grid_for(nl)), dim3(BLOCK), 0, s, nl, vol, search_marks, cnt));
     CK_LAUNCH();
   }
   low_row_offs[low] = exscan_new(cnt, (u32)nb, s);
   low_rows[low] = dalloc<u32>((size_t)nl * (low == 1 ? 2 : 4), s);
   if (nl) {
     auto k = low == 1 ? k_fill_key_rows<2> : k_fill_key_rows<3>;
-    CK(launch_kernel(k, dim3(grid_for(nl)), dim3(BLOCK), 0, s, nl, vol, low_row_offs[low], cnt,
-        low_rows[low]));
+    CK(launch_kernel(k, dim3(grid_for(nl)), dim3(BLOCK), 0, s, nl, vol, search_marks,
+        low_row_offs[low], cnt, low_rows[low]));
     CK_LAUNCH();
   }
   dev_free(cnt, s);
@@ -1012,6 +1078,35 @@ void carry_down(Mesh& m, Mesh& out, u32 high, u32 low, u32 const* same_h, u32 ns
   out.down[high][low] = dn;
 }
 
+void carry_down_all(Mesh& m, Mesh& out, u32* const* same_of, u32 const* nsame_of)
+{
+  u32 const dim = m.dim;
+  // the products whose lows are searched, and whether they touch few
+  // enough vertices for rows limited to them (a quarter of the vertices at
+  // most, four per product)
+  bool search = false;
+  u64 nprod = 0;
+  u32 first[4] = {0, 0, 0, 0};
+  for (u32 h = 2; h <= dim; ++h) {
+    first[h] = out.has_dim(h) ? out.count(h) : 0;
+    for (u32 l = 1; l < h; ++l)
+      if (same_of[h] && same_of[l] && m.down[h][l] && !out.down[h][l] && out.has_dim(h) &&
+          out.has_dim(l)) {
+        search = true;
+        first[h] = nsame_of[h];
+      }
+    nprod += out.has_dim(h) ? out.count(h) - first[h] : 0;
+  }
+  bool const marked = search && !out.low_rows[1] && !out.low_rows[2] && !out.search_marks &&
+      16 * nprod < out.count(0);
+  if (marked) out.mark_search_verts(first);
+  for (u32 h = 2; h <= dim; ++h)
+    for (u32 l = 1; l < h; ++l)
+      if (same_of[h] && same_of[l])
+        carry_down(m, out, h, l, same_of[h], nsame_of[h], same_of[l]);
+  if (marked) out.drop_search_rows();
+}
+
 // up(low, high) carried through a pass. A surviving low keeps the uses of
 // its old row whose high entity survived, in the old order, mapped to new
 // ids, followed by the uses of the entities the pass made; a low the pass
@@ -1071,14 +1166,41 @@ __global__ void k_up_gen_count(u32 first, u32 nuses, u32 const* __restrict__ loh
   if (u < nuses) atomicAdd(&cnt[loh[u]], 1u);
 }
 
+// The uses of the entities the pass made (generated uses first..nuses-1 of
+// the new down(high, low), lph per high entity): cnt holds each row's kept +
+// generated uses, and the generated ones take the slots after the kept
+// ones, from the row's end down (their order within a row is arbitrary
+// either way: the rows are marked unsorted). The fill kernels below run
+// these on their threads past the old rows, so the two parts of a row's
+// fill, which write disjoint slots, share one launch.
+struct UpGen {
+  u32 first, nuses, lph;
+  u32 const* loh;
+  u32* cnt;
+};
+
+__device__ inline void up_gen_fill(UpGen const& g, u32 k, u32 const* __restrict__ offs,
+    u32* __restrict__ adj, u32* __restrict__ dirs)
+{
+  u32 const u = g.first + k;
+  if (u >= g.nuses) return;
+  u32 l = g.loh[u];
+  u32 slot = offs[l] + atomicSub(&g.cnt[l], 1u) - 1u;
+  adj[slot] = u / g.lph;
+  dirs[slot] = u % g.lph;
+}
+
 __global__ void k_up_surv_fill(u32 nl_old, u32 const* __restrict__ same_l,
     u32 const* __restrict__ newid_h, u32 const* __restrict__ offs_old,
     u32 const* __restrict__ adj_old, u32 const* __restrict__ dirs_old,
-    u32 const* __restrict__ offs, u32* __restrict__ adj, u32* __restrict__ dirs)
+    u32 const* __restrict__ offs, u32* __restrict__ adj, u32* __restrict__ dirs, UpGen gen)
 {
   pdl_wait();
   u32 j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= nl_old) return;
+  if (j >= nl_old) {
+    up_gen_fill(gen, j - nl_old, offs, adj, dirs);
+    return;
+  }
   u32 nj = same_l[j];
   if (same_l[j + 1] == nj) return;
   u32 w = offs[nj];
@@ -1156,12 +1278,17 @@ template <u32 CG>
 __global__ void k_up_surv_fill_grouped(u32 nl_old, u32 const* __restrict__ same_l,
     u32 const* __restrict__ newid_h, u32 const* __restrict__ offs_old,
     u32 const* __restrict__ adj_old, u32 const* __restrict__ dirs_old,
-    u32 const* __restrict__ offs, u32* __restrict__ adj, u32* __restrict__ dirs)
+    u32 const* __restrict__ offs, u32* __restrict__ adj, u32* __restrict__ dirs, UpGen gen)
 {
   pdl_wait();
   u32 const t = blockIdx.x * blockDim.x + threadIdx.x;
   u32 const j = t / CG, g = t % CG;
-  if (j >= nl_old) return;
+  if (j >= nl_old) {
+    // past the rows' groups (a multiple of CG threads): one thread per
+    // generated use
+    up_gen_fill(gen, t - nl_old * CG, offs, adj, dirs);
+    return;
+  }
   u32 const nj = same_l[j];
   if (same_l[j + 1] == nj) return;
   u32 const gbase = (threadIdx.x & 31) & ~(CG - 1);
@@ -1184,21 +1311,6 @@ __global__ void k_up_surv_fill_grouped(u32 nl_old, u32 const* __restrict__ same_
     }
     w += __popc(kept);
   }
-}
-
-// cnt holds each row's kept + generated uses: the generated ones take the
-// slots after the kept ones, from the row's end down (their order within a
-// row is arbitrary either way: the rows are marked unsorted)
-__global__ void k_up_gen_fill(u32 first, u32 nuses, u32 lph, u32 const* __restrict__ loh,
-    u32 const* __restrict__ offs, u32* cnt, u32* __restrict__ adj, u32* __restrict__ dirs)
-{
-  pdl_wait();
-  u32 u = first + blockIdx.x * blockDim.x + threadIdx.x;
-  if (u >= nuses) return;
-  u32 l = loh[u];
-  u32 slot = offs[l] + atomicSub(&cnt[l], 1u) - 1u;
-  adj[slot] = u / lph;
-  dirs[slot] = u % lph;
 }
 
 u32* carry_new_ids(u32 const* same, u32 n, cudaStream_t s)
@@ -1294,29 +1406,28 @@ void carry_up_fill(Mesh& m, Mesh& out, UpCarry& c)
   u.adj = dalloc<u32>(c.nuses, s);
   u.dirs = dalloc<u32>(c.nuses, s);
   u32 const cg = tuned(TK_CARRY_GROUP), gb = tuned(TK_GATHER_BLOCK);
-  if (c.nl_old) {
+  u64 const ngen = c.nuses > c.first ? c.nuses - c.first : 0;
+  if (c.nl_old || ngen) {
     // each array once: same_l and the old offsets, the old rows' highs and
     // directions, the highs' new ids, the new offsets, the kept uses (first)
-    // written as highs and directions
+    // written as highs and directions; per generated use its low, the
+    // row's offset and count, and the use written
     // (the fill of edge and face rows, the largest single kernel of an
     // adapt, is probed on its own: carry_up_fill)
     PROBE(c.long_rows ? P_CARRY_UP : P_CARRY_UP_FILL, s, 8.0 * (c.nl_old + 1) +
-        8.0 * c.nuses_old + 4.0 * c.nh_old + 4.0 * (c.nl + 1) + 8.0 * c.first);
+        8.0 * c.nuses_old + 4.0 * c.nh_old + 4.0 * (c.nl + 1) + 8.0 * c.first + 20.0 * ngen);
+    UpGen const gen{c.first, c.nuses, c.lph, c.loh, c.cnt};
     if (c.long_rows) {
       auto kf = cg == 4 ? k_up_surv_fill_grouped<4>
               : cg == 16 ? k_up_surv_fill_grouped<16> : k_up_surv_fill_grouped<8>;
-      CK(launch_kernel(kf, dim3(grid_for((u64)c.nl_old * cg, gb)), dim3(gb), 0, s, c.nl_old,
-          c.same_l, c.newid_h, old.offs, old.adj, old.dirs, u.offs, u.adj, u.dirs));
+      CK(launch_kernel(kf, dim3(grid_for((u64)c.nl_old * cg + ngen, gb)), dim3(gb), 0, s,
+          c.nl_old, c.same_l, c.newid_h, old.offs, old.adj, old.dirs, u.offs, u.adj, u.dirs,
+          gen));
     } else {
-      CK(launch_kernel(k_up_surv_fill, dim3(grid_for(c.nl_old, gb)), dim3(gb), 0, s, c.nl_old,
-          c.same_l, c.newid_h, old.offs, old.adj, old.dirs, u.offs, u.adj, u.dirs));
+      CK(launch_kernel(k_up_surv_fill, dim3(grid_for((u64)c.nl_old + ngen, gb)), dim3(gb), 0,
+          s, c.nl_old, c.same_l, c.newid_h, old.offs, old.adj, old.dirs, u.offs, u.adj, u.dirs,
+          gen));
     }
-    CK_LAUNCH();
-  }
-  if (c.nuses > c.first) {
-    PROBE(P_UP_FILL, s, 4.0 * (c.nuses - c.first) + 8.0 * c.nl + 8.0 * (c.nuses - c.first));
-    CK(launch_kernel(k_up_gen_fill, dim3(grid_for(c.nuses - c.first, gb)), dim3(gb), 0, s,
-        c.first, c.nuses, c.lph, c.loh, u.offs, c.cnt, u.adj, u.dirs));
     CK_LAUNCH();
   }
   dev_free(c.cnt, s);

@@ -85,6 +85,9 @@ struct Mesh {
   // uint2 {v1, id} for edges, uint4 {v1, v2, id, 0} for triangles
   u32* low_row_offs[3] = {nullptr, nullptr, nullptr};
   u32* low_rows[3] = {nullptr, nullptr, nullptr};
+  // (during a pass's searches) vertices of the products whose lows are
+  // searched; the rows then list only lows with a marked smallest vertex
+  u32* search_marks = nullptr;
   std::vector<Tag> tags[4];
   u64* globals[4] = {};
   u32* own_ranks[4] = {};   // cached zeros (single rank), API only
@@ -132,6 +135,8 @@ struct Mesh {
   u32 const* ask_down(u32 high, u32 low);
   // reflect_down's rows for lows of dimension `low` (built once per state)
   void build_low_rows(u32 low);
+  void mark_search_verts(u32 const* first);
+  void drop_search_rows();
   // down(high, low) of the high entities [first, n_high) by search, into out
   void reflect_range(u32 high, u32 low, u32 first, u32* out);
   // Upward adjacency. Rows are always the same sets; `sorted` asks for the
@@ -193,6 +198,9 @@ struct Mesh {
 // (the lows' survivor offsets); the entities the pass made are searched
 void carry_down(Mesh& m, Mesh& out, u32 high, u32 low, u32 const* same_h, u32 nsame,
     u32 const* same_l);
+// every carried downward adjacency of a pass (h = 2..dim, l = 1..h-1), the
+// products' search rows limited to the products' vertices when they are few
+void carry_down_all(Mesh& m, Mesh& out, u32* const* same_of, u32 const* nsame_of);
 
 // up(low, high) of `out` for every pair m has: surviving lows keep their
 // old rows' uses by surviving highs (mapped, in order), then the uses of the

@@ -14,9 +14,12 @@ namespace osh {
 // refine_candidate (refine.cpp:11-15) fused with measure_edge (size.cpp:57)
 __global__ void k_refine_candidates(u32 ne, u32 const* __restrict__ voe,
     double const* __restrict__ x, double const* __restrict__ h, SegView sv,
-    Fp32Stats* fs, u32* __restrict__ cand, u32* any)
+    Fp32Stats* fs, u32* __restrict__ cand, u32* any, u32* zero2)
 {
   pdl_wait();
+  // (optional) two flags the quality kernel that follows sets, zeroed here
+  // instead of by a memset of their own
+  if (zero2 && blockIdx.x == 0 && threadIdx.x < 2) zero2[threadIdx.x] = 0;
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   u32 c = 0;
   bool decided = false, rechecked = false, flipped = false;
@@ -65,18 +68,21 @@ __device__ inline void refine_child(u32 dim, u32 const* __restrict__ ve, u32 dir
 // them when every child is surely upright and the worst surely below the
 // floor; otherwise only the children whose lower bound reaches the lowest
 // upper bound seen (they alone can hold the minimum) are computed in double.
-__global__ void k_refine_quality(u32 dim, u32 ne, u32 const* __restrict__ voe1,
+template <u32 DIM>
+__global__ void k_refine_quality(u32 ne, u32 const* __restrict__ voe1,
     u32 const* __restrict__ voe, u32 const* __restrict__ eo_offs,
     u32 const* __restrict__ eo, u32 const* __restrict__ eo_dirs,
     double const* __restrict__ x, double qual_floor, SegView sv, Fp32Stats* fs,
     u32* __restrict__ cand, double* __restrict__ out, u32* any, u32* inverted)
 {
   pdl_wait();
+  constexpr u32 dim = DIM;  // the element dimension (2 or 3): loops over
+                            // an element's vertices unroll, corners stay in registers
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   u32 keep = 0;
   bool decided = false, rechecked = false, audited = false, flipped = false;
   if (i < ne && cand[i]) {
-    u32 vpe = deg(dim, 0);
+    constexpr u32 vpe = deg(dim, 0);
     double const perfect = dim == 3 ? perfect_tet_quality() : perfect_tri_quality();
     u32 a = voe1[i * 2], b = voe1[i * 2 + 1];
     double split[3];
@@ -174,20 +180,40 @@ __global__ void k_refine_quality(u32 dim, u32 ne, u32 const* __restrict__ voe1,
 }
 
 // refine_node (refine_nodal.cpp:10-25)
+// every double vertex field of the refined mesh in one launch (blockIdx.y:
+// the field): the old vertices' values copied, then each new vertex's the
+// average of its edge's two vertices
+constexpr u32 MAX_NODAL_FIELDS = 8;
+struct NodalFields {
+  double const* f[MAX_NODAL_FIELDS];
+  double* out[MAX_NODAL_FIELDS];
+  u32 nc[MAX_NODAL_FIELDS];
+};
+
 __global__ void k_refine_nodal(u32 ne, u32 nv, u32 const* __restrict__ voe,
-    u32 const* __restrict__ gen_offs, u32 nc, double const* __restrict__ f,
-    double* __restrict__ out)
+    u32 const* __restrict__ gen_offs, NodalFields fields)
 {
   pdl_wait();
-  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= ne || gen_offs[i] == gen_offs[i + 1]) return;
-  u32 a = voe[i * 2], b = voe[i * 2 + 1];
-  double* o = out + (size_t)(nv + gen_offs[i]) * nc;
-  for (u32 c = 0; c < nc; ++c) {
-    double acc = 0;
-    acc += f[(size_t)a * nc + c];
-    acc += f[(size_t)b * nc + c];
-    o[c] = acc / 2u;
+  u32 const nc = fields.nc[blockIdx.y];
+  double const* __restrict__ f = fields.f[blockIdx.y];
+  double* __restrict__ out = fields.out[blockIdx.y];
+  u64 const ncopy = (u64)nv * nc, total = ncopy + ne;
+  for (u64 t = (u64)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+       t += (u64)gridDim.x * blockDim.x) {
+    if (t < ncopy) {
+      out[t] = f[t];
+      continue;
+    }
+    u32 i = (u32)(t - ncopy);
+    if (gen_offs[i] == gen_offs[i + 1]) continue;
+    u32 a = voe[i * 2], b = voe[i * 2 + 1];
+    double* o = out + (size_t)(nv + gen_offs[i]) * nc;
+    for (u32 c = 0; c < nc; ++c) {
+      double acc = 0;
+      acc += f[(size_t)a * nc + c];
+      acc += f[(size_t)b * nc + c];
+      o[c] = acc / 2u;
+    }
   }
 }
 
@@ -201,70 +227,87 @@ __global__ void k_refine_seg(u32 ne, u32 nv, u32 const* __restrict__ voe,
   out[nv + gen_offs[i]] = seg[voe[i * 2]];
 }
 
-// split_to_domain (splits_to_domains.cpp:13-31): first split edge of each
-// domain, in the domain's local edge order
-// (SPD edges per domain entity, a compile-time count: the loads of all of
-// them are issued before any is used)
+// split_to_domain (splits_to_domains.cpp:13-31): whether a domain holds a
+// split edge (SPD edges per domain entity, a compile-time count: the loads
+// of all of them are issued before any is used). Which edge (the first in
+// local order) and its new vertex are found again by the topology kernel
+// for the split domains alone.
 template <u32 SPD>
-__global__ void k_split_to_domain(u32 nd, u32 const* __restrict__ sod,
-    u32 const* __restrict__ gen_offs, u32 nv, u32* __restrict__ will,
-    u32* __restrict__ dir, u32* __restrict__ vert)
+__device__ inline bool first_split_edge(u32 const* __restrict__ sod,
+    u32 const* __restrict__ gen_offs, u32 i, u32& dir, u32& vert_off)
 {
-  pdl_wait();
-  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= nd) return;
   u32 sv[SPD], a[SPD], b[SPD];
 #pragma unroll
-  for (u32 j = 0; j < SPD; ++j) sv[j] = sod ? sod[(size_t)i * SPD + j] : i;
+  for (u32 j = 0; j < SPD; ++j) sv[j] = sod[(size_t)i * SPD + j];
 #pragma unroll
   for (u32 j = 0; j < SPD; ++j) {
     a[j] = gen_offs[sv[j]];
     b[j] = gen_offs[sv[j] + 1];
   }
-  u32 w = 0, d = INV, v = INV;
+  bool w = false;
 #pragma unroll
   for (u32 j = SPD; j-- > 0;)
     if (a[j] != b[j]) {  // the first split edge in local order wins
-      w = 1;
-      d = j;
-      v = nv + a[j];
+      w = true;
+      dir = j;
+      vert_off = a[j];
     }
-  will[i] = w;
-  dir[i] = d;
-  vert[i] = v;
+  return w;
+}
+
+template <u32 SPD>
+__global__ void k_split_to_domain(u32 nd, u32 const* __restrict__ sod,
+    u32 const* __restrict__ gen_offs, u32* __restrict__ will)
+{
+  pdl_wait();
+  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nd) return;
+  u32 d, v;
+  will[i] = first_split_edge<SPD>(sod, gen_offs, i, d, v) ? 1u : 0u;
 }
 
 // refine_domain_entity (refine_topology.cpp:26-64), for every domain
 // dimension of one product dimension in one launch (blockIdx.y: the domain
-// dimension's job)
+// dimension's job), a thread per split domain entity from the list of them
+// in order. The domain's split edge and the new vertex on it: the edge
+// itself for edge domains, else its first split edge (sod: the domain's
+// edges).
 struct TopoJob {
-  u32 dd, nd;
+  u32 dd, nsplit;
+  u32 const* list;
   u32 const* vod;
-  u32 const* offs;
-  u32 const* dir;
-  u32 const* vert;
+  u32 const* sod;
   u32* out;
 };
 struct TopoJobs {
   TopoJob j[3];
 };
 
-__global__ void k_refine_topology(TopoJobs jobs, u32 prod)
+__global__ void k_refine_topology(TopoJobs jobs, u32 prod, u32 const* __restrict__ gen_offs,
+    u32 nv)
 {
   pdl_wait();
   TopoJob const jb = jobs.j[blockIdx.y];
   u32 const dd = jb.dd;
-  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= jb.nd || jb.offs[i] == jb.offs[i + 1]) return;
+  u32 t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= jb.nsplit) return;
+  u32 const i = jb.list[t];
+  u32 di = 0, voff = 0;
+  if (dd == 1)
+    voff = gen_offs[i];
+  else if (dd == 2)
+    first_split_edge<3>(jb.sod, gen_offs, i, di, voff);
+  else
+    first_split_edge<6>(jb.sod, gen_offs, i, di, voff);
   u32 base_dim = prod - 1, opp_dim = dd - 1 - base_dim;
   u32 ops = deg(1, opp_dim), vpp = deg(prod, 0), vpb = vpp - 1, vpd = deg(dd, 0);
-  u32* p = jb.out + (size_t)jb.offs[i] * ops * vpp;
-  u32 di = jb.dir[i];
+  // the t-th split domain's products are the t-th group (its offset is t)
+  u32* p = jb.out + (size_t)t * ops * vpp;
   for (u32 j = 0; j < ops; ++j) {
     u32 o = canon(dd, 1, opp_dim, di, j);
     u32 b = opp(dd, opp_dim, o);
     for (u32 k = 0; k < vpb; ++k) p[k] = jb.vod[(size_t)i * vpd + canon(dd, base_dim, 0, b, k)];
-    p[vpb] = jb.vert[i];
+    p[vpb] = nv + voff;
     p += vpp;
   }
 }
@@ -296,17 +339,40 @@ static u32 prods_per_dom(u32 dom, u32 src, u32 prod)
 
 struct Splits {
   u32* offs = nullptr;
-  u32* dir = nullptr;
-  u32* vert = nullptr;
   u32* list = nullptr;  // the split entities, in order (nsplit of them)
   u32 nsplit = 0;
 };
 
+// the split edges' scan: each edge's new-vertex offset (gen_offs), the split
+// edges in order (list), and the surviving edges' maps (same, and newid when
+// the edges' upward adjacency is carried) -- everything the edges need as a
+// domain, from the one scan (refine_build takes list, same and newid over)
+struct EdgeSplits {
+  u32* gen_offs = nullptr;
+  u32* list = nullptr;
+  u32* same = nullptr;
+  u32* newid = nullptr;
+};
+
+// the vertices' domain offsets (no vertex splits: zeros) and their identity
+// survivor maps
+__global__ void k_vertex_maps(u32 nv, u32* __restrict__ zero, u32* __restrict__ same,
+    u32* __restrict__ newid)
+{
+  pdl_wait();
+  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i > nv) return;
+  zero[i] = 0;
+  same[i] = i;
+  if (newid && i < nv) newid[i] = i;
+}
+
 // returns the number of split edges (read back with the domain counts).
 // deferred: the independent set's outcome comes back with the same
 // read-back; nothing to split (or a failed set) leaves the mesh unchanged.
-static u32 refine_build(Mesh& m, u32 const* gen_offs, bool deferred, bool uniform)
+static u32 refine_build(Mesh& m, EdgeSplits const& es, bool deferred, bool uniform)
 {
+  u32 const* gen_offs = es.gen_offs;
   cudaStream_t s = m.s;
   u32 dim = m.dim, src = 1;
   u32 nv = m.count(0), ns = m.count(src);
@@ -314,33 +380,50 @@ static u32 refine_build(Mesh& m, u32 const* gen_offs, bool deferred, bool unifor
   // splits_to_domains for every domain dimension; the edges' count is the
   // number of split edges, so one read-back sizes everything below
   Splits sp[4];
+  // products of every dimension (refine_common.cpp:90-123, inherit.cpp:104-138):
+  // the survivors of each (same_of) and, for the dimensions whose upward
+  // adjacency is carried, each kept entity's new id (newid_of). A domain
+  // splits (mark 1) or survives (mark 0), so the domains' scan writes both
+  // as the scan of the complement; vertices all survive (identity maps).
+  u32* same_of[4] = {nullptr, nullptr, nullptr, nullptr};
+  u32 nsame_of[4] = {0, 0, 0, 0};
+  u32* newid_of[4] = {nullptr, nullptr, nullptr, nullptr};
+  auto is_prod = [&](u32 prod) { return m.full || prod == 0 || prod == dim; };
   u32* zero_v = dalloc<u32>((size_t)nv + 1, s);
-  fill_u32(zero_v, nv + 1, 0, s);
+  same_of[0] = dalloc<u32>((size_t)nv + 1, s);
+  if (carried_high(m, 0)) newid_of[0] = dalloc<u32>(nv ? nv : 1, s);
+  CK(launch_kernel(k_vertex_maps, dim3(grid_for((u64)nv + 1)), dim3(BLOCK), 0, s, nv, zero_v,
+      same_of[0], newid_of[0]));
+  CK_LAUNCH();
   sp[0].offs = zero_v;
+  // the edges as domains: the split edges' scan (the caller owns gen_offs)
+  sp[1].offs = es.gen_offs;
+  sp[1].list = es.list;
+  same_of[1] = es.same;
+  newid_of[1] = es.newid;
   u32* will[4] = {nullptr, nullptr, nullptr, nullptr};
   ScanJob jobs[4];
   u32 njobs = 0;
-  for (u32 dd = 1; dd <= dim; ++dd) {
+  for (u32 dd = 2; dd <= dim; ++dd) {
     if (!m.has_dim(dd)) continue;
     u32 nd = m.count(dd);
-    u32 const* sod = dd == 1 ? nullptr : m.ask_down(dd, 1);
+    u32 const* sod = m.ask_down(dd, 1);
     will[dd] = dalloc<u32>(nd, s);
-    sp[dd].dir = dalloc<u32>(nd, s);
-    sp[dd].vert = dalloc<u32>(nd, s);
     if (nd) {
-      u32 const spd = deg(dd, 1);
-      auto k = spd == 1 ? k_split_to_domain<1> : spd == 3 ? k_split_to_domain<3>
-                                                           : k_split_to_domain<6>;
-      CK(launch_kernel(k, dim3(grid_for(nd)), dim3(BLOCK), 0, s, nd, sod, gen_offs, nv,
-          will[dd], sp[dd].dir, sp[dd].vert));
+      auto k = dd == 2 ? k_split_to_domain<3> : k_split_to_domain<6>;
+      CK(launch_kernel(k, dim3(grid_for(nd)), dim3(BLOCK), 0, s, nd, sod, gen_offs, will[dd]));
       CK_LAUNCH();
     }
     sp[dd].offs = dalloc<u32>((size_t)nd + 1, s);
     sp[dd].list = dalloc<u32>(nd ? nd : 1, s);
-    jobs[njobs++] = ScanJob{will[dd], sp[dd].offs, m.mb->dev + 8 + dd, nullptr, nd, 0,
-        sp[dd].list};
+    ScanJob j{will[dd], sp[dd].offs, m.mb->dev + 8 + dd, nullptr, nd, 0, sp[dd].list};
+    if (is_prod(dd)) {
+      same_of[dd] = j.comp = dalloc<u32>((size_t)nd + 1, s);
+      if (carried_high(m, dd)) newid_of[dd] = j.comp_newid = dalloc<u32>(nd ? nd : 1, s);
+    }
+    jobs[njobs++] = j;
   }
-  // the domains' scans in one launch
+  // the other domains' scans in one launch
   exscan_jobs(jobs, njobs, s);
   for (u32 dd = 1; dd <= dim; ++dd) dev_free(will[dd], s);
   m.mb->fetch(s, deferred ? INDSET_FETCH_SLOTS : 16);
@@ -348,10 +431,10 @@ static u32 refine_build(Mesh& m, u32 const* gen_offs, bool deferred, bool unifor
     auto abandon = [&] {
       delete out;
       for (u32 dd = 0; dd <= dim; ++dd) {
-        dev_free(sp[dd].offs, s);
-        dev_free(sp[dd].dir, s);
-        dev_free(sp[dd].vert, s);
+        if (dd != 1) dev_free(sp[dd].offs, s);
         dev_free(sp[dd].list, s);
+        dev_free(same_of[dd], s);
+        dev_free(newid_of[dd], s);
       }
     };
     try {
@@ -376,16 +459,31 @@ static u32 refine_build(Mesh& m, u32 const* gen_offs, bool deferred, bool unifor
   u32 nv_out = nv + nsplit;
   out->set_ents(0, nv_out, nullptr);
   u32 const* voe1 = m.ask_down(1, 0);
-  for (auto const& t : m.tags[0]) {
-    if (t.type != T_F64) continue;
-    double* d = dalloc<double>((size_t)nv_out * t.ncomps, s);
-    CK(cudaMemcpyAsync(d, t.data, sizeof(double) * nv * t.ncomps, cudaMemcpyDeviceToDevice, s));
-    if (ns) {
-      CK(launch_kernel(k_refine_nodal, dim3(grid_for(ns)), dim3(BLOCK), 0, s, ns, nv, voe1, gen_offs, t.ncomps,
-          static_cast<double const*>(t.data), d));
+  {
+    NodalFields nf;
+    u32 nfields = 0;
+    u64 most = 0;
+    auto flush = [&] {
+      if (!nfields) return;
+      u32 const gb = tuned(TK_GATHER_BLOCK);
+      u32 gx = (u32)std::min<u64>(ceil_div(most, (u64)gb), 148u * 8u * 256u / gb);
+      CK(launch_kernel(k_refine_nodal, dim3(gx ? gx : 1, nfields), dim3(gb), 0, s, ns, nv, voe1,
+          gen_offs, nf));
       CK_LAUNCH();
+      nfields = 0;
+      most = 0;
+    };
+    for (auto const& t : m.tags[0]) {
+      if (t.type != T_F64) continue;
+      double* d = dalloc<double>((size_t)nv_out * t.ncomps, s);
+      nf.f[nfields] = static_cast<double const*>(t.data);
+      nf.out[nfields] = d;
+      nf.nc[nfields] = t.ncomps;
+      most = std::max<u64>(most, (u64)nv * t.ncomps + ns);
+      if (++nfields == MAX_NODAL_FIELDS) flush();
+      out->add_tag(0, T_F64, t.name.c_str(), t.ncomps, X_NOT, d);
     }
-    out->add_tag(0, T_F64, t.name.c_str(), t.ncomps, X_NOT, d);
+    flush();
   }
   if (m.parallel) inherit_globals(*out, 0, nv_out);
   if (m.seg) {
@@ -395,25 +493,6 @@ static u32 refine_build(Mesh& m, u32 const* gen_offs, bool deferred, bool unifor
       CK(launch_kernel(k_refine_seg, dim3(grid_for(ns)), dim3(BLOCK), 0, s, ns, nv, voe1, gen_offs, m.seg, out->seg));
       CK_LAUNCH();
     }
-  }
-  // products of every dimension (refine_common.cpp:90-123, inherit.cpp:104-138)
-  u32* same_of[4] = {nullptr, nullptr, nullptr, nullptr};
-  u32 nsame_of[4] = {0, 0, 0, 0};
-  // each kept entity's new id, written by the survivors' scan for the
-  // dimensions whose upward adjacency is carried
-  u32* newid_of[4] = {nullptr, nullptr, nullptr, nullptr};
-  // the survivors of every product dimension, scanned in one launch
-  {
-    ScanJob sj[4];
-    u32 nsj = 0;
-    for (u32 prod = 0; prod <= dim; ++prod) {
-      if (!m.full && 0 < prod && prod < dim) continue;
-      u32 np = m.count(prod);
-      if (carried_high(m, prod)) newid_of[prod] = dalloc<u32>(np ? np : 1, s);
-      same_of[prod] = dalloc<u32>((size_t)np + 1, s);
-      sj[nsj++] = ScanJob{sp[prod].offs, same_of[prod], nullptr, newid_of[prod], np, 1};
-    }
-    exscan_jobs(sj, nsj, s);
   }
   for (u32 prod = 0; prod <= dim; ++prod) {
     if (!m.full && 0 < prod && prod < dim) continue;
@@ -459,16 +538,17 @@ static u32 refine_build(Mesh& m, u32 const* gen_offs, bool deferred, bool unifor
       double bytes = 0;
       for (u32 dd = first; dd <= last; ++dd) {
         if (!d.ndoms[dd] || !d.scale[dd] || !sp[dd].nsplit) continue;
-        u32 nd = d.ndoms[dd];
-        tj.j[ntj++] = TopoJob{dd, nd, m.ask_down(dd, 0), sp[dd].offs, sp[dd].dir, sp[dd].vert,
-            conn + (size_t)d.ngo[dd] * vpp};
+        u32 nd = sp[dd].nsplit;
+        tj.j[ntj++] = TopoJob{dd, nd, sp[dd].list, m.ask_down(dd, 0),
+            dd == 1 ? nullptr : m.ask_down(dd, 1), conn + (size_t)d.ngo[dd] * vpp};
         ndmax = std::max(ndmax, nd);
-        bytes += 4.0 * deg(dd, 0) * nd + 12.0 * nd + 4.0 * (nd + 1) + 4.0 * vpp * (double)d.ngen[dd];
+        bytes += 4.0 * nd + 4.0 * deg(dd, 0) * nd + 12.0 * deg(dd, 1) * nd +
+            4.0 * vpp * (double)d.ngen[dd];
       }
       if (ntj) {
         PROBE(P_REFINE_TOPOLOGY, s, bytes);
         CK(launch_kernel(k_refine_topology, dim3(grid_for(ndmax), ntj), dim3(BLOCK), 0, s, tj,
-            prod));
+            prod, gen_offs, nv));
         CK_LAUNCH();
       }
       out->set_ents(prod, nout, conn);
@@ -497,17 +577,12 @@ static u32 refine_build(Mesh& m, u32 const* gen_offs, bool deferred, bool unifor
     nsame_of[prod] = np - sp[prod].nsplit;
   }
   // downward adjacency of the survivors carries over; the products are searched
-  for (u32 h = 2; h <= dim; ++h)
-    for (u32 l = 1; l < h; ++l)
-      if (same_of[h] && same_of[l])
-        carry_down(m, *out, h, l, same_of[h], nsame_of[h], same_of[l]);
+  carry_down_all(m, *out, same_of, nsame_of);
   carry_up_all(m, *out, same_of, nsame_of, newid_of);
   for (u32 h = 0; h <= dim; ++h) dev_free(newid_of[h], s);
   for (u32 dd = 0; dd <= dim; ++dd) {
     dev_free(same_of[dd], s);
-    dev_free(sp[dd].offs, s);
-    dev_free(sp[dd].dir, s);
-    dev_free(sp[dd].vert, s);
+    if (dd != 1) dev_free(sp[dd].offs, s);  // the edges' are the caller's gen_offs
     dev_free(sp[dd].list, s);
   }
   m.overwrite(out);
@@ -521,8 +596,9 @@ static u32 refine_build(Mesh& m, u32 const* gen_offs, bool deferred, bool unifor
 // refine_by_size / refine_sets left "any candidate" in mailbox slot 3
 // deferred (see refine_deferred): the set is returned unchecked, and the
 // build's read-back brings its outcome and the flags
+// zeroed: the candidate kernel already zeroed mailbox slots 1-2
 static u32* choose_refinement(Mesh& m, u32* cand, double qual_floor, double** quals_out,
-    bool uniform, bool deferred = false)
+    bool uniform, bool deferred = false, bool zeroed = false)
 {
   cudaStream_t s = m.s;
   u32 ne = m.count(1), dim = m.dim;
@@ -530,7 +606,7 @@ static u32* choose_refinement(Mesh& m, u32* cand, double qual_floor, double** qu
   if (dim < 2) CK(cudaMemsetAsync(q, 0, sizeof(double) * ne, s));
   u32* any = m.mb->dev + 1;
   u32* inverted = m.mb->dev + 2;
-  CK(cudaMemsetAsync(any, 0, 2 * sizeof(u32), s));
+  if (!zeroed) CK(cudaMemsetAsync(any, 0, 2 * sizeof(u32), s));
   if (dim >= 2) {
     UpAdj const& eo = m.ask_up(1, dim, false);
     if (ne) {
@@ -539,8 +615,8 @@ static u32* choose_refinement(Mesh& m, u32* cand, double qual_floor, double** qu
       PROBE(P_REFINE_QUALITY, s, 4.0 * (ne + 1) + 8.0 * deg(dim, 1) * nel + 8.0 * ne +
           4.0 * deg(dim, 0) * nel + 24.0 * m.counts[0] + 8.0 * ne + 8.0 * ne);
       u32 const qb = tuned(TK_QUALITY_BLOCK);
-      CK(launch_kernel(k_refine_quality, dim3(grid_for(ne, qb)), dim3(qb), 0, s, dim, ne,
-          m.ask_down(1, 0),
+      CK(launch_kernel(dim == 3 ? k_refine_quality<3> : k_refine_quality<2>,
+          dim3(grid_for(ne, qb)), dim3(qb), 0, s, ne, m.ask_down(1, 0),
           m.ask_down(dim, 0), eo.offs, eo.adj, eo.dirs, m.coords(), qual_floor, m.segview(),
           m.fp32_filter ? fp32_stats_dev() : nullptr, cand, q, any, inverted));
       CK_LAUNCH();
@@ -587,7 +663,8 @@ static bool refine_deferred(Mesh& m)
   return m.count(1) && m.dim >= 2;
 }
 
-static u32 refine_common(Mesh& m, u32* cand, double qual_floor, bool uniform)
+static u32 refine_common(Mesh& m, u32* cand, double qual_floor, bool uniform,
+    bool zeroed = false)
 {
   cudaStream_t s = m.s;
   PassStats& st = last_pass_stats();
@@ -596,19 +673,33 @@ static u32 refine_common(Mesh& m, u32* cand, double qual_floor, bool uniform)
   st.elems_in = m.count(m.dim);
   u32 ne = m.count(1);
   bool const deferred = refine_deferred(m);
-  u32* ind = choose_refinement(m, cand, qual_floor, nullptr, uniform, deferred);
+  u32* ind = choose_refinement(m, cand, qual_floor, nullptr, uniform, deferred, zeroed);
   if (!ind) return 0;
   seg_tally(m, 1, ind);
-  u32* gen_offs = exscan_new(ind, ne, s);
+  // the split edges' scan, with their list and the surviving edges' maps
+  // (the edges' count goes to mailbox slot 9 with the other domains')
+  EdgeSplits es;
+  es.gen_offs = dalloc<u32>((size_t)ne + 1, s);
+  es.list = dalloc<u32>(ne ? ne : 1, s);
+  if (m.full || m.dim == 1) {
+    es.same = dalloc<u32>((size_t)ne + 1, s);
+    if (carried_high(m, 1)) es.newid = dalloc<u32>(ne ? ne : 1, s);
+  }
+  {
+    ScanJob j{ind, es.gen_offs, m.mb->dev + 9, nullptr, ne, 0, es.list};
+    j.comp = es.same;
+    j.comp_newid = es.newid;
+    exscan_jobs(&j, 1, s);
+  }
   dev_free(ind, s);
   u32 nsplit = 0;
   try {
-    nsplit = refine_build(m, gen_offs, deferred, uniform);
+    nsplit = refine_build(m, es, deferred, uniform);
   } catch (...) {
-    dev_free(gen_offs, s);
+    dev_free(es.gen_offs, s);
     throw;
   }
-  dev_free(gen_offs, s);
+  dev_free(es.gen_offs, s);
   if (!nsplit) return 0;  // a deferred set that came back empty
   st.nselected = nsplit;
   st.elems_out = m.count(m.dim);
@@ -628,12 +719,12 @@ u32 refine_by_size(Mesh& m, double qual_floor)
     PROBE(P_REFINE_CANDIDATES, s, 8.0 * ne + 32.0 * m.counts[0] + 4.0 * ne);
     CK(launch_kernel(k_refine_candidates, dim3(grid_for(ne)), dim3(BLOCK), 0, s, ne, m.ask_down(1, 0), m.coords(),
         static_cast<double const*>(h->data), m.segview(),
-        m.fp32_filter ? fp32_stats_dev() : nullptr, cand, any));
+        m.fp32_filter ? fp32_stats_dev() : nullptr, cand, any, m.mb->dev + 1));
     CK_LAUNCH();
   }
   // no separate check for "any candidate": with none, the quality kernel
   // keeps none and refine_common returns 0 after its single read-back
-  u32 r = refine_common(m, cand, qual_floor, false);
+  u32 r = refine_common(m, cand, qual_floor, false, ne != 0);
   dev_free(cand, s);
   return r;
 }
@@ -660,7 +751,7 @@ u32 refine_sets(Mesh& m, double qual_floor, u32* cand_out, u32* good_out,
   if (ne) {
     CK(launch_kernel(k_refine_candidates, dim3(grid_for(ne)), dim3(BLOCK), 0, s, ne, m.ask_down(1, 0), m.coords(),
         static_cast<double const*>(h->data), m.segview(),
-        m.fp32_filter ? fp32_stats_dev() : nullptr, cand_out, any));
+        m.fp32_filter ? fp32_stats_dev() : nullptr, cand_out, any, nullptr));
     CK_LAUNCH();
   }
   CK(cudaMemcpyAsync(good_out, cand_out, sizeof(u32) * ne, cudaMemcpyDeviceToDevice, s));

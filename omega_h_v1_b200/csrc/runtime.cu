@@ -664,6 +664,8 @@ k_exscan(ScanJobs jobs, unsigned long long* status, u32* ticket_and_err, u32 spi
   u32* __restrict__ out = job.out;
   u32* __restrict__ newid = job.newid;
   u32* __restrict__ list = job.list;
+  u32* __restrict__ comp = job.comp;
+  u32* __restrict__ comp_newid = job.comp_newid;
 #pragma unroll
   for (int k = 0; k < SCAN_ITEMS; ++k) {
     u32 li = k * SCAN_THREADS + threadIdx.x;
@@ -671,15 +673,18 @@ k_exscan(ScanJobs jobs, unsigned long long* status, u32* ticket_and_err, u32 spi
     if (gi < n) {
       u32 const o = s_buf[li + (li >> 5)];
       out[gi] = o;
-      if (newid || list) {
+      if (comp) comp[gi] = (u32)gi - o;
+      if (newid || list || comp_newid) {
         bool const on = !mode1 ? in[gi] != 0 : in[gi + 1] == in[gi];
         if (newid) newid[gi] = on ? o : INV;
         if (list && on) list[o] = (u32)gi;
+        if (comp_newid) comp_newid[gi] = on ? INV : (u32)gi - o;
       }
     }
   }
   if (tile == last && threadIdx.x == 0) {
     out[n] = s_prefix + total;
+    if (comp) comp[n] = n - (s_prefix + total);
     if (job.total_to) *job.total_to = s_prefix + total;
   }
   // The last tile to finish returns the scratch to zero for the next scan
@@ -784,7 +789,8 @@ void exscan_jobs(ScanJob const* jobs, u32 njobs, cudaStream_t s)
     for (u32 q = 0; q < pack.njobs; ++q) {
       pack.j[q] = jobs[at + q];
       pack.tile0[q + 1] = pack.tile0[q] + job_tiles(pack.j[q].n, tile);
-      bytes += 8.0 * pack.j[q].n + 4.0 + (pack.j[q].newid ? 4.0 * pack.j[q].n : 0.0);
+      bytes += 8.0 * pack.j[q].n + 4.0 + (pack.j[q].newid ? 4.0 * pack.j[q].n : 0.0) +
+          (pack.j[q].comp ? 4.0 * pack.j[q].n : 0.0) + (pack.j[q].comp_newid ? 4.0 * pack.j[q].n : 0.0);
     }
     // [ticket, error, done, pad][status per tile], zero on entry
     u32* scratch = stream_scan_scratch(4 + 2 * (size_t)pack.tile0[pack.njobs], s);

@@ -69,6 +69,12 @@ struct ScanJob {
   // (optional, mode 0 with 0/1 items) list[out[i]] = i where item i is 1:
   // the marked items in order
   u32* list = nullptr;
+  // (optional, mode 0 with 0/1 items) the scan of the complement,
+  // comp[i] = i - out[i] for i <= n (the unmarked items before i), and
+  // comp_newid[i] = comp[i] where item i is 0 and INV where it is 1 -- each
+  // survivor's new id when the items mark what a pass removes
+  u32* comp = nullptr;
+  u32* comp_newid = nullptr;
 };
 struct ScanJobs {
   u32 njobs;

@@ -658,10 +658,7 @@ static bool swap_build(Mesh& m, SwapSel const& sel, bool deferred)
   iota_u32(same_of[0], nv + 1, 1, s);
   nsame_of[0] = nv;
   // downward adjacency of the survivors carries over; the products are searched
-  for (u32 h = 2; h <= dim; ++h)
-    for (u32 l = 1; l < h; ++l)
-      if (same_of[h] && same_of[l])
-        carry_down(m, *out, h, l, same_of[h], nsame_of[h], same_of[l]);
+  carry_down_all(m, *out, same_of, nsame_of);
   carry_up_all(m, *out, same_of, nsame_of, newid_of);
   for (u32 h = 0; h <= dim; ++h) dev_free(newid_of[h], s);
   for (u32 d = 0; d < 4; ++d) dev_free(same_of[d], s);

@@ -2,7 +2,7 @@
 libosh_b200.so: lanes per row of the long-row kernels, threads per block,
 scan tile size).
 
-    python -m omega_h_v1_b200.tune [--n 32] [--reps 5] [--out PATH]
+    python -m omega_h_v1_b200.tune [--n 48] [--reps 5] [--out PATH]
 
 Each key is swept in turn over its allowed values (the others held at the
 best found so far) on mesh_adapt of a seeded box with a radial size field,
@@ -61,7 +61,7 @@ def table(L):
 
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
-    ap.add_argument("--n", type=int, default=32, help="box edge (6 n^3 tets)")
+    ap.add_argument("--n", type=int, default=48, help="box edge (6 n^3 tets)")
     ap.add_argument("--reps", type=int, default=5, help="timed adapts per value")
     ap.add_argument("--out", default=None, help="table file (default: beside the library)")
     args = ap.parse_args(argv)
