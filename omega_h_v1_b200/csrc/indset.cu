@@ -28,13 +28,27 @@ constexpr u32 COOP_CTL_SLOT = 44, COOP_CTL_WORDS = 7;
 static_assert(COOP_CTL_SLOT + COOP_CTL_WORDS == INDSET_FETCH_SLOTS, "mailbox slots");
 
 // also zeroes the control words of the rounds
+// The states (the filter's candidates undecided, the rest out of the set)
+// and round 0's list: the candidates, appended a warp at a time to the list
+// whose length is control word 2 (zero on entry: the rounds kernel zeroes
+// it when it settles, the host when a set fails). The other control words
+// are zeroed here.
 __global__ void k_indset_init(u32 n, u32 const* __restrict__ filter, u32* __restrict__ st,
-    u32* ctl)
+    u32* __restrict__ list0, u32* ctl)
 {
   pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < COOP_CTL_WORDS) ctl[i] = 0;
-  if (i < n) st[i] = filter[i] ? (u32)UNKNOWN : (u32)NOT_IN_SET;
+  if (i < COOP_CTL_WORDS && i != 2) ctl[i] = 0;
+  bool const c = i < n && (!filter || filter[i]);
+  if (i < n) st[i] = c ? (u32)UNKNOWN : (u32)NOT_IN_SET;
+  unsigned const want = __ballot_sync(0xffffffffu, c);
+  if (want) {
+    u32 const lane = threadIdx.x & 31, leader = __ffs(want) - 1;
+    u32 base = 0;
+    if (lane == leader) base = atomicAdd(&ctl[2], (u32)__popc(want));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (c) list0[base + __popc(want & ((1u << lane) - 1u))] = i;
+  }
 }
 
 // neighbourhood walks: mode 0 = vertices via edges, mode 1 = edges via
@@ -120,14 +134,15 @@ __global__ void __launch_bounds__(BLOCK, 4) k_indset_coop(u32 n, Nbrs g, u32* st
   u32 const lane = threadIdx.x & 31;
   u32 const stride = gridDim.x * blockDim.x;
   for (u32 r = 0; r < MAX_INDSET_ROUNDS; ++r) {
-    // round 0 walks every entity; round r > 0 the list round r - 1 left
-    u32 const len = r == 0 ? n : *(volatile u32*)&ctl[2 + r % 3];
+    // round 0 walks the candidates (listed by k_indset_init), round r > 0
+    // the list round r - 1 left
+    u32 const len = *(volatile u32*)&ctl[2 + r % 3];
     u32 const* list = (r % 2 == 1) ? wl0 : wl1;
     u32* next = (r % 2 == 0) ? wl0 : wl1;
     u32* next_len = &ctl[2 + (r + 1) % 3];
     if (blockIdx.x == 0 && threadIdx.x == 0) ctl[2 + (r + 2) % 3] = 0;
     for (u64 t = (u64)blockIdx.x * blockDim.x + threadIdx.x; t < (u64)len * G; t += stride) {
-      u32 const i = r == 0 ? (u32)(t / G) : list[t / G];
+      u32 const i = list[t / G];
       u32 const s0 = __ldcg(&st[i]);
       bool undecided = false;
       if (s0 == UNKNOWN) {
@@ -178,7 +193,13 @@ __global__ void __launch_bounds__(BLOCK, 4) k_indset_coop(u32 n, Nbrs g, u32* st
     __threadfence();
     if (!coop_barrier(ctl)) return;
     if (*(volatile u32*)next_len == 0) {
-      if (blockIdx.x == 0 && threadIdx.x == 0) ctl[5] = r + 1;
+      // settled: every block has passed the last barrier and reads only
+      // next_len (zero) from here, so the list lengths go back to zero for
+      // the next set's k_indset_init
+      if (blockIdx.x == 0 && threadIdx.x == 0) {
+        ctl[5] = r + 1;
+        ctl[2] = ctl[3] = ctl[4] = 0;
+      }
       return;
     }
   }
@@ -261,9 +282,10 @@ u32* find_indset(Mesh& m, u32 ent_dim, u32 const* filter, double const* good, bo
   u64 const* glob = (m.parallel && m.globals[ent_dim]) ? m.globals[ent_dim] : nullptr;
   u32* a = dalloc<u32>(n, m.s);
   u32* b = dalloc<u32>(2 * (size_t)n, m.s);  // the two lists of undecided entities
-  // zeroes the control words even with no entity (rounds run = 0 then)
+  // zeroes the control words even with no entity (rounds run = 0 then);
+  // round 0's list is b's second half
   CK(launch_kernel(k_indset_init, dim3(grid_for(std::max<u32>(n, COOP_CTL_WORDS))),
-      dim3(BLOCK), 0, m.s, n, filter, a, m.mb->dev + COOP_CTL_SLOT));
+      dim3(BLOCK), 0, m.s, n, filter, a, b + n, m.mb->dev + COOP_CTL_SLOT));
   CK_LAUNCH();
   // All rounds run in one cooperative launch that updates a in place; its
   // control words (mailbox slots COOP_CTL_SLOT..) come back with slots 1-3,
@@ -297,13 +319,24 @@ u32* find_indset(Mesh& m, u32 ent_dim, u32 const* filter, double const* good, bo
 void indset_check(Mesh& m)
 {
   u32 const* hc = m.mb->host + COOP_CTL_SLOT;
-  if (hc[6]) throw Failure(E_TIMEOUT, "independent set: a grid barrier wait gave up");
+  // a set that failed leaves its list lengths standing: zeroed here for the
+  // next set's k_indset_init, which appends to list length 0
+  auto reset = [&] {
+    CK(cudaMemsetAsync(m.mb->dev + COOP_CTL_SLOT, 0, COOP_CTL_WORDS * sizeof(u32), m.s));
+  };
+  if (hc[6]) {
+    reset();
+    throw Failure(E_TIMEOUT, "independent set: a grid barrier wait gave up");
+  }
   u32 rounds = hc[5];
   last_pass_stats().indset_rounds = rounds;
-  // settled: no entity, or the last round left none undecided
-  // the last round left an empty list for the round after it
+  // settled: no entity, or the last round left none undecided (the rounds
+  // kernel zeroed the list lengths then)
   bool done = rounds == 0 || hc[2 + rounds % 3] == 0;
-  if (!done) throw Failure(E_NOCONVERGE, "independent set did not settle in 100 rounds");
+  if (!done) {
+    reset();
+    throw Failure(E_NOCONVERGE, "independent set did not settle in 100 rounds");
+  }
 }
 
 // ---------------------------------------------------------------------------
