@@ -494,7 +494,13 @@ double read_f64(double const* d, cudaStream_t s)
 void Mailbox::init(cudaStream_t s)
 {
   if (host) return;
-  CK(cudaMallocHost(&host, 64 * sizeof(u32)));
+  // the sequence word on a line of its own
+  CK(cudaMallocHost(&host, (SEQ_SLOT + 32) * sizeof(u32)));
+  std::memset(host, 0, (SEQ_SLOT + 32) * sizeof(u32));
+  void* hd = nullptr;
+  CK(cudaHostGetDevicePointer(&hd, host, 0));
+  hdev = static_cast<u32*>(hd);
+  seq = 0;
   dev = dalloc<u32>(64, s);
   clear(s);
 }
@@ -504,6 +510,7 @@ void Mailbox::release()
   if (host) cudaFreeHost(host);
   if (dev) cudaFree(dev);
   host = nullptr;
+  hdev = nullptr;
   dev = nullptr;
 }
 
@@ -512,10 +519,44 @@ void Mailbox::clear(cudaStream_t s)
   CK(cudaMemsetAsync(dev, 0, 64 * sizeof(u32), s));
 }
 
+__global__ void k_mailbox_post(u32 const* __restrict__ dev, u32 n, u32* host, u32 seq)
+{
+  pdl_wait();
+  u32 i = threadIdx.x;
+  if (i < n) {
+    reinterpret_cast<volatile u32*>(host)[i] = dev[i];
+    __threadfence_system();  // this slot reaches the host before the sequence word
+  }
+  __syncthreads();
+  if (i == 0) reinterpret_cast<volatile u32*>(host)[Mailbox::SEQ_SLOT] = seq;
+}
+
 void Mailbox::fetch(cudaStream_t s, u32 nslots)
 {
-  CK(cudaMemcpyAsync(host, dev, nslots * sizeof(u32), cudaMemcpyDeviceToHost, s));
-  stream_sync(s);
+  if (nslots > 64) nslots = 64;
+  u32 const want = ++seq;
+  g_syncs.fetch_add(1, std::memory_order_relaxed);
+  auto t0 = std::chrono::steady_clock::now();
+  CK(launch_kernel(k_mailbox_post, dim3(1), dim3(64), 0, s, dev, nslots, hdev, want));
+  CK_LAUNCH();
+  volatile u32* flag = host + SEQ_SLOT;
+  for (u64 it = 1; *flag != want; ++it) {
+    if ((it & 255) != 0) continue;
+    // now and then: a failed stream ends the wait with its error; a drained
+    // stream whose word has not arrived (it should have) falls back to a
+    // copy and a synchronisation
+    cudaError_t st = cudaStreamQuery(s);
+    if (st == cudaErrorNotReady) continue;
+    CK(st);
+    if (*flag == want) break;
+    CK(cudaMemcpyAsync(host, dev, nslots * sizeof(u32), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    break;
+  }
+  std::atomic_thread_fence(std::memory_order_acquire);
+  auto dt = std::chrono::steady_clock::now() - t0;
+  g_sync_ns.fetch_add((unsigned long long)std::chrono::duration_cast<std::chrono::nanoseconds>(
+      dt).count(), std::memory_order_relaxed);
 }
 
 // ---------------------------------------------------------------------------
