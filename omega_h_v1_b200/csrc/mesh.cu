@@ -1127,45 +1127,6 @@ __global__ void k_new_ids(u32 n, u32 const* __restrict__ same, u32* __restrict__
   newid[i] = same[i + 1] != a ? a : INV;
 }
 
-// threads past the old rows zero the counts of the rows the pass made (and
-// the entry after the last row), so no memset precedes the launch
-__global__ void k_up_surv_count(u32 nl_old, u32 nsame_l, u32 ntail,
-    u32 const* __restrict__ same_l, u32 const* __restrict__ newid_h,
-    u32 const* __restrict__ offs, u32 const* __restrict__ adj, u32* __restrict__ cnt,
-    u32* __restrict__ surv)
-{
-  pdl_wait();
-  u32 j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= nl_old) {
-    if (j - nl_old < ntail) {
-      u32 r = nsame_l + (j - nl_old);
-      cnt[r] = 0;
-      if (surv) surv[r] = 0;
-    }
-    return;
-  }
-  u32 nj = same_l[j];
-  if (same_l[j + 1] == nj) return;
-  u32 r = offs[j], e = offs[j + 1];
-  u32 c = 0;
-  for (; r + 4 <= e; r += 4) {
-    u32 a0 = adj[r], a1 = adj[r + 1], a2 = adj[r + 2], a3 = adj[r + 3];
-    u32 n0 = newid_h[a0], n1 = newid_h[a1], n2 = newid_h[a2], n3 = newid_h[a3];
-    c += (n0 != INV) + (n1 != INV) + (n2 != INV) + (n3 != INV);
-  }
-  for (; r < e; ++r) c += newid_h[adj[r]] != INV;
-  cnt[nj] = c;
-  if (surv) surv[nj] = c;
-}
-
-__global__ void k_up_gen_count(u32 first, u32 nuses, u32 const* __restrict__ loh,
-    u32* __restrict__ cnt)
-{
-  pdl_wait();
-  u32 u = first + blockIdx.x * blockDim.x + threadIdx.x;
-  if (u < nuses) atomicAdd(&cnt[loh[u]], 1u);
-}
-
 // The uses of the entities the pass made (generated uses first..nuses-1 of
 // the new down(high, low), lph per high entity): cnt holds each row's kept +
 // generated uses, and the generated ones take the slots after the kept
@@ -1231,48 +1192,14 @@ __global__ void k_up_surv_fill(u32 nl_old, u32 const* __restrict__ same_l,
   }
 }
 
-// The same two kernels for long rows (vertex rows, 8 or more uses on
-// average): a group of CG lanes (the tuning table's carry_group) walks one
+// The same fill for long rows (vertex rows, 8 or more uses on average): a
+// group of CG lanes (the tuning table's carry_group) walks one
 // row, each lane one use, so a row's uses are read and written by
 // consecutive lanes; a ballot over the group gives each kept use its place,
 // in the old order. (One thread per long row issues loads whose lanes are a
 // row apart and fills the load/store queue.) Groups never straddle a warp;
 // a group's lanes share their row, so they loop and leave together.
 constexpr u32 LONG_ROW_USES = 8;
-
-template <u32 CG>
-__global__ void k_up_surv_count_grouped(u32 nl_old, u32 nsame_l, u32 ntail,
-    u32 const* __restrict__ same_l, u32 const* __restrict__ newid_h,
-    u32 const* __restrict__ offs, u32 const* __restrict__ adj, u32* __restrict__ cnt,
-    u32* __restrict__ surv)
-{
-  pdl_wait();
-  u32 const t = blockIdx.x * blockDim.x + threadIdx.x;
-  u32 const j = t / CG, g = t % CG;
-  if (j >= nl_old) {
-    if (g == 0 && j - nl_old < ntail) {
-      u32 r = nsame_l + (j - nl_old);
-      cnt[r] = 0;
-      if (surv) surv[r] = 0;
-    }
-    return;
-  }
-  u32 const nj = same_l[j];
-  if (same_l[j + 1] == nj) return;
-  u32 const gbase = (threadIdx.x & 31) & ~(CG - 1);
-  u32 const gmask = ((1u << CG) - 1u) << gbase;
-  u32 const e = offs[j + 1];
-  u32 c = 0;
-  for (u32 base = offs[j]; base < e; base += CG) {
-    u32 const u = base + g;
-    bool const keep = u < e && newid_h[adj[u]] != INV;
-    c += __popc(__ballot_sync(gmask, keep) & gmask);
-  }
-  if (g == 0) {
-    cnt[nj] = c;
-    if (surv) surv[nj] = c;
-  }
-}
 
 template <u32 CG>
 __global__ void k_up_surv_fill_grouped(u32 nl_old, u32 const* __restrict__ same_l,
@@ -1311,6 +1238,55 @@ __global__ void k_up_surv_fill_grouped(u32 nl_old, u32 const* __restrict__ same_
     }
     w += __popc(kept);
   }
+}
+
+// The counts of the carried rows without a gather per use: a surviving row
+// keeps its old uses but those of the high entities the pass removed, one
+// use in each of their lows' rows, and takes the uses of the entities the
+// pass made. k_up_row_lens writes each surviving row's old length (zeroing
+// the rows the pass made); k_up_adjust takes a use off for every low of a
+// removed high (new id INV) that survives and adds the generated uses.
+// (Counting the kept uses row by row gathered a new id for every old use.)
+__global__ void k_up_row_lens(u32 nl_old, u32 nsame_l, u32 ntail,
+    u32 const* __restrict__ same_l, u32 const* __restrict__ offs_old, u32* __restrict__ cnt,
+    u32* __restrict__ surv)
+{
+  pdl_wait();
+  u32 j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= nl_old) {
+    if (j - nl_old < ntail) {
+      u32 r = nsame_l + (j - nl_old);
+      cnt[r] = 0;
+      if (surv) surv[r] = 0;
+    }
+    return;
+  }
+  u32 nj = same_l[j];
+  if (same_l[j + 1] == nj) return;
+  u32 len = offs_old[j + 1] - offs_old[j];
+  cnt[nj] = len;
+  if (surv) surv[nj] = len;
+}
+
+__global__ void k_up_adjust(u32 nh_old, u32 lph, u32 const* __restrict__ newid_h,
+    u32 const* __restrict__ old_loh, u32 const* __restrict__ same_l, u32* cnt, u32* surv,
+    u32 first, u32 nuses, u32 const* __restrict__ loh)
+{
+  pdl_wait();
+  u32 t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < nh_old) {
+    if (newid_h[t] != INV) return;
+    for (u32 k = 0; k < lph; ++k) {
+      u32 l = old_loh[(size_t)t * lph + k];
+      u32 nl = same_l[l];
+      if (same_l[l + 1] == nl) continue;
+      atomicSub(&cnt[nl], 1u);
+      if (surv) atomicSub(&surv[nl], 1u);
+    }
+    return;
+  }
+  u32 u = first + (t - nh_old);
+  if (u < nuses) atomicAdd(&cnt[loh[u]], 1u);
 }
 
 u32* carry_new_ids(u32 const* same, u32 n, cudaStream_t s)
@@ -1369,28 +1345,22 @@ bool carry_up_count(Mesh& m, Mesh& out, u32 low, u32 high, u32 const* same_l, u3
   c.nuses_old = m.counts[high] * c.lph;
   // rows of 8 or more uses on average (vertex rows) take a lane group each
   c.long_rows = c.nl_old && (u64)c.nuses_old >= (u64)LONG_ROW_USES * c.nl_old;
-  u32 const cg = tuned(TK_CARRY_GROUP), gb = tuned(TK_GATHER_BLOCK);
+  u32 const gb = tuned(TK_GATHER_BLOCK);
   {
     u32 ntail = c.nl + 1 - nsame_l;
-    // each array once: same_l and the old offsets, the old rows' highs, the
-    // highs' new ids, the new counts
-    PROBE(P_CARRY_UP, s, 8.0 * (c.nl_old + 1) + 4.0 * c.nuses_old + 4.0 * c.nh_old +
-        4.0 * c.nl);
-    if (c.long_rows) {
-      auto kc = cg == 4 ? k_up_surv_count_grouped<4>
-              : cg == 16 ? k_up_surv_count_grouped<16> : k_up_surv_count_grouped<8>;
-      CK(launch_kernel(kc, dim3(grid_for(((u64)c.nl_old + ntail) * cg, gb)), dim3(gb), 0, s,
-          c.nl_old, nsame_l, ntail, same_l, newid_h, old.offs, old.adj, c.cnt, c.surv));
-    } else {
-      CK(launch_kernel(k_up_surv_count, dim3(grid_for((u64)c.nl_old + ntail, gb)), dim3(gb), 0,
-          s, c.nl_old, nsame_l, ntail, same_l, newid_h, old.offs, old.adj, c.cnt, c.surv));
-    }
+    // same_l and the old offsets, the new counts (and kept counts)
+    PROBE(P_CARRY_UP, s, 8.0 * (c.nl_old + 1) + 4.0 * c.nl * (c.surv ? 2.0 : 1.0));
+    CK(launch_kernel(k_up_row_lens, dim3(grid_for((u64)c.nl_old + ntail, gb)), dim3(gb), 0, s,
+        c.nl_old, nsame_l, ntail, same_l, old.offs, c.cnt, c.surv));
     CK_LAUNCH();
   }
-  if (c.nuses > c.first) {
-    PROBE(P_UP_COUNT, s, 4.0 * (c.nuses - c.first) + 4.0 * c.nl);
-    CK(launch_kernel(k_up_gen_count, dim3(grid_for(c.nuses - c.first, gb)), dim3(gb), 0, s,
-        c.first, c.nuses, c.loh, c.cnt));
+  {
+    u64 const ngen = c.nuses > c.first ? c.nuses - c.first : 0;
+    // the highs' new ids, and per generated use its low and the count
+    PROBE(P_UP_COUNT, s, 4.0 * c.nh_old + 8.0 * ngen);
+    CK(launch_kernel(k_up_adjust, dim3(grid_for((u64)c.nh_old + ngen, gb)), dim3(gb), 0, s,
+        c.nh_old, c.lph, newid_h, m.ask_down(high, low), same_l, c.cnt, c.surv, c.first,
+        c.nuses, c.loh));
     CK_LAUNCH();
   }
   c.u.offs = dalloc<u32>((size_t)c.nl + 1, s);
@@ -1740,10 +1710,8 @@ double Mesh::min_quality()
 {
   double const* q = qualities();
   u32 ne = count(dim);
-  unsigned long long* hk = static_cast<unsigned long long*>(pinned_scratch());
-  CK(cudaMemcpyAsync(hk, q + ne, sizeof(*hk), cudaMemcpyDeviceToHost, s));
-  stream_sync(s);
-  unsigned long long k = *hk;
+  u32 const* w = mb->read(s, reinterpret_cast<u32 const*>(q + ne), 2);
+  unsigned long long k = (unsigned long long)w[0] | ((unsigned long long)w[1] << 32);
   if (k == ~0ull) return DBL_MAX;
   return from_order_key(k);
 }

@@ -519,25 +519,39 @@ void Mailbox::clear(cudaStream_t s)
   CK(cudaMemsetAsync(dev, 0, 64 * sizeof(u32), s));
 }
 
-__global__ void k_mailbox_post(u32 const* __restrict__ dev, u32 n, u32* host, u32 seq)
+// dst: the host words' device address; seq_at: the sequence word's
+__global__ void k_mailbox_post(u32 const* __restrict__ src, u32 n, u32* dst, u32* seq_at,
+    u32 seq)
 {
   pdl_wait();
   u32 i = threadIdx.x;
   if (i < n) {
-    reinterpret_cast<volatile u32*>(host)[i] = dev[i];
-    __threadfence_system();  // this slot reaches the host before the sequence word
+    reinterpret_cast<volatile u32*>(dst)[i] = src[i];
+    __threadfence_system();  // this word reaches the host before the sequence word
   }
   __syncthreads();
-  if (i == 0) reinterpret_cast<volatile u32*>(host)[Mailbox::SEQ_SLOT] = seq;
+  if (i == 0) *reinterpret_cast<volatile u32*>(seq_at) = seq;
+}
+
+u32 const* Mailbox::read(cudaStream_t s, u32 const* src, u32 nwords)
+{
+  if (nwords > 16) throw Failure(E_ARG, "mailbox read: at most 16 words");
+  post(s, src, nwords, READ_SLOT);
+  return host + READ_SLOT;
 }
 
 void Mailbox::fetch(cudaStream_t s, u32 nslots)
 {
-  if (nslots > 64) nslots = 64;
+  post(s, dev, nslots > 64 ? 64 : nslots, 0);
+}
+
+void Mailbox::post(cudaStream_t s, u32 const* src, u32 nslots, u32 at)
+{
   u32 const want = ++seq;
   g_syncs.fetch_add(1, std::memory_order_relaxed);
   auto t0 = std::chrono::steady_clock::now();
-  CK(launch_kernel(k_mailbox_post, dim3(1), dim3(64), 0, s, dev, nslots, hdev, want));
+  CK(launch_kernel(k_mailbox_post, dim3(1), dim3(64), 0, s, src, nslots, hdev + at,
+      hdev + SEQ_SLOT, want));
   CK_LAUNCH();
   volatile u32* flag = host + SEQ_SLOT;
   for (u64 it = 1; *flag != want; ++it) {
@@ -549,7 +563,7 @@ void Mailbox::fetch(cudaStream_t s, u32 nslots)
     if (st == cudaErrorNotReady) continue;
     CK(st);
     if (*flag == want) break;
-    CK(cudaMemcpyAsync(host, dev, nslots * sizeof(u32), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(host + at, src, nslots * sizeof(u32), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     break;
   }

@@ -216,6 +216,12 @@ struct Mailbox {
   void release();
   void clear(cudaStream_t s);                 // zero the device slots
   void fetch(cudaStream_t s, u32 nslots = 64);  // the first nslots slots to host
+  // nwords (at most 16) 32-bit words of any device array, the same way,
+  // into host[READ_SLOT..]; returns that host address
+  static constexpr u32 READ_SLOT = SEQ_SLOT + 16;
+  u32 const* read(cudaStream_t s, u32 const* src, u32 nwords);
+  // nslots words of src into host[at..] and the sequence word after them
+  void post(cudaStream_t s, u32 const* src, u32 nslots, u32 at);
 };
 
 }  // namespace osh
