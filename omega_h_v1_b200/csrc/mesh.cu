@@ -629,52 +629,91 @@ __device__ inline void low_key(u32 const* __restrict__ vol, u32 i, u32* w)
   sort_small(w, VPL);
 }
 
-// marks (optional): only entities whose smallest vertex is marked are listed
+// The rows of the edges (low 1) and the triangles (low 2) are built in the
+// same launches when both are needed (blockIdx.y: the job). marks
+// (optional): only entities whose smallest vertex is marked are listed.
+struct KeyJob {
+  u32 low, nl;
+  u32 const* vol;
+  u32* cnt;
+  u32 const* offs;
+  u32* rows;
+};
+struct KeyJobs {
+  KeyJob j[2];
+};
+
 template <u32 VPL>
-__global__ void k_count_key_rows(u32 nl, u32 const* __restrict__ vol,
-    u32 const* __restrict__ marks, u32* cnt)
+__device__ inline void count_key_row(KeyJob const& jb, u32 i, u32 const* __restrict__ marks)
+{
+  u32 w[VPL];
+  low_key<VPL>(jb.vol, i, w);
+  if (marks && !marks[w[0]]) return;
+  atomicAdd(&jb.cnt[key_row<VPL>(w)], 1u);
+}
+
+__global__ void k_count_key_rows(KeyJobs jobs, u32 const* __restrict__ marks)
 {
   pdl_wait();
+  KeyJob const& jb = jobs.j[blockIdx.y];
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= nl) return;
-  u32 w[VPL];
-  low_key<VPL>(vol, i, w);
-  if (marks && !marks[w[0]]) return;
-  atomicAdd(&cnt[key_row<VPL>(w)], 1u);
+  if (i >= jb.nl) return;
+  if (jb.low == 1)
+    count_key_row<2>(jb, i, marks);
+  else
+    count_key_row<3>(jb, i, marks);
 }
 
 // cnt holds each sub-row's count; a row's records take its slots from the
 // end down: uint2 {v1, id} for edges, uint4 {v1, v2, id, 0} for triangles
 template <u32 VPL>
-__global__ void k_fill_key_rows(u32 nl, u32 const* __restrict__ vol,
-    u32 const* __restrict__ marks, u32 const* __restrict__ offs, u32* cnt,
-    u32* __restrict__ rows)
+__device__ inline void fill_key_row(KeyJob const& jb, u32 i, u32 const* __restrict__ marks)
 {
-  pdl_wait();
-  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= nl) return;
   u32 w[VPL];
-  low_key<VPL>(vol, i, w);
+  low_key<VPL>(jb.vol, i, w);
   if (marks && !marks[w[0]]) return;
   u32 b = key_row<VPL>(w);
-  u32 slot = offs[b] + atomicSub(&cnt[b], 1u) - 1u;
+  u32 slot = jb.offs[b] + atomicSub(&jb.cnt[b], 1u) - 1u;
   if (VPL == 2)
-    reinterpret_cast<uint2*>(rows)[slot] = make_uint2(w[1], i);
+    reinterpret_cast<uint2*>(jb.rows)[slot] = make_uint2(w[1], i);
   else
-    reinterpret_cast<uint4*>(rows)[slot] = make_uint4(w[1], w[VPL - 1], i, 0u);
+    reinterpret_cast<uint4*>(jb.rows)[slot] = make_uint4(w[1], w[VPL - 1], i, 0u);
+}
+
+__global__ void k_fill_key_rows(KeyJobs jobs, u32 const* __restrict__ marks)
+{
+  pdl_wait();
+  KeyJob const& jb = jobs.j[blockIdx.y];
+  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= jb.nl) return;
+  if (jb.low == 1)
+    fill_key_row<2>(jb, i, marks);
+  else
+    fill_key_row<3>(jb, i, marks);
 }
 
 // One thread per high entity: every wanted low's sub-row bounds are loaded
-// together, then each sub-row is read four records at a time.
+// together, then each sub-row is read four records at a time. The
+// searches of a pass's pairs share a launch (blockIdx.y: the pair).
+struct ReflectJob {
+  u32 high, low, first, nh;
+  u32 const* voh;
+  u32 const* offs;
+  u32 const* rows;
+  u32* out;
+};
+struct ReflectJobs {
+  ReflectJob j[3];
+};
+
 template <u32 HIGH, u32 LOW>
-__global__ void k_reflect_keyed(u32 first, u32 nh, u32 const* __restrict__ voh,
-    u32 const* __restrict__ offs, u32 const* __restrict__ rows, u32* __restrict__ out)
+__device__ inline void reflect_keyed(ReflectJob const& jb, u32 i)
 {
-  pdl_wait();
   constexpr u32 LPH = HIGH == 3 ? (LOW == 1 ? 6 : 4) : 3;
   constexpr u32 VPH = HIGH + 1, VPL = LOW + 1;
-  u32 i = first + blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= nh) return;
+  u32 const* __restrict__ voh = jb.voh;
+  u32 const* __restrict__ offs = jb.offs;
+  u32 const* __restrict__ rows = jb.rows;
   u32 v[VPH];
 #pragma unroll
   for (u32 k = 0; k < VPH; ++k) v[k] = voh[(size_t)i * VPH + k];
@@ -714,8 +753,22 @@ __global__ void k_reflect_keyed(u32 first, u32 nh, u32 const* __restrict__ voh,
           if (x[q].x == t[j][1] && x[q].y == t[j][VPL - 1]) found = x[q].z;
       }
     }
-    out[(size_t)i * LPH + j] = found;
+    jb.out[(size_t)i * LPH + j] = found;
   }
+}
+
+__global__ void k_reflect_keyed(ReflectJobs jobs)
+{
+  pdl_wait();
+  ReflectJob const& jb = jobs.j[blockIdx.y];
+  u32 i = jb.first + blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= jb.nh) return;
+  if (jb.high == 2)
+    reflect_keyed<2, 1>(jb, i);
+  else if (jb.low == 1)
+    reflect_keyed<3, 1>(jb, i);
+  else
+    reflect_keyed<3, 2>(jb, i);
 }
 
 // ---------------------------------------------------------------------------
@@ -975,49 +1028,83 @@ void Mesh::drop_search_rows()
   search_marks = nullptr;
 }
 
-void Mesh::build_low_rows(u32 low)
+// the search rows of the listed lows (1: edges, 2: triangles) that are
+// not built yet, the two built in the same launches
+void Mesh::build_low_rows(u32 const* lows, u32 nlows)
 {
-  if (low_rows[low]) return;
-  u32 const* vol = ask_down(low, 0);
-  u32 nl = counts[low];
-  size_t nb = (size_t)counts[0] * (low == 1 ? KeyRows<2>::SUB : KeyRows<3>::SUB);
-  if (nb >= 0xffffffffull) throw Failure(E_ARG, "reflect_down: too many vertices");
-  u32* cnt = dalloc<u32>(nb + 1, s);
-  CK(cudaMemsetAsync(cnt, 0, sizeof(u32) * (nb + 1), s));
-  if (nl) {
-    auto k = low == 1 ? k_count_key_rows<2> : k_count_key_rows<3>;
-    CK(launch_kernel(k, dim3(grid_for(nl)), dim3(BLOCK), 0, s, nl, vol, search_marks, cnt));
+  KeyJobs jobs;
+  u32 nj = 0, most = 0;
+  u32* cnts[2] = {nullptr, nullptr};
+  ScanJob sj[2];
+  for (u32 q = 0; q < nlows; ++q) {
+    u32 low = lows[q];
+    if (low_rows[low]) continue;
+    u32 const* vol = ask_down(low, 0);
+    u32 nl = counts[low];
+    size_t nb = (size_t)counts[0] * (low == 1 ? KeyRows<2>::SUB : KeyRows<3>::SUB);
+    if (nb >= 0xffffffffull) throw Failure(E_ARG, "reflect_down: too many vertices");
+    u32* cnt = dalloc<u32>(nb + 1, s);
+    CK(cudaMemsetAsync(cnt, 0, sizeof(u32) * (nb + 1), s));
+    low_row_offs[low] = dalloc<u32>(nb + 1, s);
+    low_rows[low] = dalloc<u32>((size_t)nl * (low == 1 ? 2 : 4), s);
+    jobs.j[nj] = KeyJob{low, nl, vol, cnt, low_row_offs[low], low_rows[low]};
+    sj[nj] = ScanJob{cnt, low_row_offs[low], nullptr, nullptr, (u32)nb, 0};
+    cnts[nj] = cnt;
+    most = std::max(most, nl);
+    ++nj;
+  }
+  if (!nj) return;
+  if (most) {
+    CK(launch_kernel(k_count_key_rows, dim3(grid_for(most), nj), dim3(BLOCK), 0, s, jobs,
+        search_marks));
     CK_LAUNCH();
   }
-  low_row_offs[low] = exscan_new(cnt, (u32)nb, s);
-  low_rows[low] = dalloc<u32>((size_t)nl * (low == 1 ? 2 : 4), s);
-  if (nl) {
-    auto k = low == 1 ? k_fill_key_rows<2> : k_fill_key_rows<3>;
-    CK(launch_kernel(k, dim3(grid_for(nl)), dim3(BLOCK), 0, s, nl, vol, search_marks,
-        low_row_offs[low], cnt, low_rows[low]));
+  exscan_jobs(sj, nj, s);
+  if (most) {
+    CK(launch_kernel(k_fill_key_rows, dim3(grid_for(most), nj), dim3(BLOCK), 0, s, jobs,
+        search_marks));
     CK_LAUNCH();
   }
-  dev_free(cnt, s);
+  for (u32 q = 0; q < nj; ++q) dev_free(cnts[q], s);
+}
+
+// down(high, low) of the high entities first..count(high)-1 of each listed
+// pair into outs[q] (the survivors' part is the caller's), one launch
+void Mesh::reflect_many(u32 const* highs, u32 const* lows, u32 const* firsts, u32* const* outs,
+    u32 npairs)
+{
+  u32 need[2], nneed = 0;
+  for (u32 q = 0; q < npairs; ++q) {
+    if (firsts[q] >= count(highs[q])) continue;
+    bool have = false;
+    for (u32 k = 0; k < nneed; ++k) have = have || need[k] == lows[q];
+    if (!have) need[nneed++] = lows[q];
+  }
+  if (!nneed) return;
+  build_low_rows(need, nneed);
+  ReflectJobs jobs;
+  u32 nj = 0, most = 0;
+  double bytes = 0;
+  for (u32 q = 0; q < npairs; ++q) {
+    u32 high = highs[q], low = lows[q], first = firsts[q], nh = count(high);
+    if (first >= nh) continue;
+    jobs.j[nj++] = ReflectJob{high, low, first, nh, ask_down(high, 0), low_row_offs[low],
+        low_rows[low], outs[q]};
+    most = std::max(most, nh - first);
+    // voh once, each wanted low's sub-row bounds and its records (a few of
+    // 8 / 16 bytes) once, out once
+    double n = (double)(nh - first) * deg(high, low), rec = low == 1 ? 8.0 : 16.0;
+    bytes += 4.0 * deg(high, 0) * (nh - first) + (8.0 + 4.0 * rec) * n + 4.0 * n;
+  }
+  PROBE(P_REFLECT_DOWN, s, bytes);
+  u32 const gb = tuned(TK_GATHER_BLOCK);
+  CK(launch_kernel(k_reflect_keyed, dim3(grid_for(most, gb), nj), dim3(gb), 0, s, jobs));
+  CK_LAUNCH();
 }
 
 void Mesh::reflect_range(u32 high, u32 low, u32 first, u32* out)
 {
-  u32 nh = count(high);
-  if (first >= nh) return;
-  u32 const* voh = ask_down(high, 0);
-  build_low_rows(low);
-  u32 n = (nh - first) * deg(high, low);
-  // voh once, each wanted low's sub-row bounds and its records (a few of
-  // 8 / 16 bytes) once, out once
-  double rec = low == 1 ? 8.0 : 16.0;
-  PROBE(P_REFLECT_DOWN, s, 4.0 * deg(high, 0) * (nh - first) + (8.0 + 4.0 * rec) * n + 4.0 * n);
-  u32 const gb = tuned(TK_GATHER_BLOCK);
-  u32 g = grid_for(nh - first, gb);
-  auto k = high == 3 && low == 2 ? k_reflect_keyed<3, 2>
-         : high == 3 ? k_reflect_keyed<3, 1> : k_reflect_keyed<2, 1>;
-  CK(launch_kernel(k, dim3(g), dim3(gb), 0, s, first, nh, voh, low_row_offs[low],
-      low_rows[low], out));
-  CK_LAUNCH();
+  reflect_many(&high, &low, &first, &out, 1);
 }
 
 // new ids of a surviving high entity's lows: its old lows through the lows'
@@ -1028,12 +1115,26 @@ void Mesh::reflect_range(u32 high, u32 low, u32 first, u32* out)
 // waiting on two dependent loads per entry.
 constexpr u32 CARRY_UNROLL = 4;
 
+// the carries of a pass's pairs share a launch (blockIdx.y: the pair)
+struct DownJob {
+  u32 n, lph;
+  u32 const* same_h;
+  u32 const* same_l;
+  u32 const* old_down;
+  u32* out;
+};
+struct DownJobs {
+  DownJob j[3];
+};
+
 template <u32 LPH>
-__global__ void __launch_bounds__(512) k_carry_down(u32 n, u32 const* __restrict__ same_h,
-    u32 const* __restrict__ same_l, u32 const* __restrict__ old_down, u32* __restrict__ out)
+__device__ inline void carry_down_rows(DownJob const& jb)
 {
-  pdl_wait();
-  u32 const bs = blockDim.x;
+  u32 const* __restrict__ same_h = jb.same_h;
+  u32 const* __restrict__ same_l = jb.same_l;
+  u32 const* __restrict__ old_down = jb.old_down;
+  u32* __restrict__ out = jb.out;
+  u32 const n = jb.n, bs = blockDim.x;
   u32 base = blockIdx.x * (bs * CARRY_UNROLL) + threadIdx.x;
   u32 od[CARRY_UNROLL], ni[CARRY_UNROLL], nn[CARRY_UNROLL];
 #pragma unroll
@@ -1055,56 +1156,71 @@ __global__ void __launch_bounds__(512) k_carry_down(u32 n, u32 const* __restrict
   }
 }
 
-void carry_down(Mesh& m, Mesh& out, u32 high, u32 low, u32 const* same_h, u32 nsame,
-    u32 const* same_l)
+__global__ void __launch_bounds__(512) k_carry_down(DownJobs jobs)
 {
-  if (!m.down[high][low] || out.down[high][low] || !out.has_dim(high) || !out.has_dim(low))
-    return;
-  cudaStream_t s = out.s;
-  u32 nh_old = m.counts[high], nh = out.count(high), lph = deg(high, low);
-  out.count(low);
-  u32* dn = dalloc<u32>((size_t)nh * lph, s);
-  if (nh_old) {
-    u32 n = nh_old * lph;
-    u32 const gb = tuned(TK_GATHER_BLOCK);
-    u32 g = (u32)ceil_div((u64)n, (u64)gb * CARRY_UNROLL);
-    PROBE(P_CARRY, s, 4.0 * (nh_old + 1) + 12.0 * n);
-    auto k = lph == 3 ? k_carry_down<3> : lph == 4 ? k_carry_down<4> : k_carry_down<6>;
-    CK(launch_kernel(k, dim3(g), dim3(gb), 0, s, n, same_h, same_l, m.down[high][low], dn));
-    CK_LAUNCH();
-  }
-  // the survivors come first; the entities the pass made are searched
-  out.reflect_range(high, low, nsame, dn);
-  out.down[high][low] = dn;
+  pdl_wait();
+  DownJob const& jb = jobs.j[blockIdx.y];
+  if (jb.lph == 3)
+    carry_down_rows<3>(jb);
+  else if (jb.lph == 4)
+    carry_down_rows<4>(jb);
+  else
+    carry_down_rows<6>(jb);
 }
 
 void carry_down_all(Mesh& m, Mesh& out, u32* const* same_of, u32 const* nsame_of)
 {
   u32 const dim = m.dim;
-  // the products whose lows are searched, and whether they touch few
-  // enough vertices for rows limited to them (a quarter of the vertices at
-  // most, four per product)
-  bool search = false;
+  cudaStream_t s = out.s;
+  // the pairs carried: the survivors' part in one launch, then the
+  // products' part searched in one launch
+  u32 hs[3], ls[3], firsts[3];
+  u32* dns[3];
+  u32 np = 0;
+  DownJobs jobs;
+  u32 nj = 0;
+  u64 most = 0;
+  double bytes = 0;
   u64 nprod = 0;
   u32 first[4] = {0, 0, 0, 0};
   for (u32 h = 2; h <= dim; ++h) {
     first[h] = out.has_dim(h) ? out.count(h) : 0;
-    for (u32 l = 1; l < h; ++l)
-      if (same_of[h] && same_of[l] && m.down[h][l] && !out.down[h][l] && out.has_dim(h) &&
-          out.has_dim(l)) {
-        search = true;
-        first[h] = nsame_of[h];
+    for (u32 l = 1; l < h; ++l) {
+      if (!same_of[h] || !same_of[l]) continue;
+      if (!m.down[h][l] || out.down[h][l] || !out.has_dim(h) || !out.has_dim(l)) continue;
+      u32 nh_old = m.counts[h], nh = out.count(h), lph = deg(h, l);
+      out.count(l);
+      u32* dn = dalloc<u32>((size_t)nh * lph, s);
+      if (nh_old) {
+        u32 n = nh_old * lph;
+        jobs.j[nj++] = DownJob{n, lph, same_of[h], same_of[l], m.down[h][l], dn};
+        most = std::max<u64>(most, n);
+        bytes += 4.0 * (nh_old + 1) + 12.0 * n;
       }
+      hs[np] = h;
+      ls[np] = l;
+      firsts[np] = nsame_of[h];
+      dns[np] = dn;
+      ++np;
+      first[h] = nsame_of[h];
+    }
     nprod += out.has_dim(h) ? out.count(h) - first[h] : 0;
   }
-  bool const marked = search && !out.low_rows[1] && !out.low_rows[2] && !out.search_marks &&
+  if (nj) {
+    PROBE(P_CARRY, s, bytes);
+    u32 const gb = tuned(TK_GATHER_BLOCK);
+    u32 g = (u32)ceil_div(most, (u64)gb * CARRY_UNROLL);
+    CK(launch_kernel(k_carry_down, dim3(g, nj), dim3(gb), 0, s, jobs));
+    CK_LAUNCH();
+  }
+  // rows limited to the products' vertices when the products touch few
+  // enough of them (a quarter of the vertices at most, four per product)
+  bool const marked = np && !out.low_rows[1] && !out.low_rows[2] && !out.search_marks &&
       16 * nprod < out.count(0);
   if (marked) out.mark_search_verts(first);
-  for (u32 h = 2; h <= dim; ++h)
-    for (u32 l = 1; l < h; ++l)
-      if (same_of[h] && same_of[l])
-        carry_down(m, out, h, l, same_of[h], nsame_of[h], same_of[l]);
+  out.reflect_many(hs, ls, firsts, dns, np);
   if (marked) out.drop_search_rows();
+  for (u32 q = 0; q < np; ++q) out.down[hs[q]][ls[q]] = dns[q];
 }
 
 // up(low, high) carried through a pass. A surviving low keeps the uses of
@@ -1201,13 +1317,39 @@ __global__ void k_up_surv_fill(u32 nl_old, u32 const* __restrict__ same_l,
 // a group's lanes share their row, so they loop and leave together.
 constexpr u32 LONG_ROW_USES = 8;
 
+// the vertex-row fills of a pass's carried pairs share a launch
+// (blockIdx.y: the pair)
+struct UpFillJob {
+  u32 nl_old;
+  u32 const* same_l;
+  u32 const* newid_h;
+  u32 const* offs_old;
+  u32 const* adj_old;
+  u32 const* dirs_old;
+  u32 const* offs;
+  u32* adj;
+  u32* dirs;
+  UpGen gen;
+};
+struct UpFillJobs {
+  UpFillJob j[6];
+};
+
 template <u32 CG>
-__global__ void k_up_surv_fill_grouped(u32 nl_old, u32 const* __restrict__ same_l,
-    u32 const* __restrict__ newid_h, u32 const* __restrict__ offs_old,
-    u32 const* __restrict__ adj_old, u32 const* __restrict__ dirs_old,
-    u32 const* __restrict__ offs, u32* __restrict__ adj, u32* __restrict__ dirs, UpGen gen)
+__global__ void k_up_surv_fill_grouped(UpFillJobs jobs)
 {
   pdl_wait();
+  UpFillJob const& jb = jobs.j[blockIdx.y];
+  u32 const nl_old = jb.nl_old;
+  u32 const* __restrict__ same_l = jb.same_l;
+  u32 const* __restrict__ newid_h = jb.newid_h;
+  u32 const* __restrict__ offs_old = jb.offs_old;
+  u32 const* __restrict__ adj_old = jb.adj_old;
+  u32 const* __restrict__ dirs_old = jb.dirs_old;
+  u32 const* __restrict__ offs = jb.offs;
+  u32* __restrict__ adj = jb.adj;
+  u32* __restrict__ dirs = jb.dirs;
+  UpGen const gen = jb.gen;
   u32 const t = blockIdx.x * blockDim.x + threadIdx.x;
   u32 const j = t / CG, g = t % CG;
   if (j >= nl_old) {
@@ -1247,46 +1389,62 @@ __global__ void k_up_surv_fill_grouped(u32 nl_old, u32 const* __restrict__ same_
 // the rows the pass made); k_up_adjust takes a use off for every low of a
 // removed high (new id INV) that survives and adds the generated uses.
 // (Counting the kept uses row by row gathered a new id for every old use.)
-__global__ void k_up_row_lens(u32 nl_old, u32 nsame_l, u32 ntail,
-    u32 const* __restrict__ same_l, u32 const* __restrict__ offs_old, u32* __restrict__ cnt,
-    u32* __restrict__ surv)
+// (the counts of a pass's carried pairs share each launch: blockIdx.y is
+// the pair)
+struct UpCountJob {
+  u32 nl_old, nsame_l, ntail, nh_old, lph, first, nuses;
+  u32 const* same_l;
+  u32 const* offs_old;
+  u32 const* newid_h;
+  u32 const* old_loh;
+  u32 const* loh;
+  u32* cnt;
+  u32* surv;
+};
+struct UpCountJobs {
+  UpCountJob j[6];
+};
+
+__global__ void k_up_row_lens(UpCountJobs jobs)
 {
   pdl_wait();
+  UpCountJob const& jb = jobs.j[blockIdx.y];
   u32 j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= nl_old) {
-    if (j - nl_old < ntail) {
-      u32 r = nsame_l + (j - nl_old);
+  u32* __restrict__ cnt = jb.cnt;
+  u32* __restrict__ surv = jb.surv;
+  if (j >= jb.nl_old) {
+    if (j - jb.nl_old < jb.ntail) {
+      u32 r = jb.nsame_l + (j - jb.nl_old);
       cnt[r] = 0;
       if (surv) surv[r] = 0;
     }
     return;
   }
-  u32 nj = same_l[j];
-  if (same_l[j + 1] == nj) return;
-  u32 len = offs_old[j + 1] - offs_old[j];
+  u32 nj = jb.same_l[j];
+  if (jb.same_l[j + 1] == nj) return;
+  u32 len = jb.offs_old[j + 1] - jb.offs_old[j];
   cnt[nj] = len;
   if (surv) surv[nj] = len;
 }
 
-__global__ void k_up_adjust(u32 nh_old, u32 lph, u32 const* __restrict__ newid_h,
-    u32 const* __restrict__ old_loh, u32 const* __restrict__ same_l, u32* cnt, u32* surv,
-    u32 first, u32 nuses, u32 const* __restrict__ loh)
+__global__ void k_up_adjust(UpCountJobs jobs)
 {
   pdl_wait();
+  UpCountJob const& jb = jobs.j[blockIdx.y];
   u32 t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t < nh_old) {
-    if (newid_h[t] != INV) return;
-    for (u32 k = 0; k < lph; ++k) {
-      u32 l = old_loh[(size_t)t * lph + k];
-      u32 nl = same_l[l];
-      if (same_l[l + 1] == nl) continue;
-      atomicSub(&cnt[nl], 1u);
-      if (surv) atomicSub(&surv[nl], 1u);
+  if (t < jb.nh_old) {
+    if (jb.newid_h[t] != INV) return;
+    for (u32 k = 0; k < jb.lph; ++k) {
+      u32 l = jb.old_loh[(size_t)t * jb.lph + k];
+      u32 nl = jb.same_l[l];
+      if (jb.same_l[l + 1] == nl) continue;
+      atomicSub(&jb.cnt[nl], 1u);
+      if (jb.surv) atomicSub(&jb.surv[nl], 1u);
     }
     return;
   }
-  u32 u = first + (t - nh_old);
-  if (u < nuses) atomicAdd(&cnt[loh[u]], 1u);
+  u32 u = jb.first + (t - jb.nh_old);
+  if (u < jb.nuses) atomicAdd(&jb.cnt[jb.loh[u]], 1u);
 }
 
 u32* carry_new_ids(u32 const* same, u32 n, cudaStream_t s)
@@ -1313,10 +1471,11 @@ struct UpCarry {
   u32* cnt = nullptr;
   u32* surv = nullptr;
   UpAdj u;
+  UpCountJob cj;
 };
 
-// everything up to the counts: false when the pair is not carried
-bool carry_up_count(Mesh& m, Mesh& out, u32 low, u32 high, u32 const* same_l, u32 nsame_l,
+// the pair's arrays and its count job: false when the pair is not carried
+bool carry_up_setup(Mesh& m, Mesh& out, u32 low, u32 high, u32 const* same_l, u32 nsame_l,
     u32 nsame_h, u32 const* newid_h, UpCarry& c)
 {
   if (!m.have_up[low][high] || out.have_up[low][high]) return false;
@@ -1345,30 +1504,31 @@ bool carry_up_count(Mesh& m, Mesh& out, u32 low, u32 high, u32 const* same_l, u3
   c.nuses_old = m.counts[high] * c.lph;
   // rows of 8 or more uses on average (vertex rows) take a lane group each
   c.long_rows = c.nl_old && (u64)c.nuses_old >= (u64)LONG_ROW_USES * c.nl_old;
-  u32 const gb = tuned(TK_GATHER_BLOCK);
-  {
-    u32 ntail = c.nl + 1 - nsame_l;
-    // same_l and the old offsets, the new counts (and kept counts)
-    PROBE(P_CARRY_UP, s, 8.0 * (c.nl_old + 1) + 4.0 * c.nl * (c.surv ? 2.0 : 1.0));
-    CK(launch_kernel(k_up_row_lens, dim3(grid_for((u64)c.nl_old + ntail, gb)), dim3(gb), 0, s,
-        c.nl_old, nsame_l, ntail, same_l, old.offs, c.cnt, c.surv));
-    CK_LAUNCH();
-  }
-  {
-    u64 const ngen = c.nuses > c.first ? c.nuses - c.first : 0;
-    // the highs' new ids, and per generated use its low and the count
-    PROBE(P_UP_COUNT, s, 4.0 * c.nh_old + 8.0 * ngen);
-    CK(launch_kernel(k_up_adjust, dim3(grid_for((u64)c.nh_old + ngen, gb)), dim3(gb), 0, s,
-        c.nh_old, c.lph, newid_h, m.ask_down(high, low), same_l, c.cnt, c.surv, c.first,
-        c.nuses, c.loh));
-    CK_LAUNCH();
-  }
+  // the count kernels' job (launched with the other pairs')
+  UpCountJob& j = c.cj;
+  j.nl_old = c.nl_old;
+  j.nsame_l = nsame_l;
+  j.ntail = c.nl + 1 - nsame_l;
+  j.nh_old = c.nh_old;
+  j.lph = c.lph;
+  j.first = c.first;
+  j.nuses = c.nuses;
+  j.same_l = same_l;
+  j.offs_old = old.offs;
+  j.newid_h = newid_h;
+  j.old_loh = m.ask_down(high, low);
+  j.loh = c.loh;
+  j.cnt = c.cnt;
+  j.surv = c.surv;
   c.u.offs = dalloc<u32>((size_t)c.nl + 1, s);
   return true;
 }
 
-// after the scan of the counts: the rows' fill, and the adjacency installed
-void carry_up_fill(Mesh& m, Mesh& out, UpCarry& c)
+// after the scan of the counts: the rows' fill (edge and face rows here, a
+// launch per pair; vertex rows into `grouped`, launched for all pairs
+// together), and the adjacency installed
+void carry_up_fill(Mesh& m, Mesh& out, UpCarry& c, UpFillJobs& grouped, u32& ngrouped,
+    u64& gmost, double& gbytes)
 {
   cudaStream_t s = out.s;
   UpAdj const& old = m.up[c.low][c.high];
@@ -1377,29 +1537,34 @@ void carry_up_fill(Mesh& m, Mesh& out, UpCarry& c)
   u.dirs = dalloc<u32>(c.nuses, s);
   u32 const cg = tuned(TK_CARRY_GROUP), gb = tuned(TK_GATHER_BLOCK);
   u64 const ngen = c.nuses > c.first ? c.nuses - c.first : 0;
-  if (c.nl_old || ngen) {
+  UpGen const gen{c.first, c.nuses, c.lph, c.loh, c.cnt};
+  if (c.long_rows) {
+    grouped.j[ngrouped++] = UpFillJob{c.nl_old, c.same_l, c.newid_h, old.offs, old.adj,
+        old.dirs, u.offs, u.adj, u.dirs, gen};
+    gmost = std::max<u64>(gmost, (u64)c.nl_old * cg + ngen);
+    gbytes += 8.0 * (c.nl_old + 1) + 8.0 * c.nuses_old + 4.0 * c.nh_old + 4.0 * (c.nl + 1) +
+        8.0 * c.first + 20.0 * ngen;
+  } else if (c.nl_old || ngen) {
     // each array once: same_l and the old offsets, the old rows' highs and
     // directions, the highs' new ids, the new offsets, the kept uses (first)
     // written as highs and directions; per generated use its low, the
     // row's offset and count, and the use written
     // (the fill of edge and face rows, the largest single kernel of an
     // adapt, is probed on its own: carry_up_fill)
-    PROBE(c.long_rows ? P_CARRY_UP : P_CARRY_UP_FILL, s, 8.0 * (c.nl_old + 1) +
-        8.0 * c.nuses_old + 4.0 * c.nh_old + 4.0 * (c.nl + 1) + 8.0 * c.first + 20.0 * ngen);
-    UpGen const gen{c.first, c.nuses, c.lph, c.loh, c.cnt};
-    if (c.long_rows) {
-      auto kf = cg == 4 ? k_up_surv_fill_grouped<4>
-              : cg == 16 ? k_up_surv_fill_grouped<16> : k_up_surv_fill_grouped<8>;
-      CK(launch_kernel(kf, dim3(grid_for((u64)c.nl_old * cg + ngen, gb)), dim3(gb), 0, s,
-          c.nl_old, c.same_l, c.newid_h, old.offs, old.adj, old.dirs, u.offs, u.adj, u.dirs,
-          gen));
-    } else {
-      CK(launch_kernel(k_up_surv_fill, dim3(grid_for((u64)c.nl_old + ngen, gb)), dim3(gb), 0,
-          s, c.nl_old, c.same_l, c.newid_h, old.offs, old.adj, old.dirs, u.offs, u.adj, u.dirs,
-          gen));
-    }
+    PROBE(P_CARRY_UP_FILL, s, 8.0 * (c.nl_old + 1) + 8.0 * c.nuses_old + 4.0 * c.nh_old +
+        4.0 * (c.nl + 1) + 8.0 * c.first + 20.0 * ngen);
+    CK(launch_kernel(k_up_surv_fill, dim3(grid_for((u64)c.nl_old + ngen, gb)), dim3(gb), 0,
+        s, c.nl_old, c.same_l, c.newid_h, old.offs, old.adj, old.dirs, u.offs, u.adj, u.dirs,
+        gen));
     CK_LAUNCH();
   }
+}
+
+// after every fill: the counts freed and the adjacency installed
+void carry_up_install(Mesh& out, UpCarry& c)
+{
+  cudaStream_t s = out.s;
+  UpAdj& u = c.u;
   dev_free(c.cnt, s);
   if (c.surv) {
     u.pre = c.surv;
@@ -1431,14 +1596,56 @@ void carry_up_all(Mesh& m, Mesh& out, u32* const* same_of, u32 const* nsame_of,
         if (!own_newid[h]) own_newid[h] = carry_new_ids(same_of[h], m.counts[h], s);
         newid_h = own_newid[h];
       }
-      if (carry_up_count(m, out, l, h, same_of[l], nsame_of[l], nsame_of[h], newid_h, cs[nc]))
+      if (carry_up_setup(m, out, l, h, same_of[l], nsame_of[l], nsame_of[h], newid_h, cs[nc]))
         ++nc;
     }
+  if (nc) {
+    // every pair's counts in one launch per stage: the surviving rows'
+    // lengths, then the removed and generated uses
+    UpCountJobs cj;
+    u64 most_rows = 0, most_adj = 0;
+    double bytes_rows = 0, bytes_adj = 0;
+    for (u32 k = 0; k < nc; ++k) {
+      UpCarry const& c = cs[k];
+      cj.j[k] = c.cj;
+      u64 const ngen = c.nuses > c.first ? c.nuses - c.first : 0;
+      most_rows = std::max<u64>(most_rows, (u64)c.nl_old + c.cj.ntail);
+      most_adj = std::max<u64>(most_adj, (u64)c.nh_old + ngen);
+      // same_l and the old offsets, the new counts (and kept counts); the
+      // highs' new ids, and per generated use its low and the count
+      bytes_rows += 8.0 * (c.nl_old + 1) + 4.0 * c.nl * (c.surv ? 2.0 : 1.0);
+      bytes_adj += 4.0 * c.nh_old + 8.0 * ngen;
+    }
+    u32 const gb = tuned(TK_GATHER_BLOCK);
+    {
+      PROBE(P_CARRY_UP, s, bytes_rows);
+      CK(launch_kernel(k_up_row_lens, dim3(grid_for(most_rows, gb), nc), dim3(gb), 0, s, cj));
+      CK_LAUNCH();
+    }
+    {
+      PROBE(P_UP_COUNT, s, bytes_adj);
+      CK(launch_kernel(k_up_adjust, dim3(grid_for(most_adj, gb), nc), dim3(gb), 0, s, cj));
+      CK_LAUNCH();
+    }
+  }
   ScanJob jobs[6];
   for (u32 k = 0; k < nc; ++k) jobs[k] = ScanJob{cs[k].cnt, cs[k].u.offs, nullptr, nullptr,
       cs[k].nl, 0};
   exscan_jobs(jobs, nc, s);
-  for (u32 k = 0; k < nc; ++k) carry_up_fill(m, out, cs[k]);
+  UpFillJobs grouped;
+  u32 ngrouped = 0;
+  u64 gmost = 0;
+  double gbytes = 0;
+  for (u32 k = 0; k < nc; ++k) carry_up_fill(m, out, cs[k], grouped, ngrouped, gmost, gbytes);
+  if (ngrouped) {
+    PROBE(P_CARRY_UP, s, gbytes);
+    u32 const cg = tuned(TK_CARRY_GROUP), gb = tuned(TK_GATHER_BLOCK);
+    auto kf = cg == 4 ? k_up_surv_fill_grouped<4>
+            : cg == 16 ? k_up_surv_fill_grouped<16> : k_up_surv_fill_grouped<8>;
+    CK(launch_kernel(kf, dim3(grid_for(gmost, gb), ngrouped), dim3(gb), 0, s, grouped));
+    CK_LAUNCH();
+  }
+  for (u32 k = 0; k < nc; ++k) carry_up_install(out, cs[k]);
   for (u32 h = 0; h < 4; ++h) dev_free(own_newid[h], s);
 }
 

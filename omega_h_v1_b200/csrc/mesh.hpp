@@ -134,7 +134,9 @@ struct Mesh {
 
   u32 const* ask_down(u32 high, u32 low);
   // reflect_down's rows for lows of dimension `low` (built once per state)
-  void build_low_rows(u32 low);
+  void build_low_rows(u32 const* lows, u32 nlows);
+  void reflect_many(u32 const* highs, u32 const* lows, u32 const* firsts, u32* const* outs,
+      u32 npairs);
   void mark_search_verts(u32 const* first);
   void drop_search_rows();
   // down(high, low) of the high entities [first, n_high) by search, into out
@@ -192,14 +194,13 @@ struct Mesh {
   void make_parallel();
 };
 
-// down(high, low) of `out`, the mesh a pass built from `m`, when m has it:
-// surviving high entities (same_h: survivor offsets of m's highs; the nsame
-// survivors are numbered first in out) take their old lows through same_l
-// (the lows' survivor offsets); the entities the pass made are searched
-void carry_down(Mesh& m, Mesh& out, u32 high, u32 low, u32 const* same_h, u32 nsame,
-    u32 const* same_l);
-// every carried downward adjacency of a pass (h = 2..dim, l = 1..h-1), the
-// products' search rows limited to the products' vertices when they are few
+// down(high, low) of `out`, the mesh a pass built from `m`, for every pair
+// m has (h = 2..dim, l = 1..h-1): surviving high entities (same_of[h]:
+// survivor offsets of m's highs; the nsame_of[h] survivors are numbered
+// first in out) take their old lows through same_of[l] (the lows' survivor
+// offsets), all pairs in one launch; the entities the pass made are
+// searched, all pairs in one launch, with search rows limited to the
+// products' vertices when they are few
 void carry_down_all(Mesh& m, Mesh& out, u32* const* same_of, u32 const* nsame_of);
 
 // up(low, high) of `out` for every pair m has: surviving lows keep their
