@@ -28,29 +28,6 @@ constexpr u32 COOP_CTL_SLOT = 44, COOP_CTL_WORDS = 7;
 static_assert(COOP_CTL_SLOT + COOP_CTL_WORDS == INDSET_FETCH_SLOTS, "mailbox slots");
 
 // also zeroes the control words of the rounds
-// The states (the filter's candidates undecided, the rest out of the set)
-// and round 0's list: the candidates, appended a warp at a time to the list
-// whose length is control word 2 (zero on entry: the rounds kernel zeroes
-// it when it settles, the host when a set fails). The other control words
-// are zeroed here.
-__global__ void k_indset_init(u32 n, u32 const* __restrict__ filter, u32* __restrict__ st,
-    u32* __restrict__ list0, u32* ctl)
-{
-  pdl_wait();
-  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < COOP_CTL_WORDS && i != 2) ctl[i] = 0;
-  bool const c = i < n && (!filter || filter[i]);
-  if (i < n) st[i] = c ? (u32)UNKNOWN : (u32)NOT_IN_SET;
-  unsigned const want = __ballot_sync(0xffffffffu, c);
-  if (want) {
-    u32 const lane = threadIdx.x & 31, leader = __ffs(want) - 1;
-    u32 base = 0;
-    if (lane == leader) base = atomicAdd(&ctl[2], (u32)__popc(want));
-    base = __shfl_sync(0xffffffffu, base, leader);
-    if (c) list0[base + __popc(want & ((1u << lane) - 1u))] = i;
-  }
-}
-
 // neighbourhood walks: mode 0 = vertices via edges, mode 1 = edges via
 // elements (3D tets or 2D triangles)
 struct Nbrs {
@@ -82,16 +59,18 @@ struct Nbrs {
 // fills the load/store queue.)
 //
 // All rounds run in one launch: a cooperative grid (every block resident)
-// runs round 0 over every entity and later rounds over the list the round
-// before left, separated by a grid barrier, until a round leaves no entity
-// undecided or 100 rounds have run. Control words (zeroed by
-// k_indset_init): [0] barrier arrivals, [1] barrier generation, [2..4]
+// sets the states and lists the candidates, then runs round 0 over them and
+// later rounds over the list the round before left, separated by a grid
+// barrier, until a round leaves no entity undecided or 100 rounds have run.
+// Control words (zero on entry but [1]: see the prologue): [0] barrier
+// arrivals, [1] barrier generation (only its changes count), [2..4]
 // length of the list round r builds for round r + 1, r + 1 = 0, 1, 2 mod 3
 // (round r zeroes the counter of round r + 2, last read after the barrier
 // of round r - 2 that every block has passed), [5] rounds run, [6] a barrier
-// wait gave up. States are read past L1 (L1 may keep a line another block
-// has since rewritten; a stale undecided state would only delay the
-// decision, but a line kept stale for good would never let it end). The
+// wait gave up. States and list entries are read past L1 (L1 may keep a
+// line another block has since rewritten; a stale undecided state would
+// only delay the decision, but a line kept stale for good would never let
+// it end, and a stale list entry would name the wrong entity). The
 // barrier's wait is bounded: after COOP_SPIN_LIMIT polls it sets [6] and
 // every block leaves.
 constexpr u32 COOP_SPIN_LIMIT = 1u << 24;
@@ -125,24 +104,48 @@ __device__ inline bool coop_barrier(u32* ctl)
 // (at least 4 blocks per SM: without a minimum the compiler held the
 // kernel to 32 registers and spilled)
 template <int G>
-__global__ void __launch_bounds__(BLOCK, 4) k_indset_coop(u32 n, Nbrs g, u32* st, u32* wl0,
-    u32* wl1, double const* __restrict__ good, u64 const* __restrict__ glob, u32* ctl)
+__global__ void __launch_bounds__(BLOCK, 4) k_indset_coop(u32 n, Nbrs g,
+    u32 const* __restrict__ filter, u32* st, u32* wl0, u32* wl1,
+    double const* __restrict__ good, u64 const* __restrict__ glob, u32* ctl)
 {
+  pdl_wait();
   u32 const lg = threadIdx.x % G;
   u32 const gbase = (threadIdx.x & 31) & ~(u32)(G - 1);
   u32 const gmask = (G == 32 ? 0xffffffffu : ((1u << G) - 1u)) << gbase;
   u32 const lane = threadIdx.x & 31;
   u32 const stride = gridDim.x * blockDim.x;
+  // The states (the filter's candidates undecided, the rest out of the set)
+  // and round 0's list, the candidates, appended a warp at a time to the
+  // list whose length is control word 2 (zero on entry: this kernel zeroes
+  // the list lengths when it settles, the host when a set fails); then the
+  // grid barrier, so round 0 sees every state and the whole list
+  for (u64 b = (u64)blockIdx.x * blockDim.x; b < n; b += stride) {
+    u32 const i = (u32)b + threadIdx.x;
+    bool const c = i < n && (!filter || filter[i]);
+    if (i < n) __stcg(&st[i], c ? (u32)UNKNOWN : (u32)NOT_IN_SET);
+    unsigned const want = __ballot_sync(0xffffffffu, c);
+    if (want) {
+      u32 const leader = __ffs(want) - 1;
+      u32 base = 0;
+      if (lane == leader) base = atomicAdd(&ctl[2], (u32)__popc(want));
+      base = __shfl_sync(0xffffffffu, base, leader);
+      if (c) wl1[base + __popc(want & ((1u << lane) - 1u))] = i;
+    }
+  }
+  __threadfence();
+  if (!coop_barrier(ctl)) return;
   for (u32 r = 0; r < MAX_INDSET_ROUNDS; ++r) {
-    // round 0 walks the candidates (listed by k_indset_init), round r > 0
-    // the list round r - 1 left
+    // round 0 walks the candidates, round r > 0 the list round r - 1 left
     u32 const len = *(volatile u32*)&ctl[2 + r % 3];
     u32 const* list = (r % 2 == 1) ? wl0 : wl1;
     u32* next = (r % 2 == 0) ? wl0 : wl1;
     u32* next_len = &ctl[2 + (r + 1) % 3];
     if (blockIdx.x == 0 && threadIdx.x == 0) ctl[2 + (r + 2) % 3] = 0;
     for (u64 t = (u64)blockIdx.x * blockDim.x + threadIdx.x; t < (u64)len * G; t += stride) {
-      u32 const i = list[t / G];
+      // past L1, like the states: the lists alternate between two
+      // buffers, so this block may hold lines of this one from two rounds
+      // ago that other blocks have since rewritten
+      u32 const i = __ldcg(&list[t / G]);
       u32 const s0 = __ldcg(&st[i]);
       bool undecided = false;
       if (s0 == UNKNOWN) {
@@ -195,7 +198,7 @@ __global__ void __launch_bounds__(BLOCK, 4) k_indset_coop(u32 n, Nbrs g, u32* st
     if (*(volatile u32*)next_len == 0) {
       // settled: every block has passed the last barrier and reads only
       // next_len (zero) from here, so the list lengths go back to zero for
-      // the next set's k_indset_init
+      // the next set's prologue
       if (blockIdx.x == 0 && threadIdx.x == 0) {
         ctl[5] = r + 1;
         ctl[2] = ctl[3] = ctl[4] = 0;
@@ -230,8 +233,8 @@ u32 coop_blocks()
 }
 
 template <int G>
-void launch_coop(u32 n, Nbrs const& g, u32* st, u32* wl, double const* good, u64 const* glob,
-    u32* ctl, cudaStream_t s)
+void launch_coop(u32 n, Nbrs const& g, u32 const* filter, u32* st, u32* wl,
+    double const* good, u64 const* glob, u32* ctl, cudaStream_t s)
 {
   u32 blocks = std::min<u32>(grid_for((u64)n * G), coop_blocks<G>());
   if (!blocks) throw Failure(E_CUDA, "independent set: no resident blocks");
@@ -244,7 +247,8 @@ void launch_coop(u32 n, Nbrs const& g, u32* st, u32* wl, double const* good, u64
   attr[0].val.cooperative = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  CK(cudaLaunchKernelEx(&cfg, k_indset_coop<G>, n, g, st, wl, wl + n, good, glob, ctl));
+  CK(cudaLaunchKernelEx(&cfg, k_indset_coop<G>, n, g, filter, st, wl, wl + n, good, glob,
+      ctl));
   CK_LAUNCH();
 }
 }  // namespace
@@ -282,26 +286,24 @@ u32* find_indset(Mesh& m, u32 ent_dim, u32 const* filter, double const* good, bo
   u64 const* glob = (m.parallel && m.globals[ent_dim]) ? m.globals[ent_dim] : nullptr;
   u32* a = dalloc<u32>(n, m.s);
   u32* b = dalloc<u32>(2 * (size_t)n, m.s);  // the two lists of undecided entities
-  // zeroes the control words even with no entity (rounds run = 0 then);
-  // round 0's list is b's second half
-  CK(launch_kernel(k_indset_init, dim3(grid_for(std::max<u32>(n, COOP_CTL_WORDS))),
-      dim3(BLOCK), 0, m.s, n, filter, a, b + n, m.mb->dev + COOP_CTL_SLOT));
-  CK_LAUNCH();
-  // All rounds run in one cooperative launch that updates a in place; its
-  // control words (mailbox slots COOP_CTL_SLOT..) come back with slots 1-3,
-  // which a caller that left flags there reads after this call without a
-  // read-back of its own
+  // One cooperative launch sets the states, lists the candidates and runs
+  // every round, updating a in place; its control words (mailbox slots
+  // COOP_CTL_SLOT..) come back with slots 1-3, which a caller that left
+  // flags there reads after this call without a read-back of its own. With
+  // no entity, only the rounds count is zeroed.
+  u32* ctl = m.mb->dev + COOP_CTL_SLOT;
   if (n) {
-    u32* ctl = m.mb->dev + COOP_CTL_SLOT;
     double nuse = (double)read_cached_uses(m, ent_dim);
     double avg_row = nuse / n;
     u32 lanes = avg_row >= 8.0 ? tuned(TK_INDSET_VERT_GROUP)
               : avg_row >= 3.0 ? tuned(TK_INDSET_EDGE_GROUP) : 1u;
-    if (lanes == 16) launch_coop<16>(n, g, a, b, good, glob, ctl, m.s);
-    else if (lanes == 8) launch_coop<8>(n, g, a, b, good, glob, ctl, m.s);
-    else if (lanes == 4) launch_coop<4>(n, g, a, b, good, glob, ctl, m.s);
-    else if (lanes == 2) launch_coop<2>(n, g, a, b, good, glob, ctl, m.s);
-    else launch_coop<1>(n, g, a, b, good, glob, ctl, m.s);
+    if (lanes == 16) launch_coop<16>(n, g, filter, a, b, good, glob, ctl, m.s);
+    else if (lanes == 8) launch_coop<8>(n, g, filter, a, b, good, glob, ctl, m.s);
+    else if (lanes == 4) launch_coop<4>(n, g, filter, a, b, good, glob, ctl, m.s);
+    else if (lanes == 2) launch_coop<2>(n, g, filter, a, b, good, glob, ctl, m.s);
+    else launch_coop<1>(n, g, filter, a, b, good, glob, ctl, m.s);
+  } else {
+    CK(cudaMemsetAsync(ctl + 5, 0, sizeof(u32), m.s));
   }
   dev_free(b, m.s);
   if (check) {
@@ -319,8 +321,8 @@ u32* find_indset(Mesh& m, u32 ent_dim, u32 const* filter, double const* good, bo
 void indset_check(Mesh& m)
 {
   u32 const* hc = m.mb->host + COOP_CTL_SLOT;
-  // a set that failed leaves its list lengths standing: zeroed here for the
-  // next set's k_indset_init, which appends to list length 0
+  // a set that failed leaves its control words standing: zeroed here for
+  // the next set's prologue, which appends to list length 0
   auto reset = [&] {
     CK(cudaMemsetAsync(m.mb->dev + COOP_CTL_SLOT, 0, COOP_CTL_WORDS * sizeof(u32), m.s));
   };
@@ -451,7 +453,7 @@ __device__ inline void expand_same_rows(ExpandJob const& jb, u32 warp, u32 nwarp
 // Other jobs (a list of rows, k > 1, wider rows, 1-byte elements): a
 // thread per row. (At least three blocks of 512 per SM: at 56 registers
 // only four blocks of 256 fit, too few warps to keep the loads in flight.)
-__global__ void __launch_bounds__(512, 3) k_expand_many(ExpandJobs jobs)
+__global__ void __launch_bounds__(512, 3) k_expand_many(const __grid_constant__ ExpandJobs jobs)
 {
   pdl_wait();
   ExpandJob const jb = jobs.j[blockIdx.y];

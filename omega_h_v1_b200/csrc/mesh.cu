@@ -644,7 +644,7 @@ struct KeyJobs {
 };
 
 template <u32 VPL>
-__device__ inline void count_key_row(KeyJob const& jb, u32 i, u32 const* __restrict__ marks)
+__device__ inline void count_key_row(KeyJob const jb, u32 i, u32 const* __restrict__ marks)
 {
   u32 w[VPL];
   low_key<VPL>(jb.vol, i, w);
@@ -652,10 +652,11 @@ __device__ inline void count_key_row(KeyJob const& jb, u32 i, u32 const* __restr
   atomicAdd(&jb.cnt[key_row<VPL>(w)], 1u);
 }
 
-__global__ void k_count_key_rows(KeyJobs jobs, u32 const* __restrict__ marks)
+__global__ void k_count_key_rows(const __grid_constant__ KeyJobs jobs,
+    u32 const* __restrict__ marks)
 {
   pdl_wait();
-  KeyJob const& jb = jobs.j[blockIdx.y];
+  KeyJob const jb = jobs.j[blockIdx.y];
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= jb.nl) return;
   if (jb.low == 1)
@@ -667,7 +668,7 @@ __global__ void k_count_key_rows(KeyJobs jobs, u32 const* __restrict__ marks)
 // cnt holds each sub-row's count; a row's records take its slots from the
 // end down: uint2 {v1, id} for edges, uint4 {v1, v2, id, 0} for triangles
 template <u32 VPL>
-__device__ inline void fill_key_row(KeyJob const& jb, u32 i, u32 const* __restrict__ marks)
+__device__ inline void fill_key_row(KeyJob const jb, u32 i, u32 const* __restrict__ marks)
 {
   u32 w[VPL];
   low_key<VPL>(jb.vol, i, w);
@@ -680,10 +681,11 @@ __device__ inline void fill_key_row(KeyJob const& jb, u32 i, u32 const* __restri
     reinterpret_cast<uint4*>(jb.rows)[slot] = make_uint4(w[1], w[VPL - 1], i, 0u);
 }
 
-__global__ void k_fill_key_rows(KeyJobs jobs, u32 const* __restrict__ marks)
+__global__ void k_fill_key_rows(const __grid_constant__ KeyJobs jobs,
+    u32 const* __restrict__ marks)
 {
   pdl_wait();
-  KeyJob const& jb = jobs.j[blockIdx.y];
+  KeyJob const jb = jobs.j[blockIdx.y];
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= jb.nl) return;
   if (jb.low == 1)
@@ -707,7 +709,7 @@ struct ReflectJobs {
 };
 
 template <u32 HIGH, u32 LOW>
-__device__ inline void reflect_keyed(ReflectJob const& jb, u32 i)
+__device__ inline void reflect_keyed(ReflectJob const jb, u32 i)
 {
   constexpr u32 LPH = HIGH == 3 ? (LOW == 1 ? 6 : 4) : 3;
   constexpr u32 VPH = HIGH + 1, VPL = LOW + 1;
@@ -757,10 +759,10 @@ __device__ inline void reflect_keyed(ReflectJob const& jb, u32 i)
   }
 }
 
-__global__ void k_reflect_keyed(ReflectJobs jobs)
+__global__ void k_reflect_keyed(const __grid_constant__ ReflectJobs jobs)
 {
   pdl_wait();
-  ReflectJob const& jb = jobs.j[blockIdx.y];
+  ReflectJob const jb = jobs.j[blockIdx.y];
   u32 i = jb.first + blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= jb.nh) return;
   if (jb.high == 2)
@@ -981,7 +983,7 @@ struct MarkRanges {
   MarkRange r[2];
 };
 
-__global__ void k_mark_verts(MarkRanges rs, u32* __restrict__ marks)
+__global__ void k_mark_verts(const __grid_constant__ MarkRanges rs, u32* __restrict__ marks)
 {
   pdl_wait();
   MarkRange const r = rs.r[blockIdx.y];
@@ -1128,7 +1130,7 @@ struct DownJobs {
 };
 
 template <u32 LPH>
-__device__ inline void carry_down_rows(DownJob const& jb)
+__device__ inline void carry_down_rows(DownJob const jb)
 {
   u32 const* __restrict__ same_h = jb.same_h;
   u32 const* __restrict__ same_l = jb.same_l;
@@ -1156,10 +1158,12 @@ __device__ inline void carry_down_rows(DownJob const& jb)
   }
 }
 
-__global__ void __launch_bounds__(512) k_carry_down(DownJobs jobs)
+__global__ void __launch_bounds__(512) k_carry_down(const __grid_constant__ DownJobs jobs)
 {
   pdl_wait();
-  DownJob const& jb = jobs.j[blockIdx.y];
+  // (the job by value: a reference into the parameters would put the whole
+  // job array in local memory)
+  DownJob const jb = jobs.j[blockIdx.y];
   if (jb.lph == 3)
     carry_down_rows<3>(jb);
   else if (jb.lph == 4)
@@ -1336,7 +1340,7 @@ struct UpFillJobs {
 };
 
 template <u32 CG>
-__global__ void k_up_surv_fill_grouped(UpFillJobs jobs)
+__global__ void k_up_surv_fill_grouped(const __grid_constant__ UpFillJobs jobs)
 {
   pdl_wait();
   UpFillJob const& jb = jobs.j[blockIdx.y];
@@ -1405,7 +1409,7 @@ struct UpCountJobs {
   UpCountJob j[6];
 };
 
-__global__ void k_up_row_lens(UpCountJobs jobs)
+__global__ void k_up_row_lens(const __grid_constant__ UpCountJobs jobs)
 {
   pdl_wait();
   UpCountJob const& jb = jobs.j[blockIdx.y];
@@ -1427,7 +1431,7 @@ __global__ void k_up_row_lens(UpCountJobs jobs)
   if (surv) surv[nj] = len;
 }
 
-__global__ void k_up_adjust(UpCountJobs jobs)
+__global__ void k_up_adjust(const __grid_constant__ UpCountJobs jobs)
 {
   pdl_wait();
   UpCountJob const& jb = jobs.j[blockIdx.y];

@@ -191,7 +191,7 @@ struct NodalFields {
 };
 
 __global__ void k_refine_nodal(u32 ne, u32 nv, u32 const* __restrict__ voe,
-    u32 const* __restrict__ gen_offs, NodalFields fields)
+    u32 const* __restrict__ gen_offs, const __grid_constant__ NodalFields fields)
 {
   pdl_wait();
   u32 const nc = fields.nc[blockIdx.y];
@@ -255,40 +255,59 @@ __device__ inline bool first_split_edge(u32 const* __restrict__ sod,
   return w;
 }
 
+// (optional) the vertices' maps on the threads past the domains: their
+// domain offsets (no vertex splits: zeros) and their identity survivor maps
+struct VertexMaps {
+  u32 nv;
+  u32* zero;
+  u32* same;
+  u32* newid;
+};
+
+__device__ inline void vertex_maps(VertexMaps const& vm, u32 i)
+{
+  if (i > vm.nv) return;
+  vm.zero[i] = 0;
+  vm.same[i] = i;
+  if (vm.newid && i < vm.nv) vm.newid[i] = i;
+}
+
 template <u32 SPD>
 __global__ void k_split_to_domain(u32 nd, u32 const* __restrict__ sod,
-    u32 const* __restrict__ gen_offs, u32* __restrict__ will)
+    u32 const* __restrict__ gen_offs, u32* __restrict__ will, VertexMaps vm)
 {
   pdl_wait();
   u32 i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= nd) return;
+  if (i >= nd) {
+    if (vm.zero) vertex_maps(vm, i - nd);
+    return;
+  }
   u32 d, v;
   will[i] = first_split_edge<SPD>(sod, gen_offs, i, d, v) ? 1u : 0u;
 }
 
-// refine_domain_entity (refine_topology.cpp:26-64), for every domain
-// dimension of one product dimension in one launch (blockIdx.y: the domain
-// dimension's job), a thread per split domain entity from the list of them
-// in order. The domain's split edge and the new vertex on it: the edge
+// refine_domain_entity (refine_topology.cpp:26-64), for every product and
+// domain dimension of a pass in one launch (blockIdx.y: the pair's job), a
+// thread per split domain entity from the list of them in order. The domain's split edge and the new vertex on it: the edge
 // itself for edge domains, else its first split edge (sod: the domain's
 // edges).
 struct TopoJob {
-  u32 dd, nsplit;
+  u32 prod, dd, nsplit;
   u32 const* list;
   u32 const* vod;
   u32 const* sod;
   u32* out;
 };
 struct TopoJobs {
-  TopoJob j[3];
+  TopoJob j[6];  // every (product, domain) dimension pair of a 3D pass
 };
 
-__global__ void k_refine_topology(TopoJobs jobs, u32 prod, u32 const* __restrict__ gen_offs,
-    u32 nv)
+__global__ void k_refine_topology(const __grid_constant__ TopoJobs jobs,
+    u32 const* __restrict__ gen_offs, u32 nv)
 {
   pdl_wait();
   TopoJob const jb = jobs.j[blockIdx.y];
-  u32 const dd = jb.dd;
+  u32 const dd = jb.dd, prod = jb.prod;
   u32 t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= jb.nsplit) return;
   u32 const i = jb.list[t];
@@ -354,17 +373,11 @@ struct EdgeSplits {
   u32* newid = nullptr;
 };
 
-// the vertices' domain offsets (no vertex splits: zeros) and their identity
-// survivor maps
-__global__ void k_vertex_maps(u32 nv, u32* __restrict__ zero, u32* __restrict__ same,
-    u32* __restrict__ newid)
+// the vertices' maps alone (a pass without triangle or tet domains)
+__global__ void k_vertex_maps(VertexMaps vm)
 {
   pdl_wait();
-  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i > nv) return;
-  zero[i] = 0;
-  same[i] = i;
-  if (newid && i < nv) newid[i] = i;
+  vertex_maps(vm, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 // returns the number of split edges (read back with the domain counts).
@@ -392,9 +405,8 @@ static u32 refine_build(Mesh& m, EdgeSplits const& es, bool deferred, bool unifo
   u32* zero_v = dalloc<u32>((size_t)nv + 1, s);
   same_of[0] = dalloc<u32>((size_t)nv + 1, s);
   if (carried_high(m, 0)) newid_of[0] = dalloc<u32>(nv ? nv : 1, s);
-  CK(launch_kernel(k_vertex_maps, dim3(grid_for((u64)nv + 1)), dim3(BLOCK), 0, s, nv, zero_v,
-      same_of[0], newid_of[0]));
-  CK_LAUNCH();
+  // written by the first split-mark launch below (or on their own)
+  VertexMaps vm{nv, zero_v, same_of[0], newid_of[0]};
   sp[0].offs = zero_v;
   // the edges as domains: the split edges' scan (the caller owns gen_offs)
   sp[1].offs = es.gen_offs;
@@ -409,10 +421,13 @@ static u32 refine_build(Mesh& m, EdgeSplits const& es, bool deferred, bool unifo
     u32 nd = m.count(dd);
     u32 const* sod = m.ask_down(dd, 1);
     will[dd] = dalloc<u32>(nd, s);
-    if (nd) {
+    if (nd || vm.zero) {
+      u64 const nthreads = (u64)nd + (vm.zero ? (u64)nv + 1 : 0);
       auto k = dd == 2 ? k_split_to_domain<3> : k_split_to_domain<6>;
-      CK(launch_kernel(k, dim3(grid_for(nd)), dim3(BLOCK), 0, s, nd, sod, gen_offs, will[dd]));
+      CK(launch_kernel(k, dim3(grid_for(nthreads)), dim3(BLOCK), 0, s, nd, sod, gen_offs,
+          will[dd], vm));
       CK_LAUNCH();
+      vm.zero = nullptr;  // done
     }
     sp[dd].offs = dalloc<u32>((size_t)nd + 1, s);
     sp[dd].list = dalloc<u32>(nd ? nd : 1, s);
@@ -422,6 +437,10 @@ static u32 refine_build(Mesh& m, EdgeSplits const& es, bool deferred, bool unifo
       if (carried_high(m, dd)) newid_of[dd] = j.comp_newid = dalloc<u32>(nd ? nd : 1, s);
     }
     jobs[njobs++] = j;
+  }
+  if (vm.zero) {
+    CK(launch_kernel(k_vertex_maps, dim3(grid_for((u64)nv + 1)), dim3(BLOCK), 0, s, vm));
+    CK_LAUNCH();
   }
   // the other domains' scans in one launch
   exscan_jobs(jobs, njobs, s);
@@ -494,6 +513,9 @@ static u32 refine_build(Mesh& m, EdgeSplits const& es, bool deferred, bool unifo
       CK_LAUNCH();
     }
   }
+  TopoJobs tj;
+  u32 ntj = 0, tmost = 0;
+  double tbytes = 0;
   for (u32 prod = 0; prod <= dim; ++prod) {
     if (!m.full && 0 < prod && prod < dim) continue;
     u32 np = m.count(prod);
@@ -533,23 +555,16 @@ static u32 refine_build(Mesh& m, EdgeSplits const& es, bool deferred, bool unifo
       cj.width = vpp;
       cj.esz = 4;
       conn_job.push_back(cj);
-      TopoJobs tj;
-      u32 ntj = 0, ndmax = 0;
-      double bytes = 0;
+      // the products' vertices: one launch for every dimension, after
+      // this loop (they write past the survivors' rows of each array)
       for (u32 dd = first; dd <= last; ++dd) {
         if (!d.ndoms[dd] || !d.scale[dd] || !sp[dd].nsplit) continue;
         u32 nd = sp[dd].nsplit;
-        tj.j[ntj++] = TopoJob{dd, nd, sp[dd].list, m.ask_down(dd, 0),
+        tj.j[ntj++] = TopoJob{prod, dd, nd, sp[dd].list, m.ask_down(dd, 0),
             dd == 1 ? nullptr : m.ask_down(dd, 1), conn + (size_t)d.ngo[dd] * vpp};
-        ndmax = std::max(ndmax, nd);
-        bytes += 4.0 * nd + 4.0 * deg(dd, 0) * nd + 12.0 * deg(dd, 1) * nd +
+        tmost = std::max(tmost, nd);
+        tbytes += 4.0 * nd + 4.0 * deg(dd, 0) * nd + 12.0 * deg(dd, 1) * nd +
             4.0 * vpp * (double)d.ngen[dd];
-      }
-      if (ntj) {
-        PROBE(P_REFINE_TOPOLOGY, s, bytes);
-        CK(launch_kernel(k_refine_topology, dim3(grid_for(ndmax), ntj), dim3(BLOCK), 0, s, tj,
-            prod, gen_offs, nv));
-        CK_LAUNCH();
       }
       out->set_ents(prod, nout, conn);
       if (m.parallel) inherit_globals(*out, prod, nout);
@@ -575,6 +590,12 @@ static u32 refine_build(Mesh& m, EdgeSplits const& es, bool deferred, bool unifo
     }
     same_of[prod] = same;
     nsame_of[prod] = np - sp[prod].nsplit;
+  }
+  if (ntj) {
+    PROBE(P_REFINE_TOPOLOGY, s, tbytes);
+    CK(launch_kernel(k_refine_topology, dim3(grid_for(tmost), ntj), dim3(BLOCK), 0, s, tj,
+        gen_offs, nv));
+    CK_LAUNCH();
   }
   // downward adjacency of the survivors carries over; the products are searched
   carry_down_all(m, *out, same_of, nsame_of);
