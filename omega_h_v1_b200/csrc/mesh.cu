@@ -652,17 +652,18 @@ __device__ inline void count_key_row(KeyJob const jb, u32 i, u32 const* __restri
   atomicAdd(&jb.cnt[key_row<VPL>(w)], 1u);
 }
 
+// (grid-stride: with marks most threads read a vertex tuple and leave)
 __global__ void k_count_key_rows(const __grid_constant__ KeyJobs jobs,
     u32 const* __restrict__ marks)
 {
   pdl_wait();
   KeyJob const jb = jobs.j[blockIdx.y];
-  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= jb.nl) return;
-  if (jb.low == 1)
-    count_key_row<2>(jb, i, marks);
-  else
-    count_key_row<3>(jb, i, marks);
+  for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < jb.nl; i += gridDim.x * blockDim.x) {
+    if (jb.low == 1)
+      count_key_row<2>(jb, i, marks);
+    else
+      count_key_row<3>(jb, i, marks);
+  }
 }
 
 // cnt holds each sub-row's count; a row's records take its slots from the
@@ -686,12 +687,12 @@ __global__ void k_fill_key_rows(const __grid_constant__ KeyJobs jobs,
 {
   pdl_wait();
   KeyJob const jb = jobs.j[blockIdx.y];
-  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= jb.nl) return;
-  if (jb.low == 1)
-    fill_key_row<2>(jb, i, marks);
-  else
-    fill_key_row<3>(jb, i, marks);
+  for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < jb.nl; i += gridDim.x * blockDim.x) {
+    if (jb.low == 1)
+      fill_key_row<2>(jb, i, marks);
+    else
+      fill_key_row<3>(jb, i, marks);
+  }
 }
 
 // One thread per high entity: every wanted low's sub-row bounds are loaded
@@ -1057,13 +1058,15 @@ void Mesh::build_low_rows(u32 const* lows, u32 nlows)
   }
   if (!nj) return;
   if (most) {
-    CK(launch_kernel(k_count_key_rows, dim3(grid_for(most), nj), dim3(BLOCK), 0, s, jobs,
+    CK(launch_kernel(k_count_key_rows, dim3(std::min<u32>(grid_for(most), 148u * 8u), nj),
+        dim3(BLOCK), 0, s, jobs,
         search_marks));
     CK_LAUNCH();
   }
   exscan_jobs(sj, nj, s);
   if (most) {
-    CK(launch_kernel(k_fill_key_rows, dim3(grid_for(most), nj), dim3(BLOCK), 0, s, jobs,
+    CK(launch_kernel(k_fill_key_rows, dim3(std::min<u32>(grid_for(most), 148u * 8u), nj),
+        dim3(BLOCK), 0, s, jobs,
         search_marks));
     CK_LAUNCH();
   }
@@ -1409,46 +1412,51 @@ struct UpCountJobs {
   UpCountJob j[6];
 };
 
+// (grid-stride over a grid of a few blocks per SM: most threads do one or
+// two loads, and a block per 256 of them spent the launch scheduling blocks)
 __global__ void k_up_row_lens(const __grid_constant__ UpCountJobs jobs)
 {
   pdl_wait();
   UpCountJob const& jb = jobs.j[blockIdx.y];
-  u32 j = blockIdx.x * blockDim.x + threadIdx.x;
   u32* __restrict__ cnt = jb.cnt;
   u32* __restrict__ surv = jb.surv;
-  if (j >= jb.nl_old) {
-    if (j - jb.nl_old < jb.ntail) {
+  u32 const end = jb.nl_old + jb.ntail;
+  for (u32 j = blockIdx.x * blockDim.x + threadIdx.x; j < end; j += gridDim.x * blockDim.x) {
+    if (j >= jb.nl_old) {
       u32 r = jb.nsame_l + (j - jb.nl_old);
       cnt[r] = 0;
       if (surv) surv[r] = 0;
+      continue;
     }
-    return;
+    u32 nj = jb.same_l[j];
+    if (jb.same_l[j + 1] == nj) continue;
+    u32 len = jb.offs_old[j + 1] - jb.offs_old[j];
+    cnt[nj] = len;
+    if (surv) surv[nj] = len;
   }
-  u32 nj = jb.same_l[j];
-  if (jb.same_l[j + 1] == nj) return;
-  u32 len = jb.offs_old[j + 1] - jb.offs_old[j];
-  cnt[nj] = len;
-  if (surv) surv[nj] = len;
 }
 
 __global__ void k_up_adjust(const __grid_constant__ UpCountJobs jobs)
 {
   pdl_wait();
   UpCountJob const& jb = jobs.j[blockIdx.y];
-  u32 t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t < jb.nh_old) {
-    if (jb.newid_h[t] != INV) return;
-    for (u32 k = 0; k < jb.lph; ++k) {
-      u32 l = jb.old_loh[(size_t)t * jb.lph + k];
-      u32 nl = jb.same_l[l];
-      if (jb.same_l[l + 1] == nl) continue;
-      atomicSub(&jb.cnt[nl], 1u);
-      if (jb.surv) atomicSub(&jb.surv[nl], 1u);
+  u64 const end = (u64)jb.nh_old + (jb.nuses > jb.first ? jb.nuses - jb.first : 0u);
+  for (u64 t = (u64)blockIdx.x * blockDim.x + threadIdx.x; t < end;
+       t += (u64)gridDim.x * blockDim.x) {
+    if (t < jb.nh_old) {
+      if (jb.newid_h[t] != INV) continue;
+      for (u32 k = 0; k < jb.lph; ++k) {
+        u32 l = jb.old_loh[(size_t)t * jb.lph + k];
+        u32 nl = jb.same_l[l];
+        if (jb.same_l[l + 1] == nl) continue;
+        atomicSub(&jb.cnt[nl], 1u);
+        if (jb.surv) atomicSub(&jb.surv[nl], 1u);
+      }
+      continue;
     }
-    return;
+    u32 u = jb.first + (u32)(t - jb.nh_old);
+    atomicAdd(&jb.cnt[jb.loh[u]], 1u);
   }
-  u32 u = jb.first + (t - jb.nh_old);
-  if (u < jb.nuses) atomicAdd(&jb.cnt[jb.loh[u]], 1u);
 }
 
 u32* carry_new_ids(u32 const* same, u32 n, cudaStream_t s)
@@ -1623,12 +1631,14 @@ void carry_up_all(Mesh& m, Mesh& out, u32* const* same_of, u32 const* nsame_of,
     u32 const gb = tuned(TK_GATHER_BLOCK);
     {
       PROBE(P_CARRY_UP, s, bytes_rows);
-      CK(launch_kernel(k_up_row_lens, dim3(grid_for(most_rows, gb), nc), dim3(gb), 0, s, cj));
+      CK(launch_kernel(k_up_row_lens, dim3(std::min<u32>(grid_for(most_rows, gb),
+          148u * 8u * 256u / gb), nc), dim3(gb), 0, s, cj));
       CK_LAUNCH();
     }
     {
       PROBE(P_UP_COUNT, s, bytes_adj);
-      CK(launch_kernel(k_up_adjust, dim3(grid_for(most_adj, gb), nc), dim3(gb), 0, s, cj));
+      CK(launch_kernel(k_up_adjust, dim3(std::min<u32>(grid_for(most_adj, gb),
+          148u * 8u * 256u / gb), nc), dim3(gb), 0, s, cj));
       CK_LAUNCH();
     }
   }
