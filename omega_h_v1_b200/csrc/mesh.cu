@@ -163,8 +163,7 @@ void Mesh::clear_contents()
     low_row_offs[d] = nullptr;
     low_rows[d] = nullptr;
   }
-  dev_free(search_marks, s);
-  search_marks = nullptr;
+  search_marks = nullptr;  // the stream's, not the mesh's
   for (u32 d = 0; d < 4; ++d) {
     for (auto& t : tags[d]) dev_free(t.data, s);
     tags[d].clear();
@@ -209,6 +208,7 @@ void Mesh::overwrite(Mesh* with)
     with->low_rows[d] = nullptr;
   }
   search_marks = with->search_marks;
+  search_gen = with->search_gen;
   with->search_marks = nullptr;
   for (u32 d = 0; d < 4; ++d) {
     counts[d] = with->counts[d];
@@ -526,6 +526,18 @@ void up_from_down_unsorted(u32 high, u32 low, u32 nhighs, u32 nlows, u32 const* 
   dev_free(cnt, s);
 }
 
+// the packed uses of each row's part after its first pre[l] (the part the
+// sort reorders), a thread per row: a carried row's tail holds only the
+// uses of the entities the pass made, so most rows have none
+__global__ void k_join_tails(u32 nlows, u32 lph, u32 const* __restrict__ offs,
+    u32 const* __restrict__ pre, u32 const* __restrict__ adj, u32 const* __restrict__ dirs,
+    u32* __restrict__ uses)
+{
+  pdl_wait();
+  for (u32 l = blockIdx.x * blockDim.x + threadIdx.x; l < nlows; l += gridDim.x * blockDim.x)
+    for (u32 p = offs[l] + pre[l], e = offs[l + 1]; p < e; ++p) uses[p] = adj[p] * lph + dirs[p];
+}
+
 void sort_up_rows(u32 high, u32 low, u32 nhighs, u32 nlows, UpAdj const& u,
     cudaStream_t s)
 {
@@ -533,7 +545,13 @@ void sort_up_rows(u32 high, u32 low, u32 nhighs, u32 nlows, UpAdj const& u,
   u32 nuses = nhighs * lph;
   if (!nuses || !nlows) return;
   u32* uses = dalloc<u32>(nuses, s);
-  CK(launch_kernel(k_join_uses, dim3(grid_for(nuses)), dim3(BLOCK), 0, s, nuses, lph, u.adj, u.dirs, uses));
+  if (u.pre) {
+    CK(launch_kernel(k_join_tails, dim3(std::min<u32>(grid_for(nlows), 148u * 8u)),
+        dim3(BLOCK), 0, s, nlows, lph, u.offs, u.pre, u.adj, u.dirs, uses));
+  } else {
+    CK(launch_kernel(k_join_uses, dim3(grid_for(nuses)), dim3(BLOCK), 0, s, nuses, lph, u.adj,
+        u.dirs, uses));
+  }
   CK_LAUNCH();
   {
     u32 nsort = u.pre ? nuses - u.npre : nuses;
@@ -644,36 +662,38 @@ struct KeyJobs {
 };
 
 template <u32 VPL>
-__device__ inline void count_key_row(KeyJob const jb, u32 i, u32 const* __restrict__ marks)
+__device__ inline void count_key_row(KeyJob const jb, u32 i, u32 const* __restrict__ marks,
+    u32 gen)
 {
   u32 w[VPL];
   low_key<VPL>(jb.vol, i, w);
-  if (marks && !marks[w[0]]) return;
+  if (marks && marks[w[0]] != gen) return;
   atomicAdd(&jb.cnt[key_row<VPL>(w)], 1u);
 }
 
 // (grid-stride: with marks most threads read a vertex tuple and leave)
 __global__ void k_count_key_rows(const __grid_constant__ KeyJobs jobs,
-    u32 const* __restrict__ marks)
+    u32 const* __restrict__ marks, u32 gen)
 {
   pdl_wait();
   KeyJob const jb = jobs.j[blockIdx.y];
   for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < jb.nl; i += gridDim.x * blockDim.x) {
     if (jb.low == 1)
-      count_key_row<2>(jb, i, marks);
+      count_key_row<2>(jb, i, marks, gen);
     else
-      count_key_row<3>(jb, i, marks);
+      count_key_row<3>(jb, i, marks, gen);
   }
 }
 
 // cnt holds each sub-row's count; a row's records take its slots from the
 // end down: uint2 {v1, id} for edges, uint4 {v1, v2, id, 0} for triangles
 template <u32 VPL>
-__device__ inline void fill_key_row(KeyJob const jb, u32 i, u32 const* __restrict__ marks)
+__device__ inline void fill_key_row(KeyJob const jb, u32 i, u32 const* __restrict__ marks,
+    u32 gen)
 {
   u32 w[VPL];
   low_key<VPL>(jb.vol, i, w);
-  if (marks && !marks[w[0]]) return;
+  if (marks && marks[w[0]] != gen) return;
   u32 b = key_row<VPL>(w);
   u32 slot = jb.offs[b] + atomicSub(&jb.cnt[b], 1u) - 1u;
   if (VPL == 2)
@@ -683,15 +703,15 @@ __device__ inline void fill_key_row(KeyJob const jb, u32 i, u32 const* __restric
 }
 
 __global__ void k_fill_key_rows(const __grid_constant__ KeyJobs jobs,
-    u32 const* __restrict__ marks)
+    u32 const* __restrict__ marks, u32 gen)
 {
   pdl_wait();
   KeyJob const jb = jobs.j[blockIdx.y];
   for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < jb.nl; i += gridDim.x * blockDim.x) {
     if (jb.low == 1)
-      fill_key_row<2>(jb, i, marks);
+      fill_key_row<2>(jb, i, marks, gen);
     else
-      fill_key_row<3>(jb, i, marks);
+      fill_key_row<3>(jb, i, marks, gen);
   }
 }
 
@@ -984,13 +1004,14 @@ struct MarkRanges {
   MarkRange r[2];
 };
 
-__global__ void k_mark_verts(const __grid_constant__ MarkRanges rs, u32* __restrict__ marks)
+__global__ void k_mark_verts(const __grid_constant__ MarkRanges rs, u32* __restrict__ marks,
+    u32 gen)
 {
   pdl_wait();
   MarkRange const r = rs.r[blockIdx.y];
   u32 i = r.first + blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= r.nh) return;
-  for (u32 k = 0; k < r.vph; ++k) marks[r.voh[(size_t)i * r.vph + k]] = 1;
+  for (u32 k = 0; k < r.vph; ++k) marks[r.voh[(size_t)i * r.vph + k]] = gen;
 }
 
 // Search rows limited to what a pass's products need: the vertices of the
@@ -1000,9 +1021,10 @@ __global__ void k_mark_verts(const __grid_constant__ MarkRanges rs, u32* __restr
 // searches only, so drop_search_rows discards them afterwards.
 void Mesh::mark_search_verts(u32 const* first)
 {
+  // the stream's marks, stamped with a generation of their own (nothing to
+  // zero between uses)
   u32 nv = counts[0];
-  search_marks = dalloc<u32>(nv ? nv : 1, s);
-  CK(cudaMemsetAsync(search_marks, 0, sizeof(u32) * (nv ? nv : 1), s));
+  search_marks = stream_marks(nv ? nv : 1, s, &search_gen);
   MarkRanges rs;
   u32 nr = 0, most = 0;
   for (u32 h = 2; h <= dim; ++h) {
@@ -1013,7 +1035,7 @@ void Mesh::mark_search_verts(u32 const* first)
   }
   if (nr) {
     CK(launch_kernel(k_mark_verts, dim3(grid_for(most), nr), dim3(BLOCK), 0, s, rs,
-        search_marks));
+        search_marks, search_gen));
     CK_LAUNCH();
   }
 }
@@ -1027,8 +1049,7 @@ void Mesh::drop_search_rows()
     low_row_offs[d] = nullptr;
     low_rows[d] = nullptr;
   }
-  dev_free(search_marks, s);
-  search_marks = nullptr;
+  search_marks = nullptr;  // the stream's marks stay for its next use
 }
 
 // the search rows of the listed lows (1: edges, 2: triangles) that are
@@ -1037,7 +1058,6 @@ void Mesh::build_low_rows(u32 const* lows, u32 nlows)
 {
   KeyJobs jobs;
   u32 nj = 0, most = 0;
-  u32* cnts[2] = {nullptr, nullptr};
   ScanJob sj[2];
   for (u32 q = 0; q < nlows; ++q) {
     u32 low = lows[q];
@@ -1046,31 +1066,28 @@ void Mesh::build_low_rows(u32 const* lows, u32 nlows)
     u32 nl = counts[low];
     size_t nb = (size_t)counts[0] * (low == 1 ? KeyRows<2>::SUB : KeyRows<3>::SUB);
     if (nb >= 0xffffffffull) throw Failure(E_ARG, "reflect_down: too many vertices");
-    u32* cnt = dalloc<u32>(nb + 1, s);
-    CK(cudaMemsetAsync(cnt, 0, sizeof(u32) * (nb + 1), s));
+    // counts in the stream's kept scratch, zero on entry: the fill takes
+    // every count back down to zero
+    u32* cnt = stream_zero_scratch(nj == 0 ? KEPT_ROWS0 : KEPT_ROWS1, nb + 1, s);
     low_row_offs[low] = dalloc<u32>(nb + 1, s);
     low_rows[low] = dalloc<u32>((size_t)nl * (low == 1 ? 2 : 4), s);
     jobs.j[nj] = KeyJob{low, nl, vol, cnt, low_row_offs[low], low_rows[low]};
     sj[nj] = ScanJob{cnt, low_row_offs[low], nullptr, nullptr, (u32)nb, 0};
-    cnts[nj] = cnt;
     most = std::max(most, nl);
     ++nj;
   }
   if (!nj) return;
   if (most) {
     CK(launch_kernel(k_count_key_rows, dim3(std::min<u32>(grid_for(most), 148u * 8u), nj),
-        dim3(BLOCK), 0, s, jobs,
-        search_marks));
+        dim3(BLOCK), 0, s, jobs, search_marks, search_gen));
     CK_LAUNCH();
   }
   exscan_jobs(sj, nj, s);
   if (most) {
     CK(launch_kernel(k_fill_key_rows, dim3(std::min<u32>(grid_for(most), 148u * 8u), nj),
-        dim3(BLOCK), 0, s, jobs,
-        search_marks));
+        dim3(BLOCK), 0, s, jobs, search_marks, search_gen));
     CK_LAUNCH();
   }
-  for (u32 q = 0; q < nj; ++q) dev_free(cnts[q], s);
 }
 
 // down(high, low) of the high entities first..count(high)-1 of each listed

@@ -86,8 +86,10 @@ struct Mesh {
   u32* low_row_offs[3] = {nullptr, nullptr, nullptr};
   u32* low_rows[3] = {nullptr, nullptr, nullptr};
   // (during a pass's searches) vertices of the products whose lows are
-  // searched; the rows then list only lows with a marked smallest vertex
+  // searched, stamped search_gen in the stream's marks; the rows then list
+  // only lows with a marked smallest vertex
   u32* search_marks = nullptr;
+  u32 search_gen = 0;
   std::vector<Tag> tags[4];
   u64* globals[4] = {};
   u32* own_ranks[4] = {};   // cached zeros (single rank), API only

@@ -810,6 +810,69 @@ u32* stream_scan_scratch(size_t words, cudaStream_t s)
 }  // namespace
 
 namespace {
+// Per-stream scratch kept between calls, one per key (what it holds); see
+// stream_zero_scratch and stream_marks
+struct KeptScratch {
+  u32* p = nullptr;
+  size_t words = 0;
+  u32 gen = 0;
+};
+std::mutex g_kept_mu;
+using KeptKey = std::tuple<int, cudaStream_t, u32>;
+std::map<KeptKey, KeptScratch>& kept_scratches()
+{
+  static auto* m = new std::map<KeptKey, KeptScratch>();
+  return *m;
+}
+
+// at least `words` words for (this device, s, key), zeroed when (re)made
+KeptScratch& kept_scratch(u32 key, size_t words, cudaStream_t s)
+{
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  auto& all = kept_scratches();
+  if (all.size() > 4096 && !all.count({dev, s, key})) {
+    // streams come and go: past 4096 entries, wait for the device and
+    // return every other stream's scratch
+    CK(cudaDeviceSynchronize());
+    for (auto& kv : all)
+      if (kv.second.p) cudaFree(kv.second.p);
+    all.clear();
+  }
+  KeptScratch& sc = all[{dev, s, key}];
+  if (sc.words < words) {
+    size_t want = std::max(words + words / 4, (size_t)4096);
+    if (sc.p) CK(cudaFreeAsync(sc.p, s));
+    void* q = nullptr;
+    CK(cudaMallocAsync(&q, want * sizeof(u32), s));
+    CK(cudaMemsetAsync(q, 0, want * sizeof(u32), s));
+    sc.p = static_cast<u32*>(q);
+    sc.words = want;
+    sc.gen = 0;
+  }
+  return sc;
+}
+}  // namespace
+
+u32* stream_zero_scratch(u32 key, size_t words, cudaStream_t s)
+{
+  std::lock_guard<std::mutex> g(g_kept_mu);
+  return kept_scratch(key, words, s).p;
+}
+
+u32* stream_marks(size_t words, cudaStream_t s, u32* gen)
+{
+  std::lock_guard<std::mutex> g(g_kept_mu);
+  KeptScratch& sc = kept_scratch(KEPT_MARKS, words, s);
+  if (++sc.gen == 0) {  // wrapped: no stamp of old may pass for the new one
+    CK(cudaMemsetAsync(sc.p, 0, sc.words * sizeof(u32), s));
+    sc.gen = 1;
+  }
+  *gen = sc.gen;
+  return sc.p;
+}
+
+namespace {
 // tiles of a job (one at least: an empty scan still writes out[0] = 0)
 u32 job_tiles(u32 n, u32 tile) { return n ? ceil_div(n, (u64)tile) : 1u; }
 
