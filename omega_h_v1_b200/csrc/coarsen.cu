@@ -427,12 +427,14 @@ __global__ void k_vertex_dest_grouped(u32 nv, u32 const* __restrict__ ue_offs,
 // collapse_to_ent (collapses_to_ents.cpp:11-64)
 // (ED: the entities' dimension at compile time, so the loads of all their
 // vertices are issued before any is used)
+// (fused_ents / fused_sides: the entities / sides a collapse fuses, marked
+// with the stamps ents_gen / sides_gen of the stream's kept marks)
 template <u32 ED>
 __global__ void k_collapse_to_ent(u32 n, u32 const* __restrict__ voe,
     u32 const* __restrict__ soe, u32 const* __restrict__ gen_offs_v,
-    u32 const* __restrict__ gen_vert_v, u32 const* __restrict__ fused_ents,
-    u32* __restrict__ is_same, u32* __restrict__ fused_sides, u32* __restrict__ will_gen,
-    u32* __restrict__ gen_vert, u32* __restrict__ gen_dir)
+    u32 const* __restrict__ gen_vert_v, u32 const* __restrict__ fused_ents, u32 ents_gen,
+    u32* __restrict__ is_same, u32* __restrict__ fused_sides, u32 sides_gen,
+    u32* __restrict__ will_gen, u32* __restrict__ gen_vert, u32* __restrict__ gen_dir)
 {
   pdl_wait();
   constexpr u32 VPE = ED + 1, SPE = ED + 1;
@@ -465,8 +467,8 @@ __global__ void k_collapse_to_ent(u32 n, u32 const* __restrict__ voe,
   for (u32 j = 0; j < VPE; ++j)
     if (v[j] == gv) gd = j;
   if (gd != INV) {
-    fused_sides[soe[(size_t)i * SPE + opp(ED, 0, gd)]] = 1;
-  } else if (!(fused_ents && fused_ents[i])) {
+    fused_sides[soe[(size_t)i * SPE + opp(ED, 0, gd)]] = sides_gen;
+  } else if (!(fused_ents && fused_ents[i] == ents_gen)) {
     wg = 1;
     gen_vert[i] = gv;
     gen_dir[i] = dir;
@@ -834,7 +836,8 @@ static bool coarsen_build(Mesh& m, CoarsenSel const& sel, bool deferred)
   sj[nsj++] = ScanJob{gen_offs_v, same_v, m.mb->dev + 22, nullptr, nv, 1};
   u32* scan_in[6] = {};
   u32 nscan_in = 0;
-  u32* fused[4] = {nullptr, nullptr, nullptr, nullptr};
+  u32* fused[4] = {nullptr, nullptr, nullptr, nullptr};  // the stream's kept marks
+  u32 fgen[4] = {0, 0, 0, 0};
   u32* same_of[4] = {nullptr, nullptr, nullptr, nullptr};
   u32 nsame_of[4] = {0, 0, 0, 0};
   // the products and survivors of every dimension are counted first (the
@@ -854,8 +857,7 @@ static bool coarsen_build(Mesh& m, CoarsenSel const& sel, bool deferred)
     u32 const* voe = m.ask_down(ed, 0);
     u32 const* soe = m.ask_down(ed, ed - 1);
     u32 nsides = m.count(ed - 1);
-    fused[ed - 1] = dalloc<u32>(nsides, s);
-    CK(cudaMemsetAsync(fused[ed - 1], 0, sizeof(u32) * nsides, s));
+    fused[ed - 1] = stream_marks(KEPT_FUSED + ed - 1, nsides ? nsides : 1, s, &fgen[ed - 1]);
     u32* is_same = dalloc<u32>(n, s);
     u32* will_gen = dalloc<u32>(n, s);
     gvert_of[ed] = dalloc<u32>(n, s);
@@ -866,8 +868,8 @@ static bool coarsen_build(Mesh& m, CoarsenSel const& sel, bool deferred)
       auto k = ed == 1 ? k_collapse_to_ent<1> : ed == 2 ? k_collapse_to_ent<2>
                                                         : k_collapse_to_ent<3>;
       CK(launch_kernel(k, dim3(grid_for(n)), dim3(BLOCK), 0, s, n, voe, soe, gen_offs_v,
-          sel.gen_vert, fused[ed], is_same, fused[ed - 1], will_gen, gvert_of[ed],
-          gdir_of[ed]));
+          sel.gen_vert, fused[ed], fgen[ed], is_same, fused[ed - 1], fgen[ed - 1], will_gen,
+          gvert_of[ed], gdir_of[ed]));
       CK_LAUNCH();
     }
     gen_offs_of[ed] = dalloc<u32>((size_t)n + 1, s);
@@ -886,7 +888,6 @@ static bool coarsen_build(Mesh& m, CoarsenSel const& sel, bool deferred)
   if (deferred) {
     auto abandon = [&] {
       for (u32 d = 0; d < 4; ++d) {
-        dev_free(fused[d], s);
         dev_free(same_of[d], s);
         dev_free(gen_offs_of[d], s);
         dev_free(gen_list_of[d], s);
@@ -995,7 +996,6 @@ static bool coarsen_build(Mesh& m, CoarsenSel const& sel, bool deferred)
   carry_up_all(m, *out, same_of, nsame_of, newid_of);
   for (u32 h = 0; h <= dim; ++h) dev_free(newid_of[h], s);
   for (u32 d = 0; d < 4; ++d) {
-    dev_free(fused[d], s);
     dev_free(same_of[d], s);
   }
   dev_free(gen_offs_v, s);

@@ -1024,7 +1024,7 @@ void Mesh::mark_search_verts(u32 const* first)
   // the stream's marks, stamped with a generation of their own (nothing to
   // zero between uses)
   u32 nv = counts[0];
-  search_marks = stream_marks(nv ? nv : 1, s, &search_gen);
+  search_marks = stream_marks(KEPT_MARKS, nv ? nv : 1, s, &search_gen);
   MarkRanges rs;
   u32 nr = 0, most = 0;
   for (u32 h = 2; h <= dim; ++h) {

@@ -860,10 +860,10 @@ u32* stream_zero_scratch(u32 key, size_t words, cudaStream_t s)
   return kept_scratch(key, words, s).p;
 }
 
-u32* stream_marks(size_t words, cudaStream_t s, u32* gen)
+u32* stream_marks(u32 key, size_t words, cudaStream_t s, u32* gen)
 {
   std::lock_guard<std::mutex> g(g_kept_mu);
-  KeptScratch& sc = kept_scratch(KEPT_MARKS, words, s);
+  KeptScratch& sc = kept_scratch(key, words, s);
   if (++sc.gen == 0) {  // wrapped: no stamp of old may pass for the new one
     CK(cudaMemsetAsync(sc.p, 0, sc.words * sizeof(u32), s));
     sc.gen = 1;

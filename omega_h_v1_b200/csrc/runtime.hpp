@@ -87,11 +87,13 @@ void exscan_jobs(ScanJob const* jobs, u32 njobs, cudaStream_t s);
 // grown. stream_zero_scratch: the caller leaves it zero again after each use
 // (keys KEPT_ROWS0 and KEPT_ROWS1: the search rows' counts, which the rows'
 // fill counts back down to zero). stream_marks: entries stamped with a
-// per-stream generation, returned in *gen (never 0) and new on every call,
-// so no entry of an earlier use passes for a mark of this one.
-enum : u32 { KEPT_ROWS0 = 1, KEPT_ROWS1 = 2, KEPT_MARKS = 3 };
+// generation of the (stream, key), returned in *gen (never 0) and new on
+// every call, so no entry of an earlier use passes for a mark of this one
+// (KEPT_MARKS: the products' vertices of a pass's searches; KEPT_FUSED + d:
+// the collapses' fused entities of dimension d).
+enum : u32 { KEPT_ROWS0 = 1, KEPT_ROWS1 = 2, KEPT_MARKS = 3, KEPT_FUSED = 4 };
 u32* stream_zero_scratch(u32 key, size_t words, cudaStream_t s);
-u32* stream_marks(size_t words, cudaStream_t s, u32* gen);
+u32* stream_marks(u32 key, size_t words, cudaStream_t s, u32* gen);
 
 // The same scan with caller-provided scratch of at least
 // exscan_scratch_words(n) 32-bit words (zeroed here); allocates nothing.
