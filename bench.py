@@ -209,7 +209,9 @@ def pin(a):
 
 
 def e2e_step(G, L, inp, stream_ptr):
-    """One adapt through the public C ABI from pinned host buffers."""
+    """One adapt through the public C ABI from pinned host buffers: the
+    uploads and the result's read-back queued on the mesh's stream
+    (osh_b200_copy_to_*_async), all inside the timed region."""
     h2d = 0
     m = L.osh_new(3)
     G.check()
@@ -220,7 +222,7 @@ def e2e_step(G, L, inp, stream_ptr):
     for d in (1, 2, 3):
         arr = inp["pinned_conn"][d]
         p = L.osh_build_ents(m, d, inp["counts"][d])
-        L.osh_b200_copy_to_device(p, C.c_void_p(arr.data_ptr()), arr.numel() * 4)
+        L.osh_b200_copy_to_device_async(m, p, C.c_void_p(arr.data_ptr()), arr.numel() * 4)
         h2d += arr.numel() * 4
     for d in range(4):
         for (name, ty, nc, tr, _), arr in zip(inp["tags"][d], inp["pinned_tags"][d]):
@@ -229,7 +231,7 @@ def e2e_step(G, L, inp, stream_ptr):
             else:
                 p = L.osh_new_label(m, d, name.encode(), nc)
             nbytes = arr.numel() * arr.element_size()
-            L.osh_b200_copy_to_device(p, C.c_void_p(arr.data_ptr()), nbytes)
+            L.osh_b200_copy_to_device_async(m, p, C.c_void_p(arr.data_ptr()), nbytes)
             h2d += nbytes
     G.check()
     L.osh_adapt(m, SIZE_FLOOR, GOOD_QUAL, NLAYERS, MAX_OPS)
@@ -244,10 +246,11 @@ def e2e_step(G, L, inp, stream_ptr):
         inp["out_conn"] = torch.empty(nt * 4, dtype=torch.int32, pin_memory=True)
     if inp.get("out_x") is None or inp["out_x"].numel() < nvo * 3:
         inp["out_x"] = torch.empty(nvo * 3, dtype=torch.float64, pin_memory=True)
-    L.osh_b200_copy_to_host(C.c_void_p(inp["out_conn"].data_ptr()), L.osh_down(m, 3, 0),
-                            nt * 4 * 4)
-    L.osh_b200_copy_to_host(C.c_void_p(inp["out_x"].data_ptr()), L.osh_coords(m),
-                            nvo * 3 * 8)
+    L.osh_b200_copy_to_host_async(m, C.c_void_p(inp["out_conn"].data_ptr()),
+                                  L.osh_down(m, 3, 0), nt * 4 * 4)
+    L.osh_b200_copy_to_host_async(m, C.c_void_p(inp["out_x"].data_ptr()), L.osh_coords(m),
+                                  nvo * 3 * 8)
+    L.osh_b200_synchronize(m)
     G.check()
     d2h = nt * 4 * 4 + nvo * 3 * 8
     L.osh_free(m)

@@ -379,8 +379,19 @@ int osh_b200_up_from_down_noalloc(unsigned high_dim, unsigned low_dim,
     void* stream) OSH_PUBLIC;
 
 /* ---- memory helpers ----------------------------------------------------- */
+/* The arrays osh_build_ents, osh_new_field and osh_new_label return are
+   device memory, ready for these copies when the call returns. */
 void osh_b200_copy_to_host(void* host_dst, void const* dev_src, size_t bytes) OSH_PUBLIC;
 void osh_b200_copy_to_device(void* dev_dst, void const* host_src, size_t bytes) OSH_PUBLIC;
+/* The same copies queued on mesh m's stream (no counterpart in the
+   reference): they return at once, run in order with m's work, and the host
+   buffer must stay valid, and unchanged for an upload, until the stream has
+   passed the copy (osh_b200_synchronize(m), or any call that returns
+   results). Page-locked host memory makes them asynchronous. */
+void osh_b200_copy_to_host_async(osh_t m, void* host_dst, void const* dev_src, size_t bytes)
+    OSH_PUBLIC;
+void osh_b200_copy_to_device_async(osh_t m, void* dev_dst, void const* host_src, size_t bytes)
+    OSH_PUBLIC;
 void osh_b200_synchronize(osh_t m) OSH_PUBLIC;
 
 /* polygon triangulation table used by edge swapping (edge_swap.cpp:21-228):

@@ -127,6 +127,8 @@ def lib():
     f("osh_b200_edge_lengths", None, vp, _f64p)
     f("osh_b200_copy_to_host", None, vp, vp, C.c_size_t)
     f("osh_b200_copy_to_device", None, vp, vp, C.c_size_t)
+    f("osh_b200_copy_to_host_async", None, vp, vp, vp, C.c_size_t)
+    f("osh_b200_copy_to_device_async", None, vp, vp, vp, C.c_size_t)
     f("osh_b200_synchronize", None, vp)
     f("osh_b200_clone", vp, vp)
     f("osh_b200_set_stream", None, vp, vp)

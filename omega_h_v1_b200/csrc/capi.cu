@@ -68,6 +68,18 @@ void sync(Mesh* m)
   osh::check_device_timeouts(m->s);
 }
 
+// An array just allocated on m's stream, made ready for the caller's copies
+// (osh_b200_copy_to_device runs on the legacy default stream, which waits
+// for the legacy stream and for blocking streams, not for a non-blocking
+// one): a wait only when m's stream is non-blocking; no kernel ran, so no
+// timeout to check.
+void ready_for_copies(Mesh* m)
+{
+  unsigned flags = 0;
+  if (m->s) CK(cudaStreamGetFlags(m->s, &flags));
+  if (flags & cudaStreamNonBlocking) osh::stream_sync(m->s);
+}
+
 __global__ void k_mark_classified(u32 n, u32 const* __restrict__ cd,
     u32 const* __restrict__ cid, u32 target_dim, u32 target_id, u32* __restrict__ marked)
 {
@@ -174,7 +186,7 @@ unsigned* osh_build_ents(osh_t h, unsigned ent_dim, unsigned nents)
   u32* conn = osh::dalloc<u32>((size_t)nents * vpe, m->s);
   osh::dev_free(m->down[ent_dim][0], m->s);
   m->set_ents(ent_dim, nents, conn);
-  sync(m);
+  ready_for_copies(m);
   return conn;
   API_CATCH(nullptr)
 }
@@ -323,7 +335,7 @@ double* osh_new_field(osh_t h, unsigned dim, char const* name, unsigned ncomps,
   if (osh::Tag* t = m->find_tag(dim, name)) return static_cast<double*>(t->data);
   double* d = osh::dalloc<double>((size_t)m->count(dim) * ncomps, m->s);
   m->add_tag(dim, osh::T_F64, name, ncomps, (u32)tt, d);
-  sync(m);
+  ready_for_copies(m);
   return d;
   API_CATCH(nullptr)
 }
@@ -377,7 +389,7 @@ unsigned* osh_new_label(osh_t h, unsigned dim, char const* name, unsigned ncomps
   if (osh::Tag* t = m->find_tag(dim, name)) return static_cast<u32*>(t->data);
   u32* d = osh::dalloc<u32>((size_t)m->count(dim) * ncomps, m->s);
   m->add_tag(dim, osh::T_U32, name, ncomps, osh::X_NOT, d);
-  sync(m);
+  ready_for_copies(m);
   return d;
   API_CATCH(nullptr)
 }
@@ -1145,6 +1157,20 @@ void osh_b200_copy_to_device(void* dst, void const* src, size_t bytes)
 {
   API_TRY
   CK(cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice));
+  API_CATCH_VOID
+}
+
+void osh_b200_copy_to_host_async(osh_t h, void* dst, void const* src, size_t bytes)
+{
+  API_TRY
+  CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, M(h)->s));
+  API_CATCH_VOID
+}
+
+void osh_b200_copy_to_device_async(osh_t h, void* dst, void const* src, size_t bytes)
+{
+  API_TRY
+  CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, M(h)->s));
   API_CATCH_VOID
 }
 

@@ -108,3 +108,33 @@ def test_getters_and_small_entry_points():
     assert not L.osh_read_vtk(b"missing.vtu")
     assert L.osh_b200_last_error() == 9
     L.osh_b200_clear_error()
+
+
+def test_async_copies_round_trip():
+    """osh_b200_copy_to_device_async / _to_host_async run on the mesh's own
+    stream (a non-blocking one here, as osh_new makes it) in order with its
+    work: a field uploaded and copied back, read after
+    osh_b200_synchronize, equals what was sent; the array osh_new_field
+    returns takes the copies at once."""
+    import torch
+    G = _G()
+    L = G.lib()
+    h = L.osh_new(3)
+    G.check()
+    L.osh_build_ents(h, 0, 1000)
+    L.osh_build_ents(h, 3, 0)
+    p = L.osh_new_field(h, 0, b"u", 3, 0)
+    G.check()
+    src = torch.arange(3000, dtype=torch.float64).pin_memory()
+    dst = torch.full((3000,), -1.0, dtype=torch.float64).pin_memory()
+    L.osh_b200_copy_to_device_async(h, p, C.c_void_p(src.data_ptr()), 3000 * 8)
+    L.osh_b200_copy_to_host_async(h, C.c_void_p(dst.data_ptr()), p, 3000 * 8)
+    L.osh_b200_synchronize(h)
+    G.check()
+    assert torch.equal(src, dst)
+    # and the synchronous copy sees the same array
+    back = np.empty(3000)
+    L.osh_b200_copy_to_host(back.ctypes.data_as(C.c_void_p), p, back.nbytes)
+    G.check()
+    assert np.array_equal(back, np.arange(3000, dtype=np.float64))
+    L.osh_free(h)
