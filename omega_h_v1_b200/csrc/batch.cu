@@ -174,17 +174,6 @@ __global__ void k_scatter_meshes(u32 n, u32 width, T const* __restrict__ in,
   }
 }
 
-// global numbers of a single-rank mesh after a pass: the local index
-__global__ void k_scatter_iota64(u32 n, u32 const* __restrict__ es,
-    u32 const* __restrict__ local, u64* const* __restrict__ dst)
-{
-  pdl_wait();
-  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  u64* d = dst[es[i]];
-  if (d) d[local[i]] = local[i];
-}
-
 // per-segment minimum of element qualities (order-preserving keys)
 __global__ void k_seg_min_quality(u32 n, double const* __restrict__ q,
     u32 const* __restrict__ voe, u32 vpe, u32 const* __restrict__ seg,
@@ -329,7 +318,7 @@ void check_batchable(std::vector<Mesh*> const& ms)
     for (u32 d = 0; d <= dim; ++d) {
       if (m->has_dim(d) != a.has_dim(d) || !same_tags(*m, a, d))
         throw Failure(E_ARG, "batched meshes differ in their entities or tags");
-      if (a.parallel && (m->globals[d] == nullptr) != (a.globals[d] == nullptr))
+      if (a.parallel && m->has_globals(d) != a.has_globals(d))
         throw Failure(E_ARG, "batched meshes differ in their global numbers");
     }
   }
@@ -340,6 +329,11 @@ Mesh* concat_meshes(std::vector<Mesh*> const& ms, cudaStream_t stream)
   if (ms.empty()) throw Failure(E_ARG, "a batch needs at least one mesh");
   Mesh& a = *ms[0];
   u32 nm = (u32)ms.size(), dim = a.dim;
+  // identity numbers in every input stay the identity in the union; other
+  // inputs' numbers are written out (on their own streams, before the sync)
+  bool iota_glob[4] = {true, true, true, true};
+  for (Mesh* m : ms)
+    for (u32 d = 0; d < 4; ++d) iota_glob[d] = iota_glob[d] && !m->globals[d];
   for (Mesh* m : ms) {
     if (m->dim != dim || m->full != a.full || m->parallel != a.parallel)
       throw Failure(E_ARG, "batched meshes differ in dimension, representation or parallelism");
@@ -351,9 +345,14 @@ Mesh* concat_meshes(std::vector<Mesh*> const& ms, cudaStream_t stream)
     for (u32 d = 0; d <= dim; ++d) {
       if (m->has_dim(d) != a.has_dim(d) || !same_tags(*m, a, d))
         throw Failure(E_ARG, "batched meshes differ in their entities or tags");
-      if (a.parallel && (m->globals[d] == nullptr) != (a.globals[d] == nullptr))
+      if (a.parallel && m->has_globals(d) != a.has_globals(d))
         throw Failure(E_ARG, "batched meshes differ in their global numbers");
     }
+  }
+  for (Mesh* m : ms) {
+    if (a.parallel)
+      for (u32 d = 0; d <= dim; ++d)
+        if (!iota_glob[d]) m->ask_globals(d);
     stream_sync(m->s);
   }
   Mesh* u = new Mesh(dim, a.full, a.parallel, stream);
@@ -395,7 +394,7 @@ Mesh* concat_meshes(std::vector<Mesh*> const& ms, cudaStream_t stream)
         for (u32 k = 0; k < nm; ++k) p[k] = ms[k]->find_tag(d, a.tags[d][t].name.c_str())->data;
         tag_at[d].push_back(meta.add(p.data(), nm));
       }
-      if (a.parallel && a.globals[d]) {
+      if (a.parallel && a.has_globals(d) && !iota_glob[d]) {
         for (u32 k = 0; k < nm; ++k) p[k] = ms[k]->globals[d];
         glob_at[d] = meta.add(p.data(), nm);
       }
@@ -437,7 +436,9 @@ Mesh* concat_meshes(std::vector<Mesh*> const& ms, cudaStream_t stream)
               data, s);
         u->add_tag(d, tg.type, tg.name.c_str(), tg.ncomps, tg.transfer, data);
       }
-      if (a.parallel && a.globals[d]) {
+      if (a.parallel && a.has_globals(d) && iota_glob[d]) {
+        u->set_iota_globals(d);
+      } else if (a.parallel && a.has_globals(d)) {
         u64* g = dalloc<u64>(n, s);
         launch_concat<u64>(nm, meta, glob_at[d], offs_at[d], 1, meta.at<u64 const>(goff_at[d]),
             n, g, s);
@@ -533,7 +534,7 @@ std::vector<Mesh*> split_union(Mesh& u, cudaStream_t stream, std::vector<char> c
     }
     // allocate every mesh's arrays, then one scatter launch per array
     Meta meta;
-    size_t conn_at[4] = {0, 0, 0, 0}, glob_at[4] = {0, 0, 0, 0};
+    size_t conn_at[4] = {0, 0, 0, 0};
     std::vector<size_t> tag_at[4];
     std::vector<void const*> p(nm);
     for (u32 d = 0; d <= dim; ++d) {
@@ -564,16 +565,10 @@ std::vector<Mesh*> split_union(Mesh& u, cudaStream_t stream, std::vector<char> c
         }
         tag_at[d].push_back(meta.add(p.data(), nm));
       }
-      if (u.parallel && u.globals[d]) {
-        for (u32 k = 0; k < nm; ++k) {
-          p[k] = nullptr;
-          if (!out[k]) continue;
-          u64* g = dalloc<u64>(counts[d][k + 1], s);
-          out[k]->set_globals(d, g);
-          p[k] = g;
-        }
-        glob_at[d] = meta.add(p.data(), nm);
-      }
+      // each mesh's global numbers restart at 0: its local indices
+      if (u.parallel && u.has_globals(d))
+        for (u32 k = 0; k < nm; ++k)
+          if (out[k]) out[k]->set_iota_globals(d);
     }
     meta.upload(s);
     for (u32 d = 0; d <= dim; ++d) {
@@ -593,11 +588,6 @@ std::vector<Mesh*> split_union(Mesh& u, cudaStream_t stream, std::vector<char> c
         else
           launch_scatter<u64>(n, tg.ncomps, tg.data, es[d], local[d], nullptr, meta,
               tag_at[d][t], s);
-      }
-      if (u.parallel && u.globals[d] && n) {
-        CK(launch_kernel(k_scatter_iota64, dim3(grid_for(n)), dim3(BLOCK), 0, s, n, es[d], local[d],
-            meta.at<u64* const>(glob_at[d])));
-        CK_LAUNCH();
       }
     }
     stream_sync(s);
@@ -1012,7 +1002,7 @@ u64 mesh_digest(Mesh& m)
       h = host_mix(h ^ str_hash(t.name) ^ ((u64)t.type << 40) ^ ((u64)t.ncomps << 20) ^ t.transfer);
       add(t.data, (u64)n * t.ncomps * tag_esz(t.type));
     }
-    if (m.globals[d]) add(m.globals[d], (u64)n * 8);
+    if (m.has_globals(d)) add(m.ask_globals(d), (u64)n * 8);
   }
   u64 dev = 0;
   CK(cudaMemcpyAsync(&dev, acc, sizeof(u64), cudaMemcpyDeviceToHost, s));

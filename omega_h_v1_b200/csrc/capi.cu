@@ -287,18 +287,17 @@ unsigned const* osh_own_rank(osh_t h, unsigned dim)
   API_TRY
   Mesh* m = M(h);
   need(dim <= m->dim, "bad dimension");
-  if (!m->own_ranks[dim]) {
+  if (!m->has_own_ranks(dim)) {
     if (m->parallel) {
       // mesh_ask_own_ranks (parallel_mesh.cpp:77-84) derives ranks and ids
       m->note_exchange(dim);
     } else {
-      u32 n = m->count(dim);
-      m->own_ranks[dim] = osh::dalloc<u32>(n, m->s);
-      osh::fill_u32(m->own_ranks[dim], n, 0, m->s);
+      m->ranks_zero[dim] = true;
     }
   }
+  u32 const* r = m->ask_own_ranks(dim);
   sync(m);
-  return m->own_ranks[dim];
+  return r;
   API_CATCH(nullptr)
 }
 
@@ -307,13 +306,10 @@ unsigned const* osh_own_id(osh_t h, unsigned dim)
   API_TRY
   Mesh* m = M(h);
   need(dim <= m->dim, "bad dimension");
-  if (!m->own_ids[dim]) {
-    u32 n = m->count(dim);
-    m->own_ids[dim] = osh::dalloc<u32>(n, m->s);
-    osh::iota_u32(m->own_ids[dim], n, 1, m->s);
-  }
+  if (!m->has_own_ids(dim)) m->ids_iota[dim] = true;
+  u32 const* r = m->ask_own_ids(dim);
   sync(m);
-  return m->own_ids[dim];
+  return r;
   API_CATCH(nullptr)
 }
 
@@ -322,7 +318,9 @@ unsigned long const* osh_global(osh_t h, unsigned dim)
   API_TRY
   Mesh* m = M(h);
   need(dim <= m->dim, "bad dimension");
-  return m->globals[dim];
+  u64 const* g = m->ask_globals(dim);
+  if (g) sync(m);
+  return reinterpret_cast<unsigned long const*>(g);
   API_CATCH(nullptr)
 }
 

@@ -946,7 +946,7 @@ static bool coarsen_build(Mesh& m, CoarsenSel const& sel, bool deferred)
     vjobs.push_back(jb);
   }
   expand_many(vjobs, s);
-  if (m.parallel) inherit_globals(*out, 0, nv_out);
+  if (m.parallel) inherit_globals(*out, 0);
   for (u32 dd = 0; dd < dim; ++dd) {
     u32 ed = dim - dd;
     u32 n = m.count(ed), vpe = deg(ed, 0);
@@ -984,7 +984,7 @@ static bool coarsen_build(Mesh& m, CoarsenSel const& sel, bool deferred)
     d.finish();
     inherit_class(m, *out, ed, d);
     dev_free(gen_list_of[ed], s);
-    if (m.parallel) inherit_globals(*out, ed, nout);
+    if (m.parallel) inherit_globals(*out, ed);
     if (ed == dim) coarsen_transfer(m, *out, gen_offs_v, gen_offs, same_e, nsame, ngen);
     dev_free(gen_offs, s);
     nsame_of[ed] = nsame;

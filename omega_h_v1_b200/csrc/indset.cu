@@ -283,7 +283,9 @@ u32* find_indset(Mesh& m, u32 ent_dim, u32 const* filter, double const* good, bo
   } else {
     throw Failure(E_ARG, "independent sets are built on vertices or edges");
   }
-  u64 const* glob = (m.parallel && m.globals[ent_dim]) ? m.globals[ent_dim] : nullptr;
+  // global numbers held as the identity flag are the local index, which is
+  // what the kernel compares when it has no array
+  u64 const* glob = m.parallel ? m.globals[ent_dim] : nullptr;
   u32* a = dalloc<u32>(n, m.s);
   u32* b = dalloc<u32>(2 * (size_t)n, m.s);  // the two lists of undecided entities
   // One cooperative launch sets the states, lists the candidates and runs
@@ -571,11 +573,9 @@ void inherit_class(Mesh& m, Mesh& out, u32 prod, Doms const& d,
   for (u32 q = 0; q < nnames; ++q) out.add_tag(prod, T_U32, names[q], nc[q], X_NOT, data[q]);
 }
 
-void inherit_globals(Mesh& out, u32 d, u32 n)
+void inherit_globals(Mesh& out, u32 d)
 {
-  u64* g = dalloc<u64>(n, out.s);
-  iota_u64(g, n, out.s);
-  out.set_globals(d, g);
+  out.set_iota_globals(d);
 }
 
 __global__ void k_interp_coords(u32 ne, u32 vpe, u32 const* __restrict__ voe,

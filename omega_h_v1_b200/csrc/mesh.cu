@@ -90,6 +90,9 @@ Mesh* Mesh::clone()
         CK(cudaMemcpyAsync(g, globals[d], sizeof(u64) * n, cudaMemcpyDeviceToDevice, c->s));
         c->globals[d] = g;
       }
+      c->globals_iota[d] = globals_iota[d];
+      c->ranks_zero[d] = ranks_zero[d];
+      c->ids_iota[d] = ids_iota[d];
       u32* const* own[2] = {&own_ranks[d], &own_ids[d]};
       u32** cown[2] = {&c->own_ranks[d], &c->own_ids[d]};
       for (u32 k = 0; k < 2; ++k)
@@ -173,6 +176,7 @@ void Mesh::clear_contents()
     own_ranks[d] = nullptr;
     dev_free(own_ids[d], s);
     own_ids[d] = nullptr;
+    globals_iota[d] = ranks_zero[d] = ids_iota[d] = false;
     counts[d] = 0;
   }
   dev_free(qual_cache, s);
@@ -219,6 +223,9 @@ void Mesh::overwrite(Mesh* with)
     with->own_ranks[d] = nullptr;
     own_ids[d] = with->own_ids[d];
     with->own_ids[d] = nullptr;
+    globals_iota[d] = with->globals_iota[d];
+    ranks_zero[d] = with->ranks_zero[d];
+    ids_iota[d] = with->ids_iota[d];
   }
   ghost_layers = with->ghost_layers;
   qual_cache = with->qual_cache;
@@ -285,10 +292,49 @@ void Mesh::set_globals(u32 d, u64* g)
 {
   dev_free(globals[d], s);
   globals[d] = g;
+  globals_iota[d] = false;
   dev_free(own_ranks[d], s);
   own_ranks[d] = nullptr;
+  ranks_zero[d] = false;
   dev_free(own_ids[d], s);
   own_ids[d] = nullptr;
+  ids_iota[d] = false;
+}
+
+void Mesh::set_iota_globals(u32 d)
+{
+  set_globals(d, nullptr);
+  globals_iota[d] = true;
+}
+
+u64 const* Mesh::ask_globals(u32 d)
+{
+  if (!globals[d] && globals_iota[d]) {
+    u32 n = count(d);
+    globals[d] = dalloc<u64>(n ? n : 1, s);
+    iota_u64(globals[d], n, s);
+  }
+  return globals[d];
+}
+
+u32 const* Mesh::ask_own_ranks(u32 d)
+{
+  if (!own_ranks[d] && ranks_zero[d]) {
+    u32 n = count(d);
+    own_ranks[d] = dalloc<u32>(n ? n : 1, s);
+    fill_u32(own_ranks[d], n, 0, s);
+  }
+  return own_ranks[d];
+}
+
+u32 const* Mesh::ask_own_ids(u32 d)
+{
+  if (!own_ids[d] && ids_iota[d]) {
+    u32 n = count(d);
+    own_ids[d] = dalloc<u32>(n ? n : 1, s);
+    iota_u32(own_ids[d], n, 1, s);
+  }
+  return own_ids[d];
 }
 
 void Mesh::ensure_ghosting(u32 nlayers)
@@ -301,41 +347,24 @@ void Mesh::ensure_ghosting(u32 nlayers)
     own_ranks[d] = nullptr;
     dev_free(own_ids[d], s);
     own_ids[d] = nullptr;
+    ids_iota[d] = false;
+    ranks_zero[d] = nlayers && d <= dim && has_dim(d);
   }
   ghost_layers = nlayers;
-  if (!nlayers) return;
-  for (u32 d = 0; d <= dim; ++d)
-    if (has_dim(d)) {
-      u32 n = count(d);
-      own_ranks[d] = dalloc<u32>(n ? n : 1, s);
-      fill_u32(own_ranks[d], n, 0, s);
-    }
 }
 
 void Mesh::note_exchange(u32 d)
 {
   if (!parallel || seg || d > dim) return;
-  u32 n = count(d);
-  if (!own_ranks[d]) {
-    own_ranks[d] = dalloc<u32>(n ? n : 1, s);
-    fill_u32(own_ranks[d], n, 0, s);
-  }
-  if (!own_ids[d]) {
-    own_ids[d] = dalloc<u32>(n ? n : 1, s);
-    iota_u32(own_ids[d], n, 1, s);
-  }
+  if (!own_ranks[d]) ranks_zero[d] = true;
+  if (!own_ids[d]) ids_iota[d] = true;
 }
 
 void Mesh::make_parallel()
 {
   parallel = true;
   for (u32 d = 0; d <= dim; ++d)
-    if (has_dim(d)) {
-      u32 n = count(d);
-      u64* g = dalloc<u64>(n, s);
-      iota_u64(g, n, s);
-      set_globals(d, g);
-    }
+    if (has_dim(d)) set_iota_globals(d);
 }
 
 // ---------------------------------------------------------------------------

@@ -91,9 +91,16 @@ struct Mesh {
   u32* search_marks = nullptr;
   u32 search_gen = 0;
   std::vector<Tag> tags[4];
+  // Global numbers and owners. On one rank every pass renumbers them to the
+  // trivial values (global number = owner id = local index, owner rank 0);
+  // those are held as flags and written out only when read (ask_globals,
+  // ask_own_ranks, ask_own_ids). An array, when present, wins over its flag.
   u64* globals[4] = {};
-  u32* own_ranks[4] = {};   // cached zeros (single rank), API only
-  u32* own_ids[4] = {};     // cached iota, API only
+  u32* own_ranks[4] = {};
+  u32* own_ids[4] = {};
+  bool globals_iota[4] = {};
+  bool ranks_zero[4] = {};
+  bool ids_iota[4] = {};
   u32 ghost_layers = 0;
   double* qual_cache = nullptr;  // element qualities of this mesh state
   // disjoint union of nseg meshes: segment of every vertex (owned), and the
@@ -177,6 +184,16 @@ struct Mesh {
   // replaces the global numbers of dimension d and forgets its owners
   // (mesh_set_globals, parallel_mesh.cpp:191-196)
   void set_globals(u32 d, u64* g);
+  // the same with global number = local index, held as a flag
+  void set_iota_globals(u32 d);
+  bool has_globals(u32 d) const { return globals[d] || globals_iota[d]; }
+  bool has_own_ranks(u32 d) const { return own_ranks[d] || ranks_zero[d]; }
+  bool has_own_ids(u32 d) const { return own_ids[d] || ids_iota[d]; }
+  // the arrays, written out (on the mesh's stream) if held as flags; null
+  // when the mesh has none
+  u64 const* ask_globals(u32 d);
+  u32 const* ask_own_ranks(u32 d);
+  u32 const* ask_own_ids(u32 d);
 
   // Ghosting bookkeeping of a single-rank parallel mesh. The reference ghosts
   // a parallel mesh at the start of every pass (mesh_ensure_ghosting,
@@ -187,9 +204,9 @@ struct Mesh {
   // to do leaves the mesh in that state, which shows in
   // osh_num_ghost_layers, osh_own_rank / osh_own_id and the own_rank /
   // own_id arrays of its files. On one rank the owner rank is 0 and the
-  // owner id the entity's own index, so own_ranks / own_ids hold exactly
-  // those values whenever the reference would hold them. No-ops unless the
-  // mesh is parallel and not a union of segments.
+  // owner id the entity's own index, so the owners are present (as flags)
+  // exactly when the reference would hold them. No-ops unless the mesh is
+  // parallel and not a union of segments.
   void ensure_ghosting(u32 nlayers);
   void note_exchange(u32 d);
   void derive_model(double crease_angle);  // host classification

@@ -83,7 +83,7 @@ void inherit_class(Mesh& m, Mesh& out, u32 prod_dim, Doms const& d,
 // u64 global numbering of a single-rank parallel mesh after a pass
 // (inherit_globals, parallel_modify.cpp:79-111): survivors keep their order,
 // new entities follow.
-void inherit_globals(Mesh& out, u32 d, u32 n);
+void inherit_globals(Mesh& out, u32 d);
 
 // element coordinates (interp_to_elems of "coordinates", element_field.cpp)
 void interp_coords_to_elems(Mesh& m);

@@ -504,7 +504,7 @@ static u32 refine_build(Mesh& m, EdgeSplits const& es, bool deferred, bool unifo
     }
     flush();
   }
-  if (m.parallel) inherit_globals(*out, 0, nv_out);
+  if (m.parallel) inherit_globals(*out, 0);
   if (m.seg) {
     out->seg = dalloc<u32>(nv_out, s);
     CK(cudaMemcpyAsync(out->seg, m.seg, sizeof(u32) * nv, cudaMemcpyDeviceToDevice, s));
@@ -567,7 +567,7 @@ static u32 refine_build(Mesh& m, EdgeSplits const& es, bool deferred, bool unifo
             4.0 * vpp * (double)d.ngen[dd];
       }
       out->set_ents(prod, nout, conn);
-      if (m.parallel) inherit_globals(*out, prod, nout);
+      if (m.parallel) inherit_globals(*out, prod);
     }
     inherit_class(m, *out, prod, d, &conn_job);
     if (prod == dim) {

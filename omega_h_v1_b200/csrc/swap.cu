@@ -533,6 +533,8 @@ static bool swap_build(Mesh& m, SwapSel const& sel, bool deferred)
     u64* g = dalloc<u64>(nv, s);
     CK(cudaMemcpyAsync(g, m.globals[0], sizeof(u64) * nv, cudaMemcpyDeviceToDevice, s));
     out->set_globals(0, g);
+  } else if (m.parallel && m.globals_iota[0]) {
+    out->set_iota_globals(0);
   }
   UpAdj const& te = m.ask_up(1, 3);
   u32 const* voe1 = m.ask_down(1, 0);
@@ -620,7 +622,7 @@ static bool swap_build(Mesh& m, SwapSel const& sel, bool deferred)
       d.finish();
       inherit_class(m, *out, ed, d);
     }
-    if (m.parallel) inherit_globals(*out, ed, nsame + ngen);
+    if (m.parallel) inherit_globals(*out, ed);
     if (ed == dim) {
       bool any_f64 = false;
       for (auto const& t : m.tags[ed])

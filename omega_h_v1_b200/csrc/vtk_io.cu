@@ -488,11 +488,8 @@ void parallel_from_tags(Mesh& m, u32 d)
   u32 n = m.counts[d];
   u64* gl = dalloc<u64>(n ? n : 1, m.s);
   if (n) CK(cudaMemcpyAsync(gl, g->data, sizeof(u64) * n, cudaMemcpyDeviceToDevice, m.s));
-  m.set_globals(d, gl);
+  m.set_globals(d, gl);  // forgets the owners too
   m.remove_tag(d, "global_number");
-  dev_free(m.own_ranks[d], m.s);
-  dev_free(m.own_ids[d], m.s);
-  m.own_ranks[d] = m.own_ids[d] = nullptr;
   char const* names[2] = {"own_rank", "own_id"};
   u32** dst[2] = {&m.own_ranks[d], &m.own_ids[d]};
   for (u32 k = 0; k < 2; ++k) {
@@ -715,9 +712,9 @@ std::vector<ParallelTag> parallel_tags(Mesh& m, u32 d)
 {
   std::vector<ParallelTag> out;
   if (!m.parallel) return out;
-  if (m.globals[d]) out.push_back({T_U64, "global_number", m.globals[d]});
-  if (m.own_ranks[d]) out.push_back({T_U32, "own_rank", m.own_ranks[d]});
-  if (m.own_ids[d]) out.push_back({T_U32, "own_id", m.own_ids[d]});
+  if (m.has_globals(d)) out.push_back({T_U64, "global_number", m.ask_globals(d)});
+  if (m.has_own_ranks(d)) out.push_back({T_U32, "own_rank", m.ask_own_ranks(d)});
+  if (m.has_own_ids(d)) out.push_back({T_U32, "own_id", m.ask_own_ids(d)});
   return out;
 }
 
