@@ -1280,13 +1280,16 @@ void carry_down_all(Mesh& m, Mesh& out, u32* const* same_of, u32 const* nsame_of
 // its old row whose high entity survived, in the old order, mapped to new
 // ids, followed by the uses of the entities the pass made; a low the pass
 // made has only such uses (a surviving high entity's lows all survive).
-// On short rows (edges, faces) one thread walks one old row, four uses at a
-// time with their loads issued together; long rows (vertices) take a lane
+// On short rows (edges, faces) one thread walks one old row, eight uses at
+// a time with their loads issued together; long rows (vertices) take a lane
 // group each (the _grouped kernels below). newid_h holds each old high
-// entity's new id or INV, one gather per use. (Measured alternatives: a
+// entity's new id or INV, one gather per use. The kernel is bound by how
+// many rows are in flight, not by the gather. (Measured alternatives: a
 // lane group for every row left too few short rows in flight and ran at
 // half the speed; a warp per 32 rows reading their uses coalesced ran at
-// the same speed as a thread per row.)
+// the same speed as a thread per row; for passes that removed few
+// entities, new ids from a shared-memory table of id buckets, on a grid
+// capped to the blocks that fit with the table, ran 25% slower.)
 __global__ void k_new_ids(u32 n, u32 const* __restrict__ same, u32* __restrict__ newid)
 {
   pdl_wait();
@@ -1320,6 +1323,8 @@ __device__ inline void up_gen_fill(UpGen const& g, u32 k, u32 const* __restrict_
   dirs[slot] = u % g.lph;
 }
 
+constexpr u32 FILL_BATCH = 8;
+
 __global__ void k_up_surv_fill(u32 nl_old, u32 const* __restrict__ same_l,
     u32 const* __restrict__ newid_h, u32 const* __restrict__ offs_old,
     u32 const* __restrict__ adj_old, u32 const* __restrict__ dirs_old,
@@ -1334,30 +1339,30 @@ __global__ void k_up_surv_fill(u32 nl_old, u32 const* __restrict__ same_l,
   u32 nj = same_l[j];
   if (same_l[j + 1] == nj) return;
   u32 w = offs[nj];
-  u32 r = offs_old[j], e = offs_old[j + 1];
-  for (; r + 4 <= e; r += 4) {
-    u32 a[4], d[4], na[4];
+  u32 const e = offs_old[j + 1];
+  // FILL_BATCH uses per round, predicated past the row's end (INV marks
+  // those: no high entity has that id), so most rows take one round of
+  // loads and one of gathers
+  for (u32 r = offs_old[j]; r < e; r += FILL_BATCH) {
+    u32 a[FILL_BATCH], d[FILL_BATCH];
 #pragma unroll
-    for (u32 k = 0; k < 4; ++k) {
-      a[k] = adj_old[r + k];
-      d[k] = dirs_old[r + k];
+    for (u32 k = 0; k < FILL_BATCH; ++k) {
+      a[k] = INV;
+      d[k] = 0;
+      if (r + k < e) {
+        a[k] = adj_old[r + k];
+        d[k] = dirs_old[r + k];
+      }
     }
 #pragma unroll
-    for (u32 k = 0; k < 4; ++k) na[k] = newid_h[a[k]];
+    for (u32 k = 0; k < FILL_BATCH; ++k) a[k] = a[k] != INV ? newid_h[a[k]] : INV;
 #pragma unroll
-    for (u32 k = 0; k < 4; ++k)
-      if (na[k] != INV) {
-        adj[w] = na[k];
+    for (u32 k = 0; k < FILL_BATCH; ++k)
+      if (a[k] != INV) {
+        adj[w] = a[k];
         dirs[w] = d[k];
         ++w;
       }
-  }
-  for (; r < e; ++r) {
-    u32 na = newid_h[adj_old[r]];
-    if (na == INV) continue;
-    adj[w] = na;
-    dirs[w] = dirs_old[r];
-    ++w;
   }
 }
 
