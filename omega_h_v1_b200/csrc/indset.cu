@@ -61,7 +61,8 @@ struct Nbrs {
 // All rounds run in one launch: a cooperative grid (every block resident)
 // sets the states and lists the candidates, then runs round 0 over them and
 // later rounds over the list the round before left, separated by a grid
-// barrier, until a round leaves no entity undecided or 100 rounds have run.
+// barrier (by a block barrier when block 0 alone takes few candidates),
+// until a round leaves no entity undecided or 100 rounds have run.
 // Control words (zero on entry but [1]: see the prologue): [0] barrier
 // arrivals, [1] barrier generation (only its changes count), [2..4]
 // length of the list round r builds for round r + 1, r + 1 = 0, 1, 2 mod 3
@@ -134,6 +135,13 @@ __global__ void __launch_bounds__(BLOCK, 4) k_indset_coop(u32 n, Nbrs g,
   }
   __threadfence();
   if (!coop_barrier(ctl)) return;
+  // A short candidate list (two sweeps of one block at most) is left to
+  // block 0, whose rounds are separated by block barriers instead of grid
+  // barriers. Every block decides the same: one reading the length after
+  // block 0 has gone on reads a later list's length or zero, never more.
+  bool const solo = (u64)(*(volatile u32*)&ctl[2]) * G <= 2u * blockDim.x;
+  if (solo && blockIdx.x != 0) return;
+  u32 const rstride = solo ? blockDim.x : stride;
   for (u32 r = 0; r < MAX_INDSET_ROUNDS; ++r) {
     // round 0 walks the candidates, round r > 0 the list round r - 1 left
     u32 const len = *(volatile u32*)&ctl[2 + r % 3];
@@ -141,7 +149,7 @@ __global__ void __launch_bounds__(BLOCK, 4) k_indset_coop(u32 n, Nbrs g,
     u32* next = (r % 2 == 0) ? wl0 : wl1;
     u32* next_len = &ctl[2 + (r + 1) % 3];
     if (blockIdx.x == 0 && threadIdx.x == 0) ctl[2 + (r + 2) % 3] = 0;
-    for (u64 t = (u64)blockIdx.x * blockDim.x + threadIdx.x; t < (u64)len * G; t += stride) {
+    for (u64 t = (u64)blockIdx.x * blockDim.x + threadIdx.x; t < (u64)len * G; t += rstride) {
       // past L1, like the states: the lists alternate between two
       // buffers, so this block may hold lines of this one from two rounds
       // ago that other blocks have since rewritten
@@ -194,11 +202,14 @@ __global__ void __launch_bounds__(BLOCK, 4) k_indset_coop(u32 n, Nbrs g,
       }
     }
     __threadfence();
-    if (!coop_barrier(ctl)) return;
+    if (solo)
+      __syncthreads();
+    else if (!coop_barrier(ctl))
+      return;
     if (*(volatile u32*)next_len == 0) {
-      // settled: every block has passed the last barrier and reads only
-      // next_len (zero) from here, so the list lengths go back to zero for
-      // the next set's prologue
+      // settled: every block still running has passed the last barrier and
+      // reads only next_len (zero) from here, so the list lengths go back to
+      // zero for the next set's prologue
       if (blockIdx.x == 0 && threadIdx.x == 0) {
         ctl[5] = r + 1;
         ctl[2] = ctl[3] = ctl[4] = 0;
