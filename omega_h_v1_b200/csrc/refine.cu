@@ -272,6 +272,41 @@ __device__ inline void vertex_maps(VertexMaps const& vm, u32 i)
   if (vm.newid && i < vm.nv) vm.newid[i] = i;
 }
 
+// The same marks from the split edges' side: the faces and elements in the
+// upward rows of each split edge, stamped with a generation in kept marks
+// (no array of every domain entity is written or read here). A thread per
+// split edge of the list, whose length is the split edges' scan total,
+// read here; a capped grid strides over the list, then over the vertices'
+// maps.
+struct SplitMark {
+  u32 const* offs;  // up(1, dd) of the mesh being refined
+  u32 const* adj;
+  u32* marks;
+  u32 gen;
+};
+struct SplitMarks {
+  SplitMark d[2];  // domain dimensions 2 and 3 (marks null: not this way)
+};
+
+__global__ void k_mark_split_domains(u32 const* __restrict__ list,
+    u32 const* __restrict__ nsplit_at, SplitMarks sm, VertexMaps vm)
+{
+  pdl_wait();
+  u32 const stride = gridDim.x * blockDim.x, t0 = blockIdx.x * blockDim.x + threadIdx.x;
+  u32 const nsplit = *nsplit_at;
+  for (u32 t = t0; t < nsplit; t += stride) {
+    u32 const e = list[t];
+#pragma unroll
+    for (u32 q = 0; q < 2; ++q) {
+      SplitMark const& d = sm.d[q];
+      if (!d.marks) continue;
+      for (u32 j = d.offs[e], f = d.offs[e + 1]; j < f; ++j) d.marks[d.adj[j]] = d.gen;
+    }
+  }
+  if (vm.zero)
+    for (u32 t = t0; t <= vm.nv; t += stride) vertex_maps(vm, t);
+}
+
 template <u32 SPD>
 __global__ void k_split_to_domain(u32 nd, u32 const* __restrict__ sod,
     u32 const* __restrict__ gen_offs, u32* __restrict__ will, VertexMaps vm)
@@ -416,9 +451,31 @@ static u32 refine_build(Mesh& m, EdgeSplits const& es, bool deferred, bool unifo
   u32* will[4] = {nullptr, nullptr, nullptr, nullptr};
   ScanJob jobs[4];
   u32 njobs = 0;
+  // A domain dimension whose upward rows from the edges the mesh holds is
+  // marked from the split edges (k_mark_split_domains) unless every edge
+  // splits; the others by a pass over every domain entity
+  SplitMarks sm{};
+  bool any_sparse = false;
   for (u32 dd = 2; dd <= dim; ++dd) {
     if (!m.has_dim(dd)) continue;
     u32 nd = m.count(dd);
+    if (!uniform && nd && m.have_up[1][dd]) {
+      SplitMark& d = sm.d[dd - 2];
+      d.offs = m.up[1][dd].offs;
+      d.adj = m.up[1][dd].adj;
+      d.marks = stream_marks(KEPT_SPLIT + dd, nd, s, &d.gen);
+      any_sparse = true;
+      sp[dd].offs = dalloc<u32>((size_t)nd + 1, s);
+      sp[dd].list = dalloc<u32>(nd, s);
+      ScanJob j{d.marks, sp[dd].offs, m.mb->dev + 8 + dd, nullptr, nd, 2, sp[dd].list};
+      j.stamp = d.gen;
+      if (is_prod(dd)) {
+        same_of[dd] = j.comp = dalloc<u32>((size_t)nd + 1, s);
+        if (carried_high(m, dd)) newid_of[dd] = j.comp_newid = dalloc<u32>(nd, s);
+      }
+      jobs[njobs++] = j;
+      continue;
+    }
     u32 const* sod = m.ask_down(dd, 1);
     will[dd] = dalloc<u32>(nd, s);
     if (nd || vm.zero) {
@@ -437,6 +494,14 @@ static u32 refine_build(Mesh& m, EdgeSplits const& es, bool deferred, bool unifo
       if (carried_high(m, dd)) newid_of[dd] = j.comp_newid = dalloc<u32>(nd ? nd : 1, s);
     }
     jobs[njobs++] = j;
+  }
+  if (any_sparse) {
+    // the split edges' count is their scan's total, gen_offs[n_edges]
+    u32 const grid = std::min<u32>(grid_for((u64)std::max(ns, nv) + 1), 148u * 8u);
+    CK(launch_kernel(k_mark_split_domains, dim3(grid), dim3(BLOCK), 0, s, es.list,
+        gen_offs + ns, sm, vm));
+    CK_LAUNCH();
+    vm.zero = nullptr;  // done
   }
   if (vm.zero) {
     CK(launch_kernel(k_vertex_maps, dim3(grid_for((u64)nv + 1)), dim3(BLOCK), 0, s, vm));

@@ -595,9 +595,10 @@ constexpr unsigned long long FLAG_AGG = 1ull << 62;
 constexpr unsigned long long FLAG_PRE = 2ull << 62;
 constexpr u32 SCAN_SPIN_LIMIT = 1u << 24;
 
-// Several independent scans in one launch. Job j scans its `in` (mode 0)
-// or the survivors of an offsets array, (in[i + 1] == in[i]) (mode 1,
-// uints_negate_offsets, ints.cpp:227-235), into out[0..n] with the total at
+// Several independent scans in one launch. Job j scans its `in` (mode 0),
+// the survivors of an offsets array, (in[i + 1] == in[i]) (mode 1,
+// uints_negate_offsets, ints.cpp:227-235), or the entries stamped with its
+// stamp, (in[i] == stamp) (mode 2), into out[0..n] with the total at
 // out[n] (and in *total_to when given); newid (optional, for 0/1 items)
 // receives out[i] where item i is 1 and INV where it is 0 -- each old
 // entity's new id when the items mark survivors. Tiles are numbered across
@@ -627,7 +628,8 @@ k_exscan(ScanJobs jobs, unsigned long long* status, u32* ticket_and_err, u32 spi
   u32 const first = jobs.tile0[jn], last = jobs.tile0[jn + 1] - 1;
   u32 const* __restrict__ in = job.in;
   u32 const n = job.n;
-  bool const mode1 = job.mode != 0;
+  bool const mode1 = job.mode == 1, mode2 = job.mode == 2;
+  u32 const stamp = job.stamp;
   size_t const base = (size_t)(tile - first) * SCAN_TILE;
   // coalesced load into shared memory (padded to avoid bank conflicts)
 #pragma unroll
@@ -635,7 +637,9 @@ k_exscan(ScanJobs jobs, unsigned long long* status, u32* ticket_and_err, u32 spi
     u32 li = k * SCAN_THREADS + threadIdx.x;
     size_t gi = base + li;
     u32 v = 0;
-    if (gi < n) v = !mode1 ? in[gi] : (in[gi + 1] == in[gi] ? 1u : 0u);
+    if (gi < n)
+      v = mode2 ? (in[gi] == stamp ? 1u : 0u)
+                : !mode1 ? in[gi] : (in[gi + 1] == in[gi] ? 1u : 0u);
     s_buf[li + (li >> 5)] = v;
   }
   __syncthreads();
@@ -730,7 +734,7 @@ k_exscan(ScanJobs jobs, unsigned long long* status, u32* ticket_and_err, u32 spi
       out[gi] = o;
       if (comp) comp[gi] = (u32)gi - o;
       if (newid || list || comp_newid) {
-        bool const on = !mode1 ? in[gi] != 0 : in[gi + 1] == in[gi];
+        bool const on = mode2 ? in[gi] == stamp : !mode1 ? in[gi] != 0 : in[gi + 1] == in[gi];
         if (newid) newid[gi] = on ? o : INV;
         if (list && on) list[o] = (u32)gi;
         if (comp_newid) comp_newid[gi] = on ? INV : (u32)gi - o;

@@ -66,15 +66,18 @@ struct ScanJob {
   u32* newid;
   u32 n;
   u32 mode;
-  // (optional, mode 0 with 0/1 items) list[out[i]] = i where item i is 1:
-  // the marked items in order
+  // (optional, 0/1 items: mode 0 with 0/1 items, or mode 2) list[out[i]] = i
+  // where item i is 1: the marked items in order
   u32* list = nullptr;
-  // (optional, mode 0 with 0/1 items) the scan of the complement,
+  // (optional, 0/1 items) the scan of the complement,
   // comp[i] = i - out[i] for i <= n (the unmarked items before i), and
   // comp_newid[i] = comp[i] where item i is 0 and INV where it is 1 -- each
   // survivor's new id when the items mark what a pass removes
   u32* comp = nullptr;
   u32* comp_newid = nullptr;
+  // mode 2: item i is 1 where in[i] == stamp, else 0 (marks stamped with a
+  // generation, see stream_marks)
+  u32 stamp = 0;
 };
 struct ScanJobs {
   u32 njobs;
@@ -90,8 +93,9 @@ void exscan_jobs(ScanJob const* jobs, u32 njobs, cudaStream_t s);
 // generation of the (stream, key), returned in *gen (never 0) and new on
 // every call, so no entry of an earlier use passes for a mark of this one
 // (KEPT_MARKS: the products' vertices of a pass's searches; KEPT_FUSED + d:
-// the collapses' fused entities of dimension d).
-enum : u32 { KEPT_ROWS0 = 1, KEPT_ROWS1 = 2, KEPT_MARKS = 3, KEPT_FUSED = 4 };
+// the collapses' fused entities of dimension d; KEPT_SPLIT + d: a
+// refinement's split domain entities of dimension d).
+enum : u32 { KEPT_ROWS0 = 1, KEPT_ROWS1 = 2, KEPT_MARKS = 3, KEPT_FUSED = 4, KEPT_SPLIT = 8 };
 u32* stream_zero_scratch(u32 key, size_t words, cudaStream_t s);
 u32* stream_marks(u32 key, size_t words, cudaStream_t s, u32* gen);
 

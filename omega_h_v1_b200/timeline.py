@@ -27,10 +27,16 @@ def _gaps(path, top):
                                                                     "gpu_memset")]
     gpu.sort(key=lambda e: e["ts"])
     ts = [(e["ts"], e["ts"] + e["dur"], e["name"], e["cat"]) for e in gpu]
-    # the two recorded adapts, split at the largest gap between operations
-    gaps = [(ts[i + 1][0] - ts[i][1], i) for i in range(len(ts) - 1)]
-    cut = max(gaps)[1] + 1
-    for part in (ts[:cut], ts[cut:]):
+    # the two recorded adapts, split at the marker kernel run between them
+    # (a fill of torch's), else at the largest gap between operations
+    marks = [i for i, t in enumerate(ts) if t[3] == "kernel" and "FillFunctor" in t[2]]
+    if marks:
+        parts = (ts[:marks[0]], ts[marks[0] + 1:])
+    else:
+        gaps = [(ts[i + 1][0] - ts[i][1], i) for i in range(len(ts) - 1)]
+        cut = max(gaps)[1] + 1
+        parts = (ts[:cut], ts[cut:])
+    for part in parts:
         t0, t1 = part[0][0], part[-1][1]
         busy = sum(b - a for a, b, _, _ in part)
         kern = sum(b - a for a, b, _, c in part if c == "kernel")
@@ -90,6 +96,7 @@ def main(argv=None):
         L.osh_adapt(hs[i], 1 / 3., 0.3, 4, 50)
         G.check()
         L.osh_free(hs[i])
+    marker = torch.zeros(1, device="cuda")
     torch.cuda.synchronize()
     with profile(activities=[ProfilerActivity.CPU, ProfilerActivity.CUDA]) as prof:
         for i in range(4, 6):
@@ -97,6 +104,9 @@ def main(argv=None):
             G.check()
             torch.cuda.synchronize()
             L.osh_free(hs[i])
+            if i == 4:
+                marker.fill_(1.0)  # the boundary between the two adapts
+                torch.cuda.synchronize()
     path = args.trace or os.path.join(tempfile.mkdtemp(), "trace.json")
     prof.export_chrome_trace(path)
     _gaps(path, args.top)
