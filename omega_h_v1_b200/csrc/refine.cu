@@ -68,6 +68,10 @@ __device__ inline void refine_child(u32 dim, u32 const* __restrict__ ve, u32 dir
 // them when every child is surely upright and the worst surely below the
 // floor; otherwise only the children whose lower bound reaches the lowest
 // upper bound seen (they alone can hold the minimum) are computed in double.
+// (Measured alternatives, both slower over an adapt: a group of 8 lanes per
+// candidate edge, each lane some of its children, at 105 registers against
+// 82; and one wave of resident blocks striding over the edges, which left
+// the passes with many candidates to the threads that drew the most.)
 template <u32 DIM>
 __global__ void k_refine_quality(u32 ne, u32 const* __restrict__ voe1,
     u32 const* __restrict__ voe, u32 const* __restrict__ eo_offs,
@@ -190,24 +194,25 @@ struct NodalFields {
   u32 nc[MAX_NODAL_FIELDS];
 };
 
-__global__ void k_refine_nodal(u32 ne, u32 nv, u32 const* __restrict__ voe,
-    u32 const* __restrict__ gen_offs, const __grid_constant__ NodalFields fields)
+// (split: the split edges in order, nsplit of them; the k-th one's new
+// vertex is nv + k)
+__global__ void k_refine_nodal(u32 nsplit, u32 nv, u32 const* __restrict__ voe,
+    u32 const* __restrict__ split, const __grid_constant__ NodalFields fields)
 {
   pdl_wait();
   u32 const nc = fields.nc[blockIdx.y];
   double const* __restrict__ f = fields.f[blockIdx.y];
   double* __restrict__ out = fields.out[blockIdx.y];
-  u64 const ncopy = (u64)nv * nc, total = ncopy + ne;
+  u64 const ncopy = (u64)nv * nc, total = ncopy + nsplit;
   for (u64 t = (u64)blockIdx.x * blockDim.x + threadIdx.x; t < total;
        t += (u64)gridDim.x * blockDim.x) {
     if (t < ncopy) {
       out[t] = f[t];
       continue;
     }
-    u32 i = (u32)(t - ncopy);
-    if (gen_offs[i] == gen_offs[i + 1]) continue;
+    u32 const k = (u32)(t - ncopy), i = split[k];
     u32 a = voe[i * 2], b = voe[i * 2 + 1];
-    double* o = out + (size_t)(nv + gen_offs[i]) * nc;
+    double* o = out + (size_t)(nv + k) * nc;
     for (u32 c = 0; c < nc; ++c) {
       double acc = 0;
       acc += f[(size_t)a * nc + c];
@@ -551,8 +556,8 @@ static u32 refine_build(Mesh& m, EdgeSplits const& es, bool deferred, bool unifo
       if (!nfields) return;
       u32 const gb = tuned(TK_GATHER_BLOCK);
       u32 gx = (u32)std::min<u64>(ceil_div(most, (u64)gb), 148u * 8u * 256u / gb);
-      CK(launch_kernel(k_refine_nodal, dim3(gx ? gx : 1, nfields), dim3(gb), 0, s, ns, nv, voe1,
-          gen_offs, nf));
+      CK(launch_kernel(k_refine_nodal, dim3(gx ? gx : 1, nfields), dim3(gb), 0, s, nsplit, nv,
+          voe1, es.list, nf));
       CK_LAUNCH();
       nfields = 0;
       most = 0;
@@ -563,7 +568,7 @@ static u32 refine_build(Mesh& m, EdgeSplits const& es, bool deferred, bool unifo
       nf.f[nfields] = static_cast<double const*>(t.data);
       nf.out[nfields] = d;
       nf.nc[nfields] = t.ncomps;
-      most = std::max<u64>(most, (u64)nv * t.ncomps + ns);
+      most = std::max<u64>(most, (u64)nv * t.ncomps + nsplit);
       if (++nfields == MAX_NODAL_FIELDS) flush();
       out->add_tag(0, T_F64, t.name.c_str(), t.ncomps, X_NOT, d);
     }
