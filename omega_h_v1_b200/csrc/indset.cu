@@ -528,10 +528,13 @@ void expand_many(std::vector<ExpandJob> const& jobs, cudaStream_t s)
 // class_dim / class_id of the products: every domain of both labels in one
 // launch
 void inherit_class(Mesh& m, Mesh& out, u32 prod, Doms const& d,
-    std::vector<ExpandJob> const* also)
+    std::vector<ExpandJob> const* also, std::vector<ExpandJob>* defer)
 {
   if (!m.find_tag(0, "class_dim")) {
-    if (also) expand_many(*also, m.s);
+    if (also && defer)
+      defer->insert(defer->end(), also->begin(), also->end());
+    else if (also)
+      expand_many(*also, m.s);
     return;
   }
   char const* names[2] = {"class_dim", "class_id"};
@@ -580,7 +583,10 @@ void inherit_class(Mesh& m, Mesh& out, u32 prod, Doms const& d,
       jobs.push_back(jb);
     }
   }
-  expand_many(jobs, m.s);
+  if (defer)
+    defer->insert(defer->end(), jobs.begin(), jobs.end());
+  else
+    expand_many(jobs, m.s);
   for (u32 q = 0; q < nnames; ++q) out.add_tag(prod, T_U32, names[q], nc[q], X_NOT, data[q]);
 }
 

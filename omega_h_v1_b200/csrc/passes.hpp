@@ -77,8 +77,11 @@ struct Doms {
 // class_dim / class_id of the products of `prod_dim` (inherit_class,
 // inherit.cpp:217-232)
 // `also` (optional): further row expansions launched with the labels' copies
+// `defer` (optional): the copies are appended there for the caller to
+// launch (expand_many) instead of launched here; what they read must stay
+// allocated until then
 void inherit_class(Mesh& m, Mesh& out, u32 prod_dim, Doms const& d,
-    std::vector<ExpandJob> const* also = nullptr);
+    std::vector<ExpandJob> const* also = nullptr, std::vector<ExpandJob>* defer = nullptr);
 
 // u64 global numbering of a single-rank parallel mesh after a pass
 // (inherit_globals, parallel_modify.cpp:79-111): survivors keep their order,

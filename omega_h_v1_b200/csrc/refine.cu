@@ -586,6 +586,9 @@ static u32 refine_build(Mesh& m, EdgeSplits const& es, bool deferred, bool unifo
   TopoJobs tj;
   u32 ntj = 0, tmost = 0;
   double tbytes = 0;
+  // the survivors' connectivity and every dimension's label copies, launched
+  // together after the loop (8 jobs to a launch)
+  std::vector<ExpandJob> copies;
   for (u32 prod = 0; prod <= dim; ++prod) {
     if (!m.full && 0 < prod && prod < dim) continue;
     u32 np = m.count(prod);
@@ -639,7 +642,7 @@ static u32 refine_build(Mesh& m, EdgeSplits const& es, bool deferred, bool unifo
       out->set_ents(prod, nout, conn);
       if (m.parallel) inherit_globals(*out, prod);
     }
-    inherit_class(m, *out, prod, d, &conn_job);
+    inherit_class(m, *out, prod, d, &conn_job, &copies);
     if (prod == dim) {
       for (int pass = 0; pass < 2; ++pass) {
         u32 want = pass == 0 ? X_CONSERVE : X_POINTWISE;
@@ -661,6 +664,7 @@ static u32 refine_build(Mesh& m, EdgeSplits const& es, bool deferred, bool unifo
     same_of[prod] = same;
     nsame_of[prod] = np - sp[prod].nsplit;
   }
+  expand_many(copies, s);
   if (ntj) {
     PROBE(P_REFINE_TOPOLOGY, s, tbytes);
     CK(launch_kernel(k_refine_topology, dim3(grid_for(tmost), ntj), dim3(BLOCK), 0, s, tj,
