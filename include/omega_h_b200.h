@@ -319,6 +319,10 @@ int osh_b200_exscan_u32(unsigned const* in, unsigned* out, unsigned n, void* str
 /* run all further work of mesh m on the CUDA stream `stream` (a
    cudaStream_t; 0 is the legacy default stream); the caller keeps it alive */
 void osh_b200_set_stream(osh_t m, void* stream) OSH_PUBLIC;
+/* before the caller destroys a stream it gave to osh_b200_set_stream: frees
+   the scratch the library keeps for that stream (in the stream's order), so
+   that it does not outlive it. No mesh may use the stream afterwards. */
+void osh_b200_release_stream(void* stream) OSH_PUBLIC;
 
 /* ---- launch shapes (tuning table) ------------------------------------------ */
 /* No counterpart in the reference (its loops launch 256 threads per block,

@@ -132,6 +132,7 @@ def lib():
     f("osh_b200_synchronize", None, vp)
     f("osh_b200_clone", vp, vp)
     f("osh_b200_set_stream", None, vp, vp)
+    f("osh_b200_release_stream", None, vp)
     f("osh_b200_adapt_stats", None, C.POINTER(C.c_uint), C.POINTER(C.c_double))
     f("osh_b200_adapt_batch", C.c_int, C.POINTER(vp), C.c_uint, C.c_double, C.c_double,
       C.c_uint, C.c_uint, C.c_ulonglong, C.POINTER(C.c_uint), C.POINTER(C.c_int))

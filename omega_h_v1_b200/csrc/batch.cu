@@ -1145,6 +1145,7 @@ void adapt_batch(std::vector<Mesh*> const& ms, double size_floor, double good_qu
   auto cleanup = [&]() {
     for (u32 k = 0; k < n; ++k)
       if (owned[k]) delete cur[k];
+    release_stream_scratch(run.s);
     cudaStreamSynchronize(run.s);
     cudaStreamDestroy(run.s);
   };

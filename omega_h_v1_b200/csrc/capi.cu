@@ -1226,6 +1226,13 @@ void osh_b200_set_stream(osh_t h, void* stream)
   API_CATCH_VOID
 }
 
+void osh_b200_release_stream(void* stream)
+{
+  API_TRY
+  osh::release_stream_scratch(static_cast<cudaStream_t>(stream));
+  API_CATCH_VOID
+}
+
 void osh_b200_probe_enable(unsigned mask) { osh::probe_enable(mask); }
 
 void osh_b200_probe_reset(void)

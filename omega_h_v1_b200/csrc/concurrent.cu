@@ -280,6 +280,7 @@ void adapt_concurrent(std::vector<Mesh*> const& ms, AdaptParams const& ap, u32 n
       }
       cv.notify_all();
     }
+    release_stream_scratch(st);
     cudaStreamSynchronize(st);
     cudaStreamDestroy(st);
   };

@@ -49,6 +49,7 @@ Mesh::~Mesh()
   }
   if (own_stream) {
     mb.reset();
+    release_stream_scratch(s);
     cudaStreamSynchronize(s);
     cudaStreamDestroy(s);
   }
@@ -131,7 +132,10 @@ void Mesh::own_new_stream()
 void Mesh::use_stream(cudaStream_t stream)
 {
   stream_sync(s);
-  if (own_stream) CK(cudaStreamDestroy(s));
+  if (own_stream) {
+    release_stream_scratch(s);
+    CK(cudaStreamDestroy(s));
+  }
   own_stream = false;
   s = stream;
 }

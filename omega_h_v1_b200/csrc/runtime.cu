@@ -771,7 +771,8 @@ namespace {
 // Scratch of the scans issued on each stream ([ticket, error, done, pad]
 // then two words per tile), zero between scans: the scan kernel's last tile
 // clears it, so no scan pays for a memset. Scans on one stream run one
-// after another; each stream has its own.
+// after another; each stream has its own, freed by release_stream_scratch
+// when the stream goes.
 struct ScanScratch {
   u32* p = nullptr;
   size_t words = 0;
@@ -789,14 +790,6 @@ u32* stream_scan_scratch(size_t words, cudaStream_t s)
   CK(cudaGetDevice(&dev));
   std::lock_guard<std::mutex> g(g_scan_mu);
   auto& all = scan_scratches();
-  if (all.size() > 1024 && !all.count({dev, s})) {
-    // streams come and go (one per mesh that owns its stream): past 1024
-    // entries, wait for the device and return every other stream's scratch
-    CK(cudaDeviceSynchronize());
-    for (auto& kv : all)
-      if (kv.second.p) cudaFree(kv.second.p);
-    all.clear();
-  }
   ScanScratch& sc = all[{dev, s}];
   if (sc.words < words) {
     size_t want = std::max(words, (size_t)4096);
@@ -835,14 +828,6 @@ KeptScratch& kept_scratch(u32 key, size_t words, cudaStream_t s)
   int dev = 0;
   CK(cudaGetDevice(&dev));
   auto& all = kept_scratches();
-  if (all.size() > 4096 && !all.count({dev, s, key})) {
-    // streams come and go: past 4096 entries, wait for the device and
-    // return every other stream's scratch
-    CK(cudaDeviceSynchronize());
-    for (auto& kv : all)
-      if (kv.second.p) cudaFree(kv.second.p);
-    all.clear();
-  }
   KeptScratch& sc = all[{dev, s, key}];
   if (sc.words < words) {
     size_t want = std::max(words + words / 4, (size_t)4096);
@@ -857,6 +842,28 @@ KeptScratch& kept_scratch(u32 key, size_t words, cudaStream_t s)
   return sc;
 }
 }  // namespace
+
+void release_stream_scratch(cudaStream_t s)
+{
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return;
+  {
+    std::lock_guard<std::mutex> g(g_scan_mu);
+    auto& all = scan_scratches();
+    auto it = all.find({dev, s});
+    if (it != all.end()) {
+      if (it->second.p) cudaFreeAsync(it->second.p, s);
+      all.erase(it);
+    }
+  }
+  std::lock_guard<std::mutex> g(g_kept_mu);
+  auto& all = kept_scratches();
+  for (auto it = all.lower_bound(KeptKey{dev, s, 0}); it != all.end() &&
+       std::get<0>(it->first) == dev && std::get<1>(it->first) == s;) {
+    if (it->second.p) cudaFreeAsync(it->second.p, s);
+    it = all.erase(it);
+  }
+}
 
 u32* stream_zero_scratch(u32 key, size_t words, cudaStream_t s)
 {

@@ -97,6 +97,10 @@ void exscan_jobs(ScanJob const* jobs, u32 njobs, cudaStream_t s);
 // refinement's split domain entities of dimension d).
 enum : u32 { KEPT_ROWS0 = 1, KEPT_ROWS1 = 2, KEPT_MARKS = 3, KEPT_FUSED = 4, KEPT_SPLIT = 8 };
 u32* stream_zero_scratch(u32 key, size_t words, cudaStream_t s);
+// frees (in the order of s) the scan and kept scratch of stream s on the
+// current device; called before a stream is destroyed, so that scratch does
+// not outlive its stream (no kernel may use it afterwards)
+void release_stream_scratch(cudaStream_t s);
 u32* stream_marks(u32 key, size_t words, cudaStream_t s, u32* gen);
 
 // The same scan with caller-provided scratch of at least

@@ -113,6 +113,7 @@ struct Server {
       if (owned[k]) delete ms[k];
     jobs.clear();
     if (run.s) {
+      release_stream_scratch(run.s);
       cudaStreamSynchronize(run.s);
       cudaStreamDestroy(run.s);
     }

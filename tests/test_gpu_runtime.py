@@ -59,3 +59,32 @@ def test_exscan_rejects_overlap():
     p = buf.data_ptr()
     assert L.osh_b200_exscan_u32(p, p + 4 * 10, 50, None, 1) == 4   # OSH_B200_E_ARG
     L.osh_b200_clear_error()
+
+
+def test_released_stream_leaves_meshes_usable():
+    """A mesh adapted on a caller's stream, whose scratch is then released
+    (osh_b200_release_stream) and the stream destroyed, keeps working on
+    another stream, and matches the oracle: the library kept nothing of
+    the released stream. Repeated over several streams, as a caller that
+    makes one per request would."""
+    import torch
+    import omega_h_v1_b200 as G
+    from oracle import oracle as O
+    torch.cuda.set_device(0)
+    L = G.lib()
+    g, o = build_gpu(5, size=0.2), build_cpu(O.Oracle, 5, size=0.2)
+    for _ in range(3):
+        st = torch.cuda.Stream()
+        L.osh_b200_set_stream(g.h, G.C.c_void_p(st.cuda_stream))
+        G.check()
+        qf = min(0.3, o.min_quality())
+        assert g.refine_by_size(qf) == o.refine_by_size(qf)
+        L.osh_b200_set_stream(g.h, G.C.c_void_p(0))
+        G.check()
+        L.osh_b200_release_stream(G.C.c_void_p(st.cuda_stream))
+        G.check()
+        st.synchronize()
+        del st
+    qf = min(0.3, o.min_quality())
+    assert g.coarsen_by_size(qf, 1 / 3.) == o.coarsen_by_size(qf, 1 / 3.)
+    assert not O.mesh_diff(g.snapshot(), o.snapshot())
