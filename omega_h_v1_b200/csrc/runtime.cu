@@ -712,29 +712,35 @@ k_exscan(ScanJobs jobs, unsigned long long* status, u32* ticket_and_err, u32 spi
     if (lane == 0) s_prefix = prefix;
   }
   __syncthreads();
-  u32 run = s_prefix + thread_excl;
-#pragma unroll
-  for (int k = 0; k < SCAN_ITEMS; ++k) {
-    u32 li = threadIdx.x * SCAN_ITEMS + k;
-    s_buf[li + (li >> 5)] = run;
-    run += v[k];
-  }
-  __syncthreads();
   u32* __restrict__ out = job.out;
   u32* __restrict__ newid = job.newid;
   u32* __restrict__ list = job.list;
   u32* __restrict__ comp = job.comp;
   u32* __restrict__ comp_newid = job.comp_newid;
+  // jobs that need each item's mark keep it in bit 31 of its staged prefix
+  // (their prefixes count marked entities: below 2^31), so the store phase
+  // does not read the items again
+  bool const need_on = newid || list || comp_newid;
+  constexpr u32 ON_BIT = 0x80000000u;
+  u32 run = s_prefix + thread_excl;
+#pragma unroll
+  for (int k = 0; k < SCAN_ITEMS; ++k) {
+    u32 li = threadIdx.x * SCAN_ITEMS + k;
+    s_buf[li + (li >> 5)] = run | (need_on && v[k] ? ON_BIT : 0u);
+    run += v[k];
+  }
+  __syncthreads();
 #pragma unroll
   for (int k = 0; k < SCAN_ITEMS; ++k) {
     u32 li = k * SCAN_THREADS + threadIdx.x;
     size_t gi = base + li;
     if (gi < n) {
-      u32 const o = s_buf[li + (li >> 5)];
+      u32 const w = s_buf[li + (li >> 5)];
+      u32 const o = need_on ? w & ~ON_BIT : w;
       out[gi] = o;
       if (comp) comp[gi] = (u32)gi - o;
-      if (newid || list || comp_newid) {
-        bool const on = mode2 ? in[gi] == stamp : !mode1 ? in[gi] != 0 : in[gi + 1] == in[gi];
+      if (need_on) {
+        bool const on = (w & ON_BIT) != 0;
         if (newid) newid[gi] = on ? o : INV;
         if (list && on) list[o] = (u32)gi;
         if (comp_newid) comp_newid[gi] = on ? INV : (u32)gi - o;
