@@ -61,53 +61,83 @@ __global__ void k_coarsen_sliver_codes(u32 ne, u32 const* __restrict__ voe,
 }
 
 // check_basic_edge_class (check_collapse_class.cpp:12-37)
-__global__ void k_check_basic_class(u32 ne, u32 const* __restrict__ voe,
-    u32 const* __restrict__ cdv, u32 const* __restrict__ cde, u32* __restrict__ codes)
+__device__ inline u32 basic_class_code(u32 i, u32 code, u32 const* __restrict__ voe,
+    u32 const* __restrict__ cdv, u32 const* __restrict__ cde)
 {
-  pdl_wait();
-  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= ne) return;
-  u32 code = codes[i];
-  if (code == DONT_COLLAPSE) return;
   u32 c0 = cdv[voe[i * 2]], c1 = cdv[voe[i * 2 + 1]], ce = cde[i];
-  if (c0 == c1) {
-    if (c0 != ce) codes[i] = DONT_COLLAPSE;
-    return;
-  }
+  if (c0 == c1) return c0 != ce ? (u32)DONT_COLLAPSE : code;
   if (collapses(code, 0) && c0 != ce) code &= ~1u;
   if (collapses(code, 1) && c1 != ce) code &= ~2u;
-  codes[i] = code;
+  return code;
 }
 
-// check_for_exposed_side (check_collapse_class.cpp:55-103)
-__global__ void k_check_exposed_sides(u32 ed, u32 ne, u32 const* __restrict__ u_offs,
-    u32 const* __restrict__ u_adj, u32 const* __restrict__ u_dirs,
-    u32 const* __restrict__ vot, u32 const* __restrict__ voe, u32 const* __restrict__ sot,
-    u32 const* __restrict__ cdt, u32 const* __restrict__ cds, u32* __restrict__ codes)
+// check_for_exposed_side (check_collapse_class.cpp:55-103), for the
+// entities of dimension ed around edge i
+struct ExposedSides {
+  u32 ed;
+  u32 const* u_offs;  // up(1, ed)
+  u32 const* u_adj;
+  u32 const* u_dirs;
+  u32 const* vot;     // down(ed, 0)
+  u32 const* sot;     // down(ed, ed - 1)
+  u32 const* cdt;     // class_dim of dimension ed
+  u32 const* cds;     // class_dim of dimension ed - 1
+};
+
+__device__ inline u32 exposed_sides_code(u32 i, u32 code, u32 const* __restrict__ voe,
+    ExposedSides const& x)
 {
-  pdl_wait();
-  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= ne) return;
-  u32 code = codes[i];
-  if (code == DONT_COLLAPSE) return;
-  u32 vpt = deg(ed, 0), spt = deg(ed, ed - 1);
-  for (u32 j = u_offs[i]; j < u_offs[i + 1]; ++j) {
-    u32 t = u_adj[j], dir = u_dirs[j];
-    u32 tcd = cdt[t];
+  u32 const ed = x.ed, vpt = deg(ed, 0), spt = deg(ed, ed - 1);
+  for (u32 j = x.u_offs[i]; j < x.u_offs[i + 1]; ++j) {
+    u32 t = x.u_adj[j], dir = x.u_dirs[j];
+    u32 tcd = x.cdt[t];
     for (u32 k = 0; k < 2; ++k) {
       if (!collapses(code, k)) continue;
       u32 va = voe[i * 2 + (1 - k)];
       for (u32 l = 0; l < 2; ++l) {
         u32 eev = canon(ed, 1, 0, dir, l);
-        if (vot[(size_t)t * vpt + eev] == va) {
-          u32 side = sot[(size_t)t * spt + opp(ed, 0, eev)];
-          if (cds[side] != tcd) code &= ~(1u << k);
+        if (x.vot[(size_t)t * vpt + eev] == va) {
+          u32 side = x.sot[(size_t)t * spt + opp(ed, 0, eev)];
+          if (x.cds[side] != tcd) code &= ~(1u << k);
           break;
         }
       }
     }
   }
-  codes[i] = code;
+  return code;
+}
+
+// The class checks of every edge with a code (the basic check, then the
+// exposed sides for faces, then for elements: nxs of them), the code
+// written back, each edge's collapse qualities zeroed, and the edges still
+// with a code listed (a warp's appends in one counter update): one launch
+// for what were a kernel per check and one for the list
+__global__ void k_coarsen_class_list(u32 ne, u32 const* __restrict__ voe,
+    u32 const* __restrict__ cdv, u32 const* __restrict__ cde, ExposedSides xs0,
+    ExposedSides xs1, u32 nxs, u32* __restrict__ codes, u32* __restrict__ list, u32* count,
+    double2* __restrict__ q2)
+{
+  pdl_wait();
+  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+  bool on = false;
+  if (i < ne) {
+    q2[i] = make_double2(0.0, 0.0);
+    u32 code = codes[i];
+    if (code != DONT_COLLAPSE) {
+      code = basic_class_code(i, code, voe, cdv, cde);
+      if (code != DONT_COLLAPSE && nxs > 0) code = exposed_sides_code(i, code, voe, xs0);
+      if (code != DONT_COLLAPSE && nxs > 1) code = exposed_sides_code(i, code, voe, xs1);
+      codes[i] = code;
+    }
+    on = code != 0;
+  }
+  u32 mask = __ballot_sync(0xffffffffu, on);
+  if (!mask) return;
+  u32 lane = threadIdx.x & 31, leader = __ffs(mask) - 1;
+  u32 base = 0;
+  if (lane == leader) base = atomicAdd(count, (u32)__popc(mask));
+  base = __shfl_sync(0xffffffffu, base, leader);
+  if (on) list[base + __popc(mask & ((1u << lane) - 1u))] = i;
 }
 
 // coarsen_quality (coarsen_qualities.cpp:12-79): worst element of the cavity
@@ -270,22 +300,6 @@ __global__ void k_coarsen_quality(u32 const* __restrict__ list,
 // the candidate edges listed (a warp's candidates take consecutive slots,
 // warps in any order) and every edge's two collapse qualities zeroed (the
 // quality kernel writes the kept ones)
-__global__ void k_list_candidates(u32 n, u32 const* __restrict__ flags, u32* __restrict__ list,
-    u32* count, double2* __restrict__ q2)
-{
-  pdl_wait();
-  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
-  bool on = i < n && flags[i] != 0;
-  if (i < n) q2[i] = make_double2(0.0, 0.0);
-  u32 mask = __ballot_sync(0xffffffffu, on);
-  if (!mask) return;
-  u32 lane = threadIdx.x & 31, leader = __ffs(mask) - 1;
-  u32 base = 0;
-  if (lane == leader) base = atomicAdd(count, (u32)__popc(mask));
-  base = __shfl_sync(0xffffffffu, base, leader);
-  if (on) list[base + __popc(mask & ((1u << lane) - 1u))] = i;
-}
-
 // collapse_to_vert (collapses_to_verts.cpp:13-42)
 __global__ void k_collapses_to_verts(u32 nv, u32 const* __restrict__ ue_offs,
     u32 const* __restrict__ ue, u32 const* __restrict__ ue_dirs,
@@ -733,40 +747,35 @@ static bool coarsen_select(Mesh& m, u32* codes, double qual_floor, bool require_
   Tag* cde = m.find_tag(1, "class_dim");
   if (!cdv || !cde) throw Failure(E_ARG, "coarsening needs class_dim on every dimension");
   u32 const* voe1 = m.ask_down(1, 0);
-  if (ne) {
-    CK(launch_kernel(k_check_basic_class, dim3(grid_for(ne)), dim3(BLOCK), 0, s, ne, voe1,
-        static_cast<u32 const*>(cdv->data), static_cast<u32 const*>(cde->data), codes));
-    CK_LAUNCH();
-  }
+  ExposedSides xs[2] = {};
+  u32 nxs = 0;
   for (u32 ed = 2; ed <= dim; ++ed) {
     UpAdj const& u = m.ask_up(1, ed, false);
     Tag* cdt = m.find_tag(ed, "class_dim");
     Tag* cds = m.find_tag(ed - 1, "class_dim");
     if (!cdt || !cds) throw Failure(E_ARG, "coarsening needs class_dim on every dimension");
-    if (ne) {
-      CK(launch_kernel(k_check_exposed_sides, dim3(grid_for(ne)), dim3(BLOCK), 0, s, ed, ne, u.offs, u.adj, u.dirs,
-          m.ask_down(ed, 0), voe1, m.ask_down(ed, ed - 1),
-          static_cast<u32 const*>(cdt->data), static_cast<u32 const*>(cds->data), codes));
-      CK_LAUNCH();
-    }
+    xs[nxs++] = ExposedSides{ed, u.offs, u.adj, u.dirs, m.ask_down(ed, 0),
+        m.ask_down(ed, ed - 1), static_cast<u32 const*>(cdt->data),
+        static_cast<u32 const*>(cds->data)};
   }
-  if (codes_class_out)
-    CK(cudaMemcpyAsync(codes_class_out, codes, sizeof(u32) * ne, cudaMemcpyDeviceToDevice, s));
-  if (codes_qual_out)
-    CK(cudaMemcpyAsync(codes_qual_out, codes, sizeof(u32) * ne, cudaMemcpyDeviceToDevice, s));
-  // the candidate edges, listed, and the qualities of their collapses; one
-  // read-back (mailbox slots 4 and 7) tells whether any edge was a candidate
-  // and whether any collapse survived
+  // the class checks, the candidate edges listed, and the qualities of
+  // their collapses; one read-back (mailbox slots 4 and 7) tells whether any
+  // edge was a candidate and whether any collapse survived
   u32* clist = dalloc<u32>(ne ? ne : 1, s);
   sel.q2 = dalloc<double>((size_t)ne * 2, s);
   u32* any = m.mb->dev + 4;
   u32* ncand = m.mb->dev + 7;
   CK(cudaMemsetAsync(any, 0, 4 * sizeof(u32), s));  // slots 4-7
   if (ne) {
-    CK(launch_kernel(k_list_candidates, dim3(grid_for(ne)), dim3(BLOCK), 0, s, ne, codes, clist, ncand,
-        reinterpret_cast<double2*>(sel.q2)));
+    CK(launch_kernel(k_coarsen_class_list, dim3(grid_for(ne)), dim3(BLOCK), 0, s, ne, voe1,
+        static_cast<u32 const*>(cdv->data), static_cast<u32 const*>(cde->data), xs[0], xs[1],
+        nxs, codes, clist, ncand, reinterpret_cast<double2*>(sel.q2)));
     CK_LAUNCH();
   }
+  if (codes_class_out)
+    CK(cudaMemcpyAsync(codes_class_out, codes, sizeof(u32) * ne, cudaMemcpyDeviceToDevice, s));
+  if (codes_qual_out)
+    CK(cudaMemcpyAsync(codes_qual_out, codes, sizeof(u32) * ne, cudaMemcpyDeviceToDevice, s));
   if (dim >= 2 && ne) {
     double const* eq = require_better ? m.qualities() : nullptr;
     UpAdj const& ev = m.ask_up(0, dim, false);
