@@ -1293,7 +1293,9 @@ void carry_down_all(Mesh& m, Mesh& out, u32* const* same_of, u32 const* nsame_of
 // half the speed; a warp per 32 rows reading their uses coalesced ran at
 // the same speed as a thread per row; for passes that removed few
 // entities, new ids from a shared-memory table of id buckets, on a grid
-// capped to the blocks that fit with the table, ran 25% slower.)
+// capped to the blocks that fit with the table, ran 25% slower; reading a
+// row as the 16-byte words that hold it, three per array instead of eight
+// loads, took 48 registers and ran 15% slower with fewer blocks resident.)
 __global__ void k_new_ids(u32 n, u32 const* __restrict__ same, u32* __restrict__ newid)
 {
   pdl_wait();
