@@ -12,9 +12,12 @@
 namespace osh {
 
 // refine_candidate (refine.cpp:11-15) fused with measure_edge (size.cpp:57)
+// (optional) list, nlist: the candidates appended, a warp's in one counter
+// update (nlist zero on entry)
 __global__ void k_refine_candidates(u32 ne, u32 const* __restrict__ voe,
     double const* __restrict__ x, double const* __restrict__ h, SegView sv,
-    Fp32Stats* fs, u32* __restrict__ cand, u32* any, u32* zero2)
+    Fp32Stats* fs, u32* __restrict__ cand, u32* any, u32* zero2, u32* __restrict__ list,
+    u32* nlist)
 {
   pdl_wait();
   // (optional) two flags the quality kernel that follows sets, zeroed here
@@ -45,7 +48,15 @@ __global__ void k_refine_candidates(u32 ne, u32 const* __restrict__ voe,
     cand[i] = c;
   }
   if (fs) fp32_count_warp(fs, decided, rechecked, decided && fs->audit, flipped);
-  if (__any_sync(0xffffffffu, c) && (threadIdx.x & 31) == 0) atomicOr(any, 1u);
+  unsigned const want = __ballot_sync(0xffffffffu, c != 0);
+  if (want && (threadIdx.x & 31) == 0) atomicOr(any, 1u);
+  if (list && want) {
+    u32 const lane = threadIdx.x & 31, leader = __ffs(want) - 1;
+    u32 base = 0;
+    if (lane == leader) base = atomicAdd(nlist, (u32)__popc(want));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (c) list[base + __popc(want & ((1u << lane) - 1u))] = i;
+  }
 }
 
 // the two children of element e (split at its edge of direction dir)
@@ -72,8 +83,15 @@ __device__ inline void refine_child(u32 dim, u32 const* __restrict__ ve, u32 dir
 // candidate edge, each lane some of its children, at 105 registers against
 // 82; and one wave of resident blocks striding over the edges, which left
 // the passes with many candidates to the threads that drew the most.)
+//
+// With a list (the candidate kernel's, nlist of them): a grid of the blocks
+// that fit at once strides over the listed edges in block-wide steps (the
+// candidates in order, so each thread draws as many as any other), and the
+// goodness of the other edges was zeroed before. Without one: a thread per
+// edge, its candidacy read from cand.
 template <u32 DIM>
-__global__ void k_refine_quality(u32 ne, u32 const* __restrict__ voe1,
+__global__ void k_refine_quality(u32 ne, u32 const* __restrict__ list,
+    u32 const* __restrict__ nlist, u32 const* __restrict__ voe1,
     u32 const* __restrict__ voe, u32 const* __restrict__ eo_offs,
     u32 const* __restrict__ eo, u32 const* __restrict__ eo_dirs,
     double const* __restrict__ x, double qual_floor, SegView sv, Fp32Stats* fs,
@@ -82,105 +100,110 @@ __global__ void k_refine_quality(u32 ne, u32 const* __restrict__ voe1,
   pdl_wait();
   constexpr u32 dim = DIM;  // the element dimension (2 or 3): loops over
                             // an element's vertices unroll, corners stay in registers
-  u32 i = blockIdx.x * blockDim.x + threadIdx.x;
-  u32 keep = 0;
-  bool decided = false, rechecked = false, audited = false, flipped = false;
-  if (i < ne && cand[i]) {
-    constexpr u32 vpe = deg(dim, 0);
-    double const perfect = dim == 3 ? perfect_tet_quality() : perfect_tri_quality();
-    u32 a = voe1[i * 2], b = voe1[i * 2 + 1];
-    double split[3];
-    // average_element_field: (0 + x_a + x_b) / 2 per component
-    for (u32 c = 0; c < 3; ++c) {
-      double acc = 0;
-      acc += x[a * 3 + c];
-      acc += x[b * 3 + c];
-      split[c] = acc / 2u;
-    }
-    double const fl = seg_floor(sv, a, qual_floor);
-    u32 const f = eo_offs[i], e = eo_offs[i + 1];
-    // filtered: 0 = no decision on estimates, 1 = rejected on them,
-    // 2 = minimum over the children that can hold it
-    int filtered = 0;
-    double minq = 1;
-    if (fs && dim == 3) {
-      float const k6 = tet_k6_f32();
-      float upper = 1.0f;
-      bool upright = true;
-      unsigned long long need = 0;  // children (2 per element) that can hold the minimum
-      bool all = 2 * (e - f) > 64;
-      for (u32 j = f; j < e; ++j) {
-        u32 const* ve = voe + (size_t)eo[j] * vpe;
-        for (u32 k = 0; k < 2; ++k) {
-          double ex[4][3];
-          refine_child(dim, ve, eo_dirs[j], k, x, split, ex);
-          Q32 q = tet_quality_f32(ex, k6);
-          float lo = q32_lo(q);
-          upright = upright && lo > 0.0f;
-          upper = fminf(upper, q32_hi(q));
-          if (lo <= upper && !all) need |= 1ull << (2 * (j - f) + k);
-        }
+  u32 const n = list ? *nlist : ne;
+  for (u32 base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+    u32 const t = base + threadIdx.x;
+    u32 const i = t < n ? (list ? list[t] : t) : 0u;
+    u32 keep = 0;
+    bool decided = false, rechecked = false, audited = false, flipped = false;
+    if (t < n && (list || cand[i])) {
+      constexpr u32 vpe = deg(dim, 0);
+      double const perfect = dim == 3 ? perfect_tet_quality() : perfect_tri_quality();
+      u32 a = voe1[i * 2], b = voe1[i * 2 + 1];
+      double split[3];
+      // average_element_field: (0 + x_a + x_b) / 2 per component
+      for (u32 c = 0; c < 3; ++c) {
+        double acc = 0;
+        acc += x[a * 3 + c];
+        acc += x[b * 3 + c];
+        split[c] = acc / 2u;
       }
-      if (upright && (double)upper < fl) {
-        filtered = 1;
-        decided = true;
-      } else if (upright) {
-        filtered = 2;
-        rechecked = true;
+      double const fl = seg_floor(sv, a, qual_floor);
+      u32 const f = eo_offs[i], e = eo_offs[i + 1];
+      // filtered: 0 = no decision on estimates, 1 = rejected on them,
+      // 2 = minimum over the children that can hold it
+      int filtered = 0;
+      double minq = 1;
+      if (fs && dim == 3) {
+        float const k6 = tet_k6_f32();
+        float upper = 1.0f;
+        bool upright = true;
+        unsigned long long need = 0;  // children (2 per element) that can hold the minimum
+        bool all = 2 * (e - f) > 64;
         for (u32 j = f; j < e; ++j) {
           u32 const* ve = voe + (size_t)eo[j] * vpe;
           for (u32 k = 0; k < 2; ++k) {
-            if (!all && !((need >> (2 * (j - f) + k)) & 1ull)) continue;
             double ex[4][3];
             refine_child(dim, ve, eo_dirs[j], k, x, split, ex);
-            double q = tet_quality(ex, perfect);
-            if (fs->audit) fp32_note_error(fs, tet_quality_f32(ex, k6), q);
+            Q32 q = tet_quality_f32(ex, k6);
+            float lo = q32_lo(q);
+            upright = upright && lo > 0.0f;
+            upper = fminf(upper, q32_hi(q));
+            if (lo <= upper && !all) need |= 1ull << (2 * (j - f) + k);
+          }
+        }
+        if (upright && (double)upper < fl) {
+          filtered = 1;
+          decided = true;
+        } else if (upright) {
+          filtered = 2;
+          rechecked = true;
+          for (u32 j = f; j < e; ++j) {
+            u32 const* ve = voe + (size_t)eo[j] * vpe;
+            for (u32 k = 0; k < 2; ++k) {
+              if (!all && !((need >> (2 * (j - f) + k)) & 1ull)) continue;
+              double ex[4][3];
+              refine_child(dim, ve, eo_dirs[j], k, x, split, ex);
+              double q = tet_quality(ex, perfect);
+              if (fs->audit) fp32_note_error(fs, tet_quality_f32(ex, k6), q);
+              if (q < minq) minq = q;
+            }
+          }
+        }
+        if (filtered && fs->audit) {
+          // the double path's result, every child in order, and every
+          // estimate against its double value
+          audited = true;
+          double m64 = 1;
+          for (u32 j = f; j < e; ++j) {
+            u32 const* ve = voe + (size_t)eo[j] * vpe;
+            for (u32 k = 0; k < 2; ++k) {
+              double ex[4][3];
+              refine_child(dim, ve, eo_dirs[j], k, x, split, ex);
+              double q = tet_quality(ex, perfect);
+              fp32_note_error(fs, tet_quality_f32(ex, k6), q);
+              if (q < m64) m64 = q;
+            }
+          }
+          bool keep64 = !(m64 < fl);
+          flipped = filtered == 1 ? keep64
+                                  : (keep64 != !(minq < fl) || (keep64 && m64 != minq));
+        }
+      }
+      if (!filtered) {
+        for (u32 j = f; j < e; ++j) {
+          u32 const* ve = voe + (size_t)eo[j] * vpe;
+          for (u32 k = 0; k < 2; ++k) {
+            double ex[4][3];
+            refine_child(dim, ve, eo_dirs[j], k, x, split, ex);
+            double q = dim == 3 ? tet_quality(ex, perfect) : tri_quality(ex, 0, perfect);
+            if (!(q > 0)) atomicOr(inverted, 1u);
             if (q < minq) minq = q;
           }
         }
       }
-      if (filtered && fs->audit) {
-        // the double path's result, every child in order, and every
-        // estimate against its double value
-        audited = true;
-        double m64 = 1;
-        for (u32 j = f; j < e; ++j) {
-          u32 const* ve = voe + (size_t)eo[j] * vpe;
-          for (u32 k = 0; k < 2; ++k) {
-            double ex[4][3];
-            refine_child(dim, ve, eo_dirs[j], k, x, split, ex);
-            double q = tet_quality(ex, perfect);
-            fp32_note_error(fs, tet_quality_f32(ex, k6), q);
-            if (q < m64) m64 = q;
-          }
-        }
-        bool keep64 = !(m64 < fl);
-        flipped = filtered == 1 ? keep64
-                                : (keep64 != !(minq < fl) || (keep64 && m64 != minq));
+      if (filtered == 1 || minq < fl) {
+        cand[i] = 0;
+      } else {
+        out[i] = minq;
+        keep = 1;
       }
     }
-    if (!filtered) {
-      for (u32 j = f; j < e; ++j) {
-        u32 const* ve = voe + (size_t)eo[j] * vpe;
-        for (u32 k = 0; k < 2; ++k) {
-          double ex[4][3];
-          refine_child(dim, ve, eo_dirs[j], k, x, split, ex);
-          double q = dim == 3 ? tet_quality(ex, perfect) : tri_quality(ex, 0, perfect);
-          if (!(q > 0)) atomicOr(inverted, 1u);
-          if (q < minq) minq = q;
-        }
-      }
-    }
-    if (filtered == 1 || minq < fl) {
-      cand[i] = 0;
-    } else {
-      out[i] = minq;
-      keep = 1;
-    }
+    // every edge's goodness is written here (with a list: the listed ones)
+    if (t < n && !keep) out[i] = 0.0;
+    if (fs && dim == 3) fp32_count_warp(fs, decided, rechecked, audited, flipped);
+    if (__any_sync(0xffffffffu, keep) && (threadIdx.x & 31) == 0) atomicOr(any, 1u);
   }
-  if (i < ne && !keep) out[i] = 0.0;  // every edge's goodness is written here
-  if (fs && dim == 3) fp32_count_warp(fs, decided, rechecked, audited, flipped);
-  if (__any_sync(0xffffffffu, keep) && (threadIdx.x & 31) == 0) atomicOr(any, 1u);
 }
 
 // refine_node (refine_nodal.cpp:10-25)
@@ -692,8 +715,10 @@ static u32 refine_build(Mesh& m, EdgeSplits const& es, bool deferred, bool unifo
 // deferred (see refine_deferred): the set is returned unchecked, and the
 // build's read-back brings its outcome and the flags
 // zeroed: the candidate kernel already zeroed mailbox slots 1-2
+// list, nlist (optional): the candidates listed by the candidate kernel
 static u32* choose_refinement(Mesh& m, u32* cand, double qual_floor, double** quals_out,
-    bool uniform, bool deferred = false, bool zeroed = false)
+    bool uniform, bool deferred = false, bool zeroed = false, u32 const* list = nullptr,
+    u32 const* nlist = nullptr)
 {
   cudaStream_t s = m.s;
   u32 ne = m.count(1), dim = m.dim;
@@ -710,8 +735,14 @@ static u32* choose_refinement(Mesh& m, u32* cand, double qual_floor, double** qu
       PROBE(P_REFINE_QUALITY, s, 4.0 * (ne + 1) + 8.0 * deg(dim, 1) * nel + 8.0 * ne +
           4.0 * deg(dim, 0) * nel + 24.0 * m.counts[0] + 8.0 * ne + 8.0 * ne);
       u32 const qb = tuned(TK_QUALITY_BLOCK);
-      CK(launch_kernel(dim == 3 ? k_refine_quality<3> : k_refine_quality<2>,
-          dim3(grid_for(ne, qb)), dim3(qb), 0, s, ne, m.ask_down(1, 0),
+      auto kq = dim == 3 ? k_refine_quality<3> : k_refine_quality<2>;
+      u32 grid = grid_for(ne, qb);
+      if (list) {
+        // the listed edges' goodness is written by the kernel, the rest is 0
+        CK(cudaMemsetAsync(q, 0, sizeof(double) * ne, s));
+        grid = std::min(grid, resident_blocks(kq, qb));
+      }
+      CK(launch_kernel(kq, dim3(grid), dim3(qb), 0, s, ne, list, nlist, m.ask_down(1, 0),
           m.ask_down(dim, 0), eo.offs, eo.adj, eo.dirs, m.coords(), qual_floor, m.segview(),
           m.fp32_filter ? fp32_stats_dev() : nullptr, cand, q, any, inverted));
       CK_LAUNCH();
@@ -759,7 +790,7 @@ static bool refine_deferred(Mesh& m)
 }
 
 static u32 refine_common(Mesh& m, u32* cand, double qual_floor, bool uniform,
-    bool zeroed = false)
+    bool zeroed = false, u32 const* list = nullptr, u32 const* nlist = nullptr)
 {
   cudaStream_t s = m.s;
   PassStats& st = last_pass_stats();
@@ -768,7 +799,8 @@ static u32 refine_common(Mesh& m, u32* cand, double qual_floor, bool uniform,
   st.elems_in = m.count(m.dim);
   u32 ne = m.count(1);
   bool const deferred = refine_deferred(m);
-  u32* ind = choose_refinement(m, cand, qual_floor, nullptr, uniform, deferred, zeroed);
+  u32* ind = choose_refinement(m, cand, qual_floor, nullptr, uniform, deferred, zeroed, list,
+      nlist);
   if (!ind) return 0;
   seg_tally(m, 1, ind);
   // the split edges' scan, with their list and the surviving edges' maps
@@ -808,18 +840,29 @@ u32 refine_by_size(Mesh& m, double qual_floor)
   Tag* h = m.find_tag(0, "adapt_size");
   if (!h) throw Failure(E_ARG, "mesh has no adapt_size vertex field");
   u32* cand = dalloc<u32>(ne, s);
+  u32* clist = dalloc<u32>(ne ? ne : 1, s);
+  // mailbox slot 0: the candidates listed; slot 3: any candidate
+  u32* nlist = m.mb->dev + 0;
   u32* any = m.mb->dev + 3;
-  CK(cudaMemsetAsync(any, 0, sizeof(u32), s));
+  CK(cudaMemsetAsync(nlist, 0, 4 * sizeof(u32), s));  // slots 0-3
   if (ne) {
     PROBE(P_REFINE_CANDIDATES, s, 8.0 * ne + 32.0 * m.counts[0] + 4.0 * ne);
     CK(launch_kernel(k_refine_candidates, dim3(grid_for(ne)), dim3(BLOCK), 0, s, ne, m.ask_down(1, 0), m.coords(),
         static_cast<double const*>(h->data), m.segview(),
-        m.fp32_filter ? fp32_stats_dev() : nullptr, cand, any, m.mb->dev + 1));
+        m.fp32_filter ? fp32_stats_dev() : nullptr, cand, any, m.mb->dev + 1, clist, nlist));
     CK_LAUNCH();
   }
   // no separate check for "any candidate": with none, the quality kernel
   // keeps none and refine_common returns 0 after its single read-back
-  u32 r = refine_common(m, cand, qual_floor, false, ne != 0);
+  u32 r = 0;
+  try {
+    r = refine_common(m, cand, qual_floor, false, ne != 0, clist, nlist);
+  } catch (...) {
+    dev_free(clist, s);
+    dev_free(cand, s);
+    throw;
+  }
+  dev_free(clist, s);
   dev_free(cand, s);
   return r;
 }
@@ -846,7 +889,7 @@ u32 refine_sets(Mesh& m, double qual_floor, u32* cand_out, u32* good_out,
   if (ne) {
     CK(launch_kernel(k_refine_candidates, dim3(grid_for(ne)), dim3(BLOCK), 0, s, ne, m.ask_down(1, 0), m.coords(),
         static_cast<double const*>(h->data), m.segview(),
-        m.fp32_filter ? fp32_stats_dev() : nullptr, cand_out, any, nullptr));
+        m.fp32_filter ? fp32_stats_dev() : nullptr, cand_out, any, nullptr, nullptr, nullptr));
     CK_LAUNCH();
   }
   CK(cudaMemcpyAsync(good_out, cand_out, sizeof(u32) * ne, cudaMemcpyDeviceToDevice, s));

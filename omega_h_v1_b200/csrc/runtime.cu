@@ -1,5 +1,6 @@
 // Device runtime for the adaptation pass: error state, stream-ordered
 // allocation, the decoupled look-back exclusive scan and small array kernels.
+#include <algorithm>
 #include <cstdlib>
 #include <dlfcn.h>
 #include <string>
@@ -9,6 +10,7 @@
 #include <atomic>
 #include <map>
 #include <mutex>
+#include <tuple>
 #include <vector>
 
 #include "runtime.hpp"
@@ -848,6 +850,24 @@ KeptScratch& kept_scratch(u32 key, size_t words, cudaStream_t s)
   return sc;
 }
 }  // namespace
+
+u32 resident_blocks_of(void const* kernel, u32 block, size_t smem)
+{
+  static std::mutex mu;
+  static auto* cache = new std::map<std::tuple<void const*, u32, size_t, int>, u32>();
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  auto const key = std::make_tuple(kernel, block, smem, dev);
+  std::lock_guard<std::mutex> g(mu);
+  auto it = cache->find(key);
+  if (it != cache->end()) return it->second;
+  int per_sm = 0, sms = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, (int)block, smem));
+  CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  u32 const n = (u32)std::max(1, per_sm) * (u32)std::max(1, sms);
+  (*cache)[key] = n;
+  return n;
+}
 
 void release_stream_scratch(cudaStream_t s)
 {

@@ -97,6 +97,17 @@ void exscan_jobs(ScanJob const* jobs, u32 njobs, cudaStream_t s);
 // refinement's split domain entities of dimension d).
 enum : u32 { KEPT_ROWS0 = 1, KEPT_ROWS1 = 2, KEPT_MARKS = 3, KEPT_FUSED = 4, KEPT_SPLIT = 8 };
 u32* stream_zero_scratch(u32 key, size_t words, cudaStream_t s);
+
+// blocks of `block` threads (and `smem` bytes of dynamic shared memory) of a
+// kernel resident at once on the current device: the occupancy
+// calculator's blocks per SM times the SMs, computed once per kernel, shape
+// and device (for grids that stride over their work in one wave)
+u32 resident_blocks_of(void const* kernel, u32 block, size_t smem);
+template <class K>
+inline u32 resident_blocks(K kernel, u32 block, size_t smem = 0)
+{
+  return resident_blocks_of(reinterpret_cast<void const*>(kernel), block, smem);
+}
 // frees (in the order of s) the scan and kept scratch of stream s on the
 // current device; called before a stream is destroyed, so that scratch does
 // not outlive its stream (no kernel may use it afterwards)
