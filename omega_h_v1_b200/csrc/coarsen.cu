@@ -956,6 +956,11 @@ static bool coarsen_build(Mesh& m, CoarsenSel const& sel, bool deferred)
   }
   expand_many(vjobs, s);
   if (m.parallel) inherit_globals(*out, 0);
+  // every dimension's label copies launched together after the loop (the
+  // generated lists and offsets they read are freed after that launch)
+  std::vector<ExpandJob> copies;
+  u32* free_after[8] = {};
+  u32 nfree = 0;
   for (u32 dd = 0; dd < dim; ++dd) {
     u32 ed = dim - dd;
     u32 n = m.count(ed), vpe = deg(ed, 0);
@@ -991,13 +996,15 @@ static bool coarsen_build(Mesh& m, CoarsenSel const& sel, bool deferred)
     d.list[ed] = gen_list_of[ed];
     d.nlist[ed] = ngen;
     d.finish();
-    inherit_class(m, *out, ed, d);
-    dev_free(gen_list_of[ed], s);
+    inherit_class(m, *out, ed, d, nullptr, &copies);
+    free_after[nfree++] = gen_list_of[ed];
     if (m.parallel) inherit_globals(*out, ed);
     if (ed == dim) coarsen_transfer(m, *out, gen_offs_v, gen_offs, same_e, nsame, ngen);
-    dev_free(gen_offs, s);
+    free_after[nfree++] = gen_offs;
     nsame_of[ed] = nsame;
   }
+  expand_many(copies, s);
+  for (u32 k = 0; k < nfree; ++k) dev_free(free_after[k], s);
   same_of[0] = same_v;
   nsame_of[0] = nv_out;
   // downward adjacency of the survivors carries over; the products are searched

@@ -13,11 +13,12 @@ namespace osh {
 
 // refine_candidate (refine.cpp:11-15) fused with measure_edge (size.cpp:57)
 // (optional) list, nlist: the candidates appended, a warp's in one counter
-// update (nlist zero on entry)
+// update (nlist zero on entry); zero_q: every edge's goodness zeroed for
+// the quality kernel, which then writes only the listed edges'
 __global__ void k_refine_candidates(u32 ne, u32 const* __restrict__ voe,
     double const* __restrict__ x, double const* __restrict__ h, SegView sv,
     Fp32Stats* fs, u32* __restrict__ cand, u32* any, u32* zero2, u32* __restrict__ list,
-    u32* nlist)
+    u32* nlist, double* __restrict__ zero_q)
 {
   pdl_wait();
   // (optional) two flags the quality kernel that follows sets, zeroed here
@@ -46,6 +47,7 @@ __global__ void k_refine_candidates(u32 ne, u32 const* __restrict__ voe,
     }
     c = c && seg_acts(sv, a);
     cand[i] = c;
+    if (zero_q) zero_q[i] = 0.0;
   }
   if (fs) fp32_count_warp(fs, decided, rechecked, decided && fs->audit, flipped);
   unsigned const want = __ballot_sync(0xffffffffu, c != 0);
@@ -715,14 +717,15 @@ static u32 refine_build(Mesh& m, EdgeSplits const& es, bool deferred, bool unifo
 // deferred (see refine_deferred): the set is returned unchecked, and the
 // build's read-back brings its outcome and the flags
 // zeroed: the candidate kernel already zeroed mailbox slots 1-2
-// list, nlist (optional): the candidates listed by the candidate kernel
+// list, nlist (optional): the candidates listed by the candidate kernel,
+// which also zeroed q_in (the goodness array this call then owns)
 static u32* choose_refinement(Mesh& m, u32* cand, double qual_floor, double** quals_out,
     bool uniform, bool deferred = false, bool zeroed = false, u32 const* list = nullptr,
-    u32 const* nlist = nullptr)
+    u32 const* nlist = nullptr, double* q_in = nullptr)
 {
   cudaStream_t s = m.s;
   u32 ne = m.count(1), dim = m.dim;
-  double* q = dalloc<double>(ne, s);
+  double* q = q_in ? q_in : dalloc<double>(ne, s);
   if (dim < 2) CK(cudaMemsetAsync(q, 0, sizeof(double) * ne, s));
   u32* any = m.mb->dev + 1;
   u32* inverted = m.mb->dev + 2;
@@ -739,7 +742,7 @@ static u32* choose_refinement(Mesh& m, u32* cand, double qual_floor, double** qu
       u32 grid = grid_for(ne, qb);
       if (list) {
         // the listed edges' goodness is written by the kernel, the rest is 0
-        CK(cudaMemsetAsync(q, 0, sizeof(double) * ne, s));
+        if (!q_in) CK(cudaMemsetAsync(q, 0, sizeof(double) * ne, s));
         grid = std::min(grid, resident_blocks(kq, qb));
       }
       CK(launch_kernel(kq, dim3(grid), dim3(qb), 0, s, ne, list, nlist, m.ask_down(1, 0),
@@ -790,7 +793,8 @@ static bool refine_deferred(Mesh& m)
 }
 
 static u32 refine_common(Mesh& m, u32* cand, double qual_floor, bool uniform,
-    bool zeroed = false, u32 const* list = nullptr, u32 const* nlist = nullptr)
+    bool zeroed = false, u32 const* list = nullptr, u32 const* nlist = nullptr,
+    double* q_in = nullptr)
 {
   cudaStream_t s = m.s;
   PassStats& st = last_pass_stats();
@@ -800,7 +804,7 @@ static u32 refine_common(Mesh& m, u32* cand, double qual_floor, bool uniform,
   u32 ne = m.count(1);
   bool const deferred = refine_deferred(m);
   u32* ind = choose_refinement(m, cand, qual_floor, nullptr, uniform, deferred, zeroed, list,
-      nlist);
+      nlist, q_in);
   if (!ind) return 0;
   seg_tally(m, 1, ind);
   // the split edges' scan, with their list and the surviving edges' maps
@@ -841,6 +845,9 @@ u32 refine_by_size(Mesh& m, double qual_floor)
   if (!h) throw Failure(E_ARG, "mesh has no adapt_size vertex field");
   u32* cand = dalloc<u32>(ne, s);
   u32* clist = dalloc<u32>(ne ? ne : 1, s);
+  // the edges' goodness, zeroed by the candidate kernel; refine_common's
+  // selection owns it from there
+  double* q = m.dim >= 2 ? dalloc<double>(ne ? ne : 1, s) : nullptr;
   // mailbox slot 0: the candidates listed; slot 3: any candidate
   u32* nlist = m.mb->dev + 0;
   u32* any = m.mb->dev + 3;
@@ -849,14 +856,14 @@ u32 refine_by_size(Mesh& m, double qual_floor)
     PROBE(P_REFINE_CANDIDATES, s, 8.0 * ne + 32.0 * m.counts[0] + 4.0 * ne);
     CK(launch_kernel(k_refine_candidates, dim3(grid_for(ne)), dim3(BLOCK), 0, s, ne, m.ask_down(1, 0), m.coords(),
         static_cast<double const*>(h->data), m.segview(),
-        m.fp32_filter ? fp32_stats_dev() : nullptr, cand, any, m.mb->dev + 1, clist, nlist));
+        m.fp32_filter ? fp32_stats_dev() : nullptr, cand, any, m.mb->dev + 1, clist, nlist, q));
     CK_LAUNCH();
   }
   // no separate check for "any candidate": with none, the quality kernel
   // keeps none and refine_common returns 0 after its single read-back
   u32 r = 0;
   try {
-    r = refine_common(m, cand, qual_floor, false, ne != 0, clist, nlist);
+    r = refine_common(m, cand, qual_floor, false, ne != 0, clist, nlist, q);
   } catch (...) {
     dev_free(clist, s);
     dev_free(cand, s);
@@ -889,7 +896,8 @@ u32 refine_sets(Mesh& m, double qual_floor, u32* cand_out, u32* good_out,
   if (ne) {
     CK(launch_kernel(k_refine_candidates, dim3(grid_for(ne)), dim3(BLOCK), 0, s, ne, m.ask_down(1, 0), m.coords(),
         static_cast<double const*>(h->data), m.segview(),
-        m.fp32_filter ? fp32_stats_dev() : nullptr, cand_out, any, nullptr, nullptr, nullptr));
+        m.fp32_filter ? fp32_stats_dev() : nullptr, cand_out, any, nullptr, nullptr, nullptr,
+        nullptr));
     CK_LAUNCH();
   }
   CK(cudaMemcpyAsync(good_out, cand_out, sizeof(u32) * ne, cudaMemcpyDeviceToDevice, s));
